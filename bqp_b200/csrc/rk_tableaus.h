@@ -1,0 +1,47 @@
+// Generated by gen_tableaus.py -- do not edit by hand.
+// Explicit Runge-Kutta pairs used by the propagator (see gen_tableaus.py
+// for the published sources of each table).
+#pragma once
+#ifndef BQP_TAB_CONST
+#define BQP_TAB_CONST static const
+#endif
+
+// dopri5: 7 stages, order 5, error order 4
+#define BQP_DOPRI5_STAGES 7
+#define BQP_DOPRI5_ORDER_ERR 4
+#define BQP_DOPRI5_FSAL 1
+BQP_TAB_CONST double bqp_dopri5_c[7] = {0.0, 0x1.999999999999ap-3, 0x1.3333333333333p-2, 0x1.999999999999ap-1, 0x1.c71c71c71c71cp-1, 0x1.0000000000000p+0, 0x1.0000000000000p+0};
+BQP_TAB_CONST double bqp_dopri5_a[49] = {
+  0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.999999999999ap-3, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.3333333333333p-4, 0x1.ccccccccccccdp-3, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.f49f49f49f49fp-1, -0x1.ddddddddddddep+1, 0x1.c71c71c71c71cp+1, 0.0, 0.0, 0.0, 0.0,
+  0x1.79eec0fc37181p+1, -0x1.7310bd29520e4p+3, 0x1.3a552363c5290p+3, -0x1.29c9eba1e3345p-2, 0.0, 0.0, 0.0,
+  0x1.6c52bf5a814b0p+1, -0x1.583e0f83e0f84p+3, 0x1.1d016a3721e8bp+3, 0x1.1d1745d1745d1p-2, -0x1.1818970d9cc2fp-2, 0.0, 0.0,
+  0x1.7555555555555p-4, 0.0, 0x1.cc0499a5605fbp-2, 0x1.4d55555555555p-1, -0x1.4a1cfb2b78c13p-2, 0x1.0c30c30c30c31p-3, 0.0,
+};
+BQP_TAB_CONST double bqp_dopri5_b[7] = {0x1.7555555555555p-4, 0.0, 0x1.cc0499a5605fbp-2, 0x1.4d55555555555p-1, -0x1.4a1cfb2b78c13p-2, 0x1.0c30c30c30c31p-3, 0.0};
+BQP_TAB_CONST double bqp_dopri5_e[7] = {0x1.4320fedcba980p-10, 0.0, -0x1.16b5a550abfc0p-8, 0x1.2eeeeeeeeeef0p-5, -0x1.a0ad1d2ca1858p-5, 0x1.5748a7bdaf0e4p-5, -0x1.999999999999ap-6};
+
+// dop853: 12 stages, order 8, error order 5
+#define BQP_DOP853_STAGES 12
+#define BQP_DOP853_ORDER_ERR 5
+#define BQP_DOP853_FSAL 0
+BQP_TAB_CONST double bqp_dop853_c[12] = {0.0, 0x1.aee6838dae63ap-5, 0x1.432ce2aa42cacp-4, 0x1.e4c353ff64302p-4, 0x1.2068c499c08d9p-2, 0x1.5555555555555p-2, 0x1.0000000000000p-2, 0x1.3b13b13b13b14p-2, 0x1.4d74d74d74d75p-1, 0x1.3333333333333p-1, 0x1.b6db6db6db6dbp-1, 0x1.0000000000000p+0};
+BQP_TAB_CONST double bqp_dop853_a[144] = {
+  0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.aee6838dae63ap-5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.432ce2aa42cacp-6, 0x1.e4c353ff64302p-5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.e4c353ff64302p-6, 0.0, 0x1.6b927eff8b241p-4, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.ee50d7ecde9fap-3, 0.0, -0x1.c4e3ab5ad1507p-1, 0x1.d983d7ac79ef5p-1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.2f684bda12f68p-5, 0.0, 0.0, 0x1.5ddb63bdb6d36p-3, 0x1.00f533f66f19ap-3, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.3000000000000p-5, 0.0, 0.0, 0x1.5cad30f3347edp-3, 0x1.ed4b3c332e04dp-5, -0x1.2000000000000p-6, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.2fdb8fee78792p-5, 0.0, 0.0, 0x1.5cf23f6595d72p-3, 0x1.b758640dea698p-4, -0x1.f5fcc20fcd32fp-7, 0x1.0f1d92efb0b71p-7, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.3f8b78b985813p-1, 0.0, 0.0, -0x1.ae31bacc6bc8ap+1, -0x1.bc873f08e11f9p-1, 0x1.b9793d88d1855p+4, 0x1.42770f892ad69p+4, -0x1.5beb4865c42f9p+5, 0.0, 0.0, 0.0, 0.0,
+  0x1.e9205e321b655p-2, 0.0, 0.0, -0x1.3e7a8a34bd27fp+1, -0x1.2e3a9968c93c8p-1, 0x1.53ae4a6d655eep+4, 0x1.e8ef7b5f258b8p+3, -0x1.0a4e418d711b9p+5, -0x1.4d1b3d9b4a876p-6, 0.0, 0.0, 0.0,
+  -0x1.dfd121f1d399bp-1, 0.0, 0.0, 0x1.4bed869fb0b9dp+2, 0x1.1768702792ea9p+0, -0x1.04cb0e2110c1cp+3, -0x1.2852305e975a8p+4, 0x1.6bd4f06cb863ap+4, 0x1.3f2e777cf109dp+1, -0x1.85fc60d2b572cp+1, 0.0, 0.0,
+  0x1.22fbd3b09fcdcp+1, 0.0, 0.0, -0x1.511a963cafe55p+3, -0x1.001c935ac72acp+1, -0x1.1f57c8eff3006p+4, 0x1.bf2ea18b58a01p+4, -0x1.6df3a7d1cec13p+1, -0x1.1bee71a9f33a9p+3, 0x1.8b89c42c81861p+3, 0x1.496ac6253e202p-1, 0.0,
+};
+BQP_TAB_CONST double bqp_dop853_b[12] = {0x1.bcc6368d1177cp-5, 0.0, 0.0, 0.0, 0.0, 0x1.1cd1ed2ad5ae2p+2, 0x1.e43a845d5ab9fp+0, -0x1.7346ecf96af43p+2, 0x1.3ea1df2f0eb98p-2, -0x1.37a028f43b002p-3, 0x1.9c657697fe72dp-3, 0x1.6e44f50ab6bc2p-5};
+BQP_TAB_CONST double bqp_dop853_e[12] = {0x1.adeaea1607e1ap-7, 0.0, 0.0, 0.0, 0.0, -0x1.39a3da55ab5c3p+0, -0x1.fba83bede8a72p-2, 0x1.aa149f7eda509p+0, -0x1.66bc9b10e7e71p-2, 0x1.56330d0783989p-2, 0x1.4f8eb54a31435p-4, -0x1.6e44f50ab6bc2p-6};
+BQP_TAB_CONST double bqp_dop853_e3[12] = {-0x1.84b641fbfa1f1p-3, 0.0, 0.0, 0.0, 0.0, 0x1.1cd1ed2ad5ae2p+2, 0x1.e43a845d5ab9fp+0, -0x1.7346ecf96af43p+2, -0x1.b0d3a26abb716p-2, -0x1.37a028f43b002p-3, 0x1.9c657697fe72dp-3, 0x1.732080ac040edp-6};

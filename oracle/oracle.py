@@ -1,0 +1,186 @@
+"""ctypes wrapper around the CPU oracle (oracle/prop_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: tests/, ``__graft_entry__.smoke()`` and bench.py's
+CPU-baseline leg use this module as the checker.  The product package
+(``bqp_b200``) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libprop_oracle.so"
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_long)
+
+METHOD = {"dopri5": 0, "dop853": 1, "dopri5_compat": 2}
+
+
+def build(force: bool = False) -> Path:
+    src = HERE / "prop_oracle.cpp"
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB_PATH))
+        L.orc_force_new.restype = C.c_void_p
+        L.orc_force_new.argtypes = [C.c_char_p, _dp]
+        L.orc_force_free.argtypes = [C.c_void_p]
+        L.orc_field_dense.argtypes = [C.c_void_p, _dp, _dp]
+        L.orc_gravity_itrs.argtypes = [C.c_void_p, C.c_long, _dp, _dp]
+        L.orc_gmst.restype = C.c_double
+        L.orc_gmst.argtypes = [C.c_double]
+        L.orc_eci2equinoc.argtypes = [_dp, _dp]
+        L.orc_equinoc2eci.argtypes = [_dp, C.c_double, _dp]
+        L.orc_sun_moon.argtypes = [C.c_double, _dp, _dp]
+        L.orc_jb2008.restype = C.c_double
+        L.orc_jb2008.argtypes = [_dp]
+        L.orc_geodetic_altitude_km.restype = C.c_double
+        L.orc_geodetic_altitude_km.argtypes = [_dp, C.c_double]
+        L.orc_rhs.argtypes = [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_double, _dp, _dp]
+        L.orc_propagate_final_batch.argtypes = [C.c_void_p, _dp, C.c_long, _dp, _dp, _dp, _dp,
+                                                _dp, _ip, _lp, _lp, C.c_int]
+        L.orc_propagate_sampled.restype = C.c_int
+        L.orc_propagate_sampled.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, _dp, C.c_int, _dp, _lp, _ip]
+        L.orc_integrate_segment.restype = C.c_int
+        L.orc_integrate_segment.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, _dp, _lp]
+        _lib = L
+    return _lib
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Force:
+    """A force model: gravity field (normalised ``deg ord C S`` text) plus switches."""
+
+    def __init__(self, coeff_text: str, order: int, drag=False, sun=False, moon=False,
+                 earth_radius=6378.137, omega=7.292115e-5, mu_sun=1.32712440018e11,
+                 mu_moon=4902.800066, drivers=(150.0,) * 8 + (0.0,)):
+        cfg = f64([order, int(drag), int(sun), int(moon), earth_radius, omega, mu_sun, mu_moon,
+                   *drivers])
+        self.order = order
+        self.h = lib().orc_force_new(coeff_text.encode(), _d(cfg))
+        if not self.h:
+            raise ValueError("oracle: coefficient text rejected")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_force_free(self.h)
+            self.h = None
+
+    def dense(self):
+        st = self.order + 2
+        c = np.zeros(st * st)
+        s = np.zeros(st * st)
+        lib().orc_field_dense(self.h, _d(c), _d(s))
+        return c.reshape(st, st), s.reshape(st, st)
+
+    def gravity_itrs(self, pos_km: np.ndarray) -> np.ndarray:
+        p = f64(pos_km).reshape(-1, 3)
+        out = np.zeros_like(p)
+        lib().orc_gravity_itrs(self.h, p.shape[0], _d(p), _d(out))
+        return out
+
+    def rhs(self, eq, t0, jd0, am, cd, t, delta):
+        eq = f64(eq)
+        delta = f64(delta)
+        out = np.zeros(6)
+        lib().orc_rhs(self.h, _d(eq), t0, jd0, am, cd, t, _d(delta), _d(out))
+        return out
+
+
+def ctrl(method="dop853", eps=1e-8, rtol=None, atol=None, dt_max=300.0, max_steps=500000):
+    scaled = rtol is not None
+    return f64([METHOD[method], 1 if scaled else 0, eps, rtol or 0.0, atol or 0.0, dt_max,
+                max_steps])
+
+
+def propagate_final_batch(force: Force, ctl, eq0, epoch_jd, tf, ballistic, threads=0):
+    eq0 = f64(eq0).reshape(-1, 6)
+    n = eq0.shape[0]
+    epoch_jd = f64(np.broadcast_to(epoch_jd, (n,)))
+    tf = f64(np.broadcast_to(tf, (n,)))
+    ballistic = f64(np.broadcast_to(ballistic, (n, 2)))
+    out = np.zeros((n, 6))
+    status = np.zeros(n, dtype=np.int32)
+    steps = np.zeros(n, dtype=np.int64)
+    evals = np.zeros(n, dtype=np.int64)
+    lib().orc_propagate_final_batch(force.h, _d(f64(ctl)), n, _d(eq0), _d(epoch_jd), _d(tf),
+                                    _d(ballistic), _d(out), status.ctypes.data_as(_ip),
+                                    steps.ctypes.data_as(_lp), evals.ctypes.data_as(_lp),
+                                    int(threads))
+    return out, status, steps, evals
+
+
+def propagate_sampled(force: Force, ctl, eq0, epoch_jd, tf, am, cd, t_eval):
+    t_eval = f64(t_eval)
+    out = np.full((t_eval.size, 6), np.nan)
+    se = np.zeros(2, dtype=np.int64)
+    nw = C.c_int(0)
+    st = lib().orc_propagate_sampled(force.h, _d(f64(ctl)), _d(f64(eq0)), epoch_jd, tf, am, cd,
+                                     _d(t_eval), t_eval.size, _d(out), se.ctypes.data_as(_lp),
+                                     C.byref(nw))
+    return out, st, int(se[0]), int(se[1]), nw.value
+
+
+def integrate_segment(force: Force, ctl, eq, jd0, am, cd, t0, tf):
+    y = np.zeros(6)
+    se = np.zeros(2, dtype=np.int64)
+    st = lib().orc_integrate_segment(force.h, _d(f64(ctl)), _d(f64(eq)), jd0, am, cd, t0, tf,
+                                     _d(y), se.ctypes.data_as(_lp))
+    return y, st, int(se[0]), int(se[1])
+
+
+def eci2equinoc(eci):
+    out = np.zeros(6)
+    rc = lib().orc_eci2equinoc(_d(f64(eci)), _d(out))
+    return out, rc
+
+
+def equinoc2eci(eq, tof):
+    out = np.zeros(6)
+    rc = lib().orc_equinoc2eci(_d(f64(eq)), tof, _d(out))
+    return out, rc
+
+
+def gmst(jd):
+    return lib().orc_gmst(jd)
+
+
+def sun_moon(jd):
+    s = np.zeros(3)
+    m = np.zeros(3)
+    lib().orc_sun_moon(jd, _d(s), _d(m))
+    return s, m
+
+
+def jb2008(inputs14) -> float:
+    return lib().orc_jb2008(_d(f64(inputs14)))
+
+
+def geodetic_altitude_km(pos_km, a=6378.137) -> float:
+    return lib().orc_geodetic_altitude_km(_d(f64(pos_km)), a)
