@@ -1,0 +1,272 @@
+"""ctypes binding of libbqp_b200.so (the C ABI in include/bqp_prop.h).
+
+The library is built in-tree (``python -m bqp_b200.build``).  Loading fails
+loudly when it is missing: there is no CPU fallback for the propagator.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+
+# per-trajectory status codes (BQP_ST_*)
+STATUS_NAMES = {
+    0: "ok", 1: "max_steps_exceeded", 2: "step_underflow", 3: "invalid_input",
+    4: "non_finite_state", 5: "max_rejects_exceeded", 6: "gravity_invalidradius",
+    7: "rebase_failed", 8: "restart_budget_exhausted", 9: "ground", 10: "watchdog",
+}
+ST_OK, ST_GROUND, ST_GRAVITY_RADIUS = 0, 9, 6
+
+FORCE_DRAG, FORCE_SRP, FORCE_SUN, FORCE_MOON = 1, 2, 4, 8
+METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2}
+
+E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5
+
+
+class ForceConfig(C.Structure):
+    """Mirror of ``bqp_force_config``."""
+    _fields_ = [
+        ("order", C.c_int32), ("force_flags", C.c_int32), ("atm_model", C.c_int32),
+        ("method", C.c_int32), ("error_control", C.c_int32), ("ground_check", C.c_int32),
+        ("eps", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("dt_max", C.c_double),
+        ("am_ratio", C.c_double), ("cd", C.c_double), ("earth_radius", C.c_double),
+        ("omega_earth", C.c_double), ("mu_sun", C.c_double), ("mu_moon", C.c_double),
+        ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
+        ("max_kernel_seconds", C.c_double),
+    ]
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+# (name, restype, argtypes) of every exported symbol of include/bqp_prop.h
+SIGNATURES = [
+    ("bqp_force_config_default", None, [C.POINTER(ForceConfig)]),
+    ("bqp_last_error", C.c_char_p, []),
+    ("bqp_ctx_create", C.c_int, [C.c_char_p, C.c_int64, C.POINTER(ForceConfig), C.POINTER(_vp)]),
+    ("bqp_ctx_destroy", C.c_int, [_vp]),
+    ("bqp_ctx_set_stream", C.c_int, [_vp, _vp]),
+    ("bqp_ctx_info", C.c_int, [_vp, _lp]),
+    ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
+    ("bqp_gravity_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _ip]),
+    ("bqp_gravity_eval_device", C.c_int, [_vp, C.c_int64, _vp, _vp, _vp]),
+    ("bqp_rhs_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("bqp_rhs_eval_device", C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("bqp_propagate_final", C.c_int, [_vp, C.c_int64, _dp, C.c_int32, _dp, C.c_double, _dp, _dp, _dp,
+                                      _ip, _lp, _lp]),
+    ("bqp_propagate_final_device", C.c_int, [_vp, C.c_int64, _vp, C.c_int32, _vp, C.c_double, _vp, _vp,
+                                             _vp, _vp, _vp, _vp]),
+    ("bqp_propagate_sampled", C.c_int, [_vp, C.c_int64, _dp, C.c_int32, _dp, C.c_double, _dp, C.c_int32,
+                                        _dp, C.c_int32, _dp, _ip, _lp, _lp]),
+    ("bqp_propagate_sampled_device", C.c_int, [_vp, C.c_int64, _vp, C.c_int32, _vp, C.c_double, _vp,
+                                               C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp]),
+    ("bqp_eci_to_equinoctial", C.c_int, [C.c_int64, _dp, _dp, _ip]),
+    ("bqp_equinoctial_to_eci", C.c_int, [C.c_int64, _dp, _dp, _dp]),
+    ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),
+    ("bqp_eci_to_kep", C.c_int, [C.c_int64, _dp, _dp]),
+]
+
+
+def lib():
+    """Load (building first if stale) the native library."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            try:
+                _build.build()
+            except Exception as exc:  # no nvcc here: use the shipped build if present
+                if not LIB_PATH.exists():
+                    raise ImportError(f"libbqp_b200.so is missing and could not be built: {exc}")
+            if not LIB_PATH.exists():
+                raise ImportError(f"libbqp_b200.so not found at {LIB_PATH}")
+            L = C.CDLL(str(LIB_PATH))
+            for name, res, args in SIGNATURES:
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().bqp_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise NativeError(rc, last_error())
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+def lptr(a: np.ndarray):
+    return a.ctypes.data_as(_lp)
+
+
+def f64(a, shape=None) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        out = out.reshape(shape)
+    return out
+
+
+def default_config() -> ForceConfig:
+    cfg = ForceConfig()
+    lib().bqp_force_config_default(C.byref(cfg))
+    return cfg
+
+
+class Context:
+    """Owns one native propagator context (device field table + settings)."""
+
+    def __init__(self, coeff_text: str, cfg: ForceConfig):
+        self._h = _vp()
+        raw = coeff_text.encode()
+        check(lib().bqp_ctx_create(raw, len(raw), C.byref(cfg), C.byref(self._h)))
+        self.cfg = cfg
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().bqp_ctx_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        out = np.zeros(4, dtype=np.int64)
+        check(lib().bqp_ctx_info(self._h, lptr(out)))
+        return {"order": int(out[0]), "cells": int(out[1]), "table_bytes": int(out[2]),
+                "table_in_shared_memory": bool(out[3])}
+
+    def set_config(self, cfg: ForceConfig):
+        check(lib().bqp_ctx_set_config(self._h, C.byref(cfg)))
+        self.cfg = cfg
+
+    def set_stream(self, stream_ptr: int):
+        check(lib().bqp_ctx_set_stream(self._h, _vp(stream_ptr)))
+
+    # ---------------------------------------------------------------- host
+    def gravity(self, pos_km):
+        p = f64(pos_km).reshape(-1, 3)
+        acc = np.empty_like(p)
+        st = np.empty(p.shape[0], dtype=np.int32)
+        check(lib().bqp_gravity_eval(self._h, p.shape[0], dptr(p), dptr(acc), iptr(st)))
+        return acc, st
+
+    def rhs(self, equ, seg_t0, epoch_jd, t, delta, ballistic=None):
+        equ = f64(equ).reshape(-1, 6)
+        n = equ.shape[0]
+        seg_t0 = f64(np.broadcast_to(seg_t0, (n,)))
+        epoch_jd = f64(np.broadcast_to(epoch_jd, (n,)))
+        t = f64(np.broadcast_to(t, (n,)))
+        delta = f64(delta).reshape(n, 6)
+        bal = None if ballistic is None else f64(np.broadcast_to(ballistic, (n, 2)))
+        out = np.empty((n, 6))
+        check(lib().bqp_rhs_eval(self._h, n, dptr(equ), dptr(seg_t0), dptr(epoch_jd), dptr(t), dptr(delta),
+                                 None if bal is None else dptr(bal), dptr(out)))
+        return out
+
+    def propagate_final(self, states, epoch_jd, tf, t0=0.0, ballistic=None, equinoctial=False):
+        s = f64(states).reshape(-1, 6)
+        n = s.shape[0]
+        ep = f64(np.broadcast_to(epoch_jd, (n,)))
+        tfa = f64(np.broadcast_to(tf, (n,)))
+        bal = None if ballistic is None else f64(np.broadcast_to(ballistic, (n, 2)))
+        out = np.empty((n, 6))
+        st = np.empty(n, dtype=np.int32)
+        steps = np.empty(n, dtype=np.int64)
+        evals = np.empty(n, dtype=np.int64)
+        check(lib().bqp_propagate_final(self._h, n, dptr(s), int(equinoctial), dptr(ep), float(t0), dptr(tfa),
+                                        None if bal is None else dptr(bal), dptr(out), iptr(st), lptr(steps),
+                                        lptr(evals)))
+        return out, st, steps, evals
+
+    def propagate_sampled(self, states, epoch_jd, tf, t_eval, t0=0.0, deltas=False, equinoctial=False):
+        s = f64(states).reshape(-1, 6)
+        n = s.shape[0]
+        ep = f64(np.broadcast_to(epoch_jd, (n,)))
+        tfa = f64(np.broadcast_to(tf, (n,)))
+        te = f64(t_eval).reshape(-1)
+        out = np.empty((n, te.size, 6))
+        st = np.empty(n, dtype=np.int32)
+        steps = np.empty(n, dtype=np.int64)
+        evals = np.empty(n, dtype=np.int64)
+        check(lib().bqp_propagate_sampled(self._h, n, dptr(s), int(equinoctial), dptr(ep), float(t0), dptr(tfa),
+                                          te.size, dptr(te), int(deltas), dptr(out), iptr(st), lptr(steps),
+                                          lptr(evals)))
+        return out, st, steps, evals
+
+    # -------------------------------------------------------------- device
+    def propagate_final_device(self, d_in, d_epoch, d_tf, d_out, d_status, d_steps=None, d_evals=None,
+                               n=None, t0=0.0, d_ballistic=None, equinoctial=False):
+        """Device-pointer variant: arguments are raw CUDA addresses (ints)."""
+        check(lib().bqp_propagate_final_device(self._h, int(n), _vp(d_in), int(equinoctial), _vp(d_epoch),
+                                               float(t0), _vp(d_tf), _vp(d_ballistic) if d_ballistic else None,
+                                               _vp(d_out), _vp(d_status), _vp(d_steps) if d_steps else None,
+                                               _vp(d_evals) if d_evals else None))
+
+    def gravity_device(self, n, d_pos, d_acc, d_status=None):
+        check(lib().bqp_gravity_eval_device(self._h, int(n), _vp(d_pos), _vp(d_acc),
+                                            _vp(d_status) if d_status else None))
+
+
+# ----------------------------------------------------------- host helpers
+def eci_to_equinoctial(eci):
+    e = f64(eci).reshape(-1, 6)
+    out = np.empty_like(e)
+    ok = np.empty(e.shape[0], dtype=np.int32)
+    check(lib().bqp_eci_to_equinoctial(e.shape[0], dptr(e), dptr(out), iptr(ok)))
+    return out, ok.astype(bool)
+
+
+def equinoctial_to_eci(equ, tof=0.0):
+    e = f64(equ).reshape(-1, 6)
+    t = f64(np.broadcast_to(tof, (e.shape[0],)))
+    out = np.empty_like(e)
+    check(lib().bqp_equinoctial_to_eci(e.shape[0], dptr(e), dptr(t), dptr(out)))
+    return out
+
+
+def kep_to_eci(kep):
+    k = f64(kep).reshape(-1, 6)
+    out = np.empty_like(k)
+    check(lib().bqp_kep_to_eci(k.shape[0], dptr(k), dptr(out)))
+    return out
+
+
+def eci_to_kep(eci):
+    e = f64(eci).reshape(-1, 6)
+    out = np.empty_like(e)
+    check(lib().bqp_eci_to_kep(e.shape[0], dptr(e), dptr(out)))
+    return out

@@ -1,0 +1,274 @@
+"""The ``dust_transfer`` propagator surface, on the B200 propagator.
+
+Same names, keyword arguments, defaults, dict keys and exceptions as the
+reference binding (dust_transfer/src/lib.rs:200-438 and
+python/dust_transfer/__init__.py):
+
+    propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True,
+              srp=True, sun=True, moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3,
+              tol=1e-8, dt_max_s=300.0, method="vern7") -> dict
+    propagate_final(...) -> np.ndarray (6,)
+    kep_to_eci(kep) / eci_to_kep(eci)
+
+plus batch entry points (the reference's Rust batch/session APIs, which the
+Python binding does not expose): ``propagate_batch_final`` and
+``propagate_batch_sampled``.
+
+Options this build does not implement raise ``ValueError`` naming the option
+(SRP with binary eclipse; the vern7/vern9/tsit5/rkv98 tableaus); they are never
+silently replaced.  ``gravity_field`` (extra keyword) takes a normalised
+``deg ord C S`` text or a path, which lifts the embedded field's degree-15 cap.
+"""
+from __future__ import annotations
+
+import hashlib
+import time
+from collections import OrderedDict
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+MU_EARTH_KM3_S2 = 398600.4415
+SEC_PER_DAY = 86400.0
+MAX_GRAVITY_ORDER = 15  # embedded DIR-R6 field (lib.rs:53)
+DATA = Path(__file__).resolve().parent / "data"
+_DEFAULT_FIELD = DATA / "dir_r6_d15.txt"
+
+_UNBUILT_METHODS = ("vern7", "vern9", "tsit5", "rkv98")
+_METHODS = {"dop853": N.METHODS["dop853"], "dopri5": N.METHODS["dopri5"],
+            "dopri5_solver": N.METHODS["dopri5_solver"]}
+
+
+def _six(value, what):
+    try:
+        v = np.asarray(value, dtype=np.float64).reshape(-1)
+    except (TypeError, ValueError):
+        raise ValueError(f"{what} must be a sequence of 6 floats") from None
+    if v.size != 6:
+        raise ValueError(f"{what} must have exactly 6 elements")
+    if not np.all(np.isfinite(v)):
+        raise ValueError(f"{what} contains a non-finite value")
+    return v
+
+
+def _field_text(gravity_field) -> tuple[str, bool]:
+    if gravity_field is None:
+        return _DEFAULT_FIELD.read_text(), True
+    if isinstance(gravity_field, Path) or (isinstance(gravity_field, str) and "\n" not in gravity_field
+                                           and Path(gravity_field).exists()):
+        return Path(gravity_field).read_text(), False
+    if isinstance(gravity_field, str):
+        return gravity_field, False
+    raise ValueError("gravity_field must be coefficient text or a path")
+
+
+def force_config(gravity_order=5, drag=True, srp=True, sun=True, moon=True, atm_model=7, am_ratio=0.01,
+                 cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7", embedded=True,
+                 rtol=None, atol=None, jb_drivers=None, ground_check=False) -> N.ForceConfig:
+    """The reference's force_config() (lib.rs:128-190) onto bqp_force_config."""
+    limit = MAX_GRAVITY_ORDER if embedded else 128
+    if not (isinstance(gravity_order, (int, np.integer)) and 1 <= gravity_order <= limit):
+        raise ValueError(f"gravity_order must be in 1..={limit}, got {gravity_order}")
+    if not (np.isfinite(am_ratio) and am_ratio > 0 and np.isfinite(cd) and cd > 0 and np.isfinite(cr) and cr >= 0):
+        raise ValueError("am_ratio and cd must be finite and > 0, cr finite and >= 0")
+    if not (np.isfinite(tol) and tol > 0 and np.isfinite(dt_max_s) and dt_max_s > 0):
+        raise ValueError("tol and dt_max_s must be finite and > 0")
+    if drag and atm_model not in (1, 3, 4, 5, 6, 7, 8):
+        raise ValueError(f"unknown atm_model {atm_model}; use 4 (exact JB2008), 7 (fitted JB2008), "
+                         "8 (campaign persistence scenario), 1 (exponential)")
+    if drag and atm_model not in (4, 7):
+        raise ValueError(f"atm_model {atm_model} is not built here; use 4 or 7 (both evaluated with the "
+                         "exact JB2008 quadrature)")
+    name = str(method).lower()
+    if name in _UNBUILT_METHODS:
+        raise ValueError(f"integrator method {name!r} is not built here; use 'dop853' or 'dopri5'")
+    if name not in _METHODS:
+        raise ValueError(f"unknown integrator method {name!r}; use one of vern7, vern9, dop853, tsit5, rkv98, "
+                         "dopri5")
+    if srp:
+        raise ValueError("srp=True needs the binary-eclipse SRP coordinator, which is not built here; "
+                         "pass srp=False")
+    cfg = N.default_config()
+    cfg.order = int(gravity_order)
+    flags = 0
+    if drag:
+        flags |= N.FORCE_DRAG
+    if sun:
+        flags |= N.FORCE_SUN
+    if moon:
+        flags |= N.FORCE_MOON
+    cfg.force_flags = flags
+    cfg.atm_model = int(atm_model) if drag else 0
+    cfg.method = _METHODS[name]
+    cfg.am_ratio = float(am_ratio)
+    cfg.cd = float(cd)
+    cfg.dt_max = float(dt_max_s)
+    if rtol is not None:
+        cfg.error_control = 1
+        cfg.rtol = float(rtol)
+        cfg.atol = float(atol if atol is not None else 0.0)
+    else:
+        cfg.error_control = 0
+        cfg.eps = float(tol)
+    if jb_drivers is not None:
+        for i, v in enumerate(jb_drivers):
+            cfg.jb_drivers[i] = float(v)
+    cfg.ground_check = 1 if ground_check else 0
+    return cfg
+
+
+# ------------------------------------------------------------------ contexts
+_CTX: "OrderedDict[tuple, N.Context]" = OrderedDict()
+_CTX_MAX = 8
+
+
+def _cfg_key(cfg: N.ForceConfig):
+    return tuple(getattr(cfg, f) if f != "jb_drivers" else tuple(cfg.jb_drivers) for f, _ in cfg._fields_)
+
+
+def context(text: str, cfg: N.ForceConfig) -> N.Context:
+    """A cached native context for (field text, configuration)."""
+    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg))
+    ctx = _CTX.get(key)
+    if ctx is None:
+        ctx = N.Context(text, cfg)
+        _CTX[key] = ctx
+        while len(_CTX) > _CTX_MAX:
+            _CTX.popitem(last=False)[1].close()
+    else:
+        _CTX.move_to_end(key)
+    return ctx
+
+
+def _equinoctial_of(eci, what):
+    equ, ok = N.eci_to_equinoctial(eci)
+    if not ok[0]:
+        raise ValueError(f"{what} is not a bound, non-degenerate elliptical orbit (equinoctial conversion failed)")
+    return equ[0]
+
+
+# ------------------------------------------------------------------ scalar API
+def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
+              moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
+              gravity_field=None):
+    """Propagate one ECI state; sampled, rectified path (lib.rs:237-353)."""
+    init = _six(state_eci, "state_eci")
+    if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
+        raise ValueError("epoch_jd must be finite and tof_s > 0")
+    if times_s is None:
+        user = np.array([float(tof_s)])
+    else:
+        try:
+            user = np.asarray(times_s, dtype=np.float64).reshape(-1)
+        except (TypeError, ValueError):
+            raise ValueError("times_s must be a sequence of floats") from None
+    if (user.size > 1 and np.any(np.diff(user) <= 0)) or np.any(~np.isfinite(user)) or np.any(user < 0) \
+            or np.any(user > tof_s):
+        raise ValueError("times_s must be strictly increasing, within [0, tof_s]")
+    grid = []
+    if user.size == 0 or user[0] > 0.0:
+        grid.append(0.0)
+    grid.extend(user.tolist())
+    if user.size == 0 or user[-1] < tof_s:
+        grid.append(float(tof_s))
+    text, embedded = _field_text(gravity_field)
+    cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
+                       method, embedded)
+    _equinoctial_of(init, "state_eci")
+    ctx = context(text, cfg)
+    t_start = time.perf_counter()
+    out, st, steps, evals = ctx.propagate_sampled(init, epoch_jd, tof_s, np.array(grid))
+    wall_us = int((time.perf_counter() - t_start) * 1e6)
+    status = int(st[0])
+    states = out[0]
+    good = np.all(np.isfinite(states), axis=1)
+    n_ok = len(grid) if status == N.ST_OK else int(np.argmin(good)) if not good.all() else len(grid)
+    completed = status == N.ST_OK and n_ok == len(grid)
+    if status == N.ST_OK:
+        terminal = ""
+    else:
+        terminal = N.STATUS_NAMES.get(status, "incomplete")
+    return {
+        "times_s": np.array(grid[:n_ok]),
+        "states_eci": states[:n_ok].copy(),
+        "completed": bool(completed),
+        "terminal_event": terminal,
+        "max_steps_exceeded": status == 1,
+        "steps": int(steps[0]),
+        "rhs_evals": int(evals[0]),
+        "wall_us": wall_us,
+    }
+
+
+def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, srp=True, sun=True, moon=True,
+                    atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
+                    gravity_field=None):
+    """Final state with the ground check enforced (lib.rs:361-438).
+
+    Raises ValueError for a physically infeasible arc (ground impact, a radius
+    below the surface) and RuntimeError for an integration failure."""
+    init = _six(state_eci, "state_eci")
+    if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
+        raise ValueError("epoch_jd must be finite and tof_s > 0")
+    text, embedded = _field_text(gravity_field)
+    cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
+                       method, embedded, ground_check=True)
+    _equinoctial_of(init, "state_eci")
+    ctx = context(text, cfg)
+    out, st, _, _ = ctx.propagate_final(init, epoch_jd, tof_s)
+    status = int(st[0])
+    if status == N.ST_GROUND:
+        raise ValueError("physically infeasible arc: trajectory hits the ground")
+    if status == N.ST_GRAVITY_RADIUS:
+        raise ValueError("physically infeasible arc: radius fell below the Earth's surface")
+    if status != N.ST_OK:
+        raise RuntimeError(f"propagation failed: {N.STATUS_NAMES.get(status, status)}")
+    return out[0].copy()
+
+
+def kep_to_eci(kep):
+    """Keplerian [a_km, e, i_deg, raan_deg, argp_deg, true_anomaly_deg] -> ECI (lib.rs:200-211)."""
+    k = _six(kep, "kep")
+    if k[0] <= 0.0 or not (0.0 <= k[1] < 1.0):
+        raise ValueError("need a_km > 0 and 0 <= e < 1")
+    return N.kep_to_eci(k)[0]
+
+
+def eci_to_kep(eci):
+    """ECI (km, km/s) -> Keplerian elements in degrees (lib.rs:213-221)."""
+    return N.eci_to_kep(_six(eci, "eci"))[0]
+
+
+# ------------------------------------------------------------------ batch API
+def _batch_cfg(model: dict, embedded: bool):
+    m = dict(gravity_order=5, drag=True, srp=False, sun=True, moon=True, atm_model=7, am_ratio=0.01, cd=2.2,
+             cr=1.3, tol=1e-8, dt_max_s=300.0, method="dop853")
+    m.update(model)
+    return force_config(m["gravity_order"], m["drag"], m["srp"], m["sun"], m["moon"], m["atm_model"],
+                        m["am_ratio"], m["cd"], m["cr"], m["tol"], m["dt_max_s"], m["method"], embedded,
+                        rtol=m.get("rtol"), atol=m.get("atol"), jb_drivers=m.get("jb_drivers"),
+                        ground_check=m.get("ground_check", False))
+
+
+def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctial=False, gravity_field=None,
+                          **model):
+    """Final states of a batch with per-row epoch / duration / ballistics.
+
+    The reference's LightyearSession::integrate_variable_final_into
+    (session.rs:2325-2430).  Returns (states_eci [n,6], status [n], steps [n],
+    rhs_evals [n]); failed rows are NaN."""
+    text, embedded = _field_text(gravity_field)
+    ctx = context(text, _batch_cfg(model, embedded))
+    return ctx.propagate_final(states, epoch_jd, tof_s, ballistic=ballistic, equinoctial=equinoctial)
+
+
+def propagate_batch_sampled(states, epoch_jd, tof_s, t_eval, *, deltas=False, equinoctial=False,
+                            gravity_field=None, **model):
+    """Samples of a batch on one grid; the reference's
+    integrate_batch_native_into (batch.rs:247-391) with ``deltas=True``
+    (Encke deviations from the initial baseline) or ECI states."""
+    text, embedded = _field_text(gravity_field)
+    ctx = context(text, _batch_cfg(model, embedded))
+    return ctx.propagate_sampled(states, epoch_jd, tof_s, t_eval, deltas=deltas, equinoctial=equinoctial)

@@ -1,0 +1,762 @@
+// Host side of libbqp_b200.so: the C ABI declared in include/bqp_prop.h.
+//
+// A context owns the device copy of the gravity table (normalised, with the
+// recursion coefficients and the folded summation weights per V/W cell), the
+// force/solver configuration, a device work-queue counter and a growable
+// device workspace for the host-buffer entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/bqp_prop.h"
+#include "launch.h"
+
+using namespace bqp;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(BQP_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+constexpr int kMaxOrder = 128;
+constexpr size_t kSmemLimit = 227 * 1024;
+
+// Normalised coefficients, [n*(order+1) + m].
+struct Coeffs {
+    int order = 0;
+    std::vector<double> c, s;
+};
+
+// "deg ord C S" text, normalised (lightyear_odeint_rs/src/config.rs:128-225):
+// blank and '#' lines skipped, lines with fewer than four fields skipped,
+// D/d exponents accepted, rows above the requested order ignored.
+bool parse_coeffs(const char* text, int64_t len, int order, Coeffs& out, std::string& why) {
+    out.order = order;
+    out.c.assign((size_t)(order + 1) * (order + 1), 0.0);
+    out.s.assign((size_t)(order + 1) * (order + 1), 0.0);
+    std::string all(text, (size_t)len);
+    std::istringstream in(all);
+    std::string line;
+    int lineno = 0;
+    while (std::getline(in, line)) {
+        ++lineno;
+        size_t a = line.find_first_not_of(" \t\r");
+        if (a == std::string::npos || line[a] == '#') continue;
+        std::istringstream ls(line);
+        std::string f[4];
+        if (!(ls >> f[0] >> f[1] >> f[2] >> f[3])) continue;
+        for (int i = 2; i < 4; ++i)
+            for (auto& ch : f[i])
+                if (ch == 'D' || ch == 'd') ch = 'E';
+        char* end = nullptr;
+        long deg = std::strtol(f[0].c_str(), &end, 10);
+        if (*end || deg < 0) { why = "bad degree on line " + std::to_string(lineno); return false; }
+        long m = std::strtol(f[1].c_str(), &end, 10);
+        if (*end || m < 0) { why = "bad order on line " + std::to_string(lineno); return false; }
+        double cv = std::strtod(f[2].c_str(), &end);
+        if (*end || !std::isfinite(cv)) { why = "bad C value on line " + std::to_string(lineno); return false; }
+        double sv = std::strtod(f[3].c_str(), &end);
+        if (*end || !std::isfinite(sv)) { why = "bad S value on line " + std::to_string(lineno); return false; }
+        if (deg <= order && m <= deg) {
+            out.c[(size_t)deg * (order + 1) + m] = cv;
+            out.s[(size_t)deg * (order + 1) + m] = sv;
+        }
+    }
+    return true;
+}
+
+// Per-cell table of the normalised column recursion (see gravity.cuh).  The
+// C00 term is left out: the propagator removes the central term analytically
+// (rhs.rs:2735-2744, 2849-2855), which is what dropping it computes exactly.
+std::vector<double> build_gravity_table(const Coeffs& cf, int order) {
+    typedef long double LD;
+    const int N = order;
+    const int ncells = gravity_cells(N);
+    std::vector<double> tab((size_t)ncells * kCellDoubles, 0.0);
+    const int ld = cf.order + 1;
+    auto C = [&](int n, int k) -> LD {
+        if (n < 0 || k < 0 || k > n || n > N) return 0.0L;
+        if (n == 0) return 0.0L;  // central term handled analytically
+        return (LD)cf.c[(size_t)n * ld + k];
+    };
+    auto S = [&](int n, int k) -> LD {
+        if (n < 0 || k < 0 || k > n || n > N) return 0.0L;
+        return (LD)cf.s[(size_t)n * ld + k];
+    };
+    // N(n,k)/N(n+1,k+1), N(n,k)/N(n+1,k-1), N(n,k)/N(n+1,k)
+    auto r_up = [](int n, int k) -> LD {
+        LD d = (k == 0) ? 1.0L : 2.0L;
+        return std::sqrt(d * (2.0L * n + 1) * (LD)(n + k + 2) * (LD)(n + k + 1) / (2.0L * (2.0L * n + 3)));
+    };
+    auto r_dn = [](int n, int k) -> LD {
+        LD d = (k - 1 == 0) ? 1.0L : 2.0L;
+        return std::sqrt(2.0L * (2.0L * n + 1) / (d * (2.0L * n + 3) * (LD)(n - k + 2) * (LD)(n - k + 1)));
+    };
+    auto r_eq = [](int n, int k) -> LD {
+        return std::sqrt((2.0L * n + 1) * (LD)(n + k + 1) / ((2.0L * n + 3) * (LD)(n - k + 1)));
+    };
+    const LD gm_r2 = (LD)kMu / ((LD)kReGravity * (LD)kReGravity);
+    size_t cell = 0;
+    for (int j = 0; j <= N + 1; ++j) {
+        for (int l = j; l <= N + 1; ++l, ++cell) {
+            double* o = &tab[cell * kCellDoubles];
+            LD a = 0.0L, b = 0.0L;
+            if (l == j) {
+                a = (j == 0) ? 0.0L : (j == 1 ? std::sqrt(3.0L) : std::sqrt((2.0L * j + 1) / (2.0L * j)));
+            } else if (l == j + 1) {
+                a = std::sqrt(2.0L * j + 3);
+            } else {
+                a = std::sqrt((2.0L * l - 1) * (2.0L * l + 1) / ((LD)(l - j) * (LD)(l + j)));
+                b = std::sqrt((2.0L * l + 1) * (LD)(l + j - 1) * (LD)(l - j - 1) /
+                              ((2.0L * l - 3) * (LD)(l + j) * (LD)(l - j)));
+            }
+            const int n = l - 1;
+            LD Ax = 0, Bx = 0, Ay = 0, By = 0, Az = 0, Bz = 0;
+            if (n >= 0) {
+                if (j == 1) {
+                    const LD cu = C(n, 0) * r_up(n, 0);
+                    Ax += -cu;
+                    By += -cu;
+                } else if (j >= 2) {
+                    const LD r = r_up(n, j - 1);
+                    const LD cu = C(n, j - 1) * r, su = S(n, j - 1) * r;
+                    Ax += -0.5L * cu;
+                    Bx += -0.5L * su;
+                    Ay += 0.5L * su;
+                    By += -0.5L * cu;
+                }
+                if (j + 1 <= n) {
+                    const int k = j + 1;
+                    const LD f = (LD)(n - k + 2) * (LD)(n - k + 1);
+                    const LD r = r_dn(n, k);
+                    const LD cu = C(n, k) * r, su = S(n, k) * r;
+                    Ax += 0.5L * f * cu;
+                    Bx += 0.5L * f * su;
+                    Ay += 0.5L * f * su;
+                    By += -0.5L * f * cu;
+                }
+                if (j <= n) {
+                    const LD r = r_eq(n, j);
+                    const LD w = (LD)(n - j + 1);
+                    Az += -w * C(n, j) * r;
+                    Bz += -w * S(n, j) * r;
+                }
+            }
+            o[0] = (double)a;
+            o[1] = (double)b;
+            o[2] = (double)(Ax * gm_r2);
+            o[3] = (double)(Bx * gm_r2);
+            o[4] = (double)(Ay * gm_r2);
+            o[5] = (double)(By * gm_r2);
+            o[6] = (double)(Az * gm_r2);
+            o[7] = (double)(Bz * gm_r2);
+        }
+    }
+    return tab;
+}
+
+}  // namespace
+
+struct bqp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bqp_force_config cfg{};
+    Coeffs coeffs;
+    int parsed_order = 0;
+    double* d_tab = nullptr;
+    int ncells = 0;
+    size_t tab_bytes = 0;
+    int use_smem = 0;
+    unsigned long long* d_queue = nullptr;
+    void* d_ws = nullptr;
+    size_t ws_bytes = 0;
+};
+
+namespace {
+
+int validate_cfg(const bqp_force_config* c) {
+    if (!c) return fail(BQP_E_ARG, "null config");
+    if (c->order < 0 || c->order > kMaxOrder)
+        return fail(BQP_E_ARG, "order must be in 0..%d, got %d", kMaxOrder, c->order);
+    if (c->force_flags & BQP_FORCE_SRP)
+        return fail(BQP_E_UNSUPPORTED, "solar radiation pressure (binary-eclipse SRP) is not built; pass srp=False");
+    if (c->force_flags & ~(BQP_FORCE_DRAG | BQP_FORCE_SUN | BQP_FORCE_MOON | BQP_FORCE_SRP))
+        return fail(BQP_E_ARG, "unknown force flags 0x%x", c->force_flags);
+    if ((c->force_flags & BQP_FORCE_DRAG) && c->atm_model != 4 && c->atm_model != 7)
+        return fail(BQP_E_UNSUPPORTED, "atm_model %d is not built; use 4 (exact JB2008) or 7", c->atm_model);
+    if (c->method < 0 || c->method > 2) return fail(BQP_E_ARG, "unknown method %d", c->method);
+    if (c->error_control == 0) {
+        if (!(std::isfinite(c->eps) && c->eps > 0.0)) return fail(BQP_E_ARG, "eps must be finite and > 0");
+    } else if (c->error_control == 1) {
+        if (c->method == BQP_METHOD_DOPRI5_COMPAT)
+            return fail(BQP_E_ARG, "the DOPRI5 compatibility loop has absolute error control only");
+        if (!(std::isfinite(c->rtol) && c->rtol > 0.0 && std::isfinite(c->atol) && c->atol >= 0.0))
+            return fail(BQP_E_ARG, "rtol must be finite and > 0, atol finite and >= 0");
+    } else {
+        return fail(BQP_E_ARG, "error_control must be 0 or 1");
+    }
+    if (!(std::isfinite(c->dt_max) && c->dt_max > 0.0)) return fail(BQP_E_ARG, "dt_max must be finite and > 0");
+    if (!(std::isfinite(c->am_ratio) && c->am_ratio >= 0.0 && std::isfinite(c->cd) && c->cd >= 0.0))
+        return fail(BQP_E_ARG, "am_ratio and cd must be finite and >= 0");
+    if (c->max_steps <= 0 || c->max_attempts <= 0) return fail(BQP_E_ARG, "step budgets must be > 0");
+    if (!(c->max_kernel_seconds >= 0.0)) return fail(BQP_E_ARG, "max_kernel_seconds must be >= 0");
+    return 0;
+}
+
+ForceParams force_params(const bqp_ctx* ctx) {
+    const bqp_force_config& c = ctx->cfg;
+    ForceParams fp{};
+    fp.order = c.order;
+    fp.gravity_on = c.order > 0;
+    fp.drag = (c.force_flags & BQP_FORCE_DRAG) ? 1 : 0;
+    fp.sun = (c.force_flags & BQP_FORCE_SUN) ? 1 : 0;
+    fp.moon = (c.force_flags & BQP_FORCE_MOON) ? 1 : 0;
+    fp.ground_check = c.ground_check;
+    fp.earth_radius = c.earth_radius;
+    fp.omega = c.omega_earth;
+    fp.mu_sun = c.mu_sun;
+    fp.mu_moon = c.mu_moon;
+    fp.drivers = {c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
+                  c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
+    return fp;
+}
+
+CtrlParams ctrl_params(const bqp_ctx* ctx) {
+    const bqp_force_config& c = ctx->cfg;
+    CtrlParams p{};
+    p.scaled = c.error_control;
+    p.max_rejects = 50;
+    p.eps = c.error_control == 0 ? std::max(c.eps, 1e-12) : c.eps;  // integrator.rs:427
+    p.rtol = c.rtol;
+    p.atol = c.atol;
+    p.h_min = 1e-12;
+    p.h_max = c.dt_max;
+    p.max_steps = c.max_steps;
+    p.max_attempts = c.max_attempts;
+    p.max_kernel_ns = c.max_kernel_seconds > 0.0 ? (int64_t)(c.max_kernel_seconds * 1e9) : 0;
+    return p;
+}
+
+int upload_table(bqp_ctx* ctx) {
+    std::vector<double> tab = build_gravity_table(ctx->coeffs, ctx->cfg.order);
+    ctx->ncells = gravity_cells(ctx->cfg.order);
+    ctx->tab_bytes = tab.size() * sizeof(double);
+    ctx->use_smem = ctx->tab_bytes <= kSmemLimit ? 1 : 0;
+    if (ctx->d_tab) cudaFree(ctx->d_tab);
+    ctx->d_tab = nullptr;
+    cudaError_t e = cudaMalloc(&ctx->d_tab, ctx->tab_bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(gravity table)");
+    e = cudaMemcpy(ctx->d_tab, tab.data(), ctx->tab_bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(gravity table)");
+    return 0;
+}
+
+// Device workspace carve-out for the host-buffer entry points.
+struct Carve {
+    char* base;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+int ensure_ws(bqp_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->ws_bytes) return 0;
+    if (ctx->d_ws) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_ws);
+        ctx->d_ws = nullptr;
+        ctx->ws_bytes = 0;
+    }
+    size_t want = std::max(bytes, (size_t)1 << 20);
+    cudaError_t e = cudaMalloc(&ctx->d_ws, want);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(workspace)");
+    ctx->ws_bytes = want;
+    return 0;
+}
+
+size_t rounded(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int set_device(const bqp_ctx* ctx) {
+    cudaError_t e = cudaSetDevice(ctx->device);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "cudaSetDevice");
+}
+
+int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, const double* epoch,
+                double t0, const double* tf, const double* ballistic, int32_t n_t, const double* t_eval,
+                int32_t out_mode, double* out, int32_t* status, int64_t* steps, int64_t* evals) {
+    PropArgs A{};
+    A.n = n;
+    A.in = in;
+    A.input_equinoctial = input_equ;
+    A.epoch = epoch;
+    A.t0 = t0;
+    A.tf = tf;
+    A.ballistic = ballistic;
+    A.am0 = ctx->cfg.am_ratio;
+    A.cd0 = ctx->cfg.cd;
+    A.t_eval = t_eval;
+    A.n_t = n_t;
+    A.out_mode = out_mode;
+    A.out = out;
+    A.status = status;
+    A.steps = steps;
+    A.evals = evals;
+    A.queue = ctx->d_queue;
+    A.gtab = ctx->d_tab;
+    A.ncells = ctx->ncells;
+    A.use_smem = ctx->use_smem;
+    A.force = force_params(ctx);
+    A.ctrl = ctrl_params(ctx);
+    cudaError_t e = cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
+    e = launch_propagate(A, ctx->cfg.method, 256, 0, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "k_propagate launch");
+    return 0;
+}
+
+int check_prop_args(int64_t n, const double* in, const double* epoch, double t0, const double* tf,
+                    const double* out, const int32_t* status) {
+    if (n < 0) return fail(BQP_E_ARG, "n must be >= 0");
+    if (n > 0 && (!in || !epoch || !tf || !out || !status))
+        return fail(BQP_E_ARG, "null buffer");
+    if (!std::isfinite(t0)) return fail(BQP_E_ARG, "t0 must be finite");
+    return 0;
+}
+
+int check_grid(int32_t n_t, const double* t_eval) {
+    if (n_t <= 0 || !t_eval) return fail(BQP_E_ARG, "t_eval must be a non-empty array");
+    for (int32_t i = 0; i < n_t; ++i) {
+        if (!std::isfinite(t_eval[i])) return fail(BQP_E_ARG, "t_eval[%d] is not finite", i);
+        if (i > 0 && !(t_eval[i] > t_eval[i - 1]))
+            return fail(BQP_E_ARG, "t_eval must be strictly increasing (index %d)", i);
+    }
+    return 0;
+}
+
+// --- Keplerian elements (Python kep_to_eci / eci_to_kep, lib.rs:200-221)
+void kep2eci(const double* kep, double* out) {
+    const double a = kep[0], e = kep[1];
+    if (!(a > 0.0) || !(e >= 0.0 && e < 1.0)) {
+        for (int i = 0; i < 6; ++i) out[i] = NAN;
+        return;
+    }
+    const double d2r = kPi / 180.0;
+    const double inc = kep[2] * d2r, raan = kep[3] * d2r, argp = kep[4] * d2r, nu = kep[5] * d2r;
+    const double p = a * (1.0 - e * e);
+    const double cn = std::cos(nu), sn = std::sin(nu);
+    const double r = p / (1.0 + e * cn);
+    const double sp = std::sqrt(kMu / p);
+    const double xp = r * cn, yp = r * sn;
+    const double vxp = -sp * sn, vyp = sp * (e + cn);
+    const double cO = std::cos(raan), sO = std::sin(raan), cw = std::cos(argp), sw = std::sin(argp);
+    const double ci = std::cos(inc), si = std::sin(inc);
+    const double r00 = cO * cw - sO * sw * ci, r01 = -cO * sw - sO * cw * ci;
+    const double r10 = sO * cw + cO * sw * ci, r11 = -sO * sw + cO * cw * ci;
+    const double r20 = sw * si, r21 = cw * si;
+    out[0] = r00 * xp + r01 * yp;
+    out[1] = r10 * xp + r11 * yp;
+    out[2] = r20 * xp + r21 * yp;
+    out[3] = r00 * vxp + r01 * vyp;
+    out[4] = r10 * vxp + r11 * vyp;
+    out[5] = r20 * vxp + r21 * vyp;
+}
+
+double wrap360(double deg) {
+    double x = std::fmod(deg, 360.0);
+    if (x < 0.0) x += 360.0;
+    return x >= 360.0 ? x - 360.0 : x;
+}
+
+void eci2kep(const double* s, double* out) {
+    const double r[3] = {s[0], s[1], s[2]}, v[3] = {s[3], s[4], s[5]};
+    const double rn = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double rv = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
+    const double energy = 0.5 * v2 - kMu / rn;
+    if (!(energy < -1e-12) || !(rn > 0.0)) {
+        for (int i = 0; i < 6; ++i) out[i] = NAN;
+        return;
+    }
+    const double h[3] = {r[1] * v[2] - r[2] * v[1], r[2] * v[0] - r[0] * v[2], r[0] * v[1] - r[1] * v[0]};
+    const double hn = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    const double nvec[2] = {-h[1], h[0]};
+    const double nn = std::sqrt(nvec[0] * nvec[0] + nvec[1] * nvec[1]);
+    double ev[3];
+    for (int i = 0; i < 3; ++i) ev[i] = ((v2 - kMu / rn) * r[i] - rv * v[i]) / kMu;
+    const double e = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+    const double a = -kMu / (2.0 * energy);
+    const double r2d = 180.0 / kPi;
+    const double inc = std::acos(std::max(-1.0, std::min(1.0, h[2] / hn)));
+    const bool equatorial = nn < 1e-11 * hn;
+    const bool circular = e < 1e-11;
+    double raan = equatorial ? 0.0 : std::atan2(nvec[1], nvec[0]);
+    double argp = 0.0, nu = 0.0;
+    if (!circular) {
+        if (!equatorial) {
+            argp = std::acos(std::max(-1.0, std::min(1.0, (nvec[0] * ev[0] + nvec[1] * ev[1]) / (nn * e))));
+            if (ev[2] < 0.0) argp = 2.0 * kPi - argp;
+        } else {
+            argp = std::atan2(ev[1], ev[0]);
+            if (h[2] < 0.0) argp = -argp;
+        }
+        nu = std::acos(std::max(-1.0, std::min(1.0, (ev[0] * r[0] + ev[1] * r[1] + ev[2] * r[2]) / (e * rn))));
+        if (rv < 0.0) nu = 2.0 * kPi - nu;
+    } else if (!equatorial) {
+        nu = std::acos(std::max(-1.0, std::min(1.0, (nvec[0] * r[0] + nvec[1] * r[1]) / (nn * rn))));
+        if (r[2] < 0.0) nu = 2.0 * kPi - nu;
+    } else {
+        nu = std::atan2(r[1], r[0]);
+        if (h[2] < 0.0) nu = -nu;
+    }
+    out[0] = a;
+    out[1] = e;
+    out[2] = inc * r2d;
+    out[3] = wrap360(raan * r2d);
+    out[4] = wrap360(argp * r2d);
+    out[5] = wrap360(nu * r2d);
+}
+
+}  // namespace
+
+// ======================================================================
+extern "C" {
+
+void bqp_force_config_default(bqp_force_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof *c);
+    c->order = 5;                      // Python kwarg default (lib.rs:240)
+    c->force_flags = BQP_FORCE_DRAG | BQP_FORCE_SUN | BQP_FORCE_MOON;
+    c->atm_model = 7;
+    c->method = BQP_METHOD_DOP853;
+    c->error_control = 0;
+    c->ground_check = 0;
+    c->eps = 1e-8;                     // ForceConfig::default (types.rs:497)
+    c->rtol = 1e-10;
+    c->atol = 1e-9;
+    c->dt_max = 300.0;                 // Python dt_max_s default
+    c->am_ratio = 0.01;
+    c->cd = 2.2;
+    c->earth_radius = kReWgs84;
+    c->omega_earth = kEarthOmega;
+    c->mu_sun = 1.32712440018e11;      // DE431 (types.rs:461-462)
+    c->mu_moon = 4902.800066;
+    for (int i = 0; i < 8; ++i) c->jb_drivers[i] = 150.0;
+    c->jb_drivers[8] = 0.0;
+    c->max_steps = 500000;             // MAX_STEPS (integrator.rs:185)
+    c->max_attempts = (int64_t)1 << 40;
+    c->max_kernel_seconds = 600.0;
+}
+
+const char* bqp_last_error(void) { return g_err.c_str(); }
+
+int bqp_ctx_create(const char* text, int64_t len, const bqp_force_config* cfg, bqp_ctx** out) {
+    if (!out) return fail(BQP_E_ARG, "null out");
+    *out = nullptr;
+    if (!text || len < 0) return fail(BQP_E_ARG, "null coefficient text");
+    int rc = validate_cfg(cfg);
+    if (rc) return rc;
+    bqp_ctx* ctx = new bqp_ctx();
+    ctx->cfg = *cfg;
+    std::string why;
+    if (!parse_coeffs(text, len, cfg->order, ctx->coeffs, why)) {
+        delete ctx;
+        return fail(BQP_E_COEFF, "gravity coefficients failed to load: %s", why.c_str());
+    }
+    ctx->parsed_order = cfg->order;
+    cudaError_t e = cudaGetDevice(&ctx->device);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(e, "cudaGetDevice");
+    }
+    rc = upload_table(ctx);
+    if (!rc) {
+        e = cudaMalloc(&ctx->d_queue, sizeof(unsigned long long));
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(queue)");
+    }
+    if (rc) {
+        bqp_ctx_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    g_err.clear();
+    return 0;
+}
+
+int bqp_ctx_destroy(bqp_ctx* ctx) {
+    if (!ctx) return 0;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    if (ctx->d_tab) cudaFree(ctx->d_tab);
+    if (ctx->d_queue) cudaFree(ctx->d_queue);
+    if (ctx->d_ws) cudaFree(ctx->d_ws);
+    delete ctx;
+    return 0;
+}
+
+int bqp_ctx_set_stream(bqp_ctx* ctx, void* stream) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    ctx->stream = (cudaStream_t)stream;
+    return 0;
+}
+
+int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info) {
+    if (!ctx || !info) return fail(BQP_E_ARG, "null argument");
+    info[0] = ctx->cfg.order;
+    info[1] = ctx->ncells;
+    info[2] = (int64_t)ctx->tab_bytes;
+    info[3] = ctx->use_smem;
+    return 0;
+}
+
+int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = validate_cfg(cfg);
+    if (rc) return rc;
+    if (cfg->order > ctx->parsed_order)
+        return fail(BQP_E_ARG, "order %d exceeds the parsed field order %d", cfg->order, ctx->parsed_order);
+    if ((rc = set_device(ctx))) return rc;
+    const int old = ctx->cfg.order;
+    ctx->cfg = *cfg;
+    if (cfg->order != old) {
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        return upload_table(ctx);
+    }
+    return 0;
+}
+
+int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, int32_t* status) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (n < 0 || (n > 0 && (!pos || !acc))) return fail(BQP_E_ARG, "bad buffers");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaError_t e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, pos, acc,
+                                   status, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "k_gravity launch");
+}
+
+int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, int32_t* status) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (n < 0 || (n > 0 && (!pos || !acc))) return fail(BQP_E_ARG, "bad buffers");
+    if (n == 0) return 0;
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    const size_t b3 = (size_t)n * 3 * sizeof(double);
+    if ((rc = ensure_ws(ctx, 2 * rounded(b3) + rounded((size_t)n * 4) + 1024))) return rc;
+    Carve cv{(char*)ctx->d_ws};
+    double* dp = cv.take<double>((size_t)n * 3);
+    double* da = cv.take<double>((size_t)n * 3);
+    int32_t* ds = cv.take<int32_t>((size_t)n);
+    cudaError_t e = cudaMemcpyAsync(dp, pos, b3, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, dp, da, ds, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(acc, da, b3, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && status)
+        e = cudaMemcpyAsync(status, ds, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_gravity_eval");
+}
+
+int bqp_rhs_eval_device(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t0,
+                        const double* epoch_jd, const double* t, const double* delta,
+                        const double* ballistic, double* out) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (n < 0 || (n > 0 && (!equ || !seg_t0 || !epoch_jd || !t || !delta || !out)))
+        return fail(BQP_E_ARG, "bad buffers");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaError_t e = launch_rhs(ctx->d_tab, ctx->ncells, ctx->use_smem, force_params(ctx), n, equ, seg_t0,
+                               epoch_jd, t, delta, ballistic, ctx->cfg.am_ratio, ctx->cfg.cd, out, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "k_rhs launch");
+}
+
+int bqp_rhs_eval(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t0, const double* epoch_jd,
+                 const double* t, const double* delta, const double* ballistic, double* out) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (n < 0 || (n > 0 && (!equ || !seg_t0 || !epoch_jd || !t || !delta || !out)))
+        return fail(BQP_E_ARG, "bad buffers");
+    if (n == 0) return 0;
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
+    if ((rc = ensure_ws(ctx, 4 * rounded(b6) + 3 * rounded(b1) + 4096))) return rc;
+    Carve cv{(char*)ctx->d_ws};
+    double* de = cv.take<double>((size_t)n * 6);
+    double* dt0 = cv.take<double>((size_t)n);
+    double* djd = cv.take<double>((size_t)n);
+    double* dt = cv.take<double>((size_t)n);
+    double* dd = cv.take<double>((size_t)n * 6);
+    double* db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
+    double* dout = cv.take<double>((size_t)n * 6);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(de, equ, b6, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt0, seg_t0, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(djd, epoch_jd, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, t, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dd, delta, b6, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && db) e = cudaMemcpyAsync(db, ballistic, 2 * b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_rhs(ctx->d_tab, ctx->ncells, ctx->use_smem, force_params(ctx), n, de, dt0, djd, dt, dd, db,
+                       ctx->cfg.am_ratio, ctx->cfg.cd, dout, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, b6, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_rhs_eval");
+}
+
+int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ,
+                               const double* epoch_jd, double t0, const double* tf, const double* ballistic,
+                               double* out, int32_t* status, int64_t* steps, int64_t* evals) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    return launch_prop(ctx, n, in, input_equ, epoch_jd, t0, tf, ballistic, 0, nullptr, 0, out, status, steps,
+                       evals);
+}
+
+int bqp_propagate_final(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, const double* epoch_jd,
+                        double t0, const double* tf, const double* ballistic, double* out, int32_t* status,
+                        int64_t* steps, int64_t* evals) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
+    if ((rc = ensure_ws(ctx, 2 * rounded(b6) + 6 * rounded(b1) + 4096))) return rc;
+    Carve cv{(char*)ctx->d_ws};
+    double* din = cv.take<double>((size_t)n * 6);
+    double* dep = cv.take<double>((size_t)n);
+    double* dtf = cv.take<double>((size_t)n);
+    double* db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
+    double* dout = cv.take<double>((size_t)n * 6);
+    int32_t* dst = cv.take<int32_t>((size_t)n);
+    int64_t* dsteps = cv.take<int64_t>((size_t)n);
+    int64_t* devals = cv.take<int64_t>((size_t)n);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(din, in, b6, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtf, tf, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && db) e = cudaMemcpyAsync(db, ballistic, 2 * b1, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_propagate_final H2D");
+    rc = launch_prop(ctx, n, din, input_equ, dep, t0, dtf, db, 0, nullptr, 0, dout, dst, dsteps, devals);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(out, dout, b6, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, dst, (size_t)n * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && steps) e = cudaMemcpyAsync(steps, dsteps, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && evals) e = cudaMemcpyAsync(evals, devals, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_propagate_final");
+}
+
+int bqp_propagate_sampled_device(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ,
+                                 const double* epoch_jd, double t0, const double* tf, int32_t n_t,
+                                 const double* t_eval, int32_t out_deltas, double* out, int32_t* status,
+                                 int64_t* steps, int64_t* evals) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
+    if (rc) return rc;
+    if (n_t <= 0 || !t_eval) return fail(BQP_E_ARG, "t_eval must be a non-empty array");
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    return launch_prop(ctx, n, in, input_equ, epoch_jd, t0, tf, nullptr, n_t, t_eval,
+                       out_deltas ? 2 : 1, out, status, steps, evals);
+}
+
+int bqp_propagate_sampled(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, const double* epoch_jd,
+                          double t0, const double* tf, int32_t n_t, const double* t_eval, int32_t out_deltas,
+                          double* out, int32_t* status, int64_t* steps, int64_t* evals) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
+    if (rc) return rc;
+    if ((rc = check_grid(n_t, t_eval))) return rc;
+    if (t_eval[0] < t0) return fail(BQP_E_ARG, "t_eval starts before t0");
+    for (int64_t i = 0; i < n; ++i)
+        if (!(tf[i] >= t_eval[n_t - 1])) return fail(BQP_E_ARG, "t_eval ends after tf[%lld]", (long long)i);
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
+    const size_t bo = (size_t)n * n_t * 6 * sizeof(double);
+    if ((rc = ensure_ws(ctx, rounded(b6) + 5 * rounded(b1) + rounded(bo) + rounded((size_t)n_t * 8) + 4096)))
+        return rc;
+    Carve cv{(char*)ctx->d_ws};
+    double* din = cv.take<double>((size_t)n * 6);
+    double* dep = cv.take<double>((size_t)n);
+    double* dtf = cv.take<double>((size_t)n);
+    double* dte = cv.take<double>((size_t)n_t);
+    double* dout = cv.take<double>((size_t)n * n_t * 6);
+    int32_t* dst = cv.take<int32_t>((size_t)n);
+    int64_t* dsteps = cv.take<int64_t>((size_t)n);
+    int64_t* devals = cv.take<int64_t>((size_t)n);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(din, in, b6, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtf, tf, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dte, t_eval, (size_t)n_t * 8, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_propagate_sampled H2D");
+    rc = launch_prop(ctx, n, din, input_equ, dep, t0, dtf, nullptr, n_t, dte, out_deltas ? 2 : 1, dout, dst,
+                     dsteps, devals);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(out, dout, bo, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, dst, (size_t)n * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && steps) e = cudaMemcpyAsync(steps, dsteps, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && evals) e = cudaMemcpyAsync(evals, devals, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_propagate_sampled");
+}
+
+int bqp_eci_to_equinoctial(int64_t n, const double* eci, double* equ, int32_t* ok) {
+    if (n < 0 || (n > 0 && (!eci || !equ))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) {
+        bool good = eci_to_equinoctial(eci + 6 * i, equ + 6 * i);
+        if (ok) ok[i] = good ? 1 : 0;
+    }
+    return 0;
+}
+
+int bqp_equinoctial_to_eci(int64_t n, const double* equ, const double* tof, double* eci) {
+    if (n < 0 || (n > 0 && (!equ || !eci))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) equinoctial_to_eci(equ + 6 * i, tof ? tof[i] : 0.0, eci + 6 * i);
+    return 0;
+}
+
+int bqp_kep_to_eci(int64_t n, const double* kep, double* eci) {
+    if (n < 0 || (n > 0 && (!kep || !eci))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) kep2eci(kep + 6 * i, eci + 6 * i);
+    return 0;
+}
+
+int bqp_eci_to_kep(int64_t n, const double* eci, double* kep) {
+    if (n < 0 || (n > 0 && (!eci || !kep))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) eci2kep(eci + 6 * i, kep + 6 * i);
+    return 0;
+}
+
+}  // extern "C"

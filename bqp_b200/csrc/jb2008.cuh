@@ -1,0 +1,341 @@
+// Jacchia-Bowman 2008 thermospheric density (Bowman et al., AIAA 2008-6438),
+// in the form Orekit 13.1.2 implements and the reference adapts
+// (jb_rs/src/jb2008.rs, "exact" quadrature profile): exospheric temperature
+// from the solar indices, the local-temperature profile, Boole-rule
+// integration of the barometric / diffusion equations from 90 km through 105
+// and 500 km, six species, the semiannual and seasonal-latitudinal
+// corrections and the high-altitude density factor.  The coefficient tables
+// are the published model's (they must match it to reproduce the model).
+//
+// Host and device share this code.  FP64 throughout; the quadrature node
+// count depends only on altitude, so a warp whose trajectories share an
+// altitude band walks the same loop trip counts.
+#pragma once
+#include "physics.cuh"
+
+namespace bqp {
+namespace jb {
+
+// Each table exists twice: in constant memory for the kernels and as a plain
+// host array for host-side callers; JBT() picks the copy of the current pass.
+#ifdef __CUDACC__
+#define BQP_JB_TABLE(name, n, ...)                 \
+    __constant__ const double name##_dev[n] = __VA_ARGS__; \
+    static const double name##_host[n] = __VA_ARGS__;
+#else
+#define BQP_JB_TABLE(name, n, ...) static const double name##_host[n] = __VA_ARGS__;
+#endif
+#ifdef __CUDA_ARCH__
+#define JBT(name) name##_dev
+#else
+#define JBT(name) name##_host
+#endif
+
+BQP_JB_TABLE(kAmw, 6, {28.0134, 31.9988, 15.9994, 39.9480, 4.0026, 1.00797})
+BQP_JB_TABLE(kFrac, 4, {0.78110, 0.20955, 9.3400e-3, 1.2890e-5})
+BQP_JB_TABLE(kBdt, 19, {-4.57512297, -5.12114909, -69.3003609, 203.716701, 703.316291,
+                                -1943.49234, 1106.51308, -174.378996, 1885.94601, -7093.71517,
+                                9224.54523, -3845.08073, -6.45841789, 40.9703319, -482.006560,
+                                1818.70931, -2373.89204, 996.703815, 36.1416936})
+BQP_JB_TABLE(kCdt, 23, {-15.5986211, -5.12114909, -69.3003609, 203.716701, 703.316291,
+                                -1943.49234, 1106.51308, -220.835117, 1432.56989, -3184.81844,
+                                3289.81513, -1353.32119, 19.9956489, -12.7093998, 21.2825156,
+                                -2.75555432, 11.0234982, 148.881951, -751.640284, 637.876542,
+                                12.7093998, -21.2825156, 2.75555432})
+BQP_JB_TABLE(kCxamb, 7, {28.15204, -8.5586e-2, 1.2840e-4, -1.0056e-5, -1.0210e-5,
+                                 1.5044e-6, 9.9826e-8})
+BQP_JB_TABLE(kCht, 4, {0.22, -0.20e-2, 0.115e-2, -0.211e-5})
+BQP_JB_TABLE(kFzm, 5, {0.2689, -0.01176, 0.02782, -0.02782, 0.0003470})
+BQP_JB_TABLE(kGtm, 10, {-0.3633, 0.08506, 0.2401, -0.1897, -0.2554,
+                                -0.01790, 0.0005650, -0.0006407, -0.003418, -0.001252})
+
+constexpr double kAvogadro = 6.02257e26;
+constexpr double kRstar = 8.31432;
+constexpr double kW0 = 0.311111111111111, kW1 = 1.422222222222222, kW2 = 0.533333333333333;
+constexpr double kEarthR = 6356.766;  // US Standard Atmosphere geopotential radius
+constexpr double kG0 = 9.80665;
+constexpr double kLnStepLower = 0.010, kLnStepMiddle = 0.025, kLnStepUpper = 0.075;
+constexpr double kLn10 = 2.302585092994045684;
+
+// Error codes returned as negative densities.
+constexpr double kErrNonFinite = -1.0, kErrAltitude = -2.0, kErrAngle = -3.0, kErrIndex = -4.0,
+                 kErrDomain = -5.0;
+
+struct Drivers {
+    double f10, f10b, s10, s10b, m10, m10b, y10, y10b, dtc;  // dtc: temperature correction, K
+};
+
+BQP_HD double mbar(double z) {
+    double dz = z - 100.0;
+    return dz * (dz * (dz * (dz * (dz * (dz * JBT(kCxamb)[6] + JBT(kCxamb)[5]) + JBT(kCxamb)[4]) + JBT(kCxamb)[3]) +
+                       JBT(kCxamb)[2]) + JBT(kCxamb)[1]) + JBT(kCxamb)[0];
+}
+BQP_HD double grav(double z) {
+    double s = 1.0 + z / kEarthR;
+    return kG0 / (s * s);
+}
+BQP_HD double five_halves(double x) { return x * x * sqrt(x); }
+
+// Local temperature profile: below the 125 km break a polynomial in dz, above
+// it the arctangent approach to the exospheric temperature.
+BQP_HD double local_temp(double z, const double* tc) {
+    double dz = z - 125.0;
+    if (dz <= 0.0) return ((-9.8204695e-6 * dz - 7.3039742e-4) * dz * dz + 1.0) * dz * tc[1] + tc[0];
+    return tc[0] + tc[2] * atan(tc[3] * dz * (1.0 + 4.5e-6 * five_halves(dz)));
+}
+
+// Temperature correction for local solar time and latitude (the DTC term).
+BQP_HD double dtc_correction(double f10, double st_hour, double cs, double alt) {
+    if (!(alt >= 120.0 && alt <= 800.0)) return 0.0;
+    double st = st_hour / 24.0;
+    double fs = (f10 - 100.0) / 100.0;
+    const double* c = JBT(kCdt);
+    const double* b = JBT(kBdt);
+    double p1c = c[0] + fs * (c[1] + st * (c[2] + st * (c[3] + st * (c[4] + st * (c[5] + st * c[6]))))) +
+                 cs * st * (c[7] + st * (c[8] + st * (c[9] + st * (c[10] + st * c[11])))) +
+                 cs * (c[12] + fs * (c[13] + st * (c[14] + st * c[15])));
+    double p2c = c[16] + st * cs * (c[17] + st * (c[18] + st * c[19])) +
+                 fs * cs * (c[20] + st * (c[21] + st * c[22]));
+    double p2b = b[12] + st * (b[13] + st * (b[14] + st * (b[15] + st * (b[16] + st * b[17]))));
+    double p1b_base = b[0] + fs * (b[1] + st * (b[2] + st * (b[3] + st * (b[4] + st * (b[5] + st * b[6])))));
+    double p1b_st = st * (b[7] + st * (b[8] + st * (b[9] + st * (b[10] + st * b[11]))));
+    if (alt > 600.0) {
+        double aa = p1b_base + cs * (p1b_st + 6.0 * p2b + b[18]);
+        double bb = cs * p2b;
+        double cc = -(3.0 * aa + 4.0 * bb) / 4.0;
+        double dd = (aa + bb) / 4.0;
+        double zp = (alt - 600.0) / 100.0;
+        return aa + zp * (bb + zp * (cc + zp * dd));
+    } else if (alt > 300.0) {
+        return p1b_base + cs * (p1b_st + alt * p2b / 100.0 + b[18]);
+    } else if (alt > 240.0) {
+        double bb = p1c;
+        double aa = 0.8 * bb + p2c;
+        double d300 = p1b_base + cs * (p1b_st + 3.0 * p2b + b[18]);
+        double d300dz = cs * p2b;
+        double cc = 3.0 * d300 - d300dz - 3.0 * aa - 2.0 * bb;
+        double dd = d300 - aa - bb - cc;
+        double zp = (alt - 240.0) / 60.0;
+        return aa + zp * (bb + zp * (cc + zp * dd));
+    } else if (alt > 200.0) {
+        return p1c * (alt - 200.0) / 50.0 + p2c;
+    } else {
+        double cc = 3.0 * p2c - p1c;
+        double dd = p2c - cc;
+        double zp = (alt - 120.0) / 80.0;
+        return zp * zp * (cc + dd * zp);
+    }
+}
+
+// Day of year from a UTC MJD, the model's own 4-year-cycle arithmetic.
+BQP_HD double day_of_year(double mjd, bool* ok) {
+    double d1950 = mjd - 33281.0;
+    double tr = trunc(d1950);
+    if (!(fabs(tr) < 2.0e9)) {
+        *ok = false;
+        return 0.0;
+    }
+    long long iy = (long long)tr;
+    double frac = d1950 - (double)iy;
+    iy += 364;
+    long long it = iy / 1461;
+    iy -= it * 1461;
+    it = iy / 365;
+    if (it > 3) it = 3;
+    iy = iy - 365 * it + 1;
+    *ok = true;
+    return (double)iy + frac;
+}
+
+// One Boole-rule sweep of `n` log-spaced intervals from z (exclusive carry
+// `ain` at the start node).  kind 0: integrand mbar*g/T, else g/T.
+struct Sweep {
+    double sum, z, zend, tloc, gravl, mb, ain;
+};
+
+BQP_HD Sweep boole_sweep(double z, double zend_start, double zr, int n, double ain, bool with_mbar,
+                         const double* tc) {
+    Sweep s;
+    s.sum = 0.0;
+    s.zend = zend_start;
+    s.z = z;
+    s.tloc = 0.0;
+    s.gravl = 0.0;
+    s.mb = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double zz = s.zend;
+        s.zend = zr * zz;
+        double dz = 0.25 * (s.zend - zz);
+        double sum1 = kW0 * ain;
+#pragma unroll
+        for (int j = 1; j < 5; ++j) {
+            zz += dz;
+            s.tloc = local_temp(zz, tc);
+            s.gravl = grav(zz);
+            if (with_mbar) {
+                s.mb = mbar(zz);
+                ain = s.mb * s.gravl / s.tloc;
+            } else {
+                ain = s.gravl / s.tloc;
+            }
+            double w = (j == 1 || j == 3) ? kW1 : (j == 2 ? kW2 : kW0);
+            sum1 += w * ain;
+        }
+        s.sum += dz * sum1;
+        s.z = zz;
+    }
+    s.ain = ain;
+    return s;
+}
+
+// Density (kg/m^3) for: UTC MJD, solar declination, local hour angle of the
+// satellite relative to the Sun (rad), geocentric latitude (rad), altitude
+// (m) and the driver set.  Non-positive returns are the error codes above.
+BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
+                      const Drivers& d) {
+    if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) ||
+        !isfinite(alt_m) || !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) ||
+        !isfinite(d.s10b) || !isfinite(d.m10) || !isfinite(d.m10b) || !isfinite(d.y10) ||
+        !isfinite(d.y10b) || !isfinite(d.dtc))
+        return kErrNonFinite;
+    if (alt_m < 90000.0) return kErrAltitude;
+    if (!(sun_dec >= -kPi / 2 && sun_dec <= kPi / 2) || !(lat >= -kPi / 2 && lat <= kPi / 2))
+        return kErrAngle;
+    if (d.f10 <= 0.0 || d.f10b <= 0.0 || d.s10 <= 0.0 || d.s10b <= 0.0 || d.m10 <= 0.0 ||
+        d.m10b <= 0.0 || d.y10 <= 0.0 || d.y10b <= 0.0)
+        return kErrIndex;
+    double alt = alt_m / 1000.0;
+    // exospheric temperature
+    double fn = fmin(pow(d.f10b / 240.0, 0.25), 1.0);
+    double fsb = d.f10b * fn + d.s10b * (1.0 - fn);
+    double tsubc = 392.4 + 3.227 * fsb + 0.298 * (d.f10 - d.f10b) + 2.259 * (d.s10 - d.s10b) +
+                   0.312 * (d.m10 - d.m10b) + 0.178 * (d.y10 - d.y10b);
+    double eta = 0.5 * fabs(lat - sun_dec);
+    double theta = 0.5 * fabs(lat + sun_dec);
+    double h = hour_angle;
+    if (!(h >= 0.0 && h < kTwoPi)) {
+        if (h < 0.0 && h > -kTwoPi) {
+            h += kTwoPi;
+        } else {
+            h = fmod(h, kTwoPi);
+            if (h < 0.0) h += kTwoPi;
+        }
+    }
+    double tau = h - 0.64577182 + 0.10471976 * sin(h + 0.75049158);
+    double st_hour = ((h + kPi) * (180.0 / kPi)) / 15.0;
+    if (st_hour >= 24.0) st_hour -= 24.0;
+    else if (st_hour < 0.0) st_hour += 24.0;
+    double slat, clat;
+    sincos(lat, &slat, &clat);
+    double cos_eta = five_halves(cos(eta));
+    double sin_theta = five_halves(sin(theta));
+    double cos_tau = fabs(cos(0.5 * tau));
+    double df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
+    double tsubl = tsubc * (1.0 + 0.31 * df);
+    double tinf = tsubl + d.dtc + dtc_correction(d.f10, st_hour, clat, alt);
+    double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * exp(-0.0021357 * tinf);
+    double gsubx = 0.054285714 * (tsubx - 183.0);
+    double tc[4];
+    tc[0] = tsubx;
+    tc[1] = gsubx;
+    tc[2] = (tinf - tsubx) / (kPi / 2);
+    tc[3] = gsubx / tc[2];
+    // 90 km -> min(alt, 105 km)
+    const double z1 = 90.0;
+    double al = log(fmin(alt, 105.0) / z1);
+    int n = 1 + (int)floor(al / kLnStepLower);
+    double zr = exp(al / n);
+    double mb1 = mbar(z1);
+    double tloc1 = local_temp(z1, tc);
+    Sweep lo = boole_sweep(z1, z1, zr, n, mb1 * grav(z1) / tloc1, true, tc);
+    double mb2 = lo.mb, tloc2 = lo.tloc;
+    double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
+    double anm = kAvogadro * rho;
+    double an = anm / mb2;
+    double fact2 = anm / 28.960;
+    double fac[5] = {JBT(kFrac)[0] * fact2, fact2 * (1.0 + JBT(kFrac)[1]) - an, 2.0 * (an - fact2),
+                     JBT(kFrac)[2] * fact2, JBT(kFrac)[3] * fact2};
+    double aln[6];
+    for (int i = 0; i < 5; ++i) aln[i] = fac[i] < 0.0 ? NAN : log(fac[i]);
+    double z = lo.z;
+    if (alt <= 105.0) {
+        aln[5] = aln[4] - 25.0;
+    } else {
+        // 105 km -> min(alt, 500 km)
+        al = log(fmin(alt, 500.0) / z);
+        n = 1 + (int)floor(al / kLnStepMiddle);
+        zr = exp(al / n);
+        Sweep mid = boole_sweep(z, lo.zend, zr, n, lo.gravl / tloc2, false, tc);
+        double tloc3 = mid.tloc;
+        z = mid.z;
+        // between 500 km and alt (hydrogen is anchored at 500 km)
+        al = log(fmax(alt, 500.0) / z);
+        n = 1 + (int)floor(al / (alt > 500.0 ? kLnStepUpper : kLnStepMiddle));
+        zr = exp(al / n);
+        Sweep up = boole_sweep(z, mid.zend, zr, n, mid.ain, false, tc);
+        double tloc4 = up.tloc;
+        z = up.z;
+        double altr, hsign;
+        if (alt <= 500.0) {
+            altr = log(tloc3 / tloc2);
+            fact2 = mid.sum / kRstar;
+            hsign = 1.0;
+        } else {
+            altr = log(tloc4 / tloc2);
+            fact2 = (mid.sum + up.sum) / kRstar;
+            hsign = -1.0;
+        }
+        for (int i = 0; i < 4; ++i) aln[i] = aln[i] - altr - fact2 * JBT(kAmw)[i];
+        aln[4] = aln[4] - (1.0 - 0.38) * altr - fact2 * JBT(kAmw)[4];
+        double al10t5 = log10(tinf);
+        double alnh5 = (5.5 * al10t5 - 39.40) * al10t5 + 73.13;
+        aln[5] = kLn10 * (alnh5 + 6.0) + hsign * (log(tloc4 / tloc3) + up.sum * JBT(kAmw)[5] / kRstar);
+    }
+    // seasonal-latitudinal variation
+    double years = (mjd - 36204.0) / 365.2422;
+    double capphi = years - trunc(years);
+    if (capphi == 0.0) capphi = copysign(0.0, years);
+    double sgn = lat >= 0.0 ? 1.0 : -1.0;
+    double hm90 = alt - 90.0;
+    double dlrsl = 0.02 * hm90 * exp(-0.045 * hm90) * sgn * sin(kTwoPi * capphi + 1.72) * slat * slat;
+    // semiannual variation
+    double dlrsa = 0.0;
+    if (z < 2000.0) {
+        bool ok = true;
+        double day = day_of_year(mjd, &ok);
+        if (!ok) return kErrDomain;
+        double htz = alt / 1000.0;
+        double fsmb = d.f10b - 0.70 * d.s10b - 0.04 * d.m10b;
+        double fzz = JBT(kFzm)[0] + JBT(kFzm)[1] * fsmb + JBT(kFzm)[2] * fsmb * htz + JBT(kFzm)[3] * fsmb * htz * htz +
+                     JBT(kFzm)[4] * fsmb * fsmb * htz;
+        fsmb = d.f10b - 0.75 * d.s10b - 0.37 * d.m10b;
+        double s1, c1;
+        sincos(kTwoPi * (day - 1.0) / 365.0, &s1, &c1);
+        double s2 = 2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
+        double gtz = JBT(kGtm)[0] + JBT(kGtm)[1] * s1 + JBT(kGtm)[2] * c1 + JBT(kGtm)[3] * s2 + JBT(kGtm)[4] * c2 +
+                     JBT(kGtm)[5] * fsmb + JBT(kGtm)[6] * fsmb * s1 + JBT(kGtm)[7] * fsmb * c1 + JBT(kGtm)[8] * fsmb * s2 +
+                     JBT(kGtm)[9] * fsmb * c2;
+        dlrsa = fmax(fzz, 1.0e-6) * gtz;
+    }
+    double dlr = kLn10 * (dlrsl + dlrsa);
+    double sumnm = 0.0;
+    for (int i = 0; i < 6; ++i) sumnm += exp(aln[i] + dlr) * JBT(kAmw)[i];
+    rho = sumnm / kAvogadro;
+    double fex = 1.0;
+    if (alt >= 1000.0 && alt < 1500.0) {
+        double zeta = (alt - 1000.0) * 0.002;
+        double f15c = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * 1500.0 + JBT(kCht)[3] * d.f10b * 1500.0;
+        double f15cz = (JBT(kCht)[2] + JBT(kCht)[3] * d.f10b) * 500.0;
+        double fex2 = 3.0 * f15c - f15cz - 3.0;
+        double fex3 = f15cz - 2.0 * f15c + 2.0;
+        fex = 1.0 + zeta * zeta * (fex2 + fex3 * zeta);
+    } else if (alt >= 1500.0) {
+        fex = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * alt + JBT(kCht)[3] * d.f10b * alt;
+    }
+    double out = rho * fex;
+    if (!(isfinite(out) && out > 0.0)) return kErrDomain;
+    return out;
+}
+
+}  // namespace jb
+}  // namespace bqp

@@ -1,0 +1,162 @@
+// Device side of the batched propagator: the Encke force call and the
+// one-trajectory-per-thread adaptive RK driver (DOPRI5(4), DOP853 and the
+// DOPRI5 compatibility loop), as a persistent kernel that pulls trajectories
+// from a device work queue.
+#pragma once
+#include <cstdint>
+
+#include "gravity.cuh"
+#include "jb2008.cuh"
+#include "physics.cuh"
+
+namespace bqp {
+
+// Per-trajectory status words (mirroring the reference's IntegrationStatus,
+// GravityError and FinalPropagationFailure; values are part of the C ABI).
+enum Status : int32_t {
+    kOk = 0,
+    kMaxSteps = 1,
+    kStepUnderflow = 2,
+    kInvalidInput = 3,
+    kNonFinite = 4,
+    kMaxRejects = 5,
+    kGravityRadius = 6,
+    kRebaseFailed = 7,
+    kRestartBudget = 8,
+    kGround = 9,
+    kWatchdog = 10,
+};
+
+enum Method : int32_t { kDopri5 = 0, kDop853 = 1, kDopri5Compat = 2 };
+
+// Force switches and constants (ForceConfig, types.rs:332-411).
+struct ForceParams {
+    int32_t order;
+    int32_t gravity_on;
+    int32_t drag, sun, moon;
+    int32_t ground_check;  // terminal ground event (final-state path)
+    double earth_radius;
+    double omega;
+    double mu_sun, mu_moon;
+    jb::Drivers drivers;
+};
+
+// Solver controls (IntegratorConfig, solver.rs:35-60 and integrator.rs:404-558).
+struct CtrlParams {
+    int32_t scaled;  // 0: absolute eps, max-norm; 1: rtol/atol, WRMS
+    int32_t max_rejects;
+    double eps, rtol, atol;
+    double h_min, h_max;
+    int64_t max_steps;        // per segment
+    int64_t max_attempts;     // per trajectory, device watchdog
+    int64_t max_kernel_ns;    // wall-clock watchdog of one launch (0: none)
+};
+
+// Nanosecond global timer (PTX %globaltimer).
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// One Encke force evaluation: derivative of the deviation `d` from the
+// baseline orbit (rhs.rs:3885-4118).  Gravity uses the field table without
+// its C00 term, which equals the reference's full field followed by the
+// analytic removal of mu r/r^3.
+struct Encke {
+    const double* tab;
+    const ForceParams* fp;
+    Baseline base;
+    double seg_t0;
+    double jd0;
+    double am, cd;
+    int bad;  // latched invalid-radius gravity error
+
+    __device__ __noinline__ void eval(double t, const double* d, double* out) {
+        double rs[6];
+        baseline_state(base, t - seg_t0, rs);
+        double sp[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sp[i] = rs[i] + d[i];
+        const double r2 = fma(sp[0], sp[0], fma(sp[1], sp[1], sp[2] * sp[2]));
+        const double r = sqrt(r2);
+        double acc[3] = {0.0, 0.0, 0.0};
+        const double jd = jd0 + t / kSecPerDay;
+        double s = 0.0, c = 1.0;
+        if (fp->gravity_on || fp->drag) sincos(gmst_rad(jd), &s, &c);
+        double pi[3];
+        pi[0] = fma(c, sp[0], s * sp[1]);
+        pi[1] = fma(-s, sp[0], c * sp[1]);
+        pi[2] = sp[2];
+        if (fp->gravity_on) {
+            if (!(isfinite(r2) && r2 > 0.0)) bad = 1;
+            double ai[3];
+            gravity_field(tab, fp->order, pi[0], pi[1], pi[2], ai);
+            acc[0] = fma(c, ai[0], -s * ai[1]);
+            acc[1] = fma(s, ai[0], c * ai[1]);
+            acc[2] = ai[2];
+        }
+        double sun[3];
+        bool have_sun = false;
+        if (fp->drag && cd != 0.0 && am != 0.0) {
+            sun_position(jd, sun);
+            have_sun = true;
+            double rho = density_at(pi, sun, s, c, jd);
+            if (isnan(rho)) {
+                acc[0] = acc[1] = acc[2] = NAN;
+            } else if (rho > 0.0) {
+                // co-rotating atmosphere, m/s inside, km/s^2 out (rhs.rs:1119-1163)
+                const double w = fp->omega;
+                const double vr0 = (sp[3] + w * sp[1]) * 1000.0;
+                const double vr1 = (sp[4] - w * sp[0]) * 1000.0;
+                const double vr2 = sp[5] * 1000.0;
+                const double v2 = fma(vr0, vr0, fma(vr1, vr1, vr2 * vr2));
+                if (v2 != 0.0) {
+                    const double k = -0.5 * cd * am * rho * sqrt(v2) * 1e-3;
+                    acc[0] += k * vr0;
+                    acc[1] += k * vr1;
+                    acc[2] += k * vr2;
+                }
+            }
+        }
+        if (fp->sun) {
+            if (!have_sun) sun_position(jd, sun);
+            third_body(sp, sun, fp->mu_sun, acc);
+        }
+        if (fp->moon) {
+            double moon[3];
+            moon_position(jd, moon);
+            third_body(sp, moon, fp->mu_moon, acc);
+        }
+        battin(rs, d, r2, r, acc);
+        out[0] = d[3];
+        out[1] = d[4];
+        out[2] = d[5];
+        out[3] = acc[0];
+        out[4] = acc[1];
+        out[5] = acc[2];
+    }
+
+    // JB2008 adapter (rhs.rs:3551-3776): Earth-fixed satellite and Sun,
+    // geocentric latitude, WGS84 altitude, exospheric ceiling above 2500 km.
+    __device__ __forceinline__ double density_at(const double* pi, const double* sun, double s,
+                                                 double c, double jd) const {
+        double si[3];
+        si[0] = fma(c, sun[0], s * sun[1]);
+        si[1] = fma(-s, sun[0], c * sun[1]);
+        si[2] = sun[2];
+        const double sun_r = sqrt(fma(si[0], si[0], fma(si[1], si[1], si[2] * si[2])));
+        const double sat_r = sqrt(fma(pi[0], pi[0], fma(pi[1], pi[1], pi[2] * pi[2])));
+        if ((sat_r - fp->earth_radius) * 1000.0 > 2500.0e3) return 1.0e-19;
+        const double alt_m = geodetic_altitude_km(pi[0], pi[1], pi[2], fp->earth_radius) * 1000.0;
+        const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
+        const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
+        const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
+        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, fp->drivers);
+        if (!(rho > 0.0) || !isfinite(rho)) return NAN;
+        if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
+        return rho;
+    }
+};
+
+}  // namespace bqp

@@ -1,0 +1,45 @@
+// Launch interface between the C ABI (bqp_api.cu) and the kernels (propagate.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace bqp {
+
+// Arguments of k_propagate (all device pointers).
+struct PropArgs {
+    int64_t n;                     // trajectories
+    const double* in;              // [n][6] ECI or equinoctial at t0
+    int32_t input_equinoctial;
+    const double* epoch;           // [n] JD (UTC) of t = 0
+    double t0;                     // common start, seconds after epoch
+    const double* tf;              // [n] end time, seconds after epoch
+    const double* ballistic;       // [n][2] (A/m m^2/kg, Cd) or null
+    double am0, cd0;               // defaults when ballistic is null
+    const double* t_eval;          // [n_t] common sample grid (sampled modes)
+    int32_t n_t;
+    int32_t out_mode;              // 0 final ECI [n][6]; 1 sampled ECI; 2 sampled deltas [n][n_t][6]
+    double* out;
+    int32_t* status;               // [n]
+    int64_t* steps;                // [n] or null
+    int64_t* evals;                // [n] or null
+    unsigned long long* queue;     // work-queue head, zeroed before launch
+    const double* gtab;            // gravity table (global)
+    int32_t ncells;
+    int32_t use_smem;
+    ForceParams force;
+    CtrlParams ctrl;
+};
+
+cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
+                           const double* pos, double* acc, int32_t* status, cudaStream_t st);
+cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,
+                       const double* equ, const double* seg_t0, const double* jd0, const double* t,
+                       const double* delta, const double* ballistic, double am0, double cd0,
+                       double* out, cudaStream_t st);
+cudaError_t launch_propagate(const PropArgs& A, int method, int threads, int blocks, cudaStream_t st);
+int device_sm_count();
+
+}  // namespace bqp

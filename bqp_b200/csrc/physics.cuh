@@ -1,0 +1,322 @@
+// Force-model and element physics shared by the host API and the sm_100a
+// kernels (FP64).  Every function here is __host__ __device__ so the host can
+// run the same arithmetic for set-up (element conversion of inputs, table
+// builds) as the kernels use in the hot loop.
+//
+// Conventions (dust_transfer/src/lib.rs:1-24 of the reference): km, km/s, s,
+// Julian Date (UTC); the inertial frame is the propagator's ECI, the gravity
+// field is Earth-fixed; states are [x, y, z, vx, vy, vz].
+#pragma once
+#include <cmath>
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define BQP_HD __host__ __device__ __forceinline__
+#else
+#define BQP_HD inline
+#endif
+
+namespace bqp {
+
+// satpy_core/src/lib.rs:70-113 (reference constants, carried verbatim)
+constexpr double kEarthOmega = 7.2921150e-5;        // rad/s
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kPi = 3.14159265358979323846264338327950;
+constexpr double kGmstSec2Rad = (2.0 * kPi) / 86400.0;
+constexpr double kGmstLinear = 8640184.812866 + 876600.0 * 3600.0;
+constexpr double kGmstConst = 67310.54841;
+constexpr double kMu = 398600.4415;                 // km^3/s^2
+constexpr double kInvMu = 1.0 / 398600.4415;
+constexpr double kReWgs84 = 6378.137;               // km, figure of the Earth
+constexpr double kReGravity = 6378.13646;           // km, DIR-R6 reference radius
+constexpr double kWgs84F = 1.0 / 298.257223563;
+constexpr double kKeplerTol = 1e-12;
+constexpr int kKeplerMaxIter = 500;
+constexpr double kSecPerDay = 86400.0;
+constexpr double kMaxSegmentS = 5400.0;             // integrator.rs:236
+constexpr double kRebaseKm = 10.0;                  // types.rs:138
+constexpr double kGroundAltitudeKm = 100.0;         // types.rs:140
+
+BQP_HD double mod2pi(double a) {
+    if (!isfinite(a)) return NAN;
+    double x = fmod(a, kTwoPi);
+    if (x < 0.0) x += kTwoPi;
+    if (x >= kTwoPi) x -= kTwoPi;
+    return x == 0.0 ? 0.0 : x;
+}
+
+BQP_HD double clamp_ecc(double e) {
+    if (!isfinite(e) || e <= 0.0) return 0.0;
+    if (e >= 1.0) {
+        double c = 1.0 - 10.0 * kKeplerTol;
+        return c > 0.0 ? c : 0.0;
+    }
+    return e;
+}
+
+// Greenwich mean sidereal angle of a UTC Julian Date (satpy lib.rs:905-912).
+BQP_HD double gmst_rad(double jd) {
+    double t = (jd - 2451545.0) / 36525.0;
+    double sec = fma(fma(fma(-6.2e-6, t, 0.093104), t, kGmstLinear), t, kGmstConst);
+    return mod2pi(sec * kGmstSec2Rad);
+}
+
+// ----------------------------------------------------------------- elements
+// Equinoctial elements [a, h, k, p, q, L] (retrograde-singular form) from an
+// ECI state (satpy lib.rs:1879-2012).  Returns false (and NaNs) for an
+// unbound or degenerate orbit.
+BQP_HD bool eci_to_equinoctial(const double* st, double* out) {
+    double rx = st[0], ry = st[1], rz = st[2], vx = st[3], vy = st[4], vz = st[5];
+    double rn = sqrt(rx * rx + ry * ry + rz * rz);
+    double vn = sqrt(vx * vx + vy * vy + vz * vz);
+    double inv_r = 1.0 / rn;
+    double energy = fma(0.5, vn * vn, -kMu * inv_r);
+    bool ok = energy < -1e-12;
+    double hx = ry * vz - rz * vy, hy = rz * vx - rx * vz, hz = rx * vy - ry * vx;
+    double hn = sqrt(hx * hx + hy * hy + hz * hz);
+    double inv_h = 1.0 / hn;
+    double tx = vy * hz - vz * hy, ty = vz * hx - vx * hz, tz = vx * hy - vy * hx;
+    double ex = fma(tx, kInvMu, -rx * inv_r);
+    double ey = fma(ty, kInvMu, -ry * inv_r);
+    double ez = fma(tz, kInvMu, -rz * inv_r);
+    double emag = sqrt(ex * ex + ey * ey + ez * ez);
+    double es = (!isfinite(emag) || emag <= 0.0) ? 0.0 : (emag >= 1.0 ? 1.0 - 1e-11 : emag);
+    double a = -kMu / (2.0 * energy);
+    ok = ok && a > 0.0;
+    double nz = hz * inv_h;
+    double dh = 1.0 + nz;
+    double hc = fabs(dh) < 1e-12 ? 0.0 : (1.0 - nz) / dh;
+    double p = (1.0 + hc) * hx * inv_h * 0.5;
+    double q = -(1.0 + hc) * hy * inv_h * 0.5;
+    double p2 = p * p, q2 = q * q, tpq = 2.0 * p * q;
+    double coef = 1.0 / fma(p2, 1.0, fma(q2, 1.0, 1.0));
+    double xh0 = coef * fma(q2, 1.0, 1.0 - p2), xh1 = coef * tpq, xh2 = coef * (-2.0 * p);
+    double yh0 = coef * tpq, yh1 = coef * fma(p2, 1.0, 1.0 - q2), yh2 = coef * (2.0 * q);
+    double hv = yh0 * ex + yh1 * ey + yh2 * ez;
+    double kv = xh0 * ex + xh1 * ey + xh2 * ez;
+    double xd = xh0 * vx + xh1 * vy + xh2 * vz;
+    double yd = yh0 * vx + yh1 * vy + yh2 * vz;
+    double sqrt_ma = sqrt(kMu * a);
+    double coef2 = rn / sqrt_ma;
+    double sq = sqrt(fmax(1.0 - es * es, 0.0));
+    double ds = 1.0 + sq;
+    double sds = fabs(ds) < 1e-12 ? (ds >= 0.0 ? 1e-12 : -1e-12) : ds;
+    double coef3 = (rn * (1.0 / a) - 1.0) / sds;
+    double sf = fma(-xd, coef2, -hv * coef3);
+    double cf = fma(yd, coef2, -kv * coef3);
+    double fa = atan2(sf, cf);
+    double sfa, cfa;
+    sincos(fa, &sfa, &cfa);
+    double lam = fa + fma(hv, cfa, -kv * sfa);
+    if (isfinite(lam)) {
+        lam = fmod(lam, kTwoPi);
+        if (lam < 0.0) lam += kTwoPi;
+        if (lam >= kTwoPi) lam -= kTwoPi;
+    } else {
+        lam = NAN;
+    }
+    out[0] = a; out[1] = hv; out[2] = kv; out[3] = p; out[4] = q; out[5] = lam;
+    ok = ok && isfinite(a) && isfinite(hv) && isfinite(kv) && isfinite(p) && isfinite(q) &&
+         isfinite(lam);
+    if (!ok)
+        for (int i = 0; i < 6; ++i) out[i] = NAN;
+    return ok;
+}
+
+// Analytic two-body baseline from equinoctial elements (the Encke reference
+// orbit; satpy lib.rs:2191-2374): element-only terms are hoisted here, the
+// per-time half solves the equinoctial Kepler equation F + h cosF - k sinF = L
+// by Halley-type iteration.
+struct Baseline {
+    double a, h, k, n, ecoef, L0;
+    double xh0, xh1, xh2, yh0, yh1, yh2;
+    int ok;
+};
+
+BQP_HD Baseline baseline_new(const double* e) {
+    Baseline b;
+    b.ok = 0;
+    double a = e[0], h = e[1], k = e[2], p = e[3], q = e[4];
+    b.a = a; b.h = h; b.k = k; b.L0 = e[5];
+    double er = sqrt(fma(h, h, k * k));
+    double ecc = clamp_ecc(er);
+    double p2 = p * p, q2 = q * q;
+    double coef = 1.0 / fma(p2, 1.0, fma(q2, 1.0, 1.0));
+    b.n = sqrt(kMu / (a * a * a));
+    b.ecoef = 1.0 + sqrt(fmax(fma(ecc, -ecc, 1.0), 0.0));
+    b.xh0 = coef * fma(q2, 1.0, 1.0 - p2);
+    b.xh1 = coef * (2.0 * p * q);
+    b.xh2 = coef * (-2.0 * p);
+    b.yh0 = coef * (2.0 * p * q);
+    b.yh1 = coef * fma(p2, 1.0, 1.0 - q2);
+    b.yh2 = coef * (2.0 * q);
+    b.ok = (a > 0.0 && er < 1.0) ? 1 : 0;
+    return b;
+}
+
+// State on the baseline orbit `tof` seconds after the elements' epoch.
+// Returns false (out[0] = NaN) if the baseline is invalid or the iteration
+// does not converge.
+BQP_HD bool baseline_state(const Baseline& b, double tof, double* out) {
+    if (!b.ok) {
+        for (int i = 0; i < 6; ++i) out[i] = NAN;
+        return false;
+    }
+    double L = mod2pi(b.L0 + b.n * tof);
+    double F = L;
+    double sF, cF;
+    sincos(F, &sF, &cF);
+    int it = 0;
+    for (; it < kKeplerMaxIter; ++it) {
+        double at = b.h * cF - b.k * sF;
+        double bt = b.h * sF + b.k * cF;
+        double f0 = F + at - L;
+        double f1 = 1.0 - bt;
+        double d1 = -f0 / f1;
+        double d2 = -f0 / (f1 + 0.5 * d1 * (-at));
+        double d3 = -f0 / (f1 + 0.5 * d2 * (-at) + (1.0 / 6.0) * d2 * d2 * bt);
+        F = F + d3;
+        if (fabs(d3) < kKeplerTol) break;
+        double sd, cd;
+        sincos(d3, &sd, &cd);
+        double sn = fma(sF, cd, cF * sd);
+        cF = fma(cF, cd, -sF * sd);
+        sF = sn;
+    }
+    if (it == kKeplerMaxIter) {
+        for (int i = 0; i < 6; ++i) out[i] = NAN;
+        return false;
+    }
+    double cl = (L - F) / b.ecoef;
+    double X = b.a * (cF - b.k - b.h * cl);
+    double Y = b.a * (sF - b.h + b.k * cl);
+    double px = b.xh0 * X + b.yh0 * Y;
+    double py = b.xh1 * X + b.yh1 * Y;
+    double pz = b.xh2 * X + b.yh2 * Y;
+    double rn = sqrt(fma(px, px, fma(py, py, pz * pz)));
+    double Fd = b.a * b.n / rn;
+    double c3 = (b.n - Fd) / b.ecoef;
+    double Xd = b.a * fma(-Fd, sF, -b.h * c3);
+    double Yd = b.a * fma(Fd, cF, b.k * c3);
+    out[0] = px; out[1] = py; out[2] = pz;
+    out[3] = b.xh0 * Xd + b.yh0 * Yd;
+    out[4] = b.xh1 * Xd + b.yh1 * Yd;
+    out[5] = b.xh2 * Xd + b.yh2 * Yd;
+    return true;
+}
+
+BQP_HD bool equinoctial_to_eci(const double* e, double tof, double* out) {
+    Baseline b = baseline_new(e);
+    return baseline_state(b, tof, out);
+}
+
+// ---------------------------------------------------------------- ephemeris
+// Low-precision analytic Sun and Moon positions (Montenbruck & Gill,
+// "Satellite Orbits", 2000, section 3.3.2), J2000 equator/equinox, km.  The
+// reference reads precomputed tables (precomputed_ephem.rs); these series
+// stand in for them with the same force formula downstream.
+constexpr double kDeg = kPi / 180.0;
+constexpr double kArcsec = kDeg / 3600.0;
+constexpr double kObliquity = 23.43929111 * kDeg;
+
+BQP_HD void sun_position(double jd, double* out) {
+    double T = (jd - 2451545.0) / 36525.0;
+    double M = mod2pi((357.5256 + 35999.049 * T) * kDeg);
+    double sM, cM;
+    sincos(M, &sM, &cM);
+    double s2M = 2.0 * sM * cM, c2M = cM * cM - sM * sM;
+    double lam = 282.9400 * kDeg + M + 6892.0 * kArcsec * sM + 72.0 * kArcsec * s2M;
+    double r = (149.619 - 2.499 * cM - 0.021 * c2M) * 1e6;
+    double sl, cl;
+    sincos(lam, &sl, &cl);
+    const double ce = 0.9174820620768958, se = 0.3977771559141214;  // cos, sin of 23.43929111 deg
+    out[0] = r * cl;
+    out[1] = ce * (r * sl);
+    out[2] = se * (r * sl);
+}
+
+BQP_HD void moon_position(double jd, double* out) {
+    double T = (jd - 2451545.0) / 36525.0;
+    double L0 = mod2pi((218.31617 + 481267.88088 * T - 1.3972 * T) * kDeg);
+    double l = mod2pi((134.96292 + 477198.86753 * T) * kDeg);
+    double lp = mod2pi((357.52543 + 35999.04944 * T) * kDeg);
+    double F = mod2pi((93.27283 + 483202.01873 * T) * kDeg);
+    double D = mod2pi((297.85027 + 445267.11135 * T) * kDeg);
+    double dlam = 22640.0 * sin(l) + 769.0 * sin(2.0 * l) - 4586.0 * sin(l - 2.0 * D) +
+                  2370.0 * sin(2.0 * D) - 668.0 * sin(lp) - 412.0 * sin(2.0 * F) -
+                  212.0 * sin(2.0 * l - 2.0 * D) - 206.0 * sin(l + lp - 2.0 * D) +
+                  192.0 * sin(l + 2.0 * D) - 165.0 * sin(lp - 2.0 * D) + 148.0 * sin(l - lp) -
+                  125.0 * sin(D) - 110.0 * sin(l + lp) - 55.0 * sin(2.0 * F - 2.0 * D);
+    double lam = L0 + dlam * kArcsec;
+    double beta = 18520.0 * sin(F + lam - L0 + (412.0 * sin(2.0 * F) + 541.0 * sin(lp)) * kArcsec) -
+                  526.0 * sin(F - 2.0 * D) + 44.0 * sin(l + F - 2.0 * D) - 31.0 * sin(-l + F - 2.0 * D) -
+                  25.0 * sin(-2.0 * l + F) - 23.0 * sin(lp + F - 2.0 * D) + 21.0 * sin(-l + F) +
+                  11.0 * sin(-lp + F - 2.0 * D);
+    beta *= kArcsec;
+    double r = 385000.0 - 20905.0 * cos(l) - 3699.0 * cos(2.0 * D - l) - 2956.0 * cos(2.0 * D) -
+               570.0 * cos(2.0 * l) + 246.0 * cos(2.0 * l - 2.0 * D) - 205.0 * cos(lp - 2.0 * D) -
+               171.0 * cos(l + 2.0 * D) - 152.0 * cos(l + lp - 2.0 * D);
+    double sb, cb, sl, cl;
+    sincos(beta, &sb, &cb);
+    sincos(lam, &sl, &cl);
+    double xe = r * cb * cl, ye = r * cb * sl, ze = r * sb;
+    const double ce = 0.9174820620768958, se = 0.3977771559141214;
+    out[0] = xe;
+    out[1] = ce * ye - se * ze;
+    out[2] = se * ye + ce * ze;
+}
+
+// Point-mass third body in the normalised form of rhs.rs:1326-1354.
+BQP_HD void third_body(const double* sat, const double* body, double mu_body, double* acc) {
+    double d2 = body[0] * body[0] + body[1] * body[1] + body[2] * body[2];
+    if (d2 == 0.0) return;
+    double inv_d = 1.0 / sqrt(d2);
+    double mu_coef = mu_body * (inv_d * inv_d);
+    double bn0 = body[0] * inv_d, bn1 = body[1] * inv_d, bn2 = body[2] * inv_d;
+    double r0 = bn0 - sat[0] * inv_d, r1 = bn1 - sat[1] * inv_d, r2 = bn2 - sat[2] * inv_d;
+    double rd2 = fma(r0, r0, fma(r1, r1, r2 * r2));
+    if (rd2 == 0.0) return;
+    double inv3 = 1.0 / (rd2 * sqrt(rd2));
+    acc[0] += mu_coef * (r0 * inv3 - bn0);
+    acc[1] += mu_coef * (r1 * inv3 - bn1);
+    acc[2] += mu_coef * (r2 * inv3 - bn2);
+}
+
+// Battin's f(q) form of the Encke central-body difference (rhs.rs:1071-1104):
+// mu (r_b/|r_b|^3 - r_p/|r_p|^3) = mu/|r_p|^3 (f(q) r_b - dr).
+BQP_HD void battin(const double* rb, const double* dr, double rp2, double rp, double* acc) {
+    double rb2 = fma(rb[0], rb[0], fma(rb[1], rb[1], rb[2] * rb[2]));
+    if (!(rb2 > 0.0 && rp2 > 0.0)) return;
+    double ddot = fma(dr[0], rb[0], fma(dr[1], rb[1], dr[2] * rb[2]));
+    double dsq = fma(dr[0], dr[0], fma(dr[1], dr[1], dr[2] * dr[2]));
+    double q = (dsq + 2.0 * ddot) / rb2;
+    double q1 = 1.0 + q;
+    double fq = q * (3.0 + q * (3.0 + q)) / (1.0 + q1 * sqrt(q1));
+    double k = kMu * (1.0 / (rp2 * rp));
+    acc[0] += k * fma(fq, rb[0], -dr[0]);
+    acc[1] += k * fma(fq, rb[1], -dr[1]);
+    acc[2] += k * fma(fq, rb[2], -dr[2]);
+}
+
+// WGS84 geodetic altitude of an Earth-fixed position, one Bowring step
+// (rhs.rs:160-186).
+BQP_HD double geodetic_altitude_km(double x, double y, double z, double a) {
+    const double omf = 1.0 - kWgs84F;
+    const double e2 = kWgs84F * (2.0 - kWgs84F);
+    const double ep2 = e2 / (omf * omf);
+    double req = sqrt(fma(x, x, y * y));
+    if (req == 0.0) return fabs(z) - a * omf;
+    double b = a * omf;
+    double tn = z * a, td = req * b;
+    double tr = sqrt(fma(tn, tn, td * td));
+    double st = tn / tr, ct = td / tr;
+    double ln = z + ep2 * b * st * st * st;
+    double ld = req - e2 * a * ct * ct * ct;
+    double lr = sqrt(fma(ln, ln, ld * ld));
+    double sl = ln / lr, cl = ld / lr;
+    double om = 1.0 - e2 * sl * sl;
+    double nrad = a / sqrt(om);
+    return req * cl + z * sl - nrad * om;
+}
+
+}  // namespace bqp

@@ -1,0 +1,99 @@
+"""Seeded synthetic inputs of the benchmark configurations.
+
+No public dataset is involved: every input is generated here with
+``numpy.random.default_rng`` so the GPU path, the CPU oracle and the CPU
+baseline all see identical arrays.
+
+* ``synthetic_field(order, seed)``: normalised coefficients, C20 = -4.84165e-4,
+  every other C_nm, S_nm ~ N(0, (1e-5/n^2)^2) for n >= 2 (S_n0 = 0, degree 1
+  zero) -- the "synthetic N x N normalised field / Kaula rule" of the configs,
+  written as ``deg ord C S`` text (the reference loader's format).
+* ``leo_states(n, seed)``: altitude (a - R_E) U[400, 1200] km, e U[0, 0.02],
+  i U[0, 98] deg, RAAN / argp / mean anomaly U[0, 360) deg; the mean anomaly
+  is converted to the true anomaly, then to ECI.
+* ``mixed_states``: the uneven-batch mix (60% LEO, 20% MEO, 10% GEO, 10% HEO)
+  with log-uniform durations.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as N
+
+RE_KM = 6378.137
+EPOCH_JD = 2460310.5  # 2024-01-01T00:00 UTC, the reference smoke test's epoch
+
+
+def synthetic_field(order: int, seed: int | None = None) -> str:
+    if seed is None:
+        seed = 12345 + order
+    rng = np.random.default_rng(seed)
+    lines = ["# synthetic normalised field: C20 = -4.84165e-4, C/S ~ N(0, (1e-5/n^2)^2)"]
+    for n in range(2, order + 1):
+        sig = 1e-5 / (n * n)
+        c = rng.normal(0.0, sig, n + 1)
+        s = rng.normal(0.0, sig, n + 1)
+        s[0] = 0.0
+        if n == 2:
+            c[0] = -4.84165e-4
+        for m in range(n + 1):
+            lines.append(f"{n} {m} {float(c[m])!r} {float(s[m])!r}")
+    return "\n".join(lines) + "\n"
+
+
+def mean_to_true(M: np.ndarray, e: np.ndarray) -> np.ndarray:
+    E = M.copy()
+    for _ in range(50):
+        E = E - (E - e * np.sin(E) - M) / (1.0 - e * np.cos(E))
+    return 2.0 * np.arctan2(np.sqrt(1 + e) * np.sin(E / 2), np.sqrt(1 - e) * np.cos(E / 2))
+
+
+def kep_states(a, e, i_deg, raan_deg, argp_deg, M_deg) -> np.ndarray:
+    nu = np.degrees(mean_to_true(np.radians(M_deg), e)) % 360.0
+    kep = np.stack([a, e, i_deg, raan_deg, argp_deg, nu], axis=1)
+    return N.kep_to_eci(kep)
+
+
+def leo_states(n: int, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    alt = rng.uniform(400.0, 1200.0, n)
+    e = rng.uniform(0.0, 0.02, n)
+    inc = rng.uniform(0.0, 98.0, n)
+    raan = rng.uniform(0.0, 360.0, n)
+    argp = rng.uniform(0.0, 360.0, n)
+    M = rng.uniform(0.0, 360.0, n)
+    return kep_states(RE_KM + alt, e, inc, raan, argp, M)
+
+
+def leo_ballistics(n: int, seed: int = 0) -> np.ndarray:
+    """(A/m U[0.005, 0.05] m^2/kg, Cd = 2.2) per row."""
+    rng = np.random.default_rng(seed + 7919)
+    am = rng.uniform(0.005, 0.05, n)
+    return np.stack([am, np.full(n, 2.2)], axis=1)
+
+
+def mixed_states(n: int, seed: int = 0):
+    """60% LEO / 20% MEO (a U[20000, 27000]) / 10% GEO / 10% HEO (e U[0.5, 0.75],
+    perigee altitude 500 km); durations log-uniform 1 h .. 30 d.
+    Returns (states [n,6], durations_s [n], is_low [n] (drag applies))."""
+    rng = np.random.default_rng(seed)
+    kind = rng.choice(4, size=n, p=[0.6, 0.2, 0.1, 0.1])
+    a = np.empty(n)
+    e = np.empty(n)
+    a[kind == 0] = RE_KM + rng.uniform(400.0, 1200.0, (kind == 0).sum())
+    e[kind == 0] = rng.uniform(0.0, 0.02, (kind == 0).sum())
+    a[kind == 1] = rng.uniform(20000.0, 27000.0, (kind == 1).sum())
+    e[kind == 1] = rng.uniform(0.0, 0.02, (kind == 1).sum())
+    a[kind == 2] = 42164.0 + rng.uniform(-50.0, 50.0, (kind == 2).sum())
+    e[kind == 2] = rng.uniform(0.0, 0.001, (kind == 2).sum())
+    eh = rng.uniform(0.5, 0.75, (kind == 3).sum())
+    e[kind == 3] = eh
+    a[kind == 3] = (RE_KM + 500.0) / (1.0 - eh)
+    inc = rng.uniform(0.0, 98.0, n)
+    inc[kind == 2] = rng.uniform(0.0, 1.0, (kind == 2).sum())
+    raan = rng.uniform(0.0, 360.0, n)
+    argp = rng.uniform(0.0, 360.0, n)
+    M = rng.uniform(0.0, 360.0, n)
+    states = kep_states(a, e, inc, raan, argp, M)
+    dur = np.exp(rng.uniform(np.log(3600.0), np.log(30 * 86400.0), n))
+    return states, dur, kind == 0

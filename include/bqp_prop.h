@@ -1,0 +1,183 @@
+/*
+ * bqp_prop.h -- C ABI of the B200 batched orbit propagator (libbqp_b200.so).
+ *
+ * Drop-in boundary for the Lightyear propagator of tdude78/bqp
+ * (dust_transfer).  Each entry point names the reference interface it
+ * replaces (paths inside dust_transfer/).  Plain pointers and sizes only.
+ *
+ * Units and frames (reference dust_transfer/src/lib.rs:1-24): km, km/s, s,
+ * Julian Date (UTC).  States are row-major [x, y, z, vx, vy, vz] in the
+ * propagator's inertial frame; the gravity field is Earth-fixed, related to
+ * the inertial frame by the GMST rotation about +z
+ * (satpy_core/src/lib.rs:905-978).  Equinoctial elements are
+ * [a, h, k, p, q, L] (satpy_core/src/lib.rs:1738-1870).
+ *
+ * Return codes: 0 on success, a negative BQP_E_* code on a call-level error
+ * (bqp_last_error() has the message).  Per-trajectory outcomes are reported
+ * in `status` arrays with the BQP_ST_* codes; failed rows are NaN-filled
+ * (lightyear_odeint_rs/src/batch.rs:297).
+ *
+ * Entry points without `_device` take HOST buffers and copy to and from the
+ * GPU inside the call.  `_device` variants take device pointers and enqueue
+ * on the context's stream without synchronising.
+ */
+#ifndef BQP_PROP_H
+#define BQP_PROP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BQP_API_VERSION 1
+
+/* call-level return codes */
+#define BQP_E_ARG (-1)         /* invalid argument */
+#define BQP_E_CUDA (-2)        /* CUDA runtime error or no device */
+#define BQP_E_COEFF (-3)       /* gravity coefficient text rejected */
+#define BQP_E_UNSUPPORTED (-4) /* option outside this build (e.g. SRP) */
+#define BQP_E_NOMEM (-5)
+
+/* per-trajectory status (IntegrationStatus, odesolve/solver.rs:64-95;
+ * GravityError, satpy_core/src/gravity.rs:21-37; FinalPropagationFailure,
+ * lightyear_odeint_rs/src/integrator.rs:2588-2612) */
+#define BQP_ST_OK 0
+#define BQP_ST_MAX_STEPS 1
+#define BQP_ST_STEP_UNDERFLOW 2
+#define BQP_ST_INVALID_INPUT 3
+#define BQP_ST_NON_FINITE 4
+#define BQP_ST_MAX_REJECTS 5
+#define BQP_ST_GRAVITY_RADIUS 6
+#define BQP_ST_REBASE_FAILED 7
+#define BQP_ST_RESTART_BUDGET 8
+#define BQP_ST_GROUND 9
+#define BQP_ST_WATCHDOG 10
+
+/* force flags (ForceFlags, lightyear_odeint_rs/src/types.rs:266-286) */
+#define BQP_FORCE_DRAG 1
+#define BQP_FORCE_SRP 2 /* not built: rejected with BQP_E_UNSUPPORTED */
+#define BQP_FORCE_SUN 4
+#define BQP_FORCE_MOON 8
+
+/* steppers (StepperMethod, types.rs:148-157) */
+#define BQP_METHOD_DOPRI5 0        /* solver.rs Dopri5 tableau, IntegratorConfig control */
+#define BQP_METHOD_DOP853 1        /* StepperMethod::Dop853 */
+#define BQP_METHOD_DOPRI5_COMPAT 2 /* StepperMethod::Dopri5Compat, Python method="dopri5" */
+
+/* Force model and solver settings; replaces ForceConfig
+ * (lightyear_odeint_rs/src/types.rs:332-411) as built by force_config()
+ * (dust_transfer/src/lib.rs:128-190). */
+typedef struct bqp_force_config {
+    int32_t order;          /* spherical-harmonic degree/order, 0..120 */
+    int32_t force_flags;    /* BQP_FORCE_* */
+    int32_t atm_model;      /* 4 exact JB2008; 7 accepted and evaluated with the exact kernel */
+    int32_t method;         /* BQP_METHOD_* */
+    int32_t error_control;  /* 0: absolute eps, max-norm; 1: scaled rtol/atol, RMS */
+    int32_t ground_check;   /* 1: stop with BQP_ST_GROUND below 100 km altitude */
+    double eps;             /* absolute tolerance (error_control 0) */
+    double rtol, atol;      /* scaled tolerances (error_control 1) */
+    double dt_max;          /* maximum step, s */
+    double am_ratio, cd;    /* default ballistics: A/m (m^2/kg), drag coefficient */
+    double earth_radius;    /* km, altitude geometry (WGS84 6378.137) */
+    double omega_earth;     /* rad/s, co-rotating atmosphere */
+    double mu_sun, mu_moon; /* km^3/s^2 */
+    double jb_drivers[9];   /* F10.7, F10.7bar, S10, S10bar, M10, M10bar, Y10, Y10bar, dTc (K) */
+    int64_t max_steps;      /* per rectification segment (MAX_STEPS = 500000) */
+    int64_t max_attempts;   /* device watchdog: step attempts per trajectory */
+    double max_kernel_seconds; /* device watchdog: wall-clock limit of one launch (0: none);
+                                  rows not finished by then end with BQP_ST_WATCHDOG */
+} bqp_force_config;
+
+typedef struct bqp_ctx bqp_ctx;
+
+/* Defaults of the reference's ForceConfig::default + Python kwargs. */
+void bqp_force_config_default(bqp_force_config* cfg);
+
+/* Last error message of the calling thread ("" if none). */
+const char* bqp_last_error(void);
+
+/* Parse a normalised "deg ord C S" coefficient text (D exponents and '#'
+ * comments accepted), build the device field table and bind the force
+ * configuration.  Replaces packed_constants_from_bytes
+ * (lightyear_odeint_rs/src/config.rs:80-85,128-225) plus the per-context
+ * state of ScalarPropagationContext (integrator.rs).  The context lives on
+ * the CUDA device current at creation. */
+int bqp_ctx_create(const char* coeff_text, int64_t text_len, const bqp_force_config* cfg,
+                   bqp_ctx** out);
+int bqp_ctx_destroy(bqp_ctx* ctx);
+/* cudaStream_t to enqueue on (NULL: the legacy default stream). */
+int bqp_ctx_set_stream(bqp_ctx* ctx, void* cuda_stream);
+/* info[0]=order, [1]=table cells, [2]=table bytes, [3]=table staged in shared memory */
+int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info4);
+/* Replace the force/solver settings of a context (the field is kept; the
+ * order may only shrink up to the parsed order). */
+int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);
+
+/* Full-field gravity (C00 included) at Earth-fixed positions.
+ * Replaces spherical_gravity_impl_frame_packed
+ * (satpy_core/src/gravity.rs:2638-2675). pos [n][3] km -> acc [n][3] km/s^2.
+ * status[n] (nullable): BQP_ST_OK or BQP_ST_GRAVITY_RADIUS. */
+int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc_km_s2,
+                     int32_t* status);
+int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* d_pos_km, double* d_acc,
+                            int32_t* d_status);
+
+/* One Encke force evaluation per row: d(delta)/dt = [dv, a] of the deviation
+ * from the baseline orbit of elements equ (valid at seg_t0), at time t (s
+ * after epoch_jd).  Replaces LightyearRHS::compute_internal
+ * (lightyear_odeint_rs/src/rhs.rs:3872-4118).  ballistic [n][2] nullable. */
+int bqp_rhs_eval(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t0,
+                 const double* epoch_jd, const double* t, const double* delta,
+                 const double* ballistic, double* out);
+int bqp_rhs_eval_device(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t0,
+                        const double* epoch_jd, const double* t, const double* delta,
+                        const double* ballistic, double* out);
+
+/* Final-state propagation of a batch with per-row epoch, end time and
+ * ballistics, Encke rectification every 5400 s / 10 km.  Replaces
+ * integrate_final_checked (integrator.rs:3197) per row and
+ * LightyearSession::integrate_variable_final_into (session.rs:2325-2430).
+ * in [n][6]: ECI (input_equinoctial = 0) or equinoctial elements at t0.
+ * epoch_jd[n], tf[n] (s after epoch, >= t0), ballistic [n][2] nullable.
+ * out [n][6]: ECI at tf.  status/steps/evals per row (steps/evals nullable). */
+int bqp_propagate_final(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equinoctial,
+                        const double* epoch_jd, double t0, const double* tf,
+                        const double* ballistic, double* out, int32_t* status, int64_t* steps,
+                        int64_t* evals);
+int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in,
+                               int32_t input_equinoctial, const double* epoch_jd, double t0,
+                               const double* tf, const double* ballistic, double* out,
+                               int32_t* status, int64_t* steps, int64_t* evals);
+
+/* Sampled propagation on a common grid t_eval[n_t] (sorted, within
+ * [t0, tf_i], containing t0 and tf_i as the reference's binding arranges,
+ * lib.rs:277-290).  Replaces integrate_adaptive's rectified sampled path
+ * (integrator.rs:2313-2416, 2426) and integrate_batch_native_into
+ * (batch.rs:247-391).  out [n][n_t][6]: ECI states (out_deltas = 0) or Encke
+ * deviations against the initial baseline (out_deltas = 1, the batch API). */
+int bqp_propagate_sampled(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equinoctial,
+                          const double* epoch_jd, double t0, const double* tf, int32_t n_t,
+                          const double* t_eval, int32_t out_deltas, double* out,
+                          int32_t* status, int64_t* steps, int64_t* evals);
+int bqp_propagate_sampled_device(bqp_ctx* ctx, int64_t n, const double* in,
+                                 int32_t input_equinoctial, const double* epoch_jd, double t0,
+                                 const double* tf, int32_t n_t, const double* t_eval,
+                                 int32_t out_deltas, double* out, int32_t* status,
+                                 int64_t* steps, int64_t* evals);
+
+/* Element conversions on the host (no GPU).  eci_to_equinoctial replaces
+ * eci2equinoc_impl (satpy_core/src/lib.rs:1738-1870; ok[i] = 0 on an
+ * unbound or degenerate orbit); equinoctial_to_eci replaces equinoc2eci_impl
+ * (lib.rs:2580-2591) at tof[i] seconds; kep_to_eci / eci_to_kep replace the
+ * Python kep_to_eci / eci_to_kep (dust_transfer/src/lib.rs:200-221):
+ * [a_km, e, i_deg, raan_deg, argp_deg, true_anomaly_deg]. */
+int bqp_eci_to_equinoctial(int64_t n, const double* eci, double* equ, int32_t* ok);
+int bqp_equinoctial_to_eci(int64_t n, const double* equ, const double* tof, double* eci);
+int bqp_kep_to_eci(int64_t n, const double* kep, double* eci);
+int bqp_eci_to_kep(int64_t n, const double* eci, double* kep);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BQP_PROP_H */

@@ -1,0 +1,262 @@
+"""CUDA path against the CPU oracle, through the C ABI (libbqp_b200.so).
+
+Tolerances (FP64 form):
+* force evaluations: |da| <= 1e-12 |a_full| (a_full: the full-field
+  acceleration, point mass included) -- "within 1e-12 relative";
+* fixed-step trajectories: position difference <= 1e-9 relative;
+* adaptive trajectories: within the integrator tolerance (see each test).
+"""
+import json
+import struct
+
+import numpy as np
+import pytest
+
+from bqp_b200 import _native as N
+from bqp_b200 import api, workloads
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+EPOCH = workloads.EPOCH_JD
+MU = 398600.4415
+
+
+def h(s):
+    return struct.unpack(">d", bytes.fromhex(s[2:]))[0]
+
+
+def ctx_for(text, order, flags=0, method="dop853", eps=1e-8, dt_max=300.0, rtol=None, atol=None,
+            am=0.01, cd=2.2, ground=False, max_attempts=None):
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.force_flags = flags
+    cfg.method = N.METHODS[method]
+    cfg.dt_max = dt_max
+    cfg.am_ratio = am
+    cfg.cd = cd
+    cfg.ground_check = int(ground)
+    if rtol is not None:
+        cfg.error_control = 1
+        cfg.rtol = rtol
+        cfg.atol = atol
+    else:
+        cfg.eps = eps
+    if max_attempts is not None:
+        cfg.max_attempts = max_attempts
+    return N.Context(text, cfg)
+
+
+def oracle_force(text, order, flags=0):
+    return O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8))
+
+
+def random_positions(n, seed, rmin=6578.0, rmax=7578.0):
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    return np.ascontiguousarray(d * rng.uniform(rmin, rmax, n)[:, None])
+
+
+# ------------------------------------------------------------------ gravity
+def test_gravity_matches_orekit_fixture(golden_dir):
+    g = json.loads((golden_dir / "orekit_gravity_dir_r6_d5.json").read_text())
+    ctx = ctx_for((golden_dir / "dir_r6_d15.txt").read_text(), 5)
+    tol_abs, tol_rel = h(g["absolute_tolerance_m_s2"]), h(g["relative_tolerance"])
+    pos = np.array([[h(x) for x in c["position_m"]] for c in g["cases"]]) / 1000.0
+    acc, st = ctx.gravity(pos)
+    assert (st == 0).all()
+    for i, c in enumerate(g["cases"]):
+        want = np.array([h(x) for x in c["full_m_s2"]])
+        assert np.all(np.abs(acc[i] * 1000.0 - want) <= tol_abs + tol_rel * np.abs(want)), c["name"]
+
+
+@pytest.mark.parametrize("order", [2, 20, 70, 120])
+def test_gravity_matches_oracle(order):
+    text = workloads.synthetic_field(order)
+    ctx = ctx_for(text, order)
+    pos = random_positions(4096 if order <= 70 else 1024, seed=order)
+    acc, st = ctx.gravity(pos)
+    ref = oracle_force(text, order).gravity_itrs(pos)
+    assert (st == 0).all()
+    err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err.max() <= 1e-12, err.max()
+    info = ctx.info()
+    assert info["table_in_shared_memory"] == (order <= 70)
+
+
+def test_gravity_invalid_radius_status():
+    ctx = ctx_for(workloads.synthetic_field(10), 10)
+    pos = np.array([[0.0, 0.0, 0.0], [np.nan, 1.0, 2.0], [7000.0, 0.0, 0.0]])
+    acc, st = ctx.gravity(pos)
+    assert list(st) == [N.ST_GRAVITY_RADIUS, N.ST_GRAVITY_RADIUS, N.ST_OK]
+    assert np.isnan(acc[:2]).all() and np.isfinite(acc[2]).all()
+
+
+def test_gravity_empty_batch():
+    ctx = ctx_for(workloads.synthetic_field(10), 10)
+    acc, st = ctx.gravity(np.zeros((0, 3)))
+    assert acc.shape == (0, 3)
+
+
+# ---------------------------------------------------------------- force model
+@pytest.mark.parametrize("flags", [0, 1, 4 | 8, 1 | 4 | 8])
+def test_encke_rhs_matches_oracle(flags):
+    order = 70
+    text = workloads.synthetic_field(order)
+    ctx = ctx_for(text, order, flags=flags)
+    F = oracle_force(text, order, flags)
+    n = 256
+    states = workloads.leo_states(n, seed=11)
+    equ, ok = N.eci_to_equinoctial(states)
+    assert ok.all()
+    rng = np.random.default_rng(5)
+    t = rng.uniform(0.0, 5400.0, n)
+    seg_t0 = rng.uniform(0.0, 1.0, n) * t
+    delta = np.concatenate([rng.normal(0, 3.0, (n, 3)), rng.normal(0, 3e-3, (n, 3))], axis=1)
+    bal = workloads.leo_ballistics(n, seed=2)
+    epoch = EPOCH + rng.uniform(0, 30, n)
+    got = ctx.rhs(equ, seg_t0, epoch, t, delta, bal)
+    for i in range(n):
+        ref = F.rhs(equ[i], seg_t0[i], epoch[i], bal[i, 0], bal[i, 1], t[i], delta[i])
+        base, _ = O.equinoc2eci(equ[i], t[i] - seg_t0[i])
+        r = np.linalg.norm(base[:3] + delta[i, :3])
+        scale = MU / r ** 2  # full-field magnitude
+        assert np.array_equal(got[i, :3], ref[:3])
+        assert np.abs(got[i, 3:] - ref[3:]).max() <= 1e-12 * scale, (i, got[i], ref)
+
+
+# -------------------------------------------------------------- trajectories
+def test_fixed_step_dop853_matches_oracle():
+    """Constant steps (every step accepted): |dr| <= 1e-9 relative."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    h_fixed = 30.0
+    ctx = ctx_for(text, order, flags=1 | 4 | 8, eps=1e30, dt_max=h_fixed)
+    F = oracle_force(text, order, 1 | 4 | 8)
+    n = 32
+    states = workloads.leo_states(n, seed=21)
+    equ, _ = N.eci_to_equinoctial(states)
+    bal = workloads.leo_ballistics(n, seed=21)
+    tf = 2 * 5400.0 + 600.0
+    got, st, steps, evals = ctx.propagate_final(equ, EPOCH, tf, ballistic=bal, equinoctial=True)
+    ref_d, ref_st, ref_steps, ref_evals = O.propagate_final_batch(
+        F, O.ctrl("dop853", eps=1e30, dt_max=h_fixed), equ, EPOCH, tf, bal)
+    assert (st == 0).all() and (ref_st == 0).all()
+    assert np.array_equal(steps, ref_steps) and np.array_equal(evals, ref_evals)
+    for i in range(n):
+        base, _ = O.equinoc2eci(equ[i], tf)
+        ref = base + ref_d[i]
+        rel = np.linalg.norm(got[i, :3] - ref[:3]) / np.linalg.norm(ref[:3])
+        assert rel <= 1e-9, (i, rel)
+
+
+@pytest.mark.parametrize("method,eps", [("dop853", 1e-10), ("dopri5_solver", 1e-9), ("dopri5", 1e-9)])
+def test_adaptive_final_matches_oracle(method, eps):
+    """Adaptive trajectories within the integrator tolerance (70x70 + drag +
+    Sun/Moon, one and a half orbits with rectification)."""
+    order = 70
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    ctx = ctx_for(text, order, flags=flags, method=method, eps=eps)
+    F = oracle_force(text, order, flags)
+    n = 24
+    states = workloads.leo_states(n, seed=31)
+    bal = workloads.leo_ballistics(n, seed=31)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 8000.0
+    got, st, steps, evals = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    ref_d, ref_st, ref_steps, _ = O.propagate_final_batch(F, O.ctrl(method, eps=eps), equ, EPOCH, tf, bal)
+    assert (st == 0).all() and (ref_st == 0).all()
+    for i in range(n):
+        base, _ = O.equinoc2eci(equ[i], tf)
+        ref = base + ref_d[i]
+        # per-step local error <= eps; allow the accumulated bound steps * eps
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= max(steps[i], 1) * eps * 10, i
+    assert np.abs(steps - ref_steps).max() <= 3
+
+
+def test_sampled_dopri5_scaled_matches_oracle():
+    """The C1 form: DOPRI5(4), rtol 1e-10 / atol 1e-9 km, 60 s grid."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    ctx = ctx_for(text, order, flags=0, method="dopri5_solver", rtol=1e-10, atol=1e-9)
+    F = oracle_force(text, order, 0)
+    n = 8
+    states = workloads.leo_states(n, seed=0)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 3 * 3600.0
+    grid = np.arange(0.0, tf + 1.0, 60.0)
+    got, st, steps, evals = ctx.propagate_sampled(states, EPOCH, tf, grid)
+    assert (st == 0).all()
+    for i in range(n):
+        d, rs, _, ev, nw = O.propagate_sampled(F, O.ctrl("dopri5", rtol=1e-10, atol=1e-9), equ[i], EPOCH, tf,
+                                               0.01, 2.2, grid)
+        assert rs == 0 and nw == grid.size
+        base = np.array([O.equinoc2eci(equ[i], t)[0] for t in grid])
+        ref = base + d
+        err = np.linalg.norm(got[i, :, :3] - ref[:, :3], axis=1)
+        assert err.max() <= 1e-6, (i, err.max())
+        assert np.allclose(got[i, 0], base[0], atol=1e-9)
+
+
+def test_sampled_deltas_against_initial_baseline():
+    order = 10
+    text = workloads.synthetic_field(order)
+    ctx = ctx_for(text, order, flags=0, method="dop853", eps=1e-10)
+    states = workloads.leo_states(4, seed=4)
+    equ, _ = N.eci_to_equinoctial(states)
+    grid = np.linspace(0.0, 12000.0, 41)
+    d, st, _, _ = ctx.propagate_sampled(equ, EPOCH, 12000.0, grid, deltas=True, equinoctial=True)
+    e, st2, _, _ = ctx.propagate_sampled(equ, EPOCH, 12000.0, grid, deltas=False, equinoctial=True)
+    assert (st == 0).all() and (st2 == 0).all()
+    for i in range(4):
+        base = np.array([O.equinoc2eci(equ[i], t)[0] for t in grid])
+        assert np.allclose(base + d[i], e[i], atol=1e-9)
+    assert np.abs(d[:, 0]).max() == 0.0
+
+
+# ----------------------------------------------------------- failure handling
+def test_invalid_rows_are_nan_filled_with_status():
+    ctx = ctx_for(workloads.synthetic_field(8), 8)
+    states = workloads.leo_states(4, seed=9)
+    states[1] = [7000.0, 0.0, 0.0, 0.0, 12.0, 0.0]  # unbound
+    states[2, 0] = np.nan
+    tf = np.array([600.0, 600.0, 600.0, -5.0])
+    out, st, _, _ = ctx.propagate_final(states, EPOCH, tf)
+    assert list(st) == [N.ST_OK, 3, 3, 3]
+    assert np.isfinite(out[0]).all() and np.isnan(out[1:]).all()
+
+
+def test_ground_impact_is_reported():
+    # dust_transfer/tests_smoke.py:30-34: the impacting arc raises ValueError
+    eci = api.kep_to_eci([6600.0, 0.05, 30.0, 0.0, 0.0, 0.0])
+    with pytest.raises(ValueError, match="ground"):
+        api.propagate_final(eci, EPOCH, 6000.0, srp=False, method="dop853")
+
+
+def test_device_watchdog_stops_runaway_rows():
+    ctx = ctx_for(workloads.synthetic_field(8), 8, flags=0, eps=1e-10, max_attempts=5)
+    states = workloads.leo_states(3, seed=1)
+    out, st, _, _ = ctx.propagate_final(states, EPOCH, 5000.0)
+    assert (st == 10).all() and np.isnan(out).all()
+
+
+# ------------------------------------------------------------ Python surface
+def test_reference_smoke_sequence():
+    """dust_transfer/tests_smoke.py, with srp=False and a built stepper."""
+    kep = np.array([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0])
+    eci = api.kep_to_eci(kep)
+    out = api.propagate(eci, EPOCH, tof_s=600.0, gravity_order=1, drag=False, srp=False, sun=False, moon=False,
+                        method="dop853")
+    assert out["completed"], out
+    r0 = np.linalg.norm(eci[:3])
+    r1 = np.linalg.norm(out["states_eci"][-1][:3])
+    assert abs(r1 - r0) < 200.0
+    full = api.propagate(eci, EPOCH, tof_s=3600.0, times_s=np.arange(600.0, 3601.0, 600.0), srp=False,
+                         method="dop853")
+    assert full["completed"] and np.isfinite(full["states_eci"]).all()
+    assert full["states_eci"].shape == (7, 6)
+    assert full["steps"] > 0 and full["rhs_evals"] >= 12 * full["steps"]
+    fs = api.propagate_final(eci, EPOCH, tof_s=3600.0, srp=False, method="dop853")
+    assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3

@@ -1,0 +1,123 @@
+"""CPU-side checks of the native library: it loads, exports every symbol the C
+header declares, and its host-only logic (element conversions, argument and
+configuration validation) behaves like the reference's.  No kernel launches."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bqp_b200 import _native as N
+from bqp_b200 import api, workloads
+from oracle import oracle as O
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def header_functions():
+    text = (ROOT / "include" / "bqp_prop.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bqp_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = N.lib()
+    names = header_functions()
+    assert len(names) >= 19
+    for name in names:
+        assert hasattr(lib, name), name
+    assert sorted(n for n, _, _ in N.SIGNATURES) == names
+
+
+def test_config_struct_matches_header_layout():
+    # the ctypes mirror must have the C struct's size (4*6 + 8*10 + 8*9 + 8*3)
+    assert C.sizeof(N.ForceConfig) == 24 + 80 + 72 + 24
+    cfg = N.default_config()
+    assert cfg.order == 5 and cfg.eps == 1e-8 and cfg.dt_max == 300.0 and cfg.max_steps == 500000
+    assert list(cfg.jb_drivers)[:8] == [150.0] * 8
+
+
+def test_eci_equinoctial_round_trip_matches_oracle():
+    states = workloads.leo_states(64, seed=3)
+    equ, ok = N.eci_to_equinoctial(states)
+    assert ok.all()
+    for i in range(64):
+        ref, rc = O.eci2equinoc(states[i])
+        assert rc == 0
+        assert np.allclose(equ[i], ref, rtol=1e-14, atol=1e-14)
+    back = N.equinoctial_to_eci(equ, 0.0)
+    assert np.allclose(back, states, rtol=0.0, atol=1e-7)  # Kepler tolerance 1e-12 rad
+    # propagation on the two-body baseline
+    for i in range(8):
+        ref, _ = O.equinoc2eci(equ[i], 1234.5)
+        got = N.equinoctial_to_eci(equ[i], 1234.5)[0]
+        assert np.allclose(got, ref, rtol=1e-13, atol=1e-9)
+
+
+def test_unbound_orbit_is_rejected():
+    hyper = np.array([7000.0, 0.0, 0.0, 0.0, 12.0, 0.0])
+    _, ok = N.eci_to_equinoctial(hyper)
+    assert not ok[0]
+    with pytest.raises(ValueError):
+        api.propagate_final(hyper, 2460310.5, 600.0, srp=False, method="dop853")
+
+
+def test_kep_round_trip_like_reference_smoke():
+    # dust_transfer/tests_smoke.py:9-12
+    kep = np.array([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0])
+    eci = api.kep_to_eci(kep)
+    back = api.eci_to_kep(eci)
+    assert np.allclose(kep, back, rtol=1e-6, atol=1e-6)
+    with pytest.raises(ValueError):
+        api.kep_to_eci([7000.0, 1.2, 0, 0, 0, 0])
+
+
+def test_python_argument_validation_mirrors_binding():
+    eci = api.kep_to_eci([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0])
+    with pytest.raises(ValueError, match="exactly 6"):
+        api.propagate([1, 2, 3], 2460310.5, 600.0)
+    with pytest.raises(ValueError, match="non-finite"):
+        api.propagate([np.nan] * 6, 2460310.5, 600.0)
+    with pytest.raises(ValueError, match="tof_s > 0"):
+        api.propagate(eci, 2460310.5, -1.0, srp=False, method="dop853")
+    with pytest.raises(ValueError, match="strictly increasing"):
+        api.propagate(eci, 2460310.5, 600.0, times_s=[300.0, 200.0], srp=False, method="dop853")
+    with pytest.raises(ValueError, match="gravity_order"):
+        api.propagate(eci, 2460310.5, 600.0, gravity_order=16, srp=False, method="dop853")
+    with pytest.raises(ValueError, match="unknown integrator"):
+        api.propagate(eci, 2460310.5, 600.0, srp=False, method="rk4")
+    with pytest.raises(ValueError, match="not built"):
+        api.propagate(eci, 2460310.5, 600.0, srp=False, method="vern7")
+    with pytest.raises(ValueError, match="srp"):
+        api.propagate(eci, 2460310.5, 600.0, method="dop853")
+    with pytest.raises(ValueError, match="atm_model"):
+        api.propagate(eci, 2460310.5, 600.0, srp=False, method="dop853", atm_model=2)
+
+
+def test_ctx_config_validation_happens_before_device_use():
+    cfg = N.default_config()
+    cfg.force_flags |= N.FORCE_SRP
+    with pytest.raises(N.NativeError) as e:
+        N.Context("2 0 -4.8e-4 0", cfg)
+    assert e.value.code == N.E_UNSUPPORTED
+    cfg = N.default_config()
+    cfg.order = 129
+    with pytest.raises(N.NativeError) as e:
+        N.Context("2 0 -4.8e-4 0", cfg)
+    assert e.value.code == N.E_ARG
+    cfg = N.default_config()
+    cfg.eps = 0.0
+    with pytest.raises(N.NativeError):
+        N.Context("2 0 -4.8e-4 0", cfg)
+
+
+def test_synthetic_field_rule():
+    text = workloads.synthetic_field(70)
+    rows = [l.split() for l in text.splitlines() if l and not l.startswith("#")]
+    assert len(rows) == sum(n + 1 for n in range(2, 71))
+    c20 = [float(r[2]) for r in rows if r[0] == "2" and r[1] == "0"][0]
+    assert c20 == -4.84165e-4
+    hi = np.array([float(r[2]) for r in rows if int(r[0]) == 70])
+    assert 0.3e-5 / 4900 < hi.std() < 3e-5 / 4900
+    assert all(float(r[3]) == 0.0 for r in rows if r[1] == "0")
