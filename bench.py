@@ -1,0 +1,399 @@
+"""Benchmark of the batched orbit propagator (one JSON line on rank 0).
+
+Workload (the 70x70 + drag configuration): 65,536 LEO states (altitude U[400,
+1200] km, e U[0, 0.02], i U[0, 98] deg, angles U[0, 360) deg, seed 0), a
+synthetic 70x70 normalised Kaula-rule field, JB2008 drag (F10.7 = S10 = M10 =
+Y10 = 150, dTc = 20 K), A/m U[0.005, 0.05] m^2/kg, Cd 2.2, Sun/Moon point
+masses, DOP853 with absolute tolerance 1e-12 (the reference's smallest
+eps, integrator.rs:427), dt_max 300 s.
+
+One step = one Encke rectification segment (5400 s) of the whole batch: the
+7-day arc is 112 such segments, and each call continues from the previous
+call's output exactly as the reference's segment loop does
+(integrator.rs:3418-3560).  Metric: force (RHS) evaluations per second, counted
+by the device per trajectory.
+
+  value  device-resident inputs, k_propagate timed with CUDA events
+  e2e    the same steps through the host-buffer C ABI call
+         (bqp_propagate_final): H2D of the inputs and D2H of the results
+         inside the timed region
+  roofline  FP64: algorithmic flops = force evals x F(70) (the reference
+         gravity algorithm's flop count, F(N) = 9(N+2)(N+3)/2 + 13N(N+1) +
+         9(N+1) + 60, FMA = 2), peak = cuBLAS DGEMM measured in this run
+  cpu_baseline  the C++ oracle (restatement of the reference CPU path) on a
+         bounded sample, all host cores
+
+``--impl reference`` times that CPU implementation alone (rank 0) on the same
+workload and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "force evals/s @70x70+drag: plain FP64 vs split/surrogate at ≤1 m 7-day err"
+UNIT = "force_evals/s"
+ORDER = 70
+N_TRAJ = 65536
+SEGMENT_S = 5400.0
+EPS = 1e-12
+DRIVERS = (150.0,) * 8 + (20.0,)
+
+
+def f_of_n(n: int) -> float:
+    return 9 * (n + 2) * (n + 3) / 2 + 13 * n * (n + 1) + 9 * (n + 1) + 60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_TRAJ)
+    ap.add_argument("--cpu-sample", type=int, default=256, help="trajectories in the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------- workload
+def make_workload(n: int, seed: int = 0):
+    from bqp_b200 import workloads as W
+
+    states = W.leo_states(n, seed=seed)
+    bal = W.leo_ballistics(n, seed=seed)
+    return W.synthetic_field(ORDER), states, bal, W.EPOCH_JD
+
+
+def make_config():
+    from bqp_b200 import _native as N
+
+    cfg = N.default_config()
+    cfg.order = ORDER
+    cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON
+    cfg.atm_model = 4
+    cfg.method = N.METHODS["dop853"]
+    cfg.error_control = 0
+    cfg.eps = EPS
+    cfg.dt_max = 300.0
+    for i, v in enumerate(DRIVERS):
+        cfg.jb_drivers[i] = v
+    cfg.max_kernel_seconds = 300.0
+    return cfg
+
+
+def cpu_reference(sample: int, threads: int, segments: int = 1):
+    """Time the CPU oracle (restatement of the reference path) on `sample`
+    trajectories for `segments` rectification segments, all threads."""
+    from bqp_b200 import _native as N
+    from oracle import oracle as O
+
+    text, states, bal, epoch = make_workload(sample)
+    equ, _ = N.eci_to_equinoctial(states)
+    F = O.Force(text, ORDER, drag=True, sun=True, moon=True, drivers=DRIVERS)
+    ctl = O.ctrl("dop853", eps=EPS, dt_max=300.0)
+    t0 = time.perf_counter()
+    _, st, steps, evals = O.propagate_final_batch(F, ctl, equ, epoch, SEGMENT_S * segments, bal, threads=threads)
+    dt = time.perf_counter() - t0
+    return float(evals.sum()) / dt, dt, int(evals.sum()), int((st == 0).sum())
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    evals_s = []
+    for i in range(args.warmup + args.steps):
+        v, dt, ev, ok = cpu_reference(args.cpu_sample, threads)
+        if i >= args.warmup:
+            evals_s.append((v, dt))
+    value = statistics.median(v for v, _ in evals_s)
+    ms = statistics.median(dt for _, dt in evals_s) * 1e3
+    sample = f"{args.cpu_sample} of the {args.n} trajectories, one 5400 s segment per step"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.n} LEO states, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
+                               "DOP853 eps 1e-12, 5400 s Encke segment per step",
+                   "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from bqp_b200 import _native as N
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    text, states, bal, epoch = make_workload(args.n, seed=rank)
+    cfg = make_config()
+    ctx = N.Context(text, cfg)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    n = args.n
+
+    # device-resident state: chain segments in place (out of step k = in of k+1)
+    with torch.cuda.stream(stream):
+        d_a = torch.tensor(states, device=dev, dtype=torch.float64)
+        d_b = torch.empty_like(d_a)
+        d_bal = torch.tensor(bal, device=dev, dtype=torch.float64)
+        d_tf = torch.full((n,), SEGMENT_S, device=dev, dtype=torch.float64)
+        d_status = torch.empty(n, device=dev, dtype=torch.int32)
+        d_steps = torch.empty(n, device=dev, dtype=torch.int64)
+        d_evals = torch.empty(n, device=dev, dtype=torch.int64)
+        flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
+    epochs = [epoch + k * SEGMENT_S / 86400.0 for k in range(args.warmup + args.steps + 1)]
+    d_epochs = [torch.full((n,), e, device=dev, dtype=torch.float64) for e in epochs]
+    torch.cuda.synchronize()
+
+    def step(k, src, dst):
+        ctx.propagate_final_device(src.data_ptr(), d_epochs[k].data_ptr(), d_tf.data_ptr(), dst.data_ptr(),
+                                   d_status.data_ptr(), d_steps.data_ptr(), d_evals.data_ptr(), n=n,
+                                   d_ballistic=d_bal.data_ptr())
+
+    # warm-up (also advances the batch)
+    src, dst = d_a, d_b
+    for k in range(args.warmup):
+        step(k, src, dst)
+        src, dst = dst, src
+    stream.synchronize()
+
+    # timed, device-resident
+    events = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        evals_acc = torch.zeros((), device=dev, dtype=torch.int64)
+    with ClockSampler(local) as clocks:
+        e_start = torch.cuda.Event(enable_timing=True)
+        e_end = torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        for k in range(args.warmup, args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # L2 flush between timed steps (256 MiB write)
+            k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k0.record(stream)
+            step(k, src, dst)
+            k1.record(stream)
+            with torch.cuda.stream(stream):
+                evals_acc += d_evals.sum()  # the device's per-trajectory counters of this step
+            events.append((k0, k1))
+            src, dst = dst, src
+        e_end.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    elapsed_ms = e_start.elapsed_time(e_end)
+    kernel_ms = [a.elapsed_time(b) for a, b in events]
+    status_last = d_status.cpu().numpy()
+    total_evals = int(evals_acc.item())
+
+    t_local = elapsed_ms
+    if world > 1:
+        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        ev = torch.tensor([float(total_evals)], device=dev, dtype=torch.float64)
+        dist.all_reduce(ev, op=dist.ReduceOp.SUM)
+        total_all = float(ev.item())
+    else:
+        t_max = t_local
+        total_all = float(total_evals)
+    value = total_all / (t_max * 1e-3)
+
+    # e2e: pinned host buffers through the host-buffer C ABI call
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype).pin_memory().numpy()
+
+    h_in = pinned((n, 6), torch.float64)
+    h_in[:] = states
+    h_out = pinned((n, 6), torch.float64)
+    h_bal = pinned((n, 2), torch.float64)
+    h_bal[:] = bal
+    h_tf = pinned((n,), torch.float64)
+    h_tf[:] = SEGMENT_S
+    h_ep = pinned((n,), torch.float64)
+    h_st = pinned((n,), torch.int32)
+    h_steps = pinned((n,), torch.int64)
+    h_evals = pinned((n,), torch.int64)
+    for k in range(args.warmup):
+        h_ep[:] = epochs[k]
+        ctx.propagate_final(h_in, h_ep, h_tf, ballistic=h_bal, out=h_out, status=h_st, steps=h_steps,
+                            evals=h_evals)
+        h_in[:] = h_out
+    if world > 1:
+        dist.barrier()
+    e2e_evals = 0
+    t0 = time.perf_counter()
+    for k in range(args.warmup, args.warmup + args.steps):
+        h_ep[:] = epochs[k]
+        ctx.propagate_final(h_in, h_ep, h_tf, ballistic=h_bal, out=h_out, status=h_st, steps=h_steps,
+                            evals=h_evals)
+        e2e_evals += int(h_evals.sum())
+        h_in[:] = h_out
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+        ev = torch.tensor([float(e2e_evals)], device=dev, dtype=torch.float64)
+        dist.all_reduce(ev, op=dist.ReduceOp.SUM)
+        e2e_evals = float(ev.item())
+    e2e_value = e2e_evals / e2e_s
+    h2d = n * 6 * 8 + n * 8 * 2 + n * 16
+    d2h = n * 6 * 8 + n * 4 + n * 8 * 2
+
+    line = None
+    if rank == 0:
+        peak = fp64_peak_tflops(torch, dev)
+        fN = f_of_n(ORDER)
+        mean_kernel_ms = sum(kernel_ms) / len(kernel_ms)
+        achieved = (total_evals / len(kernel_ms)) * fN / (mean_kernel_ms * 1e-3) / 1e12
+        cpu = None
+        if not args.no_cpu and world >= 1:
+            threads = os.cpu_count() or 1
+            v, dt, ev, ok = cpu_reference(args.cpu_sample, threads)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_sample} trajectories x one 5400 s segment ({ev} evals, {dt:.1f} s)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
+                                   "DOP853 eps 1e-12, one 5400 s Encke segment per step",
+                       "form": "plain FP64", "order": ORDER, "trajectories_per_gpu": n,
+                       "segment_s": SEGMENT_S, "l2": "256 MiB write between timed steps",
+                       "evals_per_step": total_evals / args.steps,
+                       "trajectory_days_per_s": world * n * SEGMENT_S / 86400.0 / (t_max * 1e-3 / args.steps)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
+                                        "MEASURED_PEAKS.json)",
+                         "flops_per_eval": fN, "kernel": "k_propagate<DOP853>"},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": args.steps,
+            "status_ok_fraction": float((status_last == 0).mean()),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -197,16 +197,21 @@ class Context:
                                  None if bal is None else dptr(bal), dptr(out)))
         return out
 
-    def propagate_final(self, states, epoch_jd, tf, t0=0.0, ballistic=None, equinoctial=False):
+    def propagate_final(self, states, epoch_jd, tf, t0=0.0, ballistic=None, equinoctial=False, out=None,
+                        status=None, steps=None, evals=None):
+        """Host-buffer call; `out`/`status`/`steps`/`evals` may be preallocated
+        (e.g. pinned) arrays of the right dtype and shape."""
         s = f64(states).reshape(-1, 6)
         n = s.shape[0]
         ep = f64(np.broadcast_to(epoch_jd, (n,)))
         tfa = f64(np.broadcast_to(tf, (n,)))
         bal = None if ballistic is None else f64(np.broadcast_to(ballistic, (n, 2)))
-        out = np.empty((n, 6))
-        st = np.empty(n, dtype=np.int32)
-        steps = np.empty(n, dtype=np.int64)
-        evals = np.empty(n, dtype=np.int64)
+        out = np.empty((n, 6)) if out is None else out
+        st = np.empty(n, dtype=np.int32) if status is None else status
+        steps = np.empty(n, dtype=np.int64) if steps is None else steps
+        evals = np.empty(n, dtype=np.int64) if evals is None else evals
+        assert out.shape == (n, 6) and out.dtype == np.float64 and out.flags.c_contiguous
+        assert st.dtype == np.int32 and steps.dtype == np.int64 and evals.dtype == np.int64
         check(lib().bqp_propagate_final(self._h, n, dptr(s), int(equinoctial), dptr(ep), float(t0), dptr(tfa),
                                         None if bal is None else dptr(bal), dptr(out), iptr(st), lptr(steps),
                                         lptr(evals)))

@@ -272,14 +272,16 @@ int upload_table(bqp_ctx* ctx) {
     return 0;
 }
 
-// Device workspace carve-out for the host-buffer entry points.
+// Device workspace carve-out for the host-buffer entry points.  Each entry
+// point runs its carve sequence twice: once on a null base to size the
+// workspace, then on the allocated base, so the two can never disagree.
 struct Carve {
     char* base;
     size_t off = 0;
     template <typename T>
     T* take(size_t count) {
         off = (off + 255) & ~(size_t)255;
-        T* p = reinterpret_cast<T*>(base + off);
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
         off += count * sizeof(T);
         return p;
     }
@@ -299,8 +301,6 @@ int ensure_ws(bqp_ctx* ctx, size_t bytes) {
     ctx->ws_bytes = want;
     return 0;
 }
-
-size_t rounded(size_t b) { return (b + 255) & ~(size_t)255; }
 
 int set_device(const bqp_ctx* ctx) {
     cudaError_t e = cudaSetDevice(ctx->device);
@@ -568,11 +568,15 @@ int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, in
     int rc = set_device(ctx);
     if (rc) return rc;
     const size_t b3 = (size_t)n * 3 * sizeof(double);
-    if ((rc = ensure_ws(ctx, 2 * rounded(b3) + rounded((size_t)n * 4) + 1024))) return rc;
-    Carve cv{(char*)ctx->d_ws};
-    double* dp = cv.take<double>((size_t)n * 3);
-    double* da = cv.take<double>((size_t)n * 3);
-    int32_t* ds = cv.take<int32_t>((size_t)n);
+    double *dp = nullptr, *da = nullptr;
+    int32_t* ds = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        dp = cv.take<double>((size_t)n * 3);
+        da = cv.take<double>((size_t)n * 3);
+        ds = cv.take<int32_t>((size_t)n);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
     cudaError_t e = cudaMemcpyAsync(dp, pos, b3, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
         e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, dp, da, ds, ctx->stream);
@@ -605,15 +609,19 @@ int bqp_rhs_eval(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t
     int rc = set_device(ctx);
     if (rc) return rc;
     const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
-    if ((rc = ensure_ws(ctx, 4 * rounded(b6) + 3 * rounded(b1) + 4096))) return rc;
-    Carve cv{(char*)ctx->d_ws};
-    double* de = cv.take<double>((size_t)n * 6);
-    double* dt0 = cv.take<double>((size_t)n);
-    double* djd = cv.take<double>((size_t)n);
-    double* dt = cv.take<double>((size_t)n);
-    double* dd = cv.take<double>((size_t)n * 6);
-    double* db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
-    double* dout = cv.take<double>((size_t)n * 6);
+    double *de = nullptr, *dt0 = nullptr, *djd = nullptr, *dt = nullptr, *dd = nullptr, *db = nullptr,
+           *dout = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        de = cv.take<double>((size_t)n * 6);
+        dt0 = cv.take<double>((size_t)n);
+        djd = cv.take<double>((size_t)n);
+        dt = cv.take<double>((size_t)n);
+        dd = cv.take<double>((size_t)n * 6);
+        db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
+        dout = cv.take<double>((size_t)n * 6);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(de, equ, b6, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dt0, seg_t0, b1, cudaMemcpyHostToDevice, s);
@@ -650,16 +658,21 @@ int bqp_propagate_final(bqp_ctx* ctx, int64_t n, const double* in, int32_t input
     if (n == 0) return 0;
     if ((rc = set_device(ctx))) return rc;
     const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
-    if ((rc = ensure_ws(ctx, 2 * rounded(b6) + 6 * rounded(b1) + 4096))) return rc;
-    Carve cv{(char*)ctx->d_ws};
-    double* din = cv.take<double>((size_t)n * 6);
-    double* dep = cv.take<double>((size_t)n);
-    double* dtf = cv.take<double>((size_t)n);
-    double* db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
-    double* dout = cv.take<double>((size_t)n * 6);
-    int32_t* dst = cv.take<int32_t>((size_t)n);
-    int64_t* dsteps = cv.take<int64_t>((size_t)n);
-    int64_t* devals = cv.take<int64_t>((size_t)n);
+    double *din = nullptr, *dep = nullptr, *dtf = nullptr, *db = nullptr, *dout = nullptr;
+    int32_t* dst = nullptr;
+    int64_t *dsteps = nullptr, *devals = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        din = cv.take<double>((size_t)n * 6);
+        dep = cv.take<double>((size_t)n);
+        dtf = cv.take<double>((size_t)n);
+        db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
+        dout = cv.take<double>((size_t)n * 6);
+        dst = cv.take<int32_t>((size_t)n);
+        dsteps = cv.take<int64_t>((size_t)n);
+        devals = cv.take<int64_t>((size_t)n);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(din, in, b6, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
@@ -704,17 +717,21 @@ int bqp_propagate_sampled(bqp_ctx* ctx, int64_t n, const double* in, int32_t inp
     if ((rc = set_device(ctx))) return rc;
     const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
     const size_t bo = (size_t)n * n_t * 6 * sizeof(double);
-    if ((rc = ensure_ws(ctx, rounded(b6) + 5 * rounded(b1) + rounded(bo) + rounded((size_t)n_t * 8) + 4096)))
-        return rc;
-    Carve cv{(char*)ctx->d_ws};
-    double* din = cv.take<double>((size_t)n * 6);
-    double* dep = cv.take<double>((size_t)n);
-    double* dtf = cv.take<double>((size_t)n);
-    double* dte = cv.take<double>((size_t)n_t);
-    double* dout = cv.take<double>((size_t)n * n_t * 6);
-    int32_t* dst = cv.take<int32_t>((size_t)n);
-    int64_t* dsteps = cv.take<int64_t>((size_t)n);
-    int64_t* devals = cv.take<int64_t>((size_t)n);
+    double *din = nullptr, *dep = nullptr, *dtf = nullptr, *dte = nullptr, *dout = nullptr;
+    int32_t* dst = nullptr;
+    int64_t *dsteps = nullptr, *devals = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        din = cv.take<double>((size_t)n * 6);
+        dep = cv.take<double>((size_t)n);
+        dtf = cv.take<double>((size_t)n);
+        dte = cv.take<double>((size_t)n_t);
+        dout = cv.take<double>((size_t)n * n_t * 6);
+        dst = cv.take<int32_t>((size_t)n);
+        dsteps = cv.take<int64_t>((size_t)n);
+        devals = cv.take<int64_t>((size_t)n);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(din, in, b6, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
