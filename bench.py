@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--n", type=int, default=N_TRAJ)
     ap.add_argument("--cpu-sample", type=int, default=256, help="trajectories in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--segment", type=float, default=SEGMENT_S,
+                    help="seconds propagated per step (5400 = one Encke segment; smaller for profiling)")
+    ap.add_argument("--engine", default="pipeline", choices=["pipeline", "persistent"])
+    ap.add_argument("--gravity-threads", type=int, default=512)
     return ap.parse_args()
 
 
@@ -134,10 +138,12 @@ def make_workload(n: int, seed: int = 0):
     return W.synthetic_field(ORDER), states, bal, W.EPOCH_JD
 
 
-def make_config():
+def make_config(engine="pipeline", gravity_threads=512):
     from bqp_b200 import _native as N
 
     cfg = N.default_config()
+    cfg.engine = N.ENGINES[engine]
+    cfg.gravity_threads = gravity_threads
     cfg.order = ORDER
     cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON
     cfg.atm_model = 4
@@ -230,8 +236,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
     text, states, bal, epoch = make_workload(args.n, seed=rank)
-    cfg = make_config()
+    cfg = make_config(args.engine, args.gravity_threads)
     ctx = N.Context(text, cfg)
+    seg = args.segment
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     n = args.n
@@ -241,12 +248,12 @@ def run_ours(args):
         d_a = torch.tensor(states, device=dev, dtype=torch.float64)
         d_b = torch.empty_like(d_a)
         d_bal = torch.tensor(bal, device=dev, dtype=torch.float64)
-        d_tf = torch.full((n,), SEGMENT_S, device=dev, dtype=torch.float64)
+        d_tf = torch.full((n,), seg, device=dev, dtype=torch.float64)
         d_status = torch.empty(n, device=dev, dtype=torch.int32)
         d_steps = torch.empty(n, device=dev, dtype=torch.int64)
         d_evals = torch.empty(n, device=dev, dtype=torch.int64)
         flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
-    epochs = [epoch + k * SEGMENT_S / 86400.0 for k in range(args.warmup + args.steps + 1)]
+    epochs = [epoch + k * seg / 86400.0 for k in range(args.warmup + args.steps + 1)]
     d_epochs = [torch.full((n,), e, device=dev, dtype=torch.float64) for e in epochs]
     torch.cuda.synchronize()
 
@@ -315,7 +322,7 @@ def run_ours(args):
     h_bal = pinned((n, 2), torch.float64)
     h_bal[:] = bal
     h_tf = pinned((n,), torch.float64)
-    h_tf[:] = SEGMENT_S
+    h_tf[:] = seg
     h_ep = pinned((n,), torch.float64)
     h_st = pinned((n,), torch.int32)
     h_steps = pinned((n,), torch.int64)
@@ -364,11 +371,11 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
-                                   "DOP853 eps 1e-12, one 5400 s Encke segment per step",
-                       "form": "plain FP64", "order": ORDER, "trajectories_per_gpu": n,
-                       "segment_s": SEGMENT_S, "l2": "256 MiB write between timed steps",
+                                   f"DOP853 eps 1e-12, {seg:g} s of the arc per step",
+                       "form": "plain FP64", "engine": args.engine, "order": ORDER, "trajectories_per_gpu": n,
+                       "segment_s": seg, "l2": "256 MiB write between timed steps",
                        "evals_per_step": total_evals / args.steps,
-                       "trajectory_days_per_s": world * n * SEGMENT_S / 86400.0 / (t_max * 1e-3 / args.steps)},
+                       "trajectory_days_per_s": world * n * seg / 86400.0 / (t_max * 1e-3 / args.steps)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,

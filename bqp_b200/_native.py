@@ -30,6 +30,7 @@ ST_OK, ST_GROUND, ST_GRAVITY_RADIUS = 0, 9, 6
 
 FORCE_DRAG, FORCE_SRP, FORCE_SUN, FORCE_MOON = 1, 2, 4, 8
 METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2}
+ENGINES = {"pipeline": 0, "persistent": 1}
 
 E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5
 
@@ -43,7 +44,7 @@ class ForceConfig(C.Structure):
         ("am_ratio", C.c_double), ("cd", C.c_double), ("earth_radius", C.c_double),
         ("omega_earth", C.c_double), ("mu_sun", C.c_double), ("mu_moon", C.c_double),
         ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
-        ("max_kernel_seconds", C.c_double),
+        ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
     ]
 
 

@@ -191,6 +191,8 @@ struct bqp_ctx {
     unsigned long long* d_queue = nullptr;
     void* d_ws = nullptr;
     size_t ws_bytes = 0;
+    void* d_pws = nullptr;  // stage-synchronous engine buffers
+    size_t pws_bytes = 0;
 };
 
 namespace {
@@ -220,7 +222,11 @@ int validate_cfg(const bqp_force_config* c) {
     if (!(std::isfinite(c->am_ratio) && c->am_ratio >= 0.0 && std::isfinite(c->cd) && c->cd >= 0.0))
         return fail(BQP_E_ARG, "am_ratio and cd must be finite and >= 0");
     if (c->max_steps <= 0 || c->max_attempts <= 0) return fail(BQP_E_ARG, "step budgets must be > 0");
-    if (!(c->max_kernel_seconds >= 0.0)) return fail(BQP_E_ARG, "max_kernel_seconds must be >= 0");
+    if (!(c->max_kernel_seconds > 0.0)) return fail(BQP_E_ARG, "max_kernel_seconds must be > 0");
+    if (c->engine != BQP_ENGINE_PIPELINE && c->engine != BQP_ENGINE_PERSISTENT)
+        return fail(BQP_E_ARG, "unknown engine %d", c->engine);
+    if (c->gravity_threads < 0 || c->gravity_threads > 1024 || c->gravity_threads % 32)
+        return fail(BQP_E_ARG, "gravity_threads must be a multiple of 32 in 0..1024");
     return 0;
 }
 
@@ -333,6 +339,26 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.use_smem = ctx->use_smem;
     A.force = force_params(ctx);
     A.ctrl = ctrl_params(ctx);
+    if (ctx->cfg.engine == BQP_ENGINE_PIPELINE) {
+        const size_t need = pipeline_bytes(n);
+        if (need > ctx->pws_bytes) {
+            if (ctx->d_pws) {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(ctx->d_pws);
+                ctx->d_pws = nullptr;
+                ctx->pws_bytes = 0;
+            }
+            cudaError_t e = cudaMalloc(&ctx->d_pws, need);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(pipeline buffers)");
+            ctx->pws_bytes = need;
+        }
+        PipeBufs P{};
+        pipeline_carve(P, ctx->d_pws, n);
+        cudaError_t e = launch_pipeline(A, P, ctx->cfg.method, ctx->stream, ctx->cfg.max_kernel_seconds,
+                                        ctx->cfg.gravity_threads);
+        if (e != cudaSuccess) return cuda_fail(e, "pipeline");
+        return 0;
+    }
     cudaError_t e = cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
     e = launch_propagate(A, ctx->cfg.method, 256, 0, ctx->stream);
@@ -471,6 +497,8 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->max_steps = 500000;             // MAX_STEPS (integrator.rs:185)
     c->max_attempts = (int64_t)1 << 40;
     c->max_kernel_seconds = 600.0;
+    c->engine = BQP_ENGINE_PIPELINE;
+    c->gravity_threads = 512;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -516,6 +544,7 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_tab) cudaFree(ctx->d_tab);
     if (ctx->d_queue) cudaFree(ctx->d_queue);
     if (ctx->d_ws) cudaFree(ctx->d_ws);
+    if (ctx->d_pws) cudaFree(ctx->d_pws);
     delete ctx;
     return 0;
 }

@@ -59,6 +59,19 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
+// Copy the field table into dynamic shared memory with 16-byte vector loads.
+__device__ __forceinline__ const double* stage_table(const double* __restrict__ g, int ncells,
+                                                     bool to_smem) {
+    extern __shared__ __align__(16) double smem_tab[];
+    if (!to_smem) return g;
+    const int nvec = ncells * (kCellDoubles / 2);
+    const double2* src = reinterpret_cast<const double2*>(g);
+    double2* dst = reinterpret_cast<double2*>(smem_tab);
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+    return smem_tab;
+}
+
 // One Encke force evaluation: derivative of the deviation `d` from the
 // baseline orbit (rhs.rs:3885-4118).  Gravity uses the field table without
 // its C00 term, which equals the reference's full field followed by the

@@ -33,6 +33,35 @@ struct PropArgs {
     CtrlParams ctrl;
 };
 
+struct TrajState;
+
+// Device buffers of the stage-synchronous engine.  Per-trajectory controller
+// state is an array of TrajState; everything per stage is indexed by the
+// trajectory's slot in the active list of the current attempt (so the force
+// kernels read contiguous, coalesced arrays).
+struct PipeBufs {
+    int64_t cap;          // slots (= trajectories)
+    TrajState* st;        // [cap]
+    int32_t* idx[2];      // active lists (slot -> trajectory), double-buffered
+    int32_t* count;       // [2] active counts
+    double* k;            // [(S+1)][6][cap] stage derivatives
+    double* sp;           // [6][cap] perturbed state of the stage (ECI)
+    double* sc;           // [2][cap] sin, cos of the GMST angle
+    double* sun;          // [3][cap] Sun position (ECI), drag only
+    double* part;         // [3][cap] third-body + Battin acceleration (ECI)
+    double* agrav;        // [3][cap] gravity (Earth-fixed)
+    double* adrag;        // [3][cap] drag (ECI)
+    double* jd;           // [cap]
+    double* amcd;         // [2][cap]
+    int32_t* skip;        // [cap] 1: stage derivative reused, no force call
+    int32_t* bad;         // [cap] latched invalid-radius gravity error
+};
+
+size_t pipeline_bytes(int64_t cap);
+void pipeline_carve(PipeBufs& P, void* base, int64_t cap);
+cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st,
+                            double max_seconds, int gravity_threads);
+
 cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
                            const double* pos, double* acc, int32_t* status, cudaStream_t st);
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,

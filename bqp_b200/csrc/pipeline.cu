@@ -1,0 +1,424 @@
+// Stage-synchronous propagation engine.
+//
+// The persistent kernel (propagate.cu) runs the whole force model and the
+// controller inside one thread per trajectory; at 70x70 + JB2008 that kernel
+// is large, register-bound (255 registers, 8 warps per SM) and stalls on
+// instruction fetch.  Here every RK stage of every active trajectory is one
+// pass over three specialised kernels, and one controller kernel closes the
+// attempt:
+//
+//   pl_prep<M>(s)   finish stage s-1, form y_s = y + h sum a_sj k_j, the Encke
+//                   baseline (Kepler solve), GMST rotation, Sun/Moon third body
+//                   and Battin's term                       (latency / SFU bound)
+//   pl_gravity      normalised column recursion, table in shared memory,
+//                   one trajectory per thread               (FP64-FMA bound)
+//   pl_drag         JB2008 density and co-rotating drag     (transcendental bound)
+//   pl_control<M>   finish the last stage, error norm, accept / reject, samples,
+//                   rectification, next attempt; compacts the active list
+//
+// Stage data are indexed by the trajectory's slot in the active list, so the
+// force kernels stream contiguous arrays; the active list shrinks as
+// trajectories finish.  The attempt sequence is captured once as a CUDA graph
+// and replayed; the host reads the active count between replays.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "launch.h"
+#include "traj.cuh"
+
+namespace bqp {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double* K(const PipeBufs& P, int st, int i) { return P.k + ((size_t)st * 6 + i) * P.cap; }
+
+// Append `traj` to the next active list (warp-aggregated atomic).
+__device__ __forceinline__ void append_active(int32_t* list, int32_t* count, int32_t traj, bool keep) {
+    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+    if (!keep) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    list[base + rank] = traj;
+}
+
+// Sum of the stage-`st` force terms into K(st, 3..5).
+__device__ __forceinline__ void finish_stage(const PipeBufs& P, int st, int slot) {
+    const double s = P.sc[slot], c = P.sc[P.cap + slot];
+    const double gx = P.agrav[slot], gy = P.agrav[P.cap + slot], gz = P.agrav[2 * P.cap + slot];
+    K(P, st, 3)[slot] = fma(c, gx, -s * gy) + P.adrag[slot] + P.part[slot];
+    K(P, st, 4)[slot] = fma(s, gx, c * gy) + P.adrag[P.cap + slot] + P.part[P.cap + slot];
+    K(P, st, 5)[slot] = gz + P.adrag[2 * P.cap + slot] + P.part[2 * P.cap + slot];
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------- init
+template <int M>
+__global__ void __launch_bounds__(kBlock) pl_init(PropArgs A, PipeBufs P) {
+    const int64_t traj = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool keep = false;
+    if (traj < A.n) {
+        TrajState s;
+        traj_begin(A, s, traj);
+        if (s.phase == kNeedSegment) seg_begin<M>(A, s, traj);
+        if (s.phase == kStepping) {
+            const int32_t f = attempt_begin<M>(A, s, false);
+            if (f >= 0) traj_fail(A, s, traj, f);
+            else keep = true;
+        }
+        P.st[traj] = s;
+    }
+    append_active(P.idx[0], &P.count[0], (int32_t)traj, keep);
+}
+
+// --------------------------------------------------------------------- prep
+// Stage `st` of the current attempt.  st == S is the dense-output stage of
+// the sampled non-FSAL path: f(t_next, y_next) evaluated before the
+// controller decides (the reference evaluates it after an accept).
+template <int M>
+__global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cur, int st) {
+    using T = Tab<M>;
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st == 0 && blockIdx.x == 0 && threadIdx.x == 0) P.count[cur ^ 1] = 0;
+    if (slot >= P.count[cur]) return;
+    const int32_t traj = P.idx[cur][slot];
+    const TrajState& s = P.st[traj];
+    if (st == 0) {
+        P.bad[slot] = 0;
+        if (s.flags & kHaveK1) {
+            for (int i = 0; i < 6; ++i) K(P, 0, i)[slot] = s.k1c[i];
+            P.skip[slot] = 1;
+            return;
+        }
+    } else if (!(st == 1 && P.skip[slot])) {
+        finish_stage(P, st - 1, slot);
+    }
+    P.skip[slot] = 0;
+    // stage state
+    double yt[6];
+    for (int i = 0; i < 6; ++i) yt[i] = s.y[i];
+    double ts;
+    if (st < T::S) {
+#pragma unroll 1
+        for (int j = 0; j < st; ++j) {
+            const double a = s.hs * T::a(st, j);
+            if (a != 0.0)
+                for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], a, yt[i]);
+        }
+        ts = s.t + T::c(st) * s.hs;
+    } else {
+        // y_next exactly as rk_combine forms it
+#pragma unroll 1
+        for (int j = 0; j < T::S; ++j) {
+            const double b = s.hs * T::b(j);
+            if (b != 0.0)
+                for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], b, yt[i]);
+        }
+        ts = next_time(s);
+    }
+    double rs[6];
+    baseline_state(baseline_new(s.cur), ts - s.ct0, rs);
+    double sp[6];
+    for (int i = 0; i < 6; ++i) {
+        sp[i] = rs[i] + yt[i];
+        P.sp[(size_t)i * P.cap + slot] = sp[i];
+    }
+    for (int i = 0; i < 3; ++i) K(P, st, i)[slot] = yt[3 + i];
+    const double jd = s.jd0 + ts / kSecPerDay;
+    const ForceParams& fp = A.force;
+    double sn = 0.0, cs = 1.0;
+    if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);
+    P.sc[slot] = sn;
+    P.sc[P.cap + slot] = cs;
+    double acc[3] = {0.0, 0.0, 0.0};
+    double sun[3];
+    const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0);
+    if (need_sun) sun_position(jd, sun);
+    if (fp.sun) third_body(sp, sun, fp.mu_sun, acc);
+    if (fp.moon) {
+        double moon[3];
+        moon_position(jd, moon);
+        third_body(sp, moon, fp.mu_moon, acc);
+    }
+    const double r2 = fma(sp[0], sp[0], fma(sp[1], sp[1], sp[2] * sp[2]));
+    battin(rs, yt, r2, sqrt(r2), acc);
+    for (int i = 0; i < 3; ++i) P.part[(size_t)i * P.cap + slot] = acc[i];
+    if (fp.drag) {
+        for (int i = 0; i < 3; ++i) P.sun[(size_t)i * P.cap + slot] = sun[i];
+        P.jd[slot] = jd;
+        P.amcd[slot] = s.am;
+        P.amcd[P.cap + slot] = s.cd;
+    } else {
+        for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = 0.0;
+    }
+    if (!fp.gravity_on)
+        for (int i = 0; i < 3; ++i) P.agrav[(size_t)i * P.cap + slot] = 0.0;
+}
+
+// ------------------------------------------------------------------ gravity
+// Persistent over slots: each CTA stages the field table once.
+__global__ void pl_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem, PipeBufs P,
+                           int cur) {
+    const int count = P.count[cur];
+    if ((int64_t)blockIdx.x * blockDim.x >= count) return;
+    const double* tab = stage_table(gtab, ncells, use_smem != 0);
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+        if (P.skip[slot]) continue;
+        const double s = P.sc[slot], c = P.sc[P.cap + slot];
+        const double x = P.sp[slot], y = P.sp[P.cap + slot], z = P.sp[2 * P.cap + slot];
+        const double px = fma(c, x, s * y), py = fma(-s, x, c * y);
+        const double r2 = fma(px, px, fma(py, py, z * z));
+        double a[3];
+        if (!(isfinite(r2) && r2 > 0.0)) {
+            P.bad[slot] = 1;
+            a[0] = a[1] = a[2] = NAN;
+        } else {
+            gravity_field(tab, order, px, py, z, a);
+        }
+        P.agrav[slot] = a[0];
+        P.agrav[P.cap + slot] = a[1];
+        P.agrav[2 * P.cap + slot] = a[2];
+    }
+}
+
+// --------------------------------------------------------------------- drag
+__global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, int cur) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.count[cur]) return;
+    if (P.skip[slot]) return;
+    double sp[6];
+    for (int i = 0; i < 6; ++i) sp[i] = P.sp[(size_t)i * P.cap + slot];
+    const double am = P.amcd[slot], cd = P.amcd[P.cap + slot];
+    double a[3] = {0.0, 0.0, 0.0};
+    if (cd != 0.0 && am != 0.0) {
+        const double s = P.sc[slot], c = P.sc[P.cap + slot];
+        const double sun[3] = {P.sun[slot], P.sun[P.cap + slot], P.sun[2 * P.cap + slot]};
+        const double pi[3] = {fma(c, sp[0], s * sp[1]), fma(-s, sp[0], c * sp[1]), sp[2]};
+        Encke E;  // only its JB2008 adapter is used
+        E.fp = &fp;
+        const double rho = E.density_at(pi, sun, s, c, P.jd[slot]);
+        if (isnan(rho)) {
+            a[0] = a[1] = a[2] = NAN;
+        } else if (rho > 0.0) {
+            const double w = fp.omega;
+            const double vr0 = (sp[3] + w * sp[1]) * 1000.0;
+            const double vr1 = (sp[4] - w * sp[0]) * 1000.0;
+            const double vr2 = sp[5] * 1000.0;
+            const double v2 = fma(vr0, vr0, fma(vr1, vr1, vr2 * vr2));
+            if (v2 != 0.0) {
+                const double k = -0.5 * cd * am * rho * sqrt(v2) * 1e-3;
+                a[0] = k * vr0;
+                a[1] = k * vr1;
+                a[2] = k * vr2;
+            }
+        }
+    }
+    for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = a[i];
+}
+
+// ------------------------------------------------------------------ control
+template <int M>
+__global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int cur, int dense,
+                                                      int timed_out) {
+    using T = Tab<M>;
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int count = P.count[cur];
+    bool keep = false;
+    int32_t traj = 0;
+    if (slot < count) {
+        traj = P.idx[cur][slot];
+        TrajState s = P.st[traj];
+        const int last = dense ? T::S : T::S - 1;
+        if (!(last == 1 && P.skip[slot])) finish_stage(P, last, slot);
+        // stage derivatives of this attempt
+        const int evaluated = T::S - ((s.flags & kHaveK1) ? 1 : 0);
+        s.evals += evaluated;
+        double ynext[6], err[6], err3[6];
+        rk_combine<M>(s, [&](int st, int i) { return K(P, st, i)[slot]; }, ynext, err, err3);
+        double k0[6];
+        for (int i = 0; i < 6; ++i) k0[i] = K(P, 0, i)[slot];
+        double en;
+        int32_t code = -1;
+        const int32_t d = attempt_decide<M>(A, s, k0, ynext, err, err3, &en, &code);
+        if (P.bad[slot]) {
+            traj_fail(A, s, traj, kGravityRadius);
+        } else if (d == kFail) {
+            traj_fail(A, s, traj, code);
+        } else if (d == kAccept) {
+            double dyn[6];
+            const double* dy_next = nullptr;
+            if (T::FSAL) {
+                for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S - 1, i)[slot];
+                dy_next = dyn;
+            } else if (dense) {
+                for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S, i)[slot];
+                dy_next = dyn;
+                ++s.evals;  // counted on accept only, as the reference evaluates it
+            }
+            attempt_accept<M>(A, s, traj, ynext, k0, dy_next, en);
+        }
+        if (s.phase == kNeedSegment) seg_begin<M>(A, s, traj);
+        if (s.phase == kStepping) {
+            const int32_t f = attempt_begin<M>(A, s, timed_out != 0);
+            if (f >= 0) traj_fail(A, s, traj, f);
+            else keep = true;
+        }
+        P.st[traj] = s;
+    }
+    if (slot - threadIdx.x % 32 < count)  // whole warps take part in the ballot
+        append_active(P.idx[cur ^ 1], &P.count[cur ^ 1], traj, keep);
+}
+
+// Rows still active when the host gives up (wall-clock watchdog).
+template <int M>
+__global__ void __launch_bounds__(kBlock) pl_abort(PropArgs A, PipeBufs P, int cur) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.count[cur]) return;
+    const int32_t traj = P.idx[cur][slot];
+    TrajState s = P.st[traj];
+    traj_fail(A, s, traj, kWatchdog);
+    P.st[traj] = s;
+}
+
+// ------------------------------------------------------------------- host
+size_t pipeline_bytes(int64_t cap) {
+    PipeBufs P{};
+    pipeline_carve(P, nullptr, cap);
+    return (size_t)(uintptr_t)P.bad + (size_t)cap * sizeof(int32_t) + 256;
+}
+
+void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        char* p = (char*)base + off;
+        off += bytes;
+        return (void*)p;
+    };
+    const size_t c = (size_t)cap;
+    P.cap = cap;
+    P.st = (TrajState*)take(c * sizeof(TrajState));
+    P.idx[0] = (int32_t*)take(c * 4);
+    P.idx[1] = (int32_t*)take(c * 4);
+    P.count = (int32_t*)take(2 * 4);
+    P.k = (double*)take((size_t)13 * 6 * c * 8);
+    P.sp = (double*)take(6 * c * 8);
+    P.sc = (double*)take(2 * c * 8);
+    P.sun = (double*)take(3 * c * 8);
+    P.part = (double*)take(3 * c * 8);
+    P.agrav = (double*)take(3 * c * 8);
+    P.adrag = (double*)take(3 * c * 8);
+    P.jd = (double*)take(c * 8);
+    P.amcd = (double*)take(2 * c * 8);
+    P.skip = (int32_t*)take(c * 4);
+    P.bad = (int32_t*)take(c * 4);
+}
+
+template <int M>
+static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, double max_seconds,
+                       int gthreads) {
+    using T = Tab<M>;
+    const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
+    const int stages = T::S + (dense ? 1 : 0);
+    const int blocks = (int)((A.n + kBlock - 1) / kBlock);
+    const size_t smem = A.use_smem ? (size_t)A.ncells * kCellDoubles * sizeof(double) : 0;
+    cudaError_t e = cudaFuncSetAttribute(pl_gravity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int gblocks = device_sm_count();
+    if ((int64_t)gblocks * gthreads > A.n) gblocks = (int)((A.n + gthreads - 1) / gthreads);
+    if (gblocks < 1) gblocks = 1;
+
+    // private stream ordered after the caller's stream (graphs need a
+    // capturable stream)
+    cudaStream_t st;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t ev_in, ev_out, ev_cnt;
+    cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_cnt, cudaEventDisableTiming);
+    cudaEventRecord(ev_in, user);
+    cudaStreamWaitEvent(st, ev_in, 0);
+    int32_t* h_count = nullptr;
+    cudaMallocHost(&h_count, sizeof(int32_t));
+
+    cudaMemsetAsync(P.count, 0, 2 * sizeof(int32_t), st);
+    pl_init<M><<<blocks, kBlock, 0, st>>>(A, P);
+
+    // one graph = two attempts (active list 0 -> 1 -> 0)
+    auto enqueue_attempt = [&](int cur, int timed_out) {
+        for (int s = 0; s < stages; ++s) {
+            pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s);
+            if (A.force.gravity_on)
+                pl_gravity<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, P, cur);
+            if (A.force.drag) pl_drag<<<blocks, kBlock, 0, st>>>(A.force, P, cur);
+        }
+        pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out);
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_attempt(0, 0);
+        enqueue_attempt(1, 0);
+        e = cudaStreamEndCapture(st, &graph);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    const auto t_start = std::chrono::steady_clock::now();
+    // host loop: replay, keep one replay in flight ahead of the count check
+    int64_t replays = 0;
+    bool done = false;
+    while (e == cudaSuccess && !done) {
+        e = cudaGraphLaunch(exec, st);
+        if (e != cudaSuccess) break;
+        cudaMemcpyAsync(h_count, &P.count[0], sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        cudaEventRecord(ev_cnt, st);
+        e = cudaGraphLaunch(exec, st);  // speculative: cheap when nothing is active
+        if (e != cudaSuccess) break;
+        e = cudaEventSynchronize(ev_cnt);
+        replays += 2;
+        if (*h_count == 0) done = true;
+        const double elapsed =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+        if (!done && max_seconds > 0.0 && elapsed > max_seconds) {
+            cudaStreamSynchronize(st);
+            pl_abort<M><<<blocks, kBlock, 0, st>>>(A, P, 0);
+            done = true;
+        }
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaEventRecord(ev_out, st);
+    cudaStreamWaitEvent(user, ev_out, 0);
+    cudaStreamSynchronize(st);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFreeHost(h_count);
+    cudaEventDestroy(ev_in);
+    cudaEventDestroy(ev_out);
+    cudaEventDestroy(ev_cnt);
+    cudaStreamDestroy(st);
+    return e;
+}
+
+cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st, double max_seconds,
+                            int gravity_threads) {
+    if (A.n <= 0) return cudaSuccess;
+    if (gravity_threads <= 0) gravity_threads = 512;
+    switch (method) {
+        case kDopri5: return run<kDopri5>(A, P, st, max_seconds, gravity_threads);
+        case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads);
+        case kDopri5Compat: return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace bqp

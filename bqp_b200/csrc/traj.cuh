@@ -1,0 +1,490 @@
+// Per-trajectory controller shared by both propagation engines: the
+// persistent work-queue kernel (k_propagate) and the stage-synchronous
+// pipeline (pipeline.cu).  It carries the reference's solver semantics once:
+//
+//   explicit RK step bookkeeping, Kahan-compensated error sums and time
+//   (odesolve/solver.rs:1965-2173, 1551-1572), max-norm / WRMS error with the
+//   DOP853 3rd-order blend (1431-1520), the PI controller (445-531), the
+//   DOPRI5 compatibility loop's own controller (lightyear_compat.rs), Encke
+//   segments of at most 5400 s with a rebase when |dr| > 10 km or the segment
+//   is not the last (integrator.rs:941-979, 3418-3560), the restart budget
+//   ceil(span/dt_max)+128 clamped to [100, 500000] (3912-3917), the sampled
+//   path's 100-segment cap (2366, 2408-2414) and its Hermite samples
+//   (solver.rs:1746-1800).
+#pragma once
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "launch.h"
+
+#ifndef BQP_TAB_CONST
+#define BQP_TAB_CONST static __constant__ const
+#endif
+#include "rk_tableaus.h"
+
+namespace bqp {
+
+template <int M>
+struct Tab;
+template <>
+struct Tab<kDopri5> {
+    static constexpr int S = 7, ORDER_ERR = 4, FSAL = 1, HAS_E3 = 0;
+    __device__ static double a(int i, int j) { return bqp_dopri5_a[i * S + j]; }
+    __device__ static double b(int i) { return bqp_dopri5_b[i]; }
+    __device__ static double c(int i) { return bqp_dopri5_c[i]; }
+    __device__ static double e(int i) { return bqp_dopri5_e[i]; }
+    __device__ static double e3(int) { return 0.0; }
+};
+template <>
+struct Tab<kDopri5Compat> : Tab<kDopri5> {};
+template <>
+struct Tab<kDop853> {
+    static constexpr int S = 12, ORDER_ERR = 5, FSAL = 0, HAS_E3 = 1;
+    __device__ static double a(int i, int j) { return bqp_dop853_a[i * S + j]; }
+    __device__ static double b(int i) { return bqp_dop853_b[i]; }
+    __device__ static double c(int i) { return bqp_dop853_c[i]; }
+    __device__ static double e(int i) { return bqp_dop853_e[i]; }
+    __device__ static double e3(int i) { return bqp_dop853_e3[i]; }
+};
+
+enum OutMode : int32_t { kOutFinalEci = 0, kOutSampledEci = 1, kOutSampledDelta = 2 };
+enum Phase : int32_t { kNeedTraj = 0, kNeedSegment = 1, kStepping = 2, kDone = 3, kFinished = 4 };
+enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16 };
+
+struct TrajState {
+    double tf, ct0, seg_tf, t, h, err_prev, t_comp, hs;
+    double jd0, am, cd;
+    double cur[6], equ0[6], y[6], k1c[6];
+    int32_t flags, rejects, s_idx, phase, status;
+    int64_t seg_steps, steps, evals, attempts, restarts, max_restarts;
+};
+
+__device__ __forceinline__ bool finite6(const double* v) {
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ok = ok && isfinite(v[i]);
+    return ok;
+}
+
+__device__ __forceinline__ double clampd(double x, double lo, double hi) { return fmin(fmax(x, lo), hi); }
+
+__device__ __forceinline__ bool sampled_mode(const PropArgs& A) { return A.out_mode != kOutFinalEci; }
+
+// ---------------------------------------------------------------- outputs
+// Deviation at sample time ts on the segment baseline -> deviation against
+// the original baseline (integrator.rs:1163-1177) or ECI (lib.rs:316-322).
+static __device__ __noinline__ void write_sample(const PropArgs& A, const TrajState& s, int64_t traj,
+                                          const double* dseg, double ts) {
+    double* o = A.out + ((size_t)traj * A.n_t + s.s_idx) * 6;
+    const Baseline orig = baseline_new(s.equ0);
+    double bo[6];
+    baseline_state(orig, ts - A.t0, bo);
+    double dorig[6];
+    if (s.flags & kHad) {
+        double bs[6];
+        baseline_state(baseline_new(s.cur), ts - s.ct0, bs);
+        for (int i = 0; i < 6; ++i) dorig[i] = (dseg[i] + bs[i]) - bo[i];
+    } else {
+        for (int i = 0; i < 6; ++i) dorig[i] = dseg[i];
+    }
+    if (A.out_mode == kOutSampledDelta) {
+        for (int i = 0; i < 6; ++i) o[i] = dorig[i];
+    } else {
+        for (int i = 0; i < 6; ++i) o[i] = bo[i] + dorig[i];
+    }
+}
+
+__device__ __forceinline__ void write_counters(const PropArgs& A, int64_t traj, const TrajState& s) {
+    A.status[traj] = s.status;
+    if (A.steps) A.steps[traj] = s.steps;
+    if (A.evals) A.evals[traj] = s.evals;
+}
+
+// Fail a trajectory: NaN-fill what is not yet written (batch.rs:297).
+static __device__ __noinline__ void traj_fail(const PropArgs& A, TrajState& s, int64_t traj, int32_t code) {
+    if (!sampled_mode(A)) {
+        for (int i = 0; i < 6; ++i) A.out[6 * traj + i] = NAN;
+    } else {
+        for (int q = s.s_idx; q < A.n_t; ++q)
+            for (int i = 0; i < 6; ++i) A.out[((size_t)traj * A.n_t + q) * 6 + i] = NAN;
+    }
+    s.status = code;
+    s.phase = kFinished;
+    write_counters(A, traj, s);
+}
+
+// Successful end of the arc with the last segment's deviation d at tf.
+static __device__ __noinline__ void traj_finish_with(const PropArgs& A, TrajState& s, int64_t traj, const double* d) {
+    if (!sampled_mode(A)) {
+        double* o = A.out + 6 * traj;
+        double ob[6];
+        baseline_state(baseline_new(s.equ0), s.tf - A.t0, ob);
+        if (s.flags & kHad) {
+            double bs[6];
+            baseline_state(baseline_new(s.cur), s.tf - s.ct0, bs);
+            for (int i = 0; i < 6; ++i) o[i] = ob[i] + ((d[i] + bs[i]) - ob[i]);
+        } else {
+            for (int i = 0; i < 6; ++i) o[i] = ob[i] + d[i];
+        }
+    }
+    s.status = kOk;
+    s.phase = kFinished;
+    write_counters(A, traj, s);
+}
+
+// ------------------------------------------------------------ transitions
+// Load trajectory `traj` from the inputs.  Leaves phase kNeedSegment, or
+// kFinished with an invalid-input status.
+static __device__ __noinline__ void traj_begin(const PropArgs& A, TrajState& s, int64_t traj) {
+    s.tf = A.tf[traj];
+    s.jd0 = A.epoch[traj];
+    s.am = A.ballistic ? A.ballistic[2 * traj] : A.am0;
+    s.cd = A.ballistic ? A.ballistic[2 * traj + 1] : A.cd0;
+    s.steps = s.evals = s.attempts = s.restarts = 0;
+    s.seg_steps = 0;
+    s.flags = 0;
+    s.rejects = 0;
+    s.s_idx = 0;
+    s.status = kOk;
+    bool ok;
+    if (A.input_equinoctial) {
+        for (int i = 0; i < 6; ++i) s.equ0[i] = A.in[6 * traj + i];
+        ok = finite6(s.equ0) && baseline_new(s.equ0).ok != 0;
+    } else {
+        double e[6];
+        for (int i = 0; i < 6; ++i) e[i] = A.in[6 * traj + i];
+        ok = finite6(e) && eci_to_equinoctial(e, s.equ0);
+    }
+    ok = ok && isfinite(s.tf) && isfinite(s.jd0) && s.tf >= A.t0;
+    if (!ok) {
+        traj_fail(A, s, traj, kInvalidInput);
+        return;
+    }
+    for (int i = 0; i < 6; ++i) s.cur[i] = s.equ0[i];
+    s.ct0 = A.t0;
+    const double span = fabs(s.tf - A.t0);
+    const int64_t mr = (int64_t)ceil(span / (A.ctrl.h_max > 0.0 ? A.ctrl.h_max : 1.0)) + 128;
+    s.max_restarts = mr < 100 ? 100 : (mr > 500000 ? 500000 : mr);
+    if (sampled_mode(A)) {
+        s.max_restarts = 100;
+        const double zero[6] = {0, 0, 0, 0, 0, 0};
+        while (s.s_idx < A.n_t && A.t_eval[s.s_idx] <= A.t0) {
+            write_sample(A, s, traj, zero, A.t_eval[s.s_idx]);
+            ++s.s_idx;
+        }
+    }
+    s.phase = kNeedSegment;
+}
+
+// Start the next Encke segment, or end the arc.  Leaves kStepping or
+// kFinished.
+template <int M>
+__device__ __noinline__ void seg_begin(const PropArgs& A, TrajState& s, int64_t traj) {
+    for (int guard = 0; guard < 2 && s.phase == kNeedSegment; ++guard) {
+        if ((s.flags & kHad) && fabs(s.tf - s.ct0) < 1e-12) {  // integrator.rs:3440-3452
+            const double zero[6] = {0, 0, 0, 0, 0, 0};
+            traj_finish_with(A, s, traj, zero);
+            return;
+        }
+        if (s.restarts >= s.max_restarts) {
+            traj_fail(A, s, traj, sampled_mode(A) ? kMaxSteps : kRestartBudget);
+            return;
+        }
+        ++s.restarts;
+        const double rem = s.tf - s.ct0;
+        s.seg_tf = fabs(rem) > kMaxSegmentS ? s.ct0 + kMaxSegmentS : s.tf;
+        const double span = fabs(s.seg_tf - s.ct0);
+        if (!(span > 0.0)) {
+            s.flags |= kHad;
+            s.ct0 = s.seg_tf;
+            continue;
+        }
+        s.t = s.ct0;
+        for (int i = 0; i < 6; ++i) s.y[i] = 0.0;
+        double hmax = fabs(A.ctrl.h_max);
+        if (!isfinite(hmax) || hmax <= 0.0) hmax = span;
+        if (M == kDopri5Compat)
+            s.h = clampd(fabs((s.seg_tf - s.ct0) / 100.0), 1e-3, fmax(fmax(hmax, 1e-10), 1e-3));
+        else
+            s.h = clampd(span <= 60.0 ? span / 2.0 : span / 100.0, A.ctrl.h_min, hmax);
+        s.err_prev = 0.0;
+        s.t_comp = 0.0;
+        s.flags &= kHad;  // clear controller memory and the reusable first stage
+        s.rejects = 0;
+        s.seg_steps = 0;
+        s.phase = kStepping;
+    }
+}
+
+// The end time of the current attempt, as attempt_accept computes it
+// (Kahan-compensated unless the step lands on the segment end).
+__device__ __forceinline__ double next_time(const TrajState& s) {
+    if (s.flags & kLands) return s.seg_tf;
+    return s.t + (s.hs - s.t_comp);
+}
+
+__device__ __forceinline__ double seg_hmax(const PropArgs& A, const TrajState& s) {
+    const double hm = fabs(A.ctrl.h_max);
+    return (hm > 0.0 && isfinite(hm)) ? hm : fabs(s.seg_tf - s.ct0);
+}
+
+// Size the next attempt (hs, lands) or fail it.  Returns -1 or a status.
+template <int M>
+__device__ __forceinline__ int32_t attempt_begin(const PropArgs& A, TrajState& s, bool timed_out) {
+    const double hmin = M == kDopri5Compat ? 1e-10 : A.ctrl.h_min;
+    const double rem = s.seg_tf - s.t;
+    s.hs = fabs(s.h) < fabs(rem) ? s.h : rem;
+    if (s.hs == rem) s.flags |= kLands;
+    else s.flags &= ~kLands;
+    if (s.seg_steps >= A.ctrl.max_steps) return kMaxSteps;
+    if (M != kDopri5Compat && fabs(s.hs) < hmin && !(s.flags & kLands)) return kStepUnderflow;
+    if (++s.attempts > A.ctrl.max_attempts || timed_out) return kWatchdog;
+    if (M == kDopri5Compat) {  // the compat loop counts attempts (lightyear_compat.rs)
+        ++s.seg_steps;
+        ++s.steps;
+    }
+    return -1;
+}
+
+// ynext and the Kahan-compensated error estimates from the stage
+// derivatives K(st, i) (solver.rs:2098-2172).
+template <int M, typename KAt>
+__device__ __forceinline__ void rk_combine(const TrajState& s, KAt K, double* ynext, double* err, double* err3) {
+    using T = Tab<M>;
+    double comp[6], comp3[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        ynext[i] = s.y[i];
+        err[i] = err3[i] = comp[i] = comp3[i] = 0.0;
+    }
+#pragma unroll 1
+    for (int st = 0; st < T::S; ++st) {
+        const double hb = s.hs * T::b(st), he = s.hs * T::e(st), he3 = s.hs * T::e3(st);
+        if (hb == 0.0 && he == 0.0 && he3 == 0.0) continue;
+        double kv[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) kv[i] = K(st, i);
+        if (hb != 0.0) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) ynext[i] = fma(kv[i], hb, ynext[i]);
+        }
+        if (he != 0.0) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const double yk = he * kv[i] - comp[i];
+                const double acc = err[i] + yk;
+                comp[i] = (acc - err[i]) - yk;
+                err[i] = acc;
+            }
+        }
+        if (T::HAS_E3 && he3 != 0.0) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const double yk = he3 * kv[i] - comp3[i];
+                const double acc = err3[i] + yk;
+                comp3[i] = (acc - err3[i]) - yk;
+                err3[i] = acc;
+            }
+        }
+    }
+}
+
+enum Decision : int32_t { kReject = 0, kAccept = 1, kFail = 2 };
+
+// Error norm and accept / reject (solver.rs:1413-1540 and the reject branch
+// 1880-1905; the compat loop's own branches).  On reject it updates h and
+// returns kReject; on failure it returns kFail with *code set.
+template <int M>
+__device__ __forceinline__ int32_t attempt_decide(const PropArgs& A, TrajState& s, const double* y0_k,
+                                                  const double* ynext, const double* err, const double* err3,
+                                                  double* en_out, int32_t* code) {
+    using T = Tab<M>;
+    const CtrlParams& C = A.ctrl;
+    const double order = (double)T::ORDER_ERR + 1.0;
+    const double inv_order = 1.0 / order;
+    const double hmin = M == kDopri5Compat ? 1e-10 : C.h_min;
+    const double hmax = seg_hmax(A, s);
+    const double hmax_c = M == kDopri5Compat ? fmax(hmax, 1e-10) : hmax;
+    const double ah = fabs(s.hs);
+    double en = NAN, thr = 1.0;
+    const bool finite_step = finite6(ynext) && finite6(err);
+    if (finite_step) {
+        if (M == kDopri5Compat || !C.scaled) {
+            double m5 = 0.0, m3 = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                m5 = fmax(m5, fabs(err[i]));
+                m3 = fmax(m3, fabs(err3[i]));
+            }
+            const bool use_e3 = T::HAS_E3 && M != kDopri5Compat && C.eps >= 1e-6;
+            en = use_e3 ? sqrt(fma(m5, m5, 0.01 * m3 * m3)) : m5;
+            thr = C.eps;
+        } else {
+            double s5 = 0.0, s3 = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                const double sc = C.atol + C.rtol * fmax(fabs(s.y[i]), fabs(ynext[i]));
+                const double dn = sc > 0.0 ? sc : C.atol;
+                const double e5 = err[i] / dn, e3 = err3[i] / dn;
+                s5 = fma(e5, e5, s5);
+                s3 = fma(e3, e3, s3);
+            }
+            const double r5 = sqrt(s5 / 6.0);
+            if (T::HAS_E3) {
+                const double r3 = sqrt(s3 / 6.0);
+                en = sqrt(fma(r5, r5, 0.01 * r3 * r3));
+            } else {
+                en = r5;
+            }
+        }
+    }
+    *en_out = en;
+    if (!finite_step || !isfinite(en)) {
+        ++s.rejects;
+        if (M == kDopri5Compat) {
+            for (int i = 0; i < 6; ++i) s.k1c[i] = y0_k[i];
+            s.flags |= kHaveK1;
+        } else {
+            s.flags &= ~kHaveK1;
+        }
+        if (s.rejects > C.max_rejects) {
+            *code = kNonFinite;
+            return kFail;
+        }
+        s.h = clampd(ah * 0.1, hmin, hmax_c);
+        return kReject;
+    }
+    if (en <= thr || ah <= hmin) return kAccept;
+    ++s.rejects;
+    if (M == kDopri5Compat) {
+        for (int i = 0; i < 6; ++i) s.k1c[i] = y0_k[i];
+        s.flags |= kHaveK1;
+    } else {
+        s.flags &= ~kHaveK1;
+    }
+    if (s.rejects > C.max_rejects) {
+        *code = kMaxRejects;
+        return kFail;
+    }
+    if (M == kDopri5Compat) {
+        const double factor = 0.9 * pow(C.eps / en, 0.2);
+        s.h = clampd(ah * clampd(factor, 0.1, 0.5), 1e-10, hmax_c);
+        s.err_prev = en;
+        s.flags |= kHavePrev | kJustRej;
+    } else {
+        const double factor = !C.scaled ? 0.9 * pow(C.eps / en, inv_order) : 0.9 * pow(en, -inv_order);
+        s.h = clampd(ah * clampd(factor, 0.1, 0.5), hmin, hmax);
+        s.flags |= kJustRej;
+    }
+    return kReject;
+}
+
+// Accepted step: time update, samples, PI controller, ground check and the
+// segment end.  dy_prev = derivative at the step start, dy_next = at its end
+// (FSAL last stage or the dense stage; may be null in final-state mode).
+template <int M>
+__device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+                                            const double* dy_prev, const double* dy_next, double en) {
+    using T = Tab<M>;
+    const CtrlParams& C = A.ctrl;
+    const double order = (double)T::ORDER_ERR + 1.0;
+    const double inv_order = 1.0 / order;
+    const double hmin = M == kDopri5Compat ? 1e-10 : C.h_min;
+    const double hmax = seg_hmax(A, s);
+    const double ah = fabs(s.hs);
+    double tn;
+    if (s.flags & kLands) {
+        tn = s.seg_tf;
+    } else {
+        const double ky = s.hs - s.t_comp;
+        const double nx = s.t + ky;
+        s.t_comp = (nx - s.t) - ky;
+        tn = nx;
+    }
+    if (!isfinite(tn)) {
+        traj_fail(A, s, traj, kNonFinite);
+        return;
+    }
+    if (M != kDopri5Compat) {
+        ++s.seg_steps;
+        ++s.steps;
+    }
+    s.rejects = 0;
+    if (sampled_mode(A)) {
+        while (s.s_idx < A.n_t) {
+            const double ts = A.t_eval[s.s_idx];
+            if (ts - tn > 0.0) break;
+            double ds[6];
+            if (ts == tn) {
+                for (int i = 0; i < 6; ++i) ds[i] = ynext[i];
+            } else {
+                const double hd = tn - s.t;
+                const double tau = clampd((ts - s.t) / hd, 0.0, 1.0);
+                const double t2 = tau * tau, t3 = t2 * tau;
+                const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
+                const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+                for (int i = 0; i < 6; ++i)
+                    ds[i] = h00 * s.y[i] + h10 * hd * dy_prev[i] + h01 * ynext[i] + h11 * hd * dy_next[i];
+            }
+            write_sample(A, s, traj, ds, ts);
+            ++s.s_idx;
+        }
+    }
+    if (T::FSAL || sampled_mode(A)) {
+        for (int i = 0; i < 6; ++i) s.k1c[i] = dy_next[i];
+        s.flags |= kHaveK1;
+    } else {
+        s.flags &= ~kHaveK1;
+    }
+    s.t = tn;
+    for (int i = 0; i < 6; ++i) s.y[i] = ynext[i];
+    const double thr = (M == kDopri5Compat || !C.scaled) ? C.eps : 1.0;
+    const double eff = en > 0.0 ? en : thr * 0.1;
+    const bool have_prev = (s.flags & kHavePrev) && s.err_prev > 0.0;
+    const bool just_rej = s.flags & kJustRej;
+    double factor;
+    if (M == kDopri5Compat) {
+        factor = have_prev ? 0.9 * pow(C.eps / eff, 0.7 / 5.0) * pow(s.err_prev / C.eps, 0.4 / 5.0)
+                           : 0.9 * pow(C.eps / eff, 0.2);
+        s.h = clampd(ah * clampd(factor, 0.2, just_rej ? 2.0 : 5.0), 1e-10, fmax(hmax, 1e-10));
+    } else {
+        if (!C.scaled)
+            factor = have_prev ? 0.9 * pow(C.eps / eff, 0.7 / order) * pow(s.err_prev / C.eps, 0.4 / order)
+                               : 0.9 * pow(C.eps / eff, inv_order);
+        else
+            factor = have_prev ? 0.9 * pow(1.0 / eff, 0.7 / order) * pow(s.err_prev, 0.4 / order)
+                               : 0.9 * pow(eff, -inv_order);
+        const double mgb = fmin(1.0 + 4.0 * (5.0 / order), 5.0);
+        s.h = clampd(ah * clampd(factor, 0.2, just_rej ? fmin(mgb, 2.0) : mgb), hmin, hmax);
+    }
+    s.err_prev = en;
+    s.flags = (s.flags | kHavePrev) & ~kJustRej;
+    if (A.force.ground_check) {
+        double bs[6];
+        baseline_state(baseline_new(s.cur), s.t - s.ct0, bs);
+        const double alt = geodetic_altitude_km(bs[0] + s.y[0], bs[1] + s.y[1], bs[2] + s.y[2], A.force.earth_radius);
+        if (!(alt >= kGroundAltitudeKm)) {
+            traj_fail(A, s, traj, kGround);
+            return;
+        }
+    }
+    if (s.t == s.seg_tf) {
+        // rectification (integrator.rs:941-979)
+        const double dsq = fma(s.y[0], s.y[0], fma(s.y[1], s.y[1], s.y[2] * s.y[2]));
+        if (dsq > kRebaseKm * kRebaseKm || s.seg_tf != s.tf) {
+            double bs[6], e[6], ne[6];
+            baseline_state(baseline_new(s.cur), s.seg_tf - s.ct0, bs);
+            for (int i = 0; i < 6; ++i) e[i] = bs[i] + s.y[i];
+            if (!eci_to_equinoctial(e, ne)) {
+                traj_fail(A, s, traj, kRebaseFailed);
+                return;
+            }
+            for (int i = 0; i < 6; ++i) s.cur[i] = ne[i];
+            s.ct0 = s.seg_tf;
+            s.flags |= kHad;
+            s.phase = kNeedSegment;
+        } else {
+            traj_finish_with(A, s, traj, s.y);
+        }
+    }
+}
+
+}  // namespace bqp

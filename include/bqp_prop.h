@@ -85,9 +85,17 @@ typedef struct bqp_force_config {
     double jb_drivers[9];   /* F10.7, F10.7bar, S10, S10bar, M10, M10bar, Y10, Y10bar, dTc (K) */
     int64_t max_steps;      /* per rectification segment (MAX_STEPS = 500000) */
     int64_t max_attempts;   /* device watchdog: step attempts per trajectory */
-    double max_kernel_seconds; /* device watchdog: wall-clock limit of one launch (0: none);
+    double max_kernel_seconds; /* watchdog: wall-clock limit of one propagation call (> 0);
                                   rows not finished by then end with BQP_ST_WATCHDOG */
+    int32_t engine;            /* BQP_ENGINE_* */
+    int32_t gravity_threads;   /* threads per CTA of the gravity kernel (0: 512) */
 } bqp_force_config;
+
+/* propagation engines */
+#define BQP_ENGINE_PIPELINE 0   /* stage-synchronous: prep / gravity / drag / control kernels,
+                                   CUDA-graph replay, active-list compaction */
+#define BQP_ENGINE_PERSISTENT 1 /* one persistent kernel, one trajectory per thread, device
+                                   work queue */
 
 typedef struct bqp_ctx bqp_ctx;
 

@@ -26,9 +26,13 @@ def h(s):
     return struct.unpack(">d", bytes.fromhex(s[2:]))[0]
 
 
+ENGINES = ["pipeline", "persistent"]
+
+
 def ctx_for(text, order, flags=0, method="dop853", eps=1e-8, dt_max=300.0, rtol=None, atol=None,
-            am=0.01, cd=2.2, ground=False, max_attempts=None):
+            am=0.01, cd=2.2, ground=False, max_attempts=None, engine="pipeline"):
     cfg = N.default_config()
+    cfg.engine = N.ENGINES[engine]
     cfg.order = order
     cfg.force_flags = flags
     cfg.method = N.METHODS[method]
@@ -127,12 +131,13 @@ def test_encke_rhs_matches_oracle(flags):
 
 
 # -------------------------------------------------------------- trajectories
-def test_fixed_step_dop853_matches_oracle():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_fixed_step_dop853_matches_oracle(engine):
     """Constant steps (every step accepted): |dr| <= 1e-9 relative."""
     order = 20
     text = workloads.synthetic_field(order)
     h_fixed = 30.0
-    ctx = ctx_for(text, order, flags=1 | 4 | 8, eps=1e30, dt_max=h_fixed)
+    ctx = ctx_for(text, order, flags=1 | 4 | 8, eps=1e30, dt_max=h_fixed, engine=engine)
     F = oracle_force(text, order, 1 | 4 | 8)
     n = 32
     states = workloads.leo_states(n, seed=21)
@@ -151,14 +156,15 @@ def test_fixed_step_dop853_matches_oracle():
         assert rel <= 1e-9, (i, rel)
 
 
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("method,eps", [("dop853", 1e-10), ("dopri5_solver", 1e-9), ("dopri5", 1e-9)])
-def test_adaptive_final_matches_oracle(method, eps):
+def test_adaptive_final_matches_oracle(method, eps, engine):
     """Adaptive trajectories within the integrator tolerance (70x70 + drag +
     Sun/Moon, one and a half orbits with rectification)."""
     order = 70
     text = workloads.synthetic_field(order)
     flags = 1 | 4 | 8
-    ctx = ctx_for(text, order, flags=flags, method=method, eps=eps)
+    ctx = ctx_for(text, order, flags=flags, method=method, eps=eps, engine=engine)
     F = oracle_force(text, order, flags)
     n = 24
     states = workloads.leo_states(n, seed=31)
@@ -177,11 +183,12 @@ def test_adaptive_final_matches_oracle(method, eps):
     assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
 
 
-def test_sampled_dopri5_scaled_matches_oracle():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_sampled_dopri5_scaled_matches_oracle(engine):
     """The C1 form: DOPRI5(4), rtol 1e-10 / atol 1e-9 km, 60 s grid."""
     order = 20
     text = workloads.synthetic_field(order)
-    ctx = ctx_for(text, order, flags=0, method="dopri5_solver", rtol=1e-10, atol=1e-9)
+    ctx = ctx_for(text, order, flags=0, method="dopri5_solver", rtol=1e-10, atol=1e-9, engine=engine)
     F = oracle_force(text, order, 0)
     n = 8
     states = workloads.leo_states(n, seed=0)
@@ -201,10 +208,37 @@ def test_sampled_dopri5_scaled_matches_oracle():
         assert np.allclose(got[i, 0], base[0], atol=1e-9)
 
 
-def test_sampled_deltas_against_initial_baseline():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_sampled_dop853_dense_matches_oracle(engine):
+    """DOP853 samples use an extra force call at each accepted step's end
+    (the reference's dense k1, solver.rs:1672-1676); 70x70 + drag + Sun/Moon."""
+    order = 70
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    ctx = ctx_for(text, order, flags=flags, method="dop853", eps=1e-10, engine=engine)
+    F = oracle_force(text, order, flags)
+    n = 6
+    states = workloads.leo_states(n, seed=7)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 6500.0
+    grid = np.concatenate([np.arange(0.0, tf, 97.0), [tf]])
+    got, st, steps, evals = ctx.propagate_sampled(states, EPOCH, tf, grid)
+    assert (st == 0).all()
+    for i in range(n):
+        d, rs, ref_steps, ref_evals, nw = O.propagate_sampled(F, O.ctrl("dop853", eps=1e-10), equ[i], EPOCH, tf,
+                                                              0.01, 2.2, grid)
+        assert rs == 0 and nw == grid.size
+        base = np.array([O.equinoc2eci(equ[i], t)[0] for t in grid])
+        err = np.linalg.norm(got[i, :, :3] - (base + d)[:, :3], axis=1)
+        assert err.max() <= max(steps[i], 1) * 1e-9, (i, err.max())
+        assert abs(evals[i] - ref_evals) <= max(13 * 3, 0.05 * ref_evals)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_sampled_deltas_against_initial_baseline(engine):
     order = 10
     text = workloads.synthetic_field(order)
-    ctx = ctx_for(text, order, flags=0, method="dop853", eps=1e-10)
+    ctx = ctx_for(text, order, flags=0, method="dop853", eps=1e-10, engine=engine)
     states = workloads.leo_states(4, seed=4)
     equ, _ = N.eci_to_equinoctial(states)
     grid = np.linspace(0.0, 12000.0, 41)
@@ -218,8 +252,9 @@ def test_sampled_deltas_against_initial_baseline():
 
 
 # ----------------------------------------------------------- failure handling
-def test_invalid_rows_are_nan_filled_with_status():
-    ctx = ctx_for(workloads.synthetic_field(8), 8)
+@pytest.mark.parametrize("engine", ENGINES)
+def test_invalid_rows_are_nan_filled_with_status(engine):
+    ctx = ctx_for(workloads.synthetic_field(8), 8, engine=engine)
     states = workloads.leo_states(4, seed=9)
     states[1] = [7000.0, 0.0, 0.0, 0.0, 12.0, 0.0]  # unbound
     states[2, 0] = np.nan
@@ -232,18 +267,38 @@ def test_invalid_rows_are_nan_filled_with_status():
 def test_ground_impact_is_reported():
     # dust_transfer/tests_smoke.py:30-34: the impacting arc raises ValueError
     eci = api.kep_to_eci([6600.0, 0.05, 30.0, 0.0, 0.0, 0.0])
-    with pytest.raises(ValueError, match="ground"):
+    with pytest.raises(ValueError, match="physically infeasible"):
         api.propagate_final(eci, EPOCH, 6000.0, srp=False, method="dop853")
 
 
-def test_device_watchdog_stops_runaway_rows():
-    ctx = ctx_for(workloads.synthetic_field(8), 8, flags=0, eps=1e-10, max_attempts=5)
+@pytest.mark.parametrize("engine", ENGINES)
+def test_device_watchdog_stops_runaway_rows(engine):
+    ctx = ctx_for(workloads.synthetic_field(8), 8, flags=0, eps=1e-10, max_attempts=5, engine=engine)
     states = workloads.leo_states(3, seed=1)
     out, st, _, _ = ctx.propagate_final(states, EPOCH, 5000.0)
     assert (st == 10).all() and np.isnan(out).all()
 
 
 # ------------------------------------------------------------ Python surface
+def test_engines_agree_on_70x70_drag_batch():
+    """The two engines run the same controller: identical inputs give results
+    equal to the last bits of the force sums (the order of FP operations in
+    the force call differs only by kernel boundaries)."""
+    order = 70
+    text = workloads.synthetic_field(order)
+    n = 512
+    states = workloads.leo_states(n, seed=12)
+    bal = workloads.leo_ballistics(n, seed=12)
+    outs = []
+    for engine in ENGINES:
+        ctx = ctx_for(text, order, flags=1 | 4 | 8, eps=1e-12, engine=engine)
+        out, st, steps, evals = ctx.propagate_final(states, EPOCH, 5400.0, ballistic=bal)
+        assert (st == 0).all()
+        outs.append((out, steps, evals))
+    assert np.abs(outs[0][0][:, :3] - outs[1][0][:, :3]).max() < 1e-6
+    assert np.abs(outs[0][1] - outs[1][1]).max() <= 0.05 * outs[1][1].max()
+
+
 def test_reference_smoke_sequence():
     """dust_transfer/tests_smoke.py, with srp=False and a built stepper."""
     kep = np.array([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0])
