@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--segment", type=float, default=SEGMENT_S,
                     help="seconds propagated per step (5400 = one Encke segment; smaller for profiling)")
     ap.add_argument("--engine", default="pipeline", choices=["pipeline", "persistent"])
-    ap.add_argument("--gravity-threads", type=int, default=512)
+    ap.add_argument("--gravity-threads", type=int, default=256)
     return ap.parse_args()
 
 
@@ -138,7 +138,7 @@ def make_workload(n: int, seed: int = 0):
     return W.synthetic_field(ORDER), states, bal, W.EPOCH_JD
 
 
-def make_config(engine="pipeline", gravity_threads=512):
+def make_config(engine="pipeline", gravity_threads=256):
     from bqp_b200 import _native as N
 
     cfg = N.default_config()

@@ -498,7 +498,7 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->max_attempts = (int64_t)1 << 40;
     c->max_kernel_seconds = 600.0;
     c->engine = BQP_ENGINE_PIPELINE;
-    c->gravity_threads = 512;
+    c->gravity_threads = 256;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }

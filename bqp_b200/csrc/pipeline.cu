@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
             if (T::FSAL) {
                 for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S - 1, i)[slot];
                 dy_next = dyn;
-            } else if (dense) {
+            } else if (dense && (s.flags & kSegSampled)) {
                 for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S, i)[slot];
                 dy_next = dyn;
                 ++s.evals;  // counted on accept only, as the reference evaluates it

@@ -79,8 +79,6 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
     using T = Tab<M>;
     constexpr int S = T::S;
     const double* tab = stage_table(A.gtab, A.ncells, A.use_smem != 0);
-    const bool sampled = sampled_mode(A);
-
     Encke R;
     R.tab = tab;
     R.fp = &A.force;
@@ -167,7 +165,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
             const double* dy_next = nullptr;
             if (T::FSAL) {
                 dy_next = k + (S - 1) * 6;
-            } else if (sampled) {
+            } else if (s.flags & kSegSampled) {
                 R.eval(next_time(s), ynext, dyn);  // the reference's dense k1 (solver.rs:1672-1676)
                 ++s.evals;
                 dy_next = dyn;

@@ -49,10 +49,10 @@ struct Tab<kDop853> {
 
 enum OutMode : int32_t { kOutFinalEci = 0, kOutSampledEci = 1, kOutSampledDelta = 2 };
 enum Phase : int32_t { kNeedTraj = 0, kNeedSegment = 1, kStepping = 2, kDone = 3, kFinished = 4 };
-enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16 };
+enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16, kSegSampled = 32 };
 
 struct TrajState {
-    double tf, ct0, seg_tf, t, h, err_prev, t_comp, hs;
+    double tf, ct0, seg_tf, t, h, err_prev, t_comp, hs, hcarry;
     double jd0, am, cd;
     double cur[6], equ0[6], y[6], k1c[6];
     int32_t flags, rejects, s_idx, phase, status;
@@ -143,6 +143,7 @@ static __device__ __noinline__ void traj_begin(const PropArgs& A, TrajState& s, 
     s.steps = s.evals = s.attempts = s.restarts = 0;
     s.seg_steps = 0;
     s.flags = 0;
+    s.hcarry = 0.0;
     s.rejects = 0;
     s.s_idx = 0;
     s.status = kOk;
@@ -203,13 +204,22 @@ __device__ __noinline__ void seg_begin(const PropArgs& A, TrajState& s, int64_t 
         for (int i = 0; i < 6; ++i) s.y[i] = 0.0;
         double hmax = fabs(A.ctrl.h_max);
         if (!isfinite(hmax) || hmax <= 0.0) hmax = span;
+        // A segment holding samples runs the reference's sampled solver
+        // (integrate_segment_with_method: dense first-stage reuse, and the
+        // previous sampled segment's final step as h0 when dt_max > 60 s,
+        // integrator.rs:187-216); one without samples runs the final-state
+        // solver (integrate_final_no_events_with_rhs, h0 = None).
+        const bool seg_sampled = sampled_mode(A) && s.s_idx < A.n_t && A.t_eval[s.s_idx] <= s.seg_tf + 1e-9;
         if (M == kDopri5Compat)
             s.h = clampd(fabs((s.seg_tf - s.ct0) / 100.0), 1e-3, fmax(fmax(hmax, 1e-10), 1e-3));
+        else if (seg_sampled && s.hcarry > 0.0 && A.ctrl.h_max > 60.0)
+            s.h = clampd(s.hcarry, A.ctrl.h_min, hmax);
         else
             s.h = clampd(span <= 60.0 ? span / 2.0 : span / 100.0, A.ctrl.h_min, hmax);
         s.err_prev = 0.0;
         s.t_comp = 0.0;
         s.flags &= kHad;  // clear controller memory and the reusable first stage
+        if (seg_sampled) s.flags |= kSegSampled;
         s.rejects = 0;
         s.seg_steps = 0;
         s.phase = kStepping;
@@ -428,7 +438,7 @@ __device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int
             ++s.s_idx;
         }
     }
-    if (T::FSAL || sampled_mode(A)) {
+    if (T::FSAL || (s.flags & kSegSampled)) {
         for (int i = 0; i < 6; ++i) s.k1c[i] = dy_next[i];
         s.flags |= kHaveK1;
     } else {
@@ -457,6 +467,8 @@ __device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int
     }
     s.err_prev = en;
     s.flags = (s.flags | kHavePrev) & ~kJustRej;
+    if ((s.flags & kSegSampled) && s.t == s.seg_tf && M != kDopri5Compat && A.ctrl.h_max > 60.0 && s.h > 0.0)
+        s.hcarry = s.h;  // hcarry_store (integrator.rs:206-216)
     if (A.force.ground_check) {
         double bs[6];
         baseline_state(baseline_new(s.cur), s.t - s.ct0, bs);

@@ -1257,7 +1257,7 @@ int integrate(Rhs& R, const Ctrl& C, const double y0[6], double t0, double tf, d
 // lightyear_compat.rs: the DOPRI5 compatibility loop (final-state form,
 // fast_single = true, no events).
 int integrate_compat(Rhs& R, const Ctrl& C, const double y0[6], double t0, double tf,
-                     double y[6], Stats& st) {
+                     double y[6], Stats& st, Samples* smp = nullptr) {
     Tab T = tableau(METHOD_DOPRI5);
     double eps = std::max(C.eps, 1e-12);
     double dir = tf >= t0 ? 1.0 : -1.0;
@@ -1277,6 +1277,11 @@ int integrate_compat(Rhs& R, const Ctrl& C, const double y0[6], double t0, doubl
     bool have_prev = false, just_rej = false;
     double t_comp = 0.0;
     double ynext[6], err[6], err3[6];
+    if (smp)
+        while (smp->idx < smp->n && smp->t[smp->idx] == t) {
+            for (int i = 0; i < 6; ++i) smp->out[smp->idx * 6 + i] = y[i];
+            smp->idx++;
+        }
     while (tf != t && ((tf - t) > 0 ? 1.0 : -1.0) == dir) {
         if (st.steps >= C.max_steps) return ST_MAX_STEPS;
         double rem = tf - t;
@@ -1312,6 +1317,26 @@ int integrate_compat(Rhs& R, const Ctrl& C, const double y0[6], double t0, doubl
             }
             if (!std::isfinite(tn)) return ST_NON_FINITE;
             rejects = 0;
+            if (smp) {
+                const double* dn = &k[(T.s - 1) * 6];
+                while (smp->idx < smp->n) {
+                    double ts = smp->t[smp->idx];
+                    if (dir * (ts - tn) > 0.0) break;
+                    double* o = smp->out + smp->idx * 6;
+                    if (ts == tn) {
+                        for (int i = 0; i < 6; ++i) o[i] = ynext[i];
+                    } else {
+                        double hd = tn - t;
+                        double tau = std::min(std::max((ts - t) / hd, 0.0), 1.0);
+                        double t2 = tau * tau, t3 = t2 * tau;
+                        double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
+                        double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+                        for (int i = 0; i < 6; ++i)
+                            o[i] = h00 * y[i] + h10 * hd * dy[i] + h01 * ynext[i] + h11 * hd * dn[i];
+                    }
+                    smp->idx++;
+                }
+            }
             for (int i = 0; i < 6; ++i) {
                 y[i] = ynext[i];
                 dy[i] = k[(T.s - 1) * 6 + i];
@@ -1463,7 +1488,10 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
         double y0[6] = {0, 0, 0, 0, 0, 0}, d[6];
         Stats seg;
         double fh = 0.0;
-        double carry = (seg_i > 0 && J.C.h_max > 60.0) ? hcarry : 0.0;
+        // sampled segments take the previous sampled segment's final step
+        // (hcarry, integrator.rs:187-216); unsampled ones run the final-state
+        // solver with h0 = None and do not touch the carry
+        double carry = (cnt > 0 && J.C.h_max > 60.0) ? hcarry : 0.0;
         int s;
         std::vector<double> buf;
         if (cnt > 0) {
@@ -1479,7 +1507,10 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
             sm.t = te.data();
             sm.n = (int)te.size();
             sm.out = buf.data();
-            s = integrate(R, J.C, y0, ct0, seg_tf, d, seg, &fh, &sm, carry);
+            if (J.C.method == METHOD_DOPRI5_COMPAT)
+                s = integrate_compat(R, J.C, y0, ct0, seg_tf, d, seg, &sm);
+            else
+                s = integrate(R, J.C, y0, ct0, seg_tf, d, seg, &fh, &sm, carry);
             st.steps += seg.steps;
             st.evals += seg.evals;
             st.rejects += seg.rejects;
@@ -1498,7 +1529,10 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
             }
             for (int q = 0; q < 6; ++q) d[q] = buf[(te.size() - 1) * 6 + q];
         } else {
-            s = integrate(R, J.C, y0, ct0, seg_tf, d, seg, &fh, nullptr, carry);
+            if (J.C.method == METHOD_DOPRI5_COMPAT)
+                s = integrate_compat(R, J.C, y0, ct0, seg_tf, d, seg);
+            else
+                s = integrate(R, J.C, y0, ct0, seg_tf, d, seg, nullptr, nullptr, 0.0);
             st.steps += seg.steps;
             st.evals += seg.evals;
             st.rejects += seg.rejects;
@@ -1508,7 +1542,7 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
                 return s;
             }
         }
-        if (J.C.h_max > 60.0 && fh > 0.0) hcarry = fh;
+        if (cnt > 0 && J.C.h_max > 60.0 && fh > 0.0) hcarry = fh;
         consumed += cnt;
         *n_written = consumed;
         double dsq = std::fma(d[0], d[0], std::fma(d[1], d[1], d[2] * d[2]));

@@ -235,6 +235,30 @@ def test_sampled_dop853_dense_matches_oracle(engine):
 
 
 @pytest.mark.parametrize("engine", ENGINES)
+def test_sampled_compat_loop_matches_oracle(engine):
+    """Python method="dopri5" (the DOPRI5 compatibility loop) on the sampled path."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    ctx = ctx_for(text, order, flags=flags, method="dopri5", eps=1e-9, engine=engine)
+    F = oracle_force(text, order, flags)
+    n = 4
+    states = workloads.leo_states(n, seed=17)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 7000.0
+    grid = np.concatenate([np.arange(0.0, tf, 300.0), [tf]])
+    got, st, steps, evals = ctx.propagate_sampled(states, EPOCH, tf, grid)
+    assert (st == 0).all()
+    for i in range(n):
+        d, rs, ref_steps, ref_evals, nw = O.propagate_sampled(F, O.ctrl("dopri5", eps=1e-9), equ[i], EPOCH, tf,
+                                                              0.01, 2.2, grid)
+        assert rs == 0 and nw == grid.size
+        base = np.array([O.equinoc2eci(equ[i], t)[0] for t in grid])
+        err = np.linalg.norm(got[i, :, :3] - (base + d)[:, :3], axis=1)
+        assert err.max() <= max(steps[i], 1) * 1e-8, (i, err.max())
+
+
+@pytest.mark.parametrize("engine", ENGINES)
 def test_sampled_deltas_against_initial_baseline(engine):
     order = 10
     text = workloads.synthetic_field(order)
