@@ -45,6 +45,7 @@ class ForceConfig(C.Structure):
         ("omega_earth", C.c_double), ("mu_sun", C.c_double), ("mu_moon", C.c_double),
         ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
         ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
+        ("gravity_slots", C.c_int32), ("reserved0", C.c_int32),
     ]
 
 

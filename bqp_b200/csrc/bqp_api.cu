@@ -227,6 +227,8 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_ARG, "unknown engine %d", c->engine);
     if (c->gravity_threads < 0 || c->gravity_threads > 1024 || c->gravity_threads % 32)
         return fail(BQP_E_ARG, "gravity_threads must be a multiple of 32 in 0..1024");
+    if (c->gravity_slots != 0 && c->gravity_slots != 1 && c->gravity_slots != 2 && c->gravity_slots != 4)
+        return fail(BQP_E_ARG, "gravity_slots must be 0, 1, 2 or 4");
     return 0;
 }
 
@@ -355,7 +357,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
         PipeBufs P{};
         pipeline_carve(P, ctx->d_pws, n);
         cudaError_t e = launch_pipeline(A, P, ctx->cfg.method, ctx->stream, ctx->cfg.max_kernel_seconds,
-                                        ctx->cfg.gravity_threads);
+                                        ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
         if (e != cudaSuccess) return cuda_fail(e, "pipeline");
         return 0;
     }
@@ -499,6 +501,7 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->max_kernel_seconds = 600.0;
     c->engine = BQP_ENGINE_PIPELINE;
     c->gravity_threads = 256;
+    c->gravity_slots = 2;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -586,7 +589,7 @@ int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* pos, double* 
     int rc = set_device(ctx);
     if (rc) return rc;
     cudaError_t e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, pos, acc,
-                                   status, ctx->stream);
+                                   status, ctx->stream, ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
     return e == cudaSuccess ? 0 : cuda_fail(e, "k_gravity launch");
 }
 
@@ -608,7 +611,8 @@ int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, in
     }
     cudaError_t e = cudaMemcpyAsync(dp, pos, b3, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
-        e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, dp, da, ds, ctx->stream);
+        e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, dp, da, ds, ctx->stream,
+                           ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
     if (e == cudaSuccess) e = cudaMemcpyAsync(acc, da, b3, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && status)
         e = cudaMemcpyAsync(status, ds, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream);

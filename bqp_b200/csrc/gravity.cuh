@@ -94,4 +94,104 @@ BQP_HD void gravity_field(const double* __restrict__ tab, int order, double px, 
     acc[2] = az;
 }
 
+// NT trajectories per thread: every table read (four 16-byte broadcast loads
+// per cell) feeds NT independent recursions, which divides the shared-memory
+// traffic per trajectory by NT and gives the FP64 pipe NT-way ILP.
+template <int NT>
+BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const double* px,
+                                                    const double* py, const double* pz, double (*acc)[3]) {
+    double xc[NT], yc[NT], zc[NT], c2re[NT], vd[NT], wd[NT], ax[NT], ay[NT], az[NT];
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+        const double r2 = fma(px[q], px[q], fma(py[q], py[q], pz[q] * pz[q]));
+        const double c2 = kReGravity / r2;
+        xc[q] = px[q] * c2;
+        yc[q] = py[q] * c2;
+        zc[q] = pz[q] * c2;
+        c2re[q] = c2 * kReGravity;
+        vd[q] = sqrt(c2re[q]);
+        wd[q] = 0.0;
+        ax[q] = ay[q] = az[q] = 0.0;
+    }
+    const int last = order + 1;
+    const double2* cell = reinterpret_cast<const double2*>(tab);
+    for (int j = 0; j <= last; ++j) {
+        {
+            const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                if (j > 0) {
+                    const double nv = ab.x * fma(xc[q], vd[q], -yc[q] * wd[q]);
+                    const double nw = ab.x * fma(xc[q], wd[q], yc[q] * vd[q]);
+                    vd[q] = nv;
+                    wd[q] = nw;
+                }
+                ax[q] = fma(wx.x, vd[q], fma(wx.y, wd[q], ax[q]));
+                ay[q] = fma(wy.x, vd[q], fma(wy.y, wd[q], ay[q]));
+                az[q] = fma(wz.x, vd[q], fma(wz.y, wd[q], az[q]));
+            }
+            cell += 4;
+        }
+        if (j == last) break;
+        double v0[NT], w0[NT], v1[NT], w1[NT];
+        {
+            const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const double a = ab.x * zc[q];
+                v0[q] = vd[q];
+                w0[q] = wd[q];
+                v1[q] = a * vd[q];
+                w1[q] = a * wd[q];
+                ax[q] = fma(wx.x, v1[q], fma(wx.y, w1[q], ax[q]));
+                ay[q] = fma(wy.x, v1[q], fma(wy.y, w1[q], ay[q]));
+                az[q] = fma(wz.x, v1[q], fma(wz.y, w1[q], az[q]));
+            }
+            cell += 4;
+        }
+        // interior rows, two per iteration so the row registers rotate
+        // without moves
+        int l = j + 2;
+        for (; l + 1 <= last; l += 2) {
+            const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
+            const double2 ab2 = cell[4], wx2 = cell[5], wy2 = cell[6], wz2 = cell[7];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const double ta = ab.x * zc[q], tb = ab.y * c2re[q];
+                v0[q] = fma(ta, v1[q], -tb * v0[q]);
+                w0[q] = fma(ta, w1[q], -tb * w0[q]);
+                ax[q] = fma(wx.x, v0[q], fma(wx.y, w0[q], ax[q]));
+                ay[q] = fma(wy.x, v0[q], fma(wy.y, w0[q], ay[q]));
+                az[q] = fma(wz.x, v0[q], fma(wz.y, w0[q], az[q]));
+                const double ta2 = ab2.x * zc[q], tb2 = ab2.y * c2re[q];
+                v1[q] = fma(ta2, v0[q], -tb2 * v1[q]);
+                w1[q] = fma(ta2, w0[q], -tb2 * w1[q]);
+                ax[q] = fma(wx2.x, v1[q], fma(wx2.y, w1[q], ax[q]));
+                ay[q] = fma(wy2.x, v1[q], fma(wy2.y, w1[q], ay[q]));
+                az[q] = fma(wz2.x, v1[q], fma(wz2.y, w1[q], az[q]));
+            }
+            cell += 8;
+        }
+        if (l <= last) {
+            const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const double ta = ab.x * zc[q], tb = ab.y * c2re[q];
+                const double v2 = fma(ta, v1[q], -tb * v0[q]);
+                const double w2 = fma(ta, w1[q], -tb * w0[q]);
+                ax[q] = fma(wx.x, v2, fma(wx.y, w2, ax[q]));
+                ay[q] = fma(wy.x, v2, fma(wy.y, w2, ay[q]));
+                az[q] = fma(wz.x, v2, fma(wz.y, w2, az[q]));
+            }
+            cell += 4;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+        acc[q][0] = ax[q];
+        acc[q][1] = ay[q];
+        acc[q][2] = az[q];
+    }
+}
+
 }  // namespace bqp

@@ -337,5 +337,220 @@ BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat,
     return out;
 }
 
+#ifdef __CUDACC__
+// ------------------------------------------------------------------------
+// Lane-group form for the drag kernel: the density of one state is computed
+// by a group of L consecutive lanes.  Every lane walks the same log-spaced
+// interval chain (bit-identical node positions); lane q evaluates the Boole
+// nodes of intervals i = q (mod L), including the node carried in from
+// interval i-1, recomputed -- the same function at the same altitude, so the
+// same value.  Partial sums meet in a group-masked shuffle.  All lanes of a
+// group hold the same inputs, so they branch together.
+struct SweepG {
+    double sum, z, zend, tloc, gravl, mb, ain;
+};
+
+BQP_HD double node_ain(double z, const double* tc, bool with_mbar, double* tloc, double* gravl, double* mb) {
+    *tloc = local_temp(z, tc);
+    *gravl = grav(z);
+    if (with_mbar) {
+        *mb = mbar(z);
+        return *mb * *gravl / *tloc;
+    }
+    return *gravl / *tloc;
+}
+
+template <int L>
+__device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr, int n, double ain0,
+                                                    bool with_mbar, const double* tc, int q, unsigned gmask) {
+    SweepG s;
+    double part = 0.0;
+    double zend = zend_start, zlast = zend_start;  // zlast: last node of the previous interval
+    double tl = 0.0, gl = 0.0, mb = 0.0, ain_last = ain0;
+    for (int i = 0; i < n; ++i) {
+        double zz = zend;
+        zend = zr * zz;
+        const double dz = 0.25 * (zend - zz);
+        if ((i % L) == q) {
+            double t_, g_, m_;
+            const double carry = i == 0 ? ain0 : node_ain(zlast, tc, with_mbar, &t_, &g_, &m_);
+            double sum1 = kW0 * carry;
+#pragma unroll
+            for (int j = 1; j < 5; ++j) {
+                zz += dz;
+                const double a = node_ain(zz, tc, with_mbar, &tl, &gl, &mb);
+                sum1 += (j == 1 || j == 3 ? kW1 : (j == 2 ? kW2 : kW0)) * a;
+                ain_last = a;
+            }
+            part += dz * sum1;
+        } else {
+            zz += dz;
+            zz += dz;
+            zz += dz;
+            zz += dz;
+        }
+        zlast = zz;
+    }
+    // group reduction and the last interval's node values from its owner
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) part += __shfl_xor_sync(gmask, part, off, L);
+    const int owner = n > 0 ? (n - 1) % L : 0;
+    s.sum = part;
+    s.z = zlast;
+    s.zend = zend;
+    s.tloc = __shfl_sync(gmask, tl, owner, L);
+    s.gravl = __shfl_sync(gmask, gl, owner, L);
+    s.mb = __shfl_sync(gmask, mb, owner, L);
+    s.ain = __shfl_sync(gmask, ain_last, owner, L);
+    return s;
+}
+
+// density() evaluated by a group of L lanes (q = lane within the group,
+// gmask = the group's lanes).  Same inputs, same error codes.
+template <int L>
+__device__ double density_group(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
+                                const Drivers& d, int q, unsigned gmask) {
+    double code = 0.0;
+    if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) || !isfinite(alt_m) ||
+        !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) || !isfinite(d.s10b) || !isfinite(d.m10) ||
+        !isfinite(d.m10b) || !isfinite(d.y10) || !isfinite(d.y10b) || !isfinite(d.dtc))
+        code = kErrNonFinite;
+    else if (alt_m < 90000.0)
+        code = kErrAltitude;
+    else if (!(sun_dec >= -kPi / 2 && sun_dec <= kPi / 2) || !(lat >= -kPi / 2 && lat <= kPi / 2))
+        code = kErrAngle;
+    else if (d.f10 <= 0.0 || d.f10b <= 0.0 || d.s10 <= 0.0 || d.s10b <= 0.0 || d.m10 <= 0.0 || d.m10b <= 0.0 ||
+             d.y10 <= 0.0 || d.y10b <= 0.0)
+        code = kErrIndex;
+    if (code != 0.0) return code;  // the whole group returns together
+    const double alt = alt_m / 1000.0;
+    const double fn = fmin(pow(d.f10b / 240.0, 0.25), 1.0);
+    const double fsb = d.f10b * fn + d.s10b * (1.0 - fn);
+    const double tsubc = 392.4 + 3.227 * fsb + 0.298 * (d.f10 - d.f10b) + 2.259 * (d.s10 - d.s10b) +
+                         0.312 * (d.m10 - d.m10b) + 0.178 * (d.y10 - d.y10b);
+    const double eta = 0.5 * fabs(lat - sun_dec);
+    const double theta = 0.5 * fabs(lat + sun_dec);
+    double h = hour_angle;
+    if (!(h >= 0.0 && h < kTwoPi)) {
+        if (h < 0.0 && h > -kTwoPi) {
+            h += kTwoPi;
+        } else {
+            h = fmod(h, kTwoPi);
+            if (h < 0.0) h += kTwoPi;
+        }
+    }
+    const double tau = h - 0.64577182 + 0.10471976 * sin(h + 0.75049158);
+    double st_hour = ((h + kPi) * (180.0 / kPi)) / 15.0;
+    if (st_hour >= 24.0) st_hour -= 24.0;
+    else if (st_hour < 0.0) st_hour += 24.0;
+    double slat, clat;
+    sincos(lat, &slat, &clat);
+    const double cos_eta = five_halves(cos(eta));
+    const double sin_theta = five_halves(sin(theta));
+    const double cos_tau = fabs(cos(0.5 * tau));
+    const double df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
+    const double tsubl = tsubc * (1.0 + 0.31 * df);
+    const double tinf = tsubl + d.dtc + dtc_correction(d.f10, st_hour, clat, alt);
+    const double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * exp(-0.0021357 * tinf);
+    const double gsubx = 0.054285714 * (tsubx - 183.0);
+    double tc[4];
+    tc[0] = tsubx;
+    tc[1] = gsubx;
+    tc[2] = (tinf - tsubx) / (kPi / 2);
+    tc[3] = gsubx / tc[2];
+    const double z1 = 90.0;
+    double al = log(fmin(alt, 105.0) / z1);
+    int n = 1 + (int)floor(al / kLnStepLower);
+    double zr = exp(al / n);
+    const double mb1 = mbar(z1);
+    const double tloc1 = local_temp(z1, tc);
+    const SweepG lo = boole_sweep_group<L>(z1, zr, n, mb1 * grav(z1) / tloc1, true, tc, q, gmask);
+    const double mb2 = lo.mb, tloc2 = lo.tloc;
+    double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
+    const double anm = kAvogadro * rho;
+    const double an = anm / mb2;
+    double fact2 = anm / 28.960;
+    const double fac[5] = {JBT(kFrac)[0] * fact2, fact2 * (1.0 + JBT(kFrac)[1]) - an, 2.0 * (an - fact2),
+                           JBT(kFrac)[2] * fact2, JBT(kFrac)[3] * fact2};
+    double aln[6];
+    for (int i = 0; i < 5; ++i) aln[i] = fac[i] < 0.0 ? NAN : log(fac[i]);
+    double z = lo.z;
+    if (alt <= 105.0) {
+        aln[5] = aln[4] - 25.0;
+    } else {
+        al = log(fmin(alt, 500.0) / z);
+        n = 1 + (int)floor(al / kLnStepMiddle);
+        zr = exp(al / n);
+        const SweepG mid = boole_sweep_group<L>(lo.zend, zr, n, lo.gravl / tloc2, false, tc, q, gmask);
+        const double tloc3 = mid.tloc;
+        z = mid.z;
+        al = log(fmax(alt, 500.0) / z);
+        n = 1 + (int)floor(al / (alt > 500.0 ? kLnStepUpper : kLnStepMiddle));
+        zr = exp(al / n);
+        const SweepG up = boole_sweep_group<L>(mid.zend, zr, n, mid.ain, false, tc, q, gmask);
+        const double tloc4 = up.tloc;
+        z = up.z;
+        double altr, hsign;
+        if (alt <= 500.0) {
+            altr = log(tloc3 / tloc2);
+            fact2 = mid.sum / kRstar;
+            hsign = 1.0;
+        } else {
+            altr = log(tloc4 / tloc2);
+            fact2 = (mid.sum + up.sum) / kRstar;
+            hsign = -1.0;
+        }
+        for (int i = 0; i < 4; ++i) aln[i] = aln[i] - altr - fact2 * JBT(kAmw)[i];
+        aln[4] = aln[4] - (1.0 - 0.38) * altr - fact2 * JBT(kAmw)[4];
+        const double al10t5 = log10(tinf);
+        const double alnh5 = (5.5 * al10t5 - 39.40) * al10t5 + 73.13;
+        aln[5] = kLn10 * (alnh5 + 6.0) + hsign * (log(tloc4 / tloc3) + up.sum * JBT(kAmw)[5] / kRstar);
+    }
+    const double years = (mjd - 36204.0) / 365.2422;
+    double capphi = years - trunc(years);
+    if (capphi == 0.0) capphi = copysign(0.0, years);
+    const double sgn = lat >= 0.0 ? 1.0 : -1.0;
+    const double hm90 = alt - 90.0;
+    const double dlrsl = 0.02 * hm90 * exp(-0.045 * hm90) * sgn * sin(kTwoPi * capphi + 1.72) * slat * slat;
+    double dlrsa = 0.0;
+    if (z < 2000.0) {
+        bool ok = true;
+        const double day = day_of_year(mjd, &ok);
+        if (!ok) return kErrDomain;
+        const double htz = alt / 1000.0;
+        double fsmb = d.f10b - 0.70 * d.s10b - 0.04 * d.m10b;
+        const double fzz = JBT(kFzm)[0] + JBT(kFzm)[1] * fsmb + JBT(kFzm)[2] * fsmb * htz +
+                           JBT(kFzm)[3] * fsmb * htz * htz + JBT(kFzm)[4] * fsmb * fsmb * htz;
+        fsmb = d.f10b - 0.75 * d.s10b - 0.37 * d.m10b;
+        double s1, c1;
+        sincos(kTwoPi * (day - 1.0) / 365.0, &s1, &c1);
+        const double s2 = 2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
+        const double gtz = JBT(kGtm)[0] + JBT(kGtm)[1] * s1 + JBT(kGtm)[2] * c1 + JBT(kGtm)[3] * s2 +
+                           JBT(kGtm)[4] * c2 + JBT(kGtm)[5] * fsmb + JBT(kGtm)[6] * fsmb * s1 +
+                           JBT(kGtm)[7] * fsmb * c1 + JBT(kGtm)[8] * fsmb * s2 + JBT(kGtm)[9] * fsmb * c2;
+        dlrsa = fmax(fzz, 1.0e-6) * gtz;
+    }
+    const double dlr = kLn10 * (dlrsl + dlrsa);
+    double sumnm = 0.0;
+    for (int i = 0; i < 6; ++i) sumnm += exp(aln[i] + dlr) * JBT(kAmw)[i];
+    rho = sumnm / kAvogadro;
+    double fex = 1.0;
+    if (alt >= 1000.0 && alt < 1500.0) {
+        const double zeta = (alt - 1000.0) * 0.002;
+        const double f15c = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * 1500.0 +
+                            JBT(kCht)[3] * d.f10b * 1500.0;
+        const double f15cz = (JBT(kCht)[2] + JBT(kCht)[3] * d.f10b) * 500.0;
+        const double fex2 = 3.0 * f15c - f15cz - 3.0;
+        const double fex3 = f15cz - 2.0 * f15c + 2.0;
+        fex = 1.0 + zeta * zeta * (fex2 + fex3 * zeta);
+    } else if (alt >= 1500.0) {
+        fex = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * alt + JBT(kCht)[3] * d.f10b * alt;
+    }
+    const double out = rho * fex;
+    if (!(isfinite(out) && out > 0.0)) return kErrDomain;
+    return out;
+}
+#endif  // __CUDACC__
+
 }  // namespace jb
 }  // namespace bqp

@@ -60,10 +60,11 @@ struct PipeBufs {
 size_t pipeline_bytes(int64_t cap);
 void pipeline_carve(PipeBufs& P, void* base, int64_t cap);
 cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st,
-                            double max_seconds, int gravity_threads);
+                            double max_seconds, int gravity_threads, int gravity_slots);
 
 cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
-                           const double* pos, double* acc, int32_t* status, cudaStream_t st);
+                           const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads = 256,
+                           int slots = 2);
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,
                        const double* equ, const double* seg_t0, const double* jd0, const double* t,
                        const double* delta, const double* ballistic, double am0, double cd0,

@@ -235,31 +235,62 @@ BQP_HD void sun_position(double jd, double* out) {
     out[2] = se * (r * sl);
 }
 
+// (sin, cos) pair with angle-addition helpers: the Moon series below needs
+// the sines and cosines of ~30 integer combinations of four fundamental
+// arguments; they are built from the four sincos pairs instead of one
+// transcendental call each.
+struct SC {
+    double s, c;
+};
+BQP_HD SC sc_add(SC a, SC b) { return {fma(a.s, b.c, a.c * b.s), fma(a.c, b.c, -(a.s * b.s))}; }
+BQP_HD SC sc_sub(SC a, SC b) { return {fma(a.s, b.c, -(a.c * b.s)), fma(a.c, b.c, a.s * b.s)}; }
+BQP_HD SC sc_dbl(SC a) { return {2.0 * a.s * a.c, fma(a.c, a.c, -(a.s * a.s))}; }
+BQP_HD SC sc_of(double x) {
+    SC r;
+    sincos(x, &r.s, &r.c);
+    return r;
+}
+
 BQP_HD void moon_position(double jd, double* out) {
     double T = (jd - 2451545.0) / 36525.0;
-    double L0 = mod2pi((218.31617 + 481267.88088 * T - 1.3972 * T) * kDeg);
-    double l = mod2pi((134.96292 + 477198.86753 * T) * kDeg);
-    double lp = mod2pi((357.52543 + 35999.04944 * T) * kDeg);
-    double F = mod2pi((93.27283 + 483202.01873 * T) * kDeg);
-    double D = mod2pi((297.85027 + 445267.11135 * T) * kDeg);
-    double dlam = 22640.0 * sin(l) + 769.0 * sin(2.0 * l) - 4586.0 * sin(l - 2.0 * D) +
-                  2370.0 * sin(2.0 * D) - 668.0 * sin(lp) - 412.0 * sin(2.0 * F) -
-                  212.0 * sin(2.0 * l - 2.0 * D) - 206.0 * sin(l + lp - 2.0 * D) +
-                  192.0 * sin(l + 2.0 * D) - 165.0 * sin(lp - 2.0 * D) + 148.0 * sin(l - lp) -
-                  125.0 * sin(D) - 110.0 * sin(l + lp) - 55.0 * sin(2.0 * F - 2.0 * D);
-    double lam = L0 + dlam * kArcsec;
-    double beta = 18520.0 * sin(F + lam - L0 + (412.0 * sin(2.0 * F) + 541.0 * sin(lp)) * kArcsec) -
-                  526.0 * sin(F - 2.0 * D) + 44.0 * sin(l + F - 2.0 * D) - 31.0 * sin(-l + F - 2.0 * D) -
-                  25.0 * sin(-2.0 * l + F) - 23.0 * sin(lp + F - 2.0 * D) + 21.0 * sin(-l + F) +
-                  11.0 * sin(-lp + F - 2.0 * D);
+    const double L0 = mod2pi((218.31617 + 481267.88088 * T - 1.3972 * T) * kDeg);
+    const SC l = sc_of(mod2pi((134.96292 + 477198.86753 * T) * kDeg));
+    const SC lp = sc_of(mod2pi((357.52543 + 35999.04944 * T) * kDeg));
+    const double Fang = mod2pi((93.27283 + 483202.01873 * T) * kDeg);
+    const SC F = sc_of(Fang);
+    const SC D = sc_of(mod2pi((297.85027 + 445267.11135 * T) * kDeg));
+    const SC l2 = sc_dbl(l), D2 = sc_dbl(D), F2 = sc_dbl(F);
+    const SC l_2D = sc_sub(l, D2);          // l - 2D
+    const SC l2_2D = sc_sub(l2, D2);        // 2l - 2D
+    const SC llp_2D = sc_add(l_2D, lp);     // l + l' - 2D
+    const SC lp2D = sc_add(l, D2);          // l + 2D
+    const SC lp_2D = sc_sub(lp, D2);        // l' - 2D
+    const SC l_lp = sc_sub(l, lp);          // l - l'
+    const SC llp = sc_add(l, lp);           // l + l'
+    const SC F2_2D = sc_sub(F2, D2);        // 2F - 2D
+    const SC F_2D = sc_sub(F, D2);          // F - 2D
+    const double dlam = 22640.0 * l.s + 769.0 * l2.s - 4586.0 * l_2D.s + 2370.0 * D2.s - 668.0 * lp.s -
+                        412.0 * F2.s - 212.0 * l2_2D.s - 206.0 * llp_2D.s + 192.0 * lp2D.s - 165.0 * lp_2D.s +
+                        148.0 * l_lp.s - 125.0 * D.s - 110.0 * llp.s - 55.0 * F2_2D.s;
+    const double lam = L0 + dlam * kArcsec;
+    // argument of the main latitude term: F + (lam - L0) + (412 sin 2F + 541 sin l')"
+    const double argF = Fang + dlam * kArcsec + (412.0 * F2.s + 541.0 * lp.s) * kArcsec;
+    const SC lF_2D = sc_add(l_2D, F);       // l + F - 2D
+    const SC mlF_2D = sc_sub(F_2D, l);      // -l + F - 2D
+    const SC m2lF = sc_sub(F, l2);          // -2l + F
+    const SC lpF_2D = sc_add(F_2D, lp);     // l' + F - 2D
+    const SC mlF = sc_sub(F, l);            // -l + F
+    const SC mlpF_2D = sc_sub(F_2D, lp);    // -l' + F - 2D
+    double beta = 18520.0 * sin(argF) - 526.0 * F_2D.s + 44.0 * lF_2D.s - 31.0 * mlF_2D.s - 25.0 * m2lF.s -
+                  23.0 * lpF_2D.s + 21.0 * mlF.s + 11.0 * mlpF_2D.s;
     beta *= kArcsec;
-    double r = 385000.0 - 20905.0 * cos(l) - 3699.0 * cos(2.0 * D - l) - 2956.0 * cos(2.0 * D) -
-               570.0 * cos(2.0 * l) + 246.0 * cos(2.0 * l - 2.0 * D) - 205.0 * cos(lp - 2.0 * D) -
-               171.0 * cos(l + 2.0 * D) - 152.0 * cos(l + lp - 2.0 * D);
+    const SC D2_l = sc_sub(D2, l);          // 2D - l
+    const double r = 385000.0 - 20905.0 * l.c - 3699.0 * D2_l.c - 2956.0 * D2.c - 570.0 * l2.c + 246.0 * l2_2D.c -
+                     205.0 * lp_2D.c - 171.0 * lp2D.c - 152.0 * llp_2D.c;
     double sb, cb, sl, cl;
     sincos(beta, &sb, &cb);
     sincos(lam, &sl, &cl);
-    double xe = r * cb * cl, ye = r * cb * sl, ze = r * sb;
+    const double xe = r * cb * cl, ye = r * cb * sl, ze = r * sb;
     const double ce = 0.9174820620768958, se = 0.3977771559141214;
     out[0] = xe;
     out[1] = ce * ye - se * ze;

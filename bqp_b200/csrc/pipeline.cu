@@ -34,6 +34,7 @@ namespace bqp {
 namespace {
 
 constexpr int kBlock = 256;
+constexpr int kDragLanes = 4;  // lanes per state in pl_drag
 
 __device__ __forceinline__ double* K(const PipeBufs& P, int st, int i) { return P.k + ((size_t)st * 6 + i) * P.cap; }
 
@@ -165,47 +166,93 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
 }
 
 // ------------------------------------------------------------------ gravity
-// Persistent over slots: each CTA stages the field table once.
+// Persistent over slots: one CTA per SM stages the field table once; the
+// CTA's contiguous slot range is walked NT slots per thread.
+template <int NT>
 __global__ void pl_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem, PipeBufs P,
                            int cur) {
     const int count = P.count[cur];
-    if ((int64_t)blockIdx.x * blockDim.x >= count) return;
+    const int per_block = (count + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per_block;
+    const int b1 = min(count, b0 + per_block);
+    if (b0 >= b1) return;  // uniform across the CTA
     const double* tab = stage_table(gtab, ncells, use_smem != 0);
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
-        if (P.skip[slot]) continue;
-        const double s = P.sc[slot], c = P.sc[P.cap + slot];
-        const double x = P.sp[slot], y = P.sp[P.cap + slot], z = P.sp[2 * P.cap + slot];
-        const double px = fma(c, x, s * y), py = fma(-s, x, c * y);
-        const double r2 = fma(px, px, fma(py, py, z * z));
-        double a[3];
-        if (!(isfinite(r2) && r2 > 0.0)) {
-            P.bad[slot] = 1;
-            a[0] = a[1] = a[2] = NAN;
-        } else {
-            gravity_field(tab, order, px, py, z, a);
+    for (int base = b0; base < b1; base += blockDim.x * NT) {
+        double px[NT], py[NT], pz[NT], a[NT][3];
+        int slot[NT];
+        bool on[NT];
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            slot[q] = base + q * blockDim.x + threadIdx.x;
+            on[q] = slot[q] < b1 && !P.skip[slot[q]];
+            px[q] = 7000.0;  // a valid dummy position for idle lanes
+            py[q] = 0.0;
+            pz[q] = 0.0;
+            if (on[q]) {
+                const int sl = slot[q];
+                const double s = P.sc[sl], c = P.sc[P.cap + sl];
+                const double x = P.sp[sl], y = P.sp[P.cap + sl], z = P.sp[2 * P.cap + sl];
+                const double qx = fma(c, x, s * y), qy = fma(-s, x, c * y);
+                const double r2 = fma(qx, qx, fma(qy, qy, z * z));
+                if (!(isfinite(r2) && r2 > 0.0)) {
+                    P.bad[sl] = 1;
+                    P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
+                    on[q] = false;
+                } else {
+                    px[q] = qx;
+                    py[q] = qy;
+                    pz[q] = z;
+                }
+            }
         }
-        P.agrav[slot] = a[0];
-        P.agrav[P.cap + slot] = a[1];
-        P.agrav[2 * P.cap + slot] = a[2];
+        gravity_field_multi<NT>(tab, order, px, py, pz, a);
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            if (!on[q]) continue;
+            const int sl = slot[q];
+            P.agrav[sl] = a[q][0];
+            P.agrav[P.cap + sl] = a[q][1];
+            P.agrav[2 * P.cap + sl] = a[q][2];
+        }
     }
 }
 
 // --------------------------------------------------------------------- drag
+// One state per group of L lanes (jb::density_group): the JB2008 quadrature
+// is the costliest serial chain of the force model, and a batch has only a
+// few hundred states per SM, so each state is spread over L lanes.
+template <int L>
 __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, int cur) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= P.count[cur]) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = gt / L;
+    const int q = gt % L;
+    const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+    if (slot >= P.count[cur]) return;  // uniform across the group
     if (P.skip[slot]) return;
     double sp[6];
     for (int i = 0; i < 6; ++i) sp[i] = P.sp[(size_t)i * P.cap + slot];
     const double am = P.amcd[slot], cd = P.amcd[P.cap + slot];
     double a[3] = {0.0, 0.0, 0.0};
     if (cd != 0.0 && am != 0.0) {
+        // JB2008 adapter (rhs.rs:3551-3776), as Encke::density_at
         const double s = P.sc[slot], c = P.sc[P.cap + slot];
         const double sun[3] = {P.sun[slot], P.sun[P.cap + slot], P.sun[2 * P.cap + slot]};
         const double pi[3] = {fma(c, sp[0], s * sp[1]), fma(-s, sp[0], c * sp[1]), sp[2]};
-        Encke E;  // only its JB2008 adapter is used
-        E.fp = &fp;
-        const double rho = E.density_at(pi, sun, s, c, P.jd[slot]);
+        const double si[3] = {fma(c, sun[0], s * sun[1]), fma(-s, sun[0], c * sun[1]), sun[2]};
+        const double sun_r = sqrt(fma(si[0], si[0], fma(si[1], si[1], si[2] * si[2])));
+        const double sat_r = sqrt(fma(pi[0], pi[0], fma(pi[1], pi[1], pi[2] * pi[2])));
+        double rho;
+        if ((sat_r - fp.earth_radius) * 1000.0 > 2500.0e3) {
+            rho = 1.0e-19;
+        } else {
+            const double alt_m = geodetic_altitude_km(pi[0], pi[1], pi[2], fp.earth_radius) * 1000.0;
+            const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
+            const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
+            const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
+            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask);
+            if (!(rho > 0.0) || !isfinite(rho)) rho = NAN;
+            else if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
+        }
         if (isnan(rho)) {
             a[0] = a[1] = a[2] = NAN;
         } else if (rho > 0.0) {
@@ -222,7 +269,8 @@ __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, in
             }
         }
     }
-    for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = a[i];
+    if (q == 0)
+        for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = a[i];
 }
 
 // ------------------------------------------------------------------ control
@@ -325,16 +373,19 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
 
 template <int M>
 static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, double max_seconds,
-                       int gthreads) {
+                       int gthreads, int gslots) {
     using T = Tab<M>;
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
+    const int dblocks = (int)((A.n * kDragLanes + kBlock - 1) / kBlock);
     const size_t smem = A.use_smem ? (size_t)A.ncells * kCellDoubles * sizeof(double) : 0;
-    cudaError_t e = cudaFuncSetAttribute(pl_gravity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nt = gslots == 1 || gslots == 4 ? gslots : 2;
+    auto gker = nt == 1 ? pl_gravity<1> : (nt == 4 ? pl_gravity<4> : pl_gravity<2>);
+    cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int gblocks = device_sm_count();
-    if ((int64_t)gblocks * gthreads > A.n) gblocks = (int)((A.n + gthreads - 1) / gthreads);
+    if ((int64_t)gblocks * gthreads * nt > A.n) gblocks = (int)((A.n + (int64_t)gthreads * nt - 1) / ((int64_t)gthreads * nt));
     if (gblocks < 1) gblocks = 1;
 
     // private stream ordered after the caller's stream (graphs need a
@@ -359,8 +410,8 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
         for (int s = 0; s < stages; ++s) {
             pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s);
             if (A.force.gravity_on)
-                pl_gravity<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, P, cur);
-            if (A.force.drag) pl_drag<<<blocks, kBlock, 0, st>>>(A.force, P, cur);
+                gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, P, cur);
+            if (A.force.drag) pl_drag<kDragLanes><<<dblocks, kBlock, 0, st>>>(A.force, P, cur);
         }
         pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out);
     };
@@ -410,13 +461,13 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
 }
 
 cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st, double max_seconds,
-                            int gravity_threads) {
+                            int gravity_threads, int gravity_slots) {
     if (A.n <= 0) return cudaSuccess;
-    if (gravity_threads <= 0) gravity_threads = 512;
+    if (gravity_threads <= 0) gravity_threads = 256;
     switch (method) {
-        case kDopri5: return run<kDopri5>(A, P, st, max_seconds, gravity_threads);
-        case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads);
-        case kDopri5Compat: return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads);
+        case kDopri5: return run<kDopri5>(A, P, st, max_seconds, gravity_threads, gravity_slots);
+        case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads, gravity_slots);
+        case kDopri5Compat: return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads, gravity_slots);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -18,31 +18,54 @@
 namespace bqp {
 
 // ----------------------------------------------------------------- kernels
-__global__ void k_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem,
-                          int64_t n, const double* __restrict__ pos, double* __restrict__ acc,
-                          int32_t* __restrict__ status) {
+template <int NT>
+__global__ void k_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem, int64_t n,
+                          const double* __restrict__ pos, double* __restrict__ acc, int32_t* __restrict__ status) {
+    const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t b0 = (int64_t)blockIdx.x * per_block;
+    const int64_t b1 = b0 + per_block < n ? b0 + per_block : n;
+    if (b0 >= b1) return;  // uniform across the CTA
     const double* tab = stage_table(gtab, ncells, use_smem != 0);
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-        const double r2 = fma(x, x, fma(y, y, z * z));
-        double a[3];
-        if (!(isfinite(r2) && r2 > 0.0)) {
-            a[0] = a[1] = a[2] = NAN;
-            if (status) status[i] = kGravityRadius;
-        } else {
-            gravity_field(tab, order, x, y, z, a);
+    for (int64_t base = b0; base < b1; base += (int64_t)blockDim.x * NT) {
+        double px[NT], py[NT], pz[NT], a[NT][3];
+        int64_t idx[NT];
+        bool on[NT];
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            idx[q] = base + (int64_t)q * blockDim.x + threadIdx.x;
+            on[q] = idx[q] < b1;
+            px[q] = 7000.0;
+            py[q] = 0.0;
+            pz[q] = 0.0;
+            if (on[q]) {
+                const int64_t i = idx[q];
+                const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+                const double r2 = fma(x, x, fma(y, y, z * z));
+                if (!(isfinite(r2) && r2 > 0.0)) {
+                    acc[3 * i] = acc[3 * i + 1] = acc[3 * i + 2] = NAN;
+                    if (status) status[i] = kGravityRadius;
+                    on[q] = false;
+                } else {
+                    px[q] = x;
+                    py[q] = y;
+                    pz[q] = z;
+                }
+            }
+        }
+        gravity_field_multi<NT>(tab, order, px, py, pz, a);
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            if (!on[q]) continue;
+            const int64_t i = idx[q];
             // add the C00 point mass back: the full field of the reference's
             // spherical_gravity_impl_frame_packed (gravity.rs:2638-2675)
+            const double r2 = fma(px[q], px[q], fma(py[q], py[q], pz[q] * pz[q]));
             const double k = kMu / (r2 * sqrt(r2));
-            a[0] = fma(-k, x, a[0]);
-            a[1] = fma(-k, y, a[1]);
-            a[2] = fma(-k, z, a[2]);
+            acc[3 * i] = fma(-k, px[q], a[q][0]);
+            acc[3 * i + 1] = fma(-k, py[q], a[q][1]);
+            acc[3 * i + 2] = fma(-k, pz[q], a[q][2]);
             if (status) status[i] = kOk;
         }
-        acc[3 * i] = a[0];
-        acc[3 * i + 1] = a[1];
-        acc[3 * i + 2] = a[2];
     }
 }
 
@@ -187,18 +210,19 @@ static int sm_count() {
 }
 
 cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
-                           const double* pos, double* acc, int32_t* status, cudaStream_t st) {
+                           const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads,
+                           int slots) {
     if (n <= 0) return cudaSuccess;
     const size_t smem = use_smem ? (size_t)ncells * kCellDoubles * sizeof(double) : 0;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_gravity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    const int threads = 256;
-    int64_t blocks = (n + threads - 1) / threads;
-    const int64_t cap = (int64_t)sm_count() * 2;
+    const int nt = slots == 1 || slots == 4 ? slots : 2;
+    auto ker = nt == 1 ? k_gravity<1> : (nt == 4 ? k_gravity<4> : k_gravity<2>);
+    cudaError_t e = cudaFuncSetAttribute(ker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (threads <= 0) threads = 256;
+    int64_t blocks = (n + (int64_t)threads * nt - 1) / ((int64_t)threads * nt);
+    const int64_t cap = (int64_t)sm_count() * (use_smem ? 1 : 4);
     if (blocks > cap) blocks = cap;
-    k_gravity<<<(unsigned)blocks, threads, smem, st>>>(gtab, order, ncells, use_smem, n, pos, acc, status);
+    ker<<<(unsigned)blocks, threads, smem, st>>>(gtab, order, ncells, use_smem, n, pos, acc, status);
     return cudaGetLastError();
 }
 

@@ -88,7 +88,9 @@ typedef struct bqp_force_config {
     double max_kernel_seconds; /* watchdog: wall-clock limit of one propagation call (> 0);
                                   rows not finished by then end with BQP_ST_WATCHDOG */
     int32_t engine;            /* BQP_ENGINE_* */
-    int32_t gravity_threads;   /* threads per CTA of the gravity kernel (0: 512) */
+    int32_t gravity_threads;   /* threads per CTA of the gravity kernels (0: 256) */
+    int32_t gravity_slots;     /* trajectories per thread in the gravity kernels: 1, 2 or 4 (0: 2) */
+    int32_t reserved0;
 } bqp_force_config;
 
 /* propagation engines */
