@@ -367,29 +367,46 @@ __device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr
     double part = 0.0;
     double zend = zend_start, zlast = zend_start;  // zlast: last node of the previous interval
     double tl = 0.0, gl = 0.0, mb = 0.0, ain_last = ain0;
-    for (int i = 0; i < n; ++i) {
-        double zz = zend;
-        zend = zr * zz;
-        const double dz = 0.25 * (zend - zz);
-        if ((i % L) == q) {
+    const int rounds = (n + L - 1) / L;
+    for (int r = 0; r < rounds; ++r) {
+        // advance the interval chain by L intervals (cheap, identical on
+        // every lane) and keep this lane's interval r*L + q
+        double my_start = 0.0, my_dz = 0.0, my_prev = zlast;
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+            const int i = r * L + k;
+            if (i < n) {
+                double zz = zend;
+                zend = zr * zz;
+                const double dz = 0.25 * (zend - zz);
+                if (k == q) {
+                    my_start = zz;
+                    my_dz = dz;
+                    my_prev = zlast;
+                }
+                zz += dz;
+                zz += dz;
+                zz += dz;
+                zz += dz;
+                zlast = zz;
+            }
+        }
+        // every lane evaluates its own interval's nodes together
+        const int mi = r * L + q;
+        if (mi < n) {
             double t_, g_, m_;
-            const double carry = i == 0 ? ain0 : node_ain(zlast, tc, with_mbar, &t_, &g_, &m_);
+            const double carry = mi == 0 ? ain0 : node_ain(my_prev, tc, with_mbar, &t_, &g_, &m_);
             double sum1 = kW0 * carry;
+            double zz = my_start;
 #pragma unroll
             for (int j = 1; j < 5; ++j) {
-                zz += dz;
+                zz += my_dz;
                 const double a = node_ain(zz, tc, with_mbar, &tl, &gl, &mb);
                 sum1 += (j == 1 || j == 3 ? kW1 : (j == 2 ? kW2 : kW0)) * a;
                 ain_last = a;
             }
-            part += dz * sum1;
-        } else {
-            zz += dz;
-            zz += dz;
-            zz += dz;
-            zz += dz;
+            part += my_dz * sum1;
         }
-        zlast = zz;
     }
     // group reduction and the last interval's node values from its owner
 #pragma unroll
