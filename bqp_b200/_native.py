@@ -45,7 +45,7 @@ class ForceConfig(C.Structure):
         ("omega_earth", C.c_double), ("mu_sun", C.c_double), ("mu_moon", C.c_double),
         ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
         ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
-        ("gravity_slots", C.c_int32), ("reserved0", C.c_int32),
+        ("gravity_slots", C.c_int32), ("drag_quadrature", C.c_int32),
     ]
 
 
@@ -67,6 +67,7 @@ SIGNATURES = [
     ("bqp_ctx_set_stream", C.c_int, [_vp, _vp]),
     ("bqp_ctx_info", C.c_int, [_vp, _lp]),
     ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
+    ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
     ("bqp_gravity_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _ip]),
     ("bqp_gravity_eval_device", C.c_int, [_vp, C.c_int64, _vp, _vp, _vp]),
     ("bqp_rhs_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
@@ -168,8 +169,10 @@ class Context:
     def info(self):
         out = np.zeros(4, dtype=np.int64)
         check(lib().bqp_ctx_info(self._h, lptr(out)))
+        w = C.c_double(0.0)
+        check(lib().bqp_ctx_info_fit(self._h, C.byref(w)))
         return {"order": int(out[0]), "cells": int(out[1]), "table_bytes": int(out[2]),
-                "table_in_shared_memory": bool(out[3])}
+                "table_in_shared_memory": bool(out[3]), "jb_fit_worst_rel": w.value}
 
     def set_config(self, cfg: ForceConfig):
         check(lib().bqp_ctx_set_config(self._h, C.byref(cfg)))

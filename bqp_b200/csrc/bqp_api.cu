@@ -176,6 +176,79 @@ std::vector<double> build_gravity_table(const Coeffs& cf, int order) {
     return tab;
 }
 
+// Chebyshev fits of the JB2008 fixed-node sweeps (jb2008.cuh, JbFit): the
+// sums are evaluated by the quadrature itself at 64 Chebyshev points of
+// T_inf in [300, 3500] K, transformed in long double, and checked at 257
+// further points; a fit that misses 4e-15 relative is not used.
+void sweep_sums(double tinf, jb::Sweep* lo_out, jb::Sweep* mid_out) {
+    using namespace jb;
+    const double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * std::exp(-0.0021357 * tinf);
+    const double gsubx = 0.054285714 * (tsubx - 183.0);
+    double tc[4] = {tsubx, gsubx, (tinf - tsubx) / (kPi / 2), 0.0};
+    tc[3] = gsubx / tc[2];
+    const double z1 = 90.0;
+    double al = std::log(105.0 / z1);
+    int n = 1 + (int)std::floor(al / kLnStepLower);
+    double zr = std::exp(al / n);
+    const double tloc1 = local_temp(z1, tc);
+    *lo_out = boole_sweep(z1, z1, zr, n, mbar(z1) * grav(z1) / tloc1, true, tc);
+    const double z = lo_out->z;
+    al = std::log(500.0 / z);
+    n = 1 + (int)std::floor(al / kLnStepMiddle);
+    zr = std::exp(al / n);
+    *mid_out = boole_sweep(z, lo_out->zend, zr, n, lo_out->gravl / lo_out->tloc, false, tc);
+}
+
+bool build_jb_fit(jb::JbFit& f, double* worst) {
+    typedef long double LD;
+    const int N = jb::kFitTerms;
+    f.valid = 0;
+    f.terms = N;
+    f.lo = 300.0;
+    f.hi = 3500.0;
+    std::vector<LD> fl(N), fm(N);
+    jb::Sweep lo, mid;
+    for (int k = 0; k < N; ++k) {
+        const LD x = cosl(3.14159265358979323846264338327950288L * (k + 0.5L) / N);
+        const double t = 0.5 * (f.hi + f.lo) + 0.5 * (f.hi - f.lo) * (double)x;
+        sweep_sums(t, &lo, &mid);
+        fl[k] = lo.sum;
+        fm[k] = mid.sum;
+        if (k == 0) {
+            f.low_z = lo.z;
+            f.low_zend = lo.zend;
+            f.low_mb2 = lo.mb;
+            f.low_gravl = lo.gravl;
+            f.mid_z = mid.z;
+            f.mid_zend = mid.zend;
+            f.mid_gravl = mid.gravl;
+        } else if (lo.z != f.low_z || lo.zend != f.low_zend || mid.z != f.mid_z || mid.zend != f.mid_zend) {
+            return false;  // node altitudes must not depend on T_inf
+        }
+    }
+    for (int j = 0; j < N; ++j) {
+        LD sl = 0, sm = 0;
+        for (int k = 0; k < N; ++k) {
+            const LD c = cosl(3.14159265358979323846264338327950288L * j * (k + 0.5L) / N);
+            sl += fl[k] * c;
+            sm += fm[k] * c;
+        }
+        f.low[j] = (double)((j == 0 ? 1.0L : 2.0L) / N * sl);
+        f.mid[j] = (double)((j == 0 ? 1.0L : 2.0L) / N * sm);
+    }
+    double w = 0.0;
+    for (int i = 0; i < 257; ++i) {
+        const double t = f.lo + (f.hi - f.lo) * (i + 0.5) / 257.0;
+        sweep_sums(t, &lo, &mid);
+        const double a = jb::cheb_eval(f.low, N, f.lo, f.hi, t);
+        const double b = jb::cheb_eval(f.mid, N, f.lo, f.hi, t);
+        w = std::max(w, std::max(std::fabs(a - lo.sum) / std::fabs(lo.sum), std::fabs(b - mid.sum) / std::fabs(mid.sum)));
+    }
+    *worst = w;
+    f.valid = w <= 4e-15 ? 1 : 0;
+    return f.valid != 0;
+}
+
 }  // namespace
 
 struct bqp_ctx {
@@ -193,6 +266,8 @@ struct bqp_ctx {
     size_t ws_bytes = 0;
     void* d_pws = nullptr;  // stage-synchronous engine buffers
     size_t pws_bytes = 0;
+    jb::JbFit* d_fit = nullptr;  // JB2008 fixed-node sweep fits (device)
+    double fit_worst = -1.0;
 };
 
 namespace {
@@ -247,6 +322,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.mu_moon = c.mu_moon;
     fp.drivers = {c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
                   c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
+    fp.fit = (c.drag_quadrature || !fp.drag) ? nullptr : ctx->d_fit;
     return fp;
 }
 
@@ -530,6 +606,14 @@ int bqp_ctx_create(const char* text, int64_t len, const bqp_force_config* cfg, b
         e = cudaMalloc(&ctx->d_queue, sizeof(unsigned long long));
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(queue)");
     }
+    if (!rc) {
+        jb::JbFit fit;
+        if (build_jb_fit(fit, &ctx->fit_worst)) {
+            e = cudaMalloc(&ctx->d_fit, sizeof fit);
+            if (e == cudaSuccess) e = cudaMemcpy(ctx->d_fit, &fit, sizeof fit, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) rc = cuda_fail(e, "JB2008 fit upload");
+        }
+    }
     if (rc) {
         bqp_ctx_destroy(ctx);
         return rc;
@@ -548,6 +632,7 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_queue) cudaFree(ctx->d_queue);
     if (ctx->d_ws) cudaFree(ctx->d_ws);
     if (ctx->d_pws) cudaFree(ctx->d_pws);
+    if (ctx->d_fit) cudaFree(ctx->d_fit);
     delete ctx;
     return 0;
 }
@@ -564,6 +649,12 @@ int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info) {
     info[1] = ctx->ncells;
     info[2] = (int64_t)ctx->tab_bytes;
     info[3] = ctx->use_smem;
+    return 0;
+}
+
+int bqp_ctx_info_fit(const bqp_ctx* ctx, double* worst_rel) {
+    if (!ctx || !worst_rel) return fail(BQP_E_ARG, "null argument");
+    *worst_rel = ctx->d_fit ? ctx->fit_worst : -1.0;
     return 0;
 }
 

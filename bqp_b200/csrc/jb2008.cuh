@@ -65,6 +65,41 @@ struct Drivers {
     double f10, f10b, s10, s10b, m10, m10b, y10, y10b, dtc;  // dtc: temperature correction, K
 };
 
+// Fixed-node sweeps as functions of the exospheric temperature.  Above 105
+// km the lower Boole sweep (90 -> 105 km) always walks the same 16 intervals,
+// and above 500 km the middle sweep (105 -> 500 km) the same 63: their node
+// altitudes are constant and their sums depend only on T_inf (through the
+// temperature profile tc).  The host fits each sum with a Chebyshev series in
+// T_inf (build_jb_fit, 64 terms, checked against the quadrature to ~1e-15
+// relative over [lo, hi]); the device evaluates it by Clenshaw's recurrence
+// instead of walking ~320 nodes.  Outside [lo, hi], or below 105 / 500 km,
+// the quadrature runs as before.
+constexpr int kFitTerms = 64;
+struct JbFit {
+    int32_t valid;
+    int32_t terms;
+    double lo, hi;
+    double low[kFitTerms];  // lower-sweep sum
+    double mid[kFitTerms];  // middle-sweep sum
+    double low_z, low_zend, low_mb2, low_gravl;  // last node of the lower sweep
+    double mid_z, mid_zend, mid_gravl;           // last node of the middle sweep
+};
+
+BQP_HD double cheb_eval(const double* c, int terms, double lo, double hi, double t) {
+    const double x = (2.0 * t - (hi + lo)) / (hi - lo);
+    double b1 = 0.0, b2 = 0.0;
+    for (int j = terms - 1; j >= 1; --j) {
+        const double tmp = fma(2.0 * x, b1, -b2) + c[j];
+        b2 = b1;
+        b1 = tmp;
+    }
+    return fma(x, b1, -b2) + c[0];
+}
+
+BQP_HD bool fit_covers(const JbFit* f, double tinf) {
+    return f != nullptr && f->valid && tinf >= f->lo && tinf <= f->hi;
+}
+
 BQP_HD double mbar(double z) {
     double dz = z - 100.0;
     return dz * (dz * (dz * (dz * (dz * (dz * JBT(kCxamb)[6] + JBT(kCxamb)[5]) + JBT(kCxamb)[4]) + JBT(kCxamb)[3]) +
@@ -192,7 +227,7 @@ BQP_HD Sweep boole_sweep(double z, double zend_start, double zr, int n, double a
 // satellite relative to the Sun (rad), geocentric latitude (rad), altitude
 // (m) and the driver set.  Non-positive returns are the error codes above.
 BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
-                      const Drivers& d) {
+                      const Drivers& d, const JbFit* fit = nullptr) {
     if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) ||
         !isfinite(alt_m) || !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) ||
         !isfinite(d.s10b) || !isfinite(d.m10) || !isfinite(d.m10b) || !isfinite(d.y10) ||
@@ -242,12 +277,25 @@ BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat,
     tc[3] = gsubx / tc[2];
     // 90 km -> min(alt, 105 km)
     const double z1 = 90.0;
-    double al = log(fmin(alt, 105.0) / z1);
-    int n = 1 + (int)floor(al / kLnStepLower);
-    double zr = exp(al / n);
-    double mb1 = mbar(z1);
-    double tloc1 = local_temp(z1, tc);
-    Sweep lo = boole_sweep(z1, z1, zr, n, mb1 * grav(z1) / tloc1, true, tc);
+    double al, zr;
+    int n;
+    const double mb1 = mbar(z1);
+    const double tloc1 = local_temp(z1, tc);
+    const bool use_fit = fit_covers(fit, tinf);
+    Sweep lo;
+    if (use_fit && alt >= 105.0) {
+        lo.sum = cheb_eval(fit->low, fit->terms, fit->lo, fit->hi, tinf);
+        lo.z = fit->low_z;
+        lo.zend = fit->low_zend;
+        lo.mb = fit->low_mb2;
+        lo.gravl = fit->low_gravl;
+        lo.tloc = local_temp(lo.z, tc);
+    } else {
+        al = log(fmin(alt, 105.0) / z1);
+        n = 1 + (int)floor(al / kLnStepLower);
+        zr = exp(al / n);
+        lo = boole_sweep(z1, z1, zr, n, mb1 * grav(z1) / tloc1, true, tc);
+    }
     double mb2 = lo.mb, tloc2 = lo.tloc;
     double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
     double anm = kAvogadro * rho;
@@ -262,10 +310,20 @@ BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat,
         aln[5] = aln[4] - 25.0;
     } else {
         // 105 km -> min(alt, 500 km)
-        al = log(fmin(alt, 500.0) / z);
-        n = 1 + (int)floor(al / kLnStepMiddle);
-        zr = exp(al / n);
-        Sweep mid = boole_sweep(z, lo.zend, zr, n, lo.gravl / tloc2, false, tc);
+        Sweep mid;
+        if (use_fit && alt >= 500.0) {
+            mid.sum = cheb_eval(fit->mid, fit->terms, fit->lo, fit->hi, tinf);
+            mid.z = fit->mid_z;
+            mid.zend = fit->mid_zend;
+            mid.tloc = local_temp(mid.z, tc);
+            mid.gravl = fit->mid_gravl;
+            mid.ain = mid.gravl / mid.tloc;
+        } else {
+            al = log(fmin(alt, 500.0) / z);
+            n = 1 + (int)floor(al / kLnStepMiddle);
+            zr = exp(al / n);
+            mid = boole_sweep(z, lo.zend, zr, n, lo.gravl / tloc2, false, tc);
+        }
         double tloc3 = mid.tloc;
         z = mid.z;
         // between 500 km and alt (hydrogen is anchored at 500 km)
@@ -346,9 +404,7 @@ BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat,
 // interval i-1, recomputed -- the same function at the same altitude, so the
 // same value.  Partial sums meet in a group-masked shuffle.  All lanes of a
 // group hold the same inputs, so they branch together.
-struct SweepG {
-    double sum, z, zend, tloc, gravl, mb, ain;
-};
+typedef Sweep SweepG;
 
 BQP_HD double node_ain(double z, const double* tc, bool with_mbar, double* tloc, double* gravl, double* mb) {
     *tloc = local_temp(z, tc);
@@ -426,7 +482,7 @@ __device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr
 // gmask = the group's lanes).  Same inputs, same error codes.
 template <int L>
 __device__ double density_group(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
-                                const Drivers& d, int q, unsigned gmask) {
+                                const Drivers& d, int q, unsigned gmask, const JbFit* fit = nullptr) {
     double code = 0.0;
     if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) || !isfinite(alt_m) ||
         !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) || !isfinite(d.s10b) || !isfinite(d.m10) ||
@@ -476,12 +532,25 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
     tc[2] = (tinf - tsubx) / (kPi / 2);
     tc[3] = gsubx / tc[2];
     const double z1 = 90.0;
-    double al = log(fmin(alt, 105.0) / z1);
-    int n = 1 + (int)floor(al / kLnStepLower);
-    double zr = exp(al / n);
+    double al, zr;
+    int n;
     const double mb1 = mbar(z1);
     const double tloc1 = local_temp(z1, tc);
-    const SweepG lo = boole_sweep_group<L>(z1, zr, n, mb1 * grav(z1) / tloc1, true, tc, q, gmask);
+    const bool use_fit = fit_covers(fit, tinf);
+    SweepG lo;
+    if (use_fit && alt >= 105.0) {
+        lo.sum = cheb_eval(fit->low, fit->terms, fit->lo, fit->hi, tinf);
+        lo.z = fit->low_z;
+        lo.zend = fit->low_zend;
+        lo.mb = fit->low_mb2;
+        lo.gravl = fit->low_gravl;
+        lo.tloc = local_temp(lo.z, tc);
+    } else {
+        al = log(fmin(alt, 105.0) / z1);
+        n = 1 + (int)floor(al / kLnStepLower);
+        zr = exp(al / n);
+        lo = boole_sweep_group<L>(z1, zr, n, mb1 * grav(z1) / tloc1, true, tc, q, gmask);
+    }
     const double mb2 = lo.mb, tloc2 = lo.tloc;
     double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
     const double anm = kAvogadro * rho;
@@ -495,10 +564,20 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
     if (alt <= 105.0) {
         aln[5] = aln[4] - 25.0;
     } else {
-        al = log(fmin(alt, 500.0) / z);
-        n = 1 + (int)floor(al / kLnStepMiddle);
-        zr = exp(al / n);
-        const SweepG mid = boole_sweep_group<L>(lo.zend, zr, n, lo.gravl / tloc2, false, tc, q, gmask);
+        SweepG mid;
+        if (use_fit && alt >= 500.0) {
+            mid.sum = cheb_eval(fit->mid, fit->terms, fit->lo, fit->hi, tinf);
+            mid.z = fit->mid_z;
+            mid.zend = fit->mid_zend;
+            mid.tloc = local_temp(mid.z, tc);
+            mid.gravl = fit->mid_gravl;
+            mid.ain = mid.gravl / mid.tloc;
+        } else {
+            al = log(fmin(alt, 500.0) / z);
+            n = 1 + (int)floor(al / kLnStepMiddle);
+            zr = exp(al / n);
+            mid = boole_sweep_group<L>(lo.zend, zr, n, lo.gravl / tloc2, false, tc, q, gmask);
+        }
         const double tloc3 = mid.tloc;
         z = mid.z;
         al = log(fmax(alt, 500.0) / z);

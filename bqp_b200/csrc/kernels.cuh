@@ -39,6 +39,7 @@ struct ForceParams {
     double omega;
     double mu_sun, mu_moon;
     jb::Drivers drivers;
+    const jb::JbFit* fit;  // device copy of the fixed-node sweep fits, or null
 };
 
 // Solver controls (IntegratorConfig, solver.rs:35-60 and integrator.rs:404-558).
@@ -165,7 +166,7 @@ struct Encke {
         const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
         const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
         const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, fp->drivers);
+        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, fp->drivers, fp->fit);
         if (!(rho > 0.0) || !isfinite(rho)) return NAN;
         if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         return rho;

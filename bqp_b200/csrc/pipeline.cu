@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, in
             const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
             const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
             const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask);
+            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask, fp.fit);
             if (!(rho > 0.0) || !isfinite(rho)) rho = NAN;
             else if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         }

@@ -90,7 +90,8 @@ typedef struct bqp_force_config {
     int32_t engine;            /* BQP_ENGINE_* */
     int32_t gravity_threads;   /* threads per CTA of the gravity kernels (0: 256) */
     int32_t gravity_slots;     /* trajectories per thread in the gravity kernels: 1, 2 or 4 (0: 2) */
-    int32_t reserved0;
+    int32_t drag_quadrature;   /* 1: always walk the JB2008 Boole quadrature; 0: use the
+                                  Chebyshev fits of its fixed-node sweeps where they apply */
 } bqp_force_config;
 
 /* propagation engines */
@@ -120,6 +121,9 @@ int bqp_ctx_destroy(bqp_ctx* ctx);
 int bqp_ctx_set_stream(bqp_ctx* ctx, void* cuda_stream);
 /* info[0]=order, [1]=table cells, [2]=table bytes, [3]=table staged in shared memory */
 int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info4);
+/* Worst relative error of the JB2008 sweep fits against the quadrature at
+ * the check points (-1: no fit, the quadrature always runs). */
+int bqp_ctx_info_fit(const bqp_ctx* ctx, double* worst_rel);
 /* Replace the force/solver settings of a context (the field is kept; the
  * order may only shrink up to the parsed order). */
 int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);

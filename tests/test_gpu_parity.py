@@ -30,9 +30,10 @@ ENGINES = ["pipeline", "persistent"]
 
 
 def ctx_for(text, order, flags=0, method="dop853", eps=1e-8, dt_max=300.0, rtol=None, atol=None,
-            am=0.01, cd=2.2, ground=False, max_attempts=None, engine="pipeline"):
+            am=0.01, cd=2.2, ground=False, max_attempts=None, engine="pipeline", quadrature=False):
     cfg = N.default_config()
     cfg.engine = N.ENGINES[engine]
+    cfg.drag_quadrature = int(quadrature)
     cfg.order = order
     cfg.force_flags = flags
     cfg.method = N.METHODS[method]
@@ -128,6 +129,29 @@ def test_encke_rhs_matches_oracle(flags):
         scale = MU / r ** 2  # full-field magnitude
         assert np.array_equal(got[i, :3], ref[:3])
         assert np.abs(got[i, 3:] - ref[3:]).max() <= 1e-12 * scale, (i, got[i], ref)
+
+
+def test_jb2008_sweep_fit_matches_quadrature():
+    """The Chebyshev fits of the fixed-node JB2008 sweeps reproduce the Boole
+    quadrature: fit error at the check points, and the drag term of the force
+    call with and without the fits (LEO 400-1200 km, all local times)."""
+    order = 8
+    text = workloads.synthetic_field(order)
+    fit = ctx_for(text, order, flags=1)
+    quad = ctx_for(text, order, flags=1, quadrature=True)
+    assert 0.0 <= fit.info()["jb_fit_worst_rel"] <= 4e-15
+    n = 2048
+    states = workloads.leo_states(n, seed=23)
+    equ, _ = N.eci_to_equinoctial(states)
+    rng = np.random.default_rng(23)
+    t = rng.uniform(0.0, 86400.0, n)
+    zero = np.zeros((n, 6))
+    nodrag = ctx_for(text, order, flags=0).rhs(equ, 0.0, EPOCH, t, zero)
+    a_fit = fit.rhs(equ, 0.0, EPOCH, t, zero)[:, 3:] - nodrag[:, 3:]
+    a_quad = quad.rhs(equ, 0.0, EPOCH, t, zero)[:, 3:] - nodrag[:, 3:]
+    mag = np.linalg.norm(a_quad, axis=1)
+    assert (mag > 0).all()
+    assert (np.linalg.norm(a_fit - a_quad, axis=1) / mag).max() <= 1e-12
 
 
 # -------------------------------------------------------------- trajectories
