@@ -55,6 +55,8 @@ struct PipeBufs {
     double* amcd;         // [2][cap]
     int32_t* skip;        // [cap] 1: stage derivative reused, no force call
     int32_t* bad;         // [cap] latched invalid-radius gravity error
+    int32_t* dlist[2];    // drag work lists of the stage: 0 above ~510 km (sweep fits), 1 below
+    int32_t* dcount;      // [2]
 };
 
 size_t pipeline_bytes(int64_t cap);

@@ -34,7 +34,6 @@ namespace bqp {
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kDragLanes = 4;  // lanes per state in pl_drag
 
 __device__ __forceinline__ double* K(const PipeBufs& P, int st, int i) { return P.k + ((size_t)st * 6 + i) * P.cap; }
 
@@ -158,6 +157,22 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
         P.jd[slot] = jd;
         P.amcd[slot] = s.am;
         P.amcd[P.cap + slot] = s.cd;
+        // drag work list: states above ~510 km take the sweep fits (cheap),
+        // the rest walk the quadrature; homogeneous warps in each list
+        const int cls = sqrt(r2) - fp.earth_radius >= 510.0 ? 0 : 1;
+        const unsigned m = __activemask();
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const unsigned mm = __ballot_sync(m, cls == c);
+            if (cls == c) {
+                const int lane = threadIdx.x & 31;
+                const int leader = __ffs(mm) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(&P.dcount[c], __popc(mm));
+                base = __shfl_sync(mm, base, leader);
+                P.dlist[c][base + __popc(mm & ((1u << lane) - 1u))] = slot;
+            }
+        }
     } else {
         for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = 0.0;
     }
@@ -222,13 +237,13 @@ __global__ void pl_gravity(const double* __restrict__ gtab, int order, int ncell
 // is the costliest serial chain of the force model, and a batch has only a
 // few hundred states per SM, so each state is spread over L lanes.
 template <int L>
-__global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, int cur) {
+__global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, int list) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = gt / L;
+    const int item = gt / L;
     const int q = gt % L;
     const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
-    if (slot >= P.count[cur]) return;  // uniform across the group
-    if (P.skip[slot]) return;
+    if (item >= P.dcount[list]) return;  // uniform across the group
+    const int slot = P.dlist[list][item];
     double sp[6];
     for (int i = 0; i < 6; ++i) sp[i] = P.sp[(size_t)i * P.cap + slot];
     const double am = P.amcd[slot], cd = P.amcd[P.cap + slot];
@@ -341,7 +356,7 @@ __global__ void __launch_bounds__(kBlock) pl_abort(PropArgs A, PipeBufs P, int c
 size_t pipeline_bytes(int64_t cap) {
     PipeBufs P{};
     pipeline_carve(P, nullptr, cap);
-    return (size_t)(uintptr_t)P.bad + (size_t)cap * sizeof(int32_t) + 256;
+    return (size_t)(uintptr_t)P.dcount + 2 * sizeof(int32_t) + 256;
 }
 
 void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
@@ -369,6 +384,9 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
     P.amcd = (double*)take(2 * c * 8);
     P.skip = (int32_t*)take(c * 4);
     P.bad = (int32_t*)take(c * 4);
+    P.dlist[0] = (int32_t*)take(c * 4);
+    P.dlist[1] = (int32_t*)take(c * 4);
+    P.dcount = (int32_t*)take(2 * 4);
 }
 
 template <int M>
@@ -378,14 +396,17 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
-    const int dblocks = (int)((A.n * kDragLanes + kBlock - 1) / kBlock);
+    const int dblocks2 = (int)((A.n * 2 + kBlock - 1) / kBlock);
+    const int dblocks4 = (int)((A.n * 4 + kBlock - 1) / kBlock);
     const size_t smem = A.use_smem ? (size_t)A.ncells * kCellDoubles * sizeof(double) : 0;
     const int nt = gslots == 1 || gslots == 4 ? gslots : 2;
     auto gker = nt == 1 ? pl_gravity<1> : (nt == 4 ? pl_gravity<4> : pl_gravity<2>);
     cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // one CTA per SM (the table fills shared memory); each takes an equal
+    // share of the active slots, NT per thread
     int gblocks = device_sm_count();
-    if ((int64_t)gblocks * gthreads * nt > A.n) gblocks = (int)((A.n + (int64_t)gthreads * nt - 1) / ((int64_t)gthreads * nt));
+    if (gblocks > A.n) gblocks = (int)A.n;
     if (gblocks < 1) gblocks = 1;
 
     // private stream ordered after the caller's stream (graphs need a
@@ -408,10 +429,14 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     // one graph = two attempts (active list 0 -> 1 -> 0)
     auto enqueue_attempt = [&](int cur, int timed_out) {
         for (int s = 0; s < stages; ++s) {
+            if (A.force.drag) cudaMemsetAsync(P.dcount, 0, 2 * sizeof(int32_t), st);
             pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s);
             if (A.force.gravity_on)
                 gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, P, cur);
-            if (A.force.drag) pl_drag<kDragLanes><<<dblocks, kBlock, 0, st>>>(A.force, P, cur);
+            if (A.force.drag) {
+                pl_drag<2><<<dblocks2, kBlock, 0, st>>>(A.force, P, 0);
+                pl_drag<4><<<dblocks4, kBlock, 0, st>>>(A.force, P, 1);
+            }
         }
         pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out);
     };

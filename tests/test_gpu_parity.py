@@ -151,7 +151,9 @@ def test_jb2008_sweep_fit_matches_quadrature():
     a_quad = quad.rhs(equ, 0.0, EPOCH, t, zero)[:, 3:] - nodrag[:, 3:]
     mag = np.linalg.norm(a_quad, axis=1)
     assert (mag > 0).all()
-    assert (np.linalg.norm(a_fit - a_quad, axis=1) / mag).max() <= 1e-12
+    # the drag term is recovered as a difference of two force calls, whose
+    # rounding (~1e-21 km/s^2) sets the floor at the highest altitudes
+    assert np.all(np.linalg.norm(a_fit - a_quad, axis=1) <= 1e-12 * mag + 1e-20)
 
 
 # -------------------------------------------------------------- trajectories
