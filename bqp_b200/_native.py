@@ -33,6 +33,7 @@ METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2}
 ENGINES = {"pipeline": 0, "persistent": 1}
 
 E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5
+NOALLOC_MAX_TRAJ = 16384  # BQP_NOALLOC_MAX_TRAJ
 
 
 class ForceConfig(C.Structure):
@@ -76,6 +77,8 @@ SIGNATURES = [
                                       _ip, _lp, _lp]),
     ("bqp_propagate_final_device", C.c_int, [_vp, C.c_int64, _vp, C.c_int32, _vp, C.c_double, _vp, _vp,
                                              _vp, _vp, _vp, _vp]),
+    ("bqp_propagate_final_noalloc", C.c_int, [_vp, C.c_int64, _dp, C.c_int32, _dp, C.c_double, _dp, _dp,
+                                              _dp, _ip, _lp, _lp]),
     ("bqp_propagate_sampled", C.c_int, [_vp, C.c_int64, _dp, C.c_int32, _dp, C.c_double, _dp, C.c_int32,
                                         _dp, C.c_int32, _dp, _ip, _lp, _lp]),
     ("bqp_propagate_sampled_device", C.c_int, [_vp, C.c_int64, _vp, C.c_int32, _vp, C.c_double, _vp,
@@ -220,6 +223,23 @@ class Context:
         check(lib().bqp_propagate_final(self._h, n, dptr(s), int(equinoctial), dptr(ep), float(t0), dptr(tfa),
                                         None if bal is None else dptr(bal), dptr(out), iptr(st), lptr(steps),
                                         lptr(evals)))
+        return out, st, steps, evals
+
+    def propagate_final_noalloc(self, states, epoch_jd, tf, t0=0.0, ballistic=None, equinoctial=False):
+        """Like propagate_final, through the entry point that allocates no
+        device memory (at most NOALLOC_MAX_TRAJ rows; persistent kernel)."""
+        s = f64(states).reshape(-1, 6)
+        n = s.shape[0]
+        ep = f64(np.broadcast_to(epoch_jd, (n,)))
+        tfa = f64(np.broadcast_to(tf, (n,)))
+        bal = None if ballistic is None else f64(np.broadcast_to(ballistic, (n, 2)))
+        out = np.empty((n, 6))
+        st = np.empty(n, dtype=np.int32)
+        steps = np.empty(n, dtype=np.int64)
+        evals = np.empty(n, dtype=np.int64)
+        check(lib().bqp_propagate_final_noalloc(self._h, n, dptr(s), int(equinoctial), dptr(ep), float(t0),
+                                                dptr(tfa), None if bal is None else dptr(bal), dptr(out),
+                                                iptr(st), lptr(steps), lptr(evals)))
         return out, st, steps, evals
 
     def propagate_sampled(self, states, epoch_jd, tf, t_eval, t0=0.0, deltas=False, equinoctial=False):

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -898,6 +899,135 @@ int bqp_eci_to_kep(int64_t n, const double* eci, double* kep) {
     if (n < 0 || (n > 0 && (!eci || !kep))) return fail(BQP_E_ARG, "bad buffers");
     for (int64_t i = 0; i < n; ++i) eci2kep(eci + 6 * i, kep + 6 * i);
     return 0;
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Allocation-free final-state propagation (bqp_propagate_final_noalloc).
+//
+// For callers that cannot allocate device memory while they propagate: the
+// staging buffers of the host-buffer call live in one fixed array compiled
+// into the library instead of the context's growable workspace.  In host
+// code `g_noalloc_scratch` is only the runtime's stand-in for that array; its
+// device address comes from cudaGetSymbolAddress, looked up once per device
+// with that device current, and only that address is handed to the kernel.
+namespace {
+
+constexpr size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Bytes one call carves for n rows, in carve order: work-queue counter;
+// inputs (state, epoch, final time, ballistic pair); outputs (state, status,
+// steps, evaluations).  Every array starts on a 256-byte boundary, as Carve
+// places them.
+constexpr size_t noalloc_bytes(size_t n) {
+    return round256(sizeof(unsigned long long)) + round256(n * 6 * sizeof(double)) +
+           2 * round256(n * sizeof(double)) + round256(n * 2 * sizeof(double)) +
+           round256(n * 6 * sizeof(double)) + round256(n * sizeof(int32_t)) + 2 * round256(n * sizeof(int64_t));
+}
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[noalloc_bytes(BQP_NOALLOC_MAX_TRAJ)];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;  // serialises the calls; guards g_noalloc_base
+unsigned char* g_noalloc_base[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (which the
+// caller has made `device`), looked up on the first call on that device.
+int noalloc_base(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return fail(BQP_E_ARG, "device %d is beyond the %d devices the no-allocation path supports", device,
+                    kNoallocMaxDevices);
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+        g_noalloc_base[device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_base[device];
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ,
+                                const double* epoch_jd, double t0, const double* tf, const double* ballistic,
+                                double* out, int32_t* status, int64_t* steps, int64_t* evals) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
+    if (rc) return rc;
+    if (n > BQP_NOALLOC_MAX_TRAJ)
+        return fail(BQP_E_ARG, "n = %lld rows exceeds the no-allocation limit of %d rows", (long long)n,
+                    BQP_NOALLOC_MAX_TRAJ);
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    unsigned char* base = nullptr;
+    if ((rc = noalloc_base(ctx->device, &base))) return rc;
+
+    Carve cv{reinterpret_cast<char*>(base)};
+    unsigned long long* queue = cv.take<unsigned long long>(1);
+    double* din = cv.take<double>((size_t)n * 6);
+    double* dep = cv.take<double>((size_t)n);
+    double* dtf = cv.take<double>((size_t)n);
+    double* db = cv.take<double>((size_t)n * 2);
+    double* dout = cv.take<double>((size_t)n * 6);
+    int32_t* dst = cv.take<int32_t>((size_t)n);
+    int64_t* dsteps = cv.take<int64_t>((size_t)n);
+    int64_t* devals = cv.take<int64_t>((size_t)n);
+    if (cv.off > sizeof(g_noalloc_scratch))
+        return fail(BQP_E_ARG, "no-allocation staging of %zu bytes exceeds the %zu-byte array", cv.off,
+                    sizeof(g_noalloc_scratch));
+
+    const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
+    cudaStream_t s = ctx->stream;
+    // the work-queue counter is the one thing that must start at zero; every
+    // output row is written by the kernel (finished, failed or drained)
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(din, in, b6, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtf, tf, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && ballistic) e = cudaMemcpyAsync(db, ballistic, 2 * b1, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_propagate_final_noalloc H2D");
+
+    PropArgs A{};
+    A.n = n;
+    A.in = din;
+    A.input_equinoctial = input_equ;
+    A.epoch = dep;
+    A.t0 = t0;
+    A.tf = dtf;
+    A.ballistic = ballistic ? db : nullptr;
+    A.am0 = ctx->cfg.am_ratio;
+    A.cd0 = ctx->cfg.cd;
+    A.t_eval = nullptr;
+    A.n_t = 0;
+    A.out_mode = 0;
+    A.out = dout;
+    A.status = dst;
+    A.steps = dsteps;
+    A.evals = devals;
+    A.queue = queue;
+    A.gtab = ctx->d_tab;
+    A.ncells = ctx->ncells;
+    A.use_smem = ctx->use_smem;
+    A.force = force_params(ctx);
+    A.ctrl = ctrl_params(ctx);
+    e = launch_propagate(A, ctx->cfg.method, 256, 0, s);
+    if (e != cudaSuccess) return cuda_fail(e, "k_propagate launch (no-allocation path)");
+
+    e = cudaMemcpyAsync(out, dout, b6, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, dst, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && steps) e = cudaMemcpyAsync(steps, dsteps, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && evals) e = cudaMemcpyAsync(evals, devals, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_propagate_final_noalloc");
 }
 
 }  // extern "C"

@@ -164,6 +164,34 @@ int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in,
                                const double* tf, const double* ballistic, double* out,
                                int32_t* status, int64_t* steps, int64_t* evals);
 
+/* Final-state propagation that allocates no memory.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they propagate -- a host application whose device memory is all reserved in
+ * its own pool at start-up, or a loop that must not let a cudaFree stall the
+ * whole device -- and who still want host buffers in and out.
+ *
+ * Same arguments, results and per-row status as bqp_propagate_final, always
+ * on the persistent kernel (whatever cfg.engine says).  The inputs and
+ * outputs are staged through one fixed device array inside the library, of
+ * room for BQP_NOALLOC_MAX_TRAJ rows (about 2.3 MiB), which every GPU that
+ * loads the library holds until the process exits; n above that limit is
+ * rejected with BQP_E_ARG before any device work.  The call makes no
+ * cudaMalloc, cudaFree or host-pinning call; the context (created earlier)
+ * holds the gravity table.
+ *
+ * The first call on a device looks up that array's device address (and loads
+ * the kernel), so make it during set-up, before any stream capture.  Every
+ * call on a device shares the array and the next call overwrites it.  Calls
+ * made through this library are serialised by a lock and each returns only
+ * after its stream has finished, so two such calls never overlap on the GPU;
+ * calls that did overlap (for example from two copies of the library in one
+ * process) would race on the array. */
+#define BQP_NOALLOC_MAX_TRAJ 16384
+int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in,
+                                int32_t input_equinoctial, const double* epoch_jd, double t0,
+                                const double* tf, const double* ballistic, double* out,
+                                int32_t* status, int64_t* steps, int64_t* evals);
+
 /* Sampled propagation on a common grid t_eval[n_t] (sorted, within
  * [t0, tf_i], containing t0 and tf_i as the reference's binding arranges,
  * lib.rs:277-290).  Replaces integrate_adaptive's rectified sampled path
