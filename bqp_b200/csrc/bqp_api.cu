@@ -301,8 +301,8 @@ int validate_cfg(const bqp_force_config* c) {
     if (!(c->max_kernel_seconds > 0.0)) return fail(BQP_E_ARG, "max_kernel_seconds must be > 0");
     if (c->engine != BQP_ENGINE_PIPELINE && c->engine != BQP_ENGINE_PERSISTENT)
         return fail(BQP_E_ARG, "unknown engine %d", c->engine);
-    if (c->gravity_threads < 0 || c->gravity_threads > 1024 || c->gravity_threads % 32)
-        return fail(BQP_E_ARG, "gravity_threads must be a multiple of 32 in 0..1024");
+    if (c->gravity_threads < 0 || c->gravity_threads > 256 || c->gravity_threads % 32)
+        return fail(BQP_E_ARG, "gravity_threads must be a multiple of 32 in 0..256");
     if (c->gravity_slots != 0 && c->gravity_slots != 1 && c->gravity_slots != 2 && c->gravity_slots != 4)
         return fail(BQP_E_ARG, "gravity_slots must be 0, 1, 2 or 4");
     return 0;
@@ -578,7 +578,7 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->max_kernel_seconds = 600.0;
     c->engine = BQP_ENGINE_PIPELINE;
     c->gravity_threads = 256;
-    c->gravity_slots = 2;
+    c->gravity_slots = 4;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }

@@ -94,12 +94,37 @@ BQP_HD void gravity_field(const double* __restrict__ tab, int order, double px, 
     acc[2] = az;
 }
 
-// NT trajectories per thread: every table read (four 16-byte broadcast loads
-// per cell) feeds NT independent recursions, which divides the shared-memory
-// traffic per trajectory by NT and gives the FP64 pipe NT-way ILP.
+// Index of the first cell of column j (columns hold rows j..order+1).
+BQP_HD int gravity_col_offset(int order, int j) {
+    const int rows0 = order + 2;  // cells in column 0
+    return j * rows0 - j * (j - 1) / 2;
+}
+
+// First column of part p when the columns are cut into `parts` runs of about
+// equal cell count (p = parts gives order + 2, one past the last column).
+BQP_HD int gravity_part_column(int order, int p, int parts) {
+    const int ncol = order + 2;
+    if (p <= 0) return 0;
+    if (p >= parts) return ncol;
+    const long long target = (long long)gravity_cells(order) * p / parts;
+    int j = 0;
+    long long cells = 0;
+    while (j < ncol && cells + (ncol - j) <= target) cells += ncol - j++;
+    return j;
+}
+
+// Partial field of columns [j0, j1) for NT trajectories per thread.  Every
+// table read (four 16-byte loads per cell, the same address in every lane)
+// feeds NT independent recursions: the loads move 64 bytes per cell into
+// every lane's registers, so sharing them over NT trajectories is what keeps
+// the FP64 pipe, not the shared-memory data path, the limit.  The diagonal
+// V/W recursion is first carried (without accumulation) through columns
+// 1..j0-1, so a part that starts at j0 > 0 needs nothing from another part.
+// Interior cells are read two at a time and the next pair is loaded before
+// the current one is used.
 template <int NT>
-BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const double* px,
-                                                    const double* py, const double* pz, double (*acc)[3]) {
+BQP_HD void gravity_columns(const double* __restrict__ tab, int order, int j0, int j1, const double* px,
+                            const double* py, const double* pz, double (*acc)[3]) {
     double xc[NT], yc[NT], zc[NT], c2re[NT], vd[NT], wd[NT], ax[NT], ay[NT], az[NT];
 #pragma unroll
     for (int q = 0; q < NT; ++q) {
@@ -114,8 +139,19 @@ BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const
         ax[q] = ay[q] = az[q] = 0.0;
     }
     const int last = order + 1;
-    const double2* cell = reinterpret_cast<const double2*>(tab);
-    for (int j = 0; j <= last; ++j) {
+    const double2* tab2 = reinterpret_cast<const double2*>(tab);
+    for (int j = 1; j < j0; ++j) {
+        const double a = tab2[(size_t)gravity_col_offset(order, j) * 4].x;
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            const double nv = a * fma(xc[q], vd[q], -yc[q] * wd[q]);
+            const double nw = a * fma(xc[q], wd[q], yc[q] * vd[q]);
+            vd[q] = nv;
+            wd[q] = nw;
+        }
+    }
+    const double2* cell = tab2 + (size_t)gravity_col_offset(order, j0) * 4;
+    for (int j = j0; j < j1; ++j) {
         {
             const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
 #pragma unroll
@@ -149,30 +185,41 @@ BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const
             }
             cell += 4;
         }
-        // interior rows, two per iteration so the row registers rotate
-        // without moves
-        int l = j + 2;
-        for (; l + 1 <= last; l += 2) {
-            const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
-            const double2 ab2 = cell[4], wx2 = cell[5], wy2 = cell[6], wz2 = cell[7];
+        // interior rows j+2..last, two per iteration (the row registers
+        // rotate without moves); the next pair is in flight meanwhile
+        const int pairs = (last - j - 1) >> 1;
+        double2 nx[8];
+        if (pairs > 0) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) nx[i] = cell[i];
+        }
+#pragma unroll 2
+        for (int p = 0; p < pairs; ++p) {
+            double2 cb[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) cb[i] = nx[i];
+            if (p + 1 < pairs) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) nx[i] = cell[8 + i];
+            }
 #pragma unroll
             for (int q = 0; q < NT; ++q) {
-                const double ta = ab.x * zc[q], tb = ab.y * c2re[q];
+                const double ta = cb[0].x * zc[q], tb = cb[0].y * c2re[q];
                 v0[q] = fma(ta, v1[q], -tb * v0[q]);
                 w0[q] = fma(ta, w1[q], -tb * w0[q]);
-                ax[q] = fma(wx.x, v0[q], fma(wx.y, w0[q], ax[q]));
-                ay[q] = fma(wy.x, v0[q], fma(wy.y, w0[q], ay[q]));
-                az[q] = fma(wz.x, v0[q], fma(wz.y, w0[q], az[q]));
-                const double ta2 = ab2.x * zc[q], tb2 = ab2.y * c2re[q];
+                ax[q] = fma(cb[1].x, v0[q], fma(cb[1].y, w0[q], ax[q]));
+                ay[q] = fma(cb[2].x, v0[q], fma(cb[2].y, w0[q], ay[q]));
+                az[q] = fma(cb[3].x, v0[q], fma(cb[3].y, w0[q], az[q]));
+                const double ta2 = cb[4].x * zc[q], tb2 = cb[4].y * c2re[q];
                 v1[q] = fma(ta2, v0[q], -tb2 * v1[q]);
                 w1[q] = fma(ta2, w0[q], -tb2 * w1[q]);
-                ax[q] = fma(wx2.x, v1[q], fma(wx2.y, w1[q], ax[q]));
-                ay[q] = fma(wy2.x, v1[q], fma(wy2.y, w1[q], ay[q]));
-                az[q] = fma(wz2.x, v1[q], fma(wz2.y, w1[q], az[q]));
+                ax[q] = fma(cb[5].x, v1[q], fma(cb[5].y, w1[q], ax[q]));
+                ay[q] = fma(cb[6].x, v1[q], fma(cb[6].y, w1[q], ay[q]));
+                az[q] = fma(cb[7].x, v1[q], fma(cb[7].y, w1[q], az[q]));
             }
             cell += 8;
         }
-        if (l <= last) {
+        if ((last - j - 1) & 1) {
             const double2 ab = cell[0], wx = cell[1], wy = cell[2], wz = cell[3];
 #pragma unroll
             for (int q = 0; q < NT; ++q) {
@@ -192,6 +239,13 @@ BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const
         acc[q][1] = ay[q];
         acc[q][2] = az[q];
     }
+}
+
+// The whole field for NT trajectories per thread.
+template <int NT>
+BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const double* px, const double* py,
+                                const double* pz, double (*acc)[3]) {
+    gravity_columns<NT>(tab, order, 0, order + 2, px, py, pz, acc);
 }
 
 }  // namespace bqp

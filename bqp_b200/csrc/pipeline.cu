@@ -25,6 +25,7 @@
 #include <chrono>
 #include <cstdint>
 
+#include "gravity_cta.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 #include "traj.cuh"
@@ -184,52 +185,35 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
 // Persistent over slots: one CTA per SM stages the field table once; the
 // CTA's contiguous slot range is walked NT slots per thread.
 template <int NT>
-__global__ void pl_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem, PipeBufs P,
-                           int cur) {
+__global__ void __launch_bounds__(256, 1) pl_gravity(const double* __restrict__ gtab, int order, int ncells,
+                                                     int use_smem, int parts_max, PipeBufs P, int cur) {
     const int count = P.count[cur];
     const int per_block = (count + gridDim.x - 1) / gridDim.x;
     const int b0 = blockIdx.x * per_block;
     const int b1 = min(count, b0 + per_block);
     if (b0 >= b1) return;  // uniform across the CTA
-    const double* tab = stage_table(gtab, ncells, use_smem != 0);
-    for (int base = b0; base < b1; base += blockDim.x * NT) {
-        double px[NT], py[NT], pz[NT], a[NT][3];
-        int slot[NT];
-        bool on[NT];
-#pragma unroll
-        for (int q = 0; q < NT; ++q) {
-            slot[q] = base + q * blockDim.x + threadIdx.x;
-            on[q] = slot[q] < b1 && !P.skip[slot[q]];
-            px[q] = 7000.0;  // a valid dummy position for idle lanes
-            py[q] = 0.0;
-            pz[q] = 0.0;
-            if (on[q]) {
-                const int sl = slot[q];
-                const double s = P.sc[sl], c = P.sc[P.cap + sl];
-                const double x = P.sp[sl], y = P.sp[P.cap + sl], z = P.sp[2 * P.cap + sl];
-                const double qx = fma(c, x, s * y), qy = fma(-s, x, c * y);
-                const double r2 = fma(qx, qx, fma(qy, qy, z * z));
-                if (!(isfinite(r2) && r2 > 0.0)) {
-                    P.bad[sl] = 1;
-                    P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
-                    on[q] = false;
-                } else {
-                    px[q] = qx;
-                    py[q] = qy;
-                    pz[q] = z;
-                }
-            }
+    auto load = [&](int sl, double& x, double& y, double& z) -> bool {
+        if (P.skip[sl]) return false;
+        const double s = P.sc[sl], c = P.sc[P.cap + sl];
+        const double ex = P.sp[sl], ey = P.sp[P.cap + sl], ez = P.sp[2 * P.cap + sl];
+        const double qx = fma(c, ex, s * ey), qy = fma(-s, ex, c * ey);
+        const double r2 = fma(qx, qx, fma(qy, qy, ez * ez));
+        if (!(isfinite(r2) && r2 > 0.0)) {
+            P.bad[sl] = 1;
+            P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
+            return false;
         }
-        gravity_field_multi<NT>(tab, order, px, py, pz, a);
-#pragma unroll
-        for (int q = 0; q < NT; ++q) {
-            if (!on[q]) continue;
-            const int sl = slot[q];
-            P.agrav[sl] = a[q][0];
-            P.agrav[P.cap + sl] = a[q][1];
-            P.agrav[2 * P.cap + sl] = a[q][2];
-        }
-    }
+        x = qx;
+        y = qy;
+        z = ez;
+        return true;
+    };
+    auto store = [&](int sl, const double* a, double, double, double) {
+        P.agrav[sl] = a[0];
+        P.agrav[P.cap + sl] = a[1];
+        P.agrav[2 * P.cap + sl] = a[2];
+    };
+    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, b0, b1, load, store);
 }
 
 // --------------------------------------------------------------------- drag
@@ -398,9 +382,18 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
     const int dblocks2 = (int)((A.n * 2 + kBlock - 1) / kBlock);
     const int dblocks4 = (int)((A.n * 4 + kBlock - 1) / kBlock);
-    const size_t smem = A.use_smem ? (size_t)A.ncells * kCellDoubles * sizeof(double) : 0;
-    const int nt = gslots == 1 || gslots == 4 ? gslots : 2;
-    auto gker = nt == 1 ? pl_gravity<1> : (nt == 4 ? pl_gravity<4> : pl_gravity<2>);
+    const int nt = gslots == 1 || gslots == 2 ? gslots : 4;
+    auto gker = nt == 1 ? pl_gravity<1> : (nt == 2 ? pl_gravity<2> : pl_gravity<4>);
+    if (gthreads > 256) gthreads = 256;
+    if (gthreads < 32) gthreads = 32;
+    gthreads = gthreads / 32 * 32;
+    // column groups need room for their partial sums next to the table
+    int gparts = kGravityPartsMax;
+    size_t smem = gravity_smem_bytes(A.ncells, A.use_smem != 0, gthreads, nt, gparts);
+    if (smem > kSmemPerBlock) {
+        gparts = 1;
+        smem = gravity_smem_bytes(A.ncells, A.use_smem != 0, gthreads, nt, gparts);
+    }
     cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     // one CTA per SM (the table fills shared memory); each takes an equal
@@ -432,7 +425,8 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
             if (A.force.drag) cudaMemsetAsync(P.dcount, 0, 2 * sizeof(int32_t), st);
             pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s);
             if (A.force.gravity_on)
-                gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, P, cur);
+                gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, gparts, P,
+                                                      cur);
             if (A.force.drag) {
                 pl_drag<2><<<dblocks2, kBlock, 0, st>>>(A.force, P, 0);
                 pl_drag<4><<<dblocks4, kBlock, 0, st>>>(A.force, P, 1);

@@ -11,6 +11,7 @@
 
 #include <cstdint>
 
+#include "gravity_cta.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 #include "traj.cuh"
@@ -19,54 +20,43 @@ namespace bqp {
 
 // ----------------------------------------------------------------- kernels
 template <int NT>
-__global__ void k_gravity(const double* __restrict__ gtab, int order, int ncells, int use_smem, int64_t n,
-                          const double* __restrict__ pos, double* __restrict__ acc, int32_t* __restrict__ status) {
+__global__ void __launch_bounds__(256, 1) k_gravity(const double* __restrict__ gtab, int order, int ncells,
+                                                    int use_smem, int parts_max, int64_t n,
+                                                    const double* __restrict__ pos, double* __restrict__ acc,
+                                                    int32_t* __restrict__ status) {
+    // rows are int-indexed inside a CTA: the launcher keeps each CTA's range
+    // below 2^31 by running chunks
     const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
-    const int64_t b0 = (int64_t)blockIdx.x * per_block;
-    const int64_t b1 = b0 + per_block < n ? b0 + per_block : n;
-    if (b0 >= b1) return;  // uniform across the CTA
-    const double* tab = stage_table(gtab, ncells, use_smem != 0);
-    for (int64_t base = b0; base < b1; base += (int64_t)blockDim.x * NT) {
-        double px[NT], py[NT], pz[NT], a[NT][3];
-        int64_t idx[NT];
-        bool on[NT];
-#pragma unroll
-        for (int q = 0; q < NT; ++q) {
-            idx[q] = base + (int64_t)q * blockDim.x + threadIdx.x;
-            on[q] = idx[q] < b1;
-            px[q] = 7000.0;
-            py[q] = 0.0;
-            pz[q] = 0.0;
-            if (on[q]) {
-                const int64_t i = idx[q];
-                const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-                const double r2 = fma(x, x, fma(y, y, z * z));
-                if (!(isfinite(r2) && r2 > 0.0)) {
-                    acc[3 * i] = acc[3 * i + 1] = acc[3 * i + 2] = NAN;
-                    if (status) status[i] = kGravityRadius;
-                    on[q] = false;
-                } else {
-                    px[q] = x;
-                    py[q] = y;
-                    pz[q] = z;
-                }
-            }
+    const int64_t c0 = (int64_t)blockIdx.x * per_block;
+    const int64_t c1 = c0 + per_block < n ? c0 + per_block : n;
+    if (c0 >= c1) return;  // uniform across the CTA
+    const double* p0 = pos + 3 * c0;
+    double* a0 = acc + 3 * c0;
+    int32_t* s0 = status ? status + c0 : nullptr;
+    auto load = [&](int i, double& x, double& y, double& z) -> bool {
+        const double ex = p0[3 * i], ey = p0[3 * i + 1], ez = p0[3 * i + 2];
+        const double r2 = fma(ex, ex, fma(ey, ey, ez * ez));
+        if (!(isfinite(r2) && r2 > 0.0)) {
+            a0[3 * i] = a0[3 * i + 1] = a0[3 * i + 2] = NAN;
+            if (s0) s0[i] = kGravityRadius;
+            return false;
         }
-        gravity_field_multi<NT>(tab, order, px, py, pz, a);
-#pragma unroll
-        for (int q = 0; q < NT; ++q) {
-            if (!on[q]) continue;
-            const int64_t i = idx[q];
-            // add the C00 point mass back: the full field of the reference's
-            // spherical_gravity_impl_frame_packed (gravity.rs:2638-2675)
-            const double r2 = fma(px[q], px[q], fma(py[q], py[q], pz[q] * pz[q]));
-            const double k = kMu / (r2 * sqrt(r2));
-            acc[3 * i] = fma(-k, px[q], a[q][0]);
-            acc[3 * i + 1] = fma(-k, py[q], a[q][1]);
-            acc[3 * i + 2] = fma(-k, pz[q], a[q][2]);
-            if (status) status[i] = kOk;
-        }
-    }
+        x = ex;
+        y = ey;
+        z = ez;
+        return true;
+    };
+    auto store = [&](int i, const double* a, double x, double y, double z) {
+        // add the C00 point mass back: the full field of the reference's
+        // spherical_gravity_impl_frame_packed (gravity.rs:2638-2675)
+        const double r2 = fma(x, x, fma(y, y, z * z));
+        const double k = kMu / (r2 * sqrt(r2));
+        a0[3 * i] = fma(-k, x, a[0]);
+        a0[3 * i + 1] = fma(-k, y, a[1]);
+        a0[3 * i + 2] = fma(-k, z, a[2]);
+        if (s0) s0[i] = kOk;
+    };
+    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, 0, (int)(c1 - c0), load, store);
 }
 
 __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem, ForceParams fp,
@@ -213,17 +203,33 @@ cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_sm
                            const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads,
                            int slots) {
     if (n <= 0) return cudaSuccess;
-    const size_t smem = use_smem ? (size_t)ncells * kCellDoubles * sizeof(double) : 0;
-    const int nt = slots == 1 || slots == 4 ? slots : 2;
-    auto ker = nt == 1 ? k_gravity<1> : (nt == 4 ? k_gravity<4> : k_gravity<2>);
+    const int nt = slots == 1 || slots == 2 ? slots : 4;
+    auto ker = nt == 1 ? k_gravity<1> : (nt == 2 ? k_gravity<2> : k_gravity<4>);
+    if (threads <= 0 || threads > 256) threads = 256;
+    if (threads < 32) threads = 32;
+    threads = threads / 32 * 32;
+    int parts = kGravityPartsMax;
+    size_t smem = gravity_smem_bytes(ncells, use_smem != 0, threads, nt, parts);
+    if (smem > kSmemPerBlock) {
+        parts = 1;
+        smem = gravity_smem_bytes(ncells, use_smem != 0, threads, nt, parts);
+    }
     cudaError_t e = cudaFuncSetAttribute(ker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (threads <= 0) threads = 256;
-    int64_t blocks = (n + (int64_t)threads * nt - 1) / ((int64_t)threads * nt);
-    const int64_t cap = (int64_t)sm_count() * (use_smem ? 1 : 4);
-    if (blocks > cap) blocks = cap;
-    ker<<<(unsigned)blocks, threads, smem, st>>>(gtab, order, ncells, use_smem, n, pos, acc, status);
-    return cudaGetLastError();
+    // one CTA per SM; each takes an equal share of the rows.  Chunks of at
+    // most 2^30 rows keep a CTA's share int-indexed.
+    const int64_t grid_cap = (int64_t)sm_count();
+    const int64_t chunk = (int64_t)1 << 30;
+    for (int64_t off = 0; off < n; off += chunk) {
+        const int64_t m = n - off < chunk ? n - off : chunk;
+        int64_t blocks = (m + 32 * nt - 1) / (32 * nt);
+        if (blocks > grid_cap) blocks = grid_cap;
+        ker<<<(unsigned)blocks, threads, smem, st>>>(gtab, order, ncells, use_smem, parts, m, pos + 3 * off,
+                                                     acc + 3 * off, status ? status + off : nullptr);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,

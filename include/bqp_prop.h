@@ -88,8 +88,8 @@ typedef struct bqp_force_config {
     double max_kernel_seconds; /* watchdog: wall-clock limit of one propagation call (> 0);
                                   rows not finished by then end with BQP_ST_WATCHDOG */
     int32_t engine;            /* BQP_ENGINE_* */
-    int32_t gravity_threads;   /* threads per CTA of the gravity kernels (0: 256) */
-    int32_t gravity_slots;     /* trajectories per thread in the gravity kernels: 1, 2 or 4 (0: 2) */
+    int32_t gravity_threads;   /* threads per CTA of the gravity kernels, 32..256 (0: 256) */
+    int32_t gravity_slots;     /* trajectories per thread in the gravity kernels: 1, 2 or 4 (0: 4) */
     int32_t drag_quadrature;   /* 1: always walk the JB2008 Boole quadrature; 0: use the
                                   Chebyshev fits of its fixed-node sweeps where they apply */
 } bqp_force_config;
