@@ -13,13 +13,15 @@ call's output exactly as the reference's segment loop does
 (integrator.rs:3418-3560).  Metric: force (RHS) evaluations per second, counted
 by the device per trajectory.
 
-  value  device-resident inputs, k_propagate timed with CUDA events
+  value  device-resident inputs, each step timed with CUDA events
   e2e    the same steps through the host-buffer C ABI call
          (bqp_propagate_final): H2D of the inputs and D2H of the results
          inside the timed region
-  roofline  FP64: algorithmic flops = force evals x F(70) (the reference
-         gravity algorithm's flop count, F(N) = 9(N+2)(N+3)/2 + 13N(N+1) +
-         9(N+1) + 60, FMA = 2), peak = cuBLAS DGEMM measured in this run
+  roofline  the gravity kernel (pl_gravity), FP64: algorithmic flops =
+         force evals x F(70) (the reference gravity algorithm's flop count,
+         F(N) = 9(N+2)(N+3)/2 + 13N(N+1) + 9(N+1) + 60, FMA = 2) over the
+         kernel's summed CUDA-event time in the timed steps; peak = cuBLAS
+         DGEMM measured in this run
   cpu_baseline  the C++ oracle (restatement of the reference CPU path) on a
          bounded sample, all host cores
 
@@ -200,6 +202,19 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ ours
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu
+# capture (profiles/pl_gravity_70x70.md: 37,888 rows, one launch), scaled by
+# the rows one launch of this run processes.
+TRAFFIC_CAPTURE = {"gravity": (1895424.0, 37888)}
+
+
+def traffic_per_launch(kernel: str, rows: int):
+    if kernel not in TRAFFIC_CAPTURE:
+        return None
+    b, r = TRAFFIC_CAPTURE[kernel]
+    return b * rows / r
+
+
 def fp64_peak_tflops(torch, dev):
     """Measured FP64 peak: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
@@ -253,7 +268,7 @@ def run_ours(args):
         d_steps = torch.empty(n, device=dev, dtype=torch.int64)
         d_evals = torch.empty(n, device=dev, dtype=torch.int64)
         flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
-    epochs = [epoch + k * seg / 86400.0 for k in range(args.warmup + args.steps + 1)]
+    epochs = [epoch + k * seg / 86400.0 for k in range(args.warmup + 2 * args.steps + 1)]
     d_epochs = [torch.full((n,), e, device=dev, dtype=torch.float64) for e in epochs]
     torch.cuda.synchronize()
 
@@ -295,6 +310,23 @@ def run_ours(args):
         stream.synchronize()
     torch.cuda.synchronize()
     elapsed_ms = e_start.elapsed_time(e_end)
+    # kernel attribution: the same K steps again (continuing the arc) with a
+    # CUDA event on each side of every kernel launch; kept out of the pass
+    # above because the events cost about 8% of the step time
+    ctx.profile(True)
+    with torch.cuda.stream(stream):
+        prof_evals = torch.zeros((), device=dev, dtype=torch.int64)
+    for k in range(args.warmup + args.steps, args.warmup + 2 * args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        step(k, src, dst)
+        with torch.cuda.stream(stream):
+            prof_evals += d_evals.sum()
+        src, dst = dst, src
+    stream.synchronize()
+    ktimes = ctx.profile_read()
+    ctx.profile(False)
+    prof_evals = int(prof_evals.item())
     kernel_ms = [a.elapsed_time(b) for a, b in events]
     status_last = d_status.cpu().numpy()
     total_evals = int(evals_acc.item())
@@ -358,8 +390,17 @@ def run_ours(args):
     if rank == 0:
         peak = fp64_peak_tflops(torch, dev)
         fN = f_of_n(ORDER)
-        mean_kernel_ms = sum(kernel_ms) / len(kernel_ms)
-        achieved = (total_evals / len(kernel_ms)) * fN / (mean_kernel_ms * 1e-3) / 1e12
+        # dominant kernel: the gravity stage; every force evaluation is one
+        # gravity evaluation, F(70) algorithmic flops each
+        dom = "persistent" if args.engine == "persistent" else "gravity"
+        dom_ms, dom_launches = ktimes[dom]
+        achieved = prof_evals * fN / (dom_ms * 1e-3) / 1e12
+        step_tflops = total_evals * fN / (t_max * 1e-3) / 1e12
+        kernel_shares = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / max(1e-9, sum(
+            x[0] for x in ktimes.values())), 4)} for k, v in ktimes.items() if v[1]}
+        # kernels of the K profiled steps (plus one init kernel per step),
+        # the same launch sequence as the timed steps
+        launches = sum(v[1] for v in ktimes.values()) + (args.steps if args.engine == "pipeline" else 0)
         cpu = None
         if not args.no_cpu and world >= 1:
             threads = os.cpu_count() or 1
@@ -378,13 +419,19 @@ def run_ours(args):
                        "trajectory_days_per_s": world * n * seg / 86400.0 / (t_max * 1e-3 / args.steps)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic_per_launch(dom, n),
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
                                         "MEASURED_PEAKS.json)",
-                         "flops_per_eval": fN, "kernel": "k_propagate<DOP853>"},
+                         "flops_per_eval": fN,
+                         "kernel": "pl_gravity<4>" if dom == "gravity" else "k_propagate<DOP853>",
+                         "kernel_ms": dom_ms, "kernel_launches": dom_launches,
+                         "kernel_timing": "second pass of the K steps with a CUDA event on each side of "
+                                          "every launch",
+                         "whole_step_tflops": step_tflops, "whole_step_frac": step_tflops / peak,
+                         "kernels": kernel_shares},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "status_ok_fraction": float((status_last == 0).mean()),
         }
         print(json.dumps(line), flush=True)

@@ -34,6 +34,7 @@ ENGINES = {"pipeline": 0, "persistent": 1}
 
 E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5
 NOALLOC_MAX_TRAJ = 16384  # BQP_NOALLOC_MAX_TRAJ
+KERNEL_CLASSES = ("prep", "gravity", "drag", "control", "persistent")  # BQP_KCLASS_*
 
 
 class ForceConfig(C.Structure):
@@ -69,6 +70,8 @@ SIGNATURES = [
     ("bqp_ctx_info", C.c_int, [_vp, _lp]),
     ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
+    ("bqp_ctx_profile", C.c_int, [_vp, C.c_int32]),
+    ("bqp_ctx_profile_read", C.c_int, [_vp, _dp, _lp]),
     ("bqp_gravity_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _ip]),
     ("bqp_gravity_eval_device", C.c_int, [_vp, C.c_int64, _vp, _vp, _vp]),
     ("bqp_rhs_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
@@ -180,6 +183,17 @@ class Context:
     def set_config(self, cfg: ForceConfig):
         check(lib().bqp_ctx_set_config(self._h, C.byref(cfg)))
         self.cfg = cfg
+
+    def profile(self, on: bool = True):
+        """Start (clearing the totals) or stop kernel timing by class."""
+        check(lib().bqp_ctx_profile(self._h, int(bool(on))))
+
+    def profile_read(self):
+        """{class: (ms, launches)} since profiling was switched on."""
+        ms = np.zeros(len(KERNEL_CLASSES))
+        n = np.zeros(len(KERNEL_CLASSES), dtype=np.int64)
+        check(lib().bqp_ctx_profile_read(self._h, dptr(ms), lptr(n)))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_CLASSES)}
 
     def set_stream(self, stream_ptr: int):
         check(lib().bqp_ctx_set_stream(self._h, _vp(stream_ptr)))

@@ -269,6 +269,8 @@ struct bqp_ctx {
     size_t pws_bytes = 0;
     jb::JbFit* d_fit = nullptr;  // JB2008 fixed-node sweep fits (device)
     double fit_worst = -1.0;
+    bool profile = false;  // kernel timing on (bqp_ctx_profile)
+    KernelTimes times{};
 };
 
 namespace {
@@ -434,13 +436,31 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
         PipeBufs P{};
         pipeline_carve(P, ctx->d_pws, n);
         cudaError_t e = launch_pipeline(A, P, ctx->cfg.method, ctx->stream, ctx->cfg.max_kernel_seconds,
-                                        ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
+                                        ctx->cfg.gravity_threads, ctx->cfg.gravity_slots,
+                                        ctx->profile ? &ctx->times : nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "pipeline");
         return 0;
     }
     cudaError_t e = cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (ctx->profile) {
+        cudaEventCreate(&ev[0]);
+        cudaEventCreate(&ev[1]);
+        cudaEventRecord(ev[0], ctx->stream);
+    }
     e = launch_propagate(A, ctx->cfg.method, 256, 0, ctx->stream);
+    if (ctx->profile) {
+        cudaEventRecord(ev[1], ctx->stream);
+        float ms = 0.0f;
+        if (e == cudaSuccess && cudaEventSynchronize(ev[1]) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) {
+            ctx->times.ms[kKcPersistent] += ms;
+            ctx->times.launches[kKcPersistent] += 1;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "k_propagate launch");
     return 0;
 }
@@ -656,6 +676,22 @@ int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info) {
 int bqp_ctx_info_fit(const bqp_ctx* ctx, double* worst_rel) {
     if (!ctx || !worst_rel) return fail(BQP_E_ARG, "null argument");
     *worst_rel = ctx->d_fit ? ctx->fit_worst : -1.0;
+    return 0;
+}
+
+int bqp_ctx_profile(bqp_ctx* ctx, int32_t on) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    ctx->profile = on != 0;
+    if (ctx->profile) ctx->times = KernelTimes{};
+    return 0;
+}
+
+int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches) {
+    if (!ctx || !ms || !launches) return fail(BQP_E_ARG, "null argument");
+    for (int i = 0; i < kKcCount; ++i) {
+        ms[i] = ctx->times.ms[i];
+        launches[i] = ctx->times.launches[i];
+    }
     return 0;
 }
 

@@ -10,10 +10,60 @@
 // groups' partial sums are added in shared memory in a fixed order.
 #pragma once
 #include "gravity.cuh"
+#include "kernels.cuh"
 
 namespace bqp {
 
-constexpr size_t kSmemPerBlock = 227 * 1024;  // opt-in dynamic shared memory per CTA
+// opt-in shared memory per CTA, less room for the static mbarrier
+constexpr size_t kSmemPerBlock = 227 * 1024 - 64;
+constexpr uint64_t kStageWaitNs = 1000000000ull;  // 1 s bound on the table copy
+
+// Copy `bytes` (a multiple of 16; both addresses 16-byte aligned) from global
+// to shared memory with the bulk-copy engine, completion signalled on an
+// mbarrier.  Thread 0 issues the copy; every thread waits for at most
+// kStageWaitNs; all get false if any thread saw the copy unfinished then.
+__device__ __forceinline__ bool bulk_stage(void* smem_dst, const void* gsrc, uint32_t bytes) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&bar);
+    const uint32_t dst_a = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t state;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                     : "=l"(state)
+                     : "r"(bar_a), "r"(bytes)
+                     : "memory");
+        (void)state;
+        constexpr uint32_t kChunk = 32768;
+        for (uint32_t off = 0; off < bytes; off += kChunk) {
+            const uint32_t n = bytes - off < kChunk ? bytes - off : kChunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    dst_a + off),
+                "l"(static_cast<const char*>(gsrc) + off), "r"(n), "r"(bar_a)
+                : "memory");
+        }
+    }
+    uint32_t done = 0;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, "
+            "p;\n\t}"
+            : "=r"(done)
+            : "r"(bar_a)
+            : "memory");
+        if (done) break;
+        if ((it & 255u) == 255u && global_ns() - t0 > kStageWaitNs) break;
+    }
+    // one verdict for the whole CTA (a thread may give up just before the
+    // copy lands while another sees it land)
+    return !__syncthreads_or(done == 0);
+}
 constexpr int kGravityPartsMax = 4;
 
 struct GravLayout {
@@ -44,19 +94,18 @@ inline size_t gravity_smem_bytes(int ncells, bool table_in_smem, int block, int 
 // position and returns false for a row to leave out (it records that row's
 // outcome itself; every group calls it, so it must be idempotent).
 // store(i, a, x, y, z) receives the field of row i (group 0 only).
-template <int NT, class Load, class Store>
+// lost(i) records that row i got no field because the table copy did not
+// complete in time.
+template <int NT, class Load, class Store, class Lost>
 __device__ __forceinline__ void gravity_cta(const double* __restrict__ gtab, int order, int ncells, bool table_in_smem,
-                                            int parts_max, int b0, int b1, Load load, Store store) {
+                                            int parts_max, int b0, int b1, Load load, Store store, Lost lost) {
     extern __shared__ __align__(16) double smem_dyn[];
     const GravLayout L = gravity_layout(b1 - b0, NT, blockDim.x, parts_max);
-    if (table_in_smem) {
-        const int nvec = ncells * (kCellDoubles / 2);
-        const double2* src = reinterpret_cast<const double2*>(gtab);
-        double2* dst = reinterpret_cast<double2*>(smem_dyn);
-        for (int i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = __ldg(src + i);
+    if (table_in_smem && !bulk_stage(smem_dyn, gtab, (uint32_t)ncells * kCellDoubles * sizeof(double))) {
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) lost(i);
+        return;  // the verdict is the same in every thread
     }
     double* red = smem_dyn + (table_in_smem ? (size_t)ncells * kCellDoubles : 0);
-    __syncthreads();
     const int part = threadIdx.x / L.tpart;
     const int tid = threadIdx.x - part * L.tpart;
     const bool member = part < L.parts;

@@ -59,14 +59,23 @@ struct PipeBufs {
     int32_t* dcount;      // [2]
 };
 
+// Kernel durations by class, summed from CUDA events recorded around each
+// launch (instrumentation; null when off).
+enum KernelClass { kKcPrep = 0, kKcGravity = 1, kKcDrag = 2, kKcControl = 3, kKcPersistent = 4, kKcCount = 5 };
+struct KernelTimes {
+    double ms[kKcCount];
+    int64_t launches[kKcCount];
+};
+
 size_t pipeline_bytes(int64_t cap);
 void pipeline_carve(PipeBufs& P, void* base, int64_t cap);
 cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st,
-                            double max_seconds, int gravity_threads, int gravity_slots);
+                            double max_seconds, int gravity_threads, int gravity_slots,
+                            KernelTimes* times = nullptr);
 
 cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
                            const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads = 256,
-                           int slots = 2);
+                           int slots = 4);
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,
                        const double* equ, const double* seg_t0, const double* jd0, const double* t,
                        const double* delta, const double* ballistic, double am0, double cd0,

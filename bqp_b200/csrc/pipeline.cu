@@ -24,6 +24,7 @@
 
 #include <chrono>
 #include <cstdint>
+#include <vector>
 
 #include "gravity_cta.cuh"
 #include "kernels.cuh"
@@ -213,7 +214,11 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(const double* __restrict__ 
         P.agrav[P.cap + sl] = a[1];
         P.agrav[2 * P.cap + sl] = a[2];
     };
-    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, b0, b1, load, store);
+    auto lost = [&](int sl) {
+        P.bad[sl] = 2;
+        P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
+    };
+    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, b0, b1, load, store, lost);
 }
 
 // --------------------------------------------------------------------- drag
@@ -297,7 +302,7 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
         int32_t code = -1;
         const int32_t d = attempt_decide<M>(A, s, k0, ynext, err, err3, &en, &code);
         if (P.bad[slot]) {
-            traj_fail(A, s, traj, kGravityRadius);
+            traj_fail(A, s, traj, P.bad[slot] == 2 ? kWatchdog : kGravityRadius);
         } else if (d == kFail) {
             traj_fail(A, s, traj, code);
         } else if (d == kAccept) {
@@ -375,7 +380,7 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
 
 template <int M>
 static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, double max_seconds,
-                       int gthreads, int gslots) {
+                       int gthreads, int gslots, KernelTimes* times) {
     using T = Tab<M>;
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
@@ -419,20 +424,51 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     cudaMemsetAsync(P.count, 0, 2 * sizeof(int32_t), st);
     pl_init<M><<<blocks, kBlock, 0, st>>>(A, P);
 
+    // instrumentation: an event-record node on each side of every timed
+    // kernel of the graph; the host sums the durations after each replay
+    std::vector<cudaEvent_t> evs;
+    std::vector<int> ev_class;  // class of the kernel between evs[2i] and evs[2i+1]
+    auto timed = [&](int cls, auto&& launch) {
+        if (!times) {
+            launch();
+            return;
+        }
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecordWithFlags(a, st, cudaEventRecordExternal);
+        launch();
+        cudaEventRecordWithFlags(b, st, cudaEventRecordExternal);
+        evs.push_back(a);
+        evs.push_back(b);
+        ev_class.push_back(cls);
+    };
     // one graph = two attempts (active list 0 -> 1 -> 0)
     auto enqueue_attempt = [&](int cur, int timed_out) {
         for (int s = 0; s < stages; ++s) {
             if (A.force.drag) cudaMemsetAsync(P.dcount, 0, 2 * sizeof(int32_t), st);
-            pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s);
+            timed(kKcPrep, [&] { pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s); });
             if (A.force.gravity_on)
-                gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, gparts, P,
-                                                      cur);
-            if (A.force.drag) {
-                pl_drag<2><<<dblocks2, kBlock, 0, st>>>(A.force, P, 0);
-                pl_drag<4><<<dblocks4, kBlock, 0, st>>>(A.force, P, 1);
+                timed(kKcGravity, [&] {
+                    gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, gparts, P,
+                                                          cur);
+                });
+            if (A.force.drag)
+                timed(kKcDrag, [&] {
+                    pl_drag<2><<<dblocks2, kBlock, 0, st>>>(A.force, P, 0);
+                    pl_drag<4><<<dblocks4, kBlock, 0, st>>>(A.force, P, 1);
+                });
+        }
+        timed(kKcControl, [&] { pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out); });
+    };
+    auto collect = [&]() {
+        for (size_t i = 0; i < ev_class.size(); ++i) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, evs[2 * i], evs[2 * i + 1]) == cudaSuccess) {
+                times->ms[ev_class[i]] += ms;
+                times->launches[ev_class[i]] += ev_class[i] == kKcDrag ? 2 : 1;
             }
         }
-        pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out);
     };
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -452,9 +488,19 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
         if (e != cudaSuccess) break;
         cudaMemcpyAsync(h_count, &P.count[0], sizeof(int32_t), cudaMemcpyDeviceToHost, st);
         cudaEventRecord(ev_cnt, st);
+        if (times) {
+            // no replay in flight while the events of this one are read
+            e = cudaEventSynchronize(ev_cnt);
+            if (e != cudaSuccess) break;
+            collect();
+        }
         e = cudaGraphLaunch(exec, st);  // speculative: cheap when nothing is active
         if (e != cudaSuccess) break;
         e = cudaEventSynchronize(ev_cnt);
+        if (times && e == cudaSuccess) {
+            e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) collect();
+        }
         replays += 2;
         if (*h_count == 0) done = true;
         const double elapsed =
@@ -472,6 +518,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     cudaFreeHost(h_count);
+    for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
     cudaEventDestroy(ev_in);
     cudaEventDestroy(ev_out);
     cudaEventDestroy(ev_cnt);
@@ -480,13 +527,14 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
 }
 
 cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cudaStream_t st, double max_seconds,
-                            int gravity_threads, int gravity_slots) {
+                            int gravity_threads, int gravity_slots, KernelTimes* times) {
     if (A.n <= 0) return cudaSuccess;
     if (gravity_threads <= 0) gravity_threads = 256;
     switch (method) {
-        case kDopri5: return run<kDopri5>(A, P, st, max_seconds, gravity_threads, gravity_slots);
-        case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads, gravity_slots);
-        case kDopri5Compat: return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads, gravity_slots);
+        case kDopri5: return run<kDopri5>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
+        case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
+        case kDopri5Compat:
+            return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -56,7 +56,11 @@ __global__ void __launch_bounds__(256, 1) k_gravity(const double* __restrict__ g
         a0[3 * i + 2] = fma(-k, z, a[2]);
         if (s0) s0[i] = kOk;
     };
-    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, 0, (int)(c1 - c0), load, store);
+    auto lost = [&](int i) {
+        a0[3 * i] = a0[3 * i + 1] = a0[3 * i + 2] = NAN;
+        if (s0) s0[i] = kWatchdog;
+    };
+    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, 0, (int)(c1 - c0), load, store, lost);
 }
 
 __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem, ForceParams fp,

@@ -124,6 +124,23 @@ int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info4);
 /* Worst relative error of the JB2008 sweep fits against the quadrature at
  * the check points (-1: no fit, the quadrature always runs). */
 int bqp_ctx_info_fit(const bqp_ctx* ctx, double* worst_rel);
+/* Kernel timing, for measurement; no counterpart in the reference.  With
+ * on != 0 the propagation calls of this context record a CUDA event on each
+ * side of every kernel launch and add up the durations by kernel class
+ * (BQP_KCLASS_*); the totals restart at zero.  While it is on, the
+ * stage-synchronous engine waits for each graph replay before queueing the
+ * next.  on == 0 stops recording and keeps the totals. */
+#define BQP_KCLASS_PREP 0       /* stage preparation (baseline, frame, third body) */
+#define BQP_KCLASS_GRAVITY 1    /* spherical-harmonic gravity */
+#define BQP_KCLASS_DRAG 2       /* JB2008 density and drag (both altitude lists) */
+#define BQP_KCLASS_CONTROL 3    /* step combination, error control, compaction */
+#define BQP_KCLASS_PERSISTENT 4 /* the persistent engine's single kernel */
+#define BQP_KCLASSES 5
+int bqp_ctx_profile(bqp_ctx* ctx, int32_t on);
+/* Totals since profiling was last switched on: ms[BQP_KCLASSES] kernel
+ * milliseconds, launches[BQP_KCLASSES] kernel launches. */
+int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches);
+
 /* Replace the force/solver settings of a context (the field is kept; the
  * order may only shrink up to the parsed order). */
 int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);
@@ -131,7 +148,8 @@ int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);
 /* Full-field gravity (C00 included) at Earth-fixed positions.
  * Replaces spherical_gravity_impl_frame_packed
  * (satpy_core/src/gravity.rs:2638-2675). pos [n][3] km -> acc [n][3] km/s^2.
- * status[n] (nullable): BQP_ST_OK or BQP_ST_GRAVITY_RADIUS. */
+ * status[n] (nullable): BQP_ST_OK, BQP_ST_GRAVITY_RADIUS, or BQP_ST_WATCHDOG when
+ * the field table's copy into shared memory did not land within 1 s. */
 int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc_km_s2,
                      int32_t* status);
 int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* d_pos_km, double* d_acc,

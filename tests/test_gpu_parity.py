@@ -374,3 +374,29 @@ def test_reference_smoke_sequence():
     assert full["steps"] > 0 and full["rhs_evals"] >= 12 * full["steps"]
     fs = api.propagate_final(eci, EPOCH, tof_s=3600.0, srp=False, method="dop853")
     assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_kernel_timing_by_class(engine):
+    """bqp_ctx_profile: CUDA-event durations summed by kernel class."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    ctx = ctx_for(text, order, flags=1 | 4 | 8, engine=engine)
+    states = workloads.leo_states(300, seed=5)
+    ctx.profile(True)
+    _, st, _, evals = ctx.propagate_final(states, EPOCH, 1200.0)
+    t = ctx.profile_read()
+    ctx.profile(False)
+    assert (st == 0).all()
+    if engine == "pipeline":
+        for k in ("prep", "gravity", "drag", "control"):
+            assert t[k][0] > 0.0 and t[k][1] > 0, (k, t[k])
+        assert t["drag"][1] == 2 * t["gravity"][1]
+        assert t["persistent"] == (0.0, 0)
+    else:
+        assert t["persistent"][0] > 0.0 and t["persistent"][1] == 1
+    # totals stay after profiling stops and restart when it is switched on
+    ctx.propagate_final(states, EPOCH, 600.0)
+    assert ctx.profile_read() == t
+    ctx.profile(True)
+    assert all(v == (0.0, 0) for v in ctx.profile_read().values())
