@@ -54,6 +54,17 @@ EPS = 1e-12
 DRIVERS = (150.0,) * 8 + (20.0,)
 
 
+def form_name(args) -> str:
+    if not args.split_degree and not args.drag_fp32:
+        return "plain FP64"
+    parts = []
+    if args.split_degree:
+        parts.append(f"harmonic degrees > {args.split_degree} in FP32")
+    if args.drag_fp32:
+        parts.append("JB2008 density in FP32")
+    return "split: " + ", ".join(parts)
+
+
 def f_of_n(n: int) -> float:
     return 9 * (n + 2) * (n + 3) / 2 + 13 * n * (n + 1) + 9 * (n + 1) + 60
 
@@ -71,6 +82,9 @@ def parse():
                     help="seconds propagated per step (5400 = one Encke segment; smaller for profiling)")
     ap.add_argument("--engine", default="pipeline", choices=["pipeline", "persistent"])
     ap.add_argument("--gravity-threads", type=int, default=256)
+    ap.add_argument("--split-degree", type=int, default=0,
+                    help="split precision: harmonic degrees above this in FP32 (0: plain FP64)")
+    ap.add_argument("--drag-fp32", action="store_true", help="split precision: JB2008 density in FP32")
     return ap.parse_args()
 
 
@@ -140,10 +154,12 @@ def make_workload(n: int, seed: int = 0):
     return W.synthetic_field(ORDER), states, bal, W.EPOCH_JD
 
 
-def make_config(engine="pipeline", gravity_threads=256):
+def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp32=False):
     from bqp_b200 import _native as N
 
     cfg = N.default_config()
+    cfg.split_degree = split_degree
+    cfg.drag_fp32 = int(drag_fp32)
     cfg.engine = N.ENGINES[engine]
     cfg.gravity_threads = gravity_threads
     cfg.order = ORDER
@@ -251,7 +267,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
     text, states, bal, epoch = make_workload(args.n, seed=rank)
-    cfg = make_config(args.engine, args.gravity_threads)
+    cfg = make_config(args.engine, args.gravity_threads, args.split_degree, args.drag_fp32)
     ctx = N.Context(text, cfg)
     seg = args.segment
     stream = torch.cuda.Stream(device=dev)
@@ -413,7 +429,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
                                    f"DOP853 eps 1e-12, {seg:g} s of the arc per step",
-                       "form": "plain FP64", "engine": args.engine, "order": ORDER, "trajectories_per_gpu": n,
+                       "form": form_name(args), "engine": args.engine, "order": ORDER, "trajectories_per_gpu": n,
                        "segment_s": seg, "l2": "256 MiB write between timed steps",
                        "evals_per_step": total_evals / args.steps,
                        "trajectory_days_per_s": world * n * seg / 86400.0 / (t_max * 1e-3 / args.steps)},

@@ -47,7 +47,8 @@ class ForceConfig(C.Structure):
         ("omega_earth", C.c_double), ("mu_sun", C.c_double), ("mu_moon", C.c_double),
         ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
         ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
-        ("gravity_slots", C.c_int32), ("drag_quadrature", C.c_int32),
+        ("gravity_slots", C.c_int32), ("drag_quadrature", C.c_int32), ("split_degree", C.c_int32),
+        ("drag_fp32", C.c_int32),
     ]
 
 

@@ -262,6 +262,9 @@ struct bqp_ctx {
     int ncells = 0;
     size_t tab_bytes = 0;
     int use_smem = 0;
+    void* d_tab_split = nullptr;  // split-precision table (cfg.split_degree > 0)
+    int split_ls = 0;             // its last FP64 row
+    uint32_t split_bytes = 0;
     unsigned long long* d_queue = nullptr;
     void* d_ws = nullptr;
     size_t ws_bytes = 0;
@@ -307,6 +310,15 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_ARG, "gravity_threads must be a multiple of 32 in 0..256");
     if (c->gravity_slots != 0 && c->gravity_slots != 1 && c->gravity_slots != 2 && c->gravity_slots != 4)
         return fail(BQP_E_ARG, "gravity_slots must be 0, 1, 2 or 4");
+    if (c->split_degree != 0 && (c->split_degree < 4 || c->split_degree > kMaxOrder))
+        return fail(BQP_E_ARG, "split_degree must be 0 (plain FP64) or in 4..%d, got %d", kMaxOrder,
+                    c->split_degree);
+    if (c->split_degree != 0 && c->engine == BQP_ENGINE_PERSISTENT)
+        return fail(BQP_E_UNSUPPORTED, "split precision runs in the stage-synchronous engine");
+    if (c->drag_fp32 != 0 && c->drag_fp32 != 1) return fail(BQP_E_ARG, "drag_fp32 must be 0 or 1");
+    if (c->drag_fp32) return fail(BQP_E_UNSUPPORTED, "the FP32 JB2008 density is not built");
+    if (c->drag_fp32 && c->engine == BQP_ENGINE_PERSISTENT)
+        return fail(BQP_E_UNSUPPORTED, "the FP32 density runs in the stage-synchronous engine");
     return 0;
 }
 
@@ -356,7 +368,56 @@ int upload_table(bqp_ctx* ctx) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(gravity table)");
     e = cudaMemcpy(ctx->d_tab, tab.data(), ctx->tab_bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(gravity table)");
+    // split precision: FP64 cells of rows <= ls, FP32 cells of the rest
+    if (ctx->d_tab_split) cudaFree(ctx->d_tab_split);
+    ctx->d_tab_split = nullptr;
+    ctx->split_ls = 0;
+    ctx->split_bytes = 0;
+    const int N = ctx->cfg.order, ls = ctx->cfg.split_degree + 1;
+    if (ctx->cfg.split_degree > 0 && ls <= N) {
+        std::vector<unsigned char> buf(gravity_table_bytes(N, ls));
+        double* lo = reinterpret_cast<double*>(buf.data());
+        float* hi = reinterpret_cast<float*>(buf.data() + (size_t)split_lo_cells(ls) * kCellDoubles * 8);
+        const int last = N + 1;
+        for (int j = 0; j <= last; ++j) {
+            const size_t col = (size_t)gravity_col_offset(N, j);
+            for (int l = j; l <= last; ++l) {
+                const double* c = &tab[(col + (l - j)) * kCellDoubles];
+                if (j <= ls && l <= ls) {
+                    double* o = lo + ((size_t)split_lo_offset(ls, j) + (l - j)) * kCellDoubles;
+                    for (int k = 0; k < kCellDoubles; ++k) o[k] = c[k];
+                } else {
+                    const int first = j <= ls ? ls + 1 : j;  // first FP32 row of column j
+                    float* o = hi + ((size_t)split_hi_offset(N, ls, j) + (l - first)) * kCellDoubles;
+                    for (int k = 0; k < kCellDoubles; ++k) o[k] = (float)c[k];
+                }
+            }
+        }
+        e = cudaMalloc(&ctx->d_tab_split, buf.size());
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(split gravity table)");
+        e = cudaMemcpy(ctx->d_tab_split, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(split gravity table)");
+        ctx->split_ls = ls;
+        ctx->split_bytes = (uint32_t)buf.size();
+    }
     return 0;
+}
+
+// The table the gravity kernels read: split precision when configured.
+GravTable grav_table(const bqp_ctx* ctx) {
+    GravTable T{};
+    T.order = ctx->cfg.order;
+    if (ctx->split_ls > 0) {
+        T.tab = static_cast<const double*>(ctx->d_tab_split);
+        T.ls = ctx->split_ls;
+        T.bytes = ctx->split_bytes;
+    } else {
+        T.tab = ctx->d_tab;
+        T.ls = 0;
+        T.bytes = (uint32_t)ctx->tab_bytes;
+    }
+    T.in_smem = T.bytes <= kSmemLimit ? 1 : 0;
+    return T;
 }
 
 // Device workspace carve-out for the host-buffer entry points.  Each entry
@@ -420,6 +481,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.use_smem = ctx->use_smem;
     A.force = force_params(ctx);
     A.ctrl = ctrl_params(ctx);
+    A.grav = grav_table(ctx);
     if (ctx->cfg.engine == BQP_ENGINE_PIPELINE) {
         const size_t need = pipeline_bytes(n);
         if (need > ctx->pws_bytes) {
@@ -599,6 +661,8 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->engine = BQP_ENGINE_PIPELINE;
     c->gravity_threads = 256;
     c->gravity_slots = 4;
+    c->split_degree = 0;
+    c->drag_fp32 = 0;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -654,6 +718,7 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_ws) cudaFree(ctx->d_ws);
     if (ctx->d_pws) cudaFree(ctx->d_pws);
     if (ctx->d_fit) cudaFree(ctx->d_fit);
+    if (ctx->d_tab_split) cudaFree(ctx->d_tab_split);
     delete ctx;
     return 0;
 }
@@ -702,9 +767,9 @@ int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg) {
     if (cfg->order > ctx->parsed_order)
         return fail(BQP_E_ARG, "order %d exceeds the parsed field order %d", cfg->order, ctx->parsed_order);
     if ((rc = set_device(ctx))) return rc;
-    const int old = ctx->cfg.order;
+    const int old = ctx->cfg.order, old_split = ctx->cfg.split_degree;
     ctx->cfg = *cfg;
-    if (cfg->order != old) {
+    if (cfg->order != old || cfg->split_degree != old_split) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         return upload_table(ctx);
     }
@@ -716,8 +781,8 @@ int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* pos, double* 
     if (n < 0 || (n > 0 && (!pos || !acc))) return fail(BQP_E_ARG, "bad buffers");
     int rc = set_device(ctx);
     if (rc) return rc;
-    cudaError_t e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, pos, acc,
-                                   status, ctx->stream, ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
+    cudaError_t e = launch_gravity(grav_table(ctx), n, pos, acc, status, ctx->stream, ctx->cfg.gravity_threads,
+                                   ctx->cfg.gravity_slots);
     return e == cudaSuccess ? 0 : cuda_fail(e, "k_gravity launch");
 }
 
@@ -739,8 +804,8 @@ int bqp_gravity_eval(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, in
     }
     cudaError_t e = cudaMemcpyAsync(dp, pos, b3, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
-        e = launch_gravity(ctx->d_tab, ctx->cfg.order, ctx->ncells, ctx->use_smem, n, dp, da, ds, ctx->stream,
-                           ctx->cfg.gravity_threads, ctx->cfg.gravity_slots);
+        e = launch_gravity(grav_table(ctx), n, dp, da, ds, ctx->stream, ctx->cfg.gravity_threads,
+                           ctx->cfg.gravity_slots);
     if (e == cudaSuccess) e = cudaMemcpyAsync(acc, da, b3, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && status)
         e = cudaMemcpyAsync(status, ds, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream);

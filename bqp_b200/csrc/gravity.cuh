@@ -241,6 +241,232 @@ BQP_HD void gravity_columns(const double* __restrict__ tab, int order, int j0, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Split-precision form.  Cell (l, j) carries only degree n = l - 1, so rows
+// l <= ls hold degrees n <= ls - 1 (the central-field corrections J2...,
+// kept in FP64) and every other cell the higher degrees, evaluated in FP32:
+//   lo: FP64 cells of columns 0..ls, rows j..ls (column-major)
+//   hi: FP32 cells {a, b, Ax, Bx | Ay, By, Az, Bz} of columns 0..ls, rows
+//       ls+1..order+1, then columns ls+1..order+1, rows j..order+1
+// The V/W values of the last FP64 rows seed the FP32 rows below them; the
+// two parts are accumulated separately and added in FP64.  Needs
+// 1 <= ls <= order.
+BQP_HD int split_lo_offset(int ls, int j) { return j * (ls + 1) - j * (j - 1) / 2; }
+BQP_HD int split_lo_cells(int ls) { return (ls + 1) * (ls + 2) / 2; }
+BQP_HD int split_hi_offset(int order, int ls, int j) {
+    const int h = order + 1 - ls;  // FP32 rows under an FP64 column
+    if (j <= ls + 1) return j * h;
+    const int k = j - (ls + 1);
+    return (ls + 1) * h + k * h - k * (k - 1) / 2;
+}
+BQP_HD int split_hi_cells(int order, int ls) { return split_hi_offset(order, ls, order + 2); }
+
+template <int NT>
+BQP_HD void gravity_columns_split(const double* __restrict__ lo, const float* __restrict__ hi, int order, int ls,
+                                  int j0, int j1, const double* px, const double* py, const double* pz,
+                                  double (*acc)[3]) {
+    double xc[NT], yc[NT], zc[NT], c2re[NT], vd[NT], wd[NT], ax[NT], ay[NT], az[NT];
+    float xf[NT], yf[NT], zf[NT], cf[NT], vdf[NT], wdf[NT], fx[NT], fy[NT], fz[NT];
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+        const double r2 = fma(px[q], px[q], fma(py[q], py[q], pz[q] * pz[q]));
+        const double c2 = kReGravity / r2;
+        xc[q] = px[q] * c2;
+        yc[q] = py[q] * c2;
+        zc[q] = pz[q] * c2;
+        c2re[q] = c2 * kReGravity;
+        vd[q] = sqrt(c2re[q]);
+        wd[q] = 0.0;
+        ax[q] = ay[q] = az[q] = 0.0;
+        xf[q] = (float)xc[q];
+        yf[q] = (float)yc[q];
+        zf[q] = (float)zc[q];
+        cf[q] = (float)c2re[q];
+        vdf[q] = wdf[q] = 0.0f;
+        fx[q] = fy[q] = fz[q] = 0.0f;
+    }
+    const int last = order + 1;
+    const double2* lo2 = reinterpret_cast<const double2*>(lo);
+    const float4* hi4 = reinterpret_cast<const float4*>(hi);
+    // diagonal V(j,j), W(j,j) from column j-1's
+    auto advance_diag = [&](int j) {
+        if (j <= ls) {
+            const double a = lo2[(size_t)split_lo_offset(ls, j) * 4].x;
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const double nv = a * fma(xc[q], vd[q], -yc[q] * wd[q]);
+                const double nw = a * fma(xc[q], wd[q], yc[q] * vd[q]);
+                vd[q] = nv;
+                wd[q] = nw;
+            }
+        } else {
+            const float a = hi4[(size_t)split_hi_offset(order, ls, j) * 2].x;
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                if (j == ls + 1) {
+                    vdf[q] = (float)vd[q];
+                    wdf[q] = (float)wd[q];
+                }
+                const float nv = a * fmaf(xf[q], vdf[q], -yf[q] * wdf[q]);
+                const float nw = a * fmaf(xf[q], wdf[q], yf[q] * vdf[q]);
+                vdf[q] = nv;
+                wdf[q] = nw;
+            }
+        }
+    };
+    // FP32 interior rows: n cells from hc, recursion seeded by rows l-2, l-1
+    auto fp32_interior = [&](const float4* hc, int n, float* v0, float* w0, float* v1, float* w1) {
+        const int pairs = n >> 1;
+        float4 nx[4];
+        if (pairs > 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) nx[i] = hc[i];
+        }
+#pragma unroll 2
+        for (int p = 0; p < pairs; ++p) {
+            float4 cb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) cb[i] = nx[i];
+            if (p + 1 < pairs) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) nx[i] = hc[4 + i];
+            }
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const float ta = cb[0].x * zf[q], tb = cb[0].y * cf[q];
+                v0[q] = fmaf(ta, v1[q], -tb * v0[q]);
+                w0[q] = fmaf(ta, w1[q], -tb * w0[q]);
+                fx[q] = fmaf(cb[0].z, v0[q], fmaf(cb[0].w, w0[q], fx[q]));
+                fy[q] = fmaf(cb[1].x, v0[q], fmaf(cb[1].y, w0[q], fy[q]));
+                fz[q] = fmaf(cb[1].z, v0[q], fmaf(cb[1].w, w0[q], fz[q]));
+                const float ta2 = cb[2].x * zf[q], tb2 = cb[2].y * cf[q];
+                v1[q] = fmaf(ta2, v0[q], -tb2 * v1[q]);
+                w1[q] = fmaf(ta2, w0[q], -tb2 * w1[q]);
+                fx[q] = fmaf(cb[2].z, v1[q], fmaf(cb[2].w, w1[q], fx[q]));
+                fy[q] = fmaf(cb[3].x, v1[q], fmaf(cb[3].y, w1[q], fy[q]));
+                fz[q] = fmaf(cb[3].z, v1[q], fmaf(cb[3].w, w1[q], fz[q]));
+            }
+            hc += 4;
+        }
+        if (n & 1) {
+            const float4 c0 = hc[0], c1 = hc[1];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const float ta = c0.x * zf[q], tb = c0.y * cf[q];
+                const float v2 = fmaf(ta, v1[q], -tb * v0[q]);
+                const float w2 = fmaf(ta, w1[q], -tb * w0[q]);
+                fx[q] = fmaf(c0.z, v2, fmaf(c0.w, w2, fx[q]));
+                fy[q] = fmaf(c1.x, v2, fmaf(c1.y, w2, fy[q]));
+                fz[q] = fmaf(c1.z, v2, fmaf(c1.w, w2, fz[q]));
+            }
+        }
+    };
+    for (int j = 1; j < j0; ++j) advance_diag(j);
+    for (int j = j0; j < j1; ++j) {
+        if (j > 0) advance_diag(j);
+        float v0f[NT], w0f[NT], v1f[NT], w1f[NT];
+        if (j <= ls) {
+            // FP64 rows j..ls
+            const double2* cell = lo2 + (size_t)split_lo_offset(ls, j) * 4;
+            double v0[NT], w0[NT], v1[NT], w1[NT];
+            {
+                const double2 wxx = cell[1], wyy = cell[2], wzz = cell[3];
+#pragma unroll
+                for (int q = 0; q < NT; ++q) {
+                    ax[q] = fma(wxx.x, vd[q], fma(wxx.y, wd[q], ax[q]));
+                    ay[q] = fma(wyy.x, vd[q], fma(wyy.y, wd[q], ay[q]));
+                    az[q] = fma(wzz.x, vd[q], fma(wzz.y, wd[q], az[q]));
+                    v0[q] = 0.0;
+                    w0[q] = 0.0;
+                    v1[q] = vd[q];
+                    w1[q] = wd[q];
+                }
+                cell += 4;
+            }
+            for (int l = j + 1; l <= ls; ++l) {
+                const double2 ab = cell[0], wxx = cell[1], wyy = cell[2], wzz = cell[3];
+#pragma unroll
+                for (int q = 0; q < NT; ++q) {
+                    const double ta = ab.x * zc[q];
+                    const double v2 = l == j + 1 ? ta * v1[q] : fma(ta, v1[q], -(ab.y * c2re[q]) * v0[q]);
+                    const double w2 = l == j + 1 ? ta * w1[q] : fma(ta, w1[q], -(ab.y * c2re[q]) * w0[q]);
+                    ax[q] = fma(wxx.x, v2, fma(wxx.y, w2, ax[q]));
+                    ay[q] = fma(wyy.x, v2, fma(wyy.y, w2, ay[q]));
+                    az[q] = fma(wzz.x, v2, fma(wzz.y, w2, az[q]));
+                    v0[q] = v1[q];
+                    w0[q] = w1[q];
+                    v1[q] = v2;
+                    w1[q] = w2;
+                }
+                cell += 4;
+            }
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                v0f[q] = (float)v0[q];
+                w0f[q] = (float)w0[q];
+                v1f[q] = (float)v1[q];
+                w1f[q] = (float)w1[q];
+            }
+            // FP32 rows ls+1..last
+            const float4* hc = hi4 + (size_t)split_hi_offset(order, ls, j) * 2;
+            int n = last - ls;
+            if (j == ls) {  // row ls+1 is this column's sub-diagonal
+                const float4 c0 = hc[0], c1 = hc[1];
+#pragma unroll
+                for (int q = 0; q < NT; ++q) {
+                    const float a = c0.x * zf[q];
+                    v0f[q] = v1f[q];
+                    w0f[q] = w1f[q];
+                    v1f[q] = a * v0f[q];
+                    w1f[q] = a * w0f[q];
+                    fx[q] = fmaf(c0.z, v1f[q], fmaf(c0.w, w1f[q], fx[q]));
+                    fy[q] = fmaf(c1.x, v1f[q], fmaf(c1.y, w1f[q], fy[q]));
+                    fz[q] = fmaf(c1.z, v1f[q], fmaf(c1.w, w1f[q], fz[q]));
+                }
+                hc += 2;
+                --n;
+            }
+            fp32_interior(hc, n, v0f, w0f, v1f, w1f);
+        } else {
+            // all FP32: diagonal, sub-diagonal, interior
+            const float4* hc = hi4 + (size_t)split_hi_offset(order, ls, j) * 2;
+            {
+                const float4 c0 = hc[0], c1 = hc[1];
+#pragma unroll
+                for (int q = 0; q < NT; ++q) {
+                    fx[q] = fmaf(c0.z, vdf[q], fmaf(c0.w, wdf[q], fx[q]));
+                    fy[q] = fmaf(c1.x, vdf[q], fmaf(c1.y, wdf[q], fy[q]));
+                    fz[q] = fmaf(c1.z, vdf[q], fmaf(c1.w, wdf[q], fz[q]));
+                }
+                hc += 2;
+            }
+            if (j == last) continue;
+            {
+                const float4 c0 = hc[0], c1 = hc[1];
+#pragma unroll
+                for (int q = 0; q < NT; ++q) {
+                    const float a = c0.x * zf[q];
+                    v0f[q] = vdf[q];
+                    w0f[q] = wdf[q];
+                    v1f[q] = a * vdf[q];
+                    w1f[q] = a * wdf[q];
+                    fx[q] = fmaf(c0.z, v1f[q], fmaf(c0.w, w1f[q], fx[q]));
+                    fy[q] = fmaf(c1.x, v1f[q], fmaf(c1.y, w1f[q], fy[q]));
+                    fz[q] = fmaf(c1.z, v1f[q], fmaf(c1.w, w1f[q], fz[q]));
+                }
+                hc += 2;
+            }
+            fp32_interior(hc, last - j - 1, v0f, w0f, v1f, w1f);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+        acc[q][0] = ax[q] + (double)fx[q];
+        acc[q][1] = ay[q] + (double)fy[q];
+        acc[q][2] = az[q] + (double)fz[q];
+    }
+}
+
 // The whole field for NT trajectories per thread.
 template <int NT>
 BQP_HD void gravity_field_multi(const double* __restrict__ tab, int order, const double* px, const double* py,

@@ -82,10 +82,28 @@ BQP_HD GravLayout gravity_layout(int rows, int nt, int block, int parts_max) {
     return {tpart, parts};
 }
 
+// The field table as the gravity kernels see it.  Plain form: `tab` holds
+// the FP64 cells of every column.  Split form (ls > 0): `tab` holds the FP64
+// cells of rows <= ls followed by the FP32 cells of the rest
+// (gravity_columns_split).
+struct GravTable {
+    const double* tab;
+    int order;
+    int ls;          // 0: plain FP64; else the last FP64 row
+    uint32_t bytes;  // size of tab
+    int in_smem;     // 1: staged into shared memory per CTA
+};
+
+inline uint32_t gravity_table_bytes(int order, int ls) {
+    if (ls <= 0) return (uint32_t)gravity_cells(order) * kCellDoubles * sizeof(double);
+    return (uint32_t)(split_lo_cells(ls) * kCellDoubles * sizeof(double) +
+                      split_hi_cells(order, ls) * kCellDoubles * sizeof(float));
+}
+
 // Dynamic shared memory of a CTA of `block` threads: the table (if staged)
 // plus the partial-sum area of groups 1..parts-1.
-inline size_t gravity_smem_bytes(int ncells, bool table_in_smem, int block, int nt, int parts_max) {
-    const size_t tab = table_in_smem ? (size_t)ncells * kCellDoubles * sizeof(double) : 0;
+inline size_t gravity_smem_bytes(const GravTable& T, int block, int nt, int parts_max) {
+    const size_t tab = T.in_smem ? T.bytes : 0;
     const size_t red = parts_max > 1 ? (size_t)(block - 32) * nt * 3 * sizeof(double) : 0;
     return tab + red;
 }
@@ -97,15 +115,17 @@ inline size_t gravity_smem_bytes(int ncells, bool table_in_smem, int block, int 
 // lost(i) records that row i got no field because the table copy did not
 // complete in time.
 template <int NT, class Load, class Store, class Lost>
-__device__ __forceinline__ void gravity_cta(const double* __restrict__ gtab, int order, int ncells, bool table_in_smem,
-                                            int parts_max, int b0, int b1, Load load, Store store, Lost lost) {
+__device__ __forceinline__ void gravity_cta(const GravTable& T, int parts_max, int b0, int b1, Load load, Store store,
+                                            Lost lost) {
     extern __shared__ __align__(16) double smem_dyn[];
     const GravLayout L = gravity_layout(b1 - b0, NT, blockDim.x, parts_max);
-    if (table_in_smem && !bulk_stage(smem_dyn, gtab, (uint32_t)ncells * kCellDoubles * sizeof(double))) {
+    if (T.in_smem && !bulk_stage(smem_dyn, T.tab, T.bytes)) {
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) lost(i);
         return;  // the verdict is the same in every thread
     }
-    double* red = smem_dyn + (table_in_smem ? (size_t)ncells * kCellDoubles : 0);
+    const int order = T.order;
+    const double* __restrict__ gtab = T.tab;
+    double* red = smem_dyn + (T.in_smem ? T.bytes / sizeof(double) : 0);
     const int part = threadIdx.x / L.tpart;
     const int tid = threadIdx.x - part * L.tpart;
     const bool member = part < L.parts;
@@ -124,10 +144,20 @@ __device__ __forceinline__ void gravity_cta(const double* __restrict__ gtab, int
             on[q] = member && i < b1 && load(i, px[q], py[q], pz[q]);
         }
         if (member) {
-            if (table_in_smem)
-                gravity_columns<NT>(smem_dyn, order, j0, j1, px, py, pz, a);
-            else
-                gravity_columns<NT>(gtab, order, j0, j1, px, py, pz, a);
+            if (T.ls > 0) {
+                const size_t lo_doubles = (size_t)split_lo_cells(T.ls) * kCellDoubles;
+                if (T.in_smem)
+                    gravity_columns_split<NT>(smem_dyn, reinterpret_cast<const float*>(smem_dyn + lo_doubles),
+                                              order, T.ls, j0, j1, px, py, pz, a);
+                else
+                    gravity_columns_split<NT>(gtab, reinterpret_cast<const float*>(gtab + lo_doubles), order,
+                                              T.ls, j0, j1, px, py, pz, a);
+            } else {
+                if (T.in_smem)
+                    gravity_columns<NT>(smem_dyn, order, j0, j1, px, py, pz, a);
+                else
+                    gravity_columns<NT>(gtab, order, j0, j1, px, py, pz, a);
+            }
         }
         if (L.parts > 1) {
             if (member && part > 0) {

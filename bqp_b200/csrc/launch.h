@@ -4,6 +4,7 @@
 
 #include <cstdint>
 
+#include "gravity_cta.cuh"
 #include "kernels.cuh"
 
 namespace bqp {
@@ -26,9 +27,10 @@ struct PropArgs {
     int64_t* steps;                // [n] or null
     int64_t* evals;                // [n] or null
     unsigned long long* queue;     // work-queue head, zeroed before launch
-    const double* gtab;            // gravity table (global)
+    const double* gtab;            // gravity table (global), FP64 cells (the Encke force call)
     int32_t ncells;
     int32_t use_smem;
+    GravTable grav;                // the gravity stage's table (plain or split precision)
     ForceParams force;
     CtrlParams ctrl;
 };
@@ -73,9 +75,8 @@ cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cu
                             double max_seconds, int gravity_threads, int gravity_slots,
                             KernelTimes* times = nullptr);
 
-cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
-                           const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads = 256,
-                           int slots = 4);
+cudaError_t launch_gravity(const GravTable& T, int64_t n, const double* pos, double* acc, int32_t* status,
+                           cudaStream_t st, int threads = 256, int slots = 4);
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,
                        const double* equ, const double* seg_t0, const double* jd0, const double* t,
                        const double* delta, const double* ballistic, double am0, double cd0,

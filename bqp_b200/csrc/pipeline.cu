@@ -26,7 +26,6 @@
 #include <cstdint>
 #include <vector>
 
-#include "gravity_cta.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 #include "traj.cuh"
@@ -186,8 +185,7 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
 // Persistent over slots: one CTA per SM stages the field table once; the
 // CTA's contiguous slot range is walked NT slots per thread.
 template <int NT>
-__global__ void __launch_bounds__(256, 1) pl_gravity(const double* __restrict__ gtab, int order, int ncells,
-                                                     int use_smem, int parts_max, PipeBufs P, int cur) {
+__global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max, PipeBufs P, int cur) {
     const int count = P.count[cur];
     const int per_block = (count + gridDim.x - 1) / gridDim.x;
     const int b0 = blockIdx.x * per_block;
@@ -218,7 +216,7 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(const double* __restrict__ 
         P.bad[sl] = 2;
         P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
     };
-    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, b0, b1, load, store, lost);
+    gravity_cta<NT>(T, parts_max, b0, b1, load, store, lost);
 }
 
 // --------------------------------------------------------------------- drag
@@ -385,8 +383,11 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
-    const int dblocks2 = (int)((A.n * 2 + kBlock - 1) / kBlock);
-    const int dblocks4 = (int)((A.n * 4 + kBlock - 1) / kBlock);
+    // drag lanes per state: 4 above ~510 km (sweep fits, a short upper
+    // sweep), 16 below (the 105 km -> altitude sweep walks ~60 intervals)
+    constexpr int kLanesHigh = 4, kLanesLow = 16;
+    const int dblocks_hi = (int)((A.n * kLanesHigh + kBlock - 1) / kBlock);
+    const int dblocks_lo = (int)((A.n * kLanesLow + kBlock - 1) / kBlock);
     const int nt = gslots == 1 || gslots == 2 ? gslots : 4;
     auto gker = nt == 1 ? pl_gravity<1> : (nt == 2 ? pl_gravity<2> : pl_gravity<4>);
     if (gthreads > 256) gthreads = 256;
@@ -394,10 +395,10 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     gthreads = gthreads / 32 * 32;
     // column groups need room for their partial sums next to the table
     int gparts = kGravityPartsMax;
-    size_t smem = gravity_smem_bytes(A.ncells, A.use_smem != 0, gthreads, nt, gparts);
+    size_t smem = gravity_smem_bytes(A.grav, gthreads, nt, gparts);
     if (smem > kSmemPerBlock) {
         gparts = 1;
-        smem = gravity_smem_bytes(A.ncells, A.use_smem != 0, gthreads, nt, gparts);
+        smem = gravity_smem_bytes(A.grav, gthreads, nt, gparts);
     }
     cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -450,13 +451,12 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
             timed(kKcPrep, [&] { pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s); });
             if (A.force.gravity_on)
                 timed(kKcGravity, [&] {
-                    gker<<<gblocks, gthreads, smem, st>>>(A.gtab, A.force.order, A.ncells, A.use_smem, gparts, P,
-                                                          cur);
+                    gker<<<gblocks, gthreads, smem, st>>>(A.grav, gparts, P, cur);
                 });
             if (A.force.drag)
                 timed(kKcDrag, [&] {
-                    pl_drag<2><<<dblocks2, kBlock, 0, st>>>(A.force, P, 0);
-                    pl_drag<4><<<dblocks4, kBlock, 0, st>>>(A.force, P, 1);
+                    pl_drag<kLanesHigh><<<dblocks_hi, kBlock, 0, st>>>(A.force, P, 0);
+                    pl_drag<kLanesLow><<<dblocks_lo, kBlock, 0, st>>>(A.force, P, 1);
                 });
         }
         timed(kKcControl, [&] { pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out); });

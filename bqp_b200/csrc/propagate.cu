@@ -11,7 +11,6 @@
 
 #include <cstdint>
 
-#include "gravity_cta.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 #include "traj.cuh"
@@ -20,8 +19,7 @@ namespace bqp {
 
 // ----------------------------------------------------------------- kernels
 template <int NT>
-__global__ void __launch_bounds__(256, 1) k_gravity(const double* __restrict__ gtab, int order, int ncells,
-                                                    int use_smem, int parts_max, int64_t n,
+__global__ void __launch_bounds__(256, 1) k_gravity(GravTable T, int parts_max, int64_t n,
                                                     const double* __restrict__ pos, double* __restrict__ acc,
                                                     int32_t* __restrict__ status) {
     // rows are int-indexed inside a CTA: the launcher keeps each CTA's range
@@ -60,7 +58,7 @@ __global__ void __launch_bounds__(256, 1) k_gravity(const double* __restrict__ g
         a0[3 * i] = a0[3 * i + 1] = a0[3 * i + 2] = NAN;
         if (s0) s0[i] = kWatchdog;
     };
-    gravity_cta<NT>(gtab, order, ncells, use_smem != 0, parts_max, 0, (int)(c1 - c0), load, store, lost);
+    gravity_cta<NT>(T, parts_max, 0, (int)(c1 - c0), load, store, lost);
 }
 
 __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem, ForceParams fp,
@@ -203,9 +201,8 @@ static int sm_count() {
     return n;
 }
 
-cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_smem, int64_t n,
-                           const double* pos, double* acc, int32_t* status, cudaStream_t st, int threads,
-                           int slots) {
+cudaError_t launch_gravity(const GravTable& T, int64_t n, const double* pos, double* acc, int32_t* status,
+                           cudaStream_t st, int threads, int slots) {
     if (n <= 0) return cudaSuccess;
     const int nt = slots == 1 || slots == 2 ? slots : 4;
     auto ker = nt == 1 ? k_gravity<1> : (nt == 2 ? k_gravity<2> : k_gravity<4>);
@@ -213,10 +210,10 @@ cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_sm
     if (threads < 32) threads = 32;
     threads = threads / 32 * 32;
     int parts = kGravityPartsMax;
-    size_t smem = gravity_smem_bytes(ncells, use_smem != 0, threads, nt, parts);
+    size_t smem = gravity_smem_bytes(T, threads, nt, parts);
     if (smem > kSmemPerBlock) {
         parts = 1;
-        smem = gravity_smem_bytes(ncells, use_smem != 0, threads, nt, parts);
+        smem = gravity_smem_bytes(T, threads, nt, parts);
     }
     cudaError_t e = cudaFuncSetAttribute(ker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -228,8 +225,8 @@ cudaError_t launch_gravity(const double* gtab, int order, int ncells, int use_sm
         const int64_t m = n - off < chunk ? n - off : chunk;
         int64_t blocks = (m + 32 * nt - 1) / (32 * nt);
         if (blocks > grid_cap) blocks = grid_cap;
-        ker<<<(unsigned)blocks, threads, smem, st>>>(gtab, order, ncells, use_smem, parts, m, pos + 3 * off,
-                                                     acc + 3 * off, status ? status + off : nullptr);
+        ker<<<(unsigned)blocks, threads, smem, st>>>(T, parts, m, pos + 3 * off, acc + 3 * off,
+                                                     status ? status + off : nullptr);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -92,6 +92,10 @@ typedef struct bqp_force_config {
     int32_t gravity_slots;     /* trajectories per thread in the gravity kernels: 1, 2 or 4 (0: 4) */
     int32_t drag_quadrature;   /* 1: always walk the JB2008 Boole quadrature; 0: use the
                                   Chebyshev fits of its fixed-node sweeps where they apply */
+    int32_t split_degree;      /* split precision: 0 plain FP64; d >= 4: spherical-harmonic
+                                  degrees above d in FP32, the rest in FP64 (stage-synchronous
+                                  engine and gravity evaluation) */
+    int32_t drag_fp32;         /* split precision: 1 evaluates the JB2008 density in FP32 */
 } bqp_force_config;
 
 /* propagation engines */

@@ -400,3 +400,29 @@ def test_kernel_timing_by_class(engine):
     assert ctx.profile_read() == t
     ctx.profile(True)
     assert all(v == (0.0, 0) for v in ctx.profile_read().values())
+
+
+@pytest.mark.parametrize("order,degree", [(20, 8), (70, 8), (70, 4), (120, 8)])
+def test_split_precision_gravity(order, degree):
+    """Split form: degrees <= `degree` in FP64, the rest in FP32.  Its error
+    is bounded relative to the FP64 field of the degrees above `degree`
+    (field(order) - field(degree), both plain FP64)."""
+    text = workloads.synthetic_field(order)
+    pos = random_positions(3000, seed=order + degree)
+    full = ctx_for(text, order).gravity(pos)[0]
+    low = ctx_for(text, degree).gravity(pos)[0]
+    cfg_ctx = ctx_for(text, order)
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.split_degree = degree
+    cfg_ctx.set_config(cfg)
+    split, st = cfg_ctx.gravity(pos)
+    assert (st == 0).all()
+    high = np.linalg.norm(full - low, axis=1)
+    err = np.linalg.norm(split - full, axis=1)
+    # FP32 rounding of ~(order+2)(order+3)/2 products of size ~|high|: a few
+    # 1e-7 of the high-degree field, absolutely ~1e-14 km/s^2 at 70x70
+    assert np.median(err / high) <= 2e-6, float(np.median(err / high))
+    assert err.max() <= 1e-5 * high.max(), (float(err.max()), float(high.max()))
+    # and the FP32 part really is FP32: the error is not at FP64 level
+    assert (err / high).max() > 1e-9
