@@ -87,6 +87,11 @@ SIGNATURES = [
                                         _dp, C.c_int32, _dp, _ip, _lp, _lp]),
     ("bqp_propagate_sampled_device", C.c_int, [_vp, C.c_int64, _vp, C.c_int32, _vp, C.c_double, _vp,
                                                C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp]),
+    ("bqp_sigma_propagate", C.c_int, [_vp, C.c_int64, _dp, _dp, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                      _dp, C.c_double, _dp, _dp, _dp, _dp, _ip, _lp]),
+    ("bqp_sigma_propagate_device", C.c_int, [_vp, C.c_int64, _vp, _vp, C.c_int32, C.c_double, C.c_double,
+                                             C.c_double, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("bqp_sigma_weights", C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]),
     ("bqp_eci_to_equinoctial", C.c_int, [C.c_int64, _dp, _dp, _ip]),
     ("bqp_equinoctial_to_eci", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),
@@ -272,6 +277,25 @@ class Context:
                                           lptr(evals)))
         return out, st, steps, evals
 
+    def sigma_propagate(self, mean, cov, epoch_jd, tf, sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0,
+                        t0=0.0, ballistic=None):
+        """Unscented propagation of (mean[n][6], cov[n][6][6]) to tf[n]:
+        returns mean_out, cov_out, status, evals."""
+        m = f64(mean).reshape(-1, 6)
+        n = m.shape[0]
+        c = f64(cov).reshape(n, 36)
+        ep = f64(np.broadcast_to(epoch_jd, (n,)))
+        tfa = f64(np.broadcast_to(tf, (n,)))
+        bal = None if ballistic is None else f64(np.broadcast_to(ballistic, (n, 2)))
+        mo = np.empty((n, 6))
+        co = np.empty((n, 36))
+        st = np.empty(n, dtype=np.int32)
+        ev = np.empty(n, dtype=np.int64)
+        check(lib().bqp_sigma_propagate(self._h, n, dptr(m), dptr(c), SIGMA_SETS[sigma_set], alpha, beta, kappa,
+                                        dptr(ep), float(t0), dptr(tfa), None if bal is None else dptr(bal),
+                                        dptr(mo), dptr(co), iptr(st), lptr(ev)))
+        return mo, co.reshape(n, 6, 6), st, ev
+
     # -------------------------------------------------------------- device
     def propagate_final_device(self, d_in, d_epoch, d_tf, d_out, d_status, d_steps=None, d_evals=None,
                                n=None, t0=0.0, d_ballistic=None, equinoctial=False):
@@ -287,6 +311,21 @@ class Context:
 
 
 # ----------------------------------------------------------- host helpers
+SIGMA_SETS = {"julier7": 0, "merwe13": 1}  # BQP_SIGMA_*
+
+
+def sigma_weights(sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0):
+    """(points, wm, wc, offsets[7][6]) of a sigma set."""
+    pts = C.c_int32(0)
+    wm = np.zeros(13)
+    wc = np.zeros(13)
+    off = np.zeros((7, 6))
+    check(lib().bqp_sigma_weights(SIGMA_SETS[sigma_set], alpha, beta, kappa, C.byref(pts), dptr(wm), dptr(wc),
+                                  dptr(off)))
+    p = pts.value
+    return p, wm[:p].copy(), wc[:p].copy(), off
+
+
 def eci_to_equinoctial(eci):
     e = f64(eci).reshape(-1, 6)
     out = np.empty_like(e)

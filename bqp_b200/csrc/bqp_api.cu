@@ -629,6 +629,55 @@ void eci2kep(const double* s, double* out) {
     out[5] = wrap360(nu * r2d);
 }
 
+// Sigma-point sets (sigma.cu).  Julier's n + 2 recursion at W0 = 0 with the
+// centre dropped (dust_ukf_rs/src/lib.rs:155-200): offsets xi[7][6] such
+// that x_i = mean + chol(P) xi_i; weights 1/7.  Merwe scaled set: the
+// covariance is scaled by n + lambda before the factorisation.
+struct SigmaSet {
+    int points = 0;
+    double scale = 1.0;  // covariance factor before Cholesky
+    double offsets[7 * 6] = {};
+    double wm[13] = {}, wc[13] = {};
+};
+
+int sigma_set(int32_t set, double alpha, double beta, double kappa, SigmaSet& S) {
+    const double n = 6.0;
+    if (set == BQP_SIGMA_JULIER7) {
+        const double w1 = 1.0 / (n + 1.0);
+        double seq[8][6] = {};
+        seq[1][0] = -1.0 / std::sqrt(2.0 * w1);
+        seq[2][0] = 1.0 / std::sqrt(2.0 * w1);
+        double jf = 1.0;
+        for (int j = 2; j <= 6; ++j) {
+            jf += 1.0;
+            const double step = 1.0 / std::sqrt(jf * (jf + 1.0) * w1);
+            for (int p = 1; p <= j; ++p) seq[p][j - 1] = -step;
+            for (int k = 0; k < 6; ++k) seq[j + 1][k] = 0.0;
+            seq[j + 1][j - 1] = jf * step;
+        }
+        S.points = 7;
+        S.scale = 1.0;
+        for (int p = 0; p < 7; ++p)
+            for (int k = 0; k < 6; ++k) S.offsets[p * 6 + k] = seq[p + 1][k];
+        for (int p = 0; p < 7; ++p) S.wm[p] = S.wc[p] = w1;
+        return 0;
+    }
+    if (set == BQP_SIGMA_MERWE13) {
+        if (!(std::isfinite(alpha) && alpha > 0.0 && std::isfinite(beta) && std::isfinite(kappa)))
+            return fail(BQP_E_ARG, "Merwe sigma set: alpha must be finite and > 0, beta and kappa finite");
+        const double lambda = alpha * alpha * (n + kappa) - n;
+        const double c = n + lambda;
+        if (!(c > 0.0)) return fail(BQP_E_ARG, "Merwe sigma set: n + lambda must be > 0");
+        S.points = 13;
+        S.scale = c;
+        S.wm[0] = lambda / c;
+        S.wc[0] = lambda / c + (1.0 - alpha * alpha + beta);
+        for (int p = 1; p < 13; ++p) S.wm[p] = S.wc[p] = 1.0 / (2.0 * c);
+        return 0;
+    }
+    return fail(BQP_E_ARG, "unknown sigma set %d", set);
+}
+
 }  // namespace
 
 // ======================================================================
@@ -1129,6 +1178,150 @@ int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32
     if (e == cudaSuccess && evals) e = cudaMemcpyAsync(evals, devals, b1, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_propagate_final_noalloc");
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Sigma-point covariance propagation (sigma.cu).
+namespace {
+
+struct SigmaBufs {
+    double *rows, *row_epoch, *row_tf, *row_bal, *out_rows, *offsets, *wm, *wc;
+    int32_t* row_status;
+    int64_t* row_evals;
+};
+
+void carve_sigma(Carve& cv, int64_t n, int S, bool bal, SigmaBufs& B) {
+    const size_t m = (size_t)n * S;
+    B.rows = cv.take<double>(m * 6);
+    B.row_epoch = cv.take<double>(m);
+    B.row_tf = cv.take<double>(m);
+    B.row_bal = bal ? cv.take<double>(m * 2) : nullptr;
+    B.out_rows = cv.take<double>(m * 6);
+    B.row_status = cv.take<int32_t>(m);
+    B.row_evals = cv.take<int64_t>(m);
+    B.offsets = cv.take<double>(7 * 6);
+    B.wm = cv.take<double>(13);
+    B.wc = cv.take<double>(13);
+}
+
+// Generation -> propagation of n * S rows -> recombination, all on ctx's
+// stream; inputs and outputs are device pointers, B in the workspace.
+int sigma_run(bqp_ctx* ctx, int64_t n, const SigmaSet& SS, int32_t set, const SigmaBufs& B, const double* mean,
+              const double* cov, const double* epoch, double t0, const double* tf, const double* bal,
+              double* mean_out, double* cov_out, int32_t* status, int64_t* evals) {
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(B.offsets, SS.offsets, sizeof SS.offsets, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(B.wm, SS.wm, sizeof SS.wm, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(B.wc, SS.wc, sizeof SS.wc, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_sigma_gen(n, set == BQP_SIGMA_JULIER7 ? 0 : 1, SS.scale, B.offsets, mean, cov, epoch, tf, bal,
+                             B.rows, B.row_epoch, B.row_tf, bal ? B.row_bal : nullptr, status, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sigma-point generation");
+    int rc = launch_prop(ctx, n * SS.points, B.rows, 0, B.row_epoch, t0, B.row_tf, bal ? B.row_bal : nullptr, 0,
+                         nullptr, 0, B.out_rows, B.row_status, nullptr, B.row_evals);
+    if (rc) return rc;
+    e = launch_sigma_recombine(n, SS.points, B.wm, B.wc, B.out_rows, B.row_status, B.row_evals, mean_out, cov_out,
+                               status, evals, s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "sigma-point recombination");
+}
+
+int check_sigma_args(const bqp_ctx* ctx, int64_t n, const double* mean, const double* cov, const double* epoch,
+                     double t0, const double* tf, const double* mean_out, const double* cov_out,
+                     const int32_t* status) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (n < 0) return fail(BQP_E_ARG, "n must be >= 0");
+    if (n > 0 && (!mean || !cov || !epoch || !tf || !mean_out || !cov_out || !status))
+        return fail(BQP_E_ARG, "null buffer");
+    if (!std::isfinite(t0)) return fail(BQP_E_ARG, "t0 must be finite");
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bqp_sigma_weights(int32_t set, double alpha, double beta, double kappa, int32_t* points, double* wm,
+                      double* wc, double* offsets) {
+    SigmaSet SS;
+    int rc = sigma_set(set, alpha, beta, kappa, SS);
+    if (rc) return rc;
+    if (points) *points = SS.points;
+    for (int p = 0; p < SS.points; ++p) {
+        if (wm) wm[p] = SS.wm[p];
+        if (wc) wc[p] = SS.wc[p];
+    }
+    if (offsets)
+        for (int k = 0; k < 42; ++k) offsets[k] = SS.offsets[k];
+    return 0;
+}
+
+int bqp_sigma_propagate_device(bqp_ctx* ctx, int64_t n, const double* mean, const double* cov, int32_t set,
+                               double alpha, double beta, double kappa, const double* epoch_jd, double t0,
+                               const double* tf, const double* ballistic, double* mean_out, double* cov_out,
+                               int32_t* status, int64_t* evals) {
+    int rc = check_sigma_args(ctx, n, mean, cov, epoch_jd, t0, tf, mean_out, cov_out, status);
+    if (rc) return rc;
+    SigmaSet SS;
+    if ((rc = sigma_set(set, alpha, beta, kappa, SS))) return rc;
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    SigmaBufs B{};
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        carve_sigma(cv, n, SS.points, ballistic != nullptr, B);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
+    return sigma_run(ctx, n, SS, set, B, mean, cov, epoch_jd, t0, tf, ballistic, mean_out, cov_out, status,
+                     evals);
+}
+
+int bqp_sigma_propagate(bqp_ctx* ctx, int64_t n, const double* mean, const double* cov, int32_t set,
+                        double alpha, double beta, double kappa, const double* epoch_jd, double t0,
+                        const double* tf, const double* ballistic, double* mean_out, double* cov_out,
+                        int32_t* status, int64_t* evals) {
+    int rc = check_sigma_args(ctx, n, mean, cov, epoch_jd, t0, tf, mean_out, cov_out, status);
+    if (rc) return rc;
+    SigmaSet SS;
+    if ((rc = sigma_set(set, alpha, beta, kappa, SS))) return rc;
+    if (n == 0) return 0;
+    if ((rc = set_device(ctx))) return rc;
+    SigmaBufs B{};
+    double *dm = nullptr, *dc = nullptr, *dep = nullptr, *dtf = nullptr, *db = nullptr, *dmo = nullptr,
+           *dco = nullptr;
+    int32_t* dst = nullptr;
+    int64_t* dev = nullptr;
+    const size_t b1 = (size_t)n * sizeof(double);
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        carve_sigma(cv, n, SS.points, ballistic != nullptr, B);
+        dm = cv.take<double>((size_t)n * 6);
+        dc = cv.take<double>((size_t)n * 36);
+        dep = cv.take<double>((size_t)n);
+        dtf = cv.take<double>((size_t)n);
+        db = ballistic ? cv.take<double>((size_t)n * 2) : nullptr;
+        dmo = cv.take<double>((size_t)n * 6);
+        dco = cv.take<double>((size_t)n * 36);
+        dst = cv.take<int32_t>((size_t)n);
+        dev = cv.take<int64_t>((size_t)n);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(dm, mean, 6 * b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dc, cov, 36 * b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dep, epoch_jd, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtf, tf, b1, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && db) e = cudaMemcpyAsync(db, ballistic, 2 * b1, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_sigma_propagate H2D");
+    rc = sigma_run(ctx, n, SS, set, B, dm, dc, dep, t0, dtf, db, dmo, dco, dst, dev);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(mean_out, dmo, 6 * b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cov_out, dco, 36 * b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, dst, (size_t)n * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && evals) e = cudaMemcpyAsync(evals, dev, b1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_sigma_propagate");
 }
 
 }  // extern "C"

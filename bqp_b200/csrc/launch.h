@@ -82,6 +82,13 @@ cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const Force
                        const double* delta, const double* ballistic, double am0, double cd0,
                        double* out, cudaStream_t st);
 cudaError_t launch_propagate(const PropArgs& A, int method, int threads, int blocks, cudaStream_t st);
+cudaError_t launch_sigma_gen(int64_t n, int set, double scale, const double* offsets, const double* mean,
+                             const double* cov, const double* epoch, const double* tf, const double* ballistic,
+                             double* rows, double* row_epoch, double* row_tf, double* row_bal, int32_t* status,
+                             cudaStream_t st);
+cudaError_t launch_sigma_recombine(int64_t n, int S, const double* wm, const double* wc, const double* rows,
+                                   const int32_t* row_status, const int64_t* row_evals, double* mean_out,
+                                   double* cov_out, int32_t* status, int64_t* evals, cudaStream_t st);
 int device_sm_count();
 
 }  // namespace bqp

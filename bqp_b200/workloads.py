@@ -75,7 +75,8 @@ def leo_ballistics(n: int, seed: int = 0) -> np.ndarray:
 def mixed_states(n: int, seed: int = 0):
     """60% LEO / 20% MEO (a U[20000, 27000]) / 10% GEO / 10% HEO (e U[0.5, 0.75],
     perigee altitude 500 km); durations log-uniform 1 h .. 30 d.
-    Returns (states [n,6], durations_s [n], is_low [n] (drag applies))."""
+    Returns (states [n,6], durations_s [n], is_low [n]): is_low marks the
+    orbits whose perigee is below 2000 km (LEO and HEO), where drag applies."""
     rng = np.random.default_rng(seed)
     kind = rng.choice(4, size=n, p=[0.6, 0.2, 0.1, 0.1])
     a = np.empty(n)
@@ -96,4 +97,41 @@ def mixed_states(n: int, seed: int = 0):
     M = rng.uniform(0.0, 360.0, n)
     states = kep_states(a, e, inc, raan, argp, M)
     dur = np.exp(rng.uniform(np.log(3600.0), np.log(30 * 86400.0), n))
-    return states, dur, kind == 0
+    return states, dur, a * (1.0 - e) - RE_KM < 2000.0
+
+
+def mixed_ballistics(is_low, seed: int = 0) -> np.ndarray:
+    """Per-row (A/m, Cd) of the mixed workload: A/m U[0.005, 0.05] m^2/kg
+    where drag applies (perigee below 2000 km), 0 (no drag call) elsewhere."""
+    b = leo_ballistics(len(is_low), seed=seed)
+    b[~np.asarray(is_low), 0] = 0.0
+    return b
+
+
+def ukf_objects(n: int, seed: int = 0):
+    """Means and covariances of the sigma-point workload: LEO means (the
+    distributions of leo_states) and random SPD covariances with position
+    sigmas U[10, 1000] m and velocity sigmas U[0.01, 1] m/s, correlated
+    through a random correlation matrix.  Returns (mean[n][6] km, km/s,
+    cov[n][6][6] km^2 ...)."""
+    rng = np.random.default_rng(seed + 7919)
+    means = leo_states(n, seed=seed)
+    sig = np.concatenate([rng.uniform(10.0, 1000.0, (n, 3)) * 1e-3, rng.uniform(0.01, 1.0, (n, 3)) * 1e-3], axis=1)
+    covs = np.empty((n, 6, 6))
+    for i in range(n):
+        a = rng.normal(size=(6, 6))
+        c = a @ a.T + 6.0 * np.eye(6)
+        d = 1.0 / np.sqrt(np.diag(c))
+        corr = c * d[:, None] * d[None, :]
+        covs[i] = corr * sig[i][:, None] * sig[i][None, :]
+    return means, covs
+
+
+def orbit_period_s(states) -> np.ndarray:
+    """Two-body period of each ECI state (mu = 398600.4415 km^3/s^2)."""
+    s = np.asarray(states, dtype=np.float64).reshape(-1, 6)
+    r = np.linalg.norm(s[:, :3], axis=1)
+    v2 = np.einsum("ij,ij->i", s[:, 3:], s[:, 3:])
+    mu = 398600.4415
+    a = 1.0 / (2.0 / r - v2 / mu)
+    return 2.0 * np.pi * np.sqrt(a ** 3 / mu)

@@ -230,6 +230,38 @@ int bqp_propagate_sampled_device(bqp_ctx* ctx, int64_t n, const double* in,
                                  int32_t out_deltas, double* out, int32_t* status,
                                  int64_t* steps, int64_t* evals);
 
+/* Sigma-point (unscented) covariance propagation: per object, the sigma
+ * points of (mean[6], cov[6][6] row-major) are generated on the device,
+ * propagated as ordinary rows from t0 to tf[i] (epoch, ballistics as for
+ * bqp_propagate_final, ECI in and out), and recombined on the device into
+ * mean_out[6] and the symmetrised cov_out[6][6].  Replaces get_sigmas_ukf
+ * and rebuild_mean_covar_ukf (dust_ukf_rs/src/lib.rs:247-275, 277-312)
+ * around the batch propagation.  sigma_set BQP_SIGMA_JULIER7: the
+ * reference's 7-point simplex at W0 = 0 (lib.rs:22-37, 69-78; alpha, beta,
+ * kappa unused); BQP_SIGMA_MERWE13: the scaled 13-point set of Wan & van der
+ * Merwe (alpha, beta, kappa).  A covariance that does not factorise is
+ * repaired as the reference does (eigenvalues floored at 1e-12,
+ * lib.rs:202-240); status[i] is BQP_ST_INVALID_INPUT when even that fails,
+ * else the first failing sigma row's status.  evals[i] (nullable): force
+ * evaluations over the object's sigma rows. */
+#define BQP_SIGMA_JULIER7 0
+#define BQP_SIGMA_MERWE13 1
+int bqp_sigma_propagate(bqp_ctx* ctx, int64_t n, const double* mean, const double* cov,
+                        int32_t sigma_set, double alpha, double beta, double kappa,
+                        const double* epoch_jd, double t0, const double* tf,
+                        const double* ballistic, double* mean_out, double* cov_out,
+                        int32_t* status, int64_t* evals);
+int bqp_sigma_propagate_device(bqp_ctx* ctx, int64_t n, const double* mean, const double* cov,
+                               int32_t sigma_set, double alpha, double beta, double kappa,
+                               const double* epoch_jd, double t0, const double* tf,
+                               const double* ballistic, double* mean_out, double* cov_out,
+                               int32_t* status, int64_t* evals);
+/* The weights and offsets of a sigma set (host only): points (7 or 13),
+ * wm/wc[points], offsets[7][6] (Julier; zero for Merwe).  Any output may be
+ * NULL. */
+int bqp_sigma_weights(int32_t sigma_set, double alpha, double beta, double kappa, int32_t* points,
+                      double* wm, double* wc, double* offsets);
+
 /* Element conversions on the host (no GPU).  eci_to_equinoctial replaces
  * eci2equinoc_impl (satpy_core/src/lib.rs:1738-1870; ok[i] = 0 on an
  * unbound or degenerate orbit); equinoctial_to_eci replaces equinoc2eci_impl

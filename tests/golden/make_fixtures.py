@@ -20,6 +20,9 @@ repository (the reference tree is not available where the GPU tests run):
   cases: primitive JB2008 inputs -> density, body position -> geodetic
   altitude) plus the Orekit JAR literals pinned in ``jb_rs/src/jb2008.rs``
   (``orekit_local_input`` and the 91 ... 35000 km vectors, rel 5e-13).
+* ``julier7_offsets.json``: the reference's literal sigma-point offsets of the
+  7-point Julier simplex (``dust_ukf_rs/src/lib.rs``, JULIER_WHITENED_OFFSETS),
+  as bit patterns.
 """
 import json
 import re
@@ -122,8 +125,23 @@ def main(ref_root: str = "/root/reference") -> None:
         "literals": lits,
     }
     (HERE / "orekit_jb2008.json").write_text(json.dumps(jb, indent=1) + "\n")
+
+    # 4. The reference's literal Julier simplex offsets (bit patterns)
+    ukf = (crates / "dust_ukf_rs/src/lib.rs").read_text()
+    body = re.search(r"static JULIER_WHITENED_OFFSETS: \[\[f64; DIM\]; NUM_SIGMA\] = \[(.*?)\n\];", ukf,
+                     re.S).group(1)
+    rows = []
+    for row in re.findall(r"\[(.*?)\]", body, re.S):
+        vals = []
+        for tok in [t.strip() for t in row.split(",") if t.strip()]:
+            m = re.match(r"f64::from_bits\((0x[0-9a-f_]+)\)", tok)
+            vals.append(hex_to_f64("0x" + m.group(1)[2:].replace("_", "")) if m else float(tok))
+        rows.append(vals)
+    offs = {"source": "dust_ukf_rs/src/lib.rs (JULIER_WHITENED_OFFSETS)",
+            "offsets": rows, "bits": [[struct.pack(">d", v).hex() for v in r] for r in rows]}
+    (HERE / "julier7_offsets.json").write_text(json.dumps(offs, indent=1) + "\n")
     print("fixtures written:", len(grav["cases"]), "gravity,", len(cases), "jb2008 cases,",
-          len(lits), "jb2008 literals")
+          len(lits), "jb2008 literals,", len(rows), "sigma offset rows")
 
 
 if __name__ == "__main__":
