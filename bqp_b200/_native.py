@@ -71,6 +71,7 @@ SIGNATURES = [
     ("bqp_ctx_info", C.c_int, [_vp, _lp]),
     ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
+    ("bqp_jb_fit_check", C.c_int, [_dp, _dp]),
     ("bqp_ctx_profile", C.c_int, [_vp, C.c_int32]),
     ("bqp_ctx_profile_read", C.c_int, [_vp, _dp, _lp]),
     ("bqp_gravity_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _ip]),
@@ -324,6 +325,14 @@ def sigma_weights(sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0):
                                   dptr(off)))
     p = pts.value
     return p, wm[:p].copy(), wc[:p].copy(), off
+
+
+def jb_fit_check(drivers=(150.0,) * 8 + (20.0,)):
+    """Host-side build and self-check of the JB2008 sweep fits: dict of the
+    worst relative errors and the 2-D fits' T_inf range."""
+    w = np.zeros(6)
+    check(lib().bqp_jb_fit_check(dptr(f64(drivers)), dptr(w)))
+    return {"fixed": w[0], "mid": w[1], "uplow": w[2], "uphigh": w[3], "tinf_range": (w[4], w[5])}
 
 
 def eci_to_equinoctial(eci):

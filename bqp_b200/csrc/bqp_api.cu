@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -200,6 +201,229 @@ void sweep_sums(double tinf, jb::Sweep* lo_out, jb::Sweep* mid_out) {
     *mid_out = boole_sweep(z, lo_out->zend, zr, n, lo_out->gravl / lo_out->tloc, false, tc);
 }
 
+// 2-D fits of the altitude-dependent sweeps (jb2008.cuh, JbFit2), for the
+// T_inf range the context's drivers can produce.  Each segment's series is
+// sampled at Chebyshev points of its reachable log-ratio range and of T_inf
+// (the quadrature itself, as the device would walk it), transformed, and
+// checked at interior points off the sampling grid; a family whose worst
+// error exceeds 1e-13 of max(|sum|, 1) is switched off.
+namespace fit2 {
+
+struct Temp {
+    double tc[4];
+};
+Temp temp_profile(double tinf) {
+    Temp t;
+    const double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * std::exp(-0.0021357 * tinf);
+    const double gsubx = 0.054285714 * (tsubx - 183.0);
+    t.tc[0] = tsubx;
+    t.tc[1] = gsubx;
+    t.tc[2] = (tinf - tsubx) / (kPi / 2);
+    t.tc[3] = gsubx / t.tc[2];
+    return t;
+}
+
+// T_inf bounds for fixed drivers: the diurnal / latitude factor df spans
+// [0, 1] and the local-time / latitude / altitude temperature correction is
+// bounded on a fine grid.
+void tinf_range(const jb::Drivers& d, double* lo, double* hi) {
+    const double fn = std::fmin(std::pow(d.f10b / 240.0, 0.25), 1.0);
+    const double fsb = d.f10b * fn + d.s10b * (1.0 - fn);
+    const double tsubc = 392.4 + 3.227 * fsb + 0.298 * (d.f10 - d.f10b) + 2.259 * (d.s10 - d.s10b) +
+                         0.312 * (d.m10 - d.m10b) + 0.178 * (d.y10 - d.y10b);
+    double cmin = 1e300, cmax = -1e300;
+    for (int ih = 0; ih <= 480; ++ih)
+        for (int ic = 0; ic <= 50; ++ic)
+            for (int ia = 0; ia <= 60; ++ia) {
+                const double v = jb::dtc_correction(d.f10, ih * 0.05, ic * 0.02, 90.0 + ia * 50.0);
+                cmin = std::fmin(cmin, v);
+                cmax = std::fmax(cmax, v);
+            }
+    *lo = std::fmin(tsubc, tsubc * 1.31) + d.dtc + cmin - 10.0;
+    *hi = std::fmax(tsubc, tsubc * 1.31) + d.dtc + cmax + 10.0;
+}
+
+enum Family { kMid = 0, kUpLow = 1, kUpHigh = 2 };
+
+// Where a family's sweep starts and how it is cut, at log-ratio al.
+struct Geometry {
+    double zend_start, zr;
+    int n;
+    double ain_z;  // altitude whose g/T is carried into interval 0
+};
+// n_force > 0 fixes the sweep's interval count (a segment's ends belong to
+// its own count, though floor() at the upper end gives the next one).
+Geometry geometry(Family fam, const jb::JbFit& f1, double al, int n_force = 0) {
+    using namespace jb;
+    Geometry g{};
+    if (fam == kMid) {
+        g.n = n_force > 0 ? n_force : 1 + (int)std::floor(al / kLnStepMiddle);
+        g.zr = std::exp(al / g.n);
+        g.zend_start = f1.low_zend;
+        g.ain_z = f1.low_z;
+    } else if (fam == kUpHigh) {
+        g.n = n_force > 0 ? n_force : 1 + (int)std::floor(al / kLnStepUpper);
+        g.zr = std::exp(al / g.n);
+        g.zend_start = f1.mid_zend;
+        g.ain_z = f1.mid_z;
+    } else {
+        // the state's altitude is 500 exp(-al); its middle sweep's chain
+        // gives the start of the sweep up to 500 km
+        const double alt = 500.0 * std::exp(-al);
+        const double alm = std::log(alt / f1.low_z);
+        const int nm = 1 + (int)std::floor(alm / kLnStepMiddle);
+        double mz, mzend;
+        sweep_chain(f1.low_zend, std::exp(alm / nm), nm, &mz, &mzend);
+        const double alu = std::log(500.0 / mz);
+        g.n = n_force > 0 ? n_force : 1 + (int)std::floor(alu / kLnStepMiddle);
+        g.zr = std::exp(alu / g.n);
+        g.zend_start = mzend;
+        g.ain_z = mz;
+    }
+    return g;
+}
+
+// The quadrature's Boole sum (boole_sweep's arithmetic), leaving out the
+// intervals ex0..ex1.
+double sweep_sum_ex(const Geometry& g, const jb::JbFit& f1, Family fam, const double* tc, int ex0, int ex1) {
+    using namespace jb;
+    double ain = (fam == kMid ? f1.low_gravl : (fam == kUpHigh ? f1.mid_gravl : grav(g.ain_z))) /
+                 local_temp(g.ain_z, tc);
+    double sum = 0.0, zend = g.zend_start;
+    for (int i = 0; i < g.n; ++i) {
+        double zz = zend;
+        zend = g.zr * zz;
+        const double dz = 0.25 * (zend - zz);
+        double sum1 = kW0 * ain;
+        for (int j = 1; j < 5; ++j) {
+            zz += dz;
+            ain = grav(zz) / local_temp(zz, tc);
+            sum1 += (j == 1 || j == 3 ? kW1 : (j == 2 ? kW2 : kW0)) * ain;
+        }
+        if (!(i >= ex0 && i <= ex1)) sum += dz * sum1;
+    }
+    return sum;
+}
+
+double family_sum(Family fam, const jb::JbFit& f1, double al, double tinf, int ex0, int ex1) {
+    const Temp T = temp_profile(tinf);
+    return sweep_sum_ex(geometry(fam, f1, al), f1, fam, T.tc, ex0, ex1);
+}
+
+// Intervals whose nodes (carry included) come within kBreakAbove of the
+// 125 km break of the temperature profile anywhere in [a, b] (where its form
+// changes, the sum has a kink in the altitude): node altitudes grow
+// monotonically with the log-ratio inside a segment, so the two ends, with
+// the segment's own interval count n, bracket them.
+constexpr double kBreakAbove = 1e-6;
+void break_intervals(Family fam, const jb::JbFit& f1, double a, double b, int n, int32_t* ex) {
+    int lo = 1 << 30, hi = -1;
+    for (double al : {a, b}) {
+        const Geometry g = geometry(fam, f1, al, n);
+        double zend = g.zend_start, zlast = g.zend_start;
+        for (int i = 0; i < g.n; ++i) {
+            double zz = zend;
+            zend = g.zr * zz;
+            const double dz = 0.25 * (zend - zz);
+            const double first = std::fmin(zlast, zz);
+            zz += dz;
+            zz += dz;
+            zz += dz;
+            zz += dz;
+            if (first <= 125.0 + kBreakAbove && zz >= 125.0 - 1e-6) {
+                lo = std::min(lo, i);
+                hi = std::max(hi, i);
+            }
+            zlast = zz;
+        }
+    }
+    ex[0] = hi >= 0 ? lo : -1;
+    ex[1] = hi >= 0 ? hi : -1;
+}
+
+bool build_family(Family fam, const jb::JbFit& f1, double tlo, double thi, int nseg, double step, double rlo,
+                  double rhi, double (*rng)[2], int32_t (*ex)[2], double* coef, double* worst) {
+    typedef long double LD;
+    const LD pi = 3.14159265358979323846264338327950288L;
+    const int KA = jb::kFit2A, KT = jb::kFit2T;
+    double w = 0.0;
+    std::vector<double> vals((size_t)KA * KT);
+    std::vector<LD> ca((size_t)KA * KA), ct((size_t)KT * KT);  // cos(pi p (k + 1/2) / K)
+    for (int p = 0; p < KA; ++p)
+        for (int k = 0; k < KA; ++k) ca[(size_t)p * KA + k] = cosl(pi * p * (k + 0.5L) / KA);
+    for (int q = 0; q < KT; ++q)
+        for (int j = 0; j < KT; ++j) ct[(size_t)q * KT + j] = cosl(pi * q * (j + 0.5L) / KT);
+    for (int s = 0; s < nseg; ++s) {
+        double* c = coef + (size_t)s * KA * KT;
+        const double a = std::fmax(s * step, rlo), b = std::fmin((s + 1) * step, rhi);
+        rng[s][0] = a;
+        rng[s][1] = b;
+        ex[s][0] = ex[s][1] = -1;
+        if (!(b > a)) {  // not reachable: an empty series (never used)
+            for (int i = 0; i < KA * KT; ++i) c[i] = 0.0;
+            rng[s][1] = a + 1.0;
+            continue;
+        }
+        break_intervals(fam, f1, a, b, s + 1, ex[s]);
+        for (int k = 0; k < KA; ++k) {
+            const double xa = (double)cosl(pi * (k + 0.5L) / KA);
+            const double al = 0.5 * (a + b) + 0.5 * (b - a) * xa;
+            for (int j = 0; j < KT; ++j) {
+                const double xt = (double)cosl(pi * (j + 0.5L) / KT);
+                vals[(size_t)k * KT + j] =
+                    family_sum(fam, f1, al, 0.5 * (thi + tlo) + 0.5 * (thi - tlo) * xt, ex[s][0], ex[s][1]);
+            }
+        }
+        for (int p = 0; p < KA; ++p)
+            for (int q = 0; q < KT; ++q) {
+                LD acc = 0.0L;
+                for (int k = 0; k < KA; ++k) {
+                    LD row = 0.0L;
+                    for (int j = 0; j < KT; ++j) row += (LD)vals[(size_t)k * KT + j] * ct[(size_t)q * KT + j];
+                    acc += row * ca[(size_t)p * KA + k];
+                }
+                c[(size_t)p * KT + q] = (double)((p == 0 ? 1.0L : 2.0L) / KA * (q == 0 ? 1.0L : 2.0L) / KT * acc);
+            }
+        // check off the sampling grid: series + exact intervals = quadrature
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 5; ++j) {
+                const double fa = (i + 0.37) / 6.0, ft = (j + 0.61) / 5.0;
+                const double al = a + (b - a) * fa, t = tlo + (thi - tlo) * ft;
+                const double full = family_sum(fam, f1, al, t, -1, -1);
+                const double part = family_sum(fam, f1, al, t, ex[s][0], ex[s][1]);
+                const double got = jb::cheb2_eval(c, jb::fit2_x(rng[s], al), (2.0 * t - (thi + tlo)) / (thi - tlo)) +
+                                   (full - part);
+                // the sums enter the density through exp(-sum M / R*): below a
+                // sum of 1 the absolute error is what moves the density
+                w = std::fmax(w, std::fabs(got - full) / std::fmax(std::fabs(full), 1.0));
+            }
+    }
+    *worst = w;
+    return w <= 1e-13;
+}
+
+}  // namespace fit2
+
+// Builds f2 for the drivers; worst[3] = the families' worst relative errors.
+void build_jb_fit2(const jb::JbFit& f1, const jb::Drivers& d, jb::JbFit2& f2, double* worst) {
+    using namespace jb;
+    f2 = JbFit2{};
+    fit2::tinf_range(d, &f2.tlo, &f2.thi);
+    if (!(f1.valid && f2.tlo >= f1.lo && f2.thi <= f1.hi && f2.thi > f2.tlo)) {
+        worst[0] = worst[1] = worst[2] = -1.0;
+        return;
+    }
+    const double lmid_lo = std::log(105.0 / f1.low_z), lmid_hi = std::log(500.0 / f1.low_z);
+    f2.valid_mid = fit2::build_family(fit2::kMid, f1, f2.tlo, f2.thi, kFit2Mid, kLnStepMiddle, lmid_lo, lmid_hi,
+                                      f2.mid_rng, f2.mid_ex, &f2.mid[0][0][0], &worst[0]);
+    f2.valid_uplow = fit2::build_family(fit2::kUpLow, f1, f2.tlo, f2.thi, kFit2UpLow, kLnStepMiddle, 1e-9,
+                                        std::log(500.0 / 105.0), f2.uplow_rng, f2.uplow_ex, &f2.uplow[0][0][0],
+                                        &worst[1]);
+    f2.valid_uphigh = fit2::build_family(fit2::kUpHigh, f1, f2.tlo, f2.thi, kFit2UpHigh, kLnStepUpper,
+                                         std::log(500.0 / f1.mid_z), std::log(2500.0 / f1.mid_z), f2.uphigh_rng,
+                                         f2.uphigh_ex, &f2.uphigh[0][0][0], &worst[2]);
+}
+
 bool build_jb_fit(jb::JbFit& f, double* worst) {
     typedef long double LD;
     const int N = jb::kFitTerms;
@@ -272,6 +496,11 @@ struct bqp_ctx {
     size_t pws_bytes = 0;
     jb::JbFit* d_fit = nullptr;  // JB2008 fixed-node sweep fits (device)
     double fit_worst = -1.0;
+    jb::JbFit h_fit{};            // host copy of the same
+    jb::JbFit2* d_fit2 = nullptr; // altitude-dependent sweep fits for the drivers below
+    double fit2_drivers[9] = {};
+    double fit2_worst[3] = {-1.0, -1.0, -1.0};
+    bool fit2_built = false;
     bool profile = false;  // kernel timing on (bqp_ctx_profile)
     KernelTimes times{};
 };
@@ -338,7 +567,30 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.drivers = {c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
                   c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
     fp.fit = (c.drag_quadrature || !fp.drag) ? nullptr : ctx->d_fit;
+    fp.fit2 = fp.fit ? ctx->d_fit2 : nullptr;
     return fp;
+}
+
+// Builds (once per driver set) the altitude-dependent sweep fits; they are
+// used only where the quadrature would otherwise run and the 1-D fits hold.
+int ensure_fit2(bqp_ctx* ctx) {
+    const bqp_force_config& c = ctx->cfg;
+    if (!(c.force_flags & BQP_FORCE_DRAG) || c.drag_quadrature || !ctx->d_fit) return 0;
+    if (ctx->fit2_built && std::memcmp(ctx->fit2_drivers, c.jb_drivers, sizeof c.jb_drivers) == 0) return 0;
+    std::unique_ptr<jb::JbFit2> f2(new jb::JbFit2());
+    const jb::Drivers d{c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
+                        c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
+    build_jb_fit2(ctx->h_fit, d, *f2, ctx->fit2_worst);
+    if (!ctx->d_fit2) {
+        cudaError_t e = cudaMalloc(&ctx->d_fit2, sizeof(jb::JbFit2));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(JB2008 sweep fits)");
+    }
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaError_t e = cudaMemcpy(ctx->d_fit2, f2.get(), sizeof(jb::JbFit2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "JB2008 sweep fit upload");
+    std::memcpy(ctx->fit2_drivers, c.jb_drivers, sizeof c.jb_drivers);
+    ctx->fit2_built = true;
+    return 0;
 }
 
 CtrlParams ctrl_params(const bqp_ctx* ctx) {
@@ -479,6 +731,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.gtab = ctx->d_tab;
     A.ncells = ctx->ncells;
     A.use_smem = ctx->use_smem;
+    if (int rc = ensure_fit2(ctx)) return rc;
     A.force = force_params(ctx);
     A.ctrl = ctrl_params(ctx);
     A.grav = grav_table(ctx);
@@ -741,7 +994,7 @@ int bqp_ctx_create(const char* text, int64_t len, const bqp_force_config* cfg, b
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(queue)");
     }
     if (!rc) {
-        jb::JbFit fit;
+        jb::JbFit& fit = ctx->h_fit;
         if (build_jb_fit(fit, &ctx->fit_worst)) {
             e = cudaMalloc(&ctx->d_fit, sizeof fit);
             if (e == cudaSuccess) e = cudaMemcpy(ctx->d_fit, &fit, sizeof fit, cudaMemcpyHostToDevice);
@@ -768,6 +1021,7 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_pws) cudaFree(ctx->d_pws);
     if (ctx->d_fit) cudaFree(ctx->d_fit);
     if (ctx->d_tab_split) cudaFree(ctx->d_tab_split);
+    if (ctx->d_fit2) cudaFree(ctx->d_fit2);
     delete ctx;
     return 0;
 }
@@ -790,6 +1044,19 @@ int bqp_ctx_info(const bqp_ctx* ctx, int64_t* info) {
 int bqp_ctx_info_fit(const bqp_ctx* ctx, double* worst_rel) {
     if (!ctx || !worst_rel) return fail(BQP_E_ARG, "null argument");
     *worst_rel = ctx->d_fit ? ctx->fit_worst : -1.0;
+    return 0;
+}
+
+int bqp_jb_fit_check(const double* drivers, double* worst) {
+    if (!drivers || !worst) return fail(BQP_E_ARG, "null argument");
+    jb::JbFit f1;
+    std::unique_ptr<jb::JbFit2> f2(new jb::JbFit2());
+    build_jb_fit(f1, &worst[0]);
+    const jb::Drivers d{drivers[0], drivers[1], drivers[2], drivers[3], drivers[4],
+                        drivers[5], drivers[6], drivers[7], drivers[8]};
+    build_jb_fit2(f1, d, *f2, worst + 1);
+    worst[4] = f2->tlo;
+    worst[5] = f2->thi;
     return 0;
 }
 

@@ -85,6 +85,75 @@ struct JbFit {
     double mid_z, mid_zend, mid_gravl;           // last node of the middle sweep
 };
 
+// Sweeps whose node altitudes move with the state's altitude, fitted in two
+// variables.  Each sweep's interval count n is a step function of altitude
+// (n = 1 + floor(ln(ratio) / step)); inside one n the Boole sum is a smooth
+// function of the log-ratio and of T_inf, so each (family, n) gets a
+// Chebyshev series in both (kFit2A x kFit2T terms, T_inf over the context's
+// own range).  Families:
+//   mid:    105 km -> altitude, 105 < alt < 500 km (after the lower fit)
+//   uplow:  altitude -> 500 km (the hydrogen anchor), 105 < alt < 500 km
+//   uphigh: 500 km -> altitude, 500 < alt <= 2500 km (after the middle fit)
+// The node positions themselves are recomputed exactly (the same chain of
+// multiplications the quadrature walks); only the sum comes from the fit.
+// The host builds and checks every family (build_jb_fit2); a family that
+// misses its error bound is switched off and the quadrature runs.
+constexpr int kFit2A = 12, kFit2T = 20;
+constexpr int kFit2Mid = 64, kFit2UpLow = 64, kFit2UpHigh = 24;
+struct JbFit2 {
+    int32_t valid_mid, valid_uplow, valid_uphigh, pad;
+    double tlo, thi;  // T_inf domain
+    // per segment (index n - 1): the log-ratio range the altitudes of the
+    // family reach inside it, and the series over that range
+    double mid_rng[kFit2Mid][2], uplow_rng[kFit2UpLow][2], uphigh_rng[kFit2UpHigh][2];
+    // intervals [first, last] whose nodes can cross the 125 km break of the
+    // temperature profile inside the segment: left out of the series and
+    // walked exactly ([-1, -1]: none)
+    int32_t mid_ex[kFit2Mid][2], uplow_ex[kFit2UpLow][2], uphigh_ex[kFit2UpHigh][2];
+    double mid[kFit2Mid][kFit2A][kFit2T];
+    double uplow[kFit2UpLow][kFit2A][kFit2T];
+    double uphigh[kFit2UpHigh][kFit2A][kFit2T];
+};
+
+BQP_HD double fit2_x(const double* rng, double al) { return (2.0 * al - (rng[1] + rng[0])) / (rng[1] - rng[0]); }
+
+// 2-D Chebyshev series c[ka][kt] at (xa, xt), both in [-1, 1].
+BQP_HD double cheb2_eval(const double* c, double xa, double xt) {
+    double a1 = 0.0, a2 = 0.0;
+    for (int ka = kFit2A - 1; ka >= 0; --ka) {
+        const double* r = c + ka * kFit2T;
+        double b1 = 0.0, b2 = 0.0;
+        for (int j = kFit2T - 1; j >= 1; --j) {
+            const double tmp = fma(2.0 * xt, b1, -b2) + r[j];
+            b2 = b1;
+            b1 = tmp;
+        }
+        const double v = fma(xt, b1, -b2) + r[0];
+        if (ka == 0) return fma(xa, a1, -a2) + v;
+        const double tmp = fma(2.0 * xa, a1, -a2) + v;
+        a2 = a1;
+        a1 = tmp;
+    }
+    return 0.0;
+}
+
+// Final node altitude and interval end of an n-interval log-spaced chain
+// from zend_start with ratio zr: the same operations the quadrature walks.
+BQP_HD void sweep_chain(double zend_start, double zr, int n, double* z_last, double* zend_out) {
+    double zend = zend_start, zz = zend_start;
+    for (int i = 0; i < n; ++i) {
+        zz = zend;
+        zend = zr * zz;
+        const double dz = 0.25 * (zend - zz);
+        zz += dz;
+        zz += dz;
+        zz += dz;
+        zz += dz;
+    }
+    *z_last = zz;
+    *zend_out = zend;
+}
+
 BQP_HD double cheb_eval(const double* c, int terms, double lo, double hi, double t) {
     const double x = (2.0 * t - (hi + lo)) / (hi - lo);
     double b1 = 0.0, b2 = 0.0;
@@ -480,9 +549,84 @@ __device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr
 
 // density() evaluated by a group of L lanes (q = lane within the group,
 // gmask = the group's lanes).  Same inputs, same error codes.
+// A sweep of n intervals from zend_start whose sum comes from the 2-D fit c
+// at (xa, xt), plus the intervals ex[0]..ex[1] walked exactly (carry ain0
+// into interval 0).  The group of L lanes shares the work: lane q evaluates
+// the series rows ka = q, q + L, ... in T_inf and the exact intervals
+// i = q (mod L); shuffles combine them, and every lane runs the short
+// series in the altitude variable and recomputes the final node.
+template <int L>
+__device__ __forceinline__ SweepG fitted_sweep(const double* c, const int32_t* ex, double xa, double xt,
+                                               double zend_start, double zr, int n, double ain0, const double* tc,
+                                               int q, unsigned gmask) {
+    static_assert(kFit2A % L == 0, "series rows must split evenly over the lanes");
+    constexpr int R = kFit2A / L;
+    SweepG s;
+    // rows of the series in T_inf, this lane's share
+    double v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const double* row = c + (r * L + q) * kFit2T;
+        double b1 = 0.0, b2 = 0.0;
+        for (int j = kFit2T - 1; j >= 1; --j) {
+            const double tmp = fma(2.0 * xt, b1, -b2) + row[j];
+            b2 = b1;
+            b1 = tmp;
+        }
+        v[r] = fma(xt, b1, -b2) + row[0];
+    }
+    // the node chain (every lane), this lane's exact intervals
+    double zend = zend_start, zz = zend_start, zlast = zend_start, exact = 0.0;
+    for (int i = 0; i < n; ++i) {
+        zz = zend;
+        zend = zr * zz;
+        const double dz = 0.25 * (zend - zz);
+        if (i >= ex[0] && i <= ex[1] && (i - ex[0]) % L == q) {
+            double t_, g_, m_;
+            const double carry = i == 0 ? ain0 : node_ain(zlast, tc, false, &t_, &g_, &m_);
+            double sum1 = kW0 * carry, z2 = zz;
+#pragma unroll
+            for (int j = 1; j < 5; ++j) {
+                z2 += dz;
+                sum1 += (j == 1 || j == 3 ? kW1 : (j == 2 ? kW2 : kW0)) * node_ain(z2, tc, false, &t_, &g_, &m_);
+            }
+            exact += dz * sum1;
+        }
+        zz += dz;
+        zz += dz;
+        zz += dz;
+        zz += dz;
+        zlast = zz;
+    }
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) exact += __shfl_xor_sync(gmask, exact, off, L);
+    // the series in the altitude variable over the gathered rows
+    double a1 = 0.0, a2 = 0.0, sum = 0.0;
+#pragma unroll
+    for (int ka = kFit2A - 1; ka >= 0; --ka) {
+        const double vk = L == 1 ? v[ka] : __shfl_sync(gmask, v[ka / L], ka % L, L);
+        if (ka == 0) {
+            sum = fma(xa, a1, -a2) + vk;
+        } else {
+            const double tmp = fma(2.0 * xa, a1, -a2) + vk;
+            a2 = a1;
+            a1 = tmp;
+        }
+    }
+    s.z = zz;
+    s.zend = zend;
+    s.sum = sum + exact;
+    s.tloc = local_temp(s.z, tc);
+    s.gravl = grav(s.z);
+    s.mb = 0.0;
+    s.ain = s.gravl / s.tloc;
+    return s;
+}
+
 template <int L>
 __device__ double density_group(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
-                                const Drivers& d, int q, unsigned gmask, const JbFit* fit = nullptr) {
+                                const Drivers& d, int q, unsigned gmask, const JbFit* fit = nullptr,
+                                const JbFit2* fit2 = nullptr) {
     double code = 0.0;
     if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) || !isfinite(alt_m) ||
         !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) || !isfinite(d.s10b) || !isfinite(d.m10) ||
@@ -537,6 +681,9 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
     const double mb1 = mbar(z1);
     const double tloc1 = local_temp(z1, tc);
     const bool use_fit = fit_covers(fit, tinf);
+    // the 2-D fits need the lower (and, above 500 km, the middle) 1-D fits
+    const bool use2 = use_fit && fit2 != nullptr && tinf >= fit2->tlo && tinf <= fit2->thi;
+    const double xt2 = use2 ? (2.0 * tinf - (fit2->thi + fit2->tlo)) / (fit2->thi - fit2->tlo) : 0.0;
     SweepG lo;
     if (use_fit && alt >= 105.0) {
         lo.sum = cheb_eval(fit->low, fit->terms, fit->lo, fit->hi, tinf);
@@ -576,14 +723,27 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
             al = log(fmin(alt, 500.0) / z);
             n = 1 + (int)floor(al / kLnStepMiddle);
             zr = exp(al / n);
-            mid = boole_sweep_group<L>(lo.zend, zr, n, lo.gravl / tloc2, false, tc, q, gmask);
+            if (use2 && fit2->valid_mid && alt < 500.0 && n >= 1 && n <= kFit2Mid)
+                mid = fitted_sweep<L>(&fit2->mid[n - 1][0][0], fit2->mid_ex[n - 1], fit2_x(fit2->mid_rng[n - 1], al),
+                                      xt2, lo.zend, zr, n, lo.gravl / tloc2, tc, q, gmask);
+            else
+                mid = boole_sweep_group<L>(lo.zend, zr, n, lo.gravl / tloc2, false, tc, q, gmask);
         }
         const double tloc3 = mid.tloc;
         z = mid.z;
         al = log(fmax(alt, 500.0) / z);
-        n = 1 + (int)floor(al / (alt > 500.0 ? kLnStepUpper : kLnStepMiddle));
+        const double ustep = alt > 500.0 ? kLnStepUpper : kLnStepMiddle;
+        n = 1 + (int)floor(al / ustep);
         zr = exp(al / n);
-        const SweepG up = boole_sweep_group<L>(mid.zend, zr, n, mid.ain, false, tc, q, gmask);
+        SweepG up;
+        if (use2 && alt < 500.0 && fit2->valid_uplow && fit2->valid_mid && n >= 1 && n <= kFit2UpLow)
+            up = fitted_sweep<L>(&fit2->uplow[n - 1][0][0], fit2->uplow_ex[n - 1],
+                                 fit2_x(fit2->uplow_rng[n - 1], al), xt2, mid.zend, zr, n, mid.ain, tc, q, gmask);
+        else if (use2 && alt > 500.0 && fit2->valid_uphigh && n >= 1 && n <= kFit2UpHigh)
+            up = fitted_sweep<L>(&fit2->uphigh[n - 1][0][0], fit2->uphigh_ex[n - 1],
+                                 fit2_x(fit2->uphigh_rng[n - 1], al), xt2, mid.zend, zr, n, mid.ain, tc, q, gmask);
+        else
+            up = boole_sweep_group<L>(mid.zend, zr, n, mid.ain, false, tc, q, gmask);
         const double tloc4 = up.tloc;
         z = up.z;
         double altr, hsign;

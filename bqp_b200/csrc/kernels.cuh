@@ -40,6 +40,7 @@ struct ForceParams {
     double mu_sun, mu_moon;
     jb::Drivers drivers;
     const jb::JbFit* fit;  // device copy of the fixed-node sweep fits, or null
+    const jb::JbFit2* fit2;  // altitude-dependent sweep fits (stage-synchronous drag), or null
 };
 
 // Solver controls (IntegratorConfig, solver.rs:35-60 and integrator.rs:404-558).

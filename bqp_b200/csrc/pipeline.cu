@@ -251,7 +251,8 @@ __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, in
             const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
             const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
             const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask, fp.fit);
+            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask, fp.fit,
+                                       fp.fit2);
             if (!(rho > 0.0) || !isfinite(rho)) rho = NAN;
             else if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         }
@@ -383,9 +384,10 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
-    // drag lanes per state: 4 above ~510 km (sweep fits, a short upper
-    // sweep), 16 below (the 105 km -> altitude sweep walks ~60 intervals)
-    constexpr int kLanesHigh = 4, kLanesLow = 16;
+    // drag lanes per state (they share the sweep series and the intervals
+    // walked exactly): 2 above ~510 km, 4 below (two altitude-dependent
+    // sweeps there)
+    constexpr int kLanesHigh = 2, kLanesLow = 4;
     const int dblocks_hi = (int)((A.n * kLanesHigh + kBlock - 1) / kBlock);
     const int dblocks_lo = (int)((A.n * kLanesLow + kBlock - 1) / kBlock);
     const int nt = gslots == 1 || gslots == 2 ? gslots : 4;

@@ -145,6 +145,14 @@ int bqp_ctx_profile(bqp_ctx* ctx, int32_t on);
  * milliseconds, launches[BQP_KCLASSES] kernel launches. */
 int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches);
 
+/* Builds, on the host only, the JB2008 sweep fits for a driver set
+ * (drivers[9] as in bqp_force_config) and reports their self-check:
+ * worst[0] the fixed-node 1-D fits, worst[1..3] the altitude-dependent 2-D
+ * families (middle, up to 500 km, above 500 km; -1 when not built), worst[4],
+ * worst[5] the T_inf range of the 2-D fits.  No counterpart in the
+ * reference, whose quadrature these fits replace. */
+int bqp_jb_fit_check(const double* drivers, double* worst6);
+
 /* Replace the force/solver settings of a context (the field is kept; the
  * order may only shrink up to the parsed order). */
 int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);

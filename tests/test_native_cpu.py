@@ -121,3 +121,15 @@ def test_synthetic_field_rule():
     hi = np.array([float(r[2]) for r in rows if int(r[0]) == 70])
     assert 0.3e-5 / 4900 < hi.std() < 3e-5 / 4900
     assert all(float(r[3]) == 0.0 for r in rows if r[1] == "0")
+
+
+@pytest.mark.parametrize("level", [70.0, 150.0, 250.0])
+def test_jb2008_sweep_fits_self_check(level):
+    """The host-built sweep fits (1-D fixed-node, 2-D altitude-dependent)
+    reproduce the Boole quadrature they replace, for quiet to active drivers."""
+    w = N.jb_fit_check((level,) * 8 + (20.0,))
+    assert 0 <= w["fixed"] <= 4e-15
+    for fam in ("mid", "uplow", "uphigh"):
+        assert 0 <= w[fam] <= 1e-13, (fam, w[fam])
+    lo, hi = w["tinf_range"]
+    assert 300.0 < lo < hi < 3500.0
