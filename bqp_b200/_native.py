@@ -93,6 +93,7 @@ SIGNATURES = [
     ("bqp_sigma_propagate_device", C.c_int, [_vp, C.c_int64, _vp, _vp, C.c_int32, C.c_double, C.c_double,
                                              C.c_double, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("bqp_sigma_weights", C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]),
+    ("bqp_gemm_bf16_device", C.c_int, [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp]),
     ("bqp_eci_to_equinoctial", C.c_int, [C.c_int64, _dp, _dp, _ip]),
     ("bqp_equinoctial_to_eci", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),

@@ -1592,3 +1592,25 @@ int bqp_sigma_propagate(bqp_ctx* ctx, int64_t n, const double* mean, const doubl
 }
 
 }  // extern "C"
+
+// ======================================================================
+// Tensor-core GEMM of the gravity surrogate, exported for its tests.
+extern "C" int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void* a, const void* b, float* c,
+                                    void* stream) {
+    if (m < 0 || n < 0 || k < 0 || (m && n && k && (!a || !b || !c))) return fail(BQP_E_ARG, "bad GEMM arguments");
+    if (m % 128 || n % 256 || k % 64)
+        return fail(BQP_E_ARG, "GEMM shape %lld x %lld x %lld: M must be a multiple of 128, N of 256, K of 64",
+                    (long long)m, (long long)n, (long long)k);
+    int* derr = nullptr;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMallocAsync(&derr, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = launch_gemm_bf16(m, n, k, a, b, c, derr, s);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (derr) cudaFreeAsync(derr, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_gemm_bf16");
+    if (herr) return fail(BQP_E_CUDA, "tensor-core GEMM: an mbarrier wait timed out");
+    return 0;
+}

@@ -90,5 +90,9 @@ cudaError_t launch_sigma_recombine(int64_t n, int S, const double* wm, const dou
                                    const int32_t* row_status, const int64_t* row_evals, double* mean_out,
                                    double* cov_out, int32_t* status, int64_t* evals, cudaStream_t st);
 int device_sm_count();
+// C[M x N] (FP32) = A[M x K] B[N x K]^T, BF16 row-major operands (mlp.cu);
+// M % 128, N % 256, K % 64 == 0.  *err is set if a wait timed out.
+cudaError_t launch_gemm_bf16(int64_t M, int64_t N, int64_t K, const void* A, const void* B, float* C, int* err,
+                             cudaStream_t st);
 
 }  // namespace bqp

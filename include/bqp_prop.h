@@ -270,6 +270,13 @@ int bqp_sigma_propagate_device(bqp_ctx* ctx, int64_t n, const double* mean, cons
 int bqp_sigma_weights(int32_t sigma_set, double alpha, double beta, double kappa, int32_t* points,
                       double* wm, double* wc, double* offsets);
 
+/* BF16 tensor-core GEMM of the gravity surrogate, exported for its tests (no
+ * counterpart in the reference): c[m][n] (FP32) = a[m][k] b[n][k]^T with
+ * BF16 row-major device operands, m % 128 == 0, n % 256 == 0, k % 64 == 0;
+ * enqueued on `stream` and synchronised. */
+int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void* a, const void* b, float* c,
+                         void* stream);
+
 /* Element conversions on the host (no GPU).  eci_to_equinoctial replaces
  * eci2equinoc_impl (satpy_core/src/lib.rs:1738-1870; ok[i] = 0 on an
  * unbound or degenerate orbit); equinoctial_to_eci replaces equinoc2eci_impl

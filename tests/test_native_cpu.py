@@ -133,3 +133,11 @@ def test_jb2008_sweep_fits_self_check(level):
         assert 0 <= w[fam] <= 1e-13, (fam, w[fam])
     lo, hi = w["tinf_range"]
     assert 300.0 < lo < hi < 3500.0
+
+
+def test_tensor_core_gemm_rejects_unsupported_shapes_before_device_use():
+    lib = N.lib()
+    dummy = C.c_void_p(16)
+    for m, n, k in [(100, 256, 64), (128, 200, 64), (128, 256, 48)]:
+        rc = lib.bqp_gemm_bf16_device(m, n, k, dummy, dummy, dummy, None)
+        assert rc == N.E_ARG and b"multiple" in lib.bqp_last_error()
