@@ -18,6 +18,7 @@ LIB_PATH = _build.LIB
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _lp = C.POINTER(C.c_int64)
+_fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
 
 # per-trajectory status codes (BQP_ST_*)
@@ -35,6 +36,8 @@ ENGINES = {"pipeline": 0, "persistent": 1}
 E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5
 NOALLOC_MAX_TRAJ = 16384  # BQP_NOALLOC_MAX_TRAJ
 KERNEL_CLASSES = ("prep", "gravity", "drag", "control", "persistent")  # BQP_KCLASS_*
+SURROGATE_PARAMS = 199427  # BQP_SURROGATE_PARAMS
+SURROGATE_DEGREE = 8  # BQP_SURROGATE_DEGREE
 
 
 class ForceConfig(C.Structure):
@@ -94,6 +97,11 @@ SIGNATURES = [
                                              C.c_double, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("bqp_sigma_weights", C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]),
     ("bqp_gemm_bf16_device", C.c_int, [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp]),
+    ("bqp_surrogate_train", C.c_int, [_vp, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64, _dp]),
+    ("bqp_surrogate_infer", C.c_int, [_vp, C.c_int64, _dp, _dp, C.c_int32]),
+    ("bqp_surrogate_params", C.c_int, [_vp, _fp, _dp]),
+    ("bqp_surrogate_set_params", C.c_int, [_vp, _fp, C.c_double]),
+    ("bqp_surrogate_grad", C.c_int, [_vp, C.c_int32, _fp, _fp, _fp, _fp, _dp, _fp]),
     ("bqp_eci_to_equinoctial", C.c_int, [C.c_int64, _dp, _dp, _ip]),
     ("bqp_equinoctial_to_eci", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),
@@ -297,6 +305,45 @@ class Context:
                                         dptr(ep), float(t0), dptr(tfa), None if bal is None else dptr(bal),
                                         dptr(mo), dptr(co), iptr(st), lptr(ev)))
         return mo, co.reshape(n, 6, 6), st, ev
+
+    # ------------------------------------------------------------ surrogate
+    def surrogate_train(self, samples=1 << 20, epochs=4, batch=8192, lr=2e-3, seed=1):
+        """Train the degree > 8 gravity surrogate on the GPU; returns the
+        per-epoch training loss (normalised MSE)."""
+        loss = np.zeros(epochs)
+        check(lib().bqp_surrogate_train(self._h, int(samples), int(epochs), int(batch), float(lr), int(seed),
+                                        dptr(loss)))
+        return loss
+
+    def surrogate_infer(self, pos_km, add_low=True):
+        p = f64(pos_km).reshape(-1, 3)
+        acc = np.empty_like(p)
+        check(lib().bqp_surrogate_infer(self._h, p.shape[0], dptr(p), dptr(acc), int(add_low)))
+        return acc
+
+    def surrogate_params(self):
+        params = np.zeros(SURROGATE_PARAMS, dtype=np.float32)
+        sigma = C.c_double(0.0)
+        check(lib().bqp_surrogate_params(self._h, params.ctypes.data_as(_fp), C.byref(sigma)))
+        return params, sigma.value
+
+    def surrogate_set_params(self, params, sigma):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == SURROGATE_PARAMS
+        check(lib().bqp_surrogate_set_params(self._h, p.ctypes.data_as(_fp), float(sigma)))
+
+    def surrogate_grad(self, params, x, t):
+        """(loss, grad[SURROGATE_PARAMS], y[B][3]) of one batch on the GPU."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        xb = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 4)
+        tb = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, 3)
+        g = np.zeros(SURROGATE_PARAMS, dtype=np.float32)
+        y = np.zeros((xb.shape[0], 3), dtype=np.float32)
+        loss = C.c_double(0.0)
+        check(lib().bqp_surrogate_grad(self._h, xb.shape[0], p.ctypes.data_as(_fp), xb.ctypes.data_as(_fp),
+                                       tb.ctypes.data_as(_fp), g.ctypes.data_as(_fp), C.byref(loss),
+                                       y.ctypes.data_as(_fp)))
+        return loss.value, g, y
 
     # -------------------------------------------------------------- device
     def propagate_final_device(self, d_in, d_epoch, d_tf, d_out, d_status, d_steps=None, d_evals=None,

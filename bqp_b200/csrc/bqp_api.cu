@@ -20,6 +20,7 @@
 
 #include "../../include/bqp_prop.h"
 #include "launch.h"
+#include "surrogate.h"
 
 using namespace bqp;
 
@@ -503,6 +504,9 @@ struct bqp_ctx {
     bool fit2_built = false;
     bool profile = false;  // kernel timing on (bqp_ctx_profile)
     KernelTimes times{};
+    Model* sur = nullptr;          // learned gravity surrogate (bqp_surrogate_*)
+    double* d_tab_low = nullptr;   // FP64 table of degrees <= BQP_SURROGATE_DEGREE
+    uint32_t low_bytes = 0;
 };
 
 namespace {
@@ -1022,6 +1026,8 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_fit) cudaFree(ctx->d_fit);
     if (ctx->d_tab_split) cudaFree(ctx->d_tab_split);
     if (ctx->d_fit2) cudaFree(ctx->d_fit2);
+    if (ctx->d_tab_low) cudaFree(ctx->d_tab_low);
+    delete ctx->sur;
     delete ctx;
     return 0;
 }
@@ -1614,3 +1620,142 @@ extern "C" int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void*
     if (herr) return fail(BQP_E_CUDA, "tensor-core GEMM: an mbarrier wait timed out");
     return 0;
 }
+
+// ======================================================================
+// Learned gravity surrogate (surrogate.cu).
+namespace {
+
+GravTable plain_table(const bqp_ctx* ctx) {
+    GravTable T{};
+    T.tab = ctx->d_tab;
+    T.order = ctx->cfg.order;
+    T.ls = 0;
+    T.bytes = (uint32_t)ctx->tab_bytes;
+    T.in_smem = T.bytes <= kSmemLimit ? 1 : 0;
+    return T;
+}
+
+int ensure_low_table(bqp_ctx* ctx) {
+    if (ctx->d_tab_low) return 0;
+    if (ctx->parsed_order < BQP_SURROGATE_DEGREE)
+        return fail(BQP_E_ARG, "the surrogate needs a field of degree > %d", BQP_SURROGATE_DEGREE);
+    std::vector<double> tab = build_gravity_table(ctx->coeffs, BQP_SURROGATE_DEGREE);
+    ctx->low_bytes = (uint32_t)(tab.size() * sizeof(double));
+    cudaError_t e = cudaMalloc(&ctx->d_tab_low, ctx->low_bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->d_tab_low, tab.data(), ctx->low_bytes, cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "surrogate low-degree table");
+}
+
+GravTable low_table(const bqp_ctx* ctx) {
+    GravTable T{};
+    T.tab = ctx->d_tab_low;
+    T.order = BQP_SURROGATE_DEGREE;
+    T.ls = 0;
+    T.bytes = ctx->low_bytes;
+    T.in_smem = 1;
+    return T;
+}
+
+int surrogate_ready(bqp_ctx* ctx, bool need_trained) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    if ((rc = ensure_low_table(ctx))) return rc;
+    if (!ctx->sur) ctx->sur = new Model();
+    if (need_trained && !ctx->sur->trained) return fail(BQP_E_ARG, "the surrogate has not been trained or loaded");
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bqp_surrogate_train(bqp_ctx* ctx, int64_t samples, int32_t epochs, int32_t batch, double lr, uint64_t seed,
+                        double* loss_per_epoch) {
+    int rc = surrogate_ready(ctx, false);
+    if (rc) return rc;
+    if (ctx->cfg.order <= BQP_SURROGATE_DEGREE)
+        return fail(BQP_E_ARG, "the surrogate learns degrees above %d; the context's order is %d", BQP_SURROGATE_DEGREE,
+                    ctx->cfg.order);
+    if (samples < 1024 || epochs < 1 || batch < 128 || batch % 128 || batch > 65536 || !(lr > 0.0))
+        return fail(BQP_E_ARG, "samples >= 1024, epochs >= 1, batch a multiple of 128 up to 65536, lr > 0");
+    const GravTable full = plain_table(ctx), low = low_table(ctx);
+    cudaStream_t s = ctx->stream;
+    FieldFn ffull = [&](int64_t n, const double* pos, double* acc) {
+        return launch_gravity(full, n, pos, acc, nullptr, s, 256, 4);
+    };
+    FieldFn flow = [&](int64_t n, const double* pos, double* acc) {
+        return launch_gravity(low, n, pos, acc, nullptr, s, 256, 4);
+    };
+    TrainArgs a{samples, epochs, batch, lr, seed};
+    cudaError_t e = train(*ctx->sur, a, ffull, flow, s, loss_per_epoch);
+    if (e == cudaErrorLaunchTimeout) return fail(BQP_E_CUDA, "surrogate training: a tensor-core wait timed out");
+    return e == cudaSuccess ? 0 : cuda_fail(e, "surrogate training");
+}
+
+int bqp_surrogate_infer(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc, int32_t add_low) {
+    int rc = surrogate_ready(ctx, true);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!pos_km || !acc))) return fail(BQP_E_ARG, "bad buffers");
+    if (n == 0) return 0;
+    double *dp = nullptr, *da = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        Carve cv{pass ? (char*)ctx->d_ws : nullptr};
+        dp = cv.take<double>((size_t)n * 3);
+        da = cv.take<double>((size_t)n * 3);
+        if (!pass && (rc = ensure_ws(ctx, cv.off))) return rc;
+    }
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(dp, pos_km, (size_t)n * 24, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && add_low) e = launch_gravity(low_table(ctx), n, dp, da, nullptr, s, 256, 4);
+    if (e == cudaSuccess) e = infer(*ctx->sur, n, dp, da, add_low ? 1 : 0, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(acc, da, (size_t)n * 24, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_infer");
+}
+
+int bqp_surrogate_params(bqp_ctx* ctx, float* params, double* sigma) {
+    int rc = surrogate_ready(ctx, true);
+    if (rc) return rc;
+    if (!params || !sigma) return fail(BQP_E_ARG, "null argument");
+    cudaError_t e = cudaMemcpy(params, ctx->sur->P, sg::kParams * 4, cudaMemcpyDeviceToHost);
+    *sigma = ctx->sur->sigma;
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_params");
+}
+
+int bqp_surrogate_set_params(bqp_ctx* ctx, const float* params, double sigma) {
+    int rc = surrogate_ready(ctx, false);
+    if (rc) return rc;
+    if (!params || !(sigma > 0.0)) return fail(BQP_E_ARG, "null parameters or sigma <= 0");
+    cudaError_t e = upload_params(*ctx->sur, params, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    ctx->sur->sigma = sigma;
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_set_params");
+}
+
+int bqp_surrogate_grad(bqp_ctx* ctx, int32_t batch, const float* params, const float* x, const float* t,
+                       float* grad, double* loss, float* y) {
+    int rc = surrogate_ready(ctx, false);
+    if (rc) return rc;
+    if (batch < 128 || batch % 128 || batch > 65536 || !params || !x || !t || !grad || !loss)
+        return fail(BQP_E_ARG, "batch a multiple of 128 up to 65536 and non-null buffers");
+    Model& M = *ctx->sur;
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = upload_params(M, params, s);
+    if (e == cudaSuccess) e = M.alloc_batch(batch);
+    if (e == cudaSuccess && !M.G) e = cudaMalloc(&M.G, sg::kParams * 4);
+    M.dsum = reinterpret_cast<double*>(reinterpret_cast<char*>(M.derr) + 16);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M.xb, x, (size_t)batch * 16, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M.tb, t, (size_t)batch * 12, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M.derr, 0, 32, s);
+    if (e == cudaSuccess) e = forward_backward(M, batch, true, s);
+    double lsum = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grad, M.G, sg::kParams * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&lsum, M.dsum, 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && y) e = cudaMemcpyAsync(y, M.y, (size_t)batch * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    *loss = lsum / (3.0 * batch);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_grad");
+}
+
+}  // extern "C"

@@ -1,0 +1,552 @@
+// Learned gravity surrogate: an MLP that predicts the acceleration of the
+// spherical-harmonic degrees above 8 (the residual over the low-degree field),
+// trained on the GPU on samples the exact harmonic kernel produces.
+//
+//   input   x = (u_x, u_y, u_z, (r - r_mid) / r_half)   body-fixed unit vector, scaled radius
+//   layers  4 -> 256 -> 256 -> 256 -> 256 -> 3, SiLU after each hidden layer
+//   output  t = (a_full - a_low) (r / R)^2 / sigma        (sigma: RMS of the scaled residual)
+//
+// The three 256 x 256 layers run on the tensor cores in BF16 with FP32
+// accumulation (tc_gemm.cuh) in the forward pass and in both backward
+// products (dH = dZ W, dW = dZ^T H); the 4-wide input layer, the 3-wide
+// output layer, bias + SiLU, the transposes, the column sums and Adam run on
+// the CUDA cores in FP32.  Parameters are FP32 masters with BF16 copies (and
+// transposed copies) for the tensor cores.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "launch.h"
+#include "surrogate.h"
+
+namespace bqp {
+namespace sg {
+
+namespace {
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f + z * (1.0f - s));
+}
+
+// SplitMix64 of (seed, i): uniform doubles for the sample positions.
+__device__ __forceinline__ uint64_t mix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__device__ __forceinline__ double u01(uint64_t seed, uint64_t i, int k) {
+    return (double)(mix(seed ^ (i * 4 + k) * 0xD1B54A32D192ED03ull) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace
+
+// positions uniform in radius [r_lo, r_hi] and on the sphere
+__global__ void k_sample(int64_t n, uint64_t seed, double r_lo, double r_hi, double* __restrict__ pos) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double r = r_lo + (r_hi - r_lo) * u01(seed, i, 0);
+    const double z = 2.0 * u01(seed, i, 1) - 1.0;
+    const double phi = 2.0 * 3.14159265358979323846 * u01(seed, i, 2);
+    const double s = sqrt(fmax(0.0, 1.0 - z * z));
+    pos[3 * i] = r * s * cos(phi);
+    pos[3 * i + 1] = r * s * sin(phi);
+    pos[3 * i + 2] = r * z;
+}
+
+// network input of a position; scaled target (a_full - a_low)(r/R)^2 (before sigma)
+__global__ void k_features(int64_t n, const double* __restrict__ pos, const double* __restrict__ a_full,
+                           const double* __restrict__ a_low, float* __restrict__ x, double* __restrict__ t,
+                           Scale sc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    const double r = sqrt(px * px + py * py + pz * pz);
+    x[4 * i] = (float)(px / r);
+    x[4 * i + 1] = (float)(py / r);
+    x[4 * i + 2] = (float)(pz / r);
+    x[4 * i + 3] = (float)((r - sc.r_mid) / sc.r_half);
+    if (t) {
+        const double f = (r / sc.R) * (r / sc.R);
+        for (int k = 0; k < 3; ++k) t[3 * i + k] = (a_full[3 * i + k] - a_low[3 * i + k]) * f;
+    }
+}
+
+// sum of squares (for sigma), one block-level partial per block
+__global__ void k_sumsq(int64_t n, const double* __restrict__ v, double* __restrict__ out) {
+    __shared__ double part[256];
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += v[i] * v[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, part[0]);
+}
+
+__global__ void k_scale_targets(int64_t n, const double* __restrict__ t, const double* __restrict__ sumsq,
+                                float* __restrict__ tf, double* sigma_out) {
+    const double sigma = sqrt(*sumsq / (double)n);
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *sigma_out = sigma;
+    if (i >= n) return;
+    tf[i] = (float)(t[i] / sigma);
+}
+
+// minibatch gather: rows idx = hash(step, b) % n
+__global__ void k_gather(int B, int64_t n, uint64_t seed, uint64_t step, const float* __restrict__ x,
+                         const float* __restrict__ t, float* __restrict__ xb, float* __restrict__ tb) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const int64_t i = (int64_t)(mix(seed ^ (step * 0x9E3779B97F4A7C15ull + b)) % (uint64_t)n);
+    for (int k = 0; k < 4; ++k) xb[4 * b + k] = x[4 * i + k];
+    if (t)
+        for (int k = 0; k < 3; ++k) tb[3 * b + k] = t[3 * i + k];
+}
+
+// input layer: z0 = W0 x + b0, h0 = SiLU(z0)
+__global__ void k_in_layer(int B, const float* __restrict__ xb, const float* __restrict__ P, float* __restrict__ z,
+                           __nv_bfloat16* __restrict__ h) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)B * kH) return;
+    const int b = (int)(e / kH), j = (int)(e % kH);
+    const float* W0 = P + kOffW0;
+    float s = P[kOffB0 + j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s = fmaf(W0[j * 4 + k], xb[4 * b + k], s);
+    z[e] = s;
+    h[e] = __float2bfloat16(silu(s));
+}
+
+// hidden layer epilogue: z += b, h = SiLU(z)
+__global__ void k_bias_silu(int B, float* __restrict__ z, const float* __restrict__ bias,
+                            __nv_bfloat16* __restrict__ h) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)B * kH) return;
+    const float v = z[e] + bias[e % kH];
+    z[e] = v;
+    h[e] = __float2bfloat16(silu(v));
+}
+
+// output layer (one thread per row): y = W4 h3 + b4; with targets, the loss
+// and dY = 2 (y - t) / (3 B)
+__global__ void k_out_layer(int B, const __nv_bfloat16* __restrict__ h, const float* __restrict__ P,
+                            const float* __restrict__ tb, float* __restrict__ y, float* __restrict__ dy,
+                            double* __restrict__ loss) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (b < B) {
+        const float* W4 = P + kOffW4;
+        float o[3] = {P[kOffB4], P[kOffB4 + 1], P[kOffB4 + 2]};
+        for (int j = 0; j < kH; ++j) {
+            const float hj = __bfloat162float(h[(size_t)b * kH + j]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) o[k] = fmaf(W4[k * kH + j], hj, o[k]);
+        }
+        for (int k = 0; k < 3; ++k) {
+            if (y) y[3 * b + k] = o[k];
+            if (tb) {
+                const float d = o[k] - tb[3 * b + k];
+                dy[3 * b + k] = 2.0f * d / (3.0f * (float)B);
+                l += d * d;
+            }
+        }
+    }
+    if (tb && loss) {
+        for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(loss, (double)l);
+    }
+}
+
+// dZ3 = (dY W4) * SiLU'(z3), BF16
+__global__ void k_out_back(int B, const float* __restrict__ dy, const float* __restrict__ P,
+                           const float* __restrict__ z, __nv_bfloat16* __restrict__ dz) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)B * kH) return;
+    const int b = (int)(e / kH), j = (int)(e % kH);
+    const float* W4 = P + kOffW4;
+    const float g = dy[3 * b] * W4[j] + dy[3 * b + 1] * W4[kH + j] + dy[3 * b + 2] * W4[2 * kH + j];
+    dz[e] = __float2bfloat16(g * silu_grad(z[e]));
+}
+
+// dZ = dH * SiLU'(z), BF16
+__global__ void k_silu_back(int B, const float* __restrict__ dh, const float* __restrict__ z,
+                            __nv_bfloat16* __restrict__ dz) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)B * kH) return;
+    dz[e] = __float2bfloat16(dh[e] * silu_grad(z[e]));
+}
+
+// [rows][cols] -> [cols][rows], BF16, 32 x 32 tiles
+__global__ void k_transpose(int rows, int cols, const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ out) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[k][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][k];
+    }
+}
+
+// column sums of a [B][cols] BF16 matrix (bias gradients); one block per column
+__global__ void k_colsum(int B, int cols, const __nv_bfloat16* __restrict__ m, float* __restrict__ out) {
+    __shared__ float part[256];
+    const int c = blockIdx.x;
+    float s = 0.0f;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) s += __bfloat162float(m[(size_t)b * cols + c]);
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = part[0];
+}
+
+// output and input layer weight gradients (small reductions over the batch)
+__global__ void k_small_grads(int B, const float* __restrict__ dy, const __nv_bfloat16* __restrict__ h3,
+                              const __nv_bfloat16* __restrict__ dz0, const float* __restrict__ xb,
+                              float* __restrict__ G) {
+    __shared__ float part[256];
+    // blocks 0..767: dW4[k][j]; 768..770: db4[k]; 771..1794: dW0[j][k]
+    const int id = blockIdx.x;
+    float s = 0.0f;
+    if (id < 3 * kH) {
+        const int k = id / kH, j = id % kH;
+        for (int b = threadIdx.x; b < B; b += blockDim.x) s += dy[3 * b + k] * __bfloat162float(h3[(size_t)b * kH + j]);
+    } else if (id < 3 * kH + 3) {
+        const int k = id - 3 * kH;
+        for (int b = threadIdx.x; b < B; b += blockDim.x) s += dy[3 * b + k];
+    } else {
+        const int q = id - 3 * kH - 3, j = q / 4, k = q % 4;
+        for (int b = threadIdx.x; b < B; b += blockDim.x) s += __bfloat162float(dz0[(size_t)b * kH + j]) * xb[4 * b + k];
+    }
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (id < 3 * kH) G[kOffW4 + id] = part[0];
+        else if (id < 3 * kH + 3) G[kOffB4 + id - 3 * kH] = part[0];
+        else G[kOffW0 + id - 3 * kH - 3] = part[0];
+    }
+}
+
+// Adam on the FP32 masters; refresh the BF16 copies of the hidden layers
+__global__ void k_adam(int64_t n, float* __restrict__ P, const float* __restrict__ G, float* __restrict__ m1,
+                       float* __restrict__ m2, float lr, float b1, float b2, float c1, float c2, float eps) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float g = G[i];
+    const float a = b1 * m1[i] + (1.0f - b1) * g;
+    const float v = b2 * m2[i] + (1.0f - b2) * g * g;
+    m1[i] = a;
+    m2[i] = v;
+    P[i] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
+}
+
+__global__ void k_to_bf16(const float* __restrict__ P, __nv_bfloat16* __restrict__ W, __nv_bfloat16* __restrict__ Wt) {
+    // the three hidden matrices: W[l][o][i] and W^T[l][i][o]
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3ll * kH * kH) return;
+    const int l = (int)(e / (kH * kH)), o = (int)((e / kH) % kH), i = (int)(e % kH);
+    const float w = P[kOffW1 + e];
+    W[e] = __float2bfloat16(w);
+    Wt[(size_t)l * kH * kH + (size_t)i * kH + o] = __float2bfloat16(w);
+}
+
+// residual acceleration from the network output: sigma * y * (R/r)^2
+__global__ void k_residual(int64_t n, const double* __restrict__ pos, const float* __restrict__ y, Scale sc,
+                           double sigma, double* __restrict__ acc, int add) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    const double r2 = px * px + py * py + pz * pz;
+    const double f = sigma * (sc.R * sc.R) / r2;
+    for (int k = 0; k < 3; ++k) acc[3 * i + k] = (add ? acc[3 * i + k] : 0.0) + f * (double)y[3 * i + k];
+}
+
+}  // namespace sg
+
+// ---------------------------------------------------------------- host side
+namespace {
+
+inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+Model::~Model() { release(); }
+
+void Model::release() {
+    // dsum points into derr and is not freed on its own
+    void* ptrs[] = {P, G, m1, m2, W, Wt, x, t, xb, tb, z[0], z[1], z[2], z[3], h[0], h[1], h[2], h[3], dz[0], dz[1],
+                    dz[2], dz[3], dzt, ht, dh, y, dy, derr};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    P = G = m1 = m2 = x = t = xb = tb = dh = y = dy = nullptr;
+    W = Wt = dzt = ht = nullptr;
+    for (int l = 0; l < 4; ++l) {
+        z[l] = nullptr;
+        h[l] = nullptr;
+        dz[l] = nullptr;
+    }
+    dsum = nullptr;
+    derr = nullptr;
+    batch_cap = 0;
+    samples = 0;
+    sigma = 1.0;
+    trained = false;
+}
+
+cudaError_t Model::alloc_params() {
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess && !*p) e = cudaMalloc(p, bytes);
+    };
+    A((void**)&P, sg::kParams * 4);
+    A((void**)&W, 3ull * sg::kH * sg::kH * 2);
+    A((void**)&Wt, 3ull * sg::kH * sg::kH * 2);
+    A((void**)&derr, 32);
+    return e;
+}
+
+cudaError_t Model::alloc_batch(int B) {
+    if (B <= batch_cap) return cudaSuccess;
+    void* ptrs[] = {xb, tb, z[0], z[1], z[2], z[3], h[0], h[1], h[2], h[3], dz[0], dz[1], dz[2], dz[3], dzt, ht, dh, y, dy};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    xb = tb = nullptr;
+    for (int l = 0; l < 4; ++l) {
+        z[l] = nullptr;
+        h[l] = nullptr;
+        dz[l] = nullptr;
+    }
+    dzt = ht = nullptr;
+    dh = y = dy = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    const size_t BH = (size_t)B * sg::kH;
+    A((void**)&xb, (size_t)B * 4 * 4);
+    A((void**)&tb, (size_t)B * 3 * 4);
+    for (int l = 0; l < 4; ++l) {
+        A((void**)&z[l], BH * 4);
+        A((void**)&h[l], BH * 2);
+        A((void**)&dz[l], BH * 2);
+    }
+    A((void**)&dzt, BH * 2);
+    A((void**)&ht, BH * 2);
+    A((void**)&dh, BH * 4);
+    A((void**)&y, (size_t)B * 3 * 4);
+    A((void**)&dy, (size_t)B * 3 * 4);
+    if (e == cudaSuccess) batch_cap = B;
+    return e;
+}
+
+void init_params(std::vector<float>& p, uint64_t seed) {
+    std::mt19937_64 rng(seed);
+    p.assign(sg::kParams, 0.0f);
+    auto fill = [&](int off, int fan_in, int count, float gain) {
+        std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+        const float a = gain * std::sqrt(6.0f / (float)fan_in);
+        for (int i = 0; i < count; ++i) p[off + i] = a * U(rng);
+    };
+    // The target has no low-degree content, and a network fed plain
+    // coordinates learns low frequencies first: the first layer starts with
+    // weights U(-6, 6) and biases U(-3, 3), so its features already vary on
+    // the scale of the degree 9-20 terms (with the usual fan-in scale it
+    // stayed at the mean for hundreds of steps).
+    {
+        std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+        for (int i = 0; i < sg::kH * 4; ++i) p[sg::kOffW0 + i] = 6.0f * U(rng);
+        for (int i = 0; i < sg::kH; ++i) p[sg::kOffB0 + i] = 3.0f * U(rng);
+    }
+    for (int l = 0; l < 3; ++l) fill(sg::kOffW1 + l * sg::kH * sg::kH, sg::kH, sg::kH * sg::kH, 1.0f);
+    fill(sg::kOffW4, sg::kH, 3 * sg::kH, 0.1f);
+}
+
+// Forward pass of B rows (B % 128 == 0) from xb; y gets the outputs.  With
+// targets (tb) also the loss and the whole backward pass into G.
+cudaError_t forward_backward(Model& M, int B, bool train, cudaStream_t st) {
+    using namespace sg;
+    const int64_t BH = (int64_t)B * kH;
+    k_in_layer<<<blocks_for(BH), 256, 0, st>>>(B, M.xb, M.P, M.z[0], M.h[0]);
+    for (int l = 1; l < 4; ++l) {
+        cudaError_t e = launch_gemm_bf16(B, kH, kH, M.h[l - 1], M.W + (size_t)(l - 1) * kH * kH, M.z[l], M.derr, st);
+        if (e != cudaSuccess) return e;
+        k_bias_silu<<<blocks_for(BH), 256, 0, st>>>(B, M.z[l], M.P + kOffB1 + (l - 1) * kH, M.h[l]);
+    }
+    k_out_layer<<<blocks_for(B, 128), 128, 0, st>>>(B, M.h[3], M.P, train ? M.tb : nullptr, M.y, M.dy,
+                                                    train ? M.dsum : nullptr);
+    if (!train) return cudaGetLastError();
+    k_out_back<<<blocks_for(BH), 256, 0, st>>>(B, M.dy, M.P, M.z[3], M.dz[3]);
+    for (int l = 3; l >= 1; --l) {
+        // dW_l = dZ_l^T H_{l-1}:  A = dZ_l^T [H][B], B_op = H_{l-1}^T [H][B]
+        const dim3 tb(32, 8), tg((unsigned)(kH / 32), (unsigned)(B / 32));
+        k_transpose<<<tg, tb, 0, st>>>(B, kH, M.dz[l], M.dzt);
+        k_transpose<<<tg, tb, 0, st>>>(B, kH, M.h[l - 1], M.ht);
+        cudaError_t e = launch_gemm_bf16(kH, kH, B, M.dzt, M.ht, M.G + kOffW1 + (l - 1) * kH * kH, M.derr, st);
+        if (e != cudaSuccess) return e;
+        k_colsum<<<kH, 256, 0, st>>>(B, kH, M.dz[l], M.G + kOffB1 + (l - 1) * kH);
+        // dH_{l-1} = dZ_l W_l:  A = dZ_l [B][H(out)], B_op = W_l^T [H(in)][H(out)]
+        e = launch_gemm_bf16(B, kH, kH, M.dz[l], M.Wt + (size_t)(l - 1) * kH * kH, M.dh, M.derr, st);
+        if (e != cudaSuccess) return e;
+        k_silu_back<<<blocks_for(BH), 256, 0, st>>>(B, M.dh, M.z[l - 1], M.dz[l - 1]);
+    }
+    k_colsum<<<kH, 256, 0, st>>>(B, kH, M.dz[0], M.G + kOffB0);
+    k_small_grads<<<3 * kH + 3 + 4 * kH, 256, 0, st>>>(B, M.dy, M.h[3], M.dz[0], M.xb, M.G);
+    return cudaGetLastError();
+}
+
+cudaError_t refresh_bf16(Model& M, cudaStream_t st) {
+    sg::k_to_bf16<<<blocks_for(3ll * sg::kH * sg::kH), 256, 0, st>>>(M.P, M.W, M.Wt);
+    return cudaGetLastError();
+}
+
+cudaError_t upload_params(Model& M, const float* host, cudaStream_t st) {
+    cudaError_t e = M.alloc_params();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M.P, host, sg::kParams * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = refresh_bf16(M, st);
+    if (e == cudaSuccess) M.trained = true;
+    return e;
+}
+
+// The training loop.  a_full / a_low: callbacks that fill the exact fields
+// at n positions (device buffers).
+cudaError_t train(Model& M, const TrainArgs& a, const FieldFn& full, const FieldFn& low, cudaStream_t st,
+                  double* loss_per_epoch) {
+    using namespace sg;
+    cudaError_t e = M.alloc_params();
+    if (e != cudaSuccess) return e;
+    const int64_t n = a.samples;
+    const int B = a.batch;
+    // samples
+    double *pos = nullptr, *af = nullptr, *al = nullptr, *t64 = nullptr, *sumsq = nullptr;
+    auto A = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    A((void**)&pos, (size_t)n * 3 * 8);
+    A((void**)&af, (size_t)n * 3 * 8);
+    A((void**)&al, (size_t)n * 3 * 8);
+    A((void**)&t64, (size_t)n * 3 * 8);
+    A((void**)&sumsq, 8);
+    if (M.x && M.samples != n) {
+        cudaFree(M.x);
+        cudaFree(M.t);
+        M.x = nullptr;
+        M.t = nullptr;
+    }
+    if (!M.x) A((void**)&M.x, (size_t)n * 4 * 4);
+    if (!M.t) A((void**)&M.t, (size_t)n * 3 * 4);
+    if (e == cudaSuccess) e = M.alloc_batch(B);
+    if (e == cudaSuccess) {
+        k_sample<<<blocks_for(n), 256, 0, st>>>(n, a.seed, M.scale.r_mid - M.scale.r_half,
+                                                M.scale.r_mid + M.scale.r_half, pos);
+        e = full(n, pos, af);
+    }
+    if (e == cudaSuccess) e = low(n, pos, al);
+    if (e == cudaSuccess) {
+        k_features<<<blocks_for(n), 256, 0, st>>>(n, pos, af, al, M.x, t64, M.scale);
+        e = cudaMemsetAsync(sumsq, 0, 8, st);
+    }
+    if (e == cudaSuccess) {
+        k_sumsq<<<1024, 256, 0, st>>>(3 * n, t64, sumsq);
+        k_scale_targets<<<blocks_for(3 * n), 256, 0, st>>>(3 * n, t64, sumsq, M.t, reinterpret_cast<double*>(
+                                                                                     reinterpret_cast<char*>(M.derr) + 8));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&M.sigma, reinterpret_cast<char*>(M.derr) + 8, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(pos);
+    cudaFree(af);
+    cudaFree(al);
+    cudaFree(t64);
+    cudaFree(sumsq);
+    M.samples = n;
+    if (e != cudaSuccess) return e;
+
+    // parameters and optimizer state
+    std::vector<float> p0;
+    init_params(p0, a.seed ^ 0x5EEDull);
+    A((void**)&M.G, sg::kParams * 4);
+    A((void**)&M.m1, sg::kParams * 4);
+    A((void**)&M.m2, sg::kParams * 4);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M.P, p0.data(), sg::kParams * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M.m1, 0, sg::kParams * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M.m2, 0, sg::kParams * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M.derr, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    M.dsum = reinterpret_cast<double*>(reinterpret_cast<char*>(M.derr) + 16);
+
+    const int64_t steps_per_epoch = (n + B - 1) / B;
+    const int64_t total = steps_per_epoch * a.epochs;
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (int ep = 0; ep < a.epochs && e == cudaSuccess; ++ep) {
+        e = cudaMemsetAsync(M.dsum, 0, 8, st);
+        for (int64_t s = 0; s < steps_per_epoch && e == cudaSuccess; ++s) {
+            const int64_t step = ep * steps_per_epoch + s;
+            e = refresh_bf16(M, st);
+            if (e != cudaSuccess) break;
+            k_gather<<<blocks_for(B), 256, 0, st>>>(B, n, a.seed, (uint64_t)step, M.x, M.t, M.xb, M.tb);
+            e = forward_backward(M, B, true, st);
+            if (e != cudaSuccess) break;
+            // cosine decay from lr to lr / 100
+            const double frac = (double)step / (double)(total > 1 ? total - 1 : 1);
+            const float lr = (float)(a.lr * (0.01 + 0.99 * 0.5 * (1.0 + std::cos(3.14159265358979 * frac))));
+            const float c1 = 1.0f - std::pow(b1, (float)(step + 1)), c2 = 1.0f - std::pow(b2, (float)(step + 1));
+            sg::k_adam<<<blocks_for(sg::kParams), 256, 0, st>>>(sg::kParams, M.P, M.G, M.m1, M.m2, lr, b1, b2, c1,
+                                                                 c2, 1e-8f);
+            e = cudaGetLastError();
+        }
+        double lsum = 0.0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&lsum, M.dsum, 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (loss_per_epoch) loss_per_epoch[ep] = lsum / (3.0 * (double)B * (double)steps_per_epoch);
+    }
+    if (e == cudaSuccess) e = refresh_bf16(M, st);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, M.derr, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && herr) e = cudaErrorLaunchTimeout;
+    if (e == cudaSuccess) M.trained = true;
+    return e;
+}
+
+// residual (add = 0) or field + residual (add = 1) at n positions, device
+// buffers; rows are processed in chunks of the batch capacity
+cudaError_t infer(Model& M, int64_t n, const double* pos, double* acc, int add, cudaStream_t st) {
+    using namespace sg;
+    const int B = 16384;
+    cudaError_t e = M.alloc_batch(B);
+    for (int64_t off = 0; off < n && e == cudaSuccess; off += B) {
+        const int64_t m = n - off < B ? n - off : B;
+        const int mp = (int)((m + 127) / 128 * 128);
+        if (mp > m) e = cudaMemsetAsync(M.xb, 0, (size_t)mp * 16, st);
+        if (e != cudaSuccess) break;
+        k_features<<<blocks_for(m), 256, 0, st>>>(m, pos + 3 * off, nullptr, nullptr, M.xb, nullptr, M.scale);
+        e = forward_backward(M, mp, false, st);
+        if (e != cudaSuccess) break;
+        k_residual<<<blocks_for(m), 256, 0, st>>>(m, pos + 3 * off, M.y, M.scale, M.sigma, acc + 3 * off, add);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+}  // namespace bqp

@@ -277,6 +277,33 @@ int bqp_sigma_weights(int32_t sigma_set, double alpha, double beta, double kappa
 int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void* a, const void* b, float* c,
                          void* stream);
 
+/* Learned gravity surrogate.  An MLP (input: body-fixed unit vector and
+ * scaled radius; 4 hidden layers of 256, SiLU; output: the acceleration of the
+ * degrees above BQP_SURROGATE_DEGREE times (r/R)^2, normalised) trained on the
+ * GPU with BF16 tensor-core forward and backward GEMMs (FP32 accumulation) and
+ * Adam on FP32 masters.  No counterpart in the reference (its learned parts
+ * are elsewhere); the samples come from the context's own exact field.
+ *
+ * train: `samples` positions uniform in radius 6578-7578 km and on the sphere,
+ * targets from the exact harmonic kernel (context order) minus degrees <= 8;
+ * `epochs` passes of minibatches of `batch` (multiple of 128); Adam, cosine
+ * decay from lr; loss_per_epoch[epochs] (nullable): mean squared error of the
+ * normalised targets.
+ * infer: pos[n][3] Earth-fixed km -> acc[n][3] km/s^2: the predicted residual
+ * (add_low = 0) or the exact degree <= 8 field (C00 included) plus it.
+ * params / set_params: the BQP_SURROGATE_PARAMS FP32 parameters and the
+ * output scale sigma.  grad: loss and gradient of given parameters on one
+ * batch (x[batch][4], normalised targets t[batch][3]), for checking. */
+#define BQP_SURROGATE_DEGREE 8
+#define BQP_SURROGATE_PARAMS 199427
+int bqp_surrogate_train(bqp_ctx* ctx, int64_t samples, int32_t epochs, int32_t batch, double lr,
+                        uint64_t seed, double* loss_per_epoch);
+int bqp_surrogate_infer(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc, int32_t add_low);
+int bqp_surrogate_params(bqp_ctx* ctx, float* params, double* sigma);
+int bqp_surrogate_set_params(bqp_ctx* ctx, const float* params, double sigma);
+int bqp_surrogate_grad(bqp_ctx* ctx, int32_t batch, const float* params, const float* x, const float* t,
+                       float* grad, double* loss, float* y);
+
 /* Element conversions on the host (no GPU).  eci_to_equinoctial replaces
  * eci2equinoc_impl (satpy_core/src/lib.rs:1738-1870; ok[i] = 0 on an
  * unbound or degenerate orbit); equinoctial_to_eci replaces equinoc2eci_impl

@@ -33,3 +33,72 @@ def test_tensor_core_gemm_matches_fp32_reference(m, n, k):
     assert err <= 1e-5 * np.sqrt(k) * ref.abs().max().item() + 1e-5, err
     # and not a trivially wrong layout: every element checked, signs too
     assert torch.allclose(got, ref, rtol=1e-4, atol=1e-3)
+
+
+def _surrogate_ctx(order=20):
+    from bqp_b200 import workloads
+    cfg = N.default_config()
+    cfg.order = order
+    return N.Context(workloads.synthetic_field(order), cfg)
+
+
+def test_surrogate_gradients_match_cpu_restatement():
+    """Forward pass and every parameter's gradient of one batch against the
+    numpy restatement with the same BF16 roundings (oracle/mlp.py)."""
+    from oracle import mlp
+    rng = np.random.default_rng(7)
+    B = 256
+    p = np.zeros(mlp.PARAMS, dtype=np.float32)
+    p[mlp.OFF_W0:mlp.OFF_B0] = rng.uniform(-1.2, 1.2, 4 * mlp.H)
+    p[mlp.OFF_B0:mlp.OFF_W1] = rng.uniform(-0.1, 0.1, mlp.H)
+    p[mlp.OFF_W1:mlp.OFF_B1] = rng.uniform(-0.15, 0.15, 3 * mlp.H * mlp.H)
+    p[mlp.OFF_B1:mlp.OFF_W4] = rng.uniform(-0.1, 0.1, 3 * mlp.H)
+    p[mlp.OFF_W4:mlp.OFF_B4] = rng.uniform(-0.15, 0.15, 3 * mlp.H)
+    x = np.concatenate([rng.normal(size=(B, 3)), rng.uniform(-1, 1, (B, 1))], axis=1).astype(np.float32)
+    x[:, :3] /= np.linalg.norm(x[:, :3], axis=1, keepdims=True)
+    t = rng.normal(size=(B, 3)).astype(np.float32)
+    ctx = _surrogate_ctx()
+    loss, g, y = ctx.surrogate_grad(p, x, t)
+    oloss, og, oy = mlp.forward_backward(p, x, t)
+    # the device's SiLU uses the fast exponential: a hidden activation next to
+    # a BF16 rounding boundary can round one ulp (2^-8) the other way
+    assert np.linalg.norm(y - oy) <= 2e-3 * np.linalg.norm(oy)
+    assert np.abs(y - oy).max() <= 1e-2 * np.abs(oy).max()
+    assert abs(loss - oloss) <= 2e-3 * oloss
+    # per parameter block: relative L2 error of the gradient
+    blocks = [(mlp.OFF_W0, mlp.OFF_B0), (mlp.OFF_B0, mlp.OFF_W1)] + \
+             [(mlp.OFF_W1 + l * mlp.H * mlp.H, mlp.OFF_W1 + (l + 1) * mlp.H * mlp.H) for l in range(3)] + \
+             [(mlp.OFF_B1, mlp.OFF_W4), (mlp.OFF_W4, mlp.OFF_B4), (mlp.OFF_B4, mlp.PARAMS)]
+    for a, b in blocks:
+        rel = np.linalg.norm(g[a:b] - og[a:b]) / np.linalg.norm(og[a:b])
+        assert rel <= 2e-2, (a, b, rel)
+
+
+def test_surrogate_learns_the_high_degree_field():
+    """Training on the GPU reduces the error of the low-degree field (the
+    method without the network) by a large factor on held-out positions."""
+    order = 20
+    ctx = _surrogate_ctx(order)
+    loss = ctx.surrogate_train(samples=1 << 19, epochs=8, batch=4096, lr=2e-3, seed=3)
+    assert loss[-1] < 0.25 * loss[0], loss
+    rng = np.random.default_rng(11)
+    n = 20000
+    r = rng.uniform(6600.0, 7550.0, n)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    pos = u * r[:, None]
+    full = ctx.gravity(pos)[0]
+    cfg8 = N.default_config()
+    cfg8.order = N.SURROGATE_DEGREE
+    from bqp_b200 import workloads
+    low = N.Context(workloads.synthetic_field(order), cfg8).gravity(pos)[0]
+    surr = ctx.surrogate_infer(pos, add_low=True)
+    res = np.linalg.norm(full - low, axis=1)
+    err_without = np.sqrt(np.mean(res ** 2))
+    err_with = np.sqrt(np.mean(np.linalg.norm(full - surr, axis=1) ** 2))
+    assert err_with < 0.5 * err_without, (err_with, err_without)
+    # parameters round-trip through the host
+    p, sigma = ctx.surrogate_params()
+    ctx2 = _surrogate_ctx(order)
+    ctx2.surrogate_set_params(p, sigma)
+    assert np.allclose(ctx2.surrogate_infer(pos[:1000]), surr[:1000], rtol=0, atol=1e-15)
