@@ -99,6 +99,7 @@ SIGNATURES = [
     ("bqp_gemm_bf16_device", C.c_int, [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp]),
     ("bqp_surrogate_train", C.c_int, [_vp, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64, _dp]),
     ("bqp_surrogate_infer", C.c_int, [_vp, C.c_int64, _dp, _dp, C.c_int32]),
+    ("bqp_surrogate_infer_device", C.c_int, [_vp, C.c_int64, _vp, _vp, C.c_int32]),
     ("bqp_surrogate_params", C.c_int, [_vp, _fp, _dp]),
     ("bqp_surrogate_set_params", C.c_int, [_vp, _fp, C.c_double]),
     ("bqp_surrogate_grad", C.c_int, [_vp, C.c_int32, _fp, _fp, _fp, _fp, _dp, _fp]),
@@ -320,6 +321,9 @@ class Context:
         acc = np.empty_like(p)
         check(lib().bqp_surrogate_infer(self._h, p.shape[0], dptr(p), dptr(acc), int(add_low)))
         return acc
+
+    def surrogate_infer_device(self, n, d_pos, d_acc, add_low=True):
+        check(lib().bqp_surrogate_infer_device(self._h, int(n), _vp(d_pos), _vp(d_acc), int(add_low)))
 
     def surrogate_params(self):
         params = np.zeros(SURROGATE_PARAMS, dtype=np.float32)

@@ -1714,6 +1714,17 @@ int bqp_surrogate_infer(bqp_ctx* ctx, int64_t n, const double* pos_km, double* a
     return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_infer");
 }
 
+int bqp_surrogate_infer_device(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc, int32_t add_low) {
+    int rc = surrogate_ready(ctx, true);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!pos_km || !acc))) return fail(BQP_E_ARG, "bad buffers");
+    if (n == 0) return 0;
+    cudaError_t e = cudaSuccess;
+    if (add_low) e = launch_gravity(low_table(ctx), n, pos_km, acc, nullptr, ctx->stream, 256, 4);
+    if (e == cudaSuccess) e = infer(*ctx->sur, n, pos_km, acc, add_low ? 1 : 0, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_infer_device");
+}
+
 int bqp_surrogate_params(bqp_ctx* ctx, float* params, double* sigma) {
     int rc = surrogate_ready(ctx, true);
     if (rc) return rc;

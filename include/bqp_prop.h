@@ -299,6 +299,8 @@ int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void* a, const v
 int bqp_surrogate_train(bqp_ctx* ctx, int64_t samples, int32_t epochs, int32_t batch, double lr,
                         uint64_t seed, double* loss_per_epoch);
 int bqp_surrogate_infer(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc, int32_t add_low);
+int bqp_surrogate_infer_device(bqp_ctx* ctx, int64_t n, const double* d_pos_km, double* d_acc,
+                               int32_t add_low);
 int bqp_surrogate_params(bqp_ctx* ctx, float* params, double* sigma);
 int bqp_surrogate_set_params(bqp_ctx* ctx, const float* params, double sigma);
 int bqp_surrogate_grad(bqp_ctx* ctx, int32_t batch, const float* params, const float* x, const float* t,
