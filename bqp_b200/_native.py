@@ -316,10 +316,11 @@ class Context:
                                         dptr(loss)))
         return loss
 
-    def surrogate_infer(self, pos_km, add_low=True):
+    def surrogate_infer(self, pos_km, add_low=True, fused=True):
         p = f64(pos_km).reshape(-1, 3)
         acc = np.empty_like(p)
-        check(lib().bqp_surrogate_infer(self._h, p.shape[0], dptr(p), dptr(acc), int(add_low)))
+        flags = (1 if add_low else 0) | (0 if fused else 2)
+        check(lib().bqp_surrogate_infer(self._h, p.shape[0], dptr(p), dptr(acc), flags))
         return acc
 
     def surrogate_infer_device(self, n, d_pos, d_acc, add_low=True):

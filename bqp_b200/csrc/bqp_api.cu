@@ -1670,6 +1670,8 @@ int surrogate_ready(bqp_ctx* ctx, bool need_trained) {
 
 extern "C" {
 
+int bqp_surrogate_infer_device(bqp_ctx* ctx, int64_t n, const double* pos_km, double* acc, int32_t add_low);
+
 int bqp_surrogate_train(bqp_ctx* ctx, int64_t samples, int32_t epochs, int32_t batch, double lr, uint64_t seed,
                         double* loss_per_epoch) {
     int rc = surrogate_ready(ctx, false);
@@ -1707,9 +1709,9 @@ int bqp_surrogate_infer(bqp_ctx* ctx, int64_t n, const double* pos_km, double* a
     }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(dp, pos_km, (size_t)n * 24, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && add_low) e = launch_gravity(low_table(ctx), n, dp, da, nullptr, s, 256, 4);
-    if (e == cudaSuccess) e = infer(*ctx->sur, n, dp, da, add_low ? 1 : 0, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(acc, da, (size_t)n * 24, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bqp_surrogate_infer H2D");
+    if ((rc = bqp_surrogate_infer_device(ctx, n, dp, da, add_low))) return rc;
+    e = cudaMemcpyAsync(acc, da, (size_t)n * 24, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_infer");
 }
@@ -1719,9 +1721,20 @@ int bqp_surrogate_infer_device(bqp_ctx* ctx, int64_t n, const double* pos_km, do
     if (rc) return rc;
     if (n < 0 || (n > 0 && (!pos_km || !acc))) return fail(BQP_E_ARG, "bad buffers");
     if (n == 0) return 0;
+    cudaStream_t s = ctx->stream;
     cudaError_t e = cudaSuccess;
-    if (add_low) e = launch_gravity(low_table(ctx), n, pos_km, acc, nullptr, ctx->stream, 256, 4);
-    if (e == cudaSuccess) e = infer(*ctx->sur, n, pos_km, acc, add_low ? 1 : 0, ctx->stream);
+    const bool low = (add_low & 1) != 0, unfused = (add_low & 2) != 0;
+    if (low) e = launch_gravity(low_table(ctx), n, pos_km, acc, nullptr, s, 256, 4);
+    else e = cudaMemsetAsync(acc, 0, (size_t)n * 24, s);
+    if (e == cudaSuccess) {
+        if (unfused) {
+            e = infer(*ctx->sur, n, pos_km, acc, 1, s);
+        } else {
+            Model& M = *ctx->sur;
+            e = cudaMemsetAsync(M.derr, 0, sizeof(int), s);
+            if (e == cudaSuccess) e = infer_fused(M, n, pos_km, acc, M.derr, s);
+        }
+    }
     return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_surrogate_infer_device");
 }
 

@@ -23,6 +23,7 @@
 
 #include "launch.h"
 #include "surrogate.h"
+#include "tc_gemm.cuh"
 
 namespace bqp {
 namespace sg {
@@ -261,14 +262,216 @@ __global__ void k_adam(int64_t n, float* __restrict__ P, const float* __restrict
     P[i] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
 }
 
-__global__ void k_to_bf16(const float* __restrict__ P, __nv_bfloat16* __restrict__ W, __nv_bfloat16* __restrict__ Wt) {
-    // the three hidden matrices: W[l][o][i] and W^T[l][i][o]
+// element (r, k) of a rows x 256 K-major tile in the tensor cores' layout:
+// 8-row x 8-element core matrices, those of one 8-row group consecutive in k
+__device__ __forceinline__ int tile256(int r, int k) { return ((r >> 3) * (kH / 8) + (k >> 3)) * 64 + (r & 7) * 8 + (k & 7); }
+
+__global__ void k_to_bf16(const float* __restrict__ P, __nv_bfloat16* __restrict__ W, __nv_bfloat16* __restrict__ Wt,
+                          __nv_bfloat16* __restrict__ Wtile) {
+    // the three hidden matrices: W[l][o][i], W^T[l][i][o] and the tiled W
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= 3ll * kH * kH) return;
     const int l = (int)(e / (kH * kH)), o = (int)((e / kH) % kH), i = (int)(e % kH);
-    const float w = P[kOffW1 + e];
-    W[e] = __float2bfloat16(w);
-    Wt[(size_t)l * kH * kH + (size_t)i * kH + o] = __float2bfloat16(w);
+    const __nv_bfloat16 w = __float2bfloat16(P[kOffW1 + e]);
+    W[e] = w;
+    Wt[(size_t)l * kH * kH + (size_t)i * kH + o] = w;
+    if (Wtile) Wtile[(size_t)l * kH * kH + tile256(o, i)] = w;
+}
+
+// ------------------------------------------------------- fused inference
+// One persistent CTA per SM, 256 threads, 128-point tiles.  Shared memory:
+// the current layer's weights (128 KB, one bulk copy), the activation tile
+// (64 KB, BF16), the small layers' parameters.  Warp w reads TMEM lanes
+// 32 (w % 4) .. +31 (the tile's rows) and columns 128 (w / 4) .. +127.
+constexpr int kFusedThreads = 256;
+constexpr size_t kFusedW = (size_t)kH * kH * 2, kFusedA = (size_t)128 * kH * 2;
+// W0, b0, b1..b3, W4, b4 (FP32), rounded up so the mbarriers after them are aligned
+constexpr size_t kFusedSmall = ((size_t)(kH * 4 + kH + 3 * kH + 3 * kH + 3) * 4 + 15) / 16 * 16;
+constexpr size_t kFusedSmem = kFusedW + kFusedA + kFusedSmall + 64;
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    k_mlp_infer(int64_t n, const double* __restrict__ pos, const float* __restrict__ P,
+                const __nv_bfloat16* __restrict__ Wtile, Scale sc, double sigma, double* __restrict__ acc, int* err) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm);
+    __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(sm + kFusedW);
+    float* sW0 = reinterpret_cast<float*>(sm + kFusedW + kFusedA);
+    float* sB0 = sW0 + kH * 4;
+    float* sB = sB0 + kH;           // b1..b3
+    float* sW4 = sB + 3 * kH;       // W4[3][256]
+    float* sB4 = sW4 + 3 * kH;      // b4[3]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kFusedW + kFusedA + kFusedSmall);  // [0] MMA, [1] weights
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    float* sy = reinterpret_cast<float*>(sA);  // output partials of the second column half (after the last layer)
+    const uint32_t bar_mma = (uint32_t)__cvta_generic_to_shared(&bars[0]);
+    const uint32_t bar_w = (uint32_t)__cvta_generic_to_shared(&bars[1]);
+    const int warp = threadIdx.x >> 5, quad = warp & 3, half = warp >> 2;
+    const int row = quad * 32 + (threadIdx.x & 31);  // the tile row this thread reads back
+    const int64_t ntiles = (n + 127) / 128;
+    if ((int64_t)blockIdx.x >= ntiles) return;  // uniform per CTA
+
+    for (int i = threadIdx.x; i < kH * 4; i += kFusedThreads) sW0[i] = P[kOffW0 + i];
+    for (int i = threadIdx.x; i < kH; i += kFusedThreads) sB0[i] = P[kOffB0 + i];
+    for (int i = threadIdx.x; i < 3 * kH; i += kFusedThreads) {
+        sB[i] = P[kOffB1 + i];
+        sW4[i] = P[kOffW4 + i];
+    }
+    if (threadIdx.x < 3) sB4[threadIdx.x] = P[kOffB4 + threadIdx.x];
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(tmem_slot)),
+                     "r"(256u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_mma) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_w) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t sW_a = (uint32_t)__cvta_generic_to_shared(sW), sA_a = (uint32_t)__cvta_generic_to_shared(sA);
+
+    // weights of hidden layer l (0..2) into sW, completion on bar_w
+    auto load_w = [&](int l) {
+        uint64_t state;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                     : "=l"(state)
+                     : "r"(bar_w), "r"((uint32_t)kFusedW)
+                     : "memory");
+        (void)state;
+        const char* src = reinterpret_cast<const char*>(Wtile + (size_t)l * kH * kH);
+        for (uint32_t off = 0; off < kFusedW; off += 32768)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    sW_a + off),
+                "l"(src + off), "r"(32768u), "r"(bar_w)
+                : "memory");
+    };
+    uint32_t ph_mma = 0, ph_w = 0;
+    bool ok = true;
+    if (threadIdx.x == 0) load_w(0);
+
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t base = tile * 128;
+        // input layer: thread (row, half) computes columns half*128 .. +127
+        {
+            const int r = threadIdx.x & 127, h0 = (threadIdx.x >> 7) * 128;
+            const int64_t i = base + r;
+            float x[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+            if (i < n) {
+                const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+                const double rr = sqrt(px * px + py * py + pz * pz);
+                x[0] = (float)(px / rr);
+                x[1] = (float)(py / rr);
+                x[2] = (float)(pz / rr);
+                x[3] = (float)((rr - sc.r_mid) / sc.r_half);
+            }
+            for (int j0 = h0; j0 < h0 + 128; j0 += 8) {
+                __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int j = j0 + q;
+                    float s = sB0[j];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) s = fmaf(sW0[j * 4 + k], x[k], s);
+                    v[q] = __float2bfloat16(silu(s));
+                }
+                *reinterpret_cast<uint4*>(sA + tile256(r, j0)) = *reinterpret_cast<const uint4*>(v);
+            }
+        }
+        float y[3] = {0.0f, 0.0f, 0.0f};
+        for (int l = 0; l < 3 && ok; ++l) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            ok = tc::mbar_wait(bar_w, ph_w);  // this layer's weights
+            ph_w ^= 1u;
+            if (!__syncthreads_and(ok)) {
+                ok = false;
+                break;
+            }
+            if (threadIdx.x == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                for (int kk = 0; kk < kH; kk += 16) {
+                    const uint64_t da = tc::smem_desc(sA_a + (kk / 8) * 128, 128, (kH / 8) * 128);
+                    const uint64_t db = tc::smem_desc(sW_a + (kk / 8) * 128, 128, (kH / 8) * 128);
+                    const uint32_t accum = kk > 0 ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(tc::kIdesc), "r"(accum)
+                        : "memory");
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 bar_mma)
+                             : "memory");
+            }
+            ok = tc::mbar_wait(bar_mma, ph_mma);
+            ph_mma ^= 1u;
+            if (!__syncthreads_and(ok)) {
+                ok = false;
+                break;
+            }
+            // the weights are free: start the next layer's (or the next tile's first)
+            const bool more = l < 2 || tile + (int64_t)gridDim.x < ntiles;
+            if (threadIdx.x == 0 && more) load_w(l < 2 ? l + 1 : 0);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
+            for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
+                uint32_t rv[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(rv[0]), "=r"(rv[1]), "=r"(rv[2]), "=r"(rv[3]), "=r"(rv[4]), "=r"(rv[5]), "=r"(rv[6]),
+                      "=r"(rv[7]), "=r"(rv[8]), "=r"(rv[9]), "=r"(rv[10]), "=r"(rv[11]), "=r"(rv[12]), "=r"(rv[13]),
+                      "=r"(rv[14]), "=r"(rv[15])
+                    : "r"(lane_addr + (uint32_t)c0));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                __align__(16) __nv_bfloat16 hv[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const float hq = __bfloat162float(__float2bfloat16(silu(__uint_as_float(rv[q]) + sB[l * kH + c0 + q])));
+                    hv[q] = __float2bfloat16(hq);
+                    if (l == 2) {
+                        y[0] = fmaf(sW4[c0 + q], hq, y[0]);
+                        y[1] = fmaf(sW4[kH + c0 + q], hq, y[1]);
+                        y[2] = fmaf(sW4[2 * kH + c0 + q], hq, y[2]);
+                    }
+                }
+                if (l < 2) {
+                    *reinterpret_cast<uint4*>(sA + tile256(row, c0)) = *reinterpret_cast<const uint4*>(hv);
+                    *reinterpret_cast<uint4*>(sA + tile256(row, c0 + 8)) = *reinterpret_cast<const uint4*>(hv + 8);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        }
+        if (!ok) break;
+        // the two column halves meet in shared memory (the activation tile
+        // is free after the last layer)
+        __syncthreads();
+        if (half == 1)
+            for (int k = 0; k < 3; ++k) sy[row * 3 + k] = y[k];
+        __syncthreads();
+        if (half == 0) {
+            const int64_t i = base + row;
+            if (i < n) {
+                const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+                const double f = sigma * (sc.R * sc.R) / (px * px + py * py + pz * pz);
+                for (int k = 0; k < 3; ++k)
+                    acc[3 * i + k] += f * (double)(y[k] + sy[row * 3 + k] + sB4[k]);
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
 }
 
 // residual acceleration from the network output: sigma * y * (R/r)^2
@@ -295,12 +498,12 @@ Model::~Model() { release(); }
 
 void Model::release() {
     // dsum points into derr and is not freed on its own
-    void* ptrs[] = {P, G, m1, m2, W, Wt, x, t, xb, tb, z[0], z[1], z[2], z[3], h[0], h[1], h[2], h[3], dz[0], dz[1],
+    void* ptrs[] = {P, G, m1, m2, W, Wt, Wtile, x, t, xb, tb, z[0], z[1], z[2], z[3], h[0], h[1], h[2], h[3], dz[0], dz[1],
                     dz[2], dz[3], dzt, ht, dh, y, dy, derr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     P = G = m1 = m2 = x = t = xb = tb = dh = y = dy = nullptr;
-    W = Wt = dzt = ht = nullptr;
+    W = Wt = Wtile = dzt = ht = nullptr;
     for (int l = 0; l < 4; ++l) {
         z[l] = nullptr;
         h[l] = nullptr;
@@ -322,6 +525,7 @@ cudaError_t Model::alloc_params() {
     A((void**)&P, sg::kParams * 4);
     A((void**)&W, 3ull * sg::kH * sg::kH * 2);
     A((void**)&Wt, 3ull * sg::kH * sg::kH * 2);
+    A((void**)&Wtile, 3ull * sg::kH * sg::kH * 2);
     A((void**)&derr, 32);
     return e;
 }
@@ -416,7 +620,7 @@ cudaError_t forward_backward(Model& M, int B, bool train, cudaStream_t st) {
 }
 
 cudaError_t refresh_bf16(Model& M, cudaStream_t st) {
-    sg::k_to_bf16<<<blocks_for(3ll * sg::kH * sg::kH), 256, 0, st>>>(M.P, M.W, M.Wt);
+    sg::k_to_bf16<<<blocks_for(3ll * sg::kH * sg::kH), 256, 0, st>>>(M.P, M.W, M.Wt, M.Wtile);
     return cudaGetLastError();
 }
 
@@ -547,6 +751,18 @@ cudaError_t infer(Model& M, int64_t n, const double* pos, double* acc, int add, 
         e = cudaGetLastError();
     }
     return e;
+}
+
+cudaError_t infer_fused(Model& M, int64_t n, const double* pos, double* acc, int* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(sg::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sg::kFusedSmem);
+    if (e != cudaSuccess) return e;
+    const int64_t tiles = (n + 127) / 128;
+    const int grid = (int)(tiles < device_sm_count() ? tiles : device_sm_count());
+    sg::k_mlp_infer<<<grid, sg::kFusedThreads, sg::kFusedSmem, st>>>(n, pos, M.P, M.Wtile, M.scale, M.sigma, acc,
+                                                                      err);
+    return cudaGetLastError();
 }
 
 }  // namespace bqp

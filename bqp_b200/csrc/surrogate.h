@@ -46,6 +46,7 @@ struct Model {
     bool trained = false;
     float *P = nullptr, *G = nullptr, *m1 = nullptr, *m2 = nullptr;
     __nv_bfloat16 *W = nullptr, *Wt = nullptr;
+    __nv_bfloat16* Wtile = nullptr;  // the hidden matrices in the tensor cores' shared-memory layout
     float *x = nullptr, *t = nullptr;  // training set
     float *xb = nullptr, *tb = nullptr;
     float* z[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -65,6 +66,9 @@ struct Model {
 cudaError_t train(Model& M, const TrainArgs& a, const FieldFn& full, const FieldFn& low, cudaStream_t st,
                   double* loss_per_epoch);
 cudaError_t infer(Model& M, int64_t n, const double* pos, double* acc, int add, cudaStream_t st);
+// the same through one fused kernel (weights staged per layer, activations
+// kept on chip); adds the residual to acc
+cudaError_t infer_fused(Model& M, int64_t n, const double* pos, double* acc, int* err, cudaStream_t st);
 cudaError_t forward_backward(Model& M, int B, bool train, cudaStream_t st);
 cudaError_t refresh_bf16(Model& M, cudaStream_t st);
 cudaError_t upload_params(Model& M, const float* host, cudaStream_t st);

@@ -290,7 +290,10 @@ int bqp_gemm_bf16_device(int64_t m, int64_t n, int64_t k, const void* a, const v
  * decay from lr; loss_per_epoch[epochs] (nullable): mean squared error of the
  * normalised targets.
  * infer: pos[n][3] Earth-fixed km -> acc[n][3] km/s^2: the predicted residual
- * (add_low = 0) or the exact degree <= 8 field (C00 included) plus it.
+ * (add_low bit 0 clear) or the exact degree <= 8 field (C00 included) plus it
+ * (bit 0 set).  The network runs as one fused kernel (weights staged per layer
+ * by bulk copy, activations in shared and tensor memory); bit 1 selects the
+ * layer-by-layer kernels used in training instead, for checking.
  * params / set_params: the BQP_SURROGATE_PARAMS FP32 parameters and the
  * output scale sigma.  grad: loss and gradient of given parameters on one
  * batch (x[batch][4], normalised targets t[batch][3]), for checking. */

@@ -97,6 +97,10 @@ def test_surrogate_learns_the_high_degree_field():
     err_without = np.sqrt(np.mean(res ** 2))
     err_with = np.sqrt(np.mean(np.linalg.norm(full - surr, axis=1) ** 2))
     assert err_with < 0.5 * err_without, (err_with, err_without)
+    # the fused inference kernel and the layer-by-layer kernels agree (the
+    # same BF16 roundings; FP32 sums in another order)
+    unfused = ctx.surrogate_infer(pos, add_low=True, fused=False)
+    assert np.sqrt(np.mean(np.sum((unfused - surr) ** 2, axis=1))) <= 1e-3 * err_without
     # parameters round-trip through the host
     p, sigma = ctx.surrogate_params()
     ctx2 = _surrogate_ctx(order)
