@@ -550,6 +550,11 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_UNSUPPORTED, "split precision runs in the stage-synchronous engine");
     if (c->drag_fp32 != 0 && c->drag_fp32 != 1) return fail(BQP_E_ARG, "drag_fp32 must be 0 or 1");
     if (c->drag_fp32) return fail(BQP_E_UNSUPPORTED, "the FP32 JB2008 density is not built");
+    if (c->surrogate != 0 && c->surrogate != 1) return fail(BQP_E_ARG, "surrogate must be 0 or 1");
+    if (c->surrogate && c->engine == BQP_ENGINE_PERSISTENT)
+        return fail(BQP_E_UNSUPPORTED, "the surrogate gravity runs in the stage-synchronous engine");
+    if (c->surrogate && c->split_degree)
+        return fail(BQP_E_ARG, "choose the surrogate or split precision, not both");
     if (c->drag_fp32 && c->engine == BQP_ENGINE_PERSISTENT)
         return fail(BQP_E_UNSUPPORTED, "the FP32 density runs in the stage-synchronous engine");
     return 0;
@@ -659,6 +664,8 @@ int upload_table(bqp_ctx* ctx) {
     return 0;
 }
 
+int surrogate_stage_args(bqp_ctx* ctx, SurrogateRef& S);  // below, with the surrogate entry points
+
 // The table the gravity kernels read: split precision when configured.
 GravTable grav_table(const bqp_ctx* ctx) {
     GravTable T{};
@@ -739,6 +746,9 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.force = force_params(ctx);
     A.ctrl = ctrl_params(ctx);
     A.grav = grav_table(ctx);
+    if (ctx->cfg.surrogate) {
+        if (int rc = surrogate_stage_args(ctx, A.sur)) return rc;
+    }
     if (ctx->cfg.engine == BQP_ENGINE_PIPELINE) {
         const size_t need = pipeline_bytes(n);
         if (need > ctx->pws_bytes) {
@@ -969,6 +979,7 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->gravity_slots = 4;
     c->split_degree = 0;
     c->drag_fp32 = 0;
+    c->surrogate = 0;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -1654,6 +1665,27 @@ GravTable low_table(const bqp_ctx* ctx) {
     T.bytes = ctx->low_bytes;
     T.in_smem = 1;
     return T;
+}
+
+int surrogate_ready(bqp_ctx* ctx, bool need_trained);
+
+// The propagation's view of the trained surrogate (pipeline gravity stage).
+int surrogate_stage_args(bqp_ctx* ctx, SurrogateRef& S) {
+    int rc = surrogate_ready(ctx, true);
+    if (rc) return rc;
+    if (ctx->cfg.order <= BQP_SURROGATE_DEGREE)
+        return fail(BQP_E_ARG, "the surrogate replaces degrees above %d; the order is %d", BQP_SURROGATE_DEGREE,
+                    ctx->cfg.order);
+    Model& M = *ctx->sur;
+    S.P = M.P;
+    S.Wtile = M.Wtile;
+    S.R = M.scale.R;
+    S.r_mid = M.scale.r_mid;
+    S.r_half = M.scale.r_half;
+    S.sigma = M.sigma;
+    S.err = M.derr;
+    S.low = low_table(ctx);
+    return 0;
 }
 
 int surrogate_ready(bqp_ctx* ctx, bool need_trained) {

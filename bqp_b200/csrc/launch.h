@@ -1,5 +1,6 @@
 // Launch interface between the C ABI (bqp_api.cu) and the kernels (propagate.cu).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -8,6 +9,15 @@
 #include "kernels.cuh"
 
 namespace bqp {
+
+// A trained gravity surrogate, as the propagation's gravity stage uses it.
+struct SurrogateRef {
+    const float* P;                    // FP32 parameters (null: no surrogate)
+    const __nv_bfloat16* Wtile;        // hidden matrices in the tensor cores' layout
+    double R, r_mid, r_half, sigma;    // output and input scaling
+    int* err;                          // set when a tensor-core wait timed out
+    GravTable low;                     // exact table of the degrees the network leaves out
+};
 
 // Arguments of k_propagate (all device pointers).
 struct PropArgs {
@@ -31,6 +41,7 @@ struct PropArgs {
     int32_t ncells;
     int32_t use_smem;
     GravTable grav;                // the gravity stage's table (plain or split precision)
+    SurrogateRef sur;              // gravity stage through the surrogate (sur.P != null)
     ForceParams force;
     CtrlParams ctrl;
 };
@@ -59,6 +70,7 @@ struct PipeBufs {
     int32_t* bad;         // [cap] latched invalid-radius gravity error
     int32_t* dlist[2];    // drag work lists of the stage: 0 above ~510 km (sweep fits), 1 below
     int32_t* dcount;      // [2]
+    double* ef;           // [cap][3] Earth-fixed positions of the stage (surrogate gravity)
 };
 
 // Kernel durations by class, summed from CUDA events recorded around each
@@ -92,6 +104,10 @@ cudaError_t launch_sigma_recombine(int64_t n, int S, const double* wm, const dou
 int device_sm_count();
 // C[M x N] (FP32) = A[M x K] B[N x K]^T, BF16 row-major operands (mlp.cu);
 // M % 128, N % 256, K % 64 == 0.  *err is set if a wait timed out.
+// The surrogate's residual at the first *n_dev positions pos[i][3], added to
+// out[i * si + k * sk] (surrogate.cu).  Grid sized for up to cap rows.
+cudaError_t launch_surrogate_stage(const SurrogateRef& S, const int32_t* n_dev, int64_t cap, const double* pos,
+                                   double* out, int64_t si, int64_t sk, cudaStream_t st);
 cudaError_t launch_gemm_bf16(int64_t M, int64_t N, int64_t K, const void* A, const void* B, float* C, int* err,
                              cudaStream_t st);
 

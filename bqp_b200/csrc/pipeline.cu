@@ -219,6 +219,18 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
     gravity_cta<NT>(T, parts_max, b0, b1, load, store, lost);
 }
 
+// Earth-fixed positions of the stage's active slots, [slot][3] (the
+// surrogate's input)
+__global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= P.count[cur]) return;
+    const double s = P.sc[sl], c = P.sc[P.cap + sl];
+    const double ex = P.sp[sl], ey = P.sp[P.cap + sl], ez = P.sp[2 * P.cap + sl];
+    P.ef[3 * (size_t)sl] = fma(c, ex, s * ey);
+    P.ef[3 * (size_t)sl + 1] = fma(-s, ex, c * ey);
+    P.ef[3 * (size_t)sl + 2] = ez;
+}
+
 // --------------------------------------------------------------------- drag
 // One state per group of L lanes (jb::density_group): the JB2008 quadrature
 // is the costliest serial chain of the force model, and a batch has only a
@@ -374,6 +386,7 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
     P.bad = (int32_t*)take(c * 4);
     P.dlist[0] = (int32_t*)take(c * 4);
     P.dlist[1] = (int32_t*)take(c * 4);
+    P.ef = (double*)take(3 * c * 8);
     P.dcount = (int32_t*)take(2 * 4);
 }
 
@@ -397,10 +410,13 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     gthreads = gthreads / 32 * 32;
     // column groups need room for their partial sums next to the table
     int gparts = kGravityPartsMax;
-    size_t smem = gravity_smem_bytes(A.grav, gthreads, nt, gparts);
+    // with the surrogate, the exact stage covers only the degrees it leaves out
+    const bool sur = A.sur.P != nullptr;
+    const GravTable GT = sur ? A.sur.low : A.grav;
+    size_t smem = gravity_smem_bytes(GT, gthreads, nt, gparts);
     if (smem > kSmemPerBlock) {
         gparts = 1;
-        smem = gravity_smem_bytes(A.grav, gthreads, nt, gparts);
+        smem = gravity_smem_bytes(GT, gthreads, nt, gparts);
     }
     cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -453,7 +469,11 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
             timed(kKcPrep, [&] { pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s); });
             if (A.force.gravity_on)
                 timed(kKcGravity, [&] {
-                    gker<<<gblocks, gthreads, smem, st>>>(A.grav, gparts, P, cur);
+                    gker<<<gblocks, gthreads, smem, st>>>(GT, gparts, P, cur);
+                    if (sur) {
+                        pl_earth_fixed<<<blocks, kBlock, 0, st>>>(P, cur);
+                        launch_surrogate_stage(A.sur, &P.count[cur], A.n, P.ef, P.agrav, 1, P.cap, st);
+                    }
                 });
             if (A.force.drag)
                 timed(kKcDrag, [&] {

@@ -290,8 +290,10 @@ constexpr size_t kFusedSmall = ((size_t)(kH * 4 + kH + 3 * kH + 3 * kH + 3) * 4 
 constexpr size_t kFusedSmem = kFusedW + kFusedA + kFusedSmall + 64;
 
 __global__ void __launch_bounds__(kFusedThreads, 1)
-    k_mlp_infer(int64_t n, const double* __restrict__ pos, const float* __restrict__ P,
-                const __nv_bfloat16* __restrict__ Wtile, Scale sc, double sigma, double* __restrict__ acc, int* err) {
+    k_mlp_infer(int64_t n_host, const int32_t* __restrict__ n_dev, const double* __restrict__ pos,
+                const float* __restrict__ P, const __nv_bfloat16* __restrict__ Wtile, Scale sc, double sigma,
+                double* __restrict__ acc, int64_t si, int64_t sk, int* err) {
+    const int64_t n = n_dev ? (int64_t)*n_dev : n_host;  // rows: a device-side count inside a graph
     extern __shared__ __align__(128) unsigned char sm[];
     __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm);
     __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(sm + kFusedW);
@@ -462,7 +464,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                 const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
                 const double f = sigma * (sc.R * sc.R) / (px * px + py * py + pz * pz);
                 for (int k = 0; k < 3; ++k)
-                    acc[3 * i + k] += f * (double)(y[k] + sy[row * 3 + k] + sB4[k]);
+                    acc[i * si + k * sk] += f * (double)(y[k] + sy[row * 3 + k] + sB4[k]);
             }
         }
         __syncthreads();
@@ -760,8 +762,22 @@ cudaError_t infer_fused(Model& M, int64_t n, const double* pos, double* acc, int
     if (e != cudaSuccess) return e;
     const int64_t tiles = (n + 127) / 128;
     const int grid = (int)(tiles < device_sm_count() ? tiles : device_sm_count());
-    sg::k_mlp_infer<<<grid, sg::kFusedThreads, sg::kFusedSmem, st>>>(n, pos, M.P, M.Wtile, M.scale, M.sigma, acc,
-                                                                      err);
+    sg::k_mlp_infer<<<grid, sg::kFusedThreads, sg::kFusedSmem, st>>>(n, nullptr, pos, M.P, M.Wtile, M.scale, M.sigma,
+                                                                      acc, 3, 1, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_surrogate_stage(const SurrogateRef& S, const int32_t* n_dev, int64_t cap, const double* pos,
+                                   double* out, int64_t si, int64_t sk, cudaStream_t st) {
+    if (cap <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(sg::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sg::kFusedSmem);
+    if (e != cudaSuccess) return e;
+    const int64_t tiles = (cap + 127) / 128;
+    const int grid = (int)(tiles < device_sm_count() ? tiles : device_sm_count());
+    const sg::Scale sc{S.R, S.r_mid, S.r_half};
+    sg::k_mlp_infer<<<grid, sg::kFusedThreads, sg::kFusedSmem, st>>>(cap, n_dev, pos, S.P, S.Wtile, sc, S.sigma, out,
+                                                                      si, sk, S.err);
     return cudaGetLastError();
 }
 

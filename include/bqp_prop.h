@@ -96,6 +96,8 @@ typedef struct bqp_force_config {
                                   degrees above d in FP32, the rest in FP64 (stage-synchronous
                                   engine and gravity evaluation) */
     int32_t drag_fp32;         /* split precision: 1 evaluates the JB2008 density in FP32 */
+    int32_t surrogate;         /* 1: gravity = exact degrees <= BQP_SURROGATE_DEGREE + the trained
+                                  surrogate (stage-synchronous engine; bqp_surrogate_train first) */
 } bqp_force_config;
 
 /* propagation engines */
