@@ -557,6 +557,7 @@ cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cu
         case kDop853: return run<kDop853>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
         case kDopri5Compat:
             return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
+        case kVern7: return run<kVern7>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -45,3 +45,23 @@ BQP_TAB_CONST double bqp_dop853_a[144] = {
 BQP_TAB_CONST double bqp_dop853_b[12] = {0x1.bcc6368d1177cp-5, 0.0, 0.0, 0.0, 0.0, 0x1.1cd1ed2ad5ae2p+2, 0x1.e43a845d5ab9fp+0, -0x1.7346ecf96af43p+2, 0x1.3ea1df2f0eb98p-2, -0x1.37a028f43b002p-3, 0x1.9c657697fe72dp-3, 0x1.6e44f50ab6bc2p-5};
 BQP_TAB_CONST double bqp_dop853_e[12] = {0x1.adeaea1607e1ap-7, 0.0, 0.0, 0.0, 0.0, -0x1.39a3da55ab5c3p+0, -0x1.fba83bede8a72p-2, 0x1.aa149f7eda509p+0, -0x1.66bc9b10e7e71p-2, 0x1.56330d0783989p-2, 0x1.4f8eb54a31435p-4, -0x1.6e44f50ab6bc2p-6};
 BQP_TAB_CONST double bqp_dop853_e3[12] = {-0x1.84b641fbfa1f1p-3, 0.0, 0.0, 0.0, 0.0, 0x1.1cd1ed2ad5ae2p+2, 0x1.e43a845d5ab9fp+0, -0x1.7346ecf96af43p+2, -0x1.b0d3a26abb716p-2, -0x1.37a028f43b002p-3, 0x1.9c657697fe72dp-3, 0x1.732080ac040edp-6};
+
+// vern7: 10 stages, order 7, error order 6
+#define BQP_VERN7_STAGES 10
+#define BQP_VERN7_ORDER_ERR 6
+#define BQP_VERN7_FSAL 0
+BQP_TAB_CONST double bqp_vern7_c[10] = {0.0, 0x1.47ae147ae147bp-8, 0x1.be02468acf135p-4, 0x1.4e81b4e81b4e8p-3, 0x1.d26e978d4fdf4p-2, 0x1.38119f5c18ee8p-1, 0x1.c49ba5e353f7dp-1, 0x1.d99999999999ap-1, 0x1.0000000000000p+0, 0x1.0000000000000p+0};
+BQP_TAB_CONST double bqp_vern7_a[100] = {
+  0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.47ae147ae147bp-8, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  -0x1.13a8847ce7186p+0, 0x1.2f88a8e59409ap+0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.4e81b4e81b4e8p-5, 0.0, 0x1.f5c28f5c28f5cp-4, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.471fb9cddc9bdp-1, 0.0, -0x1.3a537b236d238p+1, 0x1.22d95fa19ff87p+1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  -0x1.54ae9142bd52dp+1, 0.0, 0x1.59be93e7f0391p+3, -0x1.0b5344d4e2ef6p+3, 0x1.a416f336399e6p-1, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.8455e02ba6d51p+2, 0.0, -0x1.8b616076cbec1p+4, 0x1.46d71d0ab3120p+4, -0x1.e7f9f82406e6ep+0, 0x1.01948128a32f7p+0, 0.0, 0.0, 0.0, 0.0,
+  0x1.81bfdb75b2798p+3, 0.0, -0x1.8e09ccb12e37ep+5, 0x1.4924a2cc6e376p+5, -0x1.1d8d7a71af007p+2, 0x1.056b3a3a7fe6cp+1, -0x1.92d5cf70abb44p-4, 0.0, 0.0, 0.0,
+  0x1.446bb241baabep+3, 0.0, -0x1.55210bed841c7p+5, 0x1.1e1c582ab6be0p+5, -0x1.164601976fe88p+2, 0x1.01432ab412663p+1, 0x1.651e784ce7ec1p-2, -0x1.15f41b4722d81p-2, 0.0, 0.0,
+  -0x1.683d96681eb23p+5, 0.0, 0x1.76a78c7eacee8p+7, -0x1.340ec1faa9e18p+7, 0x1.2908d1a693680p+4, -0x1.c91368e7b5080p+2, 0x1.4f0e1437ed68ep+0, 0.0, 0.0, 0.0,
+};
+BQP_TAB_CONST double bqp_vern7_b[10] = {0x1.824c7fe71401bp-5, 0.0, 0.0, 0x1.07af8f2c9ce02p-2, 0x1.0c7562a9bdcddp-2, 0x1.37a025dab0159p-3, 0x1.f9da53eb6a44fp-2, -0x1.2d5dcbdcea09dp-2, 0x1.4d138cc3aa307p-4, 0.0};
+BQP_TAB_CONST double bqp_vern7_e[10] = {0x1.4dd7897422b5dp-9, 0.0, 0.0, -0x1.3c7c7d0e25406p-7, 0x1.5898171705ca6p-5, -0x1.11216681df170p-4, 0x1.0f5eb708b4517p-2, -0x1.2d5dcbdcea09dp-2, 0x1.4d138cc3aa307p-4, -0x1.4c842c994e2b0p-6};

@@ -47,6 +47,16 @@ struct Tab<kDop853> {
     __device__ static double e3(int i) { return bqp_dop853_e3[i]; }
 };
 
+template <>
+struct Tab<kVern7> {
+    static constexpr int S = 10, ORDER_ERR = 6, FSAL = 0, HAS_E3 = 0;
+    __device__ static double a(int i, int j) { return bqp_vern7_a[i * S + j]; }
+    __device__ static double b(int i) { return bqp_vern7_b[i]; }
+    __device__ static double c(int i) { return bqp_vern7_c[i]; }
+    __device__ static double e(int i) { return bqp_vern7_e[i]; }
+    __device__ static double e3(int) { return 0.0; }
+};
+
 enum OutMode : int32_t { kOutFinalEci = 0, kOutSampledEci = 1, kOutSampledDelta = 2 };
 enum Phase : int32_t { kNeedTraj = 0, kNeedSegment = 1, kStepping = 2, kDone = 3, kFinished = 4 };
 enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16, kSegSampled = 32 };

@@ -158,12 +158,13 @@ def test_jb2008_sweep_fit_matches_quadrature():
 
 # -------------------------------------------------------------- trajectories
 @pytest.mark.parametrize("engine", ENGINES)
-def test_fixed_step_dop853_matches_oracle(engine):
+@pytest.mark.parametrize("method", ["dop853", "vern7"])
+def test_fixed_step_matches_oracle(method, engine):
     """Constant steps (every step accepted): |dr| <= 1e-9 relative."""
     order = 20
     text = workloads.synthetic_field(order)
     h_fixed = 30.0
-    ctx = ctx_for(text, order, flags=1 | 4 | 8, eps=1e30, dt_max=h_fixed, engine=engine)
+    ctx = ctx_for(text, order, flags=1 | 4 | 8, method=method, eps=1e30, dt_max=h_fixed, engine=engine)
     F = oracle_force(text, order, 1 | 4 | 8)
     n = 32
     states = workloads.leo_states(n, seed=21)
@@ -172,7 +173,7 @@ def test_fixed_step_dop853_matches_oracle(engine):
     tf = 2 * 5400.0 + 600.0
     got, st, steps, evals = ctx.propagate_final(equ, EPOCH, tf, ballistic=bal, equinoctial=True)
     ref_d, ref_st, ref_steps, ref_evals = O.propagate_final_batch(
-        F, O.ctrl("dop853", eps=1e30, dt_max=h_fixed), equ, EPOCH, tf, bal)
+        F, O.ctrl(method, eps=1e30, dt_max=h_fixed), equ, EPOCH, tf, bal)
     assert (st == 0).all() and (ref_st == 0).all()
     assert np.array_equal(steps, ref_steps) and np.array_equal(evals, ref_evals)
     for i in range(n):
@@ -183,7 +184,8 @@ def test_fixed_step_dop853_matches_oracle(engine):
 
 
 @pytest.mark.parametrize("engine", ENGINES)
-@pytest.mark.parametrize("method,eps", [("dop853", 1e-10), ("dopri5_solver", 1e-9), ("dopri5", 1e-9)])
+@pytest.mark.parametrize("method,eps", [("dop853", 1e-10), ("dopri5_solver", 1e-9), ("dopri5", 1e-9),
+                                        ("vern7", 1e-10)])
 def test_adaptive_final_matches_oracle(method, eps, engine):
     """Adaptive trajectories within the integrator tolerance (70x70 + drag +
     Sun/Moon, one and a half orbits with rectification)."""
@@ -235,13 +237,15 @@ def test_sampled_dopri5_scaled_matches_oracle(engine):
 
 
 @pytest.mark.parametrize("engine", ENGINES)
-def test_sampled_dop853_dense_matches_oracle(engine):
-    """DOP853 samples use an extra force call at each accepted step's end
-    (the reference's dense k1, solver.rs:1672-1676); 70x70 + drag + Sun/Moon."""
+@pytest.mark.parametrize("method", ["dop853", "vern7"])
+def test_sampled_dense_matches_oracle(method, engine):
+    """DOP853 and Vern7 (not FSAL) samples use an extra force call at each
+    accepted step's end (the reference's dense k1, solver.rs:1672-1676);
+    70x70 + drag + Sun/Moon."""
     order = 70
     text = workloads.synthetic_field(order)
     flags = 1 | 4 | 8
-    ctx = ctx_for(text, order, flags=flags, method="dop853", eps=1e-10, engine=engine)
+    ctx = ctx_for(text, order, flags=flags, method=method, eps=1e-10, engine=engine)
     F = oracle_force(text, order, flags)
     n = 6
     states = workloads.leo_states(n, seed=7)
@@ -251,7 +255,7 @@ def test_sampled_dop853_dense_matches_oracle(engine):
     got, st, steps, evals = ctx.propagate_sampled(states, EPOCH, tf, grid)
     assert (st == 0).all()
     for i in range(n):
-        d, rs, ref_steps, ref_evals, nw = O.propagate_sampled(F, O.ctrl("dop853", eps=1e-10), equ[i], EPOCH, tf,
+        d, rs, ref_steps, ref_evals, nw = O.propagate_sampled(F, O.ctrl(method, eps=1e-10), equ[i], EPOCH, tf,
                                                               0.01, 2.2, grid)
         assert rs == 0 and nw == grid.size
         base = np.array([O.equinoc2eci(equ[i], t)[0] for t in grid])
@@ -374,6 +378,18 @@ def test_reference_smoke_sequence():
     assert full["steps"] > 0 and full["rhs_evals"] >= 12 * full["steps"]
     fs = api.propagate_final(eci, EPOCH, tof_s=3600.0, srp=False, method="dop853")
     assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3
+
+
+def test_default_method_is_vern7():
+    """The reference's Python default (method="vern7", lib.rs:237-438) runs
+    Verner's pair: its final state agrees with DOP853's within the tolerance
+    and it reports 10 force calls per step."""
+    eci = api.kep_to_eci(np.array([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0]))
+    out = api.propagate(eci, EPOCH, tof_s=3600.0, srp=False)
+    assert out["completed"], out
+    assert out["rhs_evals"] >= 10 * out["steps"]
+    ref = api.propagate_final(eci, EPOCH, tof_s=3600.0, srp=False, method="dop853")
+    assert np.linalg.norm(out["states_eci"][-1][:3] - ref[:3]) < 1e-3
 
 
 @pytest.mark.parametrize("engine", ENGINES)

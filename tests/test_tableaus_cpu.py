@@ -1,0 +1,131 @@
+"""Order conditions of the explicit Runge-Kutta tables in ``rk_tableaus.h``.
+
+For every rooted tree t of order |t| <= p the weights of an order-p method
+satisfy  sum_i b_i Phi_i(t) = 1 / gamma(t)  (Butcher's conditions; Hairer,
+Norsett & Wanner, Solving ODEs I, ch. II.2), and the error weights e of an
+embedded pair of error order q satisfy  sum_i e_i Phi_i(t) = 0  for |t| <= q
+(both b and b - e are order-q rules) but not for every tree of order q + 1.
+The tables are binary64 roundings of the published decimals, so each
+condition holds to a tolerance scaled by the size of its terms.
+"""
+import re
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+HEADER = Path(__file__).resolve().parents[1] / "bqp_b200" / "csrc" / "rk_tableaus.h"
+
+# name -> (order, error order, tolerance relative to the sum of |terms|)
+PAIRS = {"dopri5": (5, 4, 1e-14), "dop853": (8, 5, 1e-11), "vern7": (7, 6, 1e-11)}
+
+
+def load(name):
+    text = HEADER.read_text()
+
+    def arr(suffix):
+        m = re.search(rf"bqp_{name}_{suffix}\[\d+\] = \{{(.*?)\}};", text, re.S)
+        return np.array([float.fromhex(t) for t in m.group(1).replace(",", " ").split()])
+
+    c, b, e = arr("c"), arr("b"), arr("e")
+    s = len(c)
+    a = arr("a").reshape(s, s)
+    return c, a, b, e
+
+
+@lru_cache(maxsize=None)
+def trees(n):
+    """Rooted trees with n vertices, each a sorted tuple of its subtrees."""
+    if n == 1:
+        return [()]
+    out = set()
+
+    def forests(total, min_tree):
+        # multisets of trees with `total` vertices, non-decreasing in (order, tree)
+        if total == 0:
+            yield ()
+            return
+        for k in range(1, total + 1):
+            for t in trees(k):
+                key = (k, t)
+                if min_tree is not None and key < min_tree:
+                    continue
+                for rest in forests(total - k, key):
+                    yield (t,) + rest
+
+    for f in forests(n - 1, None):
+        out.add(tuple(sorted(f, key=lambda t: (size(t), t))))
+    return sorted(out, key=lambda t: (len(t), t))
+
+
+def size(t):
+    return 1 + sum(size(u) for u in t)
+
+
+def gamma(t):
+    g = size(t)
+    for u in t:
+        g *= gamma(u)
+    return g
+
+
+def phi(t, a):
+    """Elementary weight vector Phi(t): Phi_i = prod over subtrees u of (A Phi(u))_i."""
+    v = np.ones(a.shape[0])
+    for u in t:
+        v = v * (a @ phi(u, a))
+    return v
+
+
+def test_tree_counts():
+    # number of rooted trees of order 1..8 (OEIS A000081)
+    assert [len(trees(n)) for n in range(1, 9)] == [1, 1, 2, 4, 9, 20, 48, 115]
+
+
+@pytest.mark.parametrize("name", sorted(PAIRS))
+def test_row_sums(name):
+    c, a, b, e = load(name)
+    assert np.allclose(a.sum(axis=1), c, rtol=0, atol=1e-13 * max(1.0, np.abs(a).max()))
+    assert np.all(np.triu(a) == 0.0)  # explicit
+
+
+@pytest.mark.parametrize("name", sorted(PAIRS))
+def test_order_conditions(name):
+    order, order_err, tol = PAIRS[name]
+    c, a, b, e = load(name)
+    for n in range(1, order + 1):
+        for t in trees(n):
+            p = phi(t, a)
+            got = b @ p
+            scale = np.abs(b * p).sum()
+            assert abs(got - 1.0 / gamma(t)) <= tol * scale, (name, t, got, 1.0 / gamma(t))
+    worst_next = 0.0
+    for n in range(1, order_err + 2):
+        for t in trees(n):
+            p = phi(t, a)
+            r = abs(e @ p)
+            scale = np.abs(e * p).sum() + np.abs(b * p).sum()
+            if n <= order_err:
+                assert r <= tol * scale, (name, "error weights", t, r)
+            else:
+                worst_next = max(worst_next, r * gamma(t))
+    assert worst_next > 1e-6, (name, "error estimate vanishes at order", order_err + 1)
+
+
+@pytest.mark.parametrize("name", sorted(PAIRS))
+def test_not_higher_order(name):
+    # the stated order is the exact order: some tree of order p + 1 fails
+    order, _, _ = PAIRS[name]
+    c, a, b, e = load(name)
+    worst = max(abs(b @ phi(t, a) - 1.0 / gamma(t)) * gamma(t) for t in trees(order + 1))
+    assert worst > 1e-8
+
+
+def test_vern7_stage_one_pin():
+    # the reference pins Vern7's second stage bit for bit
+    # (odesolve/tableau/vern7.rs:140-152): c1 = a10 = 0.005, b1 = err1 = 0
+    c, a, b, e = load("vern7")
+    assert c[1] == 0.005 and a[1, 0] == 0.005
+    assert b[1] == 0.0 and e[1] == 0.0
+    assert c[-1] == 1.0 and np.all(a[-1, 7:] == 0.0)  # error stage built on stages 0-6
