@@ -30,7 +30,7 @@ STATUS_NAMES = {
 ST_OK, ST_GROUND, ST_GRAVITY_RADIUS = 0, 9, 6
 
 FORCE_DRAG, FORCE_SRP, FORCE_SUN, FORCE_MOON = 1, 2, 4, 8
-METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3}
+METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3, "vern9": 4}
 ENGINES = {"pipeline": 0, "persistent": 1}
 
 E_ARG, E_CUDA, E_COEFF, E_UNSUPPORTED, E_NOMEM = -1, -2, -3, -4, -5

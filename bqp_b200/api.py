@@ -15,7 +15,7 @@ Python binding does not expose): ``propagate_batch_final`` and
 ``propagate_batch_sampled``.
 
 Options this build does not implement raise ``ValueError`` naming the option
-(SRP with binary eclipse; the vern9/tsit5/rkv98 tableaus); they are never
+(SRP with binary eclipse; the tsit5/rkv98 tableaus); they are never
 silently replaced.  ``gravity_field`` (extra keyword) takes a normalised
 ``deg ord C S`` text or a path, which lifts the embedded field's degree-15 cap.
 """
@@ -36,9 +36,10 @@ MAX_GRAVITY_ORDER = 15  # embedded DIR-R6 field (lib.rs:53)
 DATA = Path(__file__).resolve().parent / "data"
 _DEFAULT_FIELD = DATA / "dir_r6_d15.txt"
 
-_UNBUILT_METHODS = ("vern9", "tsit5", "rkv98")
+_UNBUILT_METHODS = ("tsit5", "rkv98")
 _METHODS = {"dop853": N.METHODS["dop853"], "dopri5": N.METHODS["dopri5"],
-            "dopri5_solver": N.METHODS["dopri5_solver"], "vern7": N.METHODS["vern7"]}
+            "dopri5_solver": N.METHODS["dopri5_solver"], "vern7": N.METHODS["vern7"],
+            "vern9": N.METHODS["vern9"]}
 
 
 def _six(value, what):
@@ -83,7 +84,7 @@ def force_config(gravity_order=5, drag=True, srp=True, sun=True, moon=True, atm_
                          "exact JB2008 quadrature)")
     name = str(method).lower()
     if name in _UNBUILT_METHODS:
-        raise ValueError(f"integrator method {name!r} is not built here; use 'vern7', 'dop853' or 'dopri5'")
+        raise ValueError(f"integrator method {name!r} is not built here; use 'vern7', 'vern9', 'dop853' or 'dopri5'")
     if name not in _METHODS:
         raise ValueError(f"unknown integrator method {name!r}; use one of vern7, vern9, dop853, tsit5, rkv98, "
                          "dopri5")

@@ -521,7 +521,7 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_ARG, "unknown force flags 0x%x", c->force_flags);
     if ((c->force_flags & BQP_FORCE_DRAG) && c->atm_model != 4 && c->atm_model != 7)
         return fail(BQP_E_UNSUPPORTED, "atm_model %d is not built; use 4 (exact JB2008) or 7", c->atm_model);
-    if (c->method < 0 || c->method > 3) return fail(BQP_E_ARG, "unknown method %d", c->method);
+    if (c->method < 0 || c->method > 4) return fail(BQP_E_ARG, "unknown method %d", c->method);
     if (c->error_control == 0) {
         if (!(std::isfinite(c->eps) && c->eps > 0.0)) return fail(BQP_E_ARG, "eps must be finite and > 0");
     } else if (c->error_control == 1) {

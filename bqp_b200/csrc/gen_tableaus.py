@@ -10,12 +10,14 @@
   dop853_coefficients``), which carries the same decimal constants as the
   reference's ``odesolve/tableau/dop853_coeffs.rs``.
 
-* Vern7: Verner's 7(6) "numerically optimal" pair (J.H. Verner, Numerical
-  Algorithms 53 (2010) 383-396), 10 stages, not FSAL; the tenth stage (c = 1,
-  built on stages 0-6) serves only the error estimate.  Its published decimal
-  constants are read from the reference's ``odesolve/tableau/vern7.rs`` when
-  the header is generated (the reference tree is needed only then), so both
-  sides step with the same binary64 numbers.
+* Vern7 and Vern9: Verner's 7(6) and 9(8) "numerically optimal" pairs (J.H.
+  Verner, Numerical Algorithms 53 (2010) 383-396), 10 and 16 stages, not
+  FSAL.  Vern7's tenth stage (c = 1, built on stages 0-6) serves only the
+  error estimate; Vern9's stages 14 and 15 both sit at c = 1, the second built
+  on stages 0-12 for the error estimate only.  Their published decimal
+  constants are read from the reference's ``odesolve/tableau/vern7.rs`` and
+  ``vern9.rs`` when the header is generated (the reference tree is needed
+  only then), so both sides step with the same binary64 numbers.
 
 Values are emitted as C99 hex-float literals so the header is bit-exact.
 Run: ``python bqp_b200/csrc/gen_tableaus.py [REFERENCE_ROOT]`` (rewrites the
@@ -62,18 +64,32 @@ def dop853():
     return c, a, b, e5, e3
 
 
-def vern7(ref_root: str):
-    src = (Path(ref_root) / "dust_transfer/crates/lightyear_odeint_rs/src/odesolve/tableau/vern7.rs").read_text()
+def verner(ref_root: str, name: str, stages: int):
+    """Arrays C, A0..A{stages-1}, B and ERR of ``tableau/<name>.rs`` (Rust
+    array literals of decimal constants with ``_`` digit separators)."""
+    src = (Path(ref_root) / f"dust_transfer/crates/lightyear_odeint_rs/src/odesolve/tableau/{name}.rs").read_text()
+    src = re.sub(r"//[^\n]*", "", src)  # comments may hold numbers
 
-    def arr(name):
-        m = re.search(r"const " + name + r": \[f64; \d+\] = \[(.*?)\];", src, re.S)
-        return [float(t.replace("_", "")) for t in re.findall(r"-?[0-9][0-9_]*\.[0-9_]*(?:e-?[0-9]+)?", m.group(1))]
+    def arr(key):
+        m = re.search(r"const " + key + r": \[f64; (\d+)\] = \[(.*?)\];", src, re.S)
+        vals = [float(t.replace("_", "")) for t in re.findall(r"-?[0-9][0-9_]*\.[0-9_]*(?:e-?[0-9]+)?", m.group(2))]
+        assert len(vals) == int(m.group(1)), (name, key)
+        return vals
 
     c = arr("C")
-    a = [arr(f"A{i}") if i else [] for i in range(10)]
+    a = [arr(f"A{i}") if i else [] for i in range(stages)]
     b = arr("B")
     e = arr("ERR")
+    assert len(c) == len(b) == len(e) == stages
     return c, a, b, e, None
+
+
+def vern7(ref_root: str):
+    return verner(ref_root, "vern7", 10)
+
+
+def vern9(ref_root: str):
+    return verner(ref_root, "vern9", 16)
 
 
 def hexf(x: float) -> str:
@@ -119,10 +135,12 @@ def main(ref_root: str = "/root/reference"):
         emit("dopri5", dopri5(), 5, 4, True),
         emit("dop853", dop853(), 8, 5, False),
         emit("vern7", vern7(ref_root), 7, 6, False),
+        emit("vern9", vern9(ref_root), 9, 8, False),
     ]
     out.write_text("\n".join(text))
     # sanity: row sums equal nodes
-    for name, tab in (("dopri5", dopri5()), ("dop853", dop853()), ("vern7", vern7(ref_root))):
+    for name, tab in (("dopri5", dopri5()), ("dop853", dop853()), ("vern7", vern7(ref_root)),
+                      ("vern9", vern9(ref_root))):
         c, a, *_ = tab
         for i, row in enumerate(a):
             # binary64 constants: the sum is exact only to the rounding of

@@ -27,7 +27,7 @@ enum Status : int32_t {
     kWatchdog = 10,
 };
 
-enum Method : int32_t { kDopri5 = 0, kDop853 = 1, kDopri5Compat = 2, kVern7 = 3 };
+enum Method : int32_t { kDopri5 = 0, kDop853 = 1, kDopri5Compat = 2, kVern7 = 3, kVern9 = 4 };
 
 // Force switches and constants (ForceConfig, types.rs:332-411).
 struct ForceParams {

@@ -35,6 +35,9 @@ namespace bqp {
 namespace {
 
 constexpr int kBlock = 256;
+// stage derivative buffers per row: the most stages of any tableau (Vern9's
+// 16) plus the dense-output stage of the sampled non-FSAL path
+constexpr int kStageBufs = Tab<kVern9>::S + 1;
 
 __device__ __forceinline__ double* K(const PipeBufs& P, int st, int i) { return P.k + ((size_t)st * 6 + i) * P.cap; }
 
@@ -373,7 +376,7 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
     P.idx[0] = (int32_t*)take(c * 4);
     P.idx[1] = (int32_t*)take(c * 4);
     P.count = (int32_t*)take(2 * 4);
-    P.k = (double*)take((size_t)13 * 6 * c * 8);
+    P.k = (double*)take((size_t)kStageBufs * 6 * c * 8);
     P.sp = (double*)take(6 * c * 8);
     P.sc = (double*)take(2 * c * 8);
     P.sun = (double*)take(3 * c * 8);
@@ -558,6 +561,7 @@ cudaError_t launch_pipeline(const PropArgs& A, const PipeBufs& P, int method, cu
         case kDopri5Compat:
             return run<kDopri5Compat>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
         case kVern7: return run<kVern7>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
+        case kVern9: return run<kVern9>(A, P, st, max_seconds, gravity_threads, gravity_slots, times);
         default: return cudaErrorInvalidValue;
     }
 }

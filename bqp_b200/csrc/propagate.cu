@@ -276,6 +276,7 @@ cudaError_t launch_propagate(const PropArgs& A, int method, int threads, int blo
         case kDop853: return launch_prop_m<kDop853>(A, threads, blocks, st);
         case kDopri5Compat: return launch_prop_m<kDopri5Compat>(A, threads, blocks, st);
         case kVern7: return launch_prop_m<kVern7>(A, threads, blocks, st);
+        case kVern9: return launch_prop_m<kVern9>(A, threads, blocks, st);
         default: return cudaErrorInvalidValue;
     }
 }

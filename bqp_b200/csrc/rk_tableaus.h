@@ -65,3 +65,29 @@ BQP_TAB_CONST double bqp_vern7_a[100] = {
 };
 BQP_TAB_CONST double bqp_vern7_b[10] = {0x1.824c7fe71401bp-5, 0.0, 0.0, 0x1.07af8f2c9ce02p-2, 0x1.0c7562a9bdcddp-2, 0x1.37a025dab0159p-3, 0x1.f9da53eb6a44fp-2, -0x1.2d5dcbdcea09dp-2, 0x1.4d138cc3aa307p-4, 0.0};
 BQP_TAB_CONST double bqp_vern7_e[10] = {0x1.4dd7897422b5dp-9, 0.0, 0.0, -0x1.3c7c7d0e25406p-7, 0x1.5898171705ca6p-5, -0x1.11216681df170p-4, 0x1.0f5eb708b4517p-2, -0x1.2d5dcbdcea09dp-2, 0x1.4d138cc3aa307p-4, -0x1.4c842c994e2b0p-6};
+
+// vern9: 16 stages, order 9, error order 8
+#define BQP_VERN9_STAGES 16
+#define BQP_VERN9_ORDER_ERR 8
+#define BQP_VERN9_FSAL 0
+BQP_TAB_CONST double bqp_vern9_c[16] = {0.0, 0x1.1b9b66f9335d2p-5, 0x1.8d6967ce8c140p-4, 0x1.2a0f0ddae90f0p-3, 0x1.1f3b645a1cac1p-1, 0x1.d5021996737dfp-3, 0x1.170933f898600p-1, 0x1.4a3d70a3d70a4p-1, 0x1.ef5c28f5c28f6p-2, 0x1.14c447c30d307p-4, 0x1.0000000000000p-2, 0x1.5170f9cd5cc3bp-1, 0x1.a425aee631f8ap-1, 0x1.cd6a161e4f766p-1, 0x1.0000000000000p+0, 0x1.0000000000000p+0};
+BQP_TAB_CONST double bqp_vern9_a[256] = {
+  0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.1b9b66f9335d2p-5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  -0x1.3ef18f369c59bp-5, 0x1.167117b4ed206p-3, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.2a0f0ddae90f0p-5, 0.0, 0x1.bf1694c85d968p-4, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.034c3b60de98fp+1, 0.0, -0x1.e8d561edf47b4p+2, 0x1.8b16b0c8c8c45p+2, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.a2cc3094af286p-5, 0.0, 0.0, 0x1.6aaa2aa3ac883p-3, 0x1.a4e2cd9b2bacap-11, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.0d84a25710b76p-3, 0.0, 0.0, -0x1.2ed338fc2e70cp-2, 0x1.67af6c2c4dcabp-4, 0x1.3e1bba5b61b13p-1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.258bf258bf259p-4, 0.0, 0.0, 0.0, 0.0, 0x1.527c9456e8906p-2, 0x1.f136a0b52b758p-3, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.261eb851eb852p-4, 0.0, 0.0, 0.0, 0.0, 0x1.515833d6d2263p-2, 0x1.dd4307aef4d7fp-4, -0x1.16a3d70a3d70ap-5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.8c3a28e31b86ap-5, 0.0, 0.0, 0.0, 0.0, 0x1.41dce40bdea02p-5, 0x1.b0059aad5ca01p-4, -0x1.5f403a3623eb5p-6, -0x1.aa7ccad443883p-4, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  -0x1.b48fcf1d415e2p-6, 0.0, 0.0, 0.0, 0.0, 0x1.1111111111111p-5, -0x1.4e0b29174ffc1p-3, 0x1.1634feb5b82f0p-5, 0x1.4202d1f0f5b35p-3, 0x1.b8c8cd1850248p-3, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+  0x1.2e342198e9114p-5, 0.0, 0.0, 0.0, 0.0, -0x1.2c11b63bca539p-3, 0x1.cb47a94a6dac5p-3, 0x1.77ea59cbdfec1p-6, -0x1.d5e4d0f53f260p-9, 0x1.6317652422c98p-4, 0x1.c0e7c09c6e85fp-2, 0.0, 0.0, 0.0, 0.0, 0.0,
+  -0x1.f247973256de2p-2, 0.0, 0.0, 0.0, 0.0, -0x1.937e9c1d4f589p+2, -0x1.1ffed9f2c94dcp-2, -0x1.56ea1a3275a6bp+1, 0x1.09a234ea69dfap-1, 0x1.5d87c9583ee69p+0, 0x1.78a55517c6c06p+2, 0x1.66c27034fd6f7p+1, 0.0, 0.0, 0.0, 0.0,
+  0x1.ac94e58d1e167p-2, 0.0, 0.0, 0.0, 0.0, 0x1.ae5efcd22bc8bp+2, -0x1.b3a7aa564f1f2p-2, 0x1.abf0923fc4fe7p+1, 0x1.3bf220b41a2b7p-1, -0x1.dc2485116b775p-1, -0x1.86658fabeb833p+2, -0x1.80484ad86ab9fp+1, 0x1.0572ac219c10cp-2, 0.0, 0.0, 0.0,
+  -0x1.8f0a1ec67ecfap-1, 0.0, 0.0, 0.0, 0.0, -0x1.bdfeb5c74a523p+3, 0x1.4086460e4235ep+0, -0x1.d620c576b34cap+3, -0x1.fa93f67e432e5p-2, 0x1.1f19cd44440d6p+1, 0x1.abc5c939fb0acp+3, 0x1.ccb15c5c836e1p+3, -0x1.985c949bcbe2ep-1, 0x1.c3848fd794123p-2, 0.0, 0.0,
+  0x1.076e39e9f4653p+1, 0.0, 0.0, 0.0, 0.0, 0x1.65ba1ce93a093p+4, 0x1.d1a9bc7c3cdb6p-1, 0x1.1f20f98d46d29p+5, -0x1.b8a45519d15a4p+1, -0x1.37640bec04168p+2, -0x1.2e8e8e718f1f2p+4, -0x1.121bbd355f980p+5, 0x1.43c7155a15e35p+0, 0.0, 0.0, 0.0,
+};
+BQP_TAB_CONST double bqp_vern9_b[16] = {0x1.dece255e50a69p-7, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -0x1.90eaee0a3fef2p-2, 0x1.d9476af99b058p-3, 0x1.05127df5b7ad1p-3, 0x1.cc11d91f87e5ap-3, 0x1.2309f29447a78p-1, 0x1.dd4161c2dc3f7p-5, 0x1.1769863774af7p-3, 0x1.f4dc75b3aef35p-6, 0.0};
+BQP_TAB_CONST double bqp_vern9_e[16] = {-0x1.5f24207ad4dafp-8, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -0x1.4aa06a5b4365ap+1, 0x1.23e2da5f7ecf5p-3, 0x1.b7c499f6c6ea1p-7, -0x1.d5c71f7fb597fp-6, 0x1.4ffffd1b94e09p+1, -0x1.21550a3cfce7cp-2, 0x1.1769863774af7p-3, 0x1.f4dc75b3aef35p-6, -0x1.8c052e109946cp-5};

@@ -57,6 +57,16 @@ struct Tab<kVern7> {
     __device__ static double e3(int) { return 0.0; }
 };
 
+template <>
+struct Tab<kVern9> {
+    static constexpr int S = 16, ORDER_ERR = 8, FSAL = 0, HAS_E3 = 0;
+    __device__ static double a(int i, int j) { return bqp_vern9_a[i * S + j]; }
+    __device__ static double b(int i) { return bqp_vern9_b[i]; }
+    __device__ static double c(int i) { return bqp_vern9_c[i]; }
+    __device__ static double e(int i) { return bqp_vern9_e[i]; }
+    __device__ static double e3(int) { return 0.0; }
+};
+
 enum OutMode : int32_t { kOutFinalEci = 0, kOutSampledEci = 1, kOutSampledDelta = 2 };
 enum Phase : int32_t { kNeedTraj = 0, kNeedSegment = 1, kStepping = 2, kDone = 3, kFinished = 4 };
 enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16, kSegSampled = 32 };

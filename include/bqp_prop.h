@@ -65,6 +65,7 @@ extern "C" {
 #define BQP_METHOD_DOP853 1        /* StepperMethod::Dop853 */
 #define BQP_METHOD_DOPRI5_COMPAT 2 /* StepperMethod::Dopri5Compat, Python method="dopri5" */
 #define BQP_METHOD_VERN7 3         /* StepperMethod::Vern7 (tableau/vern7.rs), the Python default */
+#define BQP_METHOD_VERN9 4         /* StepperMethod::Vern9 (tableau/vern9.rs) */
 
 /* Force model and solver settings; replaces ForceConfig
  * (lightyear_odeint_rs/src/types.rs:332-411) as built by force_config()

@@ -20,7 +20,7 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _lp = C.POINTER(C.c_long)
 
-METHOD = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3}  # same names as bqp_b200._native.METHODS
+METHOD = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3, "vern9": 4}  # same names as bqp_b200._native.METHODS
 
 
 def build(force: bool = False) -> Path:

@@ -964,7 +964,7 @@ struct Rhs {
 };
 
 // ------------------------------------------------------------ RK integrator
-enum Method { METHOD_DOPRI5 = 0, METHOD_DOP853 = 1, METHOD_DOPRI5_COMPAT = 2, METHOD_VERN7 = 3 };
+enum Method { METHOD_DOPRI5 = 0, METHOD_DOP853 = 1, METHOD_DOPRI5_COMPAT = 2, METHOD_VERN7 = 3, METHOD_VERN9 = 4 };
 enum Status {
     ST_SUCCESS = 0, ST_MAX_STEPS = 1, ST_STEP_UNDERFLOW = 2, ST_INVALID_INPUT = 3,
     ST_NON_FINITE = 4, ST_MAX_REJECTS = 5, ST_GRAVITY = 6, ST_REBASE_FAILED = 7,
@@ -981,6 +981,8 @@ Tab tableau(int m) {
         return {12, 5, 0, bqp_dop853_c, bqp_dop853_a, bqp_dop853_b, bqp_dop853_e, bqp_dop853_e3, 1e-6};
     if (m == METHOD_VERN7)  // tableau/vern7.rs: no third-order blend
         return {10, 6, 0, bqp_vern7_c, bqp_vern7_a, bqp_vern7_b, bqp_vern7_e, nullptr, 0.0};
+    if (m == METHOD_VERN9)  // tableau/vern9.rs
+        return {16, 8, 0, bqp_vern9_c, bqp_vern9_a, bqp_vern9_b, bqp_vern9_e, nullptr, 0.0};
     return {7, 4, 1, bqp_dopri5_c, bqp_dopri5_a, bqp_dopri5_b, bqp_dopri5_e, nullptr, 0.0};
 }
 

@@ -158,7 +158,7 @@ def test_jb2008_sweep_fit_matches_quadrature():
 
 # -------------------------------------------------------------- trajectories
 @pytest.mark.parametrize("engine", ENGINES)
-@pytest.mark.parametrize("method", ["dop853", "vern7"])
+@pytest.mark.parametrize("method", ["dop853", "vern7", "vern9"])
 def test_fixed_step_matches_oracle(method, engine):
     """Constant steps (every step accepted): |dr| <= 1e-9 relative."""
     order = 20
@@ -185,7 +185,7 @@ def test_fixed_step_matches_oracle(method, engine):
 
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("method,eps", [("dop853", 1e-10), ("dopri5_solver", 1e-9), ("dopri5", 1e-9),
-                                        ("vern7", 1e-10)])
+                                        ("vern7", 1e-10), ("vern9", 1e-10)])
 def test_adaptive_final_matches_oracle(method, eps, engine):
     """Adaptive trajectories within the integrator tolerance (70x70 + drag +
     Sun/Moon, one and a half orbits with rectification)."""
@@ -237,9 +237,9 @@ def test_sampled_dopri5_scaled_matches_oracle(engine):
 
 
 @pytest.mark.parametrize("engine", ENGINES)
-@pytest.mark.parametrize("method", ["dop853", "vern7"])
+@pytest.mark.parametrize("method", ["dop853", "vern7", "vern9"])
 def test_sampled_dense_matches_oracle(method, engine):
-    """DOP853 and Vern7 (not FSAL) samples use an extra force call at each
+    """DOP853, Vern7 and Vern9 (not FSAL) samples use an extra force call at each
     accepted step's end (the reference's dense k1, solver.rs:1672-1676);
     70x70 + drag + Sun/Moon."""
     order = 70

@@ -89,7 +89,7 @@ def test_python_argument_validation_mirrors_binding():
     with pytest.raises(ValueError, match="unknown integrator"):
         api.propagate(eci, 2460310.5, 600.0, srp=False, method="rk4")
     with pytest.raises(ValueError, match="not built"):
-        api.propagate(eci, 2460310.5, 600.0, srp=False, method="vern9")
+        api.propagate(eci, 2460310.5, 600.0, srp=False, method="tsit5")
     with pytest.raises(ValueError, match="srp"):
         api.propagate(eci, 2460310.5, 600.0, method="dop853")
     with pytest.raises(ValueError, match="atm_model"):

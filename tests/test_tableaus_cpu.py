@@ -18,7 +18,7 @@ import pytest
 HEADER = Path(__file__).resolve().parents[1] / "bqp_b200" / "csrc" / "rk_tableaus.h"
 
 # name -> (order, error order, tolerance relative to the sum of |terms|)
-PAIRS = {"dopri5": (5, 4, 1e-14), "dop853": (8, 5, 1e-11), "vern7": (7, 6, 1e-11)}
+PAIRS = {"dopri5": (5, 4, 1e-14), "dop853": (8, 5, 1e-11), "vern7": (7, 6, 1e-11), "vern9": (9, 8, 1e-11)}
 
 
 def load(name):
