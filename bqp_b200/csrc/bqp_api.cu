@@ -744,6 +744,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.use_smem = ctx->use_smem;
     if (int rc = ensure_fit2(ctx)) return rc;
     A.force = force_params(ctx);
+    A.fit_host = A.force.fit ? &ctx->h_fit : nullptr;
     A.ctrl = ctrl_params(ctx);
     A.grav = grav_table(ctx);
     if (ctx->cfg.surrogate) {

@@ -560,12 +560,13 @@ __device__ __forceinline__ SweepG fitted_sweep(const double* c, const int32_t* e
                                                double zend_start, double zr, int n, double ain0, const double* tc,
                                                int q, unsigned gmask) {
     static_assert(kFit2A % L == 0, "series rows must split evenly over the lanes");
-    constexpr int R = kFit2A / L;
+    constexpr int R = L == 1 ? 1 : kFit2A / L;
     SweepG s;
-    // rows of the series in T_inf, this lane's share
+    // rows of the series in T_inf, this lane's share (one lane: each row is
+    // summed where the series in altitude takes it)
     double v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < (L == 1 ? 0 : R); ++r) {
         const double* row = c + (r * L + q) * kFit2T;
         double b1 = 0.0, b2 = 0.0;
         for (int j = kFit2T - 1; j >= 1; --j) {
@@ -604,7 +605,19 @@ __device__ __forceinline__ SweepG fitted_sweep(const double* c, const int32_t* e
     double a1 = 0.0, a2 = 0.0, sum = 0.0;
 #pragma unroll
     for (int ka = kFit2A - 1; ka >= 0; --ka) {
-        const double vk = L == 1 ? v[ka] : __shfl_sync(gmask, v[ka / L], ka % L, L);
+        double vk;
+        if constexpr (L == 1) {
+            const double* row = c + ka * kFit2T;
+            double b1 = 0.0, b2 = 0.0;
+            for (int j = kFit2T - 1; j >= 1; --j) {
+                const double tmp = fma(2.0 * xt, b1, -b2) + row[j];
+                b2 = b1;
+                b1 = tmp;
+            }
+            vk = fma(xt, b1, -b2) + row[0];
+        } else {
+            vk = __shfl_sync(gmask, v[ka / L], ka % L, L);
+        }
         if (ka == 0) {
             sum = fma(xa, a1, -a2) + vk;
         } else {
@@ -623,10 +636,39 @@ __device__ __forceinline__ SweepG fitted_sweep(const double* c, const int32_t* e
     return s;
 }
 
+// The fixed-node sweep fits are one table for every context (the sums depend
+// only on T_inf; the node altitudes are fixed), so the density kernel of the
+// stage-synchronous engine reads them from constant memory: this
+// translation unit's copy, which the engine fills on the caller's stream
+// before each propagation's kernels.
+static __constant__ JbFit c_fixed_fit;
+
+// The two fixed-node sums at one T_inf (cheb_eval of both series, the same
+// operations): the two recurrences run in one loop as independent chains,
+// unrolled so that every coefficient is a constant-bank operand.
+__device__ __forceinline__ void cheb_eval_pair(double t, double* low, double* mid) {
+    const JbFit& f = c_fixed_fit;
+    const double x = (2.0 * t - (f.hi + f.lo)) / (f.hi - f.lo);
+    double a1 = 0.0, a2 = 0.0, b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int j = kFitTerms - 1; j >= 1; --j) {
+        const double ta = fma(2.0 * x, a1, -a2) + f.low[j];
+        const double tb = fma(2.0 * x, b1, -b2) + f.mid[j];
+        a2 = a1;
+        a1 = ta;
+        b2 = b1;
+        b1 = tb;
+    }
+    *low = fma(x, a1, -a2) + f.low[0];
+    *mid = fma(x, b1, -b2) + f.mid[0];
+}
+
+// fixed_fit: use the fixed-node sweep fits (c_fixed_fit) where they apply.
 template <int L>
 __device__ double density_group(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
-                                const Drivers& d, int q, unsigned gmask, const JbFit* fit = nullptr,
+                                const Drivers& d, int q, unsigned gmask, bool fixed_fit,
                                 const JbFit2* fit2 = nullptr) {
+    const JbFit* fit = fixed_fit ? &c_fixed_fit : nullptr;
     double code = 0.0;
     if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) || !isfinite(alt_m) ||
         !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) || !isfinite(d.s10b) || !isfinite(d.m10) ||
@@ -685,8 +727,9 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
     const bool use2 = use_fit && fit2 != nullptr && tinf >= fit2->tlo && tinf <= fit2->thi;
     const double xt2 = use2 ? (2.0 * tinf - (fit2->thi + fit2->tlo)) / (fit2->thi - fit2->tlo) : 0.0;
     SweepG lo;
+    double mid_fit_sum = 0.0;  // the middle sweep's fitted sum (used above 500 km)
     if (use_fit && alt >= 105.0) {
-        lo.sum = cheb_eval(fit->low, fit->terms, fit->lo, fit->hi, tinf);
+        cheb_eval_pair(tinf, &lo.sum, &mid_fit_sum);
         lo.z = fit->low_z;
         lo.zend = fit->low_zend;
         lo.mb = fit->low_mb2;
@@ -713,7 +756,7 @@ __device__ double density_group(double mjd, double sun_dec, double hour_angle, d
     } else {
         SweepG mid;
         if (use_fit && alt >= 500.0) {
-            mid.sum = cheb_eval(fit->mid, fit->terms, fit->lo, fit->hi, tinf);
+            mid.sum = mid_fit_sum;
             mid.z = fit->mid_z;
             mid.zend = fit->mid_zend;
             mid.tloc = local_temp(mid.z, tc);

@@ -44,6 +44,8 @@ struct PropArgs {
     SurrogateRef sur;              // gravity stage through the surrogate (sur.P != null)
     ForceParams force;
     CtrlParams ctrl;
+    const jb::JbFit* fit_host;     // host copy of *force.fit (null with it): the stage-synchronous
+                                   // drag kernel takes it by value, in kernel parameter space
 };
 
 struct TrajState;

@@ -35,6 +35,23 @@ namespace bqp {
 namespace {
 
 constexpr int kBlock = 256;
+
+// Drag lanes per state above and below ~510 km (the lanes share the sweep
+// series and the intervals walked exactly), and the drag kernel's minimum
+// resident CTAs per SM, which sets its register budget (3: 80 registers, a
+// few hundred bytes spilled).  Measured on 65,536 LEO states at 70x70: one
+// lane above 510 km and four below, both lists in one launch at 3 CTAs per
+// SM, fit every state of a stage in one wave; that took the drag kernels
+// from 1,023 ms to 701 ms per 5,400 s segment.
+#ifndef BQP_DRAG_LANES_HIGH
+#define BQP_DRAG_LANES_HIGH 1
+#endif
+#ifndef BQP_DRAG_LANES_LOW
+#define BQP_DRAG_LANES_LOW 4
+#endif
+#ifndef BQP_DRAG_MIN_BLOCKS
+#define BQP_DRAG_MIN_BLOCKS 3
+#endif
 // stage derivative buffers per row: the most stages of any tableau (Vern9's
 // 16) plus the dense-output stage of the sampled non-FSAL path
 constexpr int kStageBufs = Tab<kVern9>::S + 1;
@@ -235,12 +252,15 @@ __global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
 }
 
 // --------------------------------------------------------------------- drag
-// One state per group of L lanes (jb::density_group): the JB2008 quadrature
-// is the costliest serial chain of the force model, and a batch has only a
-// few hundred states per SM, so each state is spread over L lanes.
+// One state per group of L lanes (jb::density_group): the JB2008 model is the
+// longest serial chain of the force call, and the kernel is bound by that
+// latency, not by throughput.  Both drag lists go in one launch (blocks
+// [0, nb_hi) take list 0 with LH lanes per state, the rest list 1 with LL),
+// so that a stage's states are resident together in as few waves as the
+// register budget allows.
 template <int L>
-__global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, int list) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs& P, int list, int block) {
+    const int gt = block * blockDim.x + threadIdx.x;
     const int item = gt / L;
     const int q = gt % L;
     const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
@@ -266,8 +286,9 @@ __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, in
             const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
             const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
             const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask, fp.fit,
-                                       fp.fit2);
+            // fixed-node fits from constant memory (fp.fit holds the same numbers)
+            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask,
+                                       fp.fit != nullptr, fp.fit2);
             if (!(rho > 0.0) || !isfinite(rho)) rho = NAN;
             else if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         }
@@ -289,6 +310,12 @@ __global__ void __launch_bounds__(kBlock) pl_drag(ForceParams fp, PipeBufs P, in
     }
     if (q == 0)
         for (int i = 0; i < 3; ++i) P.adrag[(size_t)i * P.cap + slot] = a[i];
+}
+
+template <int LH, int LL>
+__global__ void __launch_bounds__(kBlock, BQP_DRAG_MIN_BLOCKS) pl_drag(ForceParams fp, PipeBufs P, int nb_hi) {
+    if ((int)blockIdx.x < nb_hi) drag_rows<LH>(fp, P, 0, blockIdx.x);
+    else drag_rows<LL>(fp, P, 1, blockIdx.x - nb_hi);
 }
 
 // ------------------------------------------------------------------ control
@@ -400,10 +427,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
-    // drag lanes per state (they share the sweep series and the intervals
-    // walked exactly): 2 above ~510 km, 4 below (two altitude-dependent
-    // sweeps there)
-    constexpr int kLanesHigh = 2, kLanesLow = 4;
+    constexpr int kLanesHigh = BQP_DRAG_LANES_HIGH, kLanesLow = BQP_DRAG_LANES_LOW;
     const int dblocks_hi = (int)((A.n * kLanesHigh + kBlock - 1) / kBlock);
     const int dblocks_lo = (int)((A.n * kLanesLow + kBlock - 1) / kBlock);
     const int nt = gslots == 1 || gslots == 2 ? gslots : 4;
@@ -423,6 +447,13 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     }
     cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (A.force.fit) {
+        // the fixed-node fits: the same table for every context, ordered on
+        // the caller's stream before this call's kernels
+        if (!A.fit_host) return cudaErrorInvalidValue;
+        e = cudaMemcpyToSymbolAsync(jb::c_fixed_fit, A.fit_host, sizeof(jb::JbFit), 0, cudaMemcpyHostToDevice, user);
+        if (e != cudaSuccess) return e;
+    }
     // one CTA per SM (the table fills shared memory); each takes an equal
     // share of the active slots, NT per thread
     int gblocks = device_sm_count();
@@ -480,8 +511,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
                 });
             if (A.force.drag)
                 timed(kKcDrag, [&] {
-                    pl_drag<kLanesHigh><<<dblocks_hi, kBlock, 0, st>>>(A.force, P, 0);
-                    pl_drag<kLanesLow><<<dblocks_lo, kBlock, 0, st>>>(A.force, P, 1);
+                    pl_drag<kLanesHigh, kLanesLow><<<dblocks_hi + dblocks_lo, kBlock, 0, st>>>(A.force, P, dblocks_hi);
                 });
         }
         timed(kKcControl, [&] { pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out); });
@@ -491,7 +521,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
             float ms = 0.0f;
             if (cudaEventElapsedTime(&ms, evs[2 * i], evs[2 * i + 1]) == cudaSuccess) {
                 times->ms[ev_class[i]] += ms;
-                times->launches[ev_class[i]] += ev_class[i] == kKcDrag ? 2 : 1;
+                times->launches[ev_class[i]] += 1;
             }
         }
     };
