@@ -9,6 +9,10 @@ end up.  The reference is the stage-synchronous FP64 form at eps = 1e-12 km,
 itself checked against the CPU restatement by the test suite.
 
     python -m bqp_b200.accuracy --n 512 --days 7 --split-degree 8 --eps 1e-10
+    python -m bqp_b200.accuracy --n 512 --days 7 --methods vern7 vern9 --eps 1e-10 1e-9
+
+With ``--methods`` the forms are the plain FP64 form with each named stepper
+at each tolerance (the reference stays DOP853 at 1e-12 km).
 """
 from __future__ import annotations
 
@@ -66,12 +70,13 @@ def compare(n=512, days=7.0, order=70, seed=0, forms=None, ref_eps=1e-12):
     for f in forms or []:
         out, st, steps, evals, wall = run_form(text, states, bal, tf,
                                                config(order, f["eps"], f.get("split_degree", 0),
-                                                      f.get("drag_fp32", False)))
+                                                      f.get("drag_fp32", False), method=f.get("method", "dop853")))
         ok = (st == 0) & (rst == 0)
         err_m = np.linalg.norm(out[ok, :3] - ref[ok, :3], axis=1) * 1e3
         low = ok & (alt < 500.0)
         rows.append({
-            "form": f.get("name", ""), "eps": f["eps"], "split_degree": f.get("split_degree", 0),
+            "form": f.get("name", ""), "method": f.get("method", "dop853"), "eps": f["eps"],
+            "split_degree": f.get("split_degree", 0),
             "drag_fp32": bool(f.get("drag_fp32", False)), "ok": int(ok.sum()), "n": n,
             "err_m_max": float(err_m.max()) if err_m.size else None,
             "err_m_median": float(np.median(err_m)) if err_m.size else None,
@@ -95,9 +100,14 @@ def main():
     ap.add_argument("--drag-fp32", action="store_true")
     ap.add_argument("--eps", type=float, nargs="+", default=[1e-12, 1e-11, 1e-10, 1e-9])
     ap.add_argument("--fp64-too", action="store_true", help="also the FP64 form at each eps")
+    ap.add_argument("--methods", nargs="+", choices=sorted(N.METHODS),
+                    help="plain FP64 forms with these steppers instead of the split forms")
     args = ap.parse_args()
     forms = []
     for e in args.eps:
+        if args.methods:
+            forms += [{"name": f"plain FP64 {m}", "eps": e, "method": m} for m in args.methods]
+            continue
         forms.append({"name": f"split d>{args.split_degree}", "eps": e, "split_degree": args.split_degree,
                       "drag_fp32": args.drag_fp32})
         if args.fp64_too:

@@ -205,8 +205,11 @@ def test_adaptive_final_matches_oracle(method, eps, engine):
     for i in range(n):
         base, _ = O.equinoc2eci(equ[i], tf)
         ref = base + ref_d[i]
-        # per-step local error <= eps; allow the accumulated bound steps * eps
-        assert np.linalg.norm(got[i, :3] - ref[:3]) <= max(steps[i], 1) * eps * 10, i
+        # each solution lies within ~steps * eps * 10 of the exact trajectory
+        # (the oracle's own Vern7/Vern9 reach 0.85 of that on these rows
+        # against a 1e-14 solution); two solutions with different rounding
+        # and accept/reject sequences differ by at most twice that
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
     # the accept/reject sequence is chaotic in the last bits; step counts agree to a few percent
     assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
 
