@@ -266,10 +266,14 @@ def test_sampled_dense_matches_oracle(method, engine):
         # samples are cubic-Hermite interpolants between accepted steps (the
         # reference's dense output); where the two controllers place step
         # boundaries differently the samples differ by that interpolant's own
-        # error, ~1e-6 km for 30-60 s steps
-        assert err.max() <= 5e-6, (i, err.max())
-        assert np.median(err) <= 5e-7, (i, np.median(err))
-        assert abs(evals[i] - ref_evals) <= max(13 * 3, 0.05 * ref_evals)
+        # error, ~1e-6 km for 30-60 s steps.  It grows as h^4: Vern9 steps
+        # ~110 s here, hence its wider bound.
+        scale = 4.0 if method == "vern9" else 1.0
+        assert err.max() <= 5e-6 * scale, (i, err.max())
+        assert np.median(err) <= 5e-7 * scale, (i, np.median(err))
+        # three steps' force calls (stages + the dense stage), or 5 %
+        per_step = {"dop853": 13, "vern7": 11, "vern9": 17}[method]
+        assert abs(evals[i] - ref_evals) <= max(per_step * 3, 0.05 * ref_evals)
 
 
 @pytest.mark.parametrize("engine", ENGINES)
@@ -410,7 +414,7 @@ def test_kernel_timing_by_class(engine):
     if engine == "pipeline":
         for k in ("prep", "gravity", "drag", "control"):
             assert t[k][0] > 0.0 and t[k][1] > 0, (k, t[k])
-        assert t["drag"][1] == 2 * t["gravity"][1]
+        assert t["drag"][1] == t["gravity"][1]  # one drag launch (both altitude lists) per stage
         assert t["persistent"] == (0.0, 0)
     else:
         assert t["persistent"][0] > 0.0 and t["persistent"][1] == 1
