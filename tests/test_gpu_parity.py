@@ -267,13 +267,18 @@ def test_sampled_dense_matches_oracle(method, engine):
         # reference's dense output); where the two controllers place step
         # boundaries differently the samples differ by that interpolant's own
         # error, ~1e-6 km for 30-60 s steps.  It grows as h^4: Vern9 steps
-        # ~110 s here, hence its wider bound.
-        scale = 4.0 if method == "vern9" else 1.0
+        # ~75 s here, and the oracle's own Vern9 samples lie up to 3.0e-5 km
+        # (median up to 4e-6) from a 1e-13 solution on these rows, so two
+        # Vern9 runs may differ by twice that.
+        scale = 20.0 if method == "vern9" else 1.0
         assert err.max() <= 5e-6 * scale, (i, err.max())
         assert np.median(err) <= 5e-7 * scale, (i, np.median(err))
-        # three steps' force calls (stages + the dense stage), or 5 %
+        # three steps' force calls (stages + the dense stage), or a share of
+        # the count: the oracle's own count moves by up to 5 % (DOP853) and
+        # 18 % (Vern9) when its input is perturbed by 1e-15 relative
         per_step = {"dop853": 13, "vern7": 11, "vern9": 17}[method]
-        assert abs(evals[i] - ref_evals) <= max(per_step * 3, 0.05 * ref_evals)
+        share = 0.2 if method == "vern9" else 0.05
+        assert abs(evals[i] - ref_evals) <= max(per_step * 3, share * ref_evals)
 
 
 @pytest.mark.parametrize("engine", ENGINES)
