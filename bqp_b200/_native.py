@@ -6,6 +6,7 @@ loudly when it is missing: there is no CPU fallback for the propagator.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
@@ -75,6 +76,11 @@ SIGNATURES = [
     ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
     ("bqp_jb_fit_check", C.c_int, [_dp, _dp]),
+    ("bqp_ctx_set_jb_drivers", C.c_int, [_vp, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_double,
+                                         C.c_double]),
+    ("bqp_ctx_jb_lookup", C.c_int, [_vp, _dp, C.c_int64, _dp, _ip]),
+    ("bqp_jb_drivers_check", C.c_int, [C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, _dp, C.c_int64, _dp, _ip,
+                                       _lp]),
     ("bqp_ctx_profile", C.c_int, [_vp, C.c_int32]),
     ("bqp_ctx_profile_read", C.c_int, [_vp, _dp, _lp]),
     ("bqp_gravity_eval", C.c_int, [_vp, C.c_int64, _dp, _dp, _ip]),
@@ -211,6 +217,32 @@ class Context:
         n = np.zeros(len(KERNEL_CLASSES), dtype=np.int64)
         check(lib().bqp_ctx_profile_read(self._h, dptr(ms), lptr(n)))
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_CLASSES)}
+
+    def set_jb_drivers(self, solfsmy, dtcfile, span_jd=(0.0, 0.0)):
+        """Take the JB2008 drivers per evaluation from SET space-weather files
+        (SOLFSMY and DTCFILE: text, bytes or a path; both None: back to the
+        configured fixed drivers).  span_jd = the UTC Julian days the
+        propagations will cover, which bounds the drag sweep fits ((0, 0):
+        the whole table).  ValueError names the first rejected line."""
+        if solfsmy is None and dtcfile is None:
+            check(lib().bqp_ctx_set_jb_drivers(self._h, None, 0, None, 0, 0.0, 0.0))
+            return
+        sol, dtc = _text_bytes(solfsmy), _text_bytes(dtcfile)
+        rc = lib().bqp_ctx_set_jb_drivers(self._h, sol, len(sol), dtc, len(dtc), float(span_jd[0]),
+                                          float(span_jd[1]))
+        if rc == E_ARG:
+            raise ValueError(last_error())
+        check(rc)
+
+    def jb_lookup(self, utc_jd):
+        """(drivers [n, 9]: F10, F81c, S10, S81c, M10, M81c, Y10, Y81c, dTc,
+        NaN rows where the tables do not cover the instant; ok [n] bool),
+        evaluated by the device lookup the force kernels use."""
+        jd = f64(np.atleast_1d(utc_jd))
+        out = np.empty((jd.size, 9))
+        ok = np.empty(jd.size, dtype=np.int32)
+        check(lib().bqp_ctx_jb_lookup(self._h, dptr(jd), jd.size, dptr(out), iptr(ok)))
+        return out, ok.astype(bool)
 
     def set_stream(self, stream_ptr: int):
         check(lib().bqp_ctx_set_stream(self._h, _vp(stream_ptr)))
@@ -378,6 +410,32 @@ def sigma_weights(sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0):
                                   dptr(off)))
     p = pts.value
     return p, wm[:p].copy(), wc[:p].copy(), off
+
+
+def _text_bytes(x) -> bytes:
+    """File contents from text, bytes or a path."""
+    if isinstance(x, bytes):
+        return x
+    if isinstance(x, os.PathLike) or (isinstance(x, str) and "\n" not in x and os.path.isfile(x)):
+        return open(x, "rb").read()
+    return str(x).encode()
+
+
+def jb_drivers_check(solfsmy, dtcfile, utc_jd=()):
+    """Host-only parse of SET space-weather files and lookups at utc_jd:
+    ((SOLFSMY rows, DTCFILE rows), drivers [n, 9], ok [n] bool).  ValueError
+    names the first rejected line."""
+    sol, dtc = _text_bytes(solfsmy), _text_bytes(dtcfile)
+    jd = f64(np.atleast_1d(np.asarray(utc_jd, dtype=np.float64)))
+    out = np.empty((jd.size, 9))
+    ok = np.empty(jd.size, dtype=np.int32)
+    counts = np.zeros(2, dtype=np.int64)
+    rc = lib().bqp_jb_drivers_check(sol, len(sol), dtc, len(dtc), dptr(jd), jd.size, dptr(out), iptr(ok),
+                                    lptr(counts))
+    if rc == E_ARG:
+        raise ValueError(last_error())
+    check(rc)
+    return (int(counts[0]), int(counts[1])), out, ok.astype(bool)
 
 
 def jb_fit_check(drivers=(150.0,) * 8 + (20.0,)):

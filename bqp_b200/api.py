@@ -129,12 +129,32 @@ def _cfg_key(cfg: N.ForceConfig):
     return tuple(getattr(cfg, f) if f != "jb_drivers" else tuple(cfg.jb_drivers) for f, _ in cfg._fields_)
 
 
-def context(text: str, cfg: N.ForceConfig) -> N.Context:
-    """A cached native context for (field text, configuration)."""
-    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg))
+def _space_weather(space_weather):
+    """(SOLFSMY bytes, DTCFILE bytes, span) of space_weather = (solfsmy,
+    dtcfile) or (solfsmy, dtcfile, (jd_lo, jd_hi)); each file as text, bytes
+    or a path."""
+    if space_weather is None:
+        return None
+    if not isinstance(space_weather, (tuple, list)) or len(space_weather) not in (2, 3):
+        raise ValueError("space_weather must be (solfsmy, dtcfile) or (solfsmy, dtcfile, (jd_lo, jd_hi))")
+    span = tuple(float(x) for x in space_weather[2]) if len(space_weather) == 3 else (0.0, 0.0)
+    return N._text_bytes(space_weather[0]), N._text_bytes(space_weather[1]), span
+
+
+def context(text: str, cfg: N.ForceConfig, space_weather=None) -> N.Context:
+    """A cached native context for (field text, configuration, space-weather
+    files).  With space_weather the JB2008 drivers come from the SET SOLFSMY
+    / DTCFILE tables at each evaluation's UTC instant (the reference's
+    compiled driver catalogue, jb_rs/src/drivers.rs) instead of the fixed
+    configured drivers."""
+    sw = _space_weather(space_weather)
+    sw_key = None if sw is None else (hashlib.sha256(sw[0]).hexdigest(), hashlib.sha256(sw[1]).hexdigest(), sw[2])
+    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg), sw_key)
     ctx = _CTX.get(key)
     if ctx is None:
         ctx = N.Context(text, cfg)
+        if sw is not None:
+            ctx.set_jb_drivers(sw[0], sw[1], sw[2])
         _CTX[key] = ctx
         while len(_CTX) > _CTX_MAX:
             _CTX.popitem(last=False)[1].close()
@@ -153,8 +173,11 @@ def _equinoctial_of(eci, what):
 # ------------------------------------------------------------------ scalar API
 def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
               moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-              gravity_field=None):
-    """Propagate one ECI state; sampled, rectified path (lib.rs:237-353)."""
+              gravity_field=None, space_weather=None):
+    """Propagate one ECI state; sampled, rectified path (lib.rs:237-353).
+
+    space_weather = (solfsmy, dtcfile[, (jd_lo, jd_hi)]): JB2008 drivers from
+    SET space-weather files (see ``context``); default the fixed drivers."""
     init = _six(state_eci, "state_eci")
     if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
         raise ValueError("epoch_jd must be finite and tof_s > 0")
@@ -178,7 +201,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg)
+    ctx = context(text, cfg, space_weather)
     t_start = time.perf_counter()
     out, st, steps, evals = ctx.propagate_sampled(init, epoch_jd, tof_s, np.array(grid))
     wall_us = int((time.perf_counter() - t_start) * 1e6)
@@ -205,7 +228,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
 
 def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, srp=True, sun=True, moon=True,
                     atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-                    gravity_field=None):
+                    gravity_field=None, space_weather=None):
     """Final state with the ground check enforced (lib.rs:361-438).
 
     Raises ValueError for a physically infeasible arc (ground impact, a radius
@@ -217,7 +240,7 @@ def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, s
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded, ground_check=True)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg)
+    ctx = context(text, cfg, space_weather)
     out, st, _, _ = ctx.propagate_final(init, epoch_jd, tof_s)
     status = int(st[0])
     if status == N.ST_GROUND:
@@ -254,22 +277,22 @@ def _batch_cfg(model: dict, embedded: bool):
 
 
 def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctial=False, gravity_field=None,
-                          **model):
+                          space_weather=None, **model):
     """Final states of a batch with per-row epoch / duration / ballistics.
 
     The reference's LightyearSession::integrate_variable_final_into
     (session.rs:2325-2430).  Returns (states_eci [n,6], status [n], steps [n],
     rhs_evals [n]); failed rows are NaN."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded))
+    ctx = context(text, _batch_cfg(model, embedded), space_weather)
     return ctx.propagate_final(states, epoch_jd, tof_s, ballistic=ballistic, equinoctial=equinoctial)
 
 
 def propagate_batch_sampled(states, epoch_jd, tof_s, t_eval, *, deltas=False, equinoctial=False,
-                            gravity_field=None, **model):
+                            gravity_field=None, space_weather=None, **model):
     """Samples of a batch on one grid; the reference's
     integrate_batch_native_into (batch.rs:247-391) with ``deltas=True``
     (Encke deviations from the initial baseline) or ECI states."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded))
+    ctx = context(text, _batch_cfg(model, embedded), space_weather)
     return ctx.propagate_sampled(states, epoch_jd, tof_s, t_eval, deltas=deltas, equinoctial=equinoctial)

@@ -20,6 +20,7 @@
 
 #include "../../include/bqp_prop.h"
 #include "launch.h"
+#include "space_weather.h"
 #include "surrogate.h"
 
 using namespace bqp;
@@ -405,11 +406,13 @@ bool build_family(Family fam, const jb::JbFit& f1, double tlo, double thi, int n
 
 }  // namespace fit2
 
-// Builds f2 for the drivers; worst[3] = the families' worst relative errors.
-void build_jb_fit2(const jb::JbFit& f1, const jb::Drivers& d, jb::JbFit2& f2, double* worst) {
+// Builds f2 over the exospheric temperatures [tlo, thi]; worst[3] = the
+// families' worst relative errors.
+void build_jb_fit2(const jb::JbFit& f1, double tlo, double thi, jb::JbFit2& f2, double* worst) {
     using namespace jb;
     f2 = JbFit2{};
-    fit2::tinf_range(d, &f2.tlo, &f2.thi);
+    f2.tlo = tlo;
+    f2.thi = thi;
     if (!(f1.valid && f2.tlo >= f1.lo && f2.thi <= f1.hi && f2.thi > f2.tlo)) {
         worst[0] = worst[1] = worst[2] = -1.0;
         return;
@@ -498,10 +501,15 @@ struct bqp_ctx {
     jb::JbFit* d_fit = nullptr;  // JB2008 fixed-node sweep fits (device)
     double fit_worst = -1.0;
     jb::JbFit h_fit{};            // host copy of the same
-    jb::JbFit2* d_fit2 = nullptr; // altitude-dependent sweep fits for the drivers below
-    double fit2_drivers[9] = {};
+    jb::JbFit2* d_fit2 = nullptr; // altitude-dependent sweep fits over the T_inf range below
+    double fit2_tinf[2] = {};     // the range they were built for
     double fit2_worst[3] = {-1.0, -1.0, -1.0};
     bool fit2_built = false;
+    SpaceWeather sw;              // space-weather tables (bqp_ctx_set_jb_drivers), host copy
+    double sw_span[2] = {};       // UTC span the fits are sized for (0, 0: the whole table)
+    double* d_sw_solar = nullptr;
+    int32_t* d_sw_dtc = nullptr;
+    jb::DriverTable dtab{};       // the device copy as the kernels see it (n_solar 0: none)
     bool profile = false;  // kernel timing on (bqp_ctx_profile)
     KernelTimes times{};
     Model* sur = nullptr;          // learned gravity surrogate (bqp_surrogate_*)
@@ -575,6 +583,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.mu_moon = c.mu_moon;
     fp.drivers = {c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
                   c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
+    fp.dtab = ctx->dtab;
     fp.fit = (c.drag_quadrature || !fp.drag) ? nullptr : ctx->d_fit;
     fp.fit2 = fp.fit ? ctx->d_fit2 : nullptr;
     return fp;
@@ -585,11 +594,19 @@ ForceParams force_params(const bqp_ctx* ctx) {
 int ensure_fit2(bqp_ctx* ctx) {
     const bqp_force_config& c = ctx->cfg;
     if (!(c.force_flags & BQP_FORCE_DRAG) || c.drag_quadrature || !ctx->d_fit) return 0;
-    if (ctx->fit2_built && std::memcmp(ctx->fit2_drivers, c.jb_drivers, sizeof c.jb_drivers) == 0) return 0;
+    // the fits depend only on the T_inf range the drivers can produce
+    double tinf[2] = {0.0, 0.0};
+    if (ctx->dtab.n_solar > 0) {
+        if (!space_weather_tinf_range(ctx->sw, ctx->sw_span[0], ctx->sw_span[1], &tinf[0], &tinf[1]))
+            tinf[0] = tinf[1] = 0.0;  // no usable day: the quadrature runs
+    } else {
+        const jb::Drivers d{c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
+                            c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
+        fit2::tinf_range(d, &tinf[0], &tinf[1]);
+    }
+    if (ctx->fit2_built && ctx->fit2_tinf[0] == tinf[0] && ctx->fit2_tinf[1] == tinf[1]) return 0;
     std::unique_ptr<jb::JbFit2> f2(new jb::JbFit2());
-    const jb::Drivers d{c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
-                        c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
-    build_jb_fit2(ctx->h_fit, d, *f2, ctx->fit2_worst);
+    build_jb_fit2(ctx->h_fit, tinf[0], tinf[1], *f2, ctx->fit2_worst);
     if (!ctx->d_fit2) {
         cudaError_t e = cudaMalloc(&ctx->d_fit2, sizeof(jb::JbFit2));
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(JB2008 sweep fits)");
@@ -597,7 +614,8 @@ int ensure_fit2(bqp_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaError_t e = cudaMemcpy(ctx->d_fit2, f2.get(), sizeof(jb::JbFit2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "JB2008 sweep fit upload");
-    std::memcpy(ctx->fit2_drivers, c.jb_drivers, sizeof c.jb_drivers);
+    ctx->fit2_tinf[0] = tinf[0];
+    ctx->fit2_tinf[1] = tinf[1];
     ctx->fit2_built = true;
     return 0;
 }
@@ -1039,6 +1057,8 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_tab_split) cudaFree(ctx->d_tab_split);
     if (ctx->d_fit2) cudaFree(ctx->d_fit2);
     if (ctx->d_tab_low) cudaFree(ctx->d_tab_low);
+    if (ctx->d_sw_solar) cudaFree(ctx->d_sw_solar);
+    if (ctx->d_sw_dtc) cudaFree(ctx->d_sw_dtc);
     delete ctx->sur;
     delete ctx;
     return 0;
@@ -1072,9 +1092,94 @@ int bqp_jb_fit_check(const double* drivers, double* worst) {
     build_jb_fit(f1, &worst[0]);
     const jb::Drivers d{drivers[0], drivers[1], drivers[2], drivers[3], drivers[4],
                         drivers[5], drivers[6], drivers[7], drivers[8]};
-    build_jb_fit2(f1, d, *f2, worst + 1);
+    double tlo, thi;
+    fit2::tinf_range(d, &tlo, &thi);
+    build_jb_fit2(f1, tlo, thi, *f2, worst + 1);
     worst[4] = f2->tlo;
     worst[5] = f2->thi;
+    return 0;
+}
+
+int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_len, const char* dtcfile,
+                           int64_t dtcfile_len, double jd_lo, double jd_hi) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (!std::isfinite(jd_lo) || !std::isfinite(jd_hi) || jd_hi < jd_lo)
+        return fail(BQP_E_ARG, "span must be finite with jd_lo <= jd_hi");
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    auto drop = [&] {
+        if (ctx->d_sw_solar) cudaFree(ctx->d_sw_solar);
+        if (ctx->d_sw_dtc) cudaFree(ctx->d_sw_dtc);
+        ctx->d_sw_solar = nullptr;
+        ctx->d_sw_dtc = nullptr;
+        ctx->dtab = jb::DriverTable{};
+        ctx->sw = SpaceWeather{};
+        ctx->fit2_built = false;
+    };
+    if (!solfsmy && !dtcfile) {
+        drop();
+        return 0;
+    }
+    SpaceWeather sw;
+    const std::string why = parse_space_weather(solfsmy, solfsmy_len, dtcfile, dtcfile_len, &sw);
+    if (!why.empty()) return fail(BQP_E_ARG, "space-weather file rejected: %s", why.c_str());
+    drop();
+    cudaError_t e = cudaMalloc(&ctx->d_sw_solar, sw.solar.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_sw_dtc, sw.dtc.size() * sizeof(int32_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctx->d_sw_solar, sw.solar.data(), sw.solar.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctx->d_sw_dtc, sw.dtc.data(), sw.dtc.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        drop();
+        return cuda_fail(e, "space-weather table upload");
+    }
+    ctx->sw = std::move(sw);
+    ctx->sw_span[0] = jd_lo;
+    ctx->sw_span[1] = jd_hi;
+    ctx->dtab = {ctx->d_sw_solar, ctx->d_sw_dtc, ctx->sw.first_jd, ctx->sw.n_solar, ctx->sw.n_dtc, ctx->sw.dtc_first};
+    return 0;
+}
+
+int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out, int32_t* ok) {
+    if (!ctx || (n > 0 && (!utc_jd || !out || !ok))) return fail(BQP_E_ARG, "null argument");
+    if (ctx->dtab.n_solar <= 0) return fail(BQP_E_ARG, "no space-weather tables set (bqp_ctx_set_jb_drivers)");
+    if (n <= 0) return 0;
+    cudaSetDevice(ctx->device);
+    double *d_jd = nullptr, *d_out = nullptr;
+    int32_t* d_ok = nullptr;
+    cudaError_t e = cudaMalloc(&d_jd, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, n * 9 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_ok, n * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_jd, utc_jd, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_jb_lookup(ctx->dtab, d_jd, n, d_out, d_ok, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, n * 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ok, d_ok, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_jd);
+    cudaFree(d_out);
+    cudaFree(d_ok);
+    if (e != cudaSuccess) return cuda_fail(e, "space-weather lookup");
+    return 0;
+}
+
+int bqp_jb_drivers_check(const char* solfsmy, int64_t solfsmy_len, const char* dtcfile, int64_t dtcfile_len,
+                         const double* utc_jd, int64_t n, double* out, int32_t* ok, int64_t* counts2) {
+    if (!counts2 || (n > 0 && (!utc_jd || !out || !ok))) return fail(BQP_E_ARG, "null argument");
+    SpaceWeather sw;
+    const std::string why = parse_space_weather(solfsmy, solfsmy_len, dtcfile, dtcfile_len, &sw);
+    if (!why.empty()) return fail(BQP_E_ARG, "space-weather file rejected: %s", why.c_str());
+    counts2[0] = sw.n_solar;
+    counts2[1] = sw.n_dtc;
+    const jb::DriverTable T = sw.host_view();
+    for (int64_t i = 0; i < n; ++i) {
+        jb::Drivers d;
+        const bool found = jb::lookup_drivers(T, utc_jd[i], &d);
+        const double v[9] = {d.f10, d.f10b, d.s10, d.s10b, d.m10, d.m10b, d.y10, d.y10b, d.dtc};
+        for (int k = 0; k < 9; ++k) out[9 * i + k] = found ? v[k] : NAN;
+        ok[i] = found ? 1 : 0;
+    }
     return 0;
 }
 

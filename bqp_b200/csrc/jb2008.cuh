@@ -65,6 +65,61 @@ struct Drivers {
     double f10, f10b, s10, s10b, m10, m10b, y10, y10b, dtc;  // dtc: temperature correction, K
 };
 
+// Space-weather tables as the kernels read them: the daily SOLFSMY indices
+// and the hourly DTCFILE temperature corrections (jb_rs/src/drivers.rs).
+// n_solar == 0: no tables, the fixed drivers apply.
+struct DriverTable {
+    const double* solar;  // [n_solar][8]: F10, F81c, S10, S81c, M10, M81c, Y10, Y81c
+    const int32_t* dtc;   // [n_dtc][24] hourly dTc, K
+    double first_jd;      // Julian day number (the row's noon key) of solar row 0
+    int32_t n_solar;
+    int32_t n_dtc;
+    int32_t dtc_first;    // solar row of DTC row 0; DTC days are consecutive SOLFSMY days
+};
+
+// Drivers at a UTC Julian day (drivers.rs:559-580, 631-780): F10/S10 and
+// their 81-day means from the day before, M10 from two days before, Y10 from
+// five; dTc interpolated between the hourly values (the next day's first
+// value in the last hour) and rounded half up, with SET's 1e-7 day bias.
+// The instant goes through MJD and back, as the reference's lookup entry
+// does.  False where the tables do not cover the instant.
+BQP_HD bool lookup_drivers(const DriverTable& T, double jd_in, Drivers* d) {
+    if (T.n_solar <= 0 || !isfinite(jd_in)) return false;
+    const double jd = (jd_in - 2400000.5) + 2400000.5;
+    const double day_jd = floor(jd + 0.5);
+    const double off = day_jd - T.first_jd;
+    if (!(off >= 0.0 && off < (double)T.n_solar)) return false;
+    const int i = (int)off;
+    if (i < 5) return false;  // the 5-day Y10 lag reaches before the table
+    const double frac = jd - (day_jd - 0.5);
+    if (!(frac >= 0.0 && frac < 1.0)) return false;
+    const int r = i - T.dtc_first;
+    if (r < 0 || r >= T.n_dtc) return false;
+    const double hour = fmin((frac + 0.0000001) * 24.0, 23.999999999999996);
+    const double lh = floor(hour);
+    const int h0 = (int)lh;
+    const double fraction = hour - lh;
+    double upper;
+    if (h0 == 23 && fraction > 0.0) {
+        if (r + 1 >= T.n_dtc) return false;
+        upper = (double)T.dtc[(size_t)(r + 1) * 24];
+    } else {
+        upper = (double)T.dtc[(size_t)r * 24 + (h0 + 1 < 23 ? h0 + 1 : 23)];
+    }
+    const double lower = (double)T.dtc[(size_t)r * 24 + h0];
+#ifdef __CUDA_ARCH__
+    const double v = trunc(__dadd_rn(__dadd_rn(lower, __dmul_rn(fraction, upper - lower)), 0.5));
+#else
+    const double v = trunc((lower + fraction * (upper - lower)) + 0.5);
+#endif
+    if (!(v >= -2147483648.0 && v <= 2147483647.0)) return false;
+    const double* a = T.solar + (size_t)(i - 1) * 8;
+    const double* m = T.solar + (size_t)(i - 2) * 8;
+    const double* y = T.solar + (size_t)(i - 5) * 8;
+    *d = Drivers{a[0], a[1], a[2], a[3], m[4], m[5], y[6], y[7], v};
+    return true;
+}
+
 // Fixed-node sweeps as functions of the exospheric temperature.  Above 105
 // km the lower Boole sweep (90 -> 105 km) always walks the same 16 intervals,
 // and above 500 km the middle sweep (105 -> 500 km) the same 63: their node

@@ -39,6 +39,7 @@ struct ForceParams {
     double omega;
     double mu_sun, mu_moon;
     jb::Drivers drivers;
+    jb::DriverTable dtab;  // space-weather tables (n_solar 0: the fixed drivers above)
     const jb::JbFit* fit;  // device copy of the fixed-node sweep fits, or null
     const jb::JbFit2* fit2;  // altitude-dependent sweep fits (stage-synchronous drag), or null
 };
@@ -167,7 +168,10 @@ struct Encke {
         const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
         const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
         const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, fp->drivers, fp->fit);
+        jb::Drivers dr = fp->drivers;
+        // rhs.rs:3560-3571: no drivers at this instant -> NaN density
+        if (fp->dtab.n_solar > 0 && !jb::lookup_drivers(fp->dtab, jd, &dr)) return NAN;
+        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->fit);
         if (!(rho > 0.0) || !isfinite(rho)) return NAN;
         if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         return rho;

@@ -286,9 +286,15 @@ __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs&
             const double dec = asin(fmin(1.0, fmax(-1.0, si[2] / sun_r)));
             const double ha = atan2(fma(pi[1], si[0], -(pi[0] * si[1])), fma(pi[0], si[0], pi[1] * si[1]));
             const double lat = asin(fmin(1.0, fmax(-1.0, pi[2] / sat_r)));
-            // fixed-node fits from constant memory (fp.fit holds the same numbers)
-            rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, fp.drivers, q, gmask,
-                                       fp.fit != nullptr, fp.fit2);
+            jb::Drivers dr = fp.drivers;
+            // fixed-node fits from constant memory (fp.fit holds the same numbers);
+            // no drivers at this instant -> NaN density (rhs.rs:3560-3571), the
+            // same verdict on every lane of the group
+            if (fp.dtab.n_solar > 0 && !jb::lookup_drivers(fp.dtab, P.jd[slot], &dr))
+                rho = NAN;
+            else
+                rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, dr, q, gmask,
+                                           fp.fit != nullptr, fp.fit2);
             if (!(rho > 0.0) || !isfinite(rho)) rho = NAN;
             else if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         }

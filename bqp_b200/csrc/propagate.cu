@@ -233,6 +233,27 @@ cudaError_t launch_gravity(const GravTable& T, int64_t n, const double* pos, dou
     return cudaSuccess;
 }
 
+// Space-weather drivers at n UTC Julian days, one per thread (the lookup the
+// force kernels make at every evaluation): out[9 i] = F10 .. Y81c, dTc.
+__global__ void k_jb_lookup(jb::DriverTable T, const double* __restrict__ jd, int64_t n, double* __restrict__ out,
+                            int32_t* __restrict__ ok) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    jb::Drivers d;
+    const bool found = jb::lookup_drivers(T, jd[i], &d);
+    const double v[9] = {d.f10, d.f10b, d.s10, d.s10b, d.m10, d.m10b, d.y10, d.y10b, d.dtc};
+    for (int k = 0; k < 9; ++k) out[9 * i + k] = found ? v[k] : NAN;
+    ok[i] = found ? 1 : 0;
+}
+
+cudaError_t launch_jb_lookup(const jb::DriverTable& T, const double* jd, int64_t n, double* out, int32_t* ok,
+                             cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    k_jb_lookup<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(T, jd, n, out, ok);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const ForceParams& fp, int64_t n,
                        const double* equ, const double* seg_t0, const double* jd0, const double* t,
                        const double* delta, const double* ballistic, double am0, double cd0,

@@ -157,6 +157,32 @@ int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches);
  * reference, whose quadrature these fits replace. */
 int bqp_jb_fit_check(const double* drivers, double* worst6);
 
+/* JB2008 space-weather tables: the SET SOLFSMY (daily F10, S10, M10, Y10 and
+ * their 81-day centred means) and DTCFILE (hourly dTc, K) texts.  Replaces
+ * Jb2008Drivers::from_set_bytes (jb_rs/src/drivers.rs:374-390, same checks,
+ * 1025-1240) together with the per-evaluation lookup of the JB2008 adapter
+ * (lightyear_odeint_rs/src/rhs.rs:3548-3571 calling drivers.rs:559-580):
+ * after this call the context's propagations take the drivers at each force
+ * evaluation's UTC instant from these tables (F10/S10 1 day lagged, M10 2,
+ * Y10 5; dTc interpolated hourly and rounded) instead of cfg.jb_drivers, and
+ * an instant the tables do not cover gives a NaN density, so the row ends
+ * with BQP_ST_NON_FINITE.  [jd_lo, jd_hi] is the UTC span the propagations
+ * will cover, which bounds the exospheric temperatures the drag sweep fits
+ * are built for (0, 0: the whole table).  NULL texts: back to
+ * cfg.jb_drivers.  BQP_E_ARG names the first rejected line. */
+int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_len, const char* dtcfile,
+                           int64_t dtcfile_len, double jd_lo, double jd_hi);
+/* The drivers the force kernels would use at n UTC Julian days, evaluated by
+ * the device lookup (Jb2008Drivers::lookup_utc_jd, drivers.rs:559-780):
+ * out[9 i] = F10, F81c, S10, S81c, M10, M81c, Y10, Y81c, dTc; ok[i] = 1, or 0
+ * with a NaN row where the tables do not cover the instant.  Host buffers. */
+int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out, int32_t* ok);
+/* The same parsing and lookup on the host, without a context or a device:
+ * counts2[0], counts2[1] = parsed SOLFSMY and DTCFILE rows, then n lookups as
+ * in bqp_ctx_jb_lookup (n may be 0).  BQP_E_ARG names a rejected line. */
+int bqp_jb_drivers_check(const char* solfsmy, int64_t solfsmy_len, const char* dtcfile, int64_t dtcfile_len,
+                         const double* utc_jd, int64_t n, double* out, int32_t* ok, int64_t* counts2);
+
 /* Replace the force/solver settings of a context (the field is kept; the
  * order may only shrink up to the parsed order). */
 int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg);

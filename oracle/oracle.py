@@ -62,6 +62,12 @@ def lib():
         L.orc_integrate_segment.restype = C.c_int
         L.orc_integrate_segment.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double,
                                             C.c_double, C.c_double, C.c_double, _dp, _lp]
+        L.orc_force_set_drivers.restype = C.c_int
+        L.orc_force_set_drivers.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
+        L.orc_jb_lookup.restype = C.c_int
+        L.orc_jb_lookup.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _ip]
+        L.orc_drivers_counts.restype = C.c_int
+        L.orc_drivers_counts.argtypes = [C.c_void_p, _lp]
         _lib = L
     return _lib
 
@@ -91,6 +97,31 @@ class Force:
         if getattr(self, "h", None):
             lib().orc_force_free(self.h)
             self.h = None
+
+    def set_drivers(self, solfsmy: str | None, dtcfile: str | None):
+        """Look the JB2008 drivers up per evaluation in these SOLFSMY / DTCFILE
+        texts (None, None: back to the fixed drivers); ValueError on a
+        rejected file."""
+        err = C.create_string_buffer(256)
+        rc = lib().orc_force_set_drivers(self.h, None if solfsmy is None else solfsmy.encode(),
+                                         None if dtcfile is None else dtcfile.encode(), err, 256)
+        if rc != 0:
+            raise ValueError(f"oracle: space-weather file rejected: {err.value.decode()}")
+
+    def jb_lookup(self, utc_jd):
+        """(drivers [n, 9] with NaN rows where the lookup fails, ok [n] bool)."""
+        jd = f64(np.atleast_1d(utc_jd))
+        out = np.zeros((jd.size, 9))
+        ok = np.zeros(jd.size, dtype=np.int32)
+        if lib().orc_jb_lookup(self.h, jd.size, _d(jd), _d(out), ok.ctypes.data_as(_ip)) != 0:
+            raise ValueError("oracle: no space-weather tables set")
+        return out, ok.astype(bool)
+
+    def driver_counts(self):
+        c = np.zeros(2, dtype=np.int64)
+        if lib().orc_drivers_counts(self.h, c.ctypes.data_as(_lp)) != 0:
+            raise ValueError("oracle: no space-weather tables set")
+        return int(c[0]), int(c[1])
 
     def dense(self):
         st = self.order + 2

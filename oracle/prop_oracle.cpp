@@ -30,6 +30,9 @@
 //                                          rectification 917-1177, final 1462-1570,
 //                                          checked final 3418-3560, sampled 2160-2416
 //   crates/jb_rs/src/jb2008.rs             JB2008 (Orekit 13.1.2 adaptation)
+//   crates/jb_rs/src/drivers.rs            SOLFSMY / DTCFILE parsing 1025-1186,
+//                                          row checks 1188-1240, lagged lookup
+//                                          and hourly dTc 631-780
 // The Sun/Moon positions come from the low-precision analytic series of
 // Montenbruck & Gill, "Satellite Orbits" (2000), section 3.3.2; the reference
 // reads tables instead, so this part follows the published series.
@@ -42,6 +45,10 @@
 #include <vector>
 #include <sstream>
 #include <algorithm>
+#include <array>
+#include <cerrno>
+#include <climits>
+#include <memory>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -848,6 +855,167 @@ double geodetic_altitude_km(double x, double y, double z, double a) {
 }
 
 // ------------------------------------------------------------- force model
+// ------------------------------------------------------ JB2008 space weather
+// Daily SOLFSMY rows (F10, F81c, S10, S81c, M10, M81c, Y10, Y81c) and hourly
+// DTCFILE dTc values, as jb_rs/src/drivers.rs reads them.
+struct DriverTable {
+    std::vector<std::array<double, 8>> solar;
+    std::vector<double> solar_jd;      // integer JD of each solar row
+    std::vector<int64_t> solar_ord;    // proleptic Gregorian day ordinal
+    std::vector<std::array<int32_t, 24>> dtc;
+    std::vector<int64_t> dtc_ord;
+};
+
+namespace drv {
+
+bool leap(int y) { return y % 4 == 0 && (y % 100 != 0 || y % 400 == 0); }
+
+// drivers.rs:1140-1170: ordinal = days since 0001-01-01 (proleptic Gregorian)
+bool date_ordinal(const std::string& ys, const std::string& ds, int64_t* ord) {
+    char* e = nullptr;
+    const long y = std::strtol(ys.c_str(), &e, 10);
+    if (*e || ys.empty()) return false;
+    const long d = std::strtol(ds.c_str(), &e, 10);
+    if (*e || ds.empty()) return false;
+    if (y < 1 || d < 1 || d > (leap((int)y) ? 366 : 365)) return false;
+    const int64_t c = y - 1;
+    *ord = c * 365 + c / 4 - c / 100 + c / 400 + (d - 1);
+    return true;
+}
+
+bool finite_number(const std::string& s, double* v) {
+    char* e = nullptr;
+    *v = std::strtod(s.c_str(), &e);
+    return !s.empty() && *e == 0 && std::isfinite(*v);
+}
+
+std::vector<std::string> fields_of(const std::string& line) {
+    std::vector<std::string> f;
+    std::istringstream is(line);
+    std::string w;
+    while (is >> w) f.push_back(w);
+    return f;
+}
+
+std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+// drivers.rs:1025-1087 and 1188-1222
+bool parse_solfsmy(const std::string& text, DriverTable& T, std::string* err) {
+    std::istringstream in(text);
+    std::string raw;
+    bool header = false;
+    while (std::getline(in, raw)) {
+        const std::string line = trim(raw);
+        if (line.empty()) continue;
+        if (line[0] == '#') {
+            if (!header) {
+                header = true;
+                if (line.rfind("# F10, S10, M10, Y10 data release", 0) != 0) return *err = "SOLFSMY header", false;
+            }
+            continue;
+        }
+        const auto f = fields_of(line);
+        if (f.size() != 12) return *err = "SOLFSMY field count", false;
+        int64_t ord;
+        if (!date_ordinal(f[0], f[1], &ord)) return *err = "SOLFSMY date", false;
+        double jd;
+        if (!finite_number(f[2], &jd) || jd != std::floor(jd)) return *err = "SOLFSMY Julian day", false;
+        std::array<double, 8> v;
+        for (int i = 0; i < 8; ++i)
+            if (!finite_number(f[3 + i], &v[i])) return *err = "SOLFSMY value", false;
+        if (jd != (double)(ord + 1721426)) return *err = "SOLFSMY date and Julian day disagree", false;
+        if (!T.solar.empty() && (jd != T.solar_jd.back() + 1.0 || ord != T.solar_ord.back() + 1))
+            return *err = "SOLFSMY rows missing, duplicated or out of order", false;
+        T.solar.push_back(v);
+        T.solar_jd.push_back(jd);
+        T.solar_ord.push_back(ord);
+    }
+    if (!header) return *err = "SOLFSMY header missing", false;
+    if (T.solar.empty()) return *err = "SOLFSMY has no rows", false;
+    return true;
+}
+
+// drivers.rs:1103-1138 and 1224-1240
+bool parse_dtcfile(const std::string& text, DriverTable& T, std::string* err) {
+    std::istringstream in(text);
+    std::string raw;
+    while (std::getline(in, raw)) {
+        const std::string line = trim(raw);
+        if (line.empty() || line[0] == '#') continue;
+        const auto f = fields_of(line);
+        if (f.size() != 27 || f[0] != "DTC") return *err = "DTCFILE field count", false;
+        int64_t ord;
+        if (!date_ordinal(f[1], f[2], &ord)) return *err = "DTCFILE date", false;
+        std::array<int32_t, 24> v;
+        for (int h = 0; h < 24; ++h) {
+            char* e = nullptr;
+            errno = 0;
+            const long long x = std::strtoll(f[3 + h].c_str(), &e, 10);
+            if (*e || errno || x < INT32_MIN || x > INT32_MAX) return *err = "DTCFILE value", false;
+            v[h] = (int32_t)x;
+        }
+        if (!T.dtc.empty() && ord != T.dtc_ord.back() + 1)
+            return *err = "DTCFILE rows missing, duplicated or out of order", false;
+        T.dtc.push_back(v);
+        T.dtc_ord.push_back(ord);
+    }
+    if (T.dtc.empty()) return *err = "DTCFILE has no rows", false;
+    // drivers.rs:392-410: both ends of the DTC coverage are SOLFSMY dates
+    for (int64_t o : {T.dtc_ord.front(), T.dtc_ord.back()})
+        if (o < T.solar_ord.front() || o > T.solar_ord.back())
+            return *err = "DTCFILE coverage outside SOLFSMY", false;
+    return true;
+}
+
+// drivers.rs:559-580, 631-780: drivers at a UTC Julian day given as MJD + 2400000.5
+bool lookup(const DriverTable& T, double jd_in, double out[9]) {
+    if (!std::isfinite(jd_in)) return false;
+    const double jd = (jd_in - 2400000.5) + 2400000.5;  // the JD -> MJD -> JD round trip
+    const double day_jd = std::floor(jd + 0.5);
+    const double off = day_jd - T.solar_jd.front();
+    if (!(off >= 0.0 && off < (double)T.solar.size())) return false;
+    const size_t i = (size_t)off;
+    if (T.solar_jd[i] != day_jd) return false;
+    if (i < 5) return false;  // F10/S10 lag 1 d, M10 2 d, Y10 5 d
+    const double frac = jd - (day_jd - 0.5);
+    if (!(frac >= 0.0 && frac < 1.0)) return false;
+    const int64_t r = T.solar_ord[i] - T.dtc_ord.front();
+    if (r < 0 || r >= (int64_t)T.dtc.size()) return false;
+    const double hour = std::min((frac + 0.0000001) * 24.0, 23.999999999999996);
+    const double lh = std::floor(hour);
+    if (!(lh >= 0.0 && lh < 24.0)) return false;
+    const int lower_hour = (int)lh;
+    const double fraction = hour - lh;
+    double upper;
+    if (lower_hour == 23 && fraction > 0.0) {
+        if (r + 1 >= (int64_t)T.dtc.size() || T.dtc_ord[r + 1] != T.solar_ord[i] + 1) return false;
+        upper = (double)T.dtc[r + 1][0];
+    } else {
+        upper = (double)T.dtc[r][std::min(lower_hour + 1, 23)];
+    }
+    const double lower = (double)T.dtc[r][lower_hour];
+    const double v = std::trunc((lower + fraction * (upper - lower)) + 0.5);
+    if (!(v >= (double)INT32_MIN && v <= (double)INT32_MAX)) return false;
+    const auto& a = T.solar[i - 1];
+    const auto& m = T.solar[i - 2];
+    const auto& y = T.solar[i - 5];
+    out[0] = a[0];
+    out[1] = a[1];
+    out[2] = a[2];
+    out[3] = a[3];
+    out[4] = m[4];
+    out[5] = m[5];
+    out[6] = y[6];
+    out[7] = y[7];
+    out[8] = v;
+    return true;
+}
+
+}  // namespace drv
+
 struct Force {
     Field field;
     int use_gravity = 1;   // spherical harmonics on (order > 0)
@@ -857,6 +1025,7 @@ struct Force {
     double omega = EARTH_OMEGA;
     double mu_sun = 1.32712440018e11, mu_moon = 4902.800066;
     double drivers[9] = {150, 150, 150, 150, 150, 150, 150, 150, 0};  // f10..y10b, dTc
+    std::shared_ptr<DriverTable> table;  // when set: drivers looked up per evaluation
 };
 
 // rhs.rs:3551-3776 with rhs.rs:1119-1163; density -> drag acceleration.
@@ -874,7 +1043,12 @@ double density_at(const Force& F, const double pos_itrs[3], const double sun_itr
                        std::fma(pos_itrs[0], sun_itrs[0], pos_itrs[1] * sun_itrs[1]));
     in[3] = std::asin(std::min(1.0, std::max(-1.0, pos_itrs[2] / sat_r)));
     in[4] = alt_m;
-    for (int i = 0; i < 9; ++i) in[5 + i] = F.drivers[i];
+    if (F.table) {
+        // rhs.rs:3560-3571: no drivers at this instant -> NaN density
+        if (!drv::lookup(*F.table, jd, in + 5)) return NAN;
+    } else {
+        for (int i = 0; i < 9; ++i) in[5 + i] = F.drivers[i];
+    }
     double rho = jb::density(in);
     if (!(rho > 0.0) || !std::isfinite(rho)) return NAN;
     if (alt_m > CEIL_M) rho = std::min(rho, CEIL_RHO);
@@ -1594,6 +1768,45 @@ void* orc_force_new(const char* coeff_text, const double* cfg) {
 }
 
 void orc_force_free(void* f) { delete (Force*)f; }
+
+// Space-weather tables for the JB2008 drivers (null texts: back to the fixed
+// drivers).  Returns 0, or -1 with the reason in err.
+int orc_force_set_drivers(void* f, const char* solfsmy, const char* dtcfile, char* err, int errlen) {
+    Force* F = (Force*)f;
+    if (!solfsmy || !dtcfile) {
+        F->table.reset();
+        return 0;
+    }
+    auto T = std::make_shared<DriverTable>();
+    std::string e;
+    if (!drv::parse_solfsmy(solfsmy, *T, &e) || !drv::parse_dtcfile(dtcfile, *T, &e)) {
+        if (err && errlen > 0) std::snprintf(err, (size_t)errlen, "%s", e.c_str());
+        return -1;
+    }
+    F->table = T;
+    return 0;
+}
+
+// Drivers at n UTC Julian days: out[9 * i] = f10 .. y10b, dTc; ok[i] = 1 or 0.
+int orc_jb_lookup(void* f, long n, const double* jd, double* out, int* ok) {
+    Force* F = (Force*)f;
+    if (!F->table) return -1;
+    for (long i = 0; i < n; ++i) {
+        ok[i] = drv::lookup(*F->table, jd[i], out + 9 * i) ? 1 : 0;
+        if (!ok[i])
+            for (int k = 0; k < 9; ++k) out[9 * i + k] = NAN;
+    }
+    return 0;
+}
+
+// Parsed row counts of the current tables: counts[0] SOLFSMY, counts[1] DTCFILE.
+int orc_drivers_counts(void* f, long* counts) {
+    Force* F = (Force*)f;
+    if (!F->table) return -1;
+    counts[0] = (long)F->table->solar.size();
+    counts[1] = (long)F->table->dtc.size();
+    return 0;
+}
 
 int orc_field_dense(void* f, double* c, double* s) {
     Force* F = (Force*)f;
