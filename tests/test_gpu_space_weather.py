@@ -20,17 +20,28 @@ ENGINES = ["pipeline", "persistent"]
 
 def tables(first_jdn, days, seed=0):
     """SOLFSMY / DTCFILE texts for `days` consecutive days from Julian day
-    number first_jdn, indices U[70, 250] sfu and hourly dTc U[-30, 300] K."""
+    number first_jdn.  The indices follow one activity level (a 27-day
+    rotation around 150 sfu plus daily noise) with the 81-day means on its
+    smooth part, as real files do; the model's semiannual term takes
+    F81c - 0.70 S81c - 0.04 M81c, and independent random indices would drive
+    it far outside the range the model is made for.  dTc follows a diurnal
+    wave plus noise."""
     rng = np.random.default_rng(seed)
     sol = ["# F10, S10, M10, Y10 data release synthetic", "# YYYY DDD JulianDay F10 F81c S10 S81c M10 M81c Y10 Y81c Ssrc"]
     dtc = []
+    phase = rng.uniform(0, 2 * np.pi)
     for k in range(days):
         jdn = first_jdn + k
         d = datetime.date.fromordinal(jdn - 1721425)
         doy = d.timetuple().tm_yday
-        vals = " ".join(f"{v:.1f}" for v in rng.uniform(70.0, 250.0, 8))
-        sol.append(f"{d.year} {doy} {jdn} {vals} TEST")
-        dtc.append(f"DTC {d.year} {doy} " + " ".join(str(int(v)) for v in rng.integers(-30, 300, 24)))
+        mean = 150.0 + 10.0 * np.sin(2 * np.pi * k / 81.0 + phase)
+        level = mean + 50.0 * np.sin(2 * np.pi * k / 27.0 + phase) + rng.normal(0.0, 5.0)
+        daily = [level * f + rng.normal(0.0, 3.0) for f in (1.0, 0.95, 1.05, 1.0)]  # F10, S10, M10, Y10
+        means = [mean * f for f in (1.0, 0.95, 1.05, 1.0)]
+        vals = [daily[0], means[0], daily[1], means[1], daily[2], means[2], daily[3], means[3]]
+        sol.append(f"{d.year} {doy} {jdn} " + " ".join(f"{v:.1f}" for v in vals) + " TEST")
+        hours = 40.0 + 60.0 * np.sin(2 * np.pi * (np.arange(24) / 24.0 + k / 7.0)) + rng.normal(0.0, 10.0, 24)
+        dtc.append(f"DTC {d.year} {doy} " + " ".join(str(int(round(v))) for v in hours))
     return "\n".join(sol) + "\n", "\n".join(dtc) + "\n"
 
 
@@ -75,7 +86,11 @@ def test_device_lookup_matches_oracle():
 
 @pytest.mark.parametrize("engine", ENGINES)
 def test_propagation_with_tables_matches_oracle(engine):
-    """Day-long arcs crossing day and hour boundaries of the tables."""
+    """Two-hour arcs from 23:00 UTC: the drivers jump at midnight and dTc
+    bends at every hour.  The jump is a discontinuity in the force that the
+    embedded error estimate does not see, so the oracle's own error there can
+    exceed steps * eps * 10; the device solution must be as close to a 1e-13
+    km solution as the oracle's is (or within that floor)."""
     order = 20
     text = workloads.synthetic_field(order)
     sol, dtc = tables(2460300, 24, seed=3)
@@ -83,22 +98,28 @@ def test_propagation_with_tables_matches_oracle(engine):
     states = workloads.leo_states(n, seed=41)
     bal = workloads.leo_ballistics(n, seed=41)
     equ, _ = N.eci_to_equinoctial(states)
-    tf = 86400.0
+    epoch = EPOCH - 1.0 / 24.0
+    tf = 7200.0
     eps = 1e-10
     ctx = ctx_for(text, order, sol, dtc, engine, eps)
-    got, st, steps, _ = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    got, st, steps, _ = ctx.propagate_final(states, epoch, tf, ballistic=bal)
     F = oracle_force(text, order, sol, dtc)
-    ref_d, ref_st, ref_steps, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, EPOCH, tf, bal)
-    assert (st == 0).all() and (ref_st == 0).all()
-    ref = np.array([O.equinoc2eci(equ[i], tf)[0] + ref_d[i] for i in range(n)])
-    err = np.linalg.norm(got[:, :3] - ref[:, :3], axis=1)
-    # each solution within ~steps * eps * 10 of the exact one; they differ by at most twice that
-    assert np.all(err <= 2 * np.maximum(steps, 1) * eps * 10), err
+    assert (st == 0).all()
+
+    def positions(tol):
+        d, s, _, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=tol), equ, epoch, tf, bal)
+        assert (s == 0).all()
+        return np.array([O.equinoc2eci(equ[i], tf)[0][:3] + d[i][:3] for i in range(n)])
+
+    ref, truth = positions(eps), positions(1e-13)
+    err = np.linalg.norm(got[:, :3] - truth, axis=1)
+    err_oracle = np.linalg.norm(ref - truth, axis=1)
+    assert np.all(err <= 3 * np.maximum(err_oracle, np.maximum(steps, 1) * eps * 10)), (err, err_oracle)
     # the tables are in effect: the fixed drivers give a different trajectory
-    fixed, st2, _, _ = ctx_for(text, order, None, None, engine, eps).propagate_final(states, EPOCH, tf, ballistic=bal)
+    fixed, st2, _, _ = ctx_for(text, order, None, None, engine, eps).propagate_final(states, epoch, tf, ballistic=bal)
     assert (st2 == 0).all()
     moved = np.linalg.norm(fixed[:, :3] - got[:, :3], axis=1)
-    assert np.median(moved) > 100 * np.median(err) and moved.max() > 1e-3
+    assert np.median(moved) > 100 * np.median(err) and moved.max() > 1e-2
 
 
 @pytest.mark.parametrize("engine", ENGINES)
