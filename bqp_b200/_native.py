@@ -79,6 +79,9 @@ SIGNATURES = [
     ("bqp_ctx_set_jb_drivers", C.c_int, [_vp, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_double,
                                          C.c_double]),
     ("bqp_ctx_jb_lookup", C.c_int, [_vp, _dp, C.c_int64, _dp, _ip]),
+    ("bqp_ctx_set_ephemeris", C.c_int, [_vp, C.c_int32, C.c_char_p, C.c_int64]),
+    ("bqp_ctx_body_positions", C.c_int, [_vp, C.c_int32, _dp, C.c_int64, _dp]),
+    ("bqp_ephemeris_check", C.c_int, [C.c_int32, C.c_char_p, C.c_int64, _dp, C.c_int64, _dp, _lp]),
     ("bqp_jb_drivers_check", C.c_int, [C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, _dp, C.c_int64, _dp, _ip,
                                        _lp]),
     ("bqp_ctx_profile", C.c_int, [_vp, C.c_int32]),
@@ -233,6 +236,27 @@ class Context:
         if rc == E_ARG:
             raise ValueError(last_error())
         check(rc)
+
+    def set_ephemeris(self, body: str, catalogue):
+        """Take the Sun's or the Moon's position from a precomputed "DUST"
+        catalogue (bytes or a path; None: back to the analytic series).
+        ValueError names what the loader rejected."""
+        b = BODIES[body]
+        if catalogue is None:
+            check(lib().bqp_ctx_set_ephemeris(self._h, b, None, 0))
+            return
+        data = _file_bytes(catalogue)
+        rc = lib().bqp_ctx_set_ephemeris(self._h, b, data, len(data))
+        if rc == E_ARG:
+            raise ValueError(last_error())
+        check(rc)
+
+    def body_positions(self, body: str, utc_jd):
+        """[n, 3] km: the body's positions as the force kernels take them."""
+        jd = f64(np.atleast_1d(utc_jd))
+        out = np.empty((jd.size, 3))
+        check(lib().bqp_ctx_body_positions(self._h, BODIES[body], dptr(jd), jd.size, dptr(out)))
+        return out
 
     def jb_lookup(self, utc_jd):
         """(drivers [n, 9]: F10, F81c, S10, S81c, M10, M81c, Y10, Y81c, dTc,
@@ -410,6 +434,30 @@ def sigma_weights(sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0):
                                   dptr(off)))
     p = pts.value
     return p, wm[:p].copy(), wc[:p].copy(), off
+
+
+BODIES = {"sun": 0, "moon": 1}
+
+
+def _file_bytes(x) -> bytes:
+    """Binary file contents from bytes or a path."""
+    if isinstance(x, (bytes, bytearray, memoryview)):
+        return bytes(x)
+    return open(x, "rb").read()
+
+
+def ephemeris_check(body: str, catalogue, utc_jd=()):
+    """Host-only parse of a "DUST" catalogue and positions at utc_jd:
+    (sample count, positions [n, 3] km).  ValueError names what was rejected."""
+    data = _file_bytes(catalogue)
+    jd = f64(np.atleast_1d(np.asarray(utc_jd, dtype=np.float64)))
+    out = np.empty((jd.size, 3))
+    n = np.zeros(1, dtype=np.int64)
+    rc = lib().bqp_ephemeris_check(BODIES[body], data, len(data), dptr(jd), jd.size, dptr(out), lptr(n))
+    if rc == E_ARG:
+        raise ValueError(last_error())
+    check(rc)
+    return int(n[0]), out
 
 
 def _text_bytes(x) -> bytes:

@@ -141,20 +141,46 @@ def _space_weather(space_weather):
     return N._text_bytes(space_weather[0]), N._text_bytes(space_weather[1]), span
 
 
-def context(text: str, cfg: N.ForceConfig, space_weather=None) -> N.Context:
+def _ephemeris(ephemeris):
+    """{"sun": bytes, "moon": bytes} of ephemeris = (sun, moon) (either may be
+    None) or a dict with those keys; each catalogue as bytes or a path."""
+    if ephemeris is None:
+        return {}
+    if isinstance(ephemeris, dict):
+        items = ephemeris.items()
+    elif isinstance(ephemeris, (tuple, list)) and len(ephemeris) == 2:
+        items = zip(("sun", "moon"), ephemeris)
+    else:
+        raise ValueError("ephemeris must be (sun, moon) or {'sun': ..., 'moon': ...}")
+    out = {}
+    for body, cat in items:
+        if body not in N.BODIES:
+            raise ValueError(f"unknown ephemeris body {body!r}")
+        if cat is not None:
+            out[body] = N._file_bytes(cat)
+    return out
+
+
+def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None) -> N.Context:
     """A cached native context for (field text, configuration, space-weather
-    files).  With space_weather the JB2008 drivers come from the SET SOLFSMY
-    / DTCFILE tables at each evaluation's UTC instant (the reference's
-    compiled driver catalogue, jb_rs/src/drivers.rs) instead of the fixed
-    configured drivers."""
+    files, ephemeris catalogues).  With space_weather the JB2008 drivers come
+    from the SET SOLFSMY / DTCFILE tables at each evaluation's UTC instant (the
+    reference's compiled driver catalogue, jb_rs/src/drivers.rs) instead of
+    the fixed configured drivers; with ephemeris the Sun and / or Moon come
+    from precomputed "DUST" catalogues (the reference's precomputed_ephem.rs)
+    instead of the analytic series."""
     sw = _space_weather(space_weather)
+    eph = _ephemeris(ephemeris)
     sw_key = None if sw is None else (hashlib.sha256(sw[0]).hexdigest(), hashlib.sha256(sw[1]).hexdigest(), sw[2])
-    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg), sw_key)
+    eph_key = tuple(sorted((b, hashlib.sha256(d).hexdigest()) for b, d in eph.items()))
+    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg), sw_key, eph_key)
     ctx = _CTX.get(key)
     if ctx is None:
         ctx = N.Context(text, cfg)
         if sw is not None:
             ctx.set_jb_drivers(sw[0], sw[1], sw[2])
+        for body, data in eph.items():
+            ctx.set_ephemeris(body, data)
         _CTX[key] = ctx
         while len(_CTX) > _CTX_MAX:
             _CTX.popitem(last=False)[1].close()
@@ -173,11 +199,12 @@ def _equinoctial_of(eci, what):
 # ------------------------------------------------------------------ scalar API
 def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
               moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-              gravity_field=None, space_weather=None):
+              gravity_field=None, space_weather=None, ephemeris=None):
     """Propagate one ECI state; sampled, rectified path (lib.rs:237-353).
 
     space_weather = (solfsmy, dtcfile[, (jd_lo, jd_hi)]): JB2008 drivers from
-    SET space-weather files (see ``context``); default the fixed drivers."""
+    SET space-weather files; ephemeris = (sun, moon): precomputed catalogues
+    (see ``context``); defaults: the fixed drivers and the analytic series."""
     init = _six(state_eci, "state_eci")
     if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
         raise ValueError("epoch_jd must be finite and tof_s > 0")
@@ -201,7 +228,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg, space_weather)
+    ctx = context(text, cfg, space_weather, ephemeris)
     t_start = time.perf_counter()
     out, st, steps, evals = ctx.propagate_sampled(init, epoch_jd, tof_s, np.array(grid))
     wall_us = int((time.perf_counter() - t_start) * 1e6)
@@ -228,7 +255,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
 
 def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, srp=True, sun=True, moon=True,
                     atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-                    gravity_field=None, space_weather=None):
+                    gravity_field=None, space_weather=None, ephemeris=None):
     """Final state with the ground check enforced (lib.rs:361-438).
 
     Raises ValueError for a physically infeasible arc (ground impact, a radius
@@ -240,7 +267,7 @@ def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, s
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded, ground_check=True)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg, space_weather)
+    ctx = context(text, cfg, space_weather, ephemeris)
     out, st, _, _ = ctx.propagate_final(init, epoch_jd, tof_s)
     status = int(st[0])
     if status == N.ST_GROUND:
@@ -277,22 +304,22 @@ def _batch_cfg(model: dict, embedded: bool):
 
 
 def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctial=False, gravity_field=None,
-                          space_weather=None, **model):
+                          space_weather=None, ephemeris=None, **model):
     """Final states of a batch with per-row epoch / duration / ballistics.
 
     The reference's LightyearSession::integrate_variable_final_into
     (session.rs:2325-2430).  Returns (states_eci [n,6], status [n], steps [n],
     rhs_evals [n]); failed rows are NaN."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded), space_weather)
+    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris)
     return ctx.propagate_final(states, epoch_jd, tof_s, ballistic=ballistic, equinoctial=equinoctial)
 
 
 def propagate_batch_sampled(states, epoch_jd, tof_s, t_eval, *, deltas=False, equinoctial=False,
-                            gravity_field=None, space_weather=None, **model):
+                            gravity_field=None, space_weather=None, ephemeris=None, **model):
     """Samples of a batch on one grid; the reference's
     integrate_batch_native_into (batch.rs:247-391) with ``deltas=True``
     (Encke deviations from the initial baseline) or ECI states."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded), space_weather)
+    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris)
     return ctx.propagate_sampled(states, epoch_jd, tof_s, t_eval, deltas=deltas, equinoctial=equinoctial)

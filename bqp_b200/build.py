@@ -17,9 +17,10 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbqp_b200.so"
-SOURCES = ["propagate.cu", "pipeline.cu", "sigma.cu", "mlp.cu", "surrogate.cu", "space_weather.cu", "bqp_api.cu"]
+SOURCES = ["propagate.cu", "pipeline.cu", "sigma.cu", "mlp.cu", "surrogate.cu", "space_weather.cu", "ephemeris.cu",
+           "bqp_api.cu"]
 HEADERS = ["kernels.cuh", "gravity.cuh", "jb2008.cuh", "physics.cuh", "launch.h", "rk_tableaus.h", "traj.cuh",
-           "space_weather.h"]
+           "space_weather.h", "ephemeris.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

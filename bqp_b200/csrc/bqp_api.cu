@@ -20,6 +20,7 @@
 
 #include "../../include/bqp_prop.h"
 #include "launch.h"
+#include "ephemeris.h"
 #include "space_weather.h"
 #include "surrogate.h"
 
@@ -510,6 +511,8 @@ struct bqp_ctx {
     double* d_sw_solar = nullptr;
     int32_t* d_sw_dtc = nullptr;
     jb::DriverTable dtab{};       // the device copy as the kernels see it (n_solar 0: none)
+    double* d_eph[2] = {nullptr, nullptr};  // Sun / Moon catalogues (bqp_ctx_set_ephemeris)
+    EphemTable eph[2] = {};                 // their device views (n 0: the analytic series)
     bool profile = false;  // kernel timing on (bqp_ctx_profile)
     KernelTimes times{};
     Model* sur = nullptr;          // learned gravity surrogate (bqp_surrogate_*)
@@ -584,6 +587,8 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.drivers = {c.jb_drivers[0], c.jb_drivers[1], c.jb_drivers[2], c.jb_drivers[3], c.jb_drivers[4],
                   c.jb_drivers[5], c.jb_drivers[6], c.jb_drivers[7], c.jb_drivers[8]};
     fp.dtab = ctx->dtab;
+    fp.eph_sun = ctx->eph[0];
+    fp.eph_moon = ctx->eph[1];
     fp.fit = (c.drag_quadrature || !fp.drag) ? nullptr : ctx->d_fit;
     fp.fit2 = fp.fit ? ctx->d_fit2 : nullptr;
     return fp;
@@ -1059,6 +1064,8 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_tab_low) cudaFree(ctx->d_tab_low);
     if (ctx->d_sw_solar) cudaFree(ctx->d_sw_solar);
     if (ctx->d_sw_dtc) cudaFree(ctx->d_sw_dtc);
+    for (double* p : ctx->d_eph)
+        if (p) cudaFree(p);
     delete ctx->sur;
     delete ctx;
     return 0;
@@ -1161,6 +1168,65 @@ int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out
     cudaFree(d_out);
     cudaFree(d_ok);
     if (e != cudaSuccess) return cuda_fail(e, "space-weather lookup");
+    return 0;
+}
+
+int bqp_ctx_set_ephemeris(bqp_ctx* ctx, int32_t body, const uint8_t* bytes, int64_t len) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (body != BQP_BODY_SUN && body != BQP_BODY_MOON) return fail(BQP_E_ARG, "body must be 0 (Sun) or 1 (Moon)");
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    Ephemeris e;
+    if (bytes) {
+        const std::string why = parse_ephemeris(bytes, len, body, &e);
+        if (!why.empty()) return fail(BQP_E_ARG, "ephemeris catalogue rejected: %s", why.c_str());
+    }
+    if (ctx->d_eph[body]) cudaFree(ctx->d_eph[body]);
+    ctx->d_eph[body] = nullptr;
+    ctx->eph[body] = EphemTable{};
+    if (!bytes) return 0;
+    cudaError_t err = cudaMalloc(&ctx->d_eph[body], e.pos.size() * sizeof(double));
+    if (err == cudaSuccess)
+        err = cudaMemcpy(ctx->d_eph[body], e.pos.data(), e.pos.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        if (ctx->d_eph[body]) cudaFree(ctx->d_eph[body]);
+        ctx->d_eph[body] = nullptr;
+        return cuda_fail(err, "ephemeris catalogue upload");
+    }
+    ctx->eph[body] = e.host_view();
+    ctx->eph[body].pos = ctx->d_eph[body];
+    return 0;
+}
+
+int bqp_ctx_body_positions(bqp_ctx* ctx, int32_t body, const double* utc_jd, int64_t n, double* out) {
+    if (!ctx || (n > 0 && (!utc_jd || !out))) return fail(BQP_E_ARG, "null argument");
+    if (body != BQP_BODY_SUN && body != BQP_BODY_MOON) return fail(BQP_E_ARG, "body must be 0 (Sun) or 1 (Moon)");
+    if (n <= 0) return 0;
+    cudaSetDevice(ctx->device);
+    double *d_jd = nullptr, *d_out = nullptr;
+    cudaError_t e = cudaMalloc(&d_jd, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, n * 3 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_jd, utc_jd, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_body_positions(ctx->eph[body], body, d_jd, n, d_out, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_jd);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return cuda_fail(e, "body positions");
+    return 0;
+}
+
+int bqp_ephemeris_check(int32_t body, const uint8_t* bytes, int64_t len, const double* utc_jd, int64_t n,
+                        double* out, int64_t* n_samples) {
+    if (!n_samples || (n > 0 && (!utc_jd || !out))) return fail(BQP_E_ARG, "null argument");
+    if (body != BQP_BODY_SUN && body != BQP_BODY_MOON) return fail(BQP_E_ARG, "body must be 0 (Sun) or 1 (Moon)");
+    Ephemeris e;
+    const std::string why = parse_ephemeris(bytes, len, body, &e);
+    if (!why.empty()) return fail(BQP_E_ARG, "ephemeris catalogue rejected: %s", why.c_str());
+    *n_samples = e.n;
+    const EphemTable T = e.host_view();
+    for (int64_t i = 0; i < n; ++i) ephem_position(T, utc_jd[i], out + 3 * i);
     return 0;
 }
 

@@ -40,6 +40,7 @@ struct ForceParams {
     double mu_sun, mu_moon;
     jb::Drivers drivers;
     jb::DriverTable dtab;  // space-weather tables (n_solar 0: the fixed drivers above)
+    EphemTable eph_sun, eph_moon;  // precomputed catalogues (n 0: the analytic series)
     const jb::JbFit* fit;  // device copy of the fixed-node sweep fits, or null
     const jb::JbFit2* fit2;  // altitude-dependent sweep fits (stage-synchronous drag), or null
 };
@@ -115,7 +116,7 @@ struct Encke {
         double sun[3];
         bool have_sun = false;
         if (fp->drag && cd != 0.0 && am != 0.0) {
-            sun_position(jd, sun);
+            sun_at(fp->eph_sun, jd, sun);
             have_sun = true;
             double rho = density_at(pi, sun, s, c, jd);
             if (isnan(rho)) {
@@ -136,12 +137,12 @@ struct Encke {
             }
         }
         if (fp->sun) {
-            if (!have_sun) sun_position(jd, sun);
+            if (!have_sun) sun_at(fp->eph_sun, jd, sun);
             third_body(sp, sun, fp->mu_sun, acc);
         }
         if (fp->moon) {
             double moon[3];
-            moon_position(jd, moon);
+            moon_at(fp->eph_moon, jd, moon);
             third_body(sp, moon, fp->mu_moon, acc);
         }
         battin(rs, d, r2, r, acc);

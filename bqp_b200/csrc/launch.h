@@ -98,6 +98,8 @@ cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const Force
 cudaError_t launch_propagate(const PropArgs& A, int method, int threads, int blocks, cudaStream_t st);
 cudaError_t launch_jb_lookup(const jb::DriverTable& T, const double* jd, int64_t n, double* out, int32_t* ok,
                              cudaStream_t st);
+cudaError_t launch_body_positions(const EphemTable& E, int body, const double* jd, int64_t n, double* out,
+                                  cudaStream_t st);
 cudaError_t launch_sigma_gen(int64_t n, int set, double scale, const double* offsets, const double* mean,
                              const double* cov, const double* epoch, const double* tf, const double* ballistic,
                              double* rows, double* row_epoch, double* row_tf, double* row_bal, int32_t* status,

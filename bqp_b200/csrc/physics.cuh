@@ -213,8 +213,9 @@ BQP_HD bool equinoctial_to_eci(const double* e, double tof, double* out) {
 // ---------------------------------------------------------------- ephemeris
 // Low-precision analytic Sun and Moon positions (Montenbruck & Gill,
 // "Satellite Orbits", 2000, section 3.3.2), J2000 equator/equinox, km.  The
-// reference reads precomputed tables (precomputed_ephem.rs); these series
-// stand in for them with the same force formula downstream.
+// reference reads precomputed catalogues (precomputed_ephem.rs); with a
+// catalogue set (EphemTable below) the kernels read it the same way, and
+// these series stand in for it otherwise.
 constexpr double kDeg = kPi / 180.0;
 constexpr double kArcsec = kDeg / 3600.0;
 constexpr double kObliquity = 23.43929111 * kDeg;
@@ -298,6 +299,72 @@ BQP_HD void moon_position(double jd, double* out) {
 }
 
 // Point-mass third body in the normalised form of rhs.rs:1326-1354.
+// Precomputed Sun / Moon catalogue as the kernels read it: samples of
+// Earth-centred ICRS positions (km) every dt days from jd_start (UTC Julian
+// days).  n == 0: no catalogue, the analytic series apply.
+struct EphemTable {
+    const double* pos;  // [n][3]
+    double jd_start, jd_end, dt, inv_dt;  // jd_end = jd_start + (n - 1) dt, inv_dt = 1 / dt
+    int64_t n;
+};
+
+// a (1 - f) + b f, as the reference rounds it (no contraction on the device)
+BQP_HD double eph_lerp(double a, double b, double f) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(__dmul_rn(a, __dsub_rn(1.0, f)), __dmul_rn(b, f));
+#else
+    return a * (1.0 - f) + b * f;
+#endif
+}
+
+BQP_HD void eph_interp(const EphemTable& E, int64_t i, double f, double* out) {
+    for (int k = 0; k < 3; ++k) out[k] = eph_lerp(E.pos[3 * i + k], E.pos[3 * (i + 1) + k], f);
+}
+
+BQP_HD void eph_sample(const EphemTable& E, int64_t i, double* out) {
+    for (int k = 0; k < 3; ++k) out[k] = E.pos[3 * i + k];
+}
+
+// Position at a UTC Julian day (precomputed_ephem.rs:1092-1131 linear
+// interpolation on the grid; outside it, only JD roundoff of 2 eps at an end
+// is clamped, rhs.rs:2996-3018); NaN otherwise.
+BQP_HD void ephem_position(const EphemTable& E, double jd, double* out) {
+    constexpr double kEps = 2.220446049250313e-16;
+    if (isfinite(jd)) {
+        if (E.n == 1) {
+            if (fabs(jd - E.jd_start) <= kEps) return eph_sample(E, 0, out);
+        } else {
+            const double fi = (jd - E.jd_start) * E.inv_dt;
+            const double last = (double)(E.n - 1);
+            if (fi >= 0.0 && fi <= last) {
+                if (fi >= last) return eph_sample(E, E.n - 1, out);
+                const int64_t i = (int64_t)fi;
+                return eph_interp(E, i, fi - (double)i, out);
+            }
+        }
+        const double cl = fmin(fmax(jd, E.jd_start), E.jd_end);
+        const double tol = 2.0 * kEps * fmax(fabs(jd), fmax(fabs(E.jd_start), fabs(E.jd_end)));
+        if (fabs(jd - cl) <= tol) {
+            if (E.n < 2 || cl <= E.jd_start) return eph_sample(E, 0, out);
+            if (cl >= E.jd_end) return eph_sample(E, E.n - 1, out);
+            const double fi = (cl - E.jd_start) * E.inv_dt;
+            const int64_t i = (int64_t)fi;
+            return eph_interp(E, i, fi - (double)i, out);
+        }
+    }
+    out[0] = out[1] = out[2] = NAN;
+}
+
+// Sun or Moon: the catalogue when one is set, else the analytic series.
+BQP_HD void sun_at(const EphemTable& E, double jd, double* out) {
+    if (E.n > 0) ephem_position(E, jd, out);
+    else sun_position(jd, out);
+}
+BQP_HD void moon_at(const EphemTable& E, double jd, double* out) {
+    if (E.n > 0) ephem_position(E, jd, out);
+    else moon_position(jd, out);
+}
+
 BQP_HD void third_body(const double* sat, const double* body, double mu_body, double* acc) {
     double d2 = body[0] * body[0] + body[1] * body[1] + body[2] * body[2];
     if (d2 == 0.0) return;

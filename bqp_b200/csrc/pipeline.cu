@@ -163,11 +163,11 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
     double acc[3] = {0.0, 0.0, 0.0};
     double sun[3];
     const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0);
-    if (need_sun) sun_position(jd, sun);
+    if (need_sun) sun_at(fp.eph_sun, jd, sun);
     if (fp.sun) third_body(sp, sun, fp.mu_sun, acc);
     if (fp.moon) {
         double moon[3];
-        moon_position(jd, moon);
+        moon_at(fp.eph_moon, jd, moon);
         third_body(sp, moon, fp.mu_moon, acc);
     }
     const double r2 = fma(sp[0], sp[0], fma(sp[1], sp[1], sp[2] * sp[2]));

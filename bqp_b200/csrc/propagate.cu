@@ -246,6 +246,23 @@ __global__ void k_jb_lookup(jb::DriverTable T, const double* __restrict__ jd, in
     ok[i] = found ? 1 : 0;
 }
 
+// Sun (body 0) / Moon (1) positions as the force kernels take them.
+__global__ void k_body_positions(EphemTable E, int body, const double* __restrict__ jd, int64_t n,
+                                 double* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (body == 0) sun_at(E, jd[i], out + 3 * i);
+    else moon_at(E, jd[i], out + 3 * i);
+}
+
+cudaError_t launch_body_positions(const EphemTable& E, int body, const double* jd, int64_t n, double* out,
+                                  cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    k_body_positions<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(E, body, jd, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_jb_lookup(const jb::DriverTable& T, const double* jd, int64_t n, double* out, int32_t* ok,
                              cudaStream_t st) {
     if (n <= 0) return cudaSuccess;

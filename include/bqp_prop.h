@@ -177,6 +177,26 @@ int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_le
  * out[9 i] = F10, F81c, S10, S81c, M10, M81c, Y10, Y81c, dTc; ok[i] = 1, or 0
  * with a NaN row where the tables do not cover the instant.  Host buffers. */
 int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out, int32_t* ok);
+/* Precomputed Sun / Moon catalogues ("DUST" binary: 48-byte header, then
+ * samples x 3 f64 Earth-centred ICRS km on a uniform UTC Julian-day grid).
+ * Replaces PrecomputedEphemeris (lightyear_odeint_rs/src/precomputed_ephem.rs:
+ * loader 680-830, linear interpolation 1066-1131) as the force model reads it
+ * (rhs.rs:2964-3018): after this call the context's propagations take that
+ * body's position by linear interpolation at each evaluation's UTC instant,
+ * JD roundoff at an end clamped and any other instant outside the grid NaN
+ * (the row then fails, BQP_ST_GRAVITY_RADIUS).  Without a catalogue the
+ * analytic series apply.  bytes NULL: back to the series. */
+#define BQP_BODY_SUN 0
+#define BQP_BODY_MOON 1
+int bqp_ctx_set_ephemeris(bqp_ctx* ctx, int32_t body, const uint8_t* bytes, int64_t len);
+/* Positions (km) of a body at n UTC Julian days as the force kernels take
+ * them (catalogue or series), evaluated on the device.  Host buffers. */
+int bqp_ctx_body_positions(bqp_ctx* ctx, int32_t body, const double* utc_jd, int64_t n, double* out);
+/* Catalogue parsing and interpolation on the host, without a context:
+ * n_samples[0] = the catalogue's sample count; out as above (n may be 0). */
+int bqp_ephemeris_check(int32_t body, const uint8_t* bytes, int64_t len, const double* utc_jd, int64_t n,
+                        double* out, int64_t* n_samples);
+
 /* The same parsing and lookup on the host, without a context or a device:
  * counts2[0], counts2[1] = parsed SOLFSMY and DTCFILE rows, then n lookups as
  * in bqp_ctx_jb_lookup (n may be 0).  BQP_E_ARG names a rejected line. */

@@ -66,6 +66,10 @@ def lib():
         L.orc_force_set_drivers.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
         L.orc_jb_lookup.restype = C.c_int
         L.orc_jb_lookup.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _ip]
+        L.orc_force_set_ephemeris.restype = C.c_int
+        L.orc_force_set_ephemeris.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_long, C.c_char_p, C.c_int]
+        L.orc_body_positions.restype = None
+        L.orc_body_positions.argtypes = [C.c_void_p, C.c_int, C.c_long, _dp, _dp]
         L.orc_drivers_counts.restype = C.c_int
         L.orc_drivers_counts.argtypes = [C.c_void_p, _lp]
         _lib = L
@@ -116,6 +120,20 @@ class Force:
         if lib().orc_jb_lookup(self.h, jd.size, _d(jd), _d(out), ok.ctypes.data_as(_ip)) != 0:
             raise ValueError("oracle: no space-weather tables set")
         return out, ok.astype(bool)
+
+    def set_ephemeris(self, body: str, data: bytes | None):
+        """Sun or Moon positions from a precomputed catalogue ("DUST" format;
+        None: back to the analytic series); ValueError on a rejected file."""
+        err = C.create_string_buffer(256)
+        b = {"sun": 0, "moon": 1}[body]
+        if lib().orc_force_set_ephemeris(self.h, b, data, 0 if data is None else len(data), err, 256) != 0:
+            raise ValueError(f"oracle: ephemeris catalogue rejected: {err.value.decode()}")
+
+    def body_positions(self, body: str, utc_jd):
+        jd = f64(np.atleast_1d(utc_jd))
+        out = np.zeros((jd.size, 3))
+        lib().orc_body_positions(self.h, {"sun": 0, "moon": 1}[body], jd.size, _d(jd), _d(out))
+        return out
 
     def driver_counts(self):
         c = np.zeros(2, dtype=np.int64)

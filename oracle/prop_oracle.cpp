@@ -30,6 +30,9 @@
 //                                          rectification 917-1177, final 1462-1570,
 //                                          checked final 3418-3560, sampled 2160-2416
 //   crates/jb_rs/src/jb2008.rs             JB2008 (Orekit 13.1.2 adaptation)
+//   crates/lightyear_odeint_rs/src/precomputed_ephem.rs  catalogue header
+//                                          680-830, interpolation 1066-1131,
+//                                          endpoint rule of rhs.rs:2985-3018
 //   crates/jb_rs/src/drivers.rs            SOLFSMY / DTCFILE parsing 1025-1186,
 //                                          row checks 1188-1240, lagged lookup
 //                                          and hourly dTc 631-780
@@ -47,6 +50,7 @@
 #include <algorithm>
 #include <array>
 #include <cerrno>
+#include <cfloat>
 #include <climits>
 #include <memory>
 #ifdef _OPENMP
@@ -1016,6 +1020,96 @@ bool lookup(const DriverTable& T, double jd_in, double out[9]) {
 
 }  // namespace drv
 
+// ---------------------------------------------- precomputed Sun / Moon tables
+// "DUST" catalogues: 48-byte header (magic, u32 version 1, u64 samples, f64
+// JD start, JD end, step in days, u8 body, u8 epoch scale, u8 epoch
+// representation, 5 zero bytes) and samples x 3 f64 Earth-centred ICRS km.
+struct EphemTable {
+    std::vector<double> pos;
+    double jd_start = 0.0, dt = 0.0, inv_dt = 0.0;
+    size_t n = 0;
+};
+
+namespace eph {
+
+template <class T>
+T le(const unsigned char* p) {
+    T v;
+    std::memcpy(&v, p, sizeof v);  // the host is little-endian, as the format
+    return v;
+}
+
+// precomputed_ephem.rs:680-830
+bool parse(const unsigned char* b, size_t len, int body, EphemTable& T, std::string* err) {
+    if (len < 48) return *err = "short header", false;
+    if (std::memcmp(b, "DUST", 4) != 0) return *err = "bad magic", false;
+    if (le<uint32_t>(b + 4) != 1) return *err = "unsupported version", false;
+    const uint64_t n = le<uint64_t>(b + 8);
+    const double js = le<double>(b + 16), je = le<double>(b + 24), dt = le<double>(b + 32);
+    if (n == 0) return *err = "no samples", false;
+    if (!std::isfinite(js) || !std::isfinite(je) || !std::isfinite(dt) || dt <= 0.0)
+        return *err = "JD start / end / step", false;
+    const double end = js + (double)(n - 1) * dt;
+    if (end != je) return *err = "declared JD end disagrees with the grid", false;
+    if (b[40] != body) return *err = "body id", false;
+    if (b[41] > 4 || b[42] > 2) return *err = "unknown epoch tag", false;
+    for (int i = 43; i < 48; ++i)
+        if (b[i] != 0) return *err = "reserved bytes", false;
+    if (n > (len - 48) / 24 || len - 48 != n * 24) return *err = "payload size", false;
+    T.pos.resize(n * 3);
+    std::memcpy(T.pos.data(), b + 48, n * 24);
+    for (double v : T.pos)
+        if (!std::isfinite(v)) return *err = "non-finite position", false;
+    T.n = (size_t)n;
+    T.jd_start = js;
+    T.dt = dt;
+    T.inv_dt = 1.0 / dt;
+    return true;
+}
+
+void lerp(const EphemTable& T, size_t i, double f, double out[3]) {
+    for (int k = 0; k < 3; ++k) out[k] = T.pos[3 * i + k] * (1.0 - f) + T.pos[3 * (i + 1) + k] * f;
+}
+
+void sample(const EphemTable& T, size_t i, double out[3]) {
+    for (int k = 0; k < 3; ++k) out[k] = T.pos[3 * i + k];
+}
+
+// get_position (1092-1131); false outside the grid
+bool inside(const EphemTable& T, double jd, double out[3]) {
+    if (T.n == 1) {
+        if (std::fabs(jd - T.jd_start) <= DBL_EPSILON) return sample(T, 0, out), true;
+        return false;
+    }
+    const double fi = (jd - T.jd_start) * T.inv_dt;
+    const double last = (double)(T.n - 1);
+    if (fi < 0.0 || fi > last) return false;
+    if (fi >= last) return sample(T, T.n - 1, out), true;
+    const size_t i = (size_t)fi;
+    lerp(T, i, fi - (double)i, out);
+    return true;
+}
+
+// rhs.rs:2985-3018: outside the grid only JD roundoff at an end is clamped;
+// anything further is NaN
+void position(const EphemTable& T, double jd, double out[3]) {
+    if (std::isfinite(jd) && inside(T, jd, out)) return;
+    out[0] = out[1] = out[2] = NAN;
+    if (!std::isfinite(jd)) return;
+    const double start = T.jd_start, end = T.jd_start + (double)(T.n - 1) * T.dt;
+    const double cl = std::min(std::max(jd, start), end);
+    const double tol = 2.0 * DBL_EPSILON * std::max(std::fabs(jd), std::max(std::fabs(start), std::fabs(end)));
+    if (!(std::fabs(jd - cl) <= tol)) return;
+    // get_position_clamped (1134-1175)
+    if (T.n < 2 || cl <= start) return sample(T, 0, out);
+    if (cl >= end) return sample(T, T.n - 1, out);
+    const double fi = (cl - T.jd_start) * T.inv_dt;
+    const size_t i = (size_t)fi;
+    lerp(T, i, fi - (double)i, out);
+}
+
+}  // namespace eph
+
 struct Force {
     Field field;
     int use_gravity = 1;   // spherical harmonics on (order > 0)
@@ -1026,7 +1120,16 @@ struct Force {
     double mu_sun = 1.32712440018e11, mu_moon = 4902.800066;
     double drivers[9] = {150, 150, 150, 150, 150, 150, 150, 150, 0};  // f10..y10b, dTc
     std::shared_ptr<DriverTable> table;  // when set: drivers looked up per evaluation
+    std::shared_ptr<EphemTable> eph[2];  // Sun, Moon catalogues; unset: the analytic series
 };
+
+// Sun (body 0) or Moon (1) at a UTC Julian day: the catalogue when set
+// (rhs.rs:2964-3018), else the analytic series.
+void body_position(const Force& F, int body, double jd, double out[3]) {
+    if (F.eph[body]) return eph::position(*F.eph[body], jd, out);
+    if (body == 0) sun_position(jd, out);
+    else moon_position(jd, out);
+}
 
 // rhs.rs:3551-3776 with rhs.rs:1119-1163; density -> drag acceleration.
 double density_at(const Force& F, const double pos_itrs[3], const double sun_itrs[3], double jd) {
@@ -1108,7 +1211,7 @@ struct Rhs {
         double sun[3] = {0, 0, 0};
         bool have_sun = false;
         if (F->drag && cd != 0.0 && am != 0.0) {
-            sun_position(jd, sun);
+            body_position(*F, 0, jd, sun);
             have_sun = true;
             double pi[3], si[3];
             eci_to_itrs(s, c, sp, pi);
@@ -1123,12 +1226,12 @@ struct Rhs {
             }
         }
         if (F->sun) {
-            if (!have_sun) sun_position(jd, sun);
+            if (!have_sun) body_position(*F, 0, jd, sun);
             third_body(sp, sun, F->mu_sun, acc);
         }
         if (F->moon) {
             double moon[3];
-            moon_position(jd, moon);
+            body_position(*F, 1, jd, moon);
             third_body(sp, moon, F->mu_moon, acc);
         }
         battin(rs, d, r2, r, acc);
@@ -1797,6 +1900,30 @@ int orc_jb_lookup(void* f, long n, const double* jd, double* out, int* ok) {
             for (int k = 0; k < 9; ++k) out[9 * i + k] = NAN;
     }
     return 0;
+}
+
+// Sun (body 0) / Moon (1) catalogue bytes (null: back to the analytic series).
+int orc_force_set_ephemeris(void* f, int body, const unsigned char* bytes, long len, char* err, int errlen) {
+    Force* F = (Force*)f;
+    if (body < 0 || body > 1) return -1;
+    if (!bytes) {
+        F->eph[body].reset();
+        return 0;
+    }
+    auto T = std::make_shared<EphemTable>();
+    std::string e;
+    if (!eph::parse(bytes, (size_t)len, body, *T, &e)) {
+        if (err && errlen > 0) std::snprintf(err, (size_t)errlen, "%s", e.c_str());
+        return -1;
+    }
+    F->eph[body] = T;
+    return 0;
+}
+
+// Positions of the Sun / Moon at n UTC Julian days as the force model takes them.
+void orc_body_positions(void* f, int body, long n, const double* jd, double* out) {
+    const Force* F = (const Force*)f;
+    for (long i = 0; i < n; ++i) body_position(*F, body, jd[i], out + 3 * i);
 }
 
 // Parsed row counts of the current tables: counts[0] SOLFSMY, counts[1] DTCFILE.
