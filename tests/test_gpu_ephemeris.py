@@ -72,10 +72,13 @@ def test_device_positions_match_oracle():
         assert ok.sum() > 15000 and (~ok).sum() > 1000
         assert np.array_equal(np.isnan(got[:, 0]), ~ok)
         assert np.array_equal(got[ok].view(np.int64), ref[ok].view(np.int64))
-    # without a catalogue the series apply, as in the oracle
+    # without a catalogue the analytic series apply, as in the oracle (to the
+    # last bits: the device series contracts into FMAs, the oracle does not)
     plain = ctx_for(text, 4, None)
-    assert np.array_equal(plain.body_positions("moon", jds[:100]).view(np.int64),
-                          oracle_force(text, 4, None).body_positions("moon", jds[:100]).view(np.int64))
+    for body in ("sun", "moon"):
+        got = plain.body_positions(body, jds[:1000])
+        ref = oracle_force(text, 4, None).body_positions(body, jds[:1000])
+        assert np.all(np.linalg.norm(got - ref, axis=1) <= 1e-12 * np.linalg.norm(ref, axis=1))
 
 
 @pytest.mark.parametrize("engine", ENGINES)
