@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--split-degree", type=int, default=0,
                     help="split precision: harmonic degrees above this in FP32 (0: plain FP64)")
     ap.add_argument("--drag-fp32", action="store_true", help="split precision: JB2008 density in FP32")
+    ap.add_argument("--method", default="dop853", choices=["dop853", "vern7", "vern9", "dopri5"],
+                    help="stepper (the metric's workload: dop853 at eps 1e-12)")
+    ap.add_argument("--eps", type=float, default=EPS, help="absolute tolerance, km")
     return ap.parse_args()
 
 
@@ -154,7 +157,8 @@ def make_workload(n: int, seed: int = 0):
     return W.synthetic_field(ORDER), states, bal, W.EPOCH_JD
 
 
-def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp32=False):
+def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp32=False, method="dop853",
+                eps=EPS):
     from bqp_b200 import _native as N
 
     cfg = N.default_config()
@@ -165,9 +169,9 @@ def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp3
     cfg.order = ORDER
     cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON
     cfg.atm_model = 4
-    cfg.method = N.METHODS["dop853"]
+    cfg.method = N.METHODS[method]
     cfg.error_control = 0
-    cfg.eps = EPS
+    cfg.eps = eps
     cfg.dt_max = 300.0
     for i, v in enumerate(DRIVERS):
         cfg.jb_drivers[i] = v
@@ -267,7 +271,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
     text, states, bal, epoch = make_workload(args.n, seed=rank)
-    cfg = make_config(args.engine, args.gravity_threads, args.split_degree, args.drag_fp32)
+    cfg = make_config(args.engine, args.gravity_threads, args.split_degree, args.drag_fp32, args.method, args.eps)
     ctx = N.Context(text, cfg)
     seg = args.segment
     stream = torch.cuda.Stream(device=dev)
@@ -428,7 +432,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
-                                   f"DOP853 eps 1e-12, {seg:g} s of the arc per step",
+                                   f"{args.method.upper()} eps {args.eps:g}, {seg:g} s of the arc per step",
                        "form": form_name(args), "engine": args.engine, "order": ORDER, "trajectories_per_gpu": n,
                        "segment_s": seg, "l2": "256 MiB write between timed steps",
                        "evals_per_step": total_evals / args.steps,
@@ -439,7 +443,7 @@ def run_ours(args):
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
                                         "MEASURED_PEAKS.json)",
                          "flops_per_eval": fN,
-                         "kernel": "pl_gravity<4>" if dom == "gravity" else "k_propagate<DOP853>",
+                         "kernel": "pl_gravity<4>" if dom == "gravity" else f"k_propagate<{args.method.upper()}>",
                          "kernel_ms": dom_ms, "kernel_launches": dom_launches,
                          "kernel_timing": "second pass of the K steps with a CUDA event on each side of "
                                           "every launch",
