@@ -69,7 +69,7 @@ def f_of_n(n: int) -> float:
     return 9 * (n + 2) * (n + 3) / 2 + 13 * n * (n + 1) + 9 * (n + 1) + 60
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -88,7 +88,7 @@ def parse():
     ap.add_argument("--method", default="dop853", choices=["dop853", "vern7", "vern9", "dopri5"],
                     help="stepper (the metric's workload: dop853 at eps 1e-12)")
     ap.add_argument("--eps", type=float, default=EPS, help="absolute tolerance, km")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ------------------------------------------------------------------- clocks
@@ -255,6 +255,22 @@ def fp64_peak_tflops(torch, dev):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def combine_ranks(t_local, evals_local, world, device):
+    """Whole-job figures of a weak-scaled run: the slowest rank's time and the
+    evaluations of all ranks (every rank takes both collectives, in this
+    order).  One rank: the local figures."""
+    if world <= 1:
+        return float(t_local), float(evals_local)
+    import torch
+    import torch.distributed as dist
+
+    tt = torch.tensor([float(t_local)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ev = torch.tensor([float(evals_local)], device=device, dtype=torch.float64)
+    dist.all_reduce(ev, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(ev.item())
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -351,17 +367,7 @@ def run_ours(args):
     status_last = d_status.cpu().numpy()
     total_evals = int(evals_acc.item())
 
-    t_local = elapsed_ms
-    if world > 1:
-        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        ev = torch.tensor([float(total_evals)], device=dev, dtype=torch.float64)
-        dist.all_reduce(ev, op=dist.ReduceOp.SUM)
-        total_all = float(ev.item())
-    else:
-        t_max = t_local
-        total_all = float(total_evals)
+    t_max, total_all = combine_ranks(elapsed_ms, total_evals, world, dev)
     value = total_all / (t_max * 1e-3)
 
     # e2e: pinned host buffers through the host-buffer C ABI call
@@ -394,14 +400,7 @@ def run_ours(args):
                             evals=h_evals)
         e2e_evals += int(h_evals.sum())
         h_in[:] = h_out
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-        ev = torch.tensor([float(e2e_evals)], device=dev, dtype=torch.float64)
-        dist.all_reduce(ev, op=dist.ReduceOp.SUM)
-        e2e_evals = float(ev.item())
+    e2e_s, e2e_evals = combine_ranks(time.perf_counter() - t0, e2e_evals, world, dev)
     e2e_value = e2e_evals / e2e_s
     h2d = n * 6 * 8 + n * 8 * 2 + n * 16
     d2h = n * 6 * 8 + n * 4 + n * 8 * 2
