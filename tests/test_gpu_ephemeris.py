@@ -128,3 +128,16 @@ def test_arc_beyond_the_catalogue_fails_like_the_oracle(engine):
     assert list(ref_st) == [0, N.ST_GRAVITY_RADIUS, N.ST_GRAVITY_RADIUS]
     assert np.array_equal(st, ref_st), (st, ref_st)
     assert np.isfinite(got[0]).all() and np.isnan(got[1:]).all()
+
+
+def test_python_surface_takes_the_catalogues():
+    from bqp_b200 import api
+
+    cats = catalogues()
+    states = workloads.leo_states(4, seed=12)
+    text = workloads.synthetic_field(8)
+    got, st, _, _ = api.propagate_batch_final(states, EPOCH, 3600.0, gravity_order=8, gravity_field=text,
+                                              tol=1e-10, ephemeris=cats)
+    ref, st2, _, _ = ctx_for(text, 8, cats).propagate_final(states, EPOCH, 3600.0, ballistic=np.array([0.01, 2.2]))
+    assert (st == 0).all() and (st2 == 0).all()
+    assert np.abs(got[:, :3] - ref[:, :3]).max() < 1e-5

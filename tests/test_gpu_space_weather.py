@@ -160,3 +160,20 @@ def test_clearing_the_tables_restores_the_fixed_drivers():
     assert np.abs(with_tables[:, :3] - fresh[:, :3]).max() > 1e-4
     with pytest.raises(ValueError):
         ctx.set_jb_drivers(sol.replace("TEST", "", 1), dtc)
+
+
+def test_python_surface_takes_the_tables():
+    """api.* with space_weather=(solfsmy, dtcfile) runs the same tables as a
+    context that was given them."""
+    from bqp_b200 import api
+
+    sol, dtc = tables(2460300, 24, seed=8)
+    states = workloads.leo_states(4, seed=11)
+    got, st, _, _ = api.propagate_batch_final(states, EPOCH, 3600.0, gravity_order=8, gravity_field=
+                                              workloads.synthetic_field(8), tol=1e-10, space_weather=(sol, dtc))
+    cfg_ctx = ctx_for(workloads.synthetic_field(8), 8, sol, dtc)
+    assert (st == 0).all()
+    ref, st2, _, _ = cfg_ctx.propagate_final(states, EPOCH, 3600.0, ballistic=np.array([0.01, 2.2]))
+    assert (st2 == 0).all()
+    # same tables and settings up to the batch defaults (DOP853, eps 1e-10, A/m 0.01, Cd 2.2)
+    assert np.abs(got[:, :3] - ref[:, :3]).max() < 1e-5

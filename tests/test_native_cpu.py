@@ -142,3 +142,23 @@ def test_tensor_core_gemm_rejects_unsupported_shapes_before_device_use():
     for m, n, k in [(100, 256, 64), (128, 200, 64), (128, 256, 48)]:
         rc = lib.bqp_gemm_bf16_device(m, n, k, dummy, dummy, dummy, None)
         assert rc == N.E_ARG and b"multiple" in lib.bqp_last_error()
+
+
+def test_space_weather_and_ephemeris_arguments():
+    """The Python surface's file arguments: shapes accepted, others rejected
+    by name, without a device."""
+    from bqp_b200 import api
+
+    assert api._space_weather(None) is None
+    sol, dtc, span = api._space_weather(("a", b"b"))
+    assert (sol, dtc, span) == (b"a", b"b", (0.0, 0.0))
+    assert api._space_weather(("a", "b", (1, 2)))[2] == (1.0, 2.0)
+    with pytest.raises(ValueError, match="space_weather"):
+        api._space_weather("just one file")
+    assert api._ephemeris(None) == {}
+    assert api._ephemeris((b"s", None)) == {"sun": b"s"}
+    assert api._ephemeris({"moon": b"m"}) == {"moon": b"m"}
+    with pytest.raises(ValueError, match="ephemeris"):
+        api._ephemeris((b"s",))
+    with pytest.raises(ValueError, match="body"):
+        api._ephemeris({"mars": b"x"})
