@@ -343,6 +343,41 @@ def test_ground_impact_is_reported():
 
 
 @pytest.mark.parametrize("engine", ENGINES)
+def test_empty_batches(engine):
+    """No rows: both entry points return empty results without launching."""
+    ctx = ctx_for(workloads.synthetic_field(8), 8, flags=1 | 4 | 8, engine=engine)
+    out, st, steps, evals = ctx.propagate_final(np.zeros((0, 6)), EPOCH, np.zeros(0))
+    assert out.shape == (0, 6) and st.shape == steps.shape == evals.shape == (0,)
+    out, st, _, _ = ctx.propagate_sampled(np.zeros((0, 6)), EPOCH, np.zeros(0), np.array([0.0, 60.0]))
+    assert out.shape == (0, 2, 6) and st.shape == (0,)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_adaptive_at_the_largest_field(engine):
+    """Degree and order 120 (the table no longer fits in shared memory and is
+    read from global memory) + drag + Sun/Moon, against the oracle."""
+    order = 120
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    eps = 1e-10
+    ctx = ctx_for(text, order, flags=flags, eps=eps, engine=engine)
+    assert not ctx.info()["table_in_shared_memory"]
+    F = oracle_force(text, order, flags)
+    n = 8
+    states = workloads.leo_states(n, seed=51)
+    bal = workloads.leo_ballistics(n, seed=51)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 3000.0
+    got, st, steps, _ = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    ref_d, ref_st, ref_steps, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, EPOCH, tf, bal)
+    assert (st == 0).all() and (ref_st == 0).all()
+    for i in range(n):
+        ref = O.equinoc2eci(equ[i], tf)[0] + ref_d[i]
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+    assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
+
+
+@pytest.mark.parametrize("engine", ENGINES)
 def test_device_watchdog_stops_runaway_rows(engine):
     ctx = ctx_for(workloads.synthetic_field(8), 8, flags=0, eps=1e-10, max_attempts=5, engine=engine)
     states = workloads.leo_states(3, seed=1)
