@@ -32,12 +32,7 @@ __device__ __forceinline__ bool bulk_stage(void* smem_dst, const void* gsrc, uin
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint64_t state;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                     : "=l"(state)
-                     : "r"(bar_a), "r"(bytes)
-                     : "memory");
-        (void)state;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
         constexpr uint32_t kChunk = 32768;
         for (uint32_t off = 0; off < bytes; off += kChunk) {
             const uint32_t n = bytes - off < kChunk ? bytes - off : kChunk;

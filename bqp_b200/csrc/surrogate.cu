@@ -339,12 +339,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 
     // weights of hidden layer l (0..2) into sW, completion on bar_w
     auto load_w = [&](int l) {
-        uint64_t state;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                     : "=l"(state)
-                     : "r"(bar_w), "r"((uint32_t)kFusedW)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_w), "r"((uint32_t)kFusedW)
                      : "memory");
-        (void)state;
         const char* src = reinterpret_cast<const char*>(Wtile + (size_t)l * kH * kH);
         for (uint32_t off = 0; off < kFusedW; off += 32768)
             asm volatile(
