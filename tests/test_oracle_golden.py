@@ -94,3 +94,28 @@ def test_geodetic_altitude_matches_orekit(jbfix):
         p = np.array([h(x) for x in case["satellite_body_m"]]) / 1000.0
         alt = O.geodetic_altitude_km(p) * 1000.0
         assert abs(alt - h(case["satellite_geodetic"]["altitude_m"])) < 1e-6, case["id"]
+
+
+def test_oracle_steppers_converge_to_one_trajectory():
+    """DOP853, Vern7, Vern9 and the Dormand-Prince solver at tight tolerance
+    reach the same final state (20x20 + drag + Sun/Moon, 3000 s, rectified):
+    the tableaus and their error estimates drive one controller correctly."""
+    import numpy as np
+
+    from bqp_b200 import _native as N
+    from bqp_b200 import workloads
+    from oracle import oracle as O
+
+    order = 20
+    text = workloads.synthetic_field(order)
+    F = O.Force(text, order, drag=True, sun=True, moon=True)
+    states = workloads.leo_states(3, seed=13)
+    bal = workloads.leo_ballistics(3, seed=13)
+    equ, _ = N.eci_to_equinoctial(states)
+    finals = {}
+    for m in ("dop853", "vern7", "vern9", "dopri5_solver"):
+        d, st, steps, _ = O.propagate_final_batch(F, O.ctrl(m, eps=1e-12), equ, 2460310.5, 3000.0, bal)
+        assert (st == 0).all(), m
+        finals[m] = d[:, :3]
+    for m, d in finals.items():
+        assert np.abs(d - finals["vern9"]).max() < 1e-6, m
