@@ -70,6 +70,14 @@ def lib():
         L.orc_force_set_ephemeris.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_long, C.c_char_p, C.c_int]
         L.orc_body_positions.restype = None
         L.orc_body_positions.argtypes = [C.c_void_p, C.c_int, C.c_long, _dp, _dp]
+        L.orc_shadow_cylinder.restype = C.c_int
+        L.orc_shadow_cylinder.argtypes = [_dp, _dp, C.c_double, _dp]
+        L.orc_srp_accel.restype = None
+        L.orc_srp_accel.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+        L.orc_eclipse_envelope_ok.restype = C.c_int
+        L.orc_eclipse_envelope_ok.argtypes = [_dp, _dp]
+        L.orc_no_crossing_certified.restype = C.c_int
+        L.orc_no_crossing_certified.argtypes = [C.c_double, C.c_double, C.c_double]
         L.orc_drivers_counts.restype = C.c_int
         L.orc_drivers_counts.argtypes = [C.c_void_p, _lp]
         _lib = L
@@ -233,3 +241,27 @@ def jb2008(inputs14) -> float:
 
 def geodetic_altitude_km(pos_km, a=6378.137) -> float:
     return lib().orc_geodetic_altitude_km(_d(f64(pos_km)), a)
+
+
+# ---------------------------------------------------- SRP and the shadow cylinder
+def shadow_cylinder(sat, sun, earth_radius=6378.137):
+    """("shadow" | "lit", margin km) of the Earth's shadow cylinder, or None for
+    invalid geometry."""
+    out = np.zeros(2)
+    if lib().orc_shadow_cylinder(_d(f64(sat)), _d(f64(sun)), float(earth_radius), _d(out)) != 0:
+        return None
+    return ("shadow" if out[0] else "lit"), float(out[1])
+
+
+def srp_accel(sat, sun, cr=1.3, am=0.01, shadow=False, p_sun=4.56e-6):
+    out = np.zeros(3)
+    lib().orc_srp_accel(_d(f64(sat)), _d(f64(sun)), float(p_sun), float(cr), float(am), int(bool(shadow)), _d(out))
+    return out
+
+
+def eclipse_envelope_ok(pos, vel) -> bool:
+    return bool(lib().orc_eclipse_envelope_ok(_d(f64(pos)), _d(f64(vel))))
+
+
+def no_crossing_certified(m_old, m_new, bound) -> bool:
+    return bool(lib().orc_no_crossing_certified(float(m_old), float(m_new), float(bound)))

@@ -33,6 +33,9 @@
 //   crates/lightyear_odeint_rs/src/precomputed_ephem.rs  catalogue header
 //                                          680-830, interpolation 1066-1131,
 //                                          endpoint rule of rhs.rs:2985-3018
+//   crates/lightyear_odeint_rs/src/eclipse.rs  binary shadow cylinder 175-262,
+//                                          envelope 124-152, certificate 325-327
+//   crates/lightyear_odeint_rs/src/rhs.rs  SRP acceleration 1269-1310
 //   crates/jb_rs/src/drivers.rs            SOLFSMY / DTCFILE parsing 1025-1186,
 //                                          row checks 1188-1240, lagged lookup
 //                                          and hourly dTc 631-780
@@ -1110,6 +1113,79 @@ void position(const EphemTable& T, double jd, double out[3]) {
 
 }  // namespace eph
 
+// ------------------------------------------ solar radiation pressure, shadow
+// The pieces of the reference's binary-eclipse SRP that are plain functions;
+// the event coordinator that sets the side per leg is not restated here.
+namespace srp {
+
+constexpr double AU_KM = 149597870.7;
+constexpr double M_TO_KM = 0.001;
+
+// eclipse.rs:189-262: side (1 shadow, 0 lit) and distance to the boundary of
+// the Earth's shadow cylinder along the Sun direction; false on bad geometry.
+bool cylinder(const double sat[3], const double sun[3], double earth_radius, int* shadow, double* margin) {
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(sat[i]) || !std::isfinite(sun[i])) return false;
+    if (!(std::isfinite(earth_radius) && earth_radius > 0.0)) return false;
+    const double sun_sq = sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2];
+    if (!(std::isfinite(sun_sq) && sun_sq > 0.0)) return false;
+    const double inv = 1.0 / std::sqrt(sun_sq);
+    const double u[3] = {sun[0] * inv, sun[1] * inv, sun[2] * inv};
+    const double axial = std::fma(sat[0], u[0], std::fma(sat[1], u[1], sat[2] * u[2]));
+    const double rad[3] = {sat[0] - axial * u[0], sat[1] - axial * u[1], sat[2] - axial * u[2]};
+    const double rad_sq = std::fma(rad[0], rad[0], std::fma(rad[1], rad[1], rad[2] * rad[2]));
+    const double r_sq = earth_radius * earth_radius;
+    if (!(std::isfinite(axial) && std::isfinite(rad_sq) && std::isfinite(r_sq))) return false;
+    const double rd = std::sqrt(rad_sq);
+    const double signed_margin = (rad_sq - r_sq) / (rd + earth_radius);
+    double m;
+    if (axial < 0.0 && rad_sq < r_sq) {
+        *shadow = 1;
+        m = std::min(-axial, -signed_margin);
+    } else {
+        *shadow = 0;
+        const bool a = axial >= 0.0, b = rad_sq >= r_sq;
+        m = a && b ? std::max(axial, signed_margin) : (a ? axial : (b ? signed_margin : 0.0));
+    }
+    if (!(std::isfinite(m) && m >= 0.0)) return false;
+    *margin = m;
+    return true;
+}
+
+// rhs.rs:1269-1310: cannonball pressure away from the Sun, none in shadow.
+void accel(const double sat[3], const double sun[3], double p_sun, double cr, double am, int shadow, double out[3]) {
+    out[0] = out[1] = out[2] = 0.0;
+    if (cr == 0.0 || am == 0.0 || p_sun == 0.0) return;
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(sat[i])) return (void)(out[0] = out[1] = out[2] = NAN);
+    if (shadow) return;
+    const double rx = sun[0] - sat[0], ry = sun[1] - sat[1], rz = sun[2] - sat[2];
+    const double d2 = std::fma(rx, rx, std::fma(ry, ry, rz * rz));
+    if (!(std::isfinite(d2) && d2 > 0.0)) return (void)(out[0] = out[1] = out[2] = NAN);
+    const double inv = 1.0 / std::sqrt(d2);
+    const double scale = (AU_KM * AU_KM) / d2;
+    const double a = p_sun * cr * am * scale * M_TO_KM;
+    out[0] = -a * rx * inv;
+    out[1] = -a * ry * inv;
+    out[2] = -a * rz * inv;
+}
+
+// eclipse.rs:124-152: the numerical envelope the coordinator accepts.
+bool envelope_ok(const double pos[3], const double vel[3]) {
+    auto norm = [](const double* v) { return std::sqrt(std::fma(v[0], v[0], std::fma(v[1], v[1], v[2] * v[2]))); };
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(pos[i]) || !std::isfinite(vel[i])) return false;
+    const double r = norm(pos), s = norm(vel);
+    return std::isfinite(r) && std::isfinite(s) && r >= 6000.0 && r <= 50000.0 && s <= 20.0;
+}
+
+// eclipse.rs:325-327: no interior instant can reach the boundary.
+bool no_crossing_certified(double margin_old, double margin_new, double motion_bound) {
+    return margin_old + margin_new > motion_bound;
+}
+
+}  // namespace srp
+
 struct Force {
     Field field;
     int use_gravity = 1;   // spherical harmonics on (order > 0)
@@ -1900,6 +1976,28 @@ int orc_jb_lookup(void* f, long n, const double* jd, double* out, int* ok) {
             for (int k = 0; k < 9; ++k) out[9 * i + k] = NAN;
     }
     return 0;
+}
+
+// Shadow-cylinder side and margin: out2 = {shadow (1) / lit (0), margin km};
+// returns 0, or -1 for invalid geometry.
+int orc_shadow_cylinder(const double* sat, const double* sun, double earth_radius, double* out2) {
+    int shadow = 0;
+    double margin = 0.0;
+    if (!srp::cylinder(sat, sun, earth_radius, &shadow, &margin)) return -1;
+    out2[0] = shadow;
+    out2[1] = margin;
+    return 0;
+}
+
+void orc_srp_accel(const double* sat, const double* sun, double p_sun, double cr, double am, int shadow,
+                   double* out) {
+    srp::accel(sat, sun, p_sun, cr, am, shadow, out);
+}
+
+int orc_eclipse_envelope_ok(const double* pos, const double* vel) { return srp::envelope_ok(pos, vel) ? 1 : 0; }
+
+int orc_no_crossing_certified(double m_old, double m_new, double bound) {
+    return srp::no_crossing_certified(m_old, m_new, bound) ? 1 : 0;
 }
 
 // Sun (body 0) / Moon (1) catalogue bytes (null: back to the analytic series).
