@@ -78,6 +78,9 @@ def lib():
         L.orc_eclipse_envelope_ok.argtypes = [_dp, _dp]
         L.orc_no_crossing_certified.restype = C.c_int
         L.orc_no_crossing_certified.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.orc_first_crossing_in_step.restype = C.c_int
+        L.orc_first_crossing_in_step.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_long,
+                                                 _STATE_FN, _BOUND_FN, _dp, _lp]
         L.orc_drivers_counts.restype = C.c_int
         L.orc_drivers_counts.argtypes = [C.c_void_p, _lp]
         _lib = L
@@ -261,6 +264,44 @@ def srp_accel(sat, sun, cr=1.3, am=0.01, shadow=False, p_sun=4.56e-6):
 
 def eclipse_envelope_ok(pos, vel) -> bool:
     return bool(lib().orc_eclipse_envelope_ok(_d(f64(pos)), _d(f64(vel))))
+
+
+_STATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, _dp, _dp, _dp)
+_BOUND_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, _dp, _dp, _dp)
+SCAN_ERRORS = {1: "geometry", 2: "bracket", 3: "non_progress", 4: "split_limit"}
+
+
+def first_crossing_in_step(t_old, t_new, state, bound, max_splits=1_000_000, earth_radius=6378.137,
+                           max_sep=1.0e-6):
+    """The oracle's shadow-crossing scan.  state(t) -> (pos, vel, sun) or None
+    for failure; bound((t, pos, vel), (t, pos, vel)) -> km or None.  Returns
+    (error name or None, result dict)."""
+
+    def c_state(_, t, pos, vel, sun):
+        got = state(t)
+        if got is None:
+            return 1
+        for dst, src in zip((pos, vel, sun), got):
+            for i in range(3):
+                dst[i] = float(src[i])
+        return 0
+
+    def c_bound(_, a, b, out):
+        got = bound((a[0], tuple(a[1:4]), tuple(a[4:7])), (b[0], tuple(b[1:4]), tuple(b[4:7])))
+        if got is None:
+            return 1
+        out[0] = float(got)
+        return 0
+
+    sf, bf = _STATE_FN(c_state), _BOUND_FN(c_bound)
+    out = np.zeros(6)
+    collapsed = np.zeros(1, dtype=np.int64)
+    e = lib().orc_first_crossing_in_step(float(t_old), float(t_new), float(earth_radius), float(max_sep),
+                                         int(max_splits), sf, bf, _d(out), collapsed.ctypes.data_as(_lp))
+    res = {"found": bool(out[0]), "t_old": out[1], "t_new": out[2],
+           "old_side": "shadow" if out[3] else "lit", "new_side": "shadow" if out[4] else "lit",
+           "bound": out[5], "collapsed_pairs": int(collapsed[0])}
+    return SCAN_ERRORS.get(e), res
 
 
 def no_crossing_certified(m_old, m_new, bound) -> bool:

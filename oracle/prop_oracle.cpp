@@ -34,7 +34,8 @@
 //                                          680-830, interpolation 1066-1131,
 //                                          endpoint rule of rhs.rs:2985-3018
 //   crates/lightyear_odeint_rs/src/eclipse.rs  binary shadow cylinder 175-262,
-//                                          envelope 124-152, certificate 325-327
+//                                          envelope 124-152, certificate 325-327,
+//                                          in-step crossing scan 341-491
 //   crates/lightyear_odeint_rs/src/rhs.rs  SRP acceleration 1269-1310
 //   crates/jb_rs/src/drivers.rs            SOLFSMY / DTCFILE parsing 1025-1186,
 //                                          row checks 1188-1240, lagged lookup
@@ -1184,6 +1185,94 @@ bool no_crossing_certified(double margin_old, double margin_new, double motion_b
     return margin_old + margin_new > motion_bound;
 }
 
+// eclipse.rs:341-491: the first side change of the shadow cylinder between
+// two instants (either order), by bisection at binary64 midpoints until the
+// geometry motion across the bracket is at most max_sep km.  state(t) gives
+// the satellite position, velocity and the Sun position at t; bound(old,
+// new) a certified upper bound on the geometry motion between two instants.
+enum ScanStatus { SCAN_OK = 0, SCAN_GEOMETRY = 1, SCAN_BRACKET = 2, SCAN_NON_PROGRESS = 3, SCAN_SPLIT_LIMIT = 4 };
+typedef int (*StateFn)(void* user, double t, double* pos, double* vel, double* sun);
+typedef int (*BoundFn)(void* user, const double* old_tpv, const double* new_tpv, double* bound);
+
+struct ScanPoint {
+    double tpv[7];  // t, position, velocity
+    int shadow;
+    double margin;
+};
+
+struct ScanResult {
+    int found;
+    double t_old, t_new;
+    int old_shadow, new_shadow;
+    double bound;
+    long collapsed;
+};
+
+struct Scan {
+    double earth_radius, max_sep;
+    long splits_left;
+    StateFn state;
+    BoundFn bound;
+    void* user;
+
+    int point(double t, ScanPoint* p) {
+        if (!std::isfinite(t)) return SCAN_GEOMETRY;
+        double sun[3];
+        p->tpv[0] = t;
+        if (state(user, t, p->tpv + 1, p->tpv + 4, sun) != 0) return SCAN_GEOMETRY;
+        if (!cylinder(p->tpv + 1, sun, earth_radius, &p->shadow, &p->margin)) return SCAN_GEOMETRY;
+        return SCAN_OK;
+    }
+
+    int interval(const ScanPoint& a, const ScanPoint& b, bool inherited, double inherited_bound, ScanResult* r) {
+        const double dx = b.tpv[1] - a.tpv[1], dy = b.tpv[2] - a.tpv[2], dz = b.tpv[3] - a.tpv[3];
+        const double sep = std::sqrt(std::fma(dx, dx, std::fma(dy, dy, dz * dz)));
+        if (!std::isfinite(sep)) return SCAN_GEOMETRY;
+        if (a.shadow == b.shadow && inherited && no_crossing_certified(a.margin, b.margin, inherited_bound))
+            return SCAN_OK;
+        double mb;
+        if (bound(user, a.tpv, b.tpv, &mb) != 0) return SCAN_GEOMETRY;
+        if (!(std::isfinite(mb) && mb >= sep && mb >= 0.0)) return SCAN_BRACKET;
+        if (a.shadow == b.shadow && no_crossing_certified(a.margin, b.margin, mb)) return SCAN_OK;
+        if (mb <= max_sep && a.shadow != b.shadow) {
+            r->found = 1;
+            r->t_old = a.tpv[0];
+            r->t_new = b.tpv[0];
+            r->old_shadow = a.shadow;
+            r->new_shadow = b.shadow;
+            r->bound = mb;
+            return SCAN_OK;
+        }
+        const double mid = a.tpv[0] + 0.5 * (b.tpv[0] - a.tpv[0]);
+        if (mid == a.tpv[0] || mid == b.tpv[0] || !std::isfinite(mid)) {
+            // adjacent binary64 instants: nothing representable in between
+            if (a.shadow == b.shadow && mb <= 1.0e-6) {
+                r->collapsed += 1;
+                return SCAN_OK;
+            }
+            return SCAN_NON_PROGRESS;
+        }
+        if (splits_left == 0) return SCAN_SPLIT_LIMIT;
+        --splits_left;
+        ScanPoint m;
+        if (int e = point(mid, &m)) return e;
+        if (int e = interval(a, m, true, mb, r)) return e;
+        if (r->found) return SCAN_OK;
+        return interval(m, b, true, mb, r);
+    }
+};
+
+int first_crossing(double t_old, double t_new, double earth_radius, double max_sep, long max_splits, StateFn state,
+                   BoundFn bound, void* user, ScanResult* r) {
+    *r = ScanResult{0, 0.0, 0.0, 0, 0, 0.0, 0};
+    if (!(std::isfinite(max_sep) && max_sep > 0.0) || t_old == t_new) return SCAN_NON_PROGRESS;
+    Scan s{earth_radius, max_sep, max_splits, state, bound, user};
+    ScanPoint a, b;
+    if (int e = s.point(t_old, &a)) return e;
+    if (int e = s.point(t_new, &b)) return e;
+    return s.interval(a, b, false, 0.0, r);
+}
+
 }  // namespace srp
 
 struct Force {
@@ -1995,6 +2084,22 @@ void orc_srp_accel(const double* sat, const double* sun, double p_sun, double cr
 }
 
 int orc_eclipse_envelope_ok(const double* pos, const double* vel) { return srp::envelope_ok(pos, vel) ? 1 : 0; }
+
+// out6 = {found, t_old, t_new, old_shadow, new_shadow, motion bound}; collapsed[0]
+// = adjacent same-side pairs resolved; returns a srp::ScanStatus.
+int orc_first_crossing_in_step(double t_old, double t_new, double earth_radius, double max_sep, long max_splits,
+                               srp::StateFn state, srp::BoundFn bound, double* out6, long* collapsed) {
+    srp::ScanResult r;
+    const int e = srp::first_crossing(t_old, t_new, earth_radius, max_sep, max_splits, state, bound, nullptr, &r);
+    out6[0] = r.found;
+    out6[1] = r.t_old;
+    out6[2] = r.t_new;
+    out6[3] = r.old_shadow;
+    out6[4] = r.new_shadow;
+    out6[5] = r.bound;
+    collapsed[0] = r.collapsed;
+    return e;
+}
 
 int orc_no_crossing_certified(double m_old, double m_new, double bound) {
     return srp::no_crossing_certified(m_old, m_new, bound) ? 1 : 0;

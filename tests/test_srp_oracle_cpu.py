@@ -64,3 +64,99 @@ def test_srp_acceleration():
     assert np.all(O.srp_accel(sat, SUN, shadow=True) == 0.0)
     assert np.all(O.srp_accel(sat, SUN, cr=0.0) == 0.0)
     assert np.isnan(O.srp_accel([np.nan, 0.0, 0.0], SUN)).all()
+
+
+# ---------------------------------------------------------------- crossing scan
+# eclipse.rs:660-862: a satellite path that dips through the cylinder boundary
+# and back during t in [0, 1], and a Sun axis that swings past a parked satellite.
+import struct
+
+MAX_SEP = 1.0e-6
+
+
+def padded_upper_bound(value):
+    bits = struct.unpack("<q", struct.pack("<d", value))[0] + 8
+    return struct.unpack("<d", struct.pack("<q", bits))[0] + 1e-9
+
+
+def double_crossing_state(t):
+    if not np.isfinite(t):
+        return None
+    offset = 8.0 * (t - 0.5) * (t - 0.5) - 1.0
+    return [-7000.0, R + offset, 0.0], [0.0, 16.0 * (t - 0.5), 0.0], SUN
+
+
+def double_crossing_bound(old, new):
+    t0, t1 = old[0], new[0]
+    max_speed = 16.0 * max(abs(t0 - 0.5), abs(t1 - 0.5))
+    return padded_upper_bound(max_speed * abs(t1 - t0))
+
+
+def midpoint(a, b):
+    return a + 0.5 * (b - a)
+
+
+def test_scan_finds_the_earliest_forward_crossing():
+    err, hit = O.first_crossing_in_step(0.0, 1.0, double_crossing_state, double_crossing_bound)
+    assert err is None and hit["found"]
+    assert (hit["old_side"], hit["new_side"]) == ("lit", "shadow")
+    assert hit["t_old"] < hit["t_new"] and hit["bound"] <= MAX_SEP
+    assert abs(midpoint(hit["t_old"], hit["t_new"]) - 0.1464466094) < 1e-5
+    err, second = O.first_crossing_in_step(hit["t_new"], 1.0, double_crossing_state, double_crossing_bound)
+    assert err is None and second["found"]
+    assert (second["old_side"], second["new_side"]) == ("shadow", "lit")
+    assert hit["t_new"] < second["t_old"]
+
+
+def test_scan_finds_the_earliest_backward_crossing():
+    err, hit = O.first_crossing_in_step(1.0, 0.0, double_crossing_state, double_crossing_bound)
+    assert err is None and hit["found"]
+    assert (hit["old_side"], hit["new_side"]) == ("lit", "shadow")
+    assert hit["t_old"] > hit["t_new"] and hit["bound"] <= MAX_SEP
+    assert abs(midpoint(hit["t_old"], hit["t_new"]) - 0.8535533906) < 1e-5
+    err, second = O.first_crossing_in_step(hit["t_new"], 0.0, double_crossing_state, double_crossing_bound)
+    assert err is None and (second["old_side"], second["new_side"]) == ("shadow", "lit")
+    assert hit["t_new"] > second["t_old"]
+
+
+def test_scan_limit_is_a_typed_failure():
+    err, _ = O.first_crossing_in_step(0.0, 1.0, double_crossing_state, double_crossing_bound, max_splits=1)
+    assert err == "split_limit"
+
+
+def test_adjacent_same_side_pair_is_counted_both_ways():
+    t0 = 1.0
+    t1 = np.nextafter(t0, 2.0)
+    state = lambda t: ([-7000.0, R, 0.0], [0.0, 0.0, 0.0], SUN)
+    for a, b in ((t0, t1), (t1, t0)):
+        err, out = O.first_crossing_in_step(a, b, state, lambda o, n: 0.5 * MAX_SEP, max_splits=0)
+        assert err is None and not out["found"] and out["collapsed_pairs"] == 1
+    err, _ = O.first_crossing_in_step(t0, t1, state, lambda o, n: 2.0 * MAX_SEP, max_splits=8)
+    assert err == "non_progress"
+
+
+def test_nonadjacent_same_side_interval_needs_the_split_budget():
+    t0 = 1.0
+    t2 = np.nextafter(np.nextafter(t0, 2.0), 2.0)
+    err, _ = O.first_crossing_in_step(t0, t2, lambda t: ([-7000.0, R, 0.0], [0.0, 0.0, 0.0], SUN),
+                                      lambda o, n: 0.5 * MAX_SEP, max_splits=0)
+    assert err == "split_limit"
+
+
+def test_moving_sun_axis_reveals_hidden_crossings():
+    sat = [-7000.0, R + 1.0, 0.0]
+    radius = float(np.sqrt(sum(c * c for c in sat)))
+
+    def state(t):
+        theta = -0.004 * t * (1.0 - t)
+        return sat, [0.0, 0.0, 0.0], [SUN[0] * np.cos(theta), SUN[0] * np.sin(theta), 0.0]
+
+    def bound(old, new):
+        t0, t1 = old[0], new[0]
+        speed = max(abs(0.004 * (1.0 - 2.0 * t0)), abs(0.004 * (1.0 - 2.0 * t1)))
+        return padded_upper_bound(2.0 * radius * speed * abs(t1 - t0))
+
+    err, hit = O.first_crossing_in_step(0.0, 1.0, state, bound)
+    assert err is None and hit["found"]
+    assert (hit["old_side"], hit["new_side"]) == ("lit", "shadow")
+    assert midpoint(hit["t_old"], hit["t_new"]) < 0.5 and hit["bound"] <= MAX_SEP
