@@ -349,7 +349,11 @@ BQP_HD void ephem_position(const EphemTable& E, double jd, double* out) {
             if (cl >= E.jd_end) return eph_sample(E, E.n - 1, out);
             const double fi = (cl - E.jd_start) * E.inv_dt;
             const int64_t i = (int64_t)fi;
-            return eph_interp(E, i, fi - (double)i, out);
+            if (i + 1 < E.n) return eph_interp(E, i, fi - (double)i, out);
+            // 1/dt rounded the index onto the last sample: the reference finds
+            // no next sample there and answers the origin
+            out[0] = out[1] = out[2] = 0.0;
+            return;
         }
     }
     out[0] = out[1] = out[2] = NAN;

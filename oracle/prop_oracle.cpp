@@ -1109,6 +1109,10 @@ void position(const EphemTable& T, double jd, double out[3]) {
     if (cl >= end) return sample(T, T.n - 1, out);
     const double fi = (cl - T.jd_start) * T.inv_dt;
     const size_t i = (size_t)fi;
+    if (i + 1 >= T.n) {  // precomputed_ephem.rs:1160-1172: no next sample -> origin
+        out[0] = out[1] = out[2] = 0.0;
+        return;
+    }
     lerp(T, i, fi - (double)i, out);
 }
 
