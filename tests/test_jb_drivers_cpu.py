@@ -164,3 +164,37 @@ def test_reference_files_known_answer():
     rng = np.random.default_rng(5)
     same_as_oracle((REF_DATA / "SOLFSMY.TXT").read_text(), (REF_DATA / "DTCFILE.TXT").read_text(),
                    np.concatenate([[2459528.0], rng.uniform(2445000.0, 2461200.0, 20000)]))
+
+
+def test_constant_tables_reproduce_the_fixed_drivers_in_propagation():
+    """A table whose every day holds the fixed drivers (150 sfu, dTc 20 K)
+    gives the oracle's fixed-driver propagation bit for bit: the per-evaluation
+    lookup feeds the same density call."""
+    order = 8
+    text = workloads.synthetic_field(order)
+    import datetime
+
+    # 40 days across the 2023 / 2024 year boundary, dated from their day numbers
+    rows = ["# F10, S10, M10, Y10 data release constant"]
+    dtc_rows = []
+    for k in range(40):
+        jdn = 2460290 + k
+        d = datetime.date.fromordinal(jdn - 1721425)
+        doy = d.timetuple().tm_yday
+        rows.append(f"{d.year} {doy} {jdn} " + " ".join(["150.0"] * 8) + " TEST")
+        dtc_rows.append(f"DTC {d.year} {doy} " + " ".join(["20"] * 24))
+    sol, dtc = "\n".join(rows) + "\n", "\n".join(dtc_rows) + "\n"
+    from bqp_b200 import _native as N
+
+    states = workloads.leo_states(4, seed=3)
+    bal = workloads.leo_ballistics(4, seed=3)
+    equ, _ = N.eci_to_equinoctial(states)
+    fixed = O.Force(text, order, drag=True, sun=True, moon=True, drivers=(150.0,) * 8 + (20.0,))
+    table = O.Force(text, order, drag=True, sun=True, moon=True, drivers=(1.0,) * 8 + (0.0,))
+    table.set_drivers(sol, dtc)
+    ctl = O.ctrl("dop853", eps=1e-10)
+    a = O.propagate_final_batch(fixed, ctl, equ, 2460310.5, 86400.0, bal)
+    b = O.propagate_final_batch(table, ctl, equ, 2460310.5, 86400.0, bal)
+    assert (a[1] == 0).all() and (b[1] == 0).all()
+    assert np.array_equal(a[0].view(np.int64), b[0].view(np.int64))
+    assert np.array_equal(a[2], b[2])
