@@ -103,17 +103,20 @@ inline size_t gravity_smem_bytes(const GravTable& T, int block, int nt, int part
     return tab + red;
 }
 
-// Rows [b0, b1) of this CTA.  load(i, x, y, z) fetches row i's Earth-fixed
+// Rows [b0, b1) of this CTA; the layout (and so the order in which a row's
+// column sums are added) follows layout_rows, the same for every CTA of a
+// launch, so a row's result does not depend on which CTA it lands in.
+// load(i, x, y, z) fetches row i's Earth-fixed
 // position and returns false for a row to leave out (it records that row's
 // outcome itself; every group calls it, so it must be idempotent).
 // store(i, a, x, y, z) receives the field of row i (group 0 only).
 // lost(i) records that row i got no field because the table copy did not
 // complete in time.
 template <int NT, class Load, class Store, class Lost>
-__device__ __forceinline__ void gravity_cta(const GravTable& T, int parts_max, int b0, int b1, Load load, Store store,
-                                            Lost lost) {
+__device__ __forceinline__ void gravity_cta(const GravTable& T, int parts_max, int layout_rows, int b0, int b1,
+                                            Load load, Store store, Lost lost) {
     extern __shared__ __align__(16) double smem_dyn[];
-    const GravLayout L = gravity_layout(b1 - b0, NT, blockDim.x, parts_max);
+    const GravLayout L = gravity_layout(layout_rows, NT, blockDim.x, parts_max);
     if (T.in_smem && !bulk_stage(smem_dyn, T.tab, T.bytes)) {
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) lost(i);
         return;  // the verdict is the same in every thread

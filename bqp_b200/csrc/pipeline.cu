@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
         P.bad[sl] = 2;
         P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
     };
-    gravity_cta<NT>(T, parts_max, b0, b1, load, store, lost);
+    gravity_cta<NT>(T, parts_max, per_block, b0, b1, load, store, lost);
 }
 
 // Earth-fixed positions of the stage's active slots, [slot][3] (the

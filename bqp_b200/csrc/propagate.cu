@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256, 1) k_gravity(GravTable T, int parts_max, 
         a0[3 * i] = a0[3 * i + 1] = a0[3 * i + 2] = NAN;
         if (s0) s0[i] = kWatchdog;
     };
-    gravity_cta<NT>(T, parts_max, 0, (int)(c1 - c0), load, store, lost);
+    gravity_cta<NT>(T, parts_max, (int)per_block, 0, (int)(c1 - c0), load, store, lost);
 }
 
 __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem, ForceParams fp,

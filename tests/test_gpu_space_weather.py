@@ -177,3 +177,31 @@ def test_python_surface_takes_the_tables():
     assert (st2 == 0).all()
     # same tables and settings up to the batch defaults (DOP853, eps 1e-10, A/m 0.01, Cd 2.2)
     assert np.abs(got[:, :3] - ref[:, :3]).max() < 1e-5
+
+
+def test_constant_tables_give_the_fixed_drivers_bits():
+    """Tables holding the default fixed drivers every day (150 sfu, dTc 0 K) give the
+    fixed-driver propagation bit for bit: the per-evaluation lookup feeds the
+    same density call."""
+    rows = ["# F10, S10, M10, Y10 data release constant"]
+    dtc_rows = []
+    for k in range(40):
+        jdn = 2460290 + k
+        d = datetime.date.fromordinal(jdn - 1721425)
+        doy = d.timetuple().tm_yday
+        rows.append(f"{d.year} {doy} {jdn} " + " ".join(["150.0"] * 8) + " TEST")
+        dtc_rows.append(f"DTC {d.year} {doy} " + " ".join(["0"] * 24))
+    sol, dtc = "\n".join(rows) + "\n", "\n".join(dtc_rows) + "\n"
+    order = 20
+    text = workloads.synthetic_field(order)
+    states = workloads.leo_states(257, seed=71)
+    bal = workloads.leo_ballistics(257, seed=71)
+    for engine in ENGINES:
+        fixed = ctx_for(text, order, None, None, engine)
+        for i, v in enumerate((150.0,) * 8 + (0.0,)):
+            assert fixed.cfg.jb_drivers[i] == v
+        with_tables = ctx_for(text, order, sol, dtc, engine)
+        a = fixed.propagate_final(states, EPOCH, 7200.0, ballistic=bal)
+        b = with_tables.propagate_final(states, EPOCH, 7200.0, ballistic=bal)
+        assert (a[1] == 0).all() and (b[1] == 0).all()
+        assert np.array_equal(a[0].view(np.int64), b[0].view(np.int64)), engine
