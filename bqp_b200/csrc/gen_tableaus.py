@@ -20,9 +20,10 @@
   only then), so both sides step with the same binary64 numbers.
 
 Values are emitted as C99 hex-float literals so the header is bit-exact.
-Run: ``python bqp_b200/csrc/gen_tableaus.py [REFERENCE_ROOT]`` (rewrites the
-header in place).
+Run: ``python bqp_b200/csrc/gen_tableaus.py REFERENCE_ROOT`` (or set
+``BQP_REFERENCE_ROOT``; rewrites the header in place).
 """
+import os
 import re
 import sys
 from fractions import Fraction as F
@@ -121,7 +122,10 @@ def emit(name, tab, order, order_err, fsal):
     return "\n".join(lines) + "\n"
 
 
-def main(ref_root: str = "/root/reference"):
+def main(ref_root: str | None = None):
+    ref_root = ref_root or os.environ.get("BQP_REFERENCE_ROOT")
+    if not ref_root:
+        raise SystemExit("usage: gen_tableaus.py REFERENCE_ROOT (or set BQP_REFERENCE_ROOT)")
     out = Path(__file__).with_name("rk_tableaus.h")
     text = [
         "// Generated by gen_tableaus.py -- do not edit by hand.",

@@ -24,8 +24,8 @@ METHOD = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3, "vern9": 4} 
 
 
 def build(force: bool = False) -> Path:
-    src = HERE / "prop_oracle.cpp"
-    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+    srcs = [HERE / "prop_oracle.cpp", HERE / "ref_tableaus.h"]
+    if force or not LIB_PATH.exists() or any(LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB_PATH
 

@@ -61,7 +61,7 @@
 #include <omp.h>
 #endif
 
-#include "../bqp_b200/csrc/rk_tableaus.h"
+#include "ref_tableaus.h"  // the reference's own tables (gen_ref_tableaus.py), not the product's
 
 namespace {
 
@@ -1424,12 +1424,12 @@ struct Tab {
 };
 Tab tableau(int m) {
     if (m == METHOD_DOP853)
-        return {12, 5, 0, bqp_dop853_c, bqp_dop853_a, bqp_dop853_b, bqp_dop853_e, bqp_dop853_e3, 1e-6};
+        return {12, 5, 0, ref_dop853_c, ref_dop853_a, ref_dop853_b, ref_dop853_e, ref_dop853_e3, 1e-6};
     if (m == METHOD_VERN7)  // tableau/vern7.rs: no third-order blend
-        return {10, 6, 0, bqp_vern7_c, bqp_vern7_a, bqp_vern7_b, bqp_vern7_e, nullptr, 0.0};
+        return {10, 6, 0, ref_vern7_c, ref_vern7_a, ref_vern7_b, ref_vern7_e, nullptr, 0.0};
     if (m == METHOD_VERN9)  // tableau/vern9.rs
-        return {16, 8, 0, bqp_vern9_c, bqp_vern9_a, bqp_vern9_b, bqp_vern9_e, nullptr, 0.0};
-    return {7, 4, 1, bqp_dopri5_c, bqp_dopri5_a, bqp_dopri5_b, bqp_dopri5_e, nullptr, 0.0};
+        return {16, 8, 0, ref_vern9_c, ref_vern9_a, ref_vern9_b, ref_vern9_e, nullptr, 0.0};
+    return {7, 4, 1, ref_dopri5_c, ref_dopri5_a, ref_dopri5_b, ref_dopri5_e, nullptr, 0.0};
 }
 
 struct Ctrl {

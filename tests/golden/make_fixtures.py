@@ -23,10 +23,17 @@ repository (the reference tree is not available where the GPU tests run):
 * ``julier7_offsets.json``: the reference's literal sigma-point offsets of the
   7-point Julier simplex (``dust_ukf_rs/src/lib.rs``, JULIER_WHITENED_OFFSETS),
   as bit patterns.
+* ``ref_tableaus.json``: every ``c``, ``a``, ``b``, ``e`` and ``e3`` entry of
+  the reference's DOPRI5, DOP853 (12 active stages), Vern7 and Vern9 tables
+  (``lightyear_odeint_rs/src/odesolve/tableau/*.rs``) as binary64 hex strings,
+  evaluated as Rust evaluates its constant expressions (``rust_tableaus.py``).
+
+The reference root is the first argument or the ``BQP_REFERENCE_ROOT``
+environment variable.
 """
 import json
+import os
 import re
-import shutil
 import struct
 import sys
 from pathlib import Path
@@ -35,19 +42,35 @@ HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 
 
+# Licence attribution carried in the field file itself ('#' lines are
+# comments to the coefficient loaders).
+ATTRIBUTION = """\
+# GOCE DIR Release 6 gravity field (GO_CONS_EGM_GOC_2__20091009T000000_20131020T235959_0201),
+# truncated to degree and order 15; the truncation is the only change.
+# Source: ICGEM, https://icgem.gfz.de/ , DOI 10.5880/ICGEM.2019.004.
+# Licence: Creative Commons Attribution 4.0 International (CC BY 4.0),
+# https://creativecommons.org/licenses/by/4.0/
+# Columns: degree, order, normalised C, normalised S.
+"""
+
+
 def hex_to_f64(h: str) -> float:
     return struct.unpack(">d", bytes.fromhex(h[2:]))[0]
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    ref_root = ref_root or os.environ.get("BQP_REFERENCE_ROOT")
+    if not ref_root:
+        raise SystemExit("usage: make_fixtures.py REFERENCE_ROOT (or set BQP_REFERENCE_ROOT)")
     ref = Path(ref_root) / "dust_transfer"
     crates = ref / "crates"
 
     # 1. DIR-R6 d/o 15 field
     src = crates / "two_phase_transfer_rs/data/spher_const/GO_CONS_GCF_2_DIR_R6_d15.txt"
-    shutil.copyfile(src, HERE / "dir_r6_d15.txt")
+    text = ATTRIBUTION + src.read_text()
+    (HERE / "dir_r6_d15.txt").write_text(text)
     (REPO / "bqp_b200/data").mkdir(parents=True, exist_ok=True)
-    shutil.copyfile(src, REPO / "bqp_b200/data/dir_r6_d15.txt")
+    (REPO / "bqp_b200/data/dir_r6_d15.txt").write_text(text)
 
     # 2. Orekit gravity comparator
     g = json.loads((crates / "lightyear_odeint_rs/tests/data/orekit_dir_r6_5x5_v1.json").read_text())
@@ -140,8 +163,23 @@ def main(ref_root: str = "/root/reference") -> None:
     offs = {"source": "dust_ukf_rs/src/lib.rs (JULIER_WHITENED_OFFSETS)",
             "offsets": rows, "bits": [[struct.pack(">d", v).hex() for v in r] for r in rows]}
     (HERE / "julier7_offsets.json").write_text(json.dumps(offs, indent=1) + "\n")
+
+    # 5. The reference's Runge-Kutta tables, bit for bit
+    sys.path.insert(0, str(HERE))
+    import rust_tableaus
+
+    tabs = rust_tableaus.read_all(ref_root)
+
+    def hx(v):
+        return None if v is None else [float(x).hex() for x in v]
+
+    tab_out = {"source": rust_tableaus.TABLEAU_DIR + "/{dopri5,dop853,dop853_coeffs,vern7,vern9}.rs",
+               "tables": {name: {"stages": len(t["c"]), "c": hx(t["c"]), "a": [hx(r) for r in t["a"]],
+                                 "b": hx(t["b"]), "e": hx(t["e"]), "e3": hx(t["e3"])}
+                          for name, t in tabs.items()}}
+    (HERE / "ref_tableaus.json").write_text(json.dumps(tab_out, indent=1) + "\n")
     print("fixtures written:", len(grav["cases"]), "gravity,", len(cases), "jb2008 cases,",
-          len(lits), "jb2008 literals,", len(rows), "sigma offset rows")
+          len(lits), "jb2008 literals,", len(rows), "sigma offset rows,", len(tabs), "RK tables")
 
 
 if __name__ == "__main__":

@@ -2,6 +2,7 @@
 lightyear_odeint_rs/src/precomputed_ephem.rs): the oracle's loader checks,
 linear interpolation and endpoint rule, and the library's host pass of the
 device lookup against the oracle, bit for bit."""
+import os
 import struct
 from pathlib import Path
 
@@ -12,7 +13,8 @@ from bqp_b200 import _native as N
 from bqp_b200 import workloads
 from oracle import oracle as O
 
-REF_EPH = Path("/root/reference/dust_transfer/crates/lightyear_odeint_rs/data/ephemeris")
+# the reference tree, when the environment names it (BQP_REFERENCE_ROOT)
+REF_EPH = Path(os.environ.get("BQP_REFERENCE_ROOT", "/nonexistent")) / "dust_transfer/crates/lightyear_odeint_rs/data/ephemeris"
 EPS = np.finfo(float).eps
 
 

@@ -8,6 +8,7 @@ DTCFILE rows ``DTC YYYY DDD`` plus 24 hourly dTc values (K).  Lookups apply the
 JB2008 lags (F10/S10 1 day, M10 2, Y10 5) and interpolate dTc hourly with the
 SET rounding.
 """
+import os
 from pathlib import Path
 
 import numpy as np
@@ -18,7 +19,8 @@ from bqp_b200 import workloads
 from oracle import oracle as O
 
 INT32_MIN, INT32_MAX = -(2 ** 31), 2 ** 31 - 1
-REF_DATA = Path("/root/reference/dust_transfer/crates/jb_rs/data/jb2008")
+# the reference tree, when the environment names it (BQP_REFERENCE_ROOT)
+REF_DATA = Path(os.environ.get("BQP_REFERENCE_ROOT", "/nonexistent")) / "dust_transfer/crates/jb_rs/data/jb2008"
 
 
 def solfsmy(days, year=2022, doy0=310, jd0=2459890, values=None, header="synthetic"):

@@ -8,6 +8,7 @@ embedded pair of error order q satisfy  sum_i e_i Phi_i(t) = 0  for |t| <= q
 The tables are binary64 roundings of the published decimals, so each
 condition holds to a tolerance scaled by the size of its terms.
 """
+import os
 import re
 from functools import lru_cache
 from pathlib import Path
@@ -129,3 +130,85 @@ def test_vern7_stage_one_pin():
     assert c[1] == 0.005 and a[1, 0] == 0.005
     assert b[1] == 0.0 and e[1] == 0.0
     assert c[-1] == 1.0 and np.all(a[-1, 7:] == 0.0)  # error stage built on stages 0-6
+
+
+# ---------------------------------------------------------------------------
+# Bit equality with the reference's own tables.  tests/golden/ref_tableaus.json
+# holds every entry of the reference's odesolve/tableau/{dopri5, dop853 +
+# dop853_coeffs, vern7, vern9}.rs as binary64 (make_fixtures.py evaluates the
+# Rust constant expressions); the product header (generated from published
+# fractions and constants) and the oracle's own header (generated from that
+# fixture) must both carry exactly those bits, so neither side can share a
+# wrong weight with the other unnoticed.  This pins the embedded error
+# weights e and DOP853's third-order e3, which the order conditions above
+# only constrain up to the error order.
+
+REF_TABLES = Path(__file__).resolve().parent / "golden" / "ref_tableaus.json"
+ORACLE_HEADER = Path(__file__).resolve().parents[1] / "oracle" / "ref_tableaus.h"
+
+
+def header_arrays(path, prefix, name):
+    text = path.read_text()
+    out = {}
+    for key in ("c", "a", "b", "e", "e3"):
+        m = re.search(rf"{prefix}_{name}_{key}\[\d+\] = \{{(.*?)\}};", text, re.S)
+        out[key] = None if m is None else [float.fromhex(t) for t in m.group(1).replace(",", " ").split()]
+    return out
+
+
+def fixture_arrays(name):
+    import json
+    t = json.loads(REF_TABLES.read_text())["tables"][name]
+    s = t["stages"]
+    flat = []
+    for row in t["a"]:
+        flat += [float.fromhex(x) for x in row] + [0.0] * (s - len(row))
+    conv = lambda v: None if v is None else [float.fromhex(x) for x in v]  # noqa: E731
+    return {"c": conv(t["c"]), "a": flat, "b": conv(t["b"]), "e": conv(t["e"]), "e3": conv(t["e3"])}
+
+
+def bits(v):
+    return [float(x).hex() for x in v]
+
+
+@pytest.mark.parametrize("name", sorted(PAIRS))
+@pytest.mark.parametrize("side", ["product", "oracle"])
+def test_tables_bit_equal_to_reference(name, side):
+    ref = fixture_arrays(name)
+    got = header_arrays(HEADER, "bqp", name) if side == "product" else header_arrays(ORACLE_HEADER, "ref", name)
+    for key in ("c", "a", "b", "e", "e3"):
+        if ref[key] is None:
+            assert got[key] is None, (name, key)
+            continue
+        assert got[key] is not None and len(got[key]) == len(ref[key]), (side, name, key)
+        diff = [i for i, (x, y) in enumerate(zip(bits(got[key]), bits(ref[key]))) if x != y]
+        assert not diff, (side, name, key, diff[:5])
+
+
+def test_reference_shapes():
+    # stage counts and the DOP853 truncation to its 12 active stages (dop853.rs:1-97)
+    import json
+    t = json.loads(REF_TABLES.read_text())["tables"]
+    assert {k: v["stages"] for k, v in t.items()} == {"dopri5": 7, "dop853": 12, "vern7": 10, "vern9": 16}
+    assert t["dop853"]["e3"] is not None and all(t[k]["e3"] is None for k in ("dopri5", "vern7", "vern9"))
+    # Vern9's last stage is built on stages 0-12 only (vern9.rs:213-227)
+    assert len(t["vern9"]["a"][15]) == 13 and len(t["vern7"]["a"][9]) == 7
+
+
+@pytest.mark.skipif(not os.environ.get("BQP_REFERENCE_ROOT"), reason="BQP_REFERENCE_ROOT not set")
+def test_fixture_matches_reference_sources():
+    # re-evaluate the reference's sources when its tree is at hand
+    import sys
+    sys.path.insert(0, str(REF_TABLES.parent))
+    import rust_tableaus
+    tabs = rust_tableaus.read_all(os.environ["BQP_REFERENCE_ROOT"])
+    for name in PAIRS:
+        ref = fixture_arrays(name)
+        t = tabs[name]
+        s = len(t["c"])
+        flat = [x for row in t["a"] for x in row + [0.0] * (s - len(row))]
+        assert bits(flat) == bits(ref["a"]) and bits(t["b"]) == bits(ref["b"]) and bits(t["e"]) == bits(ref["e"])
+        assert bits(t["c"]) == bits(ref["c"])
+        assert (t["e3"] is None) == (ref["e3"] is None)
+        if t["e3"] is not None:
+            assert bits(t["e3"]) == bits(ref["e3"])
