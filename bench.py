@@ -88,6 +88,10 @@ def parse(argv=None):
     ap.add_argument("--method", default="dop853", choices=["dop853", "vern7", "vern9", "dopri5"],
                     help="stepper (the metric's workload: dop853 at eps 1e-12)")
     ap.add_argument("--eps", type=float, default=EPS, help="absolute tolerance, km")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the forms block (split precision and other steppers against plain FP64)")
+    ap.add_argument("--forms-rows", type=int, default=512, help="rows of the 7-day accuracy runs of the forms")
+    ap.add_argument("--forms-days", type=float, default=7.0)
     return ap.parse_args(argv)
 
 
@@ -179,18 +183,30 @@ def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp3
     return cfg
 
 
-def cpu_reference(sample: int, threads: int, segments: int = 1):
-    """Time the CPU oracle (restatement of the reference path) on `sample`
-    trajectories for `segments` rectification segments, all threads."""
-    from bqp_b200 import _native as N
+def bench_config(args) -> dict:
+    """The workload's description, the same dict on both arms (the reference
+    arm's bounded sample is reported beside it, in its own key)."""
+    return {"workload": f"{args.n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
+                        f"{args.method.upper()} eps {args.eps:g}, {args.segment:g} s of the arc per step",
+            "form": form_name(args), "order": ORDER, "trajectories_per_gpu": args.n, "segment_s": args.segment,
+            "method": args.method, "eps_km": args.eps, "l2": "256 MiB write between timed steps"}
+
+
+def cpu_reference(sample: int, threads: int, segments: int = 1, method: str = "dop853", eps: float = EPS,
+                  segment_s: float = SEGMENT_S):
+    """Time the CPU oracle (restatement of the reference path) on the first
+    `sample` trajectories of the workload for `segments` segments, all
+    threads.  Only the oracle runs here: the elements come from its own
+    ECI -> equinoctial conversion, so this path loads no product library."""
     from oracle import oracle as O
 
-    text, states, bal, epoch = make_workload(sample)
-    equ, _ = N.eci_to_equinoctial(states)
+    text, states, bal, epoch = make_workload(N_TRAJ)
+    states, bal = np.ascontiguousarray(states[:sample]), np.ascontiguousarray(bal[:sample])
+    equ = np.array([O.eci2equinoc(s)[0] for s in states])
     F = O.Force(text, ORDER, drag=True, sun=True, moon=True, drivers=DRIVERS)
-    ctl = O.ctrl("dop853", eps=EPS, dt_max=300.0)
+    ctl = O.ctrl(method, eps=eps, dt_max=300.0)
     t0 = time.perf_counter()
-    _, st, steps, evals = O.propagate_final_batch(F, ctl, equ, epoch, SEGMENT_S * segments, bal, threads=threads)
+    _, st, steps, evals = O.propagate_final_batch(F, ctl, equ, epoch, segment_s * segments, bal, threads=threads)
     dt = time.perf_counter() - t0
     return float(evals.sum()) / dt, dt, int(evals.sum()), int((st == 0).sum())
 
@@ -202,19 +218,19 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     evals_s = []
     for i in range(args.warmup + args.steps):
-        v, dt, ev, ok = cpu_reference(args.cpu_sample, threads)
+        v, dt, ev, ok = cpu_reference(args.cpu_sample, threads, method=args.method, eps=args.eps,
+                                      segment_s=args.segment)
         if i >= args.warmup:
             evals_s.append((v, dt))
     value = statistics.median(v for v, _ in evals_s)
     ms = statistics.median(dt for _, dt in evals_s) * 1e3
-    sample = f"{args.cpu_sample} of the {args.n} trajectories, one 5400 s segment per step"
+    sample = f"{args.cpu_sample} of the {args.n} trajectories, one {args.segment:g} s segment per step"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"{args.n} LEO states, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
-                               "DOP853 eps 1e-12, 5400 s Encke segment per step",
-                   "sample": sample},
+        "config": bench_config(args),
+        "sample": {"trajectories": args.cpu_sample, "of": args.n, "segments_per_step": 1},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -269,6 +285,130 @@ def combine_ranks(t_local, evals_local, world, device):
     ev = torch.tensor([float(evals_local)], device=device, dtype=torch.float64)
     dist.all_reduce(ev, op=dist.ReduceOp.SUM)
     return float(tt.item()), float(ev.item())
+
+
+# ------------------------------------------------------------------ forms
+# The propagation forms the metric compares with plain FP64 (DOP853, eps
+# 1e-12 km): split precision (spherical-harmonic degrees above d in FP32) at
+# the tolerance its FP32 noise allows, and the higher-order Verner stepper.
+FORMS = [
+    {"name": "plain FP64, DOP853 eps 1e-10", "method": "dop853", "eps": 1e-10, "split_degree": 0},
+    {"name": "split d>8, DOP853 eps 1e-11", "method": "dop853", "eps": 1e-11, "split_degree": 8},
+    {"name": "split d>16, DOP853 eps 1e-11", "method": "dop853", "eps": 1e-11, "split_degree": 16},
+    {"name": "split d>32, DOP853 eps 1e-11", "method": "dop853", "eps": 1e-11, "split_degree": 32},
+    {"name": "plain FP64, Vern9 eps 1e-10", "method": "vern9", "eps": 1e-10, "split_degree": 0},
+]
+
+
+def form_throughput(f, text, states, bal, epoch, seg, dev, warmup=1, steps=2):
+    """Force evaluations/s and trajectory-days/s of one form on the full
+    batch, device-resident, `steps` segments timed with CUDA events."""
+    import torch
+
+    from bqp_b200 import _native as N
+
+    n = states.shape[0]
+    ctx = N.Context(text, make_config(split_degree=f["split_degree"], method=f["method"], eps=f["eps"]))
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        a = torch.tensor(states, device=dev, dtype=torch.float64)
+        b = torch.empty_like(a)
+        d_bal = torch.tensor(bal, device=dev, dtype=torch.float64)
+        d_tf = torch.full((n,), seg, device=dev, dtype=torch.float64)
+        d_st = torch.empty(n, device=dev, dtype=torch.int32)
+        d_steps = torch.empty(n, device=dev, dtype=torch.int64)
+        d_ev = torch.empty(n, device=dev, dtype=torch.int64)
+        eps_k = [torch.full((n,), epoch + k * seg / 86400.0, device=dev, dtype=torch.float64)
+                 for k in range(warmup + steps)]
+        flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
+        total = torch.zeros((), device=dev, dtype=torch.int64)
+    stream.synchronize()
+    ms = 0.0
+    for k in range(warmup + steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.propagate_final_device(a.data_ptr(), eps_k[k].data_ptr(), d_tf.data_ptr(), b.data_ptr(),
+                                   d_st.data_ptr(), d_steps.data_ptr(), d_ev.data_ptr(), n=n,
+                                   d_ballistic=d_bal.data_ptr())
+        e1.record(stream)
+        if k >= warmup:
+            with torch.cuda.stream(stream):
+                total += d_ev.sum()
+        stream.synchronize()
+        if k >= warmup:
+            ms += e0.elapsed_time(e1)
+        a, b = b, a
+    ok = float((d_st == 0).float().mean().item())
+    ev = int(total.item())
+    ctx.close()
+    return {"force_evals_per_s": ev / (ms * 1e-3), "trajectory_days_per_s": n * seg * steps / 86400.0 / (ms * 1e-3),
+            "evals_per_step": ev / steps, "status_ok_fraction": ok}
+
+
+def form_accuracy_runs(forms, text, states, bal, epoch, days):
+    """Final states of every form (and of plain FP64 at eps 1e-12, the
+    reference) after `days`, each on its own context and stream, all at
+    once: these small batches are latency-bound, so they share the GPU."""
+    import threading
+
+    import torch
+
+    from bqp_b200 import _native as N
+
+    results = {}
+
+    def run(key, f):
+        cfg = make_config(split_degree=f["split_degree"], method=f["method"], eps=f["eps"])
+        cfg.max_kernel_seconds = 3000.0
+        ctx = N.Context(text, cfg)
+        stream = torch.cuda.Stream()
+        ctx.set_stream(stream.cuda_stream)
+        t0 = time.perf_counter()
+        out, st, steps, ev = ctx.propagate_final(states, epoch, days * 86400.0, ballistic=bal)
+        results[key] = (out, st, ev, time.perf_counter() - t0)
+        ctx.close()
+
+    jobs = [("ref", {"method": "dop853", "eps": EPS, "split_degree": 0})] + list(enumerate(forms))
+    threads = [threading.Thread(target=run, args=job) for job in jobs]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    return results
+
+
+def run_forms(args, text, states, bal, epoch, dev, plain):
+    rows = np.linspace(0, states.shape[0] - 1, args.forms_rows).astype(np.int64)
+    sub_s, sub_b = np.ascontiguousarray(states[rows]), np.ascontiguousarray(bal[rows])
+    t0 = time.perf_counter()
+    acc = form_accuracy_runs(FORMS, text, sub_s, sub_b, epoch, args.forms_days)
+    acc_wall = time.perf_counter() - t0
+    ref_out, ref_st, ref_ev, ref_wall = acc["ref"]
+    out = []
+    for i, f in enumerate(FORMS):
+        thr = form_throughput(f, text, states, bal, epoch, args.segment, dev)
+        fo, fst, fev, fwall = acc[i]
+        ok = (fst == 0) & (ref_st == 0)
+        err_m = np.linalg.norm(fo[ok, :3] - ref_out[ok, :3], axis=1) * 1e3
+        emax = float(err_m.max()) if err_m.size else None
+        out.append({
+            "form": f["name"], "method": f["method"], "eps_km": f["eps"], "split_degree": f["split_degree"],
+            **{k: v for k, v in thr.items()},
+            "vs_plain_force_evals_per_s": thr["force_evals_per_s"] / plain["force_evals_per_s"],
+            "vs_plain_trajectory_days_per_s": thr["trajectory_days_per_s"] / plain["trajectory_days_per_s"],
+            "err_m_max": emax, "err_m_median": float(np.median(err_m)) if err_m.size else None,
+            "within_1m": bool(emax is not None and emax <= 1.0 and ok.all()),
+            "evals_vs_plain_7d": float(fev.sum() / ref_ev.sum()), "rows_ok": int(ok.sum()),
+        })
+    return {"reference": f"plain FP64, DOP853 eps {EPS:g} km on the same rows",
+            "accuracy_rows": int(rows.size), "accuracy_days": args.forms_days,
+            "accuracy_wall_s": acc_wall, "reference_evals_7d": int(ref_ev.sum()),
+            "throughput": f"{states.shape[0]} rows, one {args.segment:g} s segment per step, 2 timed steps "
+                          "after 1 warm-up, device-resident",
+            "forms": out}
 
 
 def run_ours(args):
@@ -430,12 +570,10 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
-                                   f"{args.method.upper()} eps {args.eps:g}, {seg:g} s of the arc per step",
-                       "form": form_name(args), "engine": args.engine, "order": ORDER, "trajectories_per_gpu": n,
-                       "segment_s": seg, "l2": "256 MiB write between timed steps",
-                       "evals_per_step": total_evals / args.steps,
-                       "trajectory_days_per_s": world * n * seg / 86400.0 / (t_max * 1e-3 / args.steps)},
+            "config": bench_config(args),
+            "engine": args.engine,
+            "evals_per_step": total_evals / args.steps,
+            "trajectory_days_per_s": world * n * seg / 86400.0 / (t_max * 1e-3 / args.steps),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(dom, n),
@@ -453,6 +591,10 @@ def run_ours(args):
             "gpu_launches": launches,
             "status_ok_fraction": float((status_last == 0).mean()),
         }
+        if not args.no_forms and world == 1 and args.segment == SEGMENT_S and args.method == "dop853" \
+                and args.eps == EPS and not args.split_degree and args.engine == "pipeline":
+            plain = {"force_evals_per_s": value, "trajectory_days_per_s": line["trajectory_days_per_s"]}
+            line["forms"] = run_forms(args, text, states, bal, epoch, dev, plain)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

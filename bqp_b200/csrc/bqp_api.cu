@@ -1040,6 +1040,9 @@ int bqp_ctx_create(const char* text, int64_t len, const bqp_force_config* cfg, b
             if (e != cudaSuccess) rc = cuda_fail(e, "JB2008 fit upload");
         }
     }
+    // the drag sweep fits are built here, where allocating is allowed, so the
+    // allocation-free entry point finds them current
+    if (!rc) rc = ensure_fit2(ctx);
     if (rc) {
         bqp_ctx_destroy(ctx);
         return rc;
@@ -1126,7 +1129,7 @@ int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_le
     };
     if (!solfsmy && !dtcfile) {
         drop();
-        return 0;
+        return ensure_fit2(ctx);
     }
     SpaceWeather sw;
     const std::string why = parse_space_weather(solfsmy, solfsmy_len, dtcfile, dtcfile_len, &sw);
@@ -1146,7 +1149,7 @@ int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_le
     ctx->sw_span[0] = jd_lo;
     ctx->sw_span[1] = jd_hi;
     ctx->dtab = {ctx->d_sw_solar, ctx->d_sw_dtc, ctx->sw.first_jd, ctx->sw.n_solar, ctx->sw.n_dtc, ctx->sw.dtc_first};
-    return 0;
+    return ensure_fit2(ctx);
 }
 
 int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out, int32_t* ok) {
@@ -1276,9 +1279,9 @@ int bqp_ctx_set_config(bqp_ctx* ctx, const bqp_force_config* cfg) {
     ctx->cfg = *cfg;
     if (cfg->order != old || cfg->split_degree != old_split) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-        return upload_table(ctx);
+        if ((rc = upload_table(ctx))) return rc;
     }
-    return 0;
+    return ensure_fit2(ctx);
 }
 
 int bqp_gravity_eval_device(bqp_ctx* ctx, int64_t n, const double* pos, double* acc, int32_t* status) {
@@ -1566,6 +1569,14 @@ int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32
                                 const double* epoch_jd, double t0, const double* tf, const double* ballistic,
                                 double* out, int32_t* status, int64_t* steps, int64_t* evals) {
     if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    // this path runs the persistent kernel on the FP64 field; a context set
+    // up for a form only the stage-synchronous engine has is refused, not
+    // run in plain FP64
+    if (ctx->cfg.split_degree || ctx->cfg.surrogate || ctx->cfg.drag_fp32)
+        return fail(BQP_E_UNSUPPORTED,
+                    "the no-allocation entry point runs plain FP64 only; this context is configured for %s",
+                    ctx->cfg.surrogate ? "the learned surrogate" : ctx->cfg.split_degree ? "split precision"
+                                                                                     : "the FP32 density");
     int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
     if (rc) return rc;
     if (n > BQP_NOALLOC_MAX_TRAJ)
@@ -1624,8 +1635,30 @@ int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32
     A.ncells = ctx->ncells;
     A.use_smem = ctx->use_smem;
     A.force = force_params(ctx);
+    // the sweep fits are built with the context and rebuilt by the calls that
+    // change them; if they are not current the quadrature runs instead (the
+    // same densities within the fits' 1e-13), never stale fits
+    if (!ctx->fit2_built) A.force.fit2 = nullptr;
     A.ctrl = ctrl_params(ctx);
+    // event create/record allocate no device memory
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (ctx->profile) {
+        cudaEventCreate(&ev[0]);
+        cudaEventCreate(&ev[1]);
+        cudaEventRecord(ev[0], s);
+    }
     e = launch_propagate(A, ctx->cfg.method, 256, 0, s);
+    if (ctx->profile) {
+        cudaEventRecord(ev[1], s);
+        float ms = 0.0f;
+        if (e == cudaSuccess && cudaEventSynchronize(ev[1]) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) {
+            ctx->times.ms[kKcPersistent] += ms;
+            ctx->times.launches[kKcPersistent] += 1;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "k_propagate launch (no-allocation path)");
 
     e = cudaMemcpyAsync(out, dout, b6, cudaMemcpyDeviceToHost, s);

@@ -16,12 +16,24 @@ namespace bqp {
 
 // opt-in shared memory per CTA, less room for the static mbarrier
 constexpr size_t kSmemPerBlock = 227 * 1024 - 64;
-constexpr uint64_t kStageWaitNs = 1000000000ull;  // 1 s bound on the table copy
+constexpr uint64_t kStageWaitNs = 1000000000ull;   // 1 s bound on the table copy
+constexpr uint64_t kStageDrainNs = 2000000000ull;  // after a timeout: 2 s more for the copy to land
+
+// Sticky flag of this translation unit's gravity kernels: set when a CTA's
+// table copy did not land within kStageWaitNs.  Every later CTA (of this and
+// later launches) then stages nothing and reports its rows lost, so no CTA
+// starts on an SM where an earlier CTA's copy may still be writing shared
+// memory.  It stays set until the process exits: a bulk copy that takes
+// seconds means the device is not in a state to trust.
+static __device__ unsigned int g_stage_fault = 0u;
 
 // Copy `bytes` (a multiple of 16; both addresses 16-byte aligned) from global
 // to shared memory with the bulk-copy engine, completion signalled on an
 // mbarrier.  Thread 0 issues the copy; every thread waits for at most
 // kStageWaitNs; all get false if any thread saw the copy unfinished then.
+// On that failure the CTA sets g_stage_fault and thread 0 keeps the CTA
+// resident for up to kStageDrainNs more, until the copy has landed, so the
+// CTA does not exit with its copy in flight unless the copy never completes.
 __device__ __forceinline__ bool bulk_stage(void* smem_dst, const void* gsrc, uint32_t bytes) {
     __shared__ __align__(8) uint64_t bar;
     const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&bar);
@@ -30,7 +42,10 @@ __device__ __forceinline__ bool bulk_stage(void* smem_dst, const void* gsrc, uin
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
+    // one read of the sticky flag decides for the whole CTA
+    const bool faulted =
+        __syncthreads_or(threadIdx.x == 0 && *static_cast<volatile unsigned int*>(&g_stage_fault) != 0u);
+    if (faulted) return false;
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
         constexpr uint32_t kChunk = 32768;
@@ -57,7 +72,24 @@ __device__ __forceinline__ bool bulk_stage(void* smem_dst, const void* gsrc, uin
     }
     // one verdict for the whole CTA (a thread may give up just before the
     // copy lands while another sees it land)
-    return !__syncthreads_or(done == 0);
+    if (!__syncthreads_or(done == 0)) return true;
+    if (threadIdx.x == 0) {
+        atomicExch(&g_stage_fault, 1u);
+        const uint64_t t1 = global_ns();
+        for (uint32_t it = 0;; ++it) {
+            uint32_t landed;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, "
+                "0, p;\n\t}"
+                : "=r"(landed)
+                : "r"(bar_a)
+                : "memory");
+            if (landed) break;
+            if ((it & 255u) == 255u && global_ns() - t1 > kStageDrainNs) break;
+        }
+    }
+    __syncthreads();
+    return false;
 }
 constexpr int kGravityPartsMax = 4;
 

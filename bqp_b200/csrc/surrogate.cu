@@ -351,6 +351,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     };
     uint32_t ph_mma = 0, ph_w = 0;
     bool ok = true;
+    // a weight copy / an MMA commit issued and not yet seen complete: on a
+    // failed wait the CTA drains them before it frees tensor memory and exits
+    bool w_out = true, mma_out = false;
     if (threadIdx.x == 0) load_w(0);
 
     for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -391,6 +394,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                 ok = false;
                 break;
             }
+            w_out = false;
             if (threadIdx.x == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -408,15 +412,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                                  bar_mma)
                              : "memory");
             }
+            mma_out = true;
             ok = tc::mbar_wait(bar_mma, ph_mma);
             ph_mma ^= 1u;
             if (!__syncthreads_and(ok)) {
                 ok = false;
                 break;
             }
+            mma_out = false;
             // the weights are free: start the next layer's (or the next tile's first)
             const bool more = l < 2 || tile + (int64_t)gridDim.x < ntiles;
             if (threadIdx.x == 0 && more) load_w(l < 2 ? l + 1 : 0);
+            w_out = more;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
             for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
@@ -465,7 +472,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
         __syncthreads();
     }
-    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    if (!ok && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // keep the CTA (its shared and tensor memory) until what it issued
+        // has landed, each for at most the bound of tc::mbar_wait; the
+        // phases were flipped after the wait that failed
+        if (w_out) tc::mbar_wait(bar_w, ph_w ^ 1u);
+        if (mma_out) tc::mbar_wait(bar_mma, ph_mma ^ 1u);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)

@@ -122,13 +122,16 @@ __device__ __forceinline__ void gemm_tile(const __nv_bfloat16* __restrict__ A, c
 
     const int nk = K / kBK;
     uint32_t phase[2] = {0, 0};
+    bool pending[2] = {false, false};  // a commit on this buffer's barrier not yet seen complete
     bool ok = true;
     for (int s = 0; s < nk && ok; ++s) {
         const int buf = s & 1;
         if (s >= 2) {  // the MMAs that read this buffer two stages ago
-            ok = mbar_wait(bar_a[buf], phase[buf]);
-            phase[buf] ^= 1u;
+            // one verdict for the CTA, so every thread takes the same path
+            ok = __syncthreads_and(mbar_wait(bar_a[buf], phase[buf]));
             if (!ok) break;
+            phase[buf] ^= 1u;
+            pending[buf] = false;
         }
         load_stage(A, B, K, m0, n0, s * kBK, sa[buf], sb[buf]);
         // make the generic-proxy stores visible to the tensor cores
@@ -155,17 +158,26 @@ __device__ __forceinline__ void gemm_tile(const __nv_bfloat16* __restrict__ A, c
                              bar_a[buf])
                          : "memory");
         }
+        pending[buf] = true;
     }
     // drain: the last one or two commits
     if (ok) {
         for (int s = (nk >= 2 ? nk - 2 : 0); s < nk && ok; ++s) {
             const int buf = s & 1;
-            ok = mbar_wait(bar_a[buf], phase[buf]);
+            ok = __syncthreads_and(mbar_wait(bar_a[buf], phase[buf]));
+            if (!ok) break;
             phase[buf] ^= 1u;
+            pending[buf] = false;
         }
     }
-    if (!__syncthreads_and(ok)) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
+    if (!ok) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            // keep shared and tensor memory until the MMAs issued on them
+            // have completed, each for at most the same bound
+            for (int b = 0; b < 2; ++b)
+                if (pending[b]) mbar_wait(bar_a[b], phase[b]);
+        }
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int row = warp * 32 + (threadIdx.x & 31);

@@ -18,9 +18,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import _native as N
-
 RE_KM = 6378.137
+MU_KM3_S2 = 398600.4415  # the reference's mu (satpy_core/src/lib.rs:74)
 EPOCH_JD = 2460310.5  # 2024-01-01T00:00 UTC, the reference smoke test's epoch
 
 
@@ -48,10 +47,34 @@ def mean_to_true(M: np.ndarray, e: np.ndarray) -> np.ndarray:
     return 2.0 * np.arctan2(np.sqrt(1 + e) * np.sin(E / 2), np.sqrt(1 - e) * np.cos(E / 2))
 
 
+def kep_to_eci(kep: np.ndarray, mu: float = MU_KM3_S2) -> np.ndarray:
+    """[a km, e, i, RAAN, argp, true anomaly (deg)] -> ECI [n][6]: the
+    perifocal position and velocity rotated by R3(-RAAN) R1(-i) R3(-argp).
+    Plain numpy, so generating a workload loads no native library."""
+    kep = np.asarray(kep, dtype=np.float64).reshape(-1, 6)
+    a, e = kep[:, 0], kep[:, 1]
+    inc, raan, argp, nu = (np.radians(kep[:, k]) for k in (2, 3, 4, 5))
+    p = a * (1.0 - e * e)
+    cn, sn = np.cos(nu), np.sin(nu)
+    r = p / (1.0 + e * cn)
+    sp = np.sqrt(mu / p)
+    xp, yp = r * cn, r * sn
+    vxp, vyp = -sp * sn, sp * (e + cn)
+    cO, sO, cw, sw, ci, si = np.cos(raan), np.sin(raan), np.cos(argp), np.sin(argp), np.cos(inc), np.sin(inc)
+    r00, r01 = cO * cw - sO * sw * ci, -cO * sw - sO * cw * ci
+    r10, r11 = sO * cw + cO * sw * ci, -sO * sw + cO * cw * ci
+    r20, r21 = sw * si, cw * si
+    out = np.stack([r00 * xp + r01 * yp, r10 * xp + r11 * yp, r20 * xp + r21 * yp,
+                    r00 * vxp + r01 * vyp, r10 * vxp + r11 * vyp, r20 * vxp + r21 * vyp], axis=1)
+    bad = ~((a > 0.0) & (e >= 0.0) & (e < 1.0))
+    out[bad] = np.nan
+    return np.ascontiguousarray(out)
+
+
 def kep_states(a, e, i_deg, raan_deg, argp_deg, M_deg) -> np.ndarray:
     nu = np.degrees(mean_to_true(np.radians(M_deg), e)) % 360.0
     kep = np.stack([a, e, i_deg, raan_deg, argp_deg, nu], axis=1)
-    return N.kep_to_eci(kep)
+    return kep_to_eci(kep)
 
 
 def leo_states(n: int, seed: int = 0) -> np.ndarray:

@@ -251,7 +251,14 @@ int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in,
  * whole device -- and who still want host buffers in and out.
  *
  * Same arguments, results and per-row status as bqp_propagate_final, always
- * on the persistent kernel (whatever cfg.engine says).  The inputs and
+ * on the persistent kernel (whatever cfg.engine says) with the plain FP64
+ * field: a context configured for split precision, the learned surrogate or
+ * the FP32 density (forms only the stage-synchronous engine runs) is refused
+ * with BQP_E_UNSUPPORTED.  The JB2008 sweep fits it uses are the ones the
+ * context built when it was created or last reconfigured (bqp_ctx_set_config,
+ * bqp_ctx_set_jb_drivers), so identical calls give identical bits whatever
+ * was called in between.  With bqp_ctx_profile on, its kernel time counts
+ * under BQP_KCLASS_PERSISTENT.  The inputs and
  * outputs are staged through one fixed device array inside the library, of
  * room for BQP_NOALLOC_MAX_TRAJ rows (about 2.3 MiB), which every GPU that
  * loads the library holds until the process exits; n above that limit is

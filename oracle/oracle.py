@@ -56,6 +56,8 @@ def lib():
                               C.c_double, _dp, _dp]
         L.orc_propagate_final_batch.argtypes = [C.c_void_p, _dp, C.c_long, _dp, _dp, _dp, _dp,
                                                 _dp, _ip, _lp, _lp, C.c_int]
+        L.orc_propagate_sampled_batch.argtypes = [C.c_void_p, _dp, C.c_long, _dp, _dp, _dp, _dp, _dp, C.c_int,
+                                                  _dp, _ip, _lp, _lp, _ip, C.c_int]
         L.orc_propagate_sampled.restype = C.c_int
         L.orc_propagate_sampled.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double,
                                             C.c_double, C.c_double, _dp, C.c_int, _dp, _lp, _ip]
@@ -205,6 +207,28 @@ def propagate_sampled(force: Force, ctl, eq0, epoch_jd, tf, am, cd, t_eval):
                                      _d(t_eval), t_eval.size, _d(out), se.ctypes.data_as(_lp),
                                      C.byref(nw))
     return out, st, int(se[0]), int(se[1]), nw.value
+
+
+def propagate_sampled_batch(force: Force, ctl, eq0, epoch_jd, tf, ballistic, t_eval, threads=0):
+    """Sampled path of n rows on one grid, all host threads: (delta [n][n_t][6]
+    against each row's initial baseline, status[n], steps[n], evals[n],
+    samples written[n])."""
+    eq0 = f64(eq0).reshape(-1, 6)
+    n = eq0.shape[0]
+    epoch_jd = f64(np.broadcast_to(epoch_jd, (n,)))
+    tf = f64(np.broadcast_to(tf, (n,)))
+    ballistic = f64(np.broadcast_to(ballistic, (n, 2)))
+    t_eval = f64(t_eval)
+    out = np.empty((n, t_eval.size, 6))
+    status = np.zeros(n, dtype=np.int32)
+    steps = np.zeros(n, dtype=np.int64)
+    evals = np.zeros(n, dtype=np.int64)
+    nw = np.zeros(n, dtype=np.int32)
+    lib().orc_propagate_sampled_batch(force.h, _d(f64(ctl)), n, _d(eq0), _d(epoch_jd), _d(tf), _d(ballistic),
+                                      _d(t_eval), t_eval.size, _d(out), status.ctypes.data_as(_ip),
+                                      steps.ctypes.data_as(_lp), evals.ctypes.data_as(_lp),
+                                      nw.ctypes.data_as(_ip), int(threads))
+    return out, status, steps, evals, nw
 
 
 def integrate_segment(force: Force, ctl, eq, jd0, am, cd, t0, tf):

@@ -2248,6 +2248,31 @@ int orc_propagate_sampled(void* f, const double* ctrl, const double* eq0, double
     return s;
 }
 
+// Sampled path for a batch on one grid (one trajectory per OpenMP iteration):
+// eq0 [n][6], epoch_jd[n], tf[n], ballistic [n][2]; t_eval[n_t] common to
+// every row (each row writes the samples up to its own tf).  delta_out
+// [n][n_t][6], status[n], steps/evals[n], n_written[n].
+void orc_propagate_sampled_batch(void* f, const double* ctrl, long n, const double* eq0,
+                                 const double* epoch_jd, const double* tf, const double* ballistic,
+                                 const double* t_eval, int n_t, double* delta_out, int* status, long* steps,
+                                 long* evals, int* n_written, int threads) {
+    Force* F = (Force*)f;
+    Ctrl C = ctrl_from(ctrl);
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long i = 0; i < n; ++i) {
+        Job J{F, C, epoch_jd[i], ballistic[2 * i], ballistic[2 * i + 1]};
+        Stats st;
+        double* out = delta_out + (size_t)i * n_t * 6;
+        for (long q = 0; q < (long)n_t * 6; ++q) out[q] = NAN;
+        status[i] = propagate_sampled(J, eq0 + 6 * i, 0.0, tf[i], t_eval, n_t, out, st, &n_written[i]);
+        steps[i] = st.steps;
+        evals[i] = st.evals;
+    }
+}
+
 // One fixed-time integration without rectification (for solver tests):
 // integrates the Encke delta from 0 over [t0, tf] against baseline eq.
 int orc_integrate_segment(void* f, const double* ctrl, const double* eq, double jd0, double am,

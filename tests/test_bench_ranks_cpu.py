@@ -73,3 +73,27 @@ def test_reference_arm_works_on_rank_zero_only(monkeypatch, capsys):
     args = bench.parse(["--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3"])
     assert bench.run_reference(args) is None
     assert not called and capsys.readouterr().out == ""
+
+
+def test_reference_arm_runs_only_the_oracle():
+    # the reference arm times the CPU restatement alone: the product's native
+    # library must not be loaded by that process, and its config is the GPU
+    # arm's config (its sample in a key of its own)
+    import json
+    import subprocess
+
+    code = (
+        "import sys, json; sys.path.insert(0, %r); import bench\n"
+        "args = bench.parse(['--impl', 'reference', '--steps', '1', '--warmup', '0', '--cpu-sample', '2',"
+        " '--segment', '120'])\n"
+        "bench.run_reference(args)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'native_loaded': 'libbqp_b200' in maps, 'oracle_loaded': 'libprop_oracle' in maps,"
+        " 'config': bench.bench_config(args)}))\n" % str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    line, probe = lines[0], lines[1]
+    assert not probe["native_loaded"] and probe["oracle_loaded"]
+    assert line["impl"] == "reference" and line["config"] == probe["config"]
+    assert line["sample"]["trajectories"] == 2 and line["value"] > 0

@@ -1,0 +1,178 @@
+"""Parity at the sizes of the benchmark configurations: CUDA path against the
+oracle on the same seeded inputs, through the C ABI.
+
+* 1-day configuration in full: 1,024 states (seed 0), synthetic 20x20 field,
+  no drag, DOPRI5(4) with the solver's scaled error control rtol 1e-10 /
+  atol 1e-9 km, 1 day sampled on the 60 s grid (1,441 samples), both engines.
+* 7-day configuration, a 64-row sample of the benchmark's 65,536 rows (every
+  1,024th): 70x70 field + JB2008 drag + Sun/Moon, DOP853 eps 1e-12 km, 7 days,
+  stage-synchronous engine (the benchmark's engine; the persistent kernel runs
+  one row per thread at ~1.4e3 evaluations/s, so a 7-day row at eps 1e-12,
+  ~7.6e5 evaluations, would take it ~9 minutes).
+* Sigma-point configuration, a 64-object sample: 13 scaled points (alpha
+  1e-3, beta 2, kappa 0) of random SPD covariances, adaptive DOP853 eps
+  1e-12 km, 70x70 + drag, one orbital period, recombined on the device.
+
+Each test prints its measured figures (run pytest with -s to see them).
+"""
+import os
+import threading
+
+import numpy as np
+import pytest
+
+from bqp_b200 import _native as N
+from bqp_b200 import workloads
+from oracle import oracle as O
+from oracle import ukf as U
+
+pytestmark = pytest.mark.gpu
+
+EPOCH = workloads.EPOCH_JD
+DRIVERS = (150.0,) * 8 + (20.0,)
+
+
+def make_ctx(text, order, flags, method, engine="pipeline", eps=None, rtol=None, atol=None,
+             max_kernel_seconds=1800.0):
+    cfg = N.default_config()
+    cfg.engine = N.ENGINES[engine]
+    cfg.order = order
+    cfg.force_flags = flags
+    cfg.atm_model = 4
+    cfg.method = N.METHODS[method]
+    cfg.dt_max = 300.0
+    for i, v in enumerate(DRIVERS):
+        cfg.jb_drivers[i] = v
+    if rtol is not None:
+        cfg.error_control = 1
+        cfg.rtol, cfg.atol = rtol, atol
+    else:
+        cfg.eps = eps
+    cfg.max_kernel_seconds = max_kernel_seconds
+    return N.Context(text, cfg)
+
+
+def oracle_equ(states):
+    out = np.empty_like(states)
+    for i, s in enumerate(states):
+        out[i], rc = O.eci2equinoc(s)
+        assert rc == 0
+    return out
+
+
+def in_thread(fn, *args):
+    """Run the oracle (ctypes releases the GIL) while the GPU works, leaving
+    two host cores to the thread that drives the GPU."""
+    box = {}
+    threads = max(1, (os.cpu_count() or 1) - 2)
+
+    def run():
+        box["out"] = fn(*args, threads=threads)
+
+    t = threading.Thread(target=run)
+    t.start()
+    return t, box
+
+
+@pytest.mark.parametrize("engine", ["pipeline", "persistent"])
+def test_one_day_configuration_in_full(engine):
+    order, n = 20, 1024
+    rtol, atol = 1e-10, 1e-9
+    text = workloads.synthetic_field(order)
+    states = workloads.leo_states(n, seed=0)
+    equ = oracle_equ(states)
+    tf = 86400.0
+    grid = np.arange(0.0, tf + 1.0, 60.0)
+    assert grid.size == 1441 and grid[-1] == tf
+    F = O.Force(text, order, drivers=DRIVERS)
+    th, box = in_thread(O.propagate_sampled_batch, F, O.ctrl("dopri5_solver", rtol=rtol, atol=atol), equ, EPOCH,
+                        tf, np.array([0.01, 2.2]), grid)
+    ctx = make_ctx(text, order, 0, "dopri5_solver", engine=engine, rtol=rtol, atol=atol)
+    got, st, steps, evals = ctx.propagate_sampled(states, EPOCH, tf, grid)
+    th.join()
+    d, rst, rsteps, revals, nw = box["out"]
+    assert (st == 0).all() and (rst == 0).all() and (nw == grid.size).all()
+    base = np.array([[O.equinoc2eci(equ[i], t)[0] for t in grid] for i in range(n)])
+    err = np.linalg.norm(got[:, :, :3] - (base + d)[:, :, :3], axis=2)  # [n][1441] km
+    # each solution lies within ~10 local tolerances per step of the exact
+    # one; the local tolerance of the scaled control is atol + rtol |y|, with
+    # |y| the Encke deviation (below the 10 km rectification threshold)
+    bound = 2 * 10 * steps * (atol + rtol * 10.0)
+    worst = (err.max(axis=1) / bound).max()
+    print(f"\n1-day configuration, {engine}: {n} rows x {grid.size} samples; max |dr| {err.max():.3e} km, "
+          f"median {np.median(err):.3e} km, worst share of the bound {worst:.3f}; steps GPU {steps.sum()} "
+          f"oracle {rsteps.sum()}; evaluations GPU {evals.sum()} oracle {revals.sum()}")
+    assert worst <= 1.0, worst
+    rel = np.abs(steps - rsteps) / rsteps
+    assert np.median(rel) <= 0.02 and rel.max() <= 0.1, (np.median(rel), rel.max())
+    # the grid starts at the input state
+    assert np.allclose(got[:, 0], states, rtol=0, atol=1e-9)
+
+
+def test_seven_day_configuration_sample():
+    order = 70
+    text = workloads.synthetic_field(order)
+    all_states = workloads.leo_states(65536, seed=0)
+    all_bal = workloads.leo_ballistics(65536, seed=0)
+    rows = np.arange(0, 65536, 1024)
+    states, bal = np.ascontiguousarray(all_states[rows]), np.ascontiguousarray(all_bal[rows])
+    n = rows.size
+    equ = oracle_equ(states)
+    tf = 7 * 86400.0
+    F = O.Force(text, order, drag=True, sun=True, moon=True, drivers=DRIVERS)
+    th, box = in_thread(O.propagate_final_batch, F, O.ctrl("dop853", eps=1e-12), equ, EPOCH, tf, bal)
+    ctx = make_ctx(text, order, N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON, "dop853", eps=1e-12)
+    got, st, steps, evals = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    th.join()
+    d, rst, rsteps, revals = box["out"]
+    assert (st == 0).all() and (rst == 0).all()
+    ref = np.array([O.equinoc2eci(equ[i], tf)[0] for i in range(n)]) + d
+    err_m = np.linalg.norm(got[:, :3] - ref[:, :3], axis=1) * 1e3
+    print(f"\n7-day configuration sample: {n} rows; |dr| max {err_m.max():.4f} m, median {np.median(err_m):.5f} m; "
+          f"evaluations GPU {evals.sum()} oracle {revals.sum()}")
+    # the metric's own accuracy bound: within 1 m of the FP64 oracle after 7 days
+    assert err_m.max() <= 1.0, err_m.max()
+    assert np.median(err_m) <= 0.05, np.median(err_m)
+    rel = np.abs(evals - revals) / revals
+    assert np.median(rel) <= 0.02 and rel.max() <= 0.1, (np.median(rel), rel.max())
+
+
+def test_sigma_point_configuration_sample():
+    order, flags = 70, N.FORCE_DRAG
+    text = workloads.synthetic_field(order)
+    n, alpha, beta, kappa = 64, 1e-3, 2.0, 0.0
+    mean, cov = workloads.ukf_objects(n, seed=0)
+    bal = workloads.leo_ballistics(n, seed=0)
+    tf = workloads.orbit_period_s(mean)
+    eps = 1e-12
+    # oracle: the restated sigma set, every row propagated, then recombined
+    wm, wc, _ = U.weights("merwe13", alpha, beta, kappa)
+    sig = np.stack([U.get_sigmas(mean[i], cov[i], "merwe13", alpha, beta, kappa) for i in range(n)])  # [n][13][6]
+    S = sig.shape[1]
+    rows = sig.reshape(-1, 6)
+    equ = oracle_equ(rows)
+    F = O.Force(text, order, drag=True, drivers=DRIVERS)
+    th, box = in_thread(O.propagate_final_batch, F, O.ctrl("dop853", eps=eps), equ, EPOCH, np.repeat(tf, S),
+                        np.repeat(bal, S, axis=0))
+    ctx = make_ctx(text, order, flags, "dop853", eps=eps)
+    m, c, st, ev = ctx.sigma_propagate(mean, cov, EPOCH, tf, sigma_set="merwe13", alpha=alpha, beta=beta,
+                                       kappa=kappa, ballistic=bal)
+    th.join()
+    d, rst, _, revals = box["out"]
+    assert (st == 0).all() and (rst == 0).all()
+    out = np.array([O.equinoc2eci(equ[k], tf[k // S])[0] for k in range(equ.shape[0])]) + d
+    om = np.empty((n, 6))
+    oc = np.empty((n, 6, 6))
+    for i in range(n):
+        om[i], oc[i] = U.rebuild_mean_covar(out[i * S:(i + 1) * S], wm, wc)
+    frob = np.linalg.norm(c - oc, axis=(1, 2)) / np.linalg.norm(oc, axis=(1, 2))
+    dmean = np.linalg.norm(m[:, :3] - om[:, :3], axis=1)
+    print(f"\nsigma-point configuration sample: {n} objects x {S} points; covariance Frobenius error "
+          f"max {frob.max():.3e}, median {np.median(frob):.3e} (relative); mean |dr| max {dmean.max():.3e} km; "
+          f"evaluations GPU {ev.sum()} oracle {revals.sum()}")
+    # at alpha = 1e-3 the mean weights are ~-1e6 (centre) and ~8e4 (others):
+    # the rows' independent integration errors (~1e-9 km at eps 1e-12 over
+    # one period) reach the mean multiplied by ~1e6
+    assert dmean.max() <= 1e-2, dmean.max()
+    assert frob.max() <= 1e-3, frob.max()
+    assert np.allclose(c, np.transpose(c, (0, 2, 1)), rtol=0, atol=0)

@@ -162,3 +162,32 @@ def test_space_weather_and_ephemeris_arguments():
         api._ephemeris((b"s",))
     with pytest.raises(ValueError, match="body"):
         api._ephemeris({"mars": b"x"})
+
+
+def test_workload_kep_to_eci_matches_library():
+    # the workload generator's numpy conversion (no native library needed)
+    # and the library's host kep_to_eci agree to rounding
+    rng = np.random.default_rng(1)
+    n = 1000
+    kep = np.stack([rng.uniform(6700, 42000, n), rng.uniform(0, 0.8, n), rng.uniform(0, 180, n),
+                    rng.uniform(0, 360, n), rng.uniform(0, 360, n), rng.uniform(0, 360, n)], 1)
+    a = workloads.kep_to_eci(kep)
+    b = N.kep_to_eci(kep)
+    assert np.all(np.abs(a - b) <= 1e-15 * np.abs(b).max(axis=1, keepdims=True))
+
+
+def test_oracle_sampled_batch_equals_rows():
+    order = 8
+    text = workloads.synthetic_field(order)
+    F = O.Force(text, order, drag=True, sun=True, moon=True)
+    states = workloads.leo_states(5, seed=2)
+    bal = workloads.leo_ballistics(5, seed=2)
+    equ = np.array([O.eci2equinoc(s)[0] for s in states])
+    grid = np.arange(0.0, 1801.0, 60.0)
+    ctl = O.ctrl("dop853", eps=1e-9)
+    d, st, steps, evals, nw = O.propagate_sampled_batch(F, ctl, equ, workloads.EPOCH_JD, 1800.0, bal, grid)
+    for i in range(5):
+        di, si, stp, ev, nwi = O.propagate_sampled(F, ctl, equ[i], workloads.EPOCH_JD, 1800.0, bal[i, 0], bal[i, 1],
+                                                   grid)
+        assert si == st[i] == 0 and nwi == nw[i] == grid.size
+        assert np.array_equal(di, d[i]) and stp == steps[i] and ev == evals[i]

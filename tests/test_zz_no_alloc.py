@@ -75,3 +75,53 @@ def test_noalloc_rejects_more_rows_than_its_array_holds():
     # the limit itself is accepted
     out, st, _, _ = ctx.propagate_final_noalloc(states[:N.NOALLOC_MAX_TRAJ], EPOCH, 60.0)
     assert (st == 0).all() and np.isfinite(out).all()
+
+
+def test_noalloc_refuses_forms_it_would_not_run():
+    # split precision and the surrogate live in the stage-synchronous engine;
+    # the allocation-free path must refuse them, not run plain FP64 instead
+    order = 20
+    text = workloads.synthetic_field(order)
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.split_degree = 8
+    ctx = N.Context(text, cfg)
+    s = workloads.leo_states(4, seed=3)
+    with pytest.raises(N.NativeError) as e:
+        ctx.propagate_final_noalloc(s, EPOCH, 600.0)
+    assert e.value.code == N.E_UNSUPPORTED and "split precision" in str(e.value)
+    # the same context without the split form runs
+    cfg.split_degree = 0
+    ctx.set_config(cfg)
+    out, st, _, _ = ctx.propagate_final_noalloc(s, EPOCH, 600.0)
+    assert (st == 0).all() and np.isfinite(out).all()
+
+
+def test_noalloc_bits_do_not_depend_on_call_history():
+    # the drag sweep fits are built with the context, so a first no-allocation
+    # call on a fresh context, one after a host-buffer call and one after the
+    # drivers were reset give the same bits
+    order = 20
+    text = workloads.synthetic_field(order)
+    ctx = make_ctx(text, order)
+    s = workloads.leo_states(64, seed=44)
+    b = workloads.leo_ballistics(64, seed=44)
+    first = ctx.propagate_final_noalloc(s, EPOCH, 3000.0, ballistic=b)
+    ctx.propagate_final(s, EPOCH, 3000.0, ballistic=b)
+    second = ctx.propagate_final_noalloc(s, EPOCH, 3000.0, ballistic=b)
+    ctx.set_jb_drivers(None, None)
+    third = ctx.propagate_final_noalloc(s, EPOCH, 3000.0, ballistic=b)
+    assert (first[1] == 0).all()
+    for other in (second, third):
+        assert np.array_equal(first[0], other[0]) and np.array_equal(first[1], other[1])
+        assert np.array_equal(first[2], other[2]) and np.array_equal(first[3], other[3])
+
+
+def test_noalloc_kernel_time_is_profiled():
+    text = workloads.synthetic_field(8)
+    ctx = make_ctx(text, 8)
+    ctx.profile(True)
+    ctx.propagate_final_noalloc(workloads.leo_states(32, seed=5), EPOCH, 600.0)
+    ms, launches = ctx.profile_read()["persistent"]
+    ctx.profile(False)
+    assert launches == 1 and ms > 0.0
