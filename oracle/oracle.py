@@ -41,6 +41,7 @@ def lib():
         L.orc_force_new.restype = C.c_void_p
         L.orc_force_new.argtypes = [C.c_char_p, _dp]
         L.orc_force_free.argtypes = [C.c_void_p]
+        L.orc_force_set_atm_model.argtypes = [C.c_void_p, C.c_int]
         L.orc_field_dense.argtypes = [C.c_void_p, _dp, _dp]
         L.orc_gravity_itrs.argtypes = [C.c_void_p, C.c_long, _dp, _dp]
         L.orc_gmst.restype = C.c_double
@@ -48,6 +49,8 @@ def lib():
         L.orc_eci2equinoc.argtypes = [_dp, _dp]
         L.orc_equinoc2eci.argtypes = [_dp, C.c_double, _dp]
         L.orc_sun_moon.argtypes = [C.c_double, _dp, _dp]
+        L.orc_jb2008_model.restype = C.c_double
+        L.orc_jb2008_model.argtypes = [_dp, C.c_int]
         L.orc_jb2008.restype = C.c_double
         L.orc_jb2008.argtypes = [_dp]
         L.orc_geodetic_altitude_km.restype = C.c_double
@@ -102,13 +105,15 @@ class Force:
 
     def __init__(self, coeff_text: str, order: int, drag=False, sun=False, moon=False,
                  earth_radius=6378.137, omega=7.292115e-5, mu_sun=1.32712440018e11,
-                 mu_moon=4902.800066, drivers=(150.0,) * 8 + (0.0,)):
+                 mu_moon=4902.800066, drivers=(150.0,) * 8 + (0.0,), atm_model=4):
         cfg = f64([order, int(drag), int(sun), int(moon), earth_radius, omega, mu_sun, mu_moon,
                    *drivers])
         self.order = order
         self.h = lib().orc_force_new(coeff_text.encode(), _d(cfg))
         if not self.h:
             raise ValueError("oracle: coefficient text rejected")
+        if lib().orc_force_set_atm_model(self.h, int(atm_model)) != 0:
+            raise ValueError(f"oracle: atm_model {atm_model} is not 4, 5, 6 or 7")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -260,6 +265,11 @@ def sun_moon(jd):
     m = np.zeros(3)
     lib().orc_sun_moon(jd, _d(s), _d(m))
     return s, m
+
+
+def jb2008_model(inputs14, model: int) -> float:
+    """JB2008 density of atm_model 4 (exact), 5, 6 or 7; negative: an error code."""
+    return lib().orc_jb2008_model(_d(f64(inputs14)), int(model))
 
 
 def jb2008(inputs14) -> float:

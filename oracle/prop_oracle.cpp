@@ -559,6 +559,7 @@ const double GTM[10] = {-0.3633, 0.08506, 0.2401, -0.1897, -0.2554,
 const double EARTH_R = 6356.766;
 const double G0 = 9.80665;
 const double R1 = 0.010, R2 = 0.025, R3 = 0.075;
+const double LN_10 = 2.302585092994045684017991454684364;  // f64::consts::LN_10
 
 inline double mbar(double z) {
     double dz = z - 100.0;
@@ -839,6 +840,292 @@ double density(const double* in) {
     double out = rho * fex;
     if (!(std::isfinite(out) && out > 0.0)) return -5.0;
     return out;
+}
+
+// ---- the coarse quadrature profiles: atm_model 5, 6 and 7 (jb2008.rs:365-460,
+// 770-838; jb_density 2353-2624 with P = LogQuadratureX4ApproxV1 / V2 /
+// FittedV7).  All three integrate with fewer, wider Boole panels than the
+// exact profile and carry the five species number densities as a linear
+// factor times exp(log offset) instead of exp(ln(x) + offset) (jb2008.rs:
+// 2420-2455).  Model 7 adds: the upper panel's step ratio taken directly when
+// the segment is one panel (jb2008.rs:2049-2058), the seasonal-latitudinal
+// term dropped at and above 800 km (jb2008.rs:2372-2381), and the two fixed
+// plans (90-105 km; 105-500 km) replaced by degree-14 polynomials in the
+// exospheric temperature inside [500, 2600] K (jb2008.rs:497-838).  Arctangent:
+// libm here; the reference's vector atan (a Cephes rational, within 2.2e-16
+// relative of libm) is not restated.
+struct Profile {
+    double lower_step, middle_step, upper_step;
+    bool retire_zr, fitted;
+    double dlrsl_zero_above_km;
+};
+inline Profile profile(int model) {
+    if (model == 5) return {0.040, 0.100, 0.300, false, false, INFINITY};
+    if (model == 6) return {0.040, 0.300, 0.700, false, false, INFINITY};
+    return {0.040, 0.300, 0.700, true, true, 800.0};  // model 7
+}
+
+// jb2008.rs:645-762, generated by the reference from its exact fixed-plan
+// walkers; u = 2 (Texo - 500) / 2100 - 1 (jb2008.rs:527-529)
+const double V7_SUB2_LOWER[15] = {
+    2.08308130371611e1, -2.2813199227110412e-1, 1.4879239222099155e-1, -1.139133002344331e-1,
+    6.719889370881822e-2, -3.2986547523035745e-2, 1.4447262123974028e-2, -5.996731588024651e-3,
+    2.506977417579703e-3, -1.1683682791648784e-3, 5.31782582941462e-4, -1.236948769467779e-4,
+    4.605879140433796e-5, -1.0052021764385242e-4, 4.8436805479216456e-5};
+const double V7_TLOC2[15] = {
+    2.2451892791577825e2, 8.361916544062648e0, -5.270934320812583e0, 3.939997041634312e0,
+    -2.208846067908349e0, 9.906609315622759e-1, -3.7025703779179586e-1, 1.186132114284294e-1,
+    -3.324856853041033e-2, 8.285607849008118e-3, -1.857998341613101e-3, 3.7710530702575305e-4,
+    -7.049765582078043e-5, 1.331415410018169e-5, -2.125129463136452e-6};
+const double V7_SUB2_MIDDLE[15] = {
+    3.2040046352489187e0, -1.379154303257483e0, 9.72715573920378e-1, -6.869617534038228e-1,
+    4.6837996271501126e-1, -3.319992425165518e-1, 2.3364063163661636e-1, -7.314250955188073e-2,
+    1.7496078898220538e-2, -2.2706819285120894e-1, 2.0222194979627475e-1, 1.5675573900373196e-1,
+    -1.4292464982323266e-1, -1.0640427393729598e-1, 8.289447705809763e-2};
+const double V7_AIN_MIDDLE[15] = {
+    5.459640467018433e-3, -3.677621602992105e-3, 2.492908325931464e-3, -1.6862184086503845e-3,
+    1.13828516769243e-3, -8.142832736202574e-4, 5.787786476720627e-4, -1.761805263267051e-4,
+    3.7786418569522054e-5, -5.77028261806222e-4, 5.158819094236952e-4, 4.0211633550021317e-4,
+    -3.670455396068389e-4, -2.714264714701178e-4, 2.1193481991044327e-4};
+const double V7_TLOC3[15] = {
+    1.5437971407829077e3, 1.039876918772851e3, -4.373905347259339e0, 1.1486679813161453e-1,
+    1.5536392865018533e-1, -6.297264812830576e-2, 7.581060757845705e-3, 3.246438671753597e-3,
+    -1.4342975630790944e-3, -5.114031895849491e-5, 2.0780285514906778e-4, -6.117111036343099e-5,
+    -4.124441270261577e-6, 6.126914161375104e-6, -8.797891983987146e-7};
+
+// Estrin tree of the reference's fitted scalars (jb2008.rs:561-643): pairs
+// combined by fused multiply-add through u, u^2, u^4, u^8, the odd 15th
+// coefficient joining at the u^2 level.
+inline double v7_series(const double c[15], double u) {
+    const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
+    double a[8];
+    for (int i = 0; i < 7; ++i) a[i] = std::fma(c[2 * i + 1], u, c[2 * i]);
+    a[7] = c[14];
+    const double b0 = std::fma(a[1], u2, a[0]), b1 = std::fma(a[3], u2, a[2]);
+    const double b2 = std::fma(a[5], u2, a[4]), b3 = std::fma(a[7], u2, a[6]);
+    return std::fma(std::fma(b3, u4, b2), u8, std::fma(b1, u4, b0));
+}
+
+// One segment of Boole panels from zend_start with ratio zr (jb2008.rs:1732-
+// 1773, 1825-1878, 2032-2085): the abscissae advance by repeated addition,
+// the integrand is [mbar] g / T, the last abscissa's values are kept.
+struct Panels {
+    double sum, ain, z, zend, mb, tloc, gravl;
+};
+inline Panels walk(double zend, double zr, long n, double ain, bool with_mbar, const double tc[4]) {
+    Panels P{0.0, ain, 0.0, zend, 0.0, 0.0, 0.0};
+    for (long i = 0; i < n; ++i) {
+        double z = P.zend;
+        P.zend = zr * z;
+        const double dz = 0.25 * (P.zend - z);
+        double sum1 = WT[0] * P.ain;
+        for (int j = 1; j < 5; ++j) {
+            z += dz;
+            P.tloc = local_temp(z, tc);
+            P.gravl = grav(z);
+            if (with_mbar) {
+                P.mb = mbar(z);
+                P.ain = P.mb * P.gravl / P.tloc;
+            } else {
+                P.ain = P.gravl / P.tloc;
+            }
+            sum1 += WT[j] * P.ain;
+        }
+        P.z = z;
+        P.sum += dz * sum1;
+    }
+    return P;
+}
+
+// jb2008.rs:1515-1526
+inline long step_count(double log_ratio, bool* ok) {
+    if (!(std::isfinite(log_ratio) && log_ratio >= 0.0) || std::floor(log_ratio) >= 4294967295.0) {
+        *ok = false;
+        return 0;
+    }
+    return (long)std::floor(log_ratio) + 1;
+}
+
+// in[14] as density(); model 5, 6 or 7.
+double density_coarse(const double* in, int model) {
+    const Profile P = profile(model);
+    for (int i = 0; i < 14; ++i)
+        if (!std::isfinite(in[i])) return -1.0;
+    double mjd = in[0], sdec = in[1], ha = in[2], slat = in[3], alt_m = in[4];
+    double f10 = in[5], f10b = in[6], s10 = in[7], s10b = in[8], m10 = in[9], m10b = in[10],
+           y10 = in[11], y10b = in[12], dtcv = in[13];
+    if (alt_m < 90000.0) return -2.0;
+    if (!(sdec >= -PI / 2 && sdec <= PI / 2) || !(slat >= -PI / 2 && slat <= PI / 2)) return -3.0;
+    for (int i = 5; i <= 12; ++i)
+        if (in[i] <= 0.0) return -4.0;
+    const double alt = alt_m / 1000.0;
+    // exospheric temperature and profile: as density()
+    double fn = std::min(std::pow(f10b / 240.0, 0.25), 1.0);
+    double fsb = f10b * fn + s10b * (1.0 - fn);
+    double tsubc = 392.4 + 3.227 * fsb + 0.298 * (f10 - f10b) + 2.259 * (s10 - s10b) +
+                   0.312 * (m10 - m10b) + 0.178 * (y10 - y10b);
+    double eta = 0.5 * std::fabs(slat - sdec);
+    double theta = 0.5 * std::fabs(slat + sdec);
+    double h = ha;
+    if (!(h >= 0.0 && h < TWO_PI)) {
+        if (h < 0.0 && h > -TWO_PI) h += TWO_PI;
+        else {
+            h = std::fmod(h, TWO_PI);
+            if (h < 0.0) h += TWO_PI;
+        }
+    }
+    double tau = h - 0.64577182 + 0.10471976 * std::sin(h + 0.75049158);
+    double st_hour = ((h + PI) * (180.0 / PI)) / 15.0;
+    if (st_hour >= 24.0) st_hour -= 24.0;
+    else if (st_hour < 0.0) st_hour += 24.0;
+    double slat_s = std::sin(slat), slat_c = std::cos(slat);
+    double cos_eta = five_halves(std::cos(eta));
+    double sin_theta = five_halves(std::sin(theta));
+    double cos_tau = std::fabs(std::cos(0.5 * tau));
+    double df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
+    double tsubl = tsubc * (1.0 + 0.31 * df);
+    double tinf = tsubl + dtcv + dtc(f10, st_hour, slat_c, alt);
+    double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * std::exp(-0.0021357 * tinf);
+    double gsubx = 0.054285714 * (tsubx - 183.0);
+    double tc[4];
+    tc[0] = tsubx;
+    tc[1] = gsubx;
+    tc[2] = (tinf - tsubx) / (PI / 2);
+    tc[3] = gsubx / tc[2];
+    // the fit domain is judged on Texo rebuilt from the profile (jb2008.rs:521-524)
+    const double texo = tc[0] + tc[2] * (PI / 2);
+    const bool fit_in = P.fitted && texo >= 500.0 && texo <= 2600.0;
+    const double u = 2.0 * (texo - 500.0) / (2600.0 - 500.0) - 1.0;
+    bool ok = true;
+
+    // 90 km -> min(alt, 105 km)
+    const double z1 = 90.0;
+    const double mb1 = mbar(z1);
+    const double tloc1 = local_temp(z1, tc);
+    Panels lo;
+    const bool lower_planned = alt >= 105.0;
+    {
+        // the fixed 90-105 km plan walks the same panels as this (n from
+        // ln(105/90) / 0.040 = 4 panels); only the fitted form differs
+        const double al = std::log(std::min(alt, 105.0) / z1);
+        const long n = step_count(al / P.lower_step, &ok);
+        if (!ok) return -5.0;
+        lo = walk(z1, std::exp(al / (double)n), n, mb1 * grav(z1) / tloc1, true, tc);
+        if (fit_in && lower_planned) {
+            lo.sum = v7_series(V7_SUB2_LOWER, u);
+            lo.tloc = v7_series(V7_TLOC2, u);
+        }
+    }
+    const double mb2 = lo.mb, tloc2 = lo.tloc, gravl2 = lo.gravl;
+    double rho = 3.46e-6 * mb2 * tloc1 / std::exp(lo.sum / RSTAR) / (mb1 * tloc2);
+    double anm = AVOGAD * rho;
+    double an = anm / mb2;
+    double fact2 = anm / 28.960;
+    double factor[6] = {FRAC[0] * fact2, fact2 * (1.0 + FRAC[1]) - an, 2.0 * (an - fact2),
+                        FRAC[2] * fact2, FRAC[3] * fact2, 1.0};
+    for (double& f : factor)
+        if (f < 0.0) f = NAN;  // jb2008.rs:2304-2310
+    double offset[6] = {0, 0, 0, 0, 0, 0};
+    double z = lo.z;
+    if (alt <= 105.0) {
+        factor[5] = factor[4];
+        offset[5] = offset[4] - 25.0;
+    } else {
+        // 105 km -> min(alt, 500 km)
+        const double al = std::log(std::min(alt, 500.0) / z);
+        const long n = step_count(al / P.middle_step, &ok);
+        if (!ok) return -5.0;
+        Panels mid = walk(lo.zend, std::exp(al / (double)n), n, gravl2 / tloc2, false, tc);
+        if (fit_in && lower_planned && alt >= 500.0) {
+            mid.sum = v7_series(V7_SUB2_MIDDLE, u);
+            mid.ain = v7_series(V7_AIN_MIDDLE, u);
+            mid.tloc = v7_series(V7_TLOC3, u);
+        }
+        const double tloc3 = mid.tloc;
+        z = mid.z;
+        // between 500 km and alt (jb2008.rs:2032-2085)
+        const double ratio = std::max(alt, 500.0) / z;
+        const double alu = std::max(std::log(ratio), 0.0);
+        const long nu = step_count(alu / (alt > 500.0 ? P.upper_step : P.middle_step), &ok);
+        if (!ok) return -5.0;
+        const double zr = (P.retire_zr && nu == 1) ? std::max(ratio, 1.0) : std::exp(alu / (double)nu);
+        Panels up = walk(mid.zend, zr, nu, mid.ain, false, tc);
+        double tloc4 = nu > 0 ? up.tloc : tc[0];
+        if (nu > 0) z = up.z;
+        double altr, hsign;
+        if (alt <= 500.0) {
+            fact2 = mid.sum / RSTAR;
+            altr = std::log(tloc3 / tloc2);
+            hsign = 1.0;
+        } else {
+            fact2 = (mid.sum + up.sum) / RSTAR;
+            altr = std::log(tloc4 / tloc2);
+            hsign = -1.0;
+        }
+        for (int i = 0; i < 5; ++i) offset[i] = offset[i] - (1.0 + ALPHA[i]) * altr - fact2 * AMW[i];
+        const double al10t5 = std::log10(tinf);
+        const double alnh5 = (5.5 * al10t5 - 39.40) * al10t5 + 73.13;
+        offset[5] = LN_10 * (alnh5 + 6.0) + hsign * (std::log(tloc4 / tloc3) + up.sum * AMW[5] / RSTAR);
+    }
+    // seasonal-latitudinal term (jb2008.rs:3391-3417), zero from the profile's cut
+    double dlrsl = 0.0;
+    if (!(alt >= P.dlrsl_zero_above_km)) {
+        double years = (mjd - 36204.0) / 365.2422;
+        double capphi = years - std::trunc(years);
+        if (capphi == 0.0) capphi = std::copysign(0.0, years);
+        double sgn = slat >= 0.0 ? 1.0 : -1.0;
+        double hm90 = alt - 90.0;
+        dlrsl = 0.02 * hm90 * std::exp(-0.045 * hm90) * sgn * std::sin(TWO_PI * capphi + 1.72) * slat_s * slat_s;
+    }
+    // semiannual term (jb2008.rs:3436-3461)
+    double dlrsa = 0.0;
+    if (z < 2000.0) {
+        double day = day_of_year(mjd, &ok);
+        if (!ok) return -5.0;
+        const double htz = alt / 1000.0;
+        const double fz = f10b - 0.70 * s10b - 0.04 * m10b;
+        const double fzz = FZM[0] + fz * (FZM[1] + htz * (FZM[2] + FZM[3] * htz + FZM[4] * fz));
+        const double fg = f10b - 0.75 * s10b - 0.37 * m10b;
+        const double t = TWO_PI * (day - 1.0) / 365.0;
+        const double s1 = std::sin(t), c1 = std::cos(t);
+        const double s2 = 2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
+        const double gtz = GTM[0] + GTM[1] * s1 + GTM[2] * c1 + GTM[3] * s2 + GTM[4] * c2 +
+                           fg * (GTM[5] + GTM[6] * s1 + GTM[7] * c1 + GTM[8] * s2 + GTM[9] * c2);
+        dlrsa = std::max(fzz, 1.0e-6) * gtz;
+    }
+    const double dlr = LN_10 * (dlrsl + dlrsa);
+    // compensated species sum (jb2008.rs:2584-2607)
+    double sum = 0.0, comp = 0.0, simple = 0.0;
+    for (int i = 0; i < 6; ++i) {
+        const double term = factor[i] * std::exp(offset[i] + dlr) * AMW[i];
+        const double tmp = term - comp;
+        const double next = sum + tmp;
+        comp = (next - sum) - tmp;
+        sum = next;
+        simple += term;
+    }
+    double fs = sum - comp;
+    if (std::isnan(fs) && std::isinf(simple)) fs = simple;
+    rho = fs / AVOGAD;
+    double fex = 1.0;
+    if (alt >= 1000.0 && alt < 1500.0) {
+        double zeta = (alt - 1000.0) * 0.002;
+        double f15c = CHT[0] + CHT[1] * f10b + CHT[2] * 1500.0 + CHT[3] * f10b * 1500.0;
+        double f15cz = (CHT[2] + CHT[3] * f10b) * 500.0;
+        double fex2 = 3.0 * f15c - f15cz - 3.0;
+        double fex3 = f15cz - 2.0 * f15c + 2.0;
+        fex = 1.0 + zeta * zeta * (fex2 + fex3 * zeta);
+    } else if (alt >= 1500.0) {
+        fex = CHT[0] + CHT[1] * f10b + CHT[2] * alt + CHT[3] * f10b * alt;
+    }
+    const double out = rho * fex;
+    if (!(std::isfinite(out) && out > 0.0)) return -5.0;
+    return out;
+}
+
+// atm_model 4 (exact) or 5, 6, 7
+inline double density_model(const double* in, int model) {
+    return model == 4 ? density(in) : density_coarse(in, model);
 }
 }  // namespace jb
 
@@ -1288,6 +1575,7 @@ struct Force {
     double omega = EARTH_OMEGA;
     double mu_sun = 1.32712440018e11, mu_moon = 4902.800066;
     double drivers[9] = {150, 150, 150, 150, 150, 150, 150, 150, 0};  // f10..y10b, dTc
+    int atm_model = 4;  // 4 exact JB2008; 5, 6, 7 the coarse quadrature profiles
     std::shared_ptr<DriverTable> table;  // when set: drivers looked up per evaluation
     std::shared_ptr<EphemTable> eph[2];  // Sun, Moon catalogues; unset: the analytic series
 };
@@ -1321,7 +1609,7 @@ double density_at(const Force& F, const double pos_itrs[3], const double sun_itr
     } else {
         for (int i = 0; i < 9; ++i) in[5 + i] = F.drivers[i];
     }
-    double rho = jb::density(in);
+    double rho = jb::density_model(in, F.atm_model);
     if (!(rho > 0.0) || !std::isfinite(rho)) return NAN;
     if (alt_m > CEIL_M) rho = std::min(rho, CEIL_RHO);
     return rho;
@@ -2040,6 +2328,11 @@ void* orc_force_new(const char* coeff_text, const double* cfg) {
 }
 
 void orc_force_free(void* f) { delete (Force*)f; }
+int orc_force_set_atm_model(void* f, int model) {
+    if (model < 4 || model > 7) return 1;
+    ((Force*)f)->atm_model = model;
+    return 0;
+}
 
 // Space-weather tables for the JB2008 drivers (null texts: back to the fixed
 // drivers).  Returns 0, or -1 with the reason in err.
@@ -2174,6 +2467,8 @@ void orc_sun_moon(double jd, double* sun, double* moon) {
     moon_position(jd, moon);
 }
 double orc_jb2008(const double* in14) { return jb::density(in14); }
+// atm_model 4 (exact), 5, 6 or 7 (the coarse quadrature profiles)
+double orc_jb2008_model(const double* in14, int model) { return jb::density_model(in14, model); }
 double orc_geodetic_altitude_km(const double* p, double a) {
     return geodetic_altitude_km(p[0], p[1], p[2], a);
 }

@@ -138,9 +138,19 @@ def main(ref_root: str | None = None) -> None:
         alt = re.search(r"orekit_local_input\(([0-9_.]+)\)", mm.group(1)).group(1)
         bits = re.search(r"f64::from_bits\((0x[0-9a-f_]+)\)", mm.group(1)).group(1).replace("_", "")
         lits.append({"altitude_km": num(alt), "mjd_utc": None, "density_kg_m3": hex_to_f64(bits)})
+    # the coarse-profile (atm_model 5) receipts beside the exact ones, as bit
+    # patterns (jb_rs/tests/jb2008_logquad_x4_probe.rs, shared-core checksum)
+    probe = (crates / "jb_rs/tests/jb2008_logquad_x4_probe.rs").read_text()
+    mm = re.search(r"fn shared_core_checksum_tracks_corrected_species_reduction_bits\(\) \{(.*?)\n\}\n", probe, re.S)
+    x4 = []
+    for alt, exact_bits, probe_bits in re.findall(r"\(([0-9_.]+), (0x[0-9a-f_]+), (0x[0-9a-f_]+)\)", mm.group(1)):
+        x4.append({"altitude_km": num(alt), "exact": hex_to_f64("0x" + exact_bits[2:].replace("_", "")),
+                   "model5": hex_to_f64("0x" + probe_bits[2:].replace("_", ""))})
     jb = {
         "source": ["lightyear_odeint_rs/tests/data/orekit_jb2008_eci_adapter_v1.json",
-                   "jb_rs/src/jb2008.rs (orekit_local_input and Orekit JAR literal tests)"],
+                   "jb_rs/src/jb2008.rs (orekit_local_input and Orekit JAR literal tests)",
+                   "jb_rs/tests/jb2008_logquad_x4_probe.rs (exact and model-5 receipts)"],
+        "model5_receipts": x4,
         "earth": j["earth"],
         "relative_tolerance": 5e-13,
         "cases": cases,

@@ -119,3 +119,101 @@ def test_oracle_steppers_converge_to_one_trajectory():
         finals[m] = d[:, :3]
     for m, d in finals.items():
         assert np.abs(d - finals["vern9"]).max() < 1e-6, m
+
+
+# ------------------------------------------------------ coarse JB2008 profiles
+def _local(L, alt_km):
+    return [L["mjd_utc"], L["sun_declination_rad"], L["hour_angle_rad"], L["sat_geocentric_lat_rad"],
+            alt_km * 1000.0, L["f10"], L["f10b"], L["s10"], L["s10b"], L["m10"], L["m10b"], L["y10"], L["y10b"],
+            L["dtc_k"]]
+
+
+def test_jb2008_model5_matches_reference_receipts(jbfix):
+    # jb_rs/tests/jb2008_logquad_x4_probe.rs: the exact and model-5 densities
+    # of orekit_local_input at ten altitudes, 90 ... 35,000 km, as the
+    # reference computes them; the restatement differs only in its arctangent
+    # (libm against the reference's vector rational, within 2.2e-16 per call)
+    assert len(jbfix["model5_receipts"]) == 10
+    L = jbfix["orekit_local_input"]
+    for r in jbfix["model5_receipts"]:
+        inp = _local(L, r["altitude_km"])
+        assert abs(O.jb2008_model(inp, 4) - r["exact"]) <= 5e-16 * r["exact"], r
+        assert abs(O.jb2008_model(inp, 5) - r["model5"]) <= 5e-15 * r["model5"], r
+
+
+def broad_grid_input(mjd, alt_km, lat_deg, lst_hour):
+    """jb_rs/tests/jb2008_logquad_x4_probe.rs:34-66 (same arithmetic)."""
+    import math
+    ph = math.tau * (mjd - 51999.75) / 365.2422
+    ha = lst_hour * math.tau / 24.0 - math.pi
+    f10b = 120.0 + 25.0 * math.cos(ph)
+    s10b = 112.0 + 18.0 * math.sin(ph + 0.2)
+    m10b = 128.0 + 16.0 * math.cos(ph - 0.5)
+    y10b = 138.0 + 20.0 * math.sin(ph + 0.7)
+    return [mjd, 23.44 * (math.pi / 180.0) * math.sin(ph), ha, lat_deg * (math.pi / 180.0), alt_km * 1000.0,
+            f10b + 6.0 * math.sin(ph + 0.1), f10b, s10b + 5.0 * math.cos(ph + 0.4), s10b,
+            m10b + 4.0 * math.sin(ph - 0.3), m10b, y10b + 7.0 * math.cos(ph + 0.8), y10b,
+            25.0 + 18.0 * math.sin(ph - 0.2)]
+
+
+BROAD_ALT = [90.0, 91.0, 100.0, 105.0, 120.0, 200.0, 240.0, 300.0, 400.0, 500.0, 600.0, 800.0, 1000.0, 1500.0,
+             2000.0, 3000.0, 5000.0, 35000.0]
+
+
+def test_jb2008_coarse_profiles_on_the_reference_broad_grid():
+    # jb2008_logquad_x4_probe.rs: model 5 within 3e-6 of the exact model
+    # (its own maximum there 1.605e-6), model 6 within the re-scoped 1e-4
+    # (5.747e-5), model 7 within 1e-4 and equal to model 6 to a few digits;
+    # model 7 moves the density wherever both fitted plans run (>= 500 km) and
+    # is model 6 bit for bit below 105 km, where no plan runs (:318-447)
+    err = {5: [], 6: [], 7: []}
+    moved = fitted = same_low = low = 0
+    for mjd in (51999.75, 54000.0, 57000.25, 60000.0, 60648.5):
+        for alt in BROAD_ALT:
+            for lat in (-75.0, -45.0, 0.0, 45.0, 75.0):
+                for lst in (0.0, 6.0, 12.0, 18.0):
+                    inp = broad_grid_input(mjd, alt, lat, lst)
+                    ex = O.jb2008_model(inp, 4)
+                    d = {m: O.jb2008_model(inp, m) for m in (5, 6, 7)}
+                    assert ex > 0 and all(v > 0 for v in d.values())
+                    for m in (5, 6, 7):
+                        err[m].append(abs(d[m] - ex) / ex)
+                    if alt >= 500.0:
+                        fitted += 1
+                        moved += d[7] != d[6]
+                    if alt < 105.0:
+                        low += 1
+                        same_low += d[7] == d[6]
+    mx = {m: max(v) for m, v in err.items()}
+    assert len(err[5]) == 1800
+    assert 1.0e-6 < mx[5] <= 3.0e-6, mx[5]
+    assert 5.0e-5 <= mx[6] < 1.0e-4, mx[6]
+    # the maxima the reference records for its own models 5 and 6 on this grid
+    assert abs(mx[5] - 1.605e-6) <= 0.001e-6 and abs(mx[6] - 5.747e-5) <= 0.001e-5, mx
+    assert mx[7] <= 1.0e-4 and abs(mx[7] - mx[6]) <= 1e-3 * mx[6], (mx[7], mx[6])
+    assert 2 * moved > fitted, (moved, fitted)
+    assert same_low == low
+
+
+def test_jb2008_model7_falls_back_outside_its_temperature_domain():
+    # jb2008_logquad_x4_probe.rs:449-520: sweeping dTc moves the exospheric
+    # temperature across [500, 2600] K at 700 km; model 7 equals model 6 bit
+    # for bit below and above that domain and differs inside it
+    trans, prev = [], None
+    counts = {"below": 0, "inside": 0, "above": 0}
+    for step in range(401):
+        inp = broad_grid_input(57000.25, 700.0, 0.0, 12.0)
+        inp[13] = step * 10.0 - 1500.0
+        v7, v6 = O.jb2008_model(inp, 7), O.jb2008_model(inp, 6)
+        if v7 < 0 or v6 < 0:
+            continue
+        same = v7 == v6
+        if same != prev:
+            trans.append((inp[13], same))
+            prev = same
+        if same:
+            counts["above" if counts["inside"] else "below"] += 1
+        else:
+            counts["inside"] += 1
+    assert all(counts.values()), counts
+    assert len(trans) == 3 and [t[1] for t in trans] == [True, False, True], trans
