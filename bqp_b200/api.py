@@ -79,9 +79,9 @@ def force_config(gravity_order=5, drag=True, srp=True, sun=True, moon=True, atm_
     if drag and atm_model not in (1, 3, 4, 5, 6, 7, 8):
         raise ValueError(f"unknown atm_model {atm_model}; use 4 (exact JB2008), 7 (fitted JB2008), "
                          "8 (campaign persistence scenario), 1 (exponential)")
-    if drag and atm_model not in (4, 7):
-        raise ValueError(f"atm_model {atm_model} is not built here; use 4 or 7 (both evaluated with the "
-                         "exact JB2008 quadrature)")
+    if drag and atm_model not in (4, 5, 6, 7):
+        raise ValueError(f"atm_model {atm_model} is not built here; use 4 (exact JB2008) or 5, 6, 7 (the "
+                         "coarse JB2008 quadrature profiles, 7 the fitted kernel)")
     name = str(method).lower()
     if name in _UNBUILT_METHODS:
         raise ValueError(f"integrator method {name!r} is not built here; use 'vern7', 'vern9', 'dop853' or 'dopri5'")

@@ -530,8 +530,9 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_UNSUPPORTED, "solar radiation pressure (binary-eclipse SRP) is not built; pass srp=False");
     if (c->force_flags & ~(BQP_FORCE_DRAG | BQP_FORCE_SUN | BQP_FORCE_MOON | BQP_FORCE_SRP))
         return fail(BQP_E_ARG, "unknown force flags 0x%x", c->force_flags);
-    if ((c->force_flags & BQP_FORCE_DRAG) && c->atm_model != 4 && c->atm_model != 7)
-        return fail(BQP_E_UNSUPPORTED, "atm_model %d is not built; use 4 (exact JB2008) or 7", c->atm_model);
+    if ((c->force_flags & BQP_FORCE_DRAG) && (c->atm_model < 4 || c->atm_model > 7))
+        return fail(BQP_E_UNSUPPORTED, "atm_model %d is not a JB2008 profile; use 4 (exact) or 5, 6, 7 (coarse)",
+                    c->atm_model);
     if (c->method < 0 || c->method > 4) return fail(BQP_E_ARG, "unknown method %d", c->method);
     if (c->error_control == 0) {
         if (!(std::isfinite(c->eps) && c->eps > 0.0)) return fail(BQP_E_ARG, "eps must be finite and > 0");
@@ -580,6 +581,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.sun = (c.force_flags & BQP_FORCE_SUN) ? 1 : 0;
     fp.moon = (c.force_flags & BQP_FORCE_MOON) ? 1 : 0;
     fp.ground_check = c.ground_check;
+    fp.atm_model = (c.force_flags & BQP_FORCE_DRAG) ? c.atm_model : 4;
     fp.earth_radius = c.earth_radius;
     fp.omega = c.omega_earth;
     fp.mu_sun = c.mu_sun;
@@ -589,7 +591,8 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.dtab = ctx->dtab;
     fp.eph_sun = ctx->eph[0];
     fp.eph_moon = ctx->eph[1];
-    fp.fit = (c.drag_quadrature || !fp.drag) ? nullptr : ctx->d_fit;
+    // the sweep fits replace the exact model's quadrature only
+    fp.fit = (c.drag_quadrature || !fp.drag || fp.atm_model != 4) ? nullptr : ctx->d_fit;
     fp.fit2 = fp.fit ? ctx->d_fit2 : nullptr;
     return fp;
 }
@@ -598,7 +601,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
 // used only where the quadrature would otherwise run and the 1-D fits hold.
 int ensure_fit2(bqp_ctx* ctx) {
     const bqp_force_config& c = ctx->cfg;
-    if (!(c.force_flags & BQP_FORCE_DRAG) || c.drag_quadrature || !ctx->d_fit) return 0;
+    if (!(c.force_flags & BQP_FORCE_DRAG) || c.drag_quadrature || !ctx->d_fit || c.atm_model != 4) return 0;
     // the fits depend only on the T_inf range the drivers can produce
     double tinf[2] = {0.0, 0.0};
     if (ctx->dtab.n_solar > 0) {
@@ -1107,6 +1110,17 @@ int bqp_jb_fit_check(const double* drivers, double* worst) {
     build_jb_fit2(f1, tlo, thi, *f2, worst + 1);
     worst[4] = f2->tlo;
     worst[5] = f2->thi;
+    return 0;
+}
+
+int bqp_jb_density(int32_t model, int64_t n, const double* in, double* out) {
+    if (model < 4 || model > 7) return fail(BQP_E_ARG, "model must be 4, 5, 6 or 7, got %d", model);
+    if (n < 0 || (n > 0 && (!in || !out))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) {
+        const double* x = in + 14 * i;
+        const jb::Drivers d{x[5], x[6], x[7], x[8], x[9], x[10], x[11], x[12], x[13]};
+        out[i] = jb::density_model(x[0], x[1], x[2], x[3], x[4], d, model);
+    }
     return 0;
 }
 

@@ -519,6 +519,257 @@ BQP_HD double density(double mjd, double sun_dec, double hour_angle, double lat,
     return out;
 }
 
+// ------------------------------------------------------------------------
+// The reference's coarse quadrature profiles, atm_model 5, 6 and 7
+// (jb_rs/src/jb2008.rs:365-460, 770-838; jb_density 2353-2624): fewer, wider
+// Boole panels, the five species carried as factor x exp(log offset)
+// (jb2008.rs:2420-2455) and a compensated species sum (2584-2607).  Model 7
+// (the reference's default) also takes the one-panel upper segment's step
+// ratio directly (2049-2058), drops the seasonal-latitudinal term at and
+// above 800 km (2372-2381) and replaces the two fixed plans (90-105 km,
+// 105-500 km) by degree-14 series in the exospheric temperature inside
+// [500, 2600] K (497-838).  Its costly part is small: above 500 km five
+// series, one upper panel (four arctangents) and the species; below, six
+// 105-500 km panels at most.
+constexpr double kV7TexoLo = 500.0, kV7TexoHi = 2600.0;
+// jb2008.rs:645-762 (the reference's fits of its fixed-plan walkers), lowest
+// coefficient first
+BQP_JB_TABLE(kV7Sub2Lower, 15, {2.08308130371611e1, -2.2813199227110412e-1, 1.4879239222099155e-1,
+                                -1.139133002344331e-1, 6.719889370881822e-2, -3.2986547523035745e-2,
+                                1.4447262123974028e-2, -5.996731588024651e-3, 2.506977417579703e-3,
+                                -1.1683682791648784e-3, 5.31782582941462e-4, -1.236948769467779e-4,
+                                4.605879140433796e-5, -1.0052021764385242e-4, 4.8436805479216456e-5})
+BQP_JB_TABLE(kV7Tloc2, 15, {2.2451892791577825e2, 8.361916544062648e0, -5.270934320812583e0, 3.939997041634312e0,
+                            -2.208846067908349e0, 9.906609315622759e-1, -3.7025703779179586e-1,
+                            1.186132114284294e-1, -3.324856853041033e-2, 8.285607849008118e-3,
+                            -1.857998341613101e-3, 3.7710530702575305e-4, -7.049765582078043e-5,
+                            1.331415410018169e-5, -2.125129463136452e-6})
+BQP_JB_TABLE(kV7Sub2Middle, 15, {3.2040046352489187e0, -1.379154303257483e0, 9.72715573920378e-1,
+                                 -6.869617534038228e-1, 4.6837996271501126e-1, -3.319992425165518e-1,
+                                 2.3364063163661636e-1, -7.314250955188073e-2, 1.7496078898220538e-2,
+                                 -2.2706819285120894e-1, 2.0222194979627475e-1, 1.5675573900373196e-1,
+                                 -1.4292464982323266e-1, -1.0640427393729598e-1, 8.289447705809763e-2})
+BQP_JB_TABLE(kV7AinMiddle, 15, {5.459640467018433e-3, -3.677621602992105e-3, 2.492908325931464e-3,
+                                -1.6862184086503845e-3, 1.13828516769243e-3, -8.142832736202574e-4,
+                                5.787786476720627e-4, -1.761805263267051e-4, 3.7786418569522054e-5,
+                                -5.77028261806222e-4, 5.158819094236952e-4, 4.0211633550021317e-4,
+                                -3.670455396068389e-4, -2.714264714701178e-4, 2.1193481991044327e-4})
+BQP_JB_TABLE(kV7Tloc3, 15, {1.5437971407829077e3, 1.039876918772851e3, -4.373905347259339e0,
+                            1.1486679813161453e-1, 1.5536392865018533e-1, -6.297264812830576e-2,
+                            7.581060757845705e-3, 3.246438671753597e-3, -1.4342975630790944e-3,
+                            -5.114031895849491e-5, 2.0780285514906778e-4, -6.117111036343099e-5,
+                            -4.124441270261577e-6, 6.126914161375104e-6, -8.797891983987146e-7})
+
+// Estrin evaluation of a 15-term series (the reference's tree,
+// jb2008.rs:561-643): pairs fused through u, u^2, u^4, u^8, the last
+// coefficient joining at the u^2 level.
+BQP_HD double v7_series(const double* c, double u) {
+    const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
+    const double a0 = fma(c[1], u, c[0]), a1 = fma(c[3], u, c[2]), a2 = fma(c[5], u, c[4]);
+    const double a3 = fma(c[7], u, c[6]), a4 = fma(c[9], u, c[8]), a5 = fma(c[11], u, c[10]);
+    const double a6 = fma(c[13], u, c[12]);
+    const double b0 = fma(a1, u2, a0), b1 = fma(a3, u2, a2), b2 = fma(a5, u2, a4), b3 = fma(c[14], u2, a6);
+    return fma(fma(b3, u4, b2), u8, fma(b1, u4, b0));
+}
+
+// Panel count of a log ratio (jb2008.rs:1515-1526); 0 on a domain error.
+BQP_HD int coarse_panels(double log_ratio) {
+    if (!(isfinite(log_ratio) && log_ratio >= 0.0) || floor(log_ratio) >= 2147483646.0) return 0;
+    return (int)floor(log_ratio) + 1;
+}
+
+// As density(), for atm_model 5, 6 or 7.
+BQP_HD double density_coarse(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
+                             const Drivers& d, int model) {
+    const double step_lower = 0.040, step_middle = model == 5 ? 0.100 : 0.300;
+    const double step_upper = model == 5 ? 0.300 : 0.700;
+    const bool v7 = model == 7;
+    if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) ||
+        !isfinite(alt_m) || !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) ||
+        !isfinite(d.s10b) || !isfinite(d.m10) || !isfinite(d.m10b) || !isfinite(d.y10) ||
+        !isfinite(d.y10b) || !isfinite(d.dtc))
+        return kErrNonFinite;
+    if (alt_m < 90000.0) return kErrAltitude;
+    if (!(sun_dec >= -kPi / 2 && sun_dec <= kPi / 2) || !(lat >= -kPi / 2 && lat <= kPi / 2))
+        return kErrAngle;
+    if (d.f10 <= 0.0 || d.f10b <= 0.0 || d.s10 <= 0.0 || d.s10b <= 0.0 || d.m10 <= 0.0 ||
+        d.m10b <= 0.0 || d.y10 <= 0.0 || d.y10b <= 0.0)
+        return kErrIndex;
+    const double alt = alt_m / 1000.0;
+    // exospheric temperature and profile, as density()
+    double fn = fmin(pow(d.f10b / 240.0, 0.25), 1.0);
+    double fsb = d.f10b * fn + d.s10b * (1.0 - fn);
+    double tsubc = 392.4 + 3.227 * fsb + 0.298 * (d.f10 - d.f10b) + 2.259 * (d.s10 - d.s10b) +
+                   0.312 * (d.m10 - d.m10b) + 0.178 * (d.y10 - d.y10b);
+    double eta = 0.5 * fabs(lat - sun_dec);
+    double theta = 0.5 * fabs(lat + sun_dec);
+    double h = hour_angle;
+    if (!(h >= 0.0 && h < kTwoPi)) {
+        if (h < 0.0 && h > -kTwoPi) {
+            h += kTwoPi;
+        } else {
+            h = fmod(h, kTwoPi);
+            if (h < 0.0) h += kTwoPi;
+        }
+    }
+    double tau = h - 0.64577182 + 0.10471976 * sin(h + 0.75049158);
+    double st_hour = ((h + kPi) * (180.0 / kPi)) / 15.0;
+    if (st_hour >= 24.0) st_hour -= 24.0;
+    else if (st_hour < 0.0) st_hour += 24.0;
+    double slat, clat;
+    sincos(lat, &slat, &clat);
+    double cos_eta = five_halves(cos(eta));
+    double sin_theta = five_halves(sin(theta));
+    double cos_tau = fabs(cos(0.5 * tau));
+    double df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
+    double tsubl = tsubc * (1.0 + 0.31 * df);
+    double tinf = tsubl + d.dtc + dtc_correction(d.f10, st_hour, clat, alt);
+    double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * exp(-0.0021357 * tinf);
+    double gsubx = 0.054285714 * (tsubx - 183.0);
+    double tc[4];
+    tc[0] = tsubx;
+    tc[1] = gsubx;
+    tc[2] = (tinf - tsubx) / (kPi / 2);
+    tc[3] = gsubx / tc[2];
+    // the fit domain is judged on Texo rebuilt from the profile (jb2008.rs:521-524)
+    const double texo = tc[0] + tc[2] * (kPi / 2);
+    const bool fit_in = v7 && texo >= kV7TexoLo && texo <= kV7TexoHi;
+    const double u = 2.0 * (texo - kV7TexoLo) / (kV7TexoHi - kV7TexoLo) - 1.0;
+
+    // 90 km -> min(alt, 105 km): four panels at and above 105 km (the fixed plan)
+    const double z1 = 90.0;
+    const double mb1 = mbar(z1);
+    const double tloc1 = local_temp(z1, tc);
+    const bool lower_planned = alt >= 105.0;
+    double al = log(fmin(alt, 105.0) / z1);
+    int n = coarse_panels(al / step_lower);
+    if (n == 0) return kErrDomain;
+    Sweep lo = boole_sweep(z1, z1, exp(al / n), n, mb1 * grav(z1) / tloc1, true, tc);
+    if (fit_in && lower_planned) {
+        lo.sum = v7_series(JBT(kV7Sub2Lower), u);
+        lo.tloc = v7_series(JBT(kV7Tloc2), u);
+    }
+    const double mb2 = lo.mb, tloc2 = lo.tloc;
+    double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
+    double anm = kAvogadro * rho;
+    double an = anm / mb2;
+    double fact2 = anm / 28.960;
+    double factor[6] = {JBT(kFrac)[0] * fact2, fact2 * (1.0 + JBT(kFrac)[1]) - an, 2.0 * (an - fact2),
+                        JBT(kFrac)[2] * fact2, JBT(kFrac)[3] * fact2, 1.0};
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        if (factor[i] < 0.0) factor[i] = NAN;  // jb2008.rs:2304-2310
+    double offset[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double z = lo.z;
+    if (alt <= 105.0) {
+        factor[5] = factor[4];
+        offset[5] = offset[4] - 25.0;
+    } else {
+        // 105 km -> min(alt, 500 km): the fixed six-panel plan at and above 500 km
+        al = log(fmin(alt, 500.0) / z);
+        n = coarse_panels(al / step_middle);
+        if (n == 0) return kErrDomain;
+        Sweep mid = boole_sweep(z, lo.zend, exp(al / n), n, lo.gravl / tloc2, false, tc);
+        if (fit_in && lower_planned && alt >= 500.0) {
+            mid.sum = v7_series(JBT(kV7Sub2Middle), u);
+            mid.ain = v7_series(JBT(kV7AinMiddle), u);
+            mid.tloc = v7_series(JBT(kV7Tloc3), u);
+        }
+        const double tloc3 = mid.tloc;
+        z = mid.z;
+        // between 500 km and alt (jb2008.rs:2032-2085)
+        const double ratio = fmax(alt, 500.0) / z;
+        const double alu = fmax(log(ratio), 0.0);
+        n = coarse_panels(alu / (alt > 500.0 ? step_upper : step_middle));
+        if (n == 0) return kErrDomain;
+        const double zr = (v7 && n == 1) ? fmax(ratio, 1.0) : exp(alu / n);
+        Sweep up = boole_sweep(z, mid.zend, zr, n, mid.ain, false, tc);
+        const double tloc4 = up.tloc;
+        z = up.z;
+        double altr, hsign;
+        if (alt <= 500.0) {
+            fact2 = mid.sum / kRstar;
+            altr = log(tloc3 / tloc2);
+            hsign = 1.0;
+        } else {
+            fact2 = (mid.sum + up.sum) / kRstar;
+            altr = log(tloc4 / tloc2);
+            hsign = -1.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) offset[i] = offset[i] - altr - fact2 * JBT(kAmw)[i];
+        offset[4] = offset[4] - (1.0 - 0.38) * altr - fact2 * JBT(kAmw)[4];
+        const double al10t5 = log10(tinf);
+        const double alnh5 = (5.5 * al10t5 - 39.40) * al10t5 + 73.13;
+        offset[5] = kLn10 * (alnh5 + 6.0) + hsign * (log(tloc4 / tloc3) + up.sum * JBT(kAmw)[5] / kRstar);
+    }
+    // seasonal-latitudinal term, cut at 800 km by model 7
+    double dlrsl = 0.0;
+    if (!(v7 && alt >= 800.0)) {
+        double years = (mjd - 36204.0) / 365.2422;
+        double capphi = years - trunc(years);
+        if (capphi == 0.0) capphi = copysign(0.0, years);
+        const double sgn = lat >= 0.0 ? 1.0 : -1.0;
+        const double hm90 = alt - 90.0;
+        dlrsl = 0.02 * hm90 * exp(-0.045 * hm90) * sgn * sin(kTwoPi * capphi + 1.72) * slat * slat;
+    }
+    // semiannual term (jb2008.rs:3436-3461)
+    double dlrsa = 0.0;
+    if (z < 2000.0) {
+        bool ok = true;
+        const double day = day_of_year(mjd, &ok);
+        if (!ok) return kErrDomain;
+        const double* fzm = JBT(kFzm);
+        const double* gtm = JBT(kGtm);
+        const double htz = alt / 1000.0;
+        const double fz = d.f10b - 0.70 * d.s10b - 0.04 * d.m10b;
+        const double fzz = fzm[0] + fz * (fzm[1] + htz * (fzm[2] + fzm[3] * htz + fzm[4] * fz));
+        const double fg = d.f10b - 0.75 * d.s10b - 0.37 * d.m10b;
+        double s1, c1;
+        sincos(kTwoPi * (day - 1.0) / 365.0, &s1, &c1);
+        const double s2 = 2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
+        const double gtz = gtm[0] + gtm[1] * s1 + gtm[2] * c1 + gtm[3] * s2 + gtm[4] * c2 +
+                           fg * (gtm[5] + gtm[6] * s1 + gtm[7] * c1 + gtm[8] * s2 + gtm[9] * c2);
+        dlrsa = fmax(fzz, 1.0e-6) * gtz;
+    }
+    const double dlr = kLn10 * (dlrsl + dlrsa);
+    // compensated species sum
+    double sum = 0.0, comp = 0.0, simple = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const double term = factor[i] * exp(offset[i] + dlr) * JBT(kAmw)[i];
+        const double tmp = term - comp;
+        const double next = sum + tmp;
+        comp = (next - sum) - tmp;
+        sum = next;
+        simple += term;
+    }
+    double fs = sum - comp;
+    if (isnan(fs) && isinf(simple)) fs = simple;
+    rho = fs / kAvogadro;
+    double fex = 1.0;
+    if (alt >= 1000.0 && alt < 1500.0) {
+        double zeta = (alt - 1000.0) * 0.002;
+        double f15c = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * 1500.0 + JBT(kCht)[3] * d.f10b * 1500.0;
+        double f15cz = (JBT(kCht)[2] + JBT(kCht)[3] * d.f10b) * 500.0;
+        double fex2 = 3.0 * f15c - f15cz - 3.0;
+        double fex3 = f15cz - 2.0 * f15c + 2.0;
+        fex = 1.0 + zeta * zeta * (fex2 + fex3 * zeta);
+    } else if (alt >= 1500.0) {
+        fex = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * alt + JBT(kCht)[3] * d.f10b * alt;
+    }
+    const double out = rho * fex;
+    if (!(isfinite(out) && out > 0.0)) return kErrDomain;
+    return out;
+}
+
+// The density of atm_model 4 (exact, with the optional sweep fits) or 5-7.
+BQP_HD double density_model(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
+                            const Drivers& d, int model, const JbFit* fit = nullptr) {
+    if (model == 4) return density(mjd, sun_dec, hour_angle, lat, alt_m, d, fit);
+    return density_coarse(mjd, sun_dec, hour_angle, lat, alt_m, d, model);
+}
+
 #ifdef __CUDACC__
 // ------------------------------------------------------------------------
 // Lane-group form for the drag kernel: the density of one state is computed

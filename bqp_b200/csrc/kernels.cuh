@@ -35,6 +35,7 @@ struct ForceParams {
     int32_t gravity_on;
     int32_t drag, sun, moon;
     int32_t ground_check;  // terminal ground event (final-state path)
+    int32_t atm_model;     // JB2008 profile: 4 exact; 5, 6, 7 the coarse quadrature profiles
     double earth_radius;
     double omega;
     double mu_sun, mu_moon;
@@ -172,7 +173,7 @@ struct Encke {
         jb::Drivers dr = fp->drivers;
         // rhs.rs:3560-3571: no drivers at this instant -> NaN density
         if (fp->dtab.n_solar > 0 && !jb::lookup_drivers(fp->dtab, jd, &dr)) return NAN;
-        double rho = jb::density(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->fit);
+        double rho = jb::density_model(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->atm_model, fp->fit);
         if (!(rho > 0.0) || !isfinite(rho)) return NAN;
         if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         return rho;

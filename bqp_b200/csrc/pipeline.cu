@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
 // [0, nb_hi) take list 0 with LH lanes per state, the rest list 1 with LL),
 // so that a stage's states are resident together in as few waves as the
 // register budget allows.
-template <int L>
+template <int L, bool kCoarse = false>
 __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs& P, int list, int block) {
     const int gt = block * blockDim.x + threadIdx.x;
     const int item = gt / L;
@@ -292,6 +292,8 @@ __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs&
             // same verdict on every lane of the group
             if (fp.dtab.n_solar > 0 && !jb::lookup_drivers(fp.dtab, P.jd[slot], &dr))
                 rho = NAN;
+            else if (kCoarse)
+                rho = jb::density_coarse(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, dr, fp.atm_model);
             else
                 rho = jb::density_group<L>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, dr, q, gmask,
                                            fp.fit != nullptr, fp.fit2);
@@ -322,6 +324,13 @@ template <int LH, int LL>
 __global__ void __launch_bounds__(kBlock, BQP_DRAG_MIN_BLOCKS) pl_drag(ForceParams fp, PipeBufs P, int nb_hi) {
     if ((int)blockIdx.x < nb_hi) drag_rows<LH>(fp, P, 0, blockIdx.x);
     else drag_rows<LL>(fp, P, 1, blockIdx.x - nb_hi);
+}
+
+// The coarse profiles (atm_model 5-7): a short chain per state, one lane
+// each, both altitude lists in one launch.
+__global__ void __launch_bounds__(kBlock) pl_drag_coarse(ForceParams fp, PipeBufs P, int nb_hi) {
+    if ((int)blockIdx.x < nb_hi) drag_rows<1, true>(fp, P, 0, blockIdx.x);
+    else drag_rows<1, true>(fp, P, 1, blockIdx.x - nb_hi);
 }
 
 // ------------------------------------------------------------------ control
@@ -517,7 +526,11 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
                 });
             if (A.force.drag)
                 timed(kKcDrag, [&] {
-                    pl_drag<kLanesHigh, kLanesLow><<<dblocks_hi + dblocks_lo, kBlock, 0, st>>>(A.force, P, dblocks_hi);
+                    if (A.force.atm_model == 4)
+                        pl_drag<kLanesHigh, kLanesLow><<<dblocks_hi + dblocks_lo, kBlock, 0, st>>>(A.force, P,
+                                                                                                 dblocks_hi);
+                    else
+                        pl_drag_coarse<<<2 * blocks, kBlock, 0, st>>>(A.force, P, blocks);
                 });
         }
         timed(kKcControl, [&] { pl_control<M><<<blocks, kBlock, 0, st>>>(A, P, cur, dense ? 1 : 0, timed_out); });

@@ -73,7 +73,9 @@ extern "C" {
 typedef struct bqp_force_config {
     int32_t order;          /* spherical-harmonic degree/order, 0..120 */
     int32_t force_flags;    /* BQP_FORCE_* */
-    int32_t atm_model;      /* 4 exact JB2008; 7 accepted and evaluated with the exact kernel */
+    int32_t atm_model;      /* JB2008 profile (AtmModel, lightyear_odeint_rs/src/rhs.rs:1607-1698;
+                               jb_rs/src/jb2008.rs:339-838): 4 exact; 5, 6 the coarse log-quadrature
+                               profiles; 7 the fitted kernel (the Python default) */
     int32_t method;         /* BQP_METHOD_* */
     int32_t error_control;  /* 0: absolute eps, max-norm; 1: scaled rtol/atol, RMS */
     int32_t ground_check;   /* 1: stop with BQP_ST_GROUND below 100 km altitude */
@@ -156,6 +158,16 @@ int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches);
  * worst[5] the T_inf range of the 2-D fits.  No counterpart in the
  * reference, whose quadrature these fits replace. */
 int bqp_jb_fit_check(const double* drivers, double* worst6);
+
+/* JB2008 density on the host, by the same function the force kernels run:
+ * in[14 i] = UTC MJD, solar declination (rad), hour angle of the satellite
+ * from the Sun (rad), geocentric latitude (rad), altitude (m), F10, F10bar,
+ * S10, S10bar, M10, M10bar, Y10, Y10bar, dTc (K); out[i] kg/m^3, or a
+ * negative code (-1 non-finite input, -2 altitude below 90 km, -3 angle out
+ * of range, -4 non-positive index, -5 numerical domain).  model 4: the exact
+ * quadrature (jb_rs/src/jb2008.rs:880); 5, 6, 7: the coarse profiles
+ * (jb2008.rs:890-920, 7 = jb2008_density_fitted_v7). */
+int bqp_jb_density(int32_t model, int64_t n, const double* in14, double* out);
 
 /* JB2008 space-weather tables: the SET SOLFSMY (daily F10, S10, M10, Y10 and
  * their 81-day centred means) and DTCFILE (hourly dTc, K) texts.  Replaces

@@ -30,8 +30,9 @@ ENGINES = ["pipeline", "persistent"]
 
 
 def ctx_for(text, order, flags=0, method="dop853", eps=1e-8, dt_max=300.0, rtol=None, atol=None,
-            am=0.01, cd=2.2, ground=False, max_attempts=None, engine="pipeline", quadrature=False):
+            am=0.01, cd=2.2, ground=False, max_attempts=None, engine="pipeline", quadrature=False, atm_model=4):
     cfg = N.default_config()
+    cfg.atm_model = atm_model
     cfg.engine = N.ENGINES[engine]
     cfg.drag_quadrature = int(quadrature)
     cfg.order = order
@@ -52,8 +53,8 @@ def ctx_for(text, order, flags=0, method="dop853", eps=1e-8, dt_max=300.0, rtol=
     return N.Context(text, cfg)
 
 
-def oracle_force(text, order, flags=0):
-    return O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8))
+def oracle_force(text, order, flags=0, atm_model=4):
+    return O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8), atm_model=atm_model)
 
 
 def random_positions(n, seed, rmin=6578.0, rmax=7578.0):
@@ -129,6 +130,66 @@ def test_encke_rhs_matches_oracle(flags):
         scale = MU / r ** 2  # full-field magnitude
         assert np.array_equal(got[i, :3], ref[:3])
         assert np.abs(got[i, 3:] - ref[3:]).max() <= 1e-12 * scale, (i, got[i], ref)
+
+
+@pytest.mark.parametrize("model", [5, 6, 7])
+def test_encke_rhs_coarse_atmosphere_matches_oracle(model):
+    """The coarse JB2008 profiles (7: the reference's default) in the force
+    call: 70x70 + drag + Sun/Moon on 256 states at 300-1500 km."""
+    order = 70
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    ctx = ctx_for(text, order, flags=flags, atm_model=model)
+    F = oracle_force(text, order, flags, atm_model=model)
+    n = 256
+    rng = np.random.default_rng(50 + model)
+    states = workloads.leo_states(n, seed=50 + model)
+    # spread the altitudes over the profiles' segments (below / above 500 km,
+    # the 800 km cut of the seasonal-latitudinal term, 1000-1500 km)
+    r = np.linalg.norm(states[:, :3], axis=1)
+    states[:, :3] *= ((6378.137 + rng.uniform(300.0, 1500.0, n)) / r)[:, None]
+    equ, ok = N.eci_to_equinoctial(states)
+    assert ok.all()
+    t = rng.uniform(0.0, 5400.0, n)
+    seg_t0 = rng.uniform(0.0, 1.0, n) * t
+    delta = np.concatenate([rng.normal(0, 3.0, (n, 3)), rng.normal(0, 3e-3, (n, 3))], axis=1)
+    bal = workloads.leo_ballistics(n, seed=3)
+    epoch = EPOCH + rng.uniform(0, 30, n)
+    got = ctx.rhs(equ, seg_t0, epoch, t, delta, bal)
+    exact = ctx_for(text, order, flags=flags, atm_model=4).rhs(equ, seg_t0, epoch, t, delta, bal)
+    moved = 0
+    for i in range(n):
+        ref = F.rhs(equ[i], seg_t0[i], epoch[i], bal[i, 0], bal[i, 1], t[i], delta[i])
+        base, _ = O.equinoc2eci(equ[i], t[i] - seg_t0[i])
+        scale = MU / np.linalg.norm(base[:3] + delta[i, :3]) ** 2
+        assert np.array_equal(got[i, :3], ref[:3])
+        assert np.abs(got[i, 3:] - ref[3:]).max() <= 1e-12 * scale, (i, got[i], ref)
+        moved += not np.array_equal(got[i, 3:], exact[i, 3:])
+    assert moved > n // 2  # the profile is not the exact model
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_adaptive_final_default_atmosphere_matches_oracle(engine):
+    """The reference's default atmosphere (atm_model 7) in adaptive
+    propagation, as test_adaptive_final_matches_oracle."""
+    order = 70
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    eps = 1e-10
+    ctx = ctx_for(text, order, flags=flags, method="dop853", eps=eps, engine=engine, atm_model=7)
+    F = oracle_force(text, order, flags, atm_model=7)
+    n = 24
+    states = workloads.leo_states(n, seed=37)
+    bal = workloads.leo_ballistics(n, seed=37)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 8000.0
+    got, st, steps, evals = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    ref_d, ref_st, ref_steps, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, EPOCH, tf, bal)
+    assert (st == 0).all() and (ref_st == 0).all()
+    for i in range(n):
+        ref = O.equinoc2eci(equ[i], tf)[0] + ref_d[i]
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+    assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
 
 
 def test_jb2008_sweep_fit_matches_quadrature():
@@ -443,6 +504,33 @@ def test_reference_smoke_sequence():
     assert full["steps"] > 0 and full["rhs_evals"] >= 12 * full["steps"]
     fs = api.propagate_final(eci, EPOCH, tof_s=3600.0, srp=False, method="dop853")
     assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3
+
+
+def test_python_defaults_match_oracle():
+    """api.propagate with every reference default but srp (DIR-R6 at degree
+    5, JB2008 atm_model 7 with the default drivers, Sun/Moon, Vern7 at tol
+    1e-8, dt_max 300 s) against the oracle's sampled path with the same
+    settings, on a 300 s grid over one hour."""
+    from bqp_b200 import api as A
+
+    eci = A.kep_to_eci(np.array([6778.137, 0.001, 51.6, 30.0, 40.0, 50.0]))
+    grid = np.arange(0.0, 3601.0, 300.0)
+    out = A.propagate(eci, EPOCH, 3600.0, times_s=grid, srp=False)
+    assert out["completed"] and np.array_equal(out["times_s"], grid)
+    text = A._DEFAULT_FIELD.read_text()
+    F = O.Force(text, 5, drag=True, sun=True, moon=True, atm_model=7)
+    equ, rc = O.eci2equinoc(eci)
+    assert rc == 0
+    d, st, steps, evals, nw = O.propagate_sampled(F, O.ctrl("vern7", eps=1e-8, dt_max=300.0), equ, EPOCH, 3600.0,
+                                                   0.01, 2.2, grid)
+    assert st == 0 and nw == grid.size
+    ref = np.array([O.equinoc2eci(equ, t)[0] for t in grid]) + d
+    err = np.linalg.norm(out["states_eci"][:, :3] - ref[:, :3], axis=1)
+    # each solution within ~10 eps per step of the exact one (final sample);
+    # the interior samples are the cubic-Hermite interpolants between steps
+    assert err[-1] <= 2 * 10 * max(out["steps"], steps) * 1e-8, (err[-1], out["steps"])
+    assert err.max() <= 2e-5, err
+    assert abs(out["steps"] - steps) <= max(3, 0.05 * steps)
 
 
 def test_default_method_is_vern7():

@@ -191,3 +191,20 @@ def test_oracle_sampled_batch_equals_rows():
                                                    grid)
         assert si == st[i] == 0 and nwi == nw[i] == grid.size
         assert np.array_equal(di, d[i]) and stp == steps[i] and ev == evals[i]
+
+
+@pytest.mark.parametrize("model", [4, 5, 6, 7])
+def test_library_density_equals_oracle_bit_for_bit(model):
+    # the kernels' own JB2008 function, evaluated on the host, against the
+    # oracle on the reference's broad grid (models 4-7)
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_oracle_golden import BROAD_ALT, broad_grid_input
+
+    rows = [broad_grid_input(mjd, alt, lat, lst) for mjd in (51999.75, 57000.25, 60648.5) for alt in BROAD_ALT
+            for lat in (-75.0, 0.0, 45.0) for lst in (0.0, 12.0, 18.0)]
+    got = N.jb_density(model, np.array(rows))
+    want = np.array([O.jb2008_model(r, model) for r in rows])
+    assert np.array_equal(got, want)
+    with pytest.raises(N.NativeError):
+        N.jb_density(3, np.array(rows[:1]))
