@@ -131,8 +131,31 @@ def study(order=120, samples=1 << 24, epochs=4, batch=16384, lr=2e-3, n_eval=200
     }
 
 
+def infer_probe(n: int, order: int = 20, samples: int = 1 << 20) -> dict:
+    """The capture case of the fused inference kernel: a surrogate trained for
+    one epoch on a 20x20 field, then three device-resident inference calls
+    on n positions (the launches a profiler captures)."""
+    import torch
+
+    text = W.synthetic_field(order)
+    ctx = _ctx(text, order)
+    ctx.surrogate_train(samples=samples, epochs=1, batch=8192)
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    pos = d * rng.uniform(6578.0, 7578.0, n)[:, None]
+    d_pos = torch.tensor(pos, device="cuda", dtype=torch.float64)
+    d_acc = torch.empty_like(d_pos)
+    for _ in range(3):
+        ctx.surrogate_infer_device(n, d_pos.data_ptr(), d_acc.data_ptr())
+    torch.cuda.synchronize()
+    return {"positions": n, "calls": 3, "finite": bool(torch.isfinite(d_acc).all().item())}
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--infer-probe", type=int, default=0,
+                    help="only the inference capture case: one-epoch 20x20 surrogate, 3 calls on this many positions")
     ap.add_argument("--order", type=int, default=120)
     ap.add_argument("--samples", type=int, default=1 << 24)
     ap.add_argument("--epochs", type=int, default=4)
@@ -142,6 +165,9 @@ def main():
     ap.add_argument("--prop-seconds", type=float, default=5400.0)
     ap.add_argument("--eps-form", type=float, default=1e-9)
     args = ap.parse_args()
+    if args.infer_probe:
+        print(json.dumps(infer_probe(args.infer_probe)), flush=True)
+        return
     print(json.dumps(study(args.order, args.samples, args.epochs, args.batch, args.lr, n_prop=args.propagate,
                            prop_s=args.prop_seconds, eps_form=args.eps_form)), flush=True)
 
