@@ -76,7 +76,7 @@ SIGNATURES = [
     ("bqp_ctx_set_config", C.c_int, [_vp, C.POINTER(ForceConfig)]),
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
     ("bqp_jb_fit_check", C.c_int, [_dp, _dp]),
-    ("bqp_jb_density", C.c_int, [C.c_int32, C.c_int64, _dp, _dp]),
+    ("bqp_jb_density", C.c_int, [C.c_int32, C.c_int32, C.c_int64, _dp, _dp]),
     ("bqp_ctx_set_jb_drivers", C.c_int, [_vp, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_double,
                                          C.c_double]),
     ("bqp_ctx_jb_lookup", C.c_int, [_vp, _dp, C.c_int64, _dp, _ip]),
@@ -487,12 +487,13 @@ def jb_drivers_check(solfsmy, dtcfile, utc_jd=()):
     return (int(counts[0]), int(counts[1])), out, ok.astype(bool)
 
 
-def jb_density(model: int, inputs) -> np.ndarray:
+def jb_density(model: int, inputs, fp32: bool = False) -> np.ndarray:
     """Host evaluation of the JB2008 density by the kernels' own function:
-    inputs [n][14] (see bqp_jb_density), model 4-7."""
+    inputs [n][14] (see bqp_jb_density), model 4-7; fp32: the split form's
+    FP32 arithmetic (models 5-7)."""
     x = f64(inputs).reshape(-1, 14)
     out = np.empty(x.shape[0])
-    check(lib().bqp_jb_density(int(model), x.shape[0], dptr(x), dptr(out)))
+    check(lib().bqp_jb_density(int(model), int(bool(fp32)), x.shape[0], dptr(x), dptr(out)))
     return out
 
 

@@ -561,7 +561,9 @@ int validate_cfg(const bqp_force_config* c) {
     if (c->split_degree != 0 && c->engine == BQP_ENGINE_PERSISTENT)
         return fail(BQP_E_UNSUPPORTED, "split precision runs in the stage-synchronous engine");
     if (c->drag_fp32 != 0 && c->drag_fp32 != 1) return fail(BQP_E_ARG, "drag_fp32 must be 0 or 1");
-    if (c->drag_fp32) return fail(BQP_E_UNSUPPORTED, "the FP32 JB2008 density is not built");
+    if (c->drag_fp32 && (c->force_flags & BQP_FORCE_DRAG) && c->atm_model == 4)
+        return fail(BQP_E_UNSUPPORTED,
+                    "the FP32 JB2008 density is built for the coarse profiles (atm_model 5, 6, 7), not the exact model");
     if (c->surrogate != 0 && c->surrogate != 1) return fail(BQP_E_ARG, "surrogate must be 0 or 1");
     if (c->surrogate && c->engine == BQP_ENGINE_PERSISTENT)
         return fail(BQP_E_UNSUPPORTED, "the surrogate gravity runs in the stage-synchronous engine");
@@ -582,6 +584,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.moon = (c.force_flags & BQP_FORCE_MOON) ? 1 : 0;
     fp.ground_check = c.ground_check;
     fp.atm_model = (c.force_flags & BQP_FORCE_DRAG) ? c.atm_model : 4;
+    fp.drag_fp32 = c.drag_fp32;
     fp.earth_radius = c.earth_radius;
     fp.omega = c.omega_earth;
     fp.mu_sun = c.mu_sun;
@@ -1113,13 +1116,15 @@ int bqp_jb_fit_check(const double* drivers, double* worst) {
     return 0;
 }
 
-int bqp_jb_density(int32_t model, int64_t n, const double* in, double* out) {
+int bqp_jb_density(int32_t model, int32_t fp32, int64_t n, const double* in, double* out) {
     if (model < 4 || model > 7) return fail(BQP_E_ARG, "model must be 4, 5, 6 or 7, got %d", model);
+    if (fp32 && model == 4) return fail(BQP_E_UNSUPPORTED, "the FP32 density is built for models 5, 6, 7");
     if (n < 0 || (n > 0 && (!in || !out))) return fail(BQP_E_ARG, "bad buffers");
     for (int64_t i = 0; i < n; ++i) {
         const double* x = in + 14 * i;
         const jb::Drivers d{x[5], x[6], x[7], x[8], x[9], x[10], x[11], x[12], x[13]};
-        out[i] = jb::density_model(x[0], x[1], x[2], x[3], x[4], d, model);
+        out[i] = fp32 ? jb::density_coarse_r<float>(x[0], x[1], x[2], x[3], x[4], d, model)
+                      : jb::density_model(x[0], x[1], x[2], x[3], x[4], d, model);
     }
     return 0;
 }

@@ -560,207 +560,379 @@ BQP_JB_TABLE(kV7Tloc3, 15, {1.5437971407829077e3, 1.039876918772851e3, -4.373905
                             -5.114031895849491e-5, 2.0780285514906778e-4, -6.117111036343099e-5,
                             -4.124441270261577e-6, 6.126914161375104e-6, -8.797891983987146e-7})
 
+// The coarse profiles are written once for the arithmetic type R: FP64 (the
+// reference's) or FP32 (the split form's density, drag_fp32).  These pick the
+// math function of each type; for double they are the calls the FP64 code
+// has always made.
+namespace rm {
+BQP_HD double log(double x) { return ::log(x); }
+BQP_HD float log(float x) { return ::logf(x); }
+BQP_HD double log10(double x) { return ::log10(x); }
+BQP_HD float log10(float x) { return ::log10f(x); }
+BQP_HD double exp(double x) { return ::exp(x); }
+BQP_HD float exp(float x) { return ::expf(x); }
+BQP_HD double atan(double x) { return ::atan(x); }
+BQP_HD float atan(float x) { return ::atanf(x); }
+BQP_HD double pow(double x, double y) { return ::pow(x, y); }
+BQP_HD float pow(float x, float y) { return ::powf(x, y); }
+BQP_HD double sin(double x) { return ::sin(x); }
+BQP_HD float sin(float x) { return ::sinf(x); }
+BQP_HD double cos(double x) { return ::cos(x); }
+BQP_HD float cos(float x) { return ::cosf(x); }
+BQP_HD void sincos(double x, double* s, double* c) { ::sincos(x, s, c); }
+BQP_HD void sincos(float x, float* s, float* c) { ::sincosf(x, s, c); }
+BQP_HD double sqrt(double x) { return ::sqrt(x); }
+BQP_HD float sqrt(float x) { return ::sqrtf(x); }
+BQP_HD double fma(double a, double b, double c) { return ::fma(a, b, c); }
+BQP_HD float fma(float a, float b, float c) { return ::fmaf(a, b, c); }
+BQP_HD double fmin(double a, double b) { return ::fmin(a, b); }
+BQP_HD float fmin(float a, float b) { return ::fminf(a, b); }
+BQP_HD double fmax(double a, double b) { return ::fmax(a, b); }
+BQP_HD float fmax(float a, float b) { return ::fmaxf(a, b); }
+BQP_HD double fabs(double x) { return ::fabs(x); }
+BQP_HD float fabs(float x) { return ::fabsf(x); }
+BQP_HD double floor(double x) { return ::floor(x); }
+BQP_HD float floor(float x) { return ::floorf(x); }
+BQP_HD double fmod(double a, double b) { return ::fmod(a, b); }
+BQP_HD float fmod(float a, float b) { return ::fmodf(a, b); }
+}  // namespace rm
+
 // Estrin evaluation of a 15-term series (the reference's tree,
 // jb2008.rs:561-643): pairs fused through u, u^2, u^4, u^8, the last
 // coefficient joining at the u^2 level.
-BQP_HD double v7_series(const double* c, double u) {
-    const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
-    const double a0 = fma(c[1], u, c[0]), a1 = fma(c[3], u, c[2]), a2 = fma(c[5], u, c[4]);
-    const double a3 = fma(c[7], u, c[6]), a4 = fma(c[9], u, c[8]), a5 = fma(c[11], u, c[10]);
-    const double a6 = fma(c[13], u, c[12]);
-    const double b0 = fma(a1, u2, a0), b1 = fma(a3, u2, a2), b2 = fma(a5, u2, a4), b3 = fma(c[14], u2, a6);
-    return fma(fma(b3, u4, b2), u8, fma(b1, u4, b0));
+template <class R>
+BQP_HD R v7_series(const double* cd, R u) {
+    R c[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) c[i] = (R)cd[i];
+    const R u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
+    const R a0 = rm::fma(c[1], u, c[0]), a1 = rm::fma(c[3], u, c[2]), a2 = rm::fma(c[5], u, c[4]);
+    const R a3 = rm::fma(c[7], u, c[6]), a4 = rm::fma(c[9], u, c[8]), a5 = rm::fma(c[11], u, c[10]);
+    const R a6 = rm::fma(c[13], u, c[12]);
+    const R b0 = rm::fma(a1, u2, a0), b1 = rm::fma(a3, u2, a2), b2 = rm::fma(a5, u2, a4),
+            b3 = rm::fma(c[14], u2, a6);
+    return rm::fma(rm::fma(b3, u4, b2), u8, rm::fma(b1, u4, b0));
 }
 
 // Panel count of a log ratio (jb2008.rs:1515-1526); 0 on a domain error.
-BQP_HD int coarse_panels(double log_ratio) {
-    if (!(isfinite(log_ratio) && log_ratio >= 0.0) || floor(log_ratio) >= 2147483646.0) return 0;
-    return (int)floor(log_ratio) + 1;
+template <class R>
+BQP_HD int coarse_panels(R log_ratio) {
+    if (!(isfinite(log_ratio) && log_ratio >= (R)0) || rm::floor(log_ratio) >= (R)2147483520.0) return 0;
+    return (int)rm::floor(log_ratio) + 1;
 }
 
-// As density(), for atm_model 5, 6 or 7.
-BQP_HD double density_coarse(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
-                             const Drivers& d, int model) {
-    const double step_lower = 0.040, step_middle = model == 5 ? 0.100 : 0.300;
-    const double step_upper = model == 5 ? 0.300 : 0.700;
+// mbar, grav, local_temp, dtc_correction and boole_sweep in R (the same
+// expressions as the FP64 functions above)
+template <class R>
+BQP_HD R mbar_r(R z) {
+    const double* c = JBT(kCxamb);
+    const R dz = z - (R)100.0;
+    return dz * (dz * (dz * (dz * (dz * (dz * (R)c[6] + (R)c[5]) + (R)c[4]) + (R)c[3]) + (R)c[2]) + (R)c[1]) +
+           (R)c[0];
+}
+template <class R>
+BQP_HD R grav_r(R z) {
+    const R s = (R)1.0 + z / (R)kEarthR;
+    return (R)kG0 / (s * s);
+}
+template <class R>
+BQP_HD R local_temp_r(R z, const R* tc) {
+    const R dz = z - (R)125.0;
+    if (dz <= (R)0.0) return (((R)-9.8204695e-6 * dz - (R)7.3039742e-4) * dz * dz + (R)1.0) * dz * tc[1] + tc[0];
+    return tc[0] + tc[2] * rm::atan(tc[3] * dz * ((R)1.0 + (R)4.5e-6 * (dz * dz * rm::sqrt(dz))));
+}
+template <class R>
+BQP_HD R dtc_correction_r(R f10, R st_hour, R cs, R alt) {
+    if (!(alt >= (R)120.0 && alt <= (R)800.0)) return (R)0.0;
+    const R st = st_hour / (R)24.0;
+    const R fs = (f10 - (R)100.0) / (R)100.0;
+    R c[23], b[19];
+#pragma unroll
+    for (int i = 0; i < 23; ++i) c[i] = (R)JBT(kCdt)[i];
+#pragma unroll
+    for (int i = 0; i < 19; ++i) b[i] = (R)JBT(kBdt)[i];
+    const R p1c = c[0] + fs * (c[1] + st * (c[2] + st * (c[3] + st * (c[4] + st * (c[5] + st * c[6]))))) +
+                  cs * st * (c[7] + st * (c[8] + st * (c[9] + st * (c[10] + st * c[11])))) +
+                  cs * (c[12] + fs * (c[13] + st * (c[14] + st * c[15])));
+    const R p2c = c[16] + st * cs * (c[17] + st * (c[18] + st * c[19])) +
+                  fs * cs * (c[20] + st * (c[21] + st * c[22]));
+    const R p2b = b[12] + st * (b[13] + st * (b[14] + st * (b[15] + st * (b[16] + st * b[17]))));
+    const R p1b_base = b[0] + fs * (b[1] + st * (b[2] + st * (b[3] + st * (b[4] + st * (b[5] + st * b[6])))));
+    const R p1b_st = st * (b[7] + st * (b[8] + st * (b[9] + st * (b[10] + st * b[11]))));
+    if (alt > (R)600.0) {
+        const R aa = p1b_base + cs * (p1b_st + (R)6.0 * p2b + b[18]);
+        const R bb = cs * p2b;
+        const R cc = -((R)3.0 * aa + (R)4.0 * bb) / (R)4.0;
+        const R dd = (aa + bb) / (R)4.0;
+        const R zp = (alt - (R)600.0) / (R)100.0;
+        return aa + zp * (bb + zp * (cc + zp * dd));
+    } else if (alt > (R)300.0) {
+        return p1b_base + cs * (p1b_st + alt * p2b / (R)100.0 + b[18]);
+    } else if (alt > (R)240.0) {
+        const R bb = p1c;
+        const R aa = (R)0.8 * bb + p2c;
+        const R d300 = p1b_base + cs * (p1b_st + (R)3.0 * p2b + b[18]);
+        const R d300dz = cs * p2b;
+        const R cc = (R)3.0 * d300 - d300dz - (R)3.0 * aa - (R)2.0 * bb;
+        const R dd = d300 - aa - bb - cc;
+        const R zp = (alt - (R)240.0) / (R)60.0;
+        return aa + zp * (bb + zp * (cc + zp * dd));
+    } else if (alt > (R)200.0) {
+        return p1c * (alt - (R)200.0) / (R)50.0 + p2c;
+    } else {
+        const R cc = (R)3.0 * p2c - p1c;
+        const R dd = p2c - cc;
+        const R zp = (alt - (R)120.0) / (R)80.0;
+        return zp * zp * (cc + dd * zp);
+    }
+}
+template <class R>
+struct SweepR {
+    R sum, z, zend, tloc, gravl, mb, ain;
+};
+template <class R>
+BQP_HD SweepR<R> boole_sweep_r(R z, R zend_start, R zr, int n, R ain, bool with_mbar, const R* tc) {
+    SweepR<R> s;
+    s.sum = (R)0.0;
+    s.zend = zend_start;
+    s.z = z;
+    s.tloc = (R)0.0;
+    s.gravl = (R)0.0;
+    s.mb = (R)0.0;
+    for (int i = 0; i < n; ++i) {
+        R zz = s.zend;
+        s.zend = zr * zz;
+        const R dz = (R)0.25 * (s.zend - zz);
+        R sum1 = (R)kW0 * ain;
+#pragma unroll
+        for (int j = 1; j < 5; ++j) {
+            zz += dz;
+            s.tloc = local_temp_r(zz, tc);
+            s.gravl = grav_r(zz);
+            if (with_mbar) {
+                s.mb = mbar_r(zz);
+                ain = s.mb * s.gravl / s.tloc;
+            } else {
+                ain = s.gravl / s.tloc;
+            }
+            const R w = (j == 1 || j == 3) ? (R)kW1 : (j == 2 ? (R)kW2 : (R)kW0);
+            sum1 += w * ain;
+        }
+        s.sum += dz * sum1;
+        s.z = zz;
+    }
+    s.ain = ain;
+    return s;
+}
+
+// As density(), for atm_model 5, 6 or 7, in R after the input checks.  FP64:
+// the reference's arithmetic.  FP32: the split form's density; its relative
+// error (~1e-6: the exponents reach ~45) moves the drag acceleration by
+// ~1e-15 km/s^2, and number densities (~1e21 per m^3 at 90 km) stay well
+// inside FP32's range.  The epoch terms (fractional year, day of year) are
+// kept in FP64, since an MJD does not fit FP32.
+template <class R>
+BQP_HD double density_coarse_r(double mjd, double sun_dec, double hour_angle, double lat_in, double alt_m,
+                               const Drivers& din, int model) {
+    const R step_lower = (R)0.040, step_middle = model == 5 ? (R)0.100 : (R)0.300;
+    const R step_upper = model == 5 ? (R)0.300 : (R)0.700;
     const bool v7 = model == 7;
-    if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat) ||
-        !isfinite(alt_m) || !isfinite(d.f10) || !isfinite(d.f10b) || !isfinite(d.s10) ||
-        !isfinite(d.s10b) || !isfinite(d.m10) || !isfinite(d.m10b) || !isfinite(d.y10) ||
-        !isfinite(d.y10b) || !isfinite(d.dtc))
+    if (!isfinite(mjd) || !isfinite(sun_dec) || !isfinite(hour_angle) || !isfinite(lat_in) ||
+        !isfinite(alt_m) || !isfinite(din.f10) || !isfinite(din.f10b) || !isfinite(din.s10) ||
+        !isfinite(din.s10b) || !isfinite(din.m10) || !isfinite(din.m10b) || !isfinite(din.y10) ||
+        !isfinite(din.y10b) || !isfinite(din.dtc))
         return kErrNonFinite;
     if (alt_m < 90000.0) return kErrAltitude;
-    if (!(sun_dec >= -kPi / 2 && sun_dec <= kPi / 2) || !(lat >= -kPi / 2 && lat <= kPi / 2))
+    if (!(sun_dec >= -kPi / 2 && sun_dec <= kPi / 2) || !(lat_in >= -kPi / 2 && lat_in <= kPi / 2))
         return kErrAngle;
-    if (d.f10 <= 0.0 || d.f10b <= 0.0 || d.s10 <= 0.0 || d.s10b <= 0.0 || d.m10 <= 0.0 ||
-        d.m10b <= 0.0 || d.y10 <= 0.0 || d.y10b <= 0.0)
+    if (din.f10 <= 0.0 || din.f10b <= 0.0 || din.s10 <= 0.0 || din.s10b <= 0.0 || din.m10 <= 0.0 ||
+        din.m10b <= 0.0 || din.y10 <= 0.0 || din.y10b <= 0.0)
         return kErrIndex;
-    const double alt = alt_m / 1000.0;
+    const R alt = (R)(alt_m / 1000.0);
+    const R lat = (R)lat_in, sdec = (R)sun_dec;
+    const R f10 = (R)din.f10, f10b = (R)din.f10b, s10 = (R)din.s10, s10b = (R)din.s10b, m10 = (R)din.m10,
+            m10b = (R)din.m10b, y10 = (R)din.y10, y10b = (R)din.y10b, dtc_k = (R)din.dtc;
+    const R pi = (R)kPi, two_pi = (R)kTwoPi;
     // exospheric temperature and profile, as density()
-    double fn = fmin(pow(d.f10b / 240.0, 0.25), 1.0);
-    double fsb = d.f10b * fn + d.s10b * (1.0 - fn);
-    double tsubc = 392.4 + 3.227 * fsb + 0.298 * (d.f10 - d.f10b) + 2.259 * (d.s10 - d.s10b) +
-                   0.312 * (d.m10 - d.m10b) + 0.178 * (d.y10 - d.y10b);
-    double eta = 0.5 * fabs(lat - sun_dec);
-    double theta = 0.5 * fabs(lat + sun_dec);
-    double h = hour_angle;
-    if (!(h >= 0.0 && h < kTwoPi)) {
-        if (h < 0.0 && h > -kTwoPi) {
-            h += kTwoPi;
+    const R fn = rm::fmin(rm::pow(f10b / (R)240.0, (R)0.25), (R)1.0);
+    const R fsb = f10b * fn + s10b * ((R)1.0 - fn);
+    const R tsubc = (R)392.4 + (R)3.227 * fsb + (R)0.298 * (f10 - f10b) + (R)2.259 * (s10 - s10b) +
+                    (R)0.312 * (m10 - m10b) + (R)0.178 * (y10 - y10b);
+    const R eta = (R)0.5 * rm::fabs(lat - sdec);
+    const R theta = (R)0.5 * rm::fabs(lat + sdec);
+    R h = (R)hour_angle;
+    if (!(h >= (R)0.0 && h < two_pi)) {
+        if (h < (R)0.0 && h > -two_pi) {
+            h += two_pi;
         } else {
-            h = fmod(h, kTwoPi);
-            if (h < 0.0) h += kTwoPi;
+            h = rm::fmod(h, two_pi);
+            if (h < (R)0.0) h += two_pi;
         }
     }
-    double tau = h - 0.64577182 + 0.10471976 * sin(h + 0.75049158);
-    double st_hour = ((h + kPi) * (180.0 / kPi)) / 15.0;
-    if (st_hour >= 24.0) st_hour -= 24.0;
-    else if (st_hour < 0.0) st_hour += 24.0;
-    double slat, clat;
-    sincos(lat, &slat, &clat);
-    double cos_eta = five_halves(cos(eta));
-    double sin_theta = five_halves(sin(theta));
-    double cos_tau = fabs(cos(0.5 * tau));
-    double df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
-    double tsubl = tsubc * (1.0 + 0.31 * df);
-    double tinf = tsubl + d.dtc + dtc_correction(d.f10, st_hour, clat, alt);
-    double tsubx = 444.3807 + 0.02385 * tinf - 392.8292 * exp(-0.0021357 * tinf);
-    double gsubx = 0.054285714 * (tsubx - 183.0);
-    double tc[4];
+    const R tau = h - (R)0.64577182 + (R)0.10471976 * rm::sin(h + (R)0.75049158);
+    R st_hour = ((h + pi) * ((R)180.0 / pi)) / (R)15.0;
+    if (st_hour >= (R)24.0) st_hour -= (R)24.0;
+    else if (st_hour < (R)0.0) st_hour += (R)24.0;
+    R slat, clat;
+    rm::sincos(lat, &slat, &clat);
+    const R ce = rm::cos(eta), sn = rm::sin(theta);
+    const R cos_eta = ce * ce * rm::sqrt(ce);
+    const R sin_theta = sn * sn * rm::sqrt(sn);
+    const R cos_tau = rm::fabs(rm::cos((R)0.5 * tau));
+    const R df = sin_theta + (cos_eta - sin_theta) * cos_tau * cos_tau * cos_tau;
+    const R tsubl = tsubc * ((R)1.0 + (R)0.31 * df);
+    const R tinf = tsubl + dtc_k + dtc_correction_r(f10, st_hour, clat, alt);
+    const R tsubx = (R)444.3807 + (R)0.02385 * tinf - (R)392.8292 * rm::exp((R)-0.0021357 * tinf);
+    const R gsubx = (R)0.054285714 * (tsubx - (R)183.0);
+    R tc[4];
     tc[0] = tsubx;
     tc[1] = gsubx;
-    tc[2] = (tinf - tsubx) / (kPi / 2);
+    tc[2] = (tinf - tsubx) / (pi / (R)2);
     tc[3] = gsubx / tc[2];
     // the fit domain is judged on Texo rebuilt from the profile (jb2008.rs:521-524)
-    const double texo = tc[0] + tc[2] * (kPi / 2);
-    const bool fit_in = v7 && texo >= kV7TexoLo && texo <= kV7TexoHi;
-    const double u = 2.0 * (texo - kV7TexoLo) / (kV7TexoHi - kV7TexoLo) - 1.0;
+    const R texo = tc[0] + tc[2] * (pi / (R)2);
+    const bool fit_in = v7 && texo >= (R)kV7TexoLo && texo <= (R)kV7TexoHi;
+    const R u = (R)2.0 * (texo - (R)kV7TexoLo) / (R)(kV7TexoHi - kV7TexoLo) - (R)1.0;
 
     // 90 km -> min(alt, 105 km): four panels at and above 105 km (the fixed plan)
-    const double z1 = 90.0;
-    const double mb1 = mbar(z1);
-    const double tloc1 = local_temp(z1, tc);
-    const bool lower_planned = alt >= 105.0;
-    double al = log(fmin(alt, 105.0) / z1);
+    const R z1 = (R)90.0;
+    const R mb1 = mbar_r(z1);
+    const R tloc1 = local_temp_r(z1, tc);
+    const bool lower_planned = alt >= (R)105.0;
+    R al = rm::log(rm::fmin(alt, (R)105.0) / z1);
     int n = coarse_panels(al / step_lower);
     if (n == 0) return kErrDomain;
-    Sweep lo = boole_sweep(z1, z1, exp(al / n), n, mb1 * grav(z1) / tloc1, true, tc);
+    SweepR<R> lo = boole_sweep_r(z1, z1, rm::exp(al / (R)n), n, mb1 * grav_r(z1) / tloc1, true, tc);
     if (fit_in && lower_planned) {
         lo.sum = v7_series(JBT(kV7Sub2Lower), u);
         lo.tloc = v7_series(JBT(kV7Tloc2), u);
     }
-    const double mb2 = lo.mb, tloc2 = lo.tloc;
-    double rho = 3.46e-6 * mb2 * tloc1 / exp(lo.sum / kRstar) / (mb1 * tloc2);
-    double anm = kAvogadro * rho;
-    double an = anm / mb2;
-    double fact2 = anm / 28.960;
-    double factor[6] = {JBT(kFrac)[0] * fact2, fact2 * (1.0 + JBT(kFrac)[1]) - an, 2.0 * (an - fact2),
-                        JBT(kFrac)[2] * fact2, JBT(kFrac)[3] * fact2, 1.0};
+    const R mb2 = lo.mb, tloc2 = lo.tloc;
+    const R rstar = (R)kRstar, avog = (R)kAvogadro;
+    R rho = (R)3.46e-6 * mb2 * tloc1 / rm::exp(lo.sum / rstar) / (mb1 * tloc2);
+    const R anm = avog * rho;
+    const R an = anm / mb2;
+    R fact2 = anm / (R)28.960;
+    R factor[6] = {(R)JBT(kFrac)[0] * fact2, fact2 * ((R)1.0 + (R)JBT(kFrac)[1]) - an, (R)2.0 * (an - fact2),
+                   (R)JBT(kFrac)[2] * fact2, (R)JBT(kFrac)[3] * fact2, (R)1.0};
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-        if (factor[i] < 0.0) factor[i] = NAN;  // jb2008.rs:2304-2310
-    double offset[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    double z = lo.z;
-    if (alt <= 105.0) {
+        if (factor[i] < (R)0.0) factor[i] = (R)NAN;  // jb2008.rs:2304-2310
+    R offset[6] = {(R)0.0, (R)0.0, (R)0.0, (R)0.0, (R)0.0, (R)0.0};
+    R z = lo.z;
+    if (alt <= (R)105.0) {
         factor[5] = factor[4];
-        offset[5] = offset[4] - 25.0;
+        offset[5] = offset[4] - (R)25.0;
     } else {
         // 105 km -> min(alt, 500 km): the fixed six-panel plan at and above 500 km
-        al = log(fmin(alt, 500.0) / z);
+        al = rm::log(rm::fmin(alt, (R)500.0) / z);
         n = coarse_panels(al / step_middle);
         if (n == 0) return kErrDomain;
-        Sweep mid = boole_sweep(z, lo.zend, exp(al / n), n, lo.gravl / tloc2, false, tc);
-        if (fit_in && lower_planned && alt >= 500.0) {
+        SweepR<R> mid = boole_sweep_r(z, lo.zend, rm::exp(al / (R)n), n, lo.gravl / tloc2, false, tc);
+        if (fit_in && lower_planned && alt >= (R)500.0) {
             mid.sum = v7_series(JBT(kV7Sub2Middle), u);
             mid.ain = v7_series(JBT(kV7AinMiddle), u);
             mid.tloc = v7_series(JBT(kV7Tloc3), u);
         }
-        const double tloc3 = mid.tloc;
+        const R tloc3 = mid.tloc;
         z = mid.z;
         // between 500 km and alt (jb2008.rs:2032-2085)
-        const double ratio = fmax(alt, 500.0) / z;
-        const double alu = fmax(log(ratio), 0.0);
-        n = coarse_panels(alu / (alt > 500.0 ? step_upper : step_middle));
+        const R ratio = rm::fmax(alt, (R)500.0) / z;
+        const R alu = rm::fmax(rm::log(ratio), (R)0.0);
+        n = coarse_panels(alu / (alt > (R)500.0 ? step_upper : step_middle));
         if (n == 0) return kErrDomain;
-        const double zr = (v7 && n == 1) ? fmax(ratio, 1.0) : exp(alu / n);
-        Sweep up = boole_sweep(z, mid.zend, zr, n, mid.ain, false, tc);
-        const double tloc4 = up.tloc;
+        const R zr = (v7 && n == 1) ? rm::fmax(ratio, (R)1.0) : rm::exp(alu / (R)n);
+        SweepR<R> up = boole_sweep_r(z, mid.zend, zr, n, mid.ain, false, tc);
+        const R tloc4 = up.tloc;
         z = up.z;
-        double altr, hsign;
-        if (alt <= 500.0) {
-            fact2 = mid.sum / kRstar;
-            altr = log(tloc3 / tloc2);
-            hsign = 1.0;
+        R altr, hsign;
+        if (alt <= (R)500.0) {
+            fact2 = mid.sum / rstar;
+            altr = rm::log(tloc3 / tloc2);
+            hsign = (R)1.0;
         } else {
-            fact2 = (mid.sum + up.sum) / kRstar;
-            altr = log(tloc4 / tloc2);
-            hsign = -1.0;
+            fact2 = (mid.sum + up.sum) / rstar;
+            altr = rm::log(tloc4 / tloc2);
+            hsign = (R)-1.0;
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) offset[i] = offset[i] - altr - fact2 * JBT(kAmw)[i];
-        offset[4] = offset[4] - (1.0 - 0.38) * altr - fact2 * JBT(kAmw)[4];
-        const double al10t5 = log10(tinf);
-        const double alnh5 = (5.5 * al10t5 - 39.40) * al10t5 + 73.13;
-        offset[5] = kLn10 * (alnh5 + 6.0) + hsign * (log(tloc4 / tloc3) + up.sum * JBT(kAmw)[5] / kRstar);
+        for (int i = 0; i < 4; ++i) offset[i] = offset[i] - altr - fact2 * (R)JBT(kAmw)[i];
+        offset[4] = offset[4] - ((R)1.0 - (R)0.38) * altr - fact2 * (R)JBT(kAmw)[4];
+        const R al10t5 = rm::log10(tinf);
+        const R alnh5 = ((R)5.5 * al10t5 - (R)39.40) * al10t5 + (R)73.13;
+        offset[5] = (R)kLn10 * (alnh5 + (R)6.0) +
+                    hsign * (rm::log(tloc4 / tloc3) + up.sum * (R)JBT(kAmw)[5] / rstar);
     }
     // seasonal-latitudinal term, cut at 800 km by model 7
-    double dlrsl = 0.0;
-    if (!(v7 && alt >= 800.0)) {
-        double years = (mjd - 36204.0) / 365.2422;
-        double capphi = years - trunc(years);
-        if (capphi == 0.0) capphi = copysign(0.0, years);
-        const double sgn = lat >= 0.0 ? 1.0 : -1.0;
-        const double hm90 = alt - 90.0;
-        dlrsl = 0.02 * hm90 * exp(-0.045 * hm90) * sgn * sin(kTwoPi * capphi + 1.72) * slat * slat;
+    R dlrsl = (R)0.0;
+    if (!(v7 && alt >= (R)800.0)) {
+        const double years = (mjd - 36204.0) / 365.2422;
+        double capphi = years - ::trunc(years);
+        if (capphi == 0.0) capphi = ::copysign(0.0, years);
+        const R sgn = lat_in >= 0.0 ? (R)1.0 : (R)-1.0;
+        const R hm90 = alt - (R)90.0;
+        dlrsl = (R)0.02 * hm90 * rm::exp((R)-0.045 * hm90) * sgn * rm::sin((R)(kTwoPi * capphi + 1.72)) * slat *
+                slat;
     }
     // semiannual term (jb2008.rs:3436-3461)
-    double dlrsa = 0.0;
-    if (z < 2000.0) {
+    R dlrsa = (R)0.0;
+    if (z < (R)2000.0) {
         bool ok = true;
         const double day = day_of_year(mjd, &ok);
         if (!ok) return kErrDomain;
-        const double* fzm = JBT(kFzm);
-        const double* gtm = JBT(kGtm);
-        const double htz = alt / 1000.0;
-        const double fz = d.f10b - 0.70 * d.s10b - 0.04 * d.m10b;
-        const double fzz = fzm[0] + fz * (fzm[1] + htz * (fzm[2] + fzm[3] * htz + fzm[4] * fz));
-        const double fg = d.f10b - 0.75 * d.s10b - 0.37 * d.m10b;
-        double s1, c1;
-        sincos(kTwoPi * (day - 1.0) / 365.0, &s1, &c1);
-        const double s2 = 2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
-        const double gtz = gtm[0] + gtm[1] * s1 + gtm[2] * c1 + gtm[3] * s2 + gtm[4] * c2 +
-                           fg * (gtm[5] + gtm[6] * s1 + gtm[7] * c1 + gtm[8] * s2 + gtm[9] * c2);
-        dlrsa = fmax(fzz, 1.0e-6) * gtz;
+        R fzm[5], gtm[10];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) fzm[i] = (R)JBT(kFzm)[i];
+#pragma unroll
+        for (int i = 0; i < 10; ++i) gtm[i] = (R)JBT(kGtm)[i];
+        const R htz = alt / (R)1000.0;
+        const R fz = f10b - (R)0.70 * s10b - (R)0.04 * m10b;
+        const R fzz = fzm[0] + fz * (fzm[1] + htz * (fzm[2] + fzm[3] * htz + fzm[4] * fz));
+        const R fg = f10b - (R)0.75 * s10b - (R)0.37 * m10b;
+        R s1, c1;
+        rm::sincos((R)(kTwoPi * (day - 1.0) / 365.0), &s1, &c1);
+        const R s2 = (R)2.0 * s1 * c1, c2 = c1 * c1 - s1 * s1;
+        const R gtz = gtm[0] + gtm[1] * s1 + gtm[2] * c1 + gtm[3] * s2 + gtm[4] * c2 +
+                      fg * (gtm[5] + gtm[6] * s1 + gtm[7] * c1 + gtm[8] * s2 + gtm[9] * c2);
+        dlrsa = rm::fmax(fzz, (R)1.0e-6) * gtz;
     }
-    const double dlr = kLn10 * (dlrsl + dlrsa);
+    const R dlr = (R)kLn10 * (dlrsl + dlrsa);
     // compensated species sum
-    double sum = 0.0, comp = 0.0, simple = 0.0;
+    R sum = (R)0.0, comp = (R)0.0, simple = (R)0.0;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        const double term = factor[i] * exp(offset[i] + dlr) * JBT(kAmw)[i];
-        const double tmp = term - comp;
-        const double next = sum + tmp;
+        const R term = factor[i] * rm::exp(offset[i] + dlr) * (R)JBT(kAmw)[i];
+        const R tmp = term - comp;
+        const R next = sum + tmp;
         comp = (next - sum) - tmp;
         sum = next;
         simple += term;
     }
-    double fs = sum - comp;
+    R fs = sum - comp;
     if (isnan(fs) && isinf(simple)) fs = simple;
-    rho = fs / kAvogadro;
-    double fex = 1.0;
-    if (alt >= 1000.0 && alt < 1500.0) {
-        double zeta = (alt - 1000.0) * 0.002;
-        double f15c = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * 1500.0 + JBT(kCht)[3] * d.f10b * 1500.0;
-        double f15cz = (JBT(kCht)[2] + JBT(kCht)[3] * d.f10b) * 500.0;
-        double fex2 = 3.0 * f15c - f15cz - 3.0;
-        double fex3 = f15cz - 2.0 * f15c + 2.0;
-        fex = 1.0 + zeta * zeta * (fex2 + fex3 * zeta);
-    } else if (alt >= 1500.0) {
-        fex = JBT(kCht)[0] + JBT(kCht)[1] * d.f10b + JBT(kCht)[2] * alt + JBT(kCht)[3] * d.f10b * alt;
+    rho = fs / avog;
+    R fex = (R)1.0;
+    if (alt >= (R)1000.0 && alt < (R)1500.0) {
+        R cht[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) cht[i] = (R)JBT(kCht)[i];
+        const R zeta = (alt - (R)1000.0) * (R)0.002;
+        const R f15c = cht[0] + cht[1] * f10b + cht[2] * (R)1500.0 + cht[3] * f10b * (R)1500.0;
+        const R f15cz = (cht[2] + cht[3] * f10b) * (R)500.0;
+        const R fex2 = (R)3.0 * f15c - f15cz - (R)3.0;
+        const R fex3 = f15cz - (R)2.0 * f15c + (R)2.0;
+        fex = (R)1.0 + zeta * zeta * (fex2 + fex3 * zeta);
+    } else if (alt >= (R)1500.0) {
+        fex = (R)JBT(kCht)[0] + (R)JBT(kCht)[1] * f10b + (R)JBT(kCht)[2] * alt + (R)JBT(kCht)[3] * f10b * alt;
     }
-    const double out = rho * fex;
+    const double out = (double)(rho * fex);
     if (!(isfinite(out) && out > 0.0)) return kErrDomain;
     return out;
+}
+
+BQP_HD double density_coarse(double mjd, double sun_dec, double hour_angle, double lat, double alt_m,
+                             const Drivers& d, int model) {
+    return density_coarse_r<double>(mjd, sun_dec, hour_angle, lat, alt_m, d, model);
 }
 
 // The density of atm_model 4 (exact, with the optional sweep fits) or 5-7.

@@ -36,6 +36,7 @@ struct ForceParams {
     int32_t drag, sun, moon;
     int32_t ground_check;  // terminal ground event (final-state path)
     int32_t atm_model;     // JB2008 profile: 4 exact; 5, 6, 7 the coarse quadrature profiles
+    int32_t drag_fp32;     // split precision: the coarse profile's density in FP32
     double earth_radius;
     double omega;
     double mu_sun, mu_moon;
@@ -173,7 +174,9 @@ struct Encke {
         jb::Drivers dr = fp->drivers;
         // rhs.rs:3560-3571: no drivers at this instant -> NaN density
         if (fp->dtab.n_solar > 0 && !jb::lookup_drivers(fp->dtab, jd, &dr)) return NAN;
-        double rho = jb::density_model(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->atm_model, fp->fit);
+        double rho = (fp->drag_fp32 && fp->atm_model != 4)
+                         ? jb::density_coarse_r<float>(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->atm_model)
+                         : jb::density_model(jd - 2400000.5, dec, ha, lat, alt_m, dr, fp->atm_model, fp->fit);
         if (!(rho > 0.0) || !isfinite(rho)) return NAN;
         if (alt_m > 2500.0e3) rho = fmin(rho, 1.0e-19);
         return rho;

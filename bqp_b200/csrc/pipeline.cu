@@ -292,6 +292,8 @@ __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs&
             // same verdict on every lane of the group
             if (fp.dtab.n_solar > 0 && !jb::lookup_drivers(fp.dtab, P.jd[slot], &dr))
                 rho = NAN;
+            else if (kCoarse && fp.drag_fp32)
+                rho = jb::density_coarse_r<float>(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, dr, fp.atm_model);
             else if (kCoarse)
                 rho = jb::density_coarse(P.jd[slot] - 2400000.5, dec, ha, lat, alt_m, dr, fp.atm_model);
             else

@@ -99,7 +99,8 @@ typedef struct bqp_force_config {
     int32_t split_degree;      /* split precision: 0 plain FP64; d >= 4: spherical-harmonic
                                   degrees above d in FP32, the rest in FP64 (stage-synchronous
                                   engine and gravity evaluation) */
-    int32_t drag_fp32;         /* split precision: 1 evaluates the JB2008 density in FP32 */
+    int32_t drag_fp32;         /* split precision: 1 evaluates the JB2008 density in FP32 (the coarse
+                                  profiles, atm_model 5-7; stage-synchronous engine and force calls) */
     int32_t surrogate;         /* 1: gravity = exact degrees <= BQP_SURROGATE_DEGREE + the trained
                                   surrogate (stage-synchronous engine; bqp_surrogate_train first) */
 } bqp_force_config;
@@ -166,8 +167,10 @@ int bqp_jb_fit_check(const double* drivers, double* worst6);
  * negative code (-1 non-finite input, -2 altitude below 90 km, -3 angle out
  * of range, -4 non-positive index, -5 numerical domain).  model 4: the exact
  * quadrature (jb_rs/src/jb2008.rs:880); 5, 6, 7: the coarse profiles
- * (jb2008.rs:890-920, 7 = jb2008_density_fitted_v7). */
-int bqp_jb_density(int32_t model, int64_t n, const double* in14, double* out);
+ * (jb2008.rs:890-920, 7 = jb2008_density_fitted_v7).  fp32 != 0: a coarse
+ * profile in FP32 arithmetic, as the split form's drag evaluates it (no
+ * counterpart in the reference). */
+int bqp_jb_density(int32_t model, int32_t fp32, int64_t n, const double* in14, double* out);
 
 /* JB2008 space-weather tables: the SET SOLFSMY (daily F10, S10, M10, Y10 and
  * their 81-day centred means) and DTCFILE (hourly dTc, K) texts.  Replaces

@@ -168,6 +168,35 @@ def test_encke_rhs_coarse_atmosphere_matches_oracle(model):
     assert moved > n // 2  # the profile is not the exact model
 
 
+def test_encke_rhs_fp32_density_tracks_oracle():
+    """Split form's FP32 density (drag_fp32, atm_model 7) in the force call
+    against the oracle's FP64 force: the difference is the density's FP32
+    error (<= 1e-5 relative below 1000 km) times the drag term, on top of
+    the FP64 force bound."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    cfg_ctx = ctx_for(text, order, flags=flags, atm_model=7)
+    cfg = cfg_ctx.cfg
+    cfg.drag_fp32 = 1
+    ctx = N.Context(text, cfg)
+    nodrag = ctx_for(text, order, flags=4 | 8, atm_model=7)
+    F = oracle_force(text, order, flags, atm_model=7)
+    n = 128
+    states = workloads.leo_states(n, seed=61)
+    equ, _ = N.eci_to_equinoctial(states)
+    rng = np.random.default_rng(61)
+    t = rng.uniform(0.0, 5400.0, n)
+    zero = np.zeros((n, 6))
+    bal = workloads.leo_ballistics(n, seed=61)
+    got = ctx.rhs(equ, 0.0, EPOCH, t, zero, bal)
+    a_drag = np.linalg.norm(got[:, 3:] - nodrag.rhs(equ, 0.0, EPOCH, t, zero, bal)[:, 3:], axis=1)
+    for i in range(n):
+        ref = F.rhs(equ[i], 0.0, EPOCH, bal[i, 0], bal[i, 1], t[i], zero[i])
+        scale = MU / np.linalg.norm(O.equinoc2eci(equ[i], t[i])[0][:3]) ** 2
+        assert np.abs(got[i, 3:] - ref[3:]).max() <= 1e-5 * a_drag[i] + 1e-12 * scale, i
+
+
 @pytest.mark.parametrize("engine", ENGINES)
 def test_adaptive_final_default_atmosphere_matches_oracle(engine):
     """The reference's default atmosphere (atm_model 7) in adaptive

@@ -208,3 +208,26 @@ def test_library_density_equals_oracle_bit_for_bit(model):
     assert np.array_equal(got, want)
     with pytest.raises(N.NativeError):
         N.jb_density(3, np.array(rows[:1]))
+
+
+@pytest.mark.parametrize("model", [5, 6, 7])
+def test_fp32_density_tracks_fp64(model):
+    # the split form's FP32 density against the FP64 one on the broad grid:
+    # FP32 rounding (~6e-8 per operation) enters exponents of up to ~45, so
+    # the density moves by ~1e-6: within 1e-5 relative up to 1000 km, where
+    # drag matters, and 5e-5 above (the hydrogen term's exponent is a
+    # difference of large numbers; above 2500 km the density is capped)
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_oracle_golden import BROAD_ALT, broad_grid_input
+
+    rows = np.array([broad_grid_input(mjd, alt, lat, lst) for mjd in (51999.75, 57000.25, 60648.5)
+                     for alt in BROAD_ALT for lat in (-75.0, 0.0, 45.0) for lst in (0.0, 12.0, 18.0)])
+    f64 = N.jb_density(model, rows)
+    f32 = N.jb_density(model, rows, fp32=True)
+    assert (f32 > 0).all()
+    rel = np.abs(f32 - f64) / f64
+    low = rows[:, 4] <= 1000e3
+    assert rel[low].max() <= 1e-5 and rel.max() <= 5e-5, (rel[low].max(), rel.max())
+    with pytest.raises(N.NativeError):
+        N.jb_density(4, rows[:1], fp32=True)
