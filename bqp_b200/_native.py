@@ -77,6 +77,7 @@ SIGNATURES = [
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
     ("bqp_jb_fit_check", C.c_int, [_dp, _dp]),
     ("bqp_jb_density", C.c_int, [C.c_int32, C.c_int32, C.c_int64, _dp, _dp]),
+    ("bqp_utc_jd", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_ctx_set_jb_drivers", C.c_int, [_vp, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_double,
                                          C.c_double]),
     ("bqp_ctx_jb_lookup", C.c_int, [_vp, _dp, C.c_int64, _dp, _ip]),
@@ -494,6 +495,16 @@ def jb_density(model: int, inputs, fp32: bool = False) -> np.ndarray:
     x = f64(inputs).reshape(-1, 14)
     out = np.empty(x.shape[0])
     check(lib().bqp_jb_density(int(model), int(bool(fp32)), x.shape[0], dptr(x), dptr(out)))
+    return out
+
+
+def utc_jd(jd0, t) -> np.ndarray:
+    """UTC Julian days of instants t (elapsed seconds) after UTC epochs jd0,
+    as the kernels form them (bqp_utc_jd)."""
+    t = f64(np.atleast_1d(t))
+    j = f64(np.broadcast_to(jd0, t.shape))
+    out = np.empty(t.size)
+    check(lib().bqp_utc_jd(t.size, dptr(j), dptr(t), dptr(out)))
     return out
 
 

@@ -1502,6 +1502,12 @@ int bqp_propagate_sampled(bqp_ctx* ctx, int64_t n, const double* in, int32_t inp
     return e == cudaSuccess ? 0 : cuda_fail(e, "bqp_propagate_sampled");
 }
 
+int bqp_utc_jd(int64_t n, const double* jd0, const double* t, double* out) {
+    if (n < 0 || (n > 0 && (!jd0 || !t || !out))) return fail(BQP_E_ARG, "bad buffers");
+    for (int64_t i = 0; i < n; ++i) out[i] = utc_jd_at(jd0[i], t[i]);
+    return 0;
+}
+
 int bqp_eci_to_equinoctial(int64_t n, const double* eci, double* equ, int32_t* ok) {
     if (n < 0 || (n > 0 && (!eci || !equ))) return fail(BQP_E_ARG, "bad buffers");
     for (int64_t i = 0; i < n; ++i) {

@@ -100,7 +100,7 @@ struct Encke {
         const double r2 = fma(sp[0], sp[0], fma(sp[1], sp[1], sp[2] * sp[2]));
         const double r = sqrt(r2);
         double acc[3] = {0.0, 0.0, 0.0};
-        const double jd = jd0 + t / kSecPerDay;
+        const double jd = utc_jd_at(jd0, t);
         double s = 0.0, c = 1.0;
         if (fp->gravity_on || fp->drag) sincos(gmst_rad(jd), &s, &c);
         double pi[3];

@@ -37,6 +37,70 @@ constexpr double kMaxSegmentS = 5400.0;             // integrator.rs:236
 constexpr double kRebaseKm = 10.0;                  // types.rs:138
 constexpr double kGroundAltitudeKm = 100.0;         // types.rs:140
 
+// ---------------------------------------------------------------- UTC / TAI
+// UTC days that start with a new TAI - UTC (IERS Bulletin C): the MJD of
+// each day from 1972-01-01 (TAI - UTC = 10 s) on, each later one adding one
+// second (the last, 2017-01-01, makes it 37 s).  The day before each later
+// entry ends with a leap second and lasts 86,401 s.
+#define BQP_LEAP_MJD_LIST                                                                                 \
+    {41317, 41499, 41683, 42048, 42413, 42778, 43144, 43509, 43874, 44239, 44786, 45151, 45516, 46247, \
+     47161, 47892, 48257, 48804, 49169, 49534, 50083, 50630, 51179, 53736, 54832, 56109, 57204, 57754}
+constexpr int kLeapCount = 28;
+#ifdef __CUDACC__
+__constant__ const int32_t kLeapMjdDev[kLeapCount] = BQP_LEAP_MJD_LIST;
+#endif
+static const int32_t kLeapMjdHost[kLeapCount] = BQP_LEAP_MJD_LIST;
+#ifdef __CUDA_ARCH__
+#define BQP_LEAP_MJD kLeapMjdDev
+#else
+#define BQP_LEAP_MJD kLeapMjdHost
+#endif
+
+// Length in SI seconds of UTC day `mjd_day` (an integral MJD).
+BQP_HD double utc_day_seconds(double mjd_day) {
+    for (int k = 1; k < kLeapCount; ++k)
+        if ((double)BQP_LEAP_MJD[k] == mjd_day + 1.0) return 86401.0;
+    return 86400.0;
+}
+
+// UTC Julian day of the instant t seconds after the epoch jd0 (a UTC Julian
+// day): the propagator integrates in continuous (TAI) seconds, and the
+// JB2008 drivers, the ephemeris catalogues and the Earth's rotation are
+// looked up on UTC (lightyear_odeint_rs/src/rhs.rs:3090-3110, 3264-3300).  UTC
+// Julian days of a day that ends in a leap second run over 86,401 s (the
+// ERFA convention the reference follows), so the leap second 23:59:60 is day
+// fraction 86400/86401.  Where no such day is within a day of the arc this
+// is jd0 + t/86400 to the bit; before 1972 it is that always.
+BQP_HD double utc_jd_at(double jd0, double t) {
+    const double plain = jd0 + t / kSecPerDay;
+    const double mjd0 = jd0 - 2400000.5;
+    if (!(isfinite(mjd0) && isfinite(t)) || mjd0 < (double)BQP_LEAP_MJD[0]) return plain;
+    const double d0 = floor(mjd0), d1 = floor(mjd0 + t / kSecPerDay);
+    const double lo = fmin(d0, d1) - 1.0, hi = fmax(d0, d1) + 1.0;
+    bool near_leap = false;
+    for (int k = 1; k < kLeapCount; ++k) {
+        const double last = (double)BQP_LEAP_MJD[k] - 1.0;  // the day that ends in the leap second
+        if (last >= lo && last <= hi) near_leap = true;
+    }
+    if (!near_leap) return plain;
+    // walk whole UTC days from the epoch's, in SI seconds (arcs span days;
+    // the bound only guarantees an end)
+    double d = d0;
+    double sec = (mjd0 - d0) * utc_day_seconds(d0) + t;
+    for (int it = 0; it < 100000; ++it) {
+        if (sec < 0.0) {
+            d -= 1.0;
+            sec += utc_day_seconds(d);
+        } else if (sec >= utc_day_seconds(d)) {
+            sec -= utc_day_seconds(d);
+            d += 1.0;
+        } else {
+            break;
+        }
+    }
+    return (2400000.5 + d) + sec / utc_day_seconds(d);
+}
+
 BQP_HD double mod2pi(double a) {
     if (!isfinite(a)) return NAN;
     double x = fmod(a, kTwoPi);

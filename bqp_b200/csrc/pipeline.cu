@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
         P.sp[(size_t)i * P.cap + slot] = sp[i];
     }
     for (int i = 0; i < 3; ++i) K(P, st, i)[slot] = yt[3 + i];
-    const double jd = s.jd0 + ts / kSecPerDay;
+    const double jd = utc_jd_at(s.jd0, ts);
     const ForceParams& fp = A.force;
     double sn = 0.0, cs = 1.0;
     if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);

@@ -381,6 +381,14 @@ int bqp_surrogate_set_params(bqp_ctx* ctx, const float* params, double sigma);
 int bqp_surrogate_grad(bqp_ctx* ctx, int32_t batch, const float* params, const float* x, const float* t,
                        float* grad, double* loss, float* y);
 
+/* UTC Julian day of each force evaluation as the kernels form it, on the
+ * host: out[i] = the instant t[i] elapsed (SI/TAI) seconds after the UTC
+ * epoch jd0[i], with UTC days that end in a leap second running over 86,401 s
+ * (the reference's TAI integration time and its taiutc lookup seam,
+ * lightyear_odeint_rs/src/rhs.rs:3090-3110, 3264-3300).  Without a
+ * leap-second day within a day of the arc it is jd0 + t/86400. */
+int bqp_utc_jd(int64_t n, const double* jd0, const double* t, double* out);
+
 /* Element conversions on the host (no GPU).  eci_to_equinoctial replaces
  * eci2equinoc_impl (satpy_core/src/lib.rs:1738-1870; ok[i] = 0 on an
  * unbound or degenerate orbit); equinoctial_to_eci replaces equinoc2eci_impl

@@ -44,6 +44,8 @@ def lib():
         L.orc_force_set_atm_model.argtypes = [C.c_void_p, C.c_int]
         L.orc_field_dense.argtypes = [C.c_void_p, _dp, _dp]
         L.orc_gravity_itrs.argtypes = [C.c_void_p, C.c_long, _dp, _dp]
+        L.orc_utc_jd_at.restype = C.c_double
+        L.orc_utc_jd_at.argtypes = [C.c_double, C.c_double]
         L.orc_gmst.restype = C.c_double
         L.orc_gmst.argtypes = [C.c_double]
         L.orc_eci2equinoc.argtypes = [_dp, _dp]
@@ -254,6 +256,11 @@ def equinoc2eci(eq, tof):
     out = np.zeros(6)
     rc = lib().orc_equinoc2eci(_d(f64(eq)), tof, _d(out))
     return out, rc
+
+
+def utc_jd_at(jd0, t):
+    """UTC Julian day t elapsed (TAI) seconds after the UTC epoch jd0."""
+    return lib().orc_utc_jd_at(float(jd0), float(t))
 
 
 def gmst(jd):

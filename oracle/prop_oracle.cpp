@@ -530,6 +530,49 @@ void battin(const double rb[3], const double dr[3], double rp2, double rp, doubl
     for (int i = 0; i < 3; ++i) acc[i] += k * std::fma(fq, rb[i], -dr[i]);
 }
 
+// --------------------------------------------------------------- UTC / TAI
+// The reference integrates in continuous (TAI) seconds from the epoch's TAI
+// instant and looks its drivers and ephemeris up on UTC through ERFA's
+// taiutc, whose UTC Julian day of a day that ends in a leap second runs over
+// 86,401 s (rhs.rs:3090-3110, 3264-3300; satpy_core/src/frame_time/
+// timescale.rs:440-600).  Restated as UTC -> TAI -> + t -> UTC through the
+// IERS Bulletin C table (TAI - UTC from 1972: 10 s, then one second at each
+// listed day).  Arcs with no leap-second day within a day of either end keep
+// jd0 + t/86400, and so do epochs before 1972.
+namespace tsc {
+const int LEAP_MJD[28] = {41317, 41499, 41683, 42048, 42413, 42778, 43144, 43509, 43874, 44239,
+                          44786, 45151, 45516, 46247, 47161, 47892, 48257, 48804, 49169, 49534,
+                          50083, 50630, 51179, 53736, 54832, 56109, 57204, 57754};
+// TAI - UTC (s) during UTC day `day` (integral MJD >= 41317)
+double dat(double day) {
+    int n = 0;
+    for (int k = 0; k < 28; ++k)
+        if (LEAP_MJD[k] <= day) ++n;
+    return 9.0 + n;
+}
+double day_seconds(double day) { return 86400.0 + (dat(day + 1.0) - dat(day)); }
+// TAI seconds, counted on the MJD axis (86400 per TAI day), of UTC (day, s)
+double tai_seconds(double day, double s) { return day * 86400.0 + dat(day) + s; }
+double utc_jd_at(double jd0, double t) {
+    const double mjd0 = jd0 - 2400000.5;
+    if (!(std::isfinite(mjd0) && std::isfinite(t)) || mjd0 < LEAP_MJD[0]) return jd0 + t / SEC_PER_DAY;
+    const double d0 = std::floor(mjd0), d1 = std::floor(mjd0 + t / SEC_PER_DAY);
+    bool near = false;
+    for (int k = 1; k < 28; ++k) {
+        const double last = LEAP_MJD[k] - 1.0;
+        if (last >= std::min(d0, d1) - 1.0 && last <= std::max(d0, d1) + 1.0) near = true;
+    }
+    if (!near) return jd0 + t / SEC_PER_DAY;
+    // utctai: the epoch's TAI seconds; then back through the table (taiutc)
+    const double tai = tai_seconds(d0, (mjd0 - d0) * day_seconds(d0)) + t;
+    double day = std::floor(tai / 86400.0);
+    while (tai_seconds(day, 0.0) > tai) day -= 1.0;
+    while (tai_seconds(day + 1.0, 0.0) <= tai) day += 1.0;
+    const double s = tai - tai_seconds(day, 0.0);
+    return (2400000.5 + day) + s / day_seconds(day);
+}
+}  // namespace tsc
+
 // ------------------------------------------------------------------- JB2008
 // jb_rs/src/jb2008.rs (Orekit 13.1.2 JB2008 adaptation), exact quadrature
 // profile: lower step ln-ratio 0.010, middle 0.025, upper 0.075.
@@ -1648,7 +1691,7 @@ struct Rhs {
         double r2 = std::fma(sp[0], sp[0], std::fma(sp[1], sp[1], sp[2] * sp[2]));
         double r = std::sqrt(r2);
         double acc[3] = {0, 0, 0};
-        double jd = jd0 + t / SEC_PER_DAY;
+        double jd = tsc::utc_jd_at(jd0, t);
         double th = gmst_rad(jd);
         double s = std::sin(th), c = std::cos(th);
         if (F->use_gravity && F->field.order > 0) {
@@ -2457,6 +2500,7 @@ int orc_gravity_itrs(void* f, long n, const double* pos, double* acc) {
 }
 
 double orc_gmst(double jd) { return gmst_rad(jd); }
+double orc_utc_jd_at(double jd0, double t) { return tsc::utc_jd_at(jd0, t); }
 
 int orc_eci2equinoc(const double* eci, double* equ) { return eci2equinoc(eci, equ) ? 0 : 1; }
 int orc_equinoc2eci(const double* equ, double tof, double* eci) {

@@ -221,6 +221,35 @@ def test_adaptive_final_default_atmosphere_matches_oracle(engine):
     assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
 
 
+@pytest.mark.parametrize("engine", ENGINES)
+def test_arc_across_the_2016_leap_second_matches_oracle(engine):
+    """An arc from 2016-12-31T20:00 UTC over the leap second: the drivers,
+    the Sun/Moon and the Earth's rotation are taken at UTC formed from the
+    integration's continuous seconds (the oracle restates the seam
+    independently)."""
+    order = 20
+    text = workloads.synthetic_field(order)
+    flags = 1 | 4 | 8
+    eps = 1e-10
+    epoch = 2457753.5 + 20.0 / 24.0
+    ctx = ctx_for(text, order, flags=flags, method="dop853", eps=eps, engine=engine, atm_model=7)
+    F = oracle_force(text, order, flags, atm_model=7)
+    n = 16
+    states = workloads.leo_states(n, seed=71)
+    bal = workloads.leo_ballistics(n, seed=71)
+    equ, _ = N.eci_to_equinoctial(states)
+    tf = 8 * 3600.0
+    got, st, steps, evals = ctx.propagate_final(states, epoch, tf, ballistic=bal)
+    ref_d, ref_st, ref_steps, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, epoch, tf, bal)
+    assert (st == 0).all() and (ref_st == 0).all()
+    for i in range(n):
+        ref = O.equinoc2eci(equ[i], tf)[0] + ref_d[i]
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+    assert np.all(np.abs(steps - ref_steps) <= np.maximum(3, 0.05 * ref_steps))
+    # the seam moves the end instant by one UTC second
+    assert abs((N.utc_jd(epoch, tf)[0] - (epoch + tf / 86400.0)) * 86400.0 + 1.0) < 1e-4
+
+
 def test_jb2008_sweep_fit_matches_quadrature():
     """The Chebyshev fits of the fixed-node JB2008 sweeps reproduce the Boole
     quadrature: fit error at the check points, and the drag term of the force
