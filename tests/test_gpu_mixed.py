@@ -35,7 +35,9 @@ def test_mixed_orbits_uneven_durations_match_oracle(engine):
     assert (rst == 0).all()
     for i in range(len(states)):
         ref = O.equinoc2eci(equ[i], dur[i])[0] + d[i]
-        assert np.linalg.norm(got[i, :3] - ref[:3]) <= max(steps[i], 1) * eps * 10, i
+        # each solution within ~10 eps per step of the exact one, so two
+        # solutions within twice that (as test_adaptive_final_matches_oracle)
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
     # accept/reject sequences are chaotic in the last bits: a few steps apart
     # on short, eccentric rows, a few percent on long ones
     assert np.all(np.abs(steps - rsteps) <= np.maximum(5, 0.1 * rsteps))
