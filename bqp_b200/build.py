@@ -46,6 +46,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objs = []
     flags = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH,
              "-I", str(CSRC), "-I", str(PKG.parent / "include")]
+    # extra nvcc definitions for measured build variants (e.g. -DBQP_DRAG_MIN_BLOCKS=4)
+    flags += os.environ.get("BQP_NVCC_DEFINES", "").split()
     if verbose:
         flags += ["-Xptxas", "-v"]
     for src in SOURCES:

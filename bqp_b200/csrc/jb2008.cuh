@@ -964,7 +964,13 @@ BQP_HD double node_ain(double z, const double* tc, bool with_mbar, double* tloc,
 }
 
 template <int L>
-__device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr, int n, double ain0,
+// How the drag kernel's sweep helpers are compiled: inlined at each of their
+// call sites (the default) or as one out-of-line copy each, which shrinks
+// the kernel's code when instruction fetch limits it.
+#ifndef BQP_JB_SWEEP_INLINE
+#define BQP_JB_SWEEP_INLINE __forceinline__
+#endif
+__device__ BQP_JB_SWEEP_INLINE SweepG boole_sweep_group(double zend_start, double zr, int n, double ain0,
                                                     bool with_mbar, const double* tc, int q, unsigned gmask) {
     SweepG s;
     double part = 0.0;
@@ -1034,7 +1040,7 @@ __device__ __forceinline__ SweepG boole_sweep_group(double zend_start, double zr
 // i = q (mod L); shuffles combine them, and every lane runs the short
 // series in the altitude variable and recomputes the final node.
 template <int L>
-__device__ __forceinline__ SweepG fitted_sweep(const double* c, const int32_t* ex, double xa, double xt,
+__device__ BQP_JB_SWEEP_INLINE SweepG fitted_sweep(const double* c, const int32_t* ex, double xa, double xt,
                                                double zend_start, double zr, int n, double ain0, const double* tc,
                                                int q, unsigned gmask) {
     static_assert(kFit2A % L == 0, "series rows must split evenly over the lanes");
