@@ -25,8 +25,16 @@ by the device per trajectory.
   cpu_baseline  the C++ oracle (restatement of the reference CPU path) on a
          bounded sample, all host cores
 
+  forms  (N = 1 only) the propagation forms the metric compares with plain
+         FP64: split precision at eps 1e-11 (degrees above 8, 16, 32 in FP32),
+         plain FP64 at eps 1e-10 and Vern9 at eps 1e-10 -- each form's force
+         evaluations/s and trajectory-days/s on the full batch, and its 7-day
+         final-position error against plain FP64 at eps 1e-12 on 512 rows
+         (``--no-forms`` skips it)
+
 ``--impl reference`` times that CPU implementation alone (rank 0) on the same
-workload and prints its line.
+workload and prints its line.  ``--atm-model 7`` measures the reference's
+default (fitted) JB2008 profile instead of the exact model.
 """
 from __future__ import annotations
 
