@@ -74,6 +74,8 @@ def main():
     ap.add_argument("--sample", type=int, default=16384)
     ap.add_argument("--trial-s", type=float, default=1800.0)
     ap.add_argument("--run", action="store_true", help="then propagate the whole batch with the choice")
+    ap.add_argument("--eps", type=float, default=1e-12, help="absolute tolerance, km (DOP853)")
+    ap.add_argument("--atm-model", type=int, default=4, choices=[4, 5, 6, 7], help="JB2008 profile")
     args = ap.parse_args()
     from .accuracy import config
     text = W.synthetic_field(args.order)
@@ -84,9 +86,11 @@ def main():
         states = W.leo_states(args.n, seed=0)
         dur = np.full(args.n, 5400.0)
         bal = W.leo_ballistics(args.n, seed=0)
-    cfg = config(args.order, 1e-12)
+    cfg = config(args.order, args.eps)
+    cfg.atm_model = args.atm_model
     best, results = tune(text, cfg, states, W.EPOCH_JD, dur, bal, args.sample, args.trial_s)
-    out = {"workload": args.workload, "n": args.n, "trials": results,
+    out = {"workload": args.workload, "n": args.n, "eps_km": args.eps, "atm_model": args.atm_model,
+           "trials": results,
            "choice": {"engine": [k for k, v in N.ENGINES.items() if v == best.engine][0],
                       "gravity_threads": best.gravity_threads, "gravity_slots": best.gravity_slots}}
     if args.run:
@@ -95,7 +99,8 @@ def main():
         _, st, _, ev = ctx.propagate_final(states, W.EPOCH_JD, dur, ballistic=bal)
         dt = time.perf_counter() - t0
         out["run"] = {"wall_s": dt, "evals": int(ev.sum()), "evals_per_s": float(ev.sum() / dt),
-                      "trajectory_days_per_s": float(dur.sum() / 86400.0 / dt), "ok": int((st == 0).sum())}
+                      "trajectory_days_per_s": float(dur.sum() / 86400.0 / dt), "ok": int((st == 0).sum()),
+                      "status_counts": {int(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}}
     print(json.dumps(out), flush=True)
 
 
