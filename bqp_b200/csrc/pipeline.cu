@@ -105,106 +105,77 @@ __global__ void __launch_bounds__(kBlock) pl_init(PropArgs A, PipeBufs P) {
 // Stage `st` of the current attempt.  st == S is the dense-output stage of
 // the sampled non-FSAL path: f(t_next, y_next) evaluated before the
 // controller decides (the reference evaluates it after an accept).
-//
-// A CTA takes kPrepRows slots with twice as many threads: warps 0-3 form the
-// stage state and its Kepler baseline, warps 4-7 meanwhile the evaluation's
-// UTC instant, the Earth rotation and the Sun / Moon positions (functions of
-// the stage time alone); the two halves meet in shared memory for the third
-// body, Battin's term and the drag work lists.  One row's serial chain is
-// split in two and the kernel has twice the warps to hide its latency.
-constexpr int kPrepRows = kBlock / 2;
-
 template <int M>
 __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cur, int st) {
     using T = Tab<M>;
-    __shared__ double sh_sun[3][kPrepRows], sh_moon[3][kPrepRows];
-    const bool frame_half = threadIdx.x >= kPrepRows;
-    const int r = threadIdx.x - (frame_half ? kPrepRows : 0);
-    const int slot = blockIdx.x * kPrepRows + r;
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (st == 0 && blockIdx.x == 0 && threadIdx.x == 0) P.count[cur ^ 1] = 0;
-    const bool active = slot < P.count[cur];
-    const int32_t traj = active ? P.idx[cur][slot] : 0;
+    if (slot >= P.count[cur]) return;
+    const int32_t traj = P.idx[cur][slot];
     const TrajState& s = P.st[traj];
-    // the stage's first force call is the carried k1: nothing to evaluate
-    const bool carried = active && st == 0 && (s.flags & kHaveK1);
-    const bool work = active && !carried;
+    if (st == 0) {
+        P.bad[slot] = 0;
+        if (s.flags & kHaveK1) {
+            for (int i = 0; i < 6; ++i) K(P, 0, i)[slot] = s.k1c[i];
+            P.skip[slot] = 1;
+            return;
+        }
+    } else if (!(st == 1 && P.skip[slot])) {
+        finish_stage(P, st - 1, slot);
+    }
+    P.skip[slot] = 0;
+    // stage state
+    double yt[6];
+    for (int i = 0; i < 6; ++i) yt[i] = s.y[i];
+    double ts;
+    if (st < T::S) {
+#pragma unroll 1
+        for (int j = 0; j < st; ++j) {
+            const double a = s.hs * T::a(st, j);
+            if (a != 0.0)
+                for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], a, yt[i]);
+        }
+        ts = s.t + T::c(st) * s.hs;
+    } else {
+        // y_next exactly as rk_combine forms it
+#pragma unroll 1
+        for (int j = 0; j < T::S; ++j) {
+            const double b = s.hs * T::b(j);
+            if (b != 0.0)
+                for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], b, yt[i]);
+        }
+        ts = next_time(s);
+    }
+    double rs[6];
+    baseline_state(baseline_new(s.cur), ts - s.ct0, rs);
+    double sp[6];
+    for (int i = 0; i < 6; ++i) {
+        sp[i] = rs[i] + yt[i];
+        P.sp[(size_t)i * P.cap + slot] = sp[i];
+    }
+    for (int i = 0; i < 3; ++i) K(P, st, i)[slot] = yt[3 + i];
+    const double jd = utc_jd_at(s.jd0, ts);
     const ForceParams& fp = A.force;
-    const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0);
-    double ts = 0.0;
-    if (work) ts = st < T::S ? s.t + T::c(st) * s.hs : next_time(s);
-
-    double yt[6], rs[6], sp[6];
-    if (!frame_half && active) {
-        if (st == 0) {
-            P.bad[slot] = 0;
-            if (carried) {
-                for (int i = 0; i < 6; ++i) K(P, 0, i)[slot] = s.k1c[i];
-                P.skip[slot] = 1;
-            }
-        } else if (!(st == 1 && P.skip[slot])) {
-            finish_stage(P, st - 1, slot);
-        }
-        if (!carried) P.skip[slot] = 0;
-    }
-    if (!frame_half && work) {
-        // stage state
-        for (int i = 0; i < 6; ++i) yt[i] = s.y[i];
-        if (st < T::S) {
-#pragma unroll 1
-            for (int j = 0; j < st; ++j) {
-                const double a = s.hs * T::a(st, j);
-                if (a != 0.0)
-                    for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], a, yt[i]);
-            }
-        } else {
-            // y_next exactly as rk_combine forms it
-#pragma unroll 1
-            for (int j = 0; j < T::S; ++j) {
-                const double b = s.hs * T::b(j);
-                if (b != 0.0)
-                    for (int i = 0; i < 6; ++i) yt[i] = fma(K(P, j, i)[slot], b, yt[i]);
-            }
-        }
-        baseline_state(baseline_new(s.cur), ts - s.ct0, rs);
-        for (int i = 0; i < 6; ++i) {
-            sp[i] = rs[i] + yt[i];
-            P.sp[(size_t)i * P.cap + slot] = sp[i];
-        }
-        for (int i = 0; i < 3; ++i) K(P, st, i)[slot] = yt[3 + i];
-    }
-    if (frame_half && work) {
-        const double jd = utc_jd_at(s.jd0, ts);
-        double sn = 0.0, cs = 1.0;
-        if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);
-        P.sc[slot] = sn;
-        P.sc[P.cap + slot] = cs;
-        double sun[3] = {0.0, 0.0, 0.0}, moon[3] = {0.0, 0.0, 0.0};
-        if (need_sun) sun_at(fp.eph_sun, jd, sun);
-        if (fp.moon) moon_at(fp.eph_moon, jd, moon);
-        for (int i = 0; i < 3; ++i) {
-            sh_sun[i][r] = sun[i];
-            sh_moon[i][r] = moon[i];
-        }
-        if (fp.drag) {
-            P.jd[slot] = jd;
-            for (int i = 0; i < 3; ++i) P.sun[(size_t)i * P.cap + slot] = sun[i];
-        }
-    }
-    __syncthreads();
-    if (frame_half || !work) return;
+    double sn = 0.0, cs = 1.0;
+    if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);
+    P.sc[slot] = sn;
+    P.sc[P.cap + slot] = cs;
     double acc[3] = {0.0, 0.0, 0.0};
-    if (fp.sun) {
-        const double sun[3] = {sh_sun[0][r], sh_sun[1][r], sh_sun[2][r]};
-        third_body(sp, sun, fp.mu_sun, acc);
-    }
+    double sun[3];
+    const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0);
+    if (need_sun) sun_at(fp.eph_sun, jd, sun);
+    if (fp.sun) third_body(sp, sun, fp.mu_sun, acc);
     if (fp.moon) {
-        const double moon[3] = {sh_moon[0][r], sh_moon[1][r], sh_moon[2][r]};
+        double moon[3];
+        moon_at(fp.eph_moon, jd, moon);
         third_body(sp, moon, fp.mu_moon, acc);
     }
     const double r2 = fma(sp[0], sp[0], fma(sp[1], sp[1], sp[2] * sp[2]));
     battin(rs, yt, r2, sqrt(r2), acc);
     for (int i = 0; i < 3; ++i) P.part[(size_t)i * P.cap + slot] = acc[i];
     if (fp.drag) {
+        for (int i = 0; i < 3; ++i) P.sun[(size_t)i * P.cap + slot] = sun[i];
+        P.jd[slot] = jd;
         P.amcd[slot] = s.am;
         P.amcd[P.cap + slot] = s.cd;
         // drag work list: states above ~510 km take the sweep fits (cheap),
@@ -359,7 +330,7 @@ __global__ void __launch_bounds__(kBlock, BQP_DRAG_MIN_BLOCKS) pl_drag(ForcePara
 
 // The coarse profiles (atm_model 5-7): a short chain per state, one lane
 // each, both altitude lists in one launch.
-__global__ void __launch_bounds__(kBlock, BQP_DRAG_MIN_BLOCKS) pl_drag_coarse(ForceParams fp, PipeBufs P, int nb_hi) {
+__global__ void __launch_bounds__(kBlock) pl_drag_coarse(ForceParams fp, PipeBufs P, int nb_hi) {
     if ((int)blockIdx.x < nb_hi) drag_rows<1, true>(fp, P, 0, blockIdx.x);
     else drag_rows<1, true>(fp, P, 1, blockIdx.x - nb_hi);
 }
@@ -473,7 +444,6 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
-    const int pblocks = (int)((A.n + kPrepRows - 1) / kPrepRows);
     constexpr int kLanesHigh = BQP_DRAG_LANES_HIGH, kLanesLow = BQP_DRAG_LANES_LOW;
     const int dblocks_hi = (int)((A.n * kLanesHigh + kBlock - 1) / kBlock);
     const int dblocks_lo = (int)((A.n * kLanesLow + kBlock - 1) / kBlock);
@@ -547,7 +517,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     auto enqueue_attempt = [&](int cur, int timed_out) {
         for (int s = 0; s < stages; ++s) {
             if (A.force.drag) cudaMemsetAsync(P.dcount, 0, 2 * sizeof(int32_t), st);
-            timed(kKcPrep, [&] { pl_prep<M><<<pblocks, kBlock, 0, st>>>(A, P, cur, s); });
+            timed(kKcPrep, [&] { pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s); });
             if (A.force.gravity_on)
                 timed(kKcGravity, [&] {
                     gker<<<gblocks, gthreads, smem, st>>>(GT, gparts, P, cur);
