@@ -29,7 +29,7 @@ def test_mixed_orbits_uneven_durations_match_oracle(engine):
     ctx = N.Context(text, cfg)
     got, st, steps, evals = ctx.propagate_final(states, EPOCH, dur, ballistic=bal)
     assert (st == 0).all()
-    F = O.Force(text, order, drag=True, sun=True, moon=True)
+    F = O.Force(text, order, drag=True, sun=True, moon=True, atm_model=cfg.atm_model)
     equ, _ = N.eci_to_equinoctial(states)
     d, rst, rsteps, _ = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, EPOCH, dur, bal)
     assert (rst == 0).all()

@@ -27,7 +27,9 @@ def fixed_step_ctx(text, order, flags):
 
 
 def oracle_sigma_propagate(text, order, flags, mean, cov, tf, bal, sigma_set, alpha, beta, kappa):
-    F = O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8))
+    # the atmosphere of N.default_config(), the reference's default (model 7)
+    F = O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8),
+                atm_model=N.default_config().atm_model)
     ctl = O.ctrl("dop853", eps=1e3, dt_max=60.0)
     wm, wc, _ = U.weights(sigma_set, alpha, beta, kappa)
     means, covs = [], []
@@ -57,9 +59,7 @@ def test_sigma_propagate_matches_oracle(sigma_set, alpha, mean_tol, cov_tol):
     bal = workloads.leo_ballistics(n, seed=4)
     # half a period: inside one rectification segment and below the 10 km
     # deviation threshold, so both sides take the same steps and rebase
-    # decisions and the comparison isolates the transform (over a full
-    # period a threshold crossing within rounding can move one sigma row's
-    # segmentation, i.e. its truncation error, by ~1e-6 km)
+    # decisions and the comparison isolates the transform
     tf = 0.5 * workloads.orbit_period_s(mean)
     ctx = fixed_step_ctx(text, order, flags)
     m, c, st, ev = ctx.sigma_propagate(mean, cov, EPOCH, tf, sigma_set=sigma_set, alpha=alpha, beta=2.0,
