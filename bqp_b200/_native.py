@@ -52,7 +52,7 @@ class ForceConfig(C.Structure):
         ("jb_drivers", C.c_double * 9), ("max_steps", C.c_int64), ("max_attempts", C.c_int64),
         ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
         ("gravity_slots", C.c_int32), ("drag_quadrature", C.c_int32), ("split_degree", C.c_int32),
-        ("drag_fp32", C.c_int32), ("surrogate", C.c_int32),
+        ("drag_fp32", C.c_int32), ("surrogate", C.c_int32), ("surrogate_check", C.c_double),
     ]
 
 

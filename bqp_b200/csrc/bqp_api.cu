@@ -569,6 +569,8 @@ int validate_cfg(const bqp_force_config* c) {
         return fail(BQP_E_UNSUPPORTED, "the surrogate gravity runs in the stage-synchronous engine");
     if (c->surrogate && c->split_degree)
         return fail(BQP_E_ARG, "choose the surrogate or split precision, not both");
+    if (!(std::isfinite(c->surrogate_check) && c->surrogate_check >= 0.0))
+        return fail(BQP_E_ARG, "surrogate_check must be finite and >= 0");
     if (c->drag_fp32 && c->engine == BQP_ENGINE_PERSISTENT)
         return fail(BQP_E_UNSUPPORTED, "the FP32 density runs in the stage-synchronous engine");
     return 0;
@@ -1010,6 +1012,7 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->split_degree = 0;
     c->drag_fp32 = 0;
     c->surrogate = 0;
+    c->surrogate_check = 0.0;
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -1915,6 +1918,8 @@ int surrogate_stage_args(bqp_ctx* ctx, SurrogateRef& S) {
     S.sigma = M.sigma;
     S.err = M.derr;
     S.low = low_table(ctx);
+    S.full = grav_table(ctx);
+    S.check = ctx->cfg.surrogate_check;
     return 0;
 }
 

@@ -17,6 +17,8 @@ struct SurrogateRef {
     double R, r_mid, r_half, sigma;    // output and input scaling
     int* err;                          // set when a tensor-core wait timed out
     GravTable low;                     // exact table of the degrees the network leaves out
+    GravTable full;                    // the whole exact field (the per-step check's fallback)
+    double check;                      // residual check threshold (0: none)
 };
 
 // Arguments of k_propagate (all device pointers).
@@ -73,6 +75,11 @@ struct PipeBufs {
     int32_t* dlist[2];    // drag work lists of the stage: 0 above ~510 km (sweep fits), 1 below
     int32_t* dcount;      // [2]
     double* ef;           // [cap][3] Earth-fixed positions of the stage (surrogate gravity)
+    // surrogate residual check (surrogate with a check only)
+    double* agx;          // [3][cap] the exact field of the step's first stage
+    int32_t* fall;        // [cap] by trajectory: 1 while the row's step takes the exact field
+    int32_t* flist;       // [cap] slots of this step's rows on the exact field
+    int32_t* fcount;      // [1]
 };
 
 // Kernel durations by class, summed from CUDA events recorded around each

@@ -204,14 +204,18 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
 // ------------------------------------------------------------------ gravity
 // Persistent over slots: one CTA per SM stages the field table once; the
 // CTA's contiguous slot range is walked NT slots per thread.
+// `out` receives the field; with `list` set the rows are the slots
+// list[0 .. *list_count) instead of the active slots 0 .. count.
 template <int NT>
-__global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max, PipeBufs P, int cur) {
-    const int count = P.count[cur];
+__global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max, PipeBufs P, int cur, double* out,
+                                                     const int32_t* list, const int32_t* list_count) {
+    const int count = list ? *list_count : P.count[cur];
     const int per_block = (count + gridDim.x - 1) / gridDim.x;
     const int b0 = blockIdx.x * per_block;
     const int b1 = min(count, b0 + per_block);
     if (b0 >= b1) return;  // uniform across the CTA
-    auto load = [&](int sl, double& x, double& y, double& z) -> bool {
+    auto load = [&](int row, double& x, double& y, double& z) -> bool {
+        const int sl = list ? list[row] : row;
         if (P.skip[sl]) return false;
         const double s = P.sc[sl], c = P.sc[P.cap + sl];
         const double ex = P.sp[sl], ey = P.sp[P.cap + sl], ez = P.sp[2 * P.cap + sl];
@@ -219,7 +223,7 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
         const double r2 = fma(qx, qx, fma(qy, qy, ez * ez));
         if (!(isfinite(r2) && r2 > 0.0)) {
             P.bad[sl] = 1;
-            P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
+            out[sl] = out[P.cap + sl] = out[2 * P.cap + sl] = NAN;
             return false;
         }
         x = qx;
@@ -227,14 +231,16 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
         z = ez;
         return true;
     };
-    auto store = [&](int sl, const double* a, double, double, double) {
-        P.agrav[sl] = a[0];
-        P.agrav[P.cap + sl] = a[1];
-        P.agrav[2 * P.cap + sl] = a[2];
+    auto store = [&](int row, const double* a, double, double, double) {
+        const int sl = list ? list[row] : row;
+        out[sl] = a[0];
+        out[P.cap + sl] = a[1];
+        out[2 * P.cap + sl] = a[2];
     };
-    auto lost = [&](int sl) {
+    auto lost = [&](int row) {
+        const int sl = list ? list[row] : row;
         P.bad[sl] = 2;
-        P.agrav[sl] = P.agrav[P.cap + sl] = P.agrav[2 * P.cap + sl] = NAN;
+        out[sl] = out[P.cap + sl] = out[2 * P.cap + sl] = NAN;
     };
     gravity_cta<NT>(T, parts_max, per_block, b0, b1, load, store, lost);
 }
@@ -249,6 +255,33 @@ __global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
     P.ef[3 * (size_t)sl] = fma(c, ex, s * ey);
     P.ef[3 * (size_t)sl + 1] = fma(-s, ex, c * ey);
     P.ef[3 * (size_t)sl + 2] = ez;
+}
+
+// ------------------------------------------------------- surrogate check
+// Per step, at its first stage: the network's field (agrav) against the
+// exact one (agx).  A row off by more than `thr` of the exact field's
+// magnitude takes the exact field now and, through the slot list, at the
+// step's later stages.  A row whose first stage was carried over (a retried
+// step, or the FSAL stage of the step before) keeps the verdict under which
+// that stage was evaluated.
+__global__ void __launch_bounds__(kBlock) pl_sur_check(PipeBufs P, int cur, double thr) {
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= P.count[cur]) return;
+    const int32_t traj = P.idx[cur][sl];
+    if (!P.skip[sl]) {
+        double d2 = 0.0, a2 = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const size_t o = (size_t)k * P.cap + sl;
+            const double d = P.agrav[o] - P.agx[o];
+            d2 = fma(d, d, d2);
+            a2 = fma(P.agx[o], P.agx[o], a2);
+        }
+        const bool fall = !(d2 <= thr * thr * a2);  // NaN falls back too
+        P.fall[traj] = fall ? 1 : 0;
+        if (fall)
+            for (int k = 0; k < 3; ++k) P.agrav[(size_t)k * P.cap + sl] = P.agx[(size_t)k * P.cap + sl];
+    }
+    if (P.fall[traj]) P.flist[atomicAdd(P.fcount, 1)] = sl;
 }
 
 // --------------------------------------------------------------------- drag
@@ -434,7 +467,11 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
     P.dlist[0] = (int32_t*)take(c * 4);
     P.dlist[1] = (int32_t*)take(c * 4);
     P.ef = (double*)take(3 * c * 8);
-    P.dcount = (int32_t*)take(2 * 4);
+    P.agx = (double*)take(3 * c * 8);
+    P.fall = (int32_t*)take(c * 4);
+    P.flist = (int32_t*)take(c * 4);
+    P.fcount = (int32_t*)take(4);
+    P.dcount = (int32_t*)take(2 * 4);  // last: pipeline_bytes measures up to it
 }
 
 template <int M>
@@ -462,7 +499,19 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
         gparts = 1;
         smem = gravity_smem_bytes(GT, gthreads, nt, gparts);
     }
-    cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the surrogate's residual check also runs the whole exact field
+    const bool check = sur && A.sur.check > 0.0;
+    int gparts_full = kGravityPartsMax;
+    size_t smem_full = 0;
+    if (check) {
+        smem_full = gravity_smem_bytes(A.sur.full, gthreads, nt, gparts_full);
+        if (smem_full > kSmemPerBlock) {
+            gparts_full = 1;
+            smem_full = gravity_smem_bytes(A.sur.full, gthreads, nt, gparts_full);
+        }
+    }
+    cudaError_t e = cudaFuncSetAttribute(gker, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(smem > smem_full ? smem : smem_full));
     if (e != cudaSuccess) return e;
     if (A.force.fit) {
         // the fixed-node fits: the same table for every context, ordered on
@@ -492,6 +541,7 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
     cudaMallocHost(&h_count, sizeof(int32_t));
 
     cudaMemsetAsync(P.count, 0, 2 * sizeof(int32_t), st);
+    if (check) cudaMemsetAsync(P.fall, 0, (size_t)A.n * sizeof(int32_t), st);
     pl_init<M><<<blocks, kBlock, 0, st>>>(A, P);
 
     // instrumentation: an event-record node on each side of every timed
@@ -520,10 +570,21 @@ static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, 
             timed(kKcPrep, [&] { pl_prep<M><<<blocks, kBlock, 0, st>>>(A, P, cur, s); });
             if (A.force.gravity_on)
                 timed(kKcGravity, [&] {
-                    gker<<<gblocks, gthreads, smem, st>>>(GT, gparts, P, cur);
+                    gker<<<gblocks, gthreads, smem, st>>>(GT, gparts, P, cur, P.agrav, nullptr, nullptr);
                     if (sur) {
                         pl_earth_fixed<<<blocks, kBlock, 0, st>>>(P, cur);
                         launch_surrogate_stage(A.sur, &P.count[cur], A.n, P.ef, P.agrav, 1, P.cap, st);
+                        if (check && s == 0) {
+                            // the exact field of every evaluated row, then the verdicts
+                            cudaMemsetAsync(P.fcount, 0, sizeof(int32_t), st);
+                            gker<<<gblocks, gthreads, smem_full, st>>>(A.sur.full, gparts_full, P, cur, P.agx,
+                                                                      nullptr, nullptr);
+                            pl_sur_check<<<blocks, kBlock, 0, st>>>(P, cur, A.sur.check);
+                        } else if (check) {
+                            // the rows on the exact field for this step
+                            gker<<<gblocks, gthreads, smem_full, st>>>(A.sur.full, gparts_full, P, cur, P.agrav,
+                                                                      P.flist, P.fcount);
+                        }
                     }
                 });
             if (A.force.drag)

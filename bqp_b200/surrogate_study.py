@@ -42,25 +42,29 @@ def _timed(torch, fn, reps=5):
     return e0.elapsed_time(e1) / reps
 
 
-def propagation(text, order, sur_ctx, n, seconds, eps_ref=1e-12, eps_form=1e-9, limit_s=120.0):
+def propagation(text, order, sur_ctx, n, seconds, eps_ref=1e-12, eps_form=1e-9, limit_s=120.0, check=1e-3):
     """n LEO rows (the bench distributions) over `seconds` with DOP853,
     gravity + Sun/Moon.  Reference: the exact FP64 field at eps_ref.  Forms at
-    eps_form: the exact field, the degree-8 field alone and the surrogate (its
+    eps_form: the exact field, the degree-8 field alone, the surrogate (its
     BF16-level field error drives the step controller at a 1e-12 km
-    tolerance, so it runs at its own).  Wall-clock rates and final-position
+    tolerance, so it runs at its own) and the surrogate with the per-step
+    residual check at `check`.  Wall-clock rates and final-position
     differences from the reference (m); every run is limited to limit_s."""
     states = W.leo_states(n, seed=5)
-    out = {"rows": n, "seconds": seconds, "eps_ref": eps_ref, "eps_form": eps_form}
+    out = {"rows": n, "seconds": seconds, "eps_ref": eps_ref, "eps_form": eps_form, "check": check}
     res = {}
-    for name, order_, sur, eps in (("exact_ref", order, False, eps_ref), ("exact", order, False, eps_form),
-                                   ("degree8", N.SURROGATE_DEGREE, False, eps_form),
-                                   ("surrogate", order, True, eps_form)):
+    for name, order_, sur, eps, chk in (("exact_ref", order, False, eps_ref, 0.0),
+                                        ("exact", order, False, eps_form, 0.0),
+                                        ("degree8", N.SURROGATE_DEGREE, False, eps_form, 0.0),
+                                        ("surrogate", order, True, eps_form, 0.0),
+                                        ("surrogate_checked", order, True, eps_form, check)):
         c = sur_ctx if sur else _ctx(text, order_)
         cfg = N.default_config()
         cfg.order = order_
         cfg.force_flags = N.FORCE_SUN | N.FORCE_MOON
         cfg.eps = eps
         cfg.surrogate = int(sur)
+        cfg.surrogate_check = chk
         cfg.max_kernel_seconds = limit_s
         c.set_config(cfg)
         c.propagate_final(states[:1024], W.EPOCH_JD, 60.0)  # warm-up
@@ -70,7 +74,7 @@ def propagation(text, order, sur_ctx, n, seconds, eps_ref=1e-12, eps_form=1e-9, 
         res[name] = r
         out[name] = {"wall_s": wall, "evals": int(ev.sum()), "evals_per_s": float(ev.sum() / wall),
                      "trajectory_days_per_s": n * seconds / 86400.0 / wall, "ok": int((st == 0).sum())}
-    for name in ("exact", "degree8", "surrogate"):
+    for name in ("exact", "degree8", "surrogate", "surrogate_checked"):
         d = np.linalg.norm(res[name][:, :3] - res["exact_ref"][:, :3], axis=1) * 1e3
         out[name]["err_m_rms"] = float(np.sqrt(np.mean(d ** 2)))
         out[name]["err_m_max"] = float(d.max())
@@ -78,7 +82,7 @@ def propagation(text, order, sur_ctx, n, seconds, eps_ref=1e-12, eps_form=1e-9, 
 
 
 def study(order=120, samples=1 << 24, epochs=4, batch=16384, lr=2e-3, n_eval=200000, n_rate=1 << 20, seed=1,
-          n_prop=0, prop_s=5400.0, eps_form=1e-9):
+          n_prop=0, prop_s=5400.0, eps_form=1e-9, check=1e-3):
     import torch
     text = W.synthetic_field(order)
     ctx = _ctx(text, order)
@@ -112,7 +116,7 @@ def study(order=120, samples=1 << 24, epochs=4, batch=16384, lr=2e-3, n_eval=200
     ms_exact = _timed(torch, lambda: ctx.gravity_device(n_rate, d_pos.data_ptr(), d_acc.data_ptr()))
     ms_surr = _timed(torch, lambda: ctx.surrogate_infer_device(n_rate, d_pos.data_ptr(), d_acc.data_ptr(), True))
     gemm_flops = 3 * 2 * 256 * 256 * n_rate
-    prop = propagation(text, order, ctx, n_prop, prop_s, eps_form=eps_form) if n_prop else None
+    prop = propagation(text, order, ctx, n_prop, prop_s, eps_form=eps_form, check=check) if n_prop else None
     return {
         "propagation": prop,
         "order": order, "samples": samples, "epochs": epochs, "batch": batch, "train_s": train_s,
@@ -164,12 +168,13 @@ def main():
     ap.add_argument("--propagate", type=int, default=0, help="rows of the propagation comparison (0: none)")
     ap.add_argument("--prop-seconds", type=float, default=5400.0)
     ap.add_argument("--eps-form", type=float, default=1e-9)
+    ap.add_argument("--check", type=float, default=1e-3, help="surrogate_check of the checked propagation form")
     args = ap.parse_args()
     if args.infer_probe:
         print(json.dumps(infer_probe(args.infer_probe)), flush=True)
         return
     print(json.dumps(study(args.order, args.samples, args.epochs, args.batch, args.lr, n_prop=args.propagate,
-                           prop_s=args.prop_seconds, eps_form=args.eps_form)), flush=True)
+                           prop_s=args.prop_seconds, eps_form=args.eps_form, check=args.check)), flush=True)
 
 
 if __name__ == "__main__":

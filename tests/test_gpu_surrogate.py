@@ -120,24 +120,56 @@ def test_propagation_with_surrogate_gravity():
     n = 512
     states = workloads.leo_states(n, seed=9)
 
-    def run(c, order_, surrogate):
+    def run(c, order_, surrogate, check=0.0):
         cfg = N.default_config()
         cfg.order = order_
         cfg.force_flags = N.FORCE_SUN | N.FORCE_MOON
         cfg.eps = 1e-9
         cfg.surrogate = int(surrogate)
+        cfg.surrogate_check = check
         c.set_config(cfg)
         out, st, _, ev = c.propagate_final(states, workloads.EPOCH_JD, 5400.0)
         assert (st == 0).all()
         return out, ev
 
-    exact, _ = run(_surrogate_ctx(order), order, False)
+    exact, ev_exact = run(_surrogate_ctx(order), order, False)
     low, _ = run(_surrogate_ctx(order), N.SURROGATE_DEGREE, False)
     sur, ev = run(ctx, order, True)
     d_sur = np.linalg.norm(sur[:, :3] - exact[:, :3], axis=1)
     d_low = np.linalg.norm(low[:, :3] - exact[:, :3], axis=1)
     assert (ev > 0).all()
     assert np.sqrt(np.mean(d_sur ** 2)) < 0.5 * np.sqrt(np.mean(d_low ** 2)), (d_sur.mean(), d_low.mean())
+
+    # the per-step residual check with the exact field as fallback: a
+    # threshold no row meets puts every step on the exact field (the exact
+    # run's trajectory), one every row meets leaves the surrogate run as it was
+    # (the exact kernel's column split follows the launch's rows per CTA, so
+    # the fallback rows' sums may differ from the exact run's in the last bits)
+    every, ev_every = run(ctx, order, True, check=1e-30)
+    assert np.abs(every[:, :3] - exact[:, :3]).max() <= 1e-5, np.abs(every - exact).max()
+    assert abs(ev_every.mean() / ev_exact.mean() - 1.0) < 0.01
+    none, ev_none = run(ctx, order, True, check=1e30)
+    assert np.abs(none - sur).max() <= 1e-9, np.abs(none - sur).max()
+    assert (ev_none == ev).all()
+    # between them: the median of the network's relative error at the orbits'
+    # starting positions sends some rows' steps to the exact field
+    full = ctx.gravity(states[:, :3])[0]
+    rel = np.linalg.norm(ctx.surrogate_infer(states[:, :3], add_low=True) - full, axis=1) / np.linalg.norm(full, axis=1)
+    mixed, _ = run(ctx, order, True, check=float(np.median(rel)))
+    d_mixed = np.linalg.norm(mixed[:, :3] - exact[:, :3], axis=1)
+    moved = np.linalg.norm(mixed[:, :3] - sur[:, :3], axis=1) > 0
+    assert moved.any() and (d_mixed > 1e-9).any()
+    assert np.sqrt(np.mean(d_mixed ** 2)) < np.sqrt(np.mean(d_sur ** 2)), (d_mixed.mean(), d_sur.mean())
+    print(f"\nsurrogate RMS miss {np.sqrt(np.mean(d_sur ** 2)):.3e} km; with the check at the median relative "
+          f"error {np.median(rel):.2e}: {np.sqrt(np.mean(d_mixed ** 2)):.3e} km, {moved.sum()} of {n} rows moved")
+    # the check is refused when negative or not finite
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.surrogate = 1
+    for bad in (-1.0, float("nan"), float("inf")):
+        cfg.surrogate_check = bad
+        with pytest.raises(N.NativeError):
+            ctx.set_config(cfg)
     # the surrogate form refuses to run untrained
     cfg = N.default_config()
     cfg.order = order

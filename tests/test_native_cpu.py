@@ -32,8 +32,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_config_struct_matches_header_layout():
     # the ctypes mirror must have the C struct's size (4*6 + 8*10 + 8*9 + 8*3 + 4*7,
-    # padded to the 8-byte alignment of its doubles)
-    assert C.sizeof(N.ForceConfig) == 24 + 80 + 72 + 24 + 32
+    # padded to the 8-byte alignment of its doubles, + 8 for surrogate_check)
+    assert C.sizeof(N.ForceConfig) == 24 + 80 + 72 + 24 + 32 + 8
     cfg = N.default_config()
     assert cfg.order == 5 and cfg.eps == 1e-8 and cfg.dt_max == 300.0 and cfg.max_steps == 500000
     assert list(cfg.jb_drivers)[:8] == [150.0] * 8
