@@ -259,22 +259,27 @@ __global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
 
 // ------------------------------------------------------- surrogate check
 // Per step, at its first stage: the network's field (agrav) against the
-// exact one (agx).  A row off by more than `thr` of the exact field's
-// magnitude takes the exact field now and, through the slot list, at the
-// step's later stages.  A row whose first stage was carried over (a retried
-// step, or the FSAL stage of the step before) keeps the verdict under which
-// that stage was evaluated.
+// exact one (agx), both without the central term.  A row off by more than
+// `thr` of the whole exact field's magnitude (central term included) takes
+// the exact field now and, through the slot list, at the step's later
+// stages.  A row whose first stage was carried over (a retried step, or the
+// FSAL stage of the step before) keeps the verdict under which that stage
+// was evaluated.
 __global__ void __launch_bounds__(kBlock) pl_sur_check(PipeBufs P, int cur, double thr) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= P.count[cur]) return;
     const int32_t traj = P.idx[cur][sl];
     if (!P.skip[sl]) {
+        const double* q = P.ef + 3 * (size_t)sl;  // Earth-fixed position
+        const double r2 = fma(q[0], q[0], fma(q[1], q[1], q[2] * q[2]));
+        const double kc = -kMu / (r2 * sqrt(r2));
         double d2 = 0.0, a2 = 0.0;
         for (int k = 0; k < 3; ++k) {
             const size_t o = (size_t)k * P.cap + sl;
             const double d = P.agrav[o] - P.agx[o];
+            const double a = fma(kc, q[k], P.agx[o]);
             d2 = fma(d, d, d2);
-            a2 = fma(P.agx[o], P.agx[o], a2);
+            a2 = fma(a, a, a2);
         }
         const bool fall = !(d2 <= thr * thr * a2);  // NaN falls back too
         P.fall[traj] = fall ? 1 : 0;

@@ -105,8 +105,8 @@ typedef struct bqp_force_config {
                                   surrogate (stage-synchronous engine; bqp_surrogate_train first) */
     double surrogate_check;    /* surrogate only: at each step's first stage the whole exact field
                                   is evaluated too; a row whose surrogate field misses it by more
-                                  than this fraction of its magnitude (e.g. 1e-3) takes the exact
-                                  field for the whole step.  0: no check (no counterpart in the
+                                  than this fraction of the whole field's magnitude (central term
+                                  included; e.g. 1e-3) takes the exact field for the whole step.  0: no check (no counterpart in the
                                   reference) */
 } bqp_force_config;
 

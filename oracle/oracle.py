@@ -90,6 +90,22 @@ def lib():
                                                  _STATE_FN, _BOUND_FN, _dp, _lp]
         L.orc_drivers_counts.restype = C.c_int
         L.orc_drivers_counts.argtypes = [C.c_void_p, _lp]
+        L.orc_force_set_srp.restype = None
+        L.orc_force_set_srp.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+        L.orc_sun_rate_bound.restype = C.c_double
+        L.orc_sun_rate_bound.argtypes = [C.c_void_p]
+        L.orc_propagate_srp_roots.restype = C.c_int
+        L.orc_propagate_srp_roots.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              _dp, _dp, C.c_int, _ip, _lp]
+        L.orc_ecl_decisive_margin.restype = C.c_int
+        L.orc_ecl_decisive_margin.argtypes = [C.c_double, _dp]
+        L.orc_ecl_replay_unc.restype = C.c_int
+        L.orc_ecl_replay_unc.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp]
+        L.orc_ecl_deepest.restype = C.c_int
+        L.orc_ecl_deepest.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, _dp]
+        L.orc_propagate_srp_batch.restype = None
+        L.orc_propagate_srp_batch.argtypes = [C.c_void_p, _dp, C.c_long, _dp, _dp, _dp, _dp, _dp, C.c_int,
+                                              _dp, _dp, _ip, _lp, _lp, _ip, C.c_int]
         _lib = L
     return _lib
 
@@ -116,6 +132,15 @@ class Force:
             raise ValueError("oracle: coefficient text rejected")
         if lib().orc_force_set_atm_model(self.h, int(atm_model)) != 0:
             raise ValueError(f"oracle: atm_model {atm_model} is not 4, 5, 6 or 7")
+
+    def set_srp(self, on=True, cr=1.3, p_sun=4.56e-6):
+        """Solar radiation pressure with the binary-eclipse coordinator (rows
+        whose A/m, cr and p_sun are all > 0)."""
+        lib().orc_force_set_srp(self.h, int(bool(on)), float(cr), float(p_sun))
+
+    def sun_rate_bound(self) -> float:
+        """Upper bound of the Sun direction's angular rate, rad/day."""
+        return float(lib().orc_sun_rate_bound(self.h))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -236,6 +261,65 @@ def propagate_sampled_batch(force: Force, ctl, eq0, epoch_jd, tf, ballistic, t_e
                                       steps.ctypes.data_as(_lp), evals.ctypes.data_as(_lp),
                                       nw.ctypes.data_as(_ip), int(threads))
     return out, status, steps, evals, nw
+
+
+# eclipse coordinator status words (EclipseError)
+ECLIPSE_STATUS = {11: "envelope", 12: "chatter", 13: "bracket", 14: "non_progress", 15: "geometry",
+                  16: "split_limit"}
+
+
+def propagate_srp_batch(force: Force, ctl, eq0, epoch_jd, tf, ballistic, t_eval=None, threads=0):
+    """Rows through the binary-eclipse coordinator (force.set_srp first):
+    (final delta [n][6] against each row's initial baseline, samples
+    [n][n_t][6] or None, status[n], steps[n], evals[n], samples written[n])."""
+    eq0 = f64(eq0).reshape(-1, 6)
+    n = eq0.shape[0]
+    epoch_jd = f64(np.broadcast_to(epoch_jd, (n,)))
+    tf = f64(np.broadcast_to(tf, (n,)))
+    ballistic = f64(np.broadcast_to(ballistic, (n, 2)))
+    te = f64(t_eval) if t_eval is not None else np.zeros(0)
+    out = np.zeros((n, 6))
+    smp = np.empty((n, te.size, 6)) if t_eval is not None else None
+    status = np.zeros(n, dtype=np.int32)
+    steps = np.zeros(n, dtype=np.int64)
+    evals = np.zeros(n, dtype=np.int64)
+    nw = np.zeros(n, dtype=np.int32)
+    lib().orc_propagate_srp_batch(force.h, _d(f64(ctl)), n, _d(eq0), _d(epoch_jd), _d(tf), _d(ballistic),
+                                  _d(te) if te.size else None, int(te.size), _d(out),
+                                  _d(smp) if smp is not None else None, status.ctypes.data_as(_ip),
+                                  steps.ctypes.data_as(_lp), evals.ctypes.data_as(_lp), nw.ctypes.data_as(_ip),
+                                  int(threads))
+    return out, smp, status, steps, evals, nw
+
+
+def propagate_srp_roots(force: Force, ctl, eq0, epoch_jd, tf, am, cd, max_roots=4096):
+    """One row through the coordinator: (final delta, committed root instants,
+    status, steps, evals)."""
+    d = np.zeros(6)
+    roots = np.zeros(max_roots)
+    nr = C.c_int(0)
+    se = np.zeros(2, dtype=np.int64)
+    st = lib().orc_propagate_srp_roots(force.h, _d(f64(ctl)), _d(f64(eq0)), float(epoch_jd), float(tf), float(am),
+                                       float(cd), _d(d), _d(roots), max_roots, C.byref(nr), se.ctypes.data_as(_lp))
+    return d, roots[:min(nr.value, max_roots)].copy(), st, int(se[0]), int(se[1])
+
+
+def ecl_decisive_margin(err):
+    out = C.c_double(0.0)
+    st = lib().orc_ecl_decisive_margin(float(err), C.byref(out))
+    return (out.value if st == 0 else None), st
+
+
+def ecl_replay_uncertainty(force: Force, epoch_jd, t0, t1):
+    out = C.c_double(0.0)
+    st = lib().orc_ecl_replay_unc(force.h, float(epoch_jd), float(t0), float(t1), C.byref(out))
+    return (out.value if st == 0 else None), st
+
+
+def ecl_deepest(force: Force, epoch_jd, old_t, lim, max_km):
+    out = C.c_double(0.0)
+    st = lib().orc_ecl_deepest(force.h, float(epoch_jd), float(old_t), float(lim), float(max_km), C.byref(out))
+    return (out.value if st == 0 else None), st
 
 
 def integrate_segment(force: Force, ctl, eq, jd0, am, cd, t0, tf):

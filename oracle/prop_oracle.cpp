@@ -1449,8 +1449,8 @@ void position(const EphemTable& T, double jd, double out[3]) {
 }  // namespace eph
 
 // ------------------------------------------ solar radiation pressure, shadow
-// The pieces of the reference's binary-eclipse SRP that are plain functions;
-// the event coordinator that sets the side per leg is not restated here.
+// The plain functions of the reference's binary-eclipse SRP; the coordinator
+// that holds the side per leg is namespace ecl below.
 namespace srp {
 
 constexpr double AU_KM = 149597870.7;
@@ -1621,6 +1621,10 @@ struct Force {
     int atm_model = 4;  // 4 exact JB2008; 5, 6, 7 the coarse quadrature profiles
     std::shared_ptr<DriverTable> table;  // when set: drivers looked up per evaluation
     std::shared_ptr<EphemTable> eph[2];  // Sun, Moon catalogues; unset: the analytic series
+    // solar radiation pressure (rhs.rs:1269-1310, types.rs:347, 459): on when
+    // srp and cr, p_sun and the row's A/m are all > 0 (rhs.rs:31-36)
+    int srp = 0;
+    double cr = 0.0, p_sun = 4.56e-6;
 };
 
 // Sun (body 0) or Moon (1) at a UTC Julian day: the catalogue when set
@@ -1677,6 +1681,7 @@ struct Rhs {
     double t0;    // seconds after epoch at which the baseline elements hold
     double jd0;   // epoch (JD, UTC)
     double am, cd;
+    int side = -1;     // SRP eclipse side of the leg: 1 shadow, 0 lit (-1: SRP off)
     bool bad = false;  // latched invalid-radius gravity error
     long evals = 0;
 
@@ -1724,6 +1729,15 @@ struct Rhs {
                     drag_acc(*F, sp, rho, am, cd, acc);
                 }
             }
+        }
+        if (side >= 0) {
+            // rhs.rs:4033-4063: after drag, before the third bodies, on the
+            // leg's fixed side
+            if (!have_sun) body_position(*F, 0, jd, sun);
+            have_sun = true;
+            double a[3];
+            srp::accel(sp, sun, F->p_sun, F->cr, am, side, a);
+            for (int i = 0; i < 3; ++i) acc[i] += a[i];
         }
         if (F->sun) {
             if (!have_sun) body_position(*F, 0, jd, sun);
@@ -2340,6 +2354,744 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
     return status;
 }
 
+// ================================================== binary-eclipse SRP legs
+// The reference's eclipse coordinator (lightyear_odeint_rs/src/
+// eclipse_coordinator.rs) for the propagation without terminal events
+// (enable_events = false, the path of lib.rs propagate): integration legs
+// with the eclipse side held fixed, a crossing scan of every accepted step's
+// cubic Hermite path, a fine replay of the step that crossed (steps of at
+// most 10 s), an old-side proof leg and a window leg that commits the root,
+// and a rebase at the root with the side flipped.
+namespace ecl {
+
+constexpr double MAX_SEP_KM = 1.0e-6;          // eclipse.rs:39 MAX_BOUNDARY_SEPARATION_KM
+constexpr double SPEED_CAP = 20.0;             // eclipse.rs:50
+constexpr double RADIUS_CAP = 50000.0;         // eclipse.rs:46
+constexpr double MAX_ROOT_UNC_KM = 1.0e-4;     // eclipse_coordinator.rs:93
+constexpr double OLD_SIDE_MARGIN_KM = 2.5e-5;  // eclipse_coordinator.rs:94
+constexpr int MAX_PROOF_RESTARTS = 2;          // eclipse_coordinator.rs:110
+constexpr double POST_ROOT_SAFETY = 16.0;      // eclipse_coordinator.rs:117
+constexpr double MIN_DECISIVE_KM = 1.0e-9;     // eclipse_coordinator.rs:130
+constexpr double REFINE_STEP_S = 10.0;         // eclipse_coordinator.rs:254
+constexpr long MAX_SPLITS = 4096;              // eclipse_coordinator.rs:256
+constexpr double HCARRY_MIN_DTMAX = 60.0;      // integrator.rs HCARRY_UNCLAMPED_DT_MAX_S
+constexpr long MAX_ITER = 500000;              // integrator.rs:185 MAX_STEPS
+// Upper bound of the analytic Sun series' direction rate (rad/day): the
+// ecliptic longitude advances at most 0.98565 + 1.955 x 0.0172 deg/day
+// (mean motion plus the equation of centre's two terms) = 0.01779 rad/day.
+// The catalogue takes its own grid supremum instead (precomputed_ephem.rs:947-1021).
+constexpr double SUN_RATE_ANALYTIC = 0.0185;
+
+// status words of the coordinator's failures (EclipseError, eclipse.rs)
+enum Err { OK = 0, ENVELOPE = 11, CHATTER = 12, BRACKET = 13, NON_PROGRESS = 14, GEOMETRY = 15, SPLIT_LIMIT = 16 };
+
+inline double ulps_up(double v, uint64_t k) {
+    uint64_t b;
+    std::memcpy(&b, &v, 8);
+    b += k;
+    std::memcpy(&v, &b, 8);
+    return v;
+}
+
+// eclipse_coordinator.rs:570-588: one representable value outward
+inline bool outward(double v, double* out) {
+    if (!(std::isfinite(v) && v >= 0.0)) return false;
+    if (v == 0.0) return *out = 0.0, true;
+    const double r = ulps_up(v, 1);
+    if (!std::isfinite(r)) return false;
+    *out = r;
+    return true;
+}
+
+inline double dist3(const double a[3], const double b[3]) {
+    const double dx = b[0] - a[0], dy = b[1] - a[1], dz = b[2] - a[2];
+    return std::sqrt(std::fma(dx, dx, std::fma(dy, dy, dz * dz)));
+}
+
+// Largest angular rate of the catalogue's Sun direction over its linear
+// pieces, rad/day: for p(s) = b + s d the unit vector turns at
+// |b x d| / |p(s)|^2 per step, largest at the point closest to the origin.
+double table_direction_rate(const EphemTable& T) {
+    if (T.n < 2 || !(std::isfinite(T.dt) && T.dt > 0.0)) return 0.0;
+    double sup = 0.0;
+    for (size_t i = 0; i + 1 < T.n; ++i) {
+        const double* b = &T.pos[3 * i];
+        const double* a = &T.pos[3 * (i + 1)];
+        const double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+        const double c[3] = {b[1] * d[2] - b[2] * d[1], b[2] * d[0] - b[0] * d[2], b[0] * d[1] - b[1] * d[0]};
+        const double cn = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        const double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        const double pr = std::fma(b[0], d[0], std::fma(b[1], d[1], b[2] * d[2]));
+        const double s = d2 > 0.0 ? std::min(std::max(-pr / d2, 0.0), 1.0) : 0.0;
+        const double q[3] = {std::fma(s, d[0], b[0]), std::fma(s, d[1], b[1]), std::fma(s, d[2], b[2])};
+        const double q2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        if (!(std::isfinite(q2) && q2 > 0.0)) return NAN;
+        sup = std::max(sup, cn / (T.dt * q2));
+    }
+    return sup;
+}
+
+// Geometry of one row's arc: the Sun on the UTC day of each TAI-like solver
+// second (rhs.rs:4475-4480) and the bounds the coordinator takes on it.
+struct Geo {
+    const Force* F;
+    double jd0;
+    double re;
+    double rate;  // rad/day
+
+    bool sun(double t, double o[3]) const {
+        if (!std::isfinite(t)) return false;
+        const double jd = tsc::utc_jd_at(jd0, t);
+        if (F->eph[0]) {
+            const EphemTable& T = *F->eph[0];
+            if (!(jd >= T.jd_start && jd <= T.jd_start + (double)(T.n - 1) * T.dt)) return false;
+        }
+        body_position(*F, 0, jd, o);
+        const double n2 = o[0] * o[0] + o[1] * o[1] + o[2] * o[2];
+        return std::isfinite(n2) && n2 > 0.0;
+    }
+    // rhs.rs:4788-4866: rate x elapsed days, one value outward
+    int sun_angle(double a, double b, double* out) const {
+        if (!std::isfinite(a) || !std::isfinite(b)) return GEOMETRY;
+        if (F->eph[0]) {
+            const EphemTable& T = *F->eph[0];
+            const double hi = T.jd_start + (double)(T.n - 1) * T.dt;
+            const double ja = tsc::utc_jd_at(jd0, a), jb = tsc::utc_jd_at(jd0, b);
+            if (!(ja >= T.jd_start && ja <= hi && jb >= T.jd_start && jb <= hi)) return GEOMETRY;
+        }
+        if (!(std::isfinite(rate) && rate >= 0.0)) return GEOMETRY;
+        const double bound = rate * (std::fabs(b - a) / 86400.0);
+        if (!std::isfinite(bound)) return GEOMETRY;
+        if (bound == 0.0) return *out = 0.0, OK;
+        const double r = ulps_up(bound, 1);
+        if (!std::isfinite(r)) return GEOMETRY;
+        *out = r;
+        return OK;
+    }
+    // eclipse_coordinator.rs:590-596: geometry motion a replay over [t0, t1]
+    // can hide (speed cap x dt + diameter cap x Sun sweep)
+    int replay_unc(double t0, double t1, double* out) const {
+        double dtb, dia, ang, axis;
+        if (!outward(SPEED_CAP * std::fabs(t1 - t0), &dtb)) return GEOMETRY;
+        if (!outward(2.0 * RADIUS_CAP, &dia)) return GEOMETRY;
+        if (int e = sun_angle(t0, t1, &ang)) return e;
+        if (!outward(dia * ang, &axis)) return GEOMETRY;
+        if (!outward(dtb + axis, out)) return GEOMETRY;
+        return OK;
+    }
+    // eclipse_coordinator.rs:598-631: the instant farthest from old_t toward
+    // lim whose replay uncertainty stays within maxb (binary64 bisection)
+    int deepest(double old_t, double lim, double maxb, double* out) const {
+        if (old_t == lim || !std::isfinite(lim) || !(std::isfinite(maxb) && maxb > 0.0)) return NON_PROGRESS;
+        double u;
+        if (int e = replay_unc(old_t, lim, &u)) return e;
+        if (u <= maxb) return *out = lim, OK;
+        double inside = old_t, outside = lim;
+        for (int i = 0; i < 64; ++i) {
+            const double mid = inside + 0.5 * (outside - inside);
+            if (mid == inside || mid == outside) break;
+            if (int e = replay_unc(old_t, mid, &u)) return e;
+            if (u <= maxb) inside = mid;
+            else outside = mid;
+        }
+        if (inside == old_t || !std::isfinite(inside)) return NON_PROGRESS;
+        *out = inside;
+        return OK;
+    }
+};
+
+// eclipse_coordinator.rs:182-194
+int decisive_margin(double err, double* out) {
+    if (!(std::isfinite(err) && err >= 0.0)) return GEOMETRY;
+    double sc;
+    if (!outward(POST_ROOT_SAFETY * err, &sc)) return GEOMETRY;
+    *out = std::min(std::max(sc, MIN_DECISIVE_KM), MAX_SEP_KM);
+    return OK;
+}
+
+// eclipse_coordinator.rs:313-361: cubic Hermite position and velocity
+int hermite_pv(const double p0[3], const double v0[3], const double p1[3], const double v1[3], double t0,
+               double t1, double t, double pos[3], double vel[3]) {
+    const double h = t1 - t0;
+    if (!std::isfinite(h) || h == 0.0 || !std::isfinite(t)) return NON_PROGRESS;
+    const double tau = std::min(std::max((t - t0) / h, 0.0), 1.0);
+    const double t2 = tau * tau, t3 = t2 * tau;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    const double g00 = (6.0 * t2 - 6.0 * tau) / h, g10 = 3.0 * t2 - 4.0 * tau + 1.0;
+    const double g01 = (-6.0 * t2 + 6.0 * tau) / h, g11 = 3.0 * t2 - 2.0 * tau;
+    for (int i = 0; i < 3; ++i) {
+        pos[i] = h00 * p0[i] + h10 * h * v0[i] + h01 * p1[i] + h11 * h * v1[i];
+        vel[i] = g00 * p0[i] + g10 * v0[i] + g01 * p1[i] + g11 * v1[i];
+    }
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(pos[i]) || !std::isfinite(vel[i])) return GEOMETRY;
+    return OK;
+}
+
+struct Root {
+    bool have = false;
+    double t = 0.0, err = 0.0;
+};
+
+struct Bracket {
+    double t_old = 0.0, t_new = 0.0;
+    int old_side = 0, new_side = 0;
+    double bound = 0.0;
+};
+
+// One accepted step as the handler sees it (deltas and their derivatives).
+struct StepView {
+    double t0, t1;
+    double y0[6], d0[6], y1[6], d1[6];
+};
+
+struct ScanUser {
+    const Geo* G;
+    double p0[3], v0[3], p1[3], v1[3], t0, t1;
+    int err;
+};
+
+int scan_state(void* u, double t, double* pos, double* vel, double* sun) {
+    ScanUser* S = (ScanUser*)u;
+    if (int e = hermite_pv(S->p0, S->v0, S->p1, S->v1, S->t0, S->t1, t, pos, vel)) return S->err = e, 1;
+    if (!S->G->sun(t, sun)) return S->err = GEOMETRY, 1;
+    return 0;
+}
+
+// eclipse_coordinator.rs:499-547: Bezier control-polygon length of the
+// Hermite path plus the swing of the Sun axis, eight values outward
+int scan_bound(void* u, const double* a, const double* b, double* out) {
+    ScanUser* S = (ScanUser*)u;
+    const double t0 = a[0], t1 = b[0];
+    const double *p0 = a + 1, *v0 = a + 4, *p1 = b + 1, *v1 = b + 4;
+    const double h = t1 - t0;
+    const double c1[3] = {p0[0] + h * v0[0] / 3.0, p0[1] + h * v0[1] / 3.0, p0[2] + h * v0[2] / 3.0};
+    const double c2[3] = {p1[0] - h * v1[0] / 3.0, p1[1] - h * v1[1] / 3.0, p1[2] - h * v1[2] / 3.0};
+    const double path = dist3(p0, c1) + dist3(c1, c2) + dist3(c2, p1);
+    const double zero[3] = {0.0, 0.0, 0.0};
+    double m2 = 0.0;
+    for (const double* p : {p0, (const double*)c1, (const double*)c2, p1}) {
+        const double dx = zero[0] - p[0], dy = zero[1] - p[1], dz = zero[2] - p[2];
+        const double r2 = std::fma(dx, dx, std::fma(dy, dy, dz * dz));
+        if (r2 > m2) m2 = r2;  // a NaN radius is discarded, as f64::max does
+    }
+    const double maxr = std::sqrt(m2);
+    double ang;
+    if (int e = S->G->sun_angle(t0, t1, &ang)) return S->err = e, 1;
+    const double bound = path + 2.0 * maxr * ang;
+    if (!std::isfinite(bound)) return S->err = GEOMETRY, 1;
+    if (bound == 0.0) return *out = 0.0, 0;
+    const double r = ulps_up(bound, 8);
+    if (!std::isfinite(r)) return S->err = GEOMETRY, 1;
+    *out = r;
+    return 0;
+}
+
+// eclipse.rs:124-152 on baseline + delta
+bool envelope_at(const Baseline& base, double bt0, const double d[6], double t) {
+    double b[6];
+    baseline_state(base, t - bt0, b);
+    const double p[3] = {b[0] + d[0], b[1] + d[1], b[2] + d[2]};
+    const double v[3] = {b[3] + d[3], b[4] + d[4], b[5] + d[5]};
+    return srp::envelope_ok(p, v);
+}
+
+// Side and margin of baseline + delta at t (rhs.rs:4422-4444).
+int geometry_at(const Geo& G, const Baseline& base, double bt0, const double d[6], double t, int* side,
+                double* margin) {
+    double b[6], sun[3];
+    baseline_state(base, t - bt0, b);
+    const double p[3] = {b[0] + d[0], b[1] + d[1], b[2] + d[2]};
+    if (!G.sun(t, sun)) return GEOMETRY;
+    if (!srp::cylinder(p, sun, G.re, side, margin)) return GEOMETRY;
+    return OK;
+}
+
+// CoordinatedEventHandler::on_step (eclipse_coordinator.rs:720-934) without
+// the normal event handler: checks the step, scans it, and reports the
+// earliest crossing.
+int on_step(const Geo& G, const Baseline& base, double bt0, int fixed, const Root& root, const StepView& S,
+            bool* found, Bracket* br) {
+    *found = false;
+    if (!envelope_at(base, bt0, S.y0, S.t0) || !envelope_at(base, bt0, S.y1, S.t1)) return ENVELOPE;
+    ScanUser U;
+    U.G = &G;
+    U.t0 = S.t0;
+    U.t1 = S.t1;
+    U.err = OK;
+    double b0[6], b1[6];
+    baseline_state(base, S.t0 - bt0, b0);
+    baseline_state(base, S.t1 - bt0, b1);
+    for (int i = 0; i < 3; ++i) {
+        U.p0[i] = b0[i] + S.y0[i];
+        U.v0[i] = b0[3 + i] + S.d0[i];
+        U.p1[i] = b1[i] + S.y1[i];
+        U.v1[i] = b1[3 + i] + S.d1[i];
+    }
+    double pos[3], vel[3], sun[3];
+    if (int e = hermite_pv(U.p0, U.v0, U.p1, U.v1, S.t0, S.t1, S.t0, pos, vel)) return e;
+    if (!G.sun(S.t0, sun)) return GEOMETRY;
+    int side;
+    double margin;
+    if (!srp::cylinder(pos, sun, G.re, &side, &margin)) return GEOMETRY;
+    const bool certified = root.have && root.t == S.t0;
+    if (side != fixed && !certified) return CHATTER;
+    double from = S.t0;
+    if (certified) {
+        double edge;
+        if (int e = G.deepest(S.t0, S.t1, MAX_ROOT_UNC_KM, &edge)) return e;
+        if (int e = hermite_pv(U.p0, U.v0, U.p1, U.v1, S.t0, S.t1, edge, pos, vel)) return e;
+        if (!G.sun(edge, sun)) return GEOMETRY;
+        int es;
+        double em, dm;
+        if (!srp::cylinder(pos, sun, G.re, &es, &em)) return GEOMETRY;
+        if (int e = decisive_margin(root.err, &dm)) return e;
+        if (es != fixed || em <= dm) return CHATTER;
+        from = edge;
+    }
+    srp::ScanResult r;
+    const int sc = srp::first_crossing(from, S.t1, G.re, MAX_SEP_KM, MAX_SPLITS, scan_state, scan_bound, &U, &r);
+    if (sc != srp::SCAN_OK) {
+        if (sc == srp::SCAN_GEOMETRY) return U.err ? U.err : GEOMETRY;
+        return sc == srp::SCAN_BRACKET ? BRACKET : (sc == srp::SCAN_NON_PROGRESS ? NON_PROGRESS : SPLIT_LIMIT);
+    }
+    if (!r.found) return OK;
+    br->t_old = r.t_old;
+    br->t_new = r.t_new;
+    br->old_side = r.old_shadow;
+    br->new_side = r.new_shadow;
+    br->bound = r.bound;
+    if (br->old_side != fixed) return CHATTER;
+    *found = true;
+    return OK;
+}
+
+// Requested output times, converted to deltas against the original baseline
+// (integrator.rs:1163-1178) as each leg reaches them.
+struct Sink {
+    const double* t = nullptr;
+    int n = 0, idx = 0;
+    double* out = nullptr;  // [n][6]
+    const double* eq0 = nullptr;
+    double t0 = 0.0;
+    void put(const double ds[6], double ts, const double seg_eq[6], double seg_t0) {
+        to_original(ds, ts, seg_eq, seg_t0, eq0, t0, out + (size_t)idx * 6);
+        ++idx;
+    }
+};
+
+struct LegIn {
+    double t0, tf;
+    double y0[6];
+    double h_max, h0;
+    const Root* root;
+    bool emit_stop;  // the stopping step's samples belong to this leg
+};
+
+struct LegOut {
+    int status = ST_SUCCESS;  // ST_* or an Err
+    bool stopped = false;     // a crossing stopped the leg at its step's end
+    Bracket br;
+    StepView step;
+    double t_end = 0.0, y_end[6] = {0, 0, 0, 0, 0, 0};
+    double fch = 0.0;  // final controller h (hcarry_store)
+};
+
+// One leg: integrate_sampled_unforced with the coordinated handler
+// (odesolve/solver.rs:1551-1830): absolute max-norm control at eps, the
+// end-of-step derivative handed forward as the next first stage, the
+// handler after each accepted step and before its samples and controller
+// update; a crossing stops the leg at the step's end.
+void leg(Rhs& R, const Ctrl& C, const Geo& G, const LegIn& L, LegOut& O, Stats& st, Sink* sk,
+         const double* seg_eq) {
+    Tab T = tableau(C.method);
+    O = LegOut();
+    double y[6];
+    for (int i = 0; i < 6; ++i) y[i] = L.y0[i];
+    double t = L.t0;
+    const double tf = L.tf;
+    O.t_end = t;
+    for (int i = 0; i < 6; ++i) O.y_end[i] = y[i];
+    const double dir = tf >= t ? 1.0 : -1.0;
+    const double span = std::fabs(tf - t);
+    if (!(span > 0.0)) {
+        O.status = NON_PROGRESS;
+        return;
+    }
+    double h_max = std::fabs(L.h_max);
+    const double h_min = std::min(h_max, 1e-12);
+    if (h_max < h_min) h_max = h_min;
+    double h = (L.h0 > 0.0 ? std::min(std::max(L.h0, h_min), h_max)
+                           : std::min(std::max(default_h0(span), h_min), h_max)) * dir;
+    long rejects = 0, steps = 0;
+    std::vector<double> k((size_t)T.s * 6);
+    double k1c[6];
+    bool have_k1 = false, have_prev = false, just_rej = false;
+    double err_prev = 0.0, t_comp = 0.0;
+    const double order = (double)T.order_err + 1.0, inv_order = 1.0 / order;
+    const bool use_e3 = T.e3 && C.eps >= T.err3_min_eps;
+    if (sk)
+        while (sk->idx < sk->n && sk->t[sk->idx] == t) sk->put(y, t, seg_eq, R.t0);
+    double ynext[6], err[6], err3[6];
+    while (tf != t && ((tf - t) > 0 ? 1.0 : -1.0) == dir) {
+        if (steps >= C.max_steps) {
+            O.status = ST_MAX_STEPS;
+            break;
+        }
+        double hs = h;
+        const double rem = tf - t;
+        if (std::fabs(rem) < std::fabs(hs)) hs = rem;
+        const bool lands = hs == rem;
+        if (std::fabs(hs) < h_min && !lands) {
+            O.status = ST_STEP_UNDERFLOW;
+            break;
+        }
+        if (have_k1)
+            for (int i = 0; i < 6; ++i) k[i] = k1c[i];
+        rk_step(R, T, t, y, hs, k.data(), have_k1, ynext, err, err3, st.evals);
+        double en = NAN;
+        if (finite6(ynext) && finite6(err)) {
+            double m5 = 0.0, m3 = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                m5 = std::max(m5, std::fabs(err[i]));
+                if (use_e3) m3 = std::max(m3, std::fabs(err3[i]));
+            }
+            en = use_e3 ? std::sqrt(std::fma(m5, m5, 0.01 * m3 * m3)) : m5;
+        }
+        if (!std::isfinite(en)) {
+            ++rejects;
+            ++st.rejects;
+            have_k1 = false;
+            if (rejects > C.max_rejects) {
+                O.status = ST_NON_FINITE;
+                break;
+            }
+            h = std::min(std::max(std::fabs(hs) * 0.1, h_min), h_max) * dir;
+            continue;
+        }
+        if (en <= C.eps || std::fabs(hs) <= h_min) {
+            double tn;
+            if (lands) tn = tf;
+            else {
+                const double ky = hs - t_comp;
+                const double nx = t + ky;
+                t_comp = (nx - t) - ky;
+                tn = nx;
+            }
+            if (!std::isfinite(tn)) {
+                O.status = ST_NON_FINITE;
+                break;
+            }
+            ++steps;
+            ++st.steps;
+            rejects = 0;
+            StepView S;
+            S.t0 = t;
+            S.t1 = tn;
+            for (int i = 0; i < 6; ++i) {
+                S.y0[i] = y[i];
+                S.d0[i] = k[i];
+                S.y1[i] = ynext[i];
+            }
+            if (T.fsal) {
+                for (int i = 0; i < 6; ++i) k1c[i] = k[(T.s - 1) * 6 + i];
+            } else {
+                R.eval(tn, ynext, k1c);
+                st.evals++;
+            }
+            have_k1 = true;
+            for (int i = 0; i < 6; ++i) S.d1[i] = k1c[i];
+            bool found = false;
+            Bracket br;
+            if (int e = on_step(G, R.base, R.t0, R.side, *L.root, S, &found, &br)) {
+                O.status = e;
+                O.t_end = tn;
+                for (int i = 0; i < 6; ++i) O.y_end[i] = ynext[i];
+                return;
+            }
+            const bool emit = !found || L.emit_stop;
+            if (sk && emit) {
+                while (sk->idx < sk->n) {
+                    const double ts = sk->t[sk->idx];
+                    if (dir * (ts - tn) > 0.0) break;
+                    double ds[6];
+                    if (ts == tn) {
+                        for (int i = 0; i < 6; ++i) ds[i] = ynext[i];
+                    } else {
+                        const double hd = tn - t;
+                        const double tau = std::min(std::max((ts - t) / hd, 0.0), 1.0);
+                        const double t2 = tau * tau, t3 = t2 * tau;
+                        const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
+                        const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+                        for (int i = 0; i < 6; ++i)
+                            ds[i] = h00 * y[i] + h10 * hd * S.d0[i] + h01 * ynext[i] + h11 * hd * S.d1[i];
+                    }
+                    sk->put(ds, ts, seg_eq, R.t0);
+                }
+            }
+            if (found) {
+                O.stopped = true;
+                O.br = br;
+                O.step = S;
+                O.t_end = tn;
+                for (int i = 0; i < 6; ++i) O.y_end[i] = ynext[i];
+                return;
+            }
+            t = tn;
+            for (int i = 0; i < 6; ++i) y[i] = ynext[i];
+            const double eff = en > 0.0 ? en : C.eps * 0.1;
+            double factor = have_prev && err_prev > 0.0
+                                ? 0.9 * std::pow(C.eps / eff, 0.7 / order) * std::pow(err_prev / C.eps, 0.4 / order)
+                                : 0.9 * std::pow(C.eps / eff, inv_order);
+            const double mgb = std::min(1.0 + 4.0 * (5.0 / order), 5.0);
+            factor = std::min(std::max(factor, 0.2), just_rej ? std::min(mgb, 2.0) : mgb);
+            h = std::min(std::max(std::fabs(hs) * factor, h_min), h_max) * dir;
+            O.fch = std::fabs(h);
+            err_prev = en;
+            have_prev = true;
+            just_rej = false;
+        } else {
+            ++rejects;
+            ++st.rejects;
+            have_k1 = false;
+            if (rejects > C.max_rejects) {
+                O.status = ST_MAX_REJECTS;
+                break;
+            }
+            double factor = 0.9 * std::pow(C.eps / en, inv_order);
+            factor = std::min(std::max(factor, 0.1), 0.5);
+            h = std::min(std::max(std::fabs(hs) * factor, h_min), h_max) * dir;
+            just_rej = true;
+        }
+    }
+    O.t_end = t;
+    for (int i = 0; i < 6; ++i) O.y_end[i] = y[i];
+}
+
+inline void eci_of(const double eq[6], double bt0, const double d[6], double t, double out[6]) {
+    double b[6];
+    equinoc2eci(eq, t - bt0, b);
+    for (int i = 0; i < 6; ++i) out[i] = b[i] + d[i];
+}
+
+// integrate_binary_eclipse_scalar_with_rhs_inner (eclipse_coordinator.rs:
+// 1228-1443) with resolve_eclipse_split (1453-1619), refine_eclipse_bracket
+// (1621-1738), commit_eclipse_root_transaction (2164-2370) and
+// complete_non_eclipse_segment (2372-2583), events off.  Final delta against
+// the original baseline in delta[6]; samples at t_eval[n_t] (forward, sorted)
+// into smp[n_t][6] when given.  Returns ST_SUCCESS, an ST_* of a failed leg,
+// ST_GRAVITY, ST_REBASE_FAILED or an Err.
+int propagate(const Job& J, const double eq0[6], double t0, double tf, const double* t_eval, int n_t,
+              double* smp, double delta[6], Stats& st, int* n_written, std::vector<double>* roots = nullptr) {
+    const Force* F = J.F;
+    Geo G{F, J.jd0, F->earth_radius,
+          F->eph[0] ? table_direction_rate(*F->eph[0]) : SUN_RATE_ANALYTIC};
+    Sink sink;
+    sink.t = t_eval;
+    sink.n = smp ? n_t : 0;
+    sink.out = smp;
+    sink.eq0 = eq0;
+    sink.t0 = t0;
+    Sink* sk = smp ? &sink : nullptr;
+    if (n_written) *n_written = 0;
+    auto done = [&](int s) {
+        if (n_written) *n_written = sink.idx;
+        return s;
+    };
+    for (int i = 0; i < 6; ++i) delta[i] = 0.0;
+    if (tf == t0) {
+        while (sk && sk->idx < sk->n) {
+            for (int i = 0; i < 6; ++i) smp[(size_t)sk->idx * 6 + i] = 0.0;
+            ++sk->idx;
+        }
+        return done(ST_SUCCESS);
+    }
+    if (!(tf > t0)) return done(ST_INVALID_INPUT);
+    while (sk && sk->idx < sk->n && sk->t[sk->idx] < t0) ++sk->idx;
+    const double dtmax = J.C.h_max;
+    double cur[6];
+    for (int i = 0; i < 6; ++i) cur[i] = eq0[i];
+    double ct = t0;
+    Root root;
+    long splits = 0;
+    double hcarry = 0.0;
+    const double zero[6] = {0, 0, 0, 0, 0, 0};
+    Baseline b0 = baseline_new(cur);
+    if (!b0.ok) return done(ST_INVALID_INPUT);
+    if (!envelope_at(b0, ct, zero, ct)) return done(ENVELOPE);
+    int side;
+    double margin;
+    if (int e = geometry_at(G, b0, ct, zero, ct, &side, &margin)) return done(e);
+    auto make_rhs = [&](const double* eq, double bt0, int sd) {
+        Rhs R;
+        R.F = F;
+        R.base = baseline_new(eq);
+        R.t0 = bt0;
+        R.jd0 = J.jd0;
+        R.am = J.am;
+        R.cd = J.cd;
+        R.side = sd;
+        return R;
+    };
+    auto rebase = [&](const double* eq, double bt0, const double* d, double t, double* out) -> bool {
+        double e[6];
+        eci_of(eq, bt0, d, t, e);
+        return eci2equinoc(e, out);
+    };
+    for (long it = 0; it < MAX_ITER; ++it) {
+        if (ct == tf) {
+            to_original(zero, tf, cur, ct, eq0, t0, delta);
+            return done(ST_SUCCESS);
+        }
+        const double seg_tf = bounded_end(ct, tf, MAX_SEGMENT_S);
+        Rhs R = make_rhs(cur, ct, side);
+        LegIn L{ct, seg_tf, {0, 0, 0, 0, 0, 0}, dtmax, dtmax > HCARRY_MIN_DTMAX ? hcarry : 0.0, &root, false};
+        LegOut O;
+        leg(R, J.C, G, L, O, st, sk, cur);
+        if (R.bad) return done(ST_GRAVITY);
+        if (dtmax > HCARRY_MIN_DTMAX && std::isfinite(O.fch) && O.fch > 0.0) hcarry = O.fch;
+        // a handler error, or complete_non_eclipse_segment's failed solver status
+        if (O.status != ST_SUCCESS && !O.stopped) return done(O.status);
+        if (!O.stopped) {
+            if (seg_tf == tf) {
+                to_original(O.y_end, tf, cur, ct, eq0, t0, delta);
+                return done(ST_SUCCESS);
+            }
+            double ne[6];
+            if (!rebase(cur, ct, O.y_end, seg_tf, ne)) return done(ST_REBASE_FAILED);
+            for (int i = 0; i < 6; ++i) cur[i] = ne[i];
+            ct = seg_tf;
+            root = Root();
+            continue;
+        }
+        // ---- resolve_eclipse_split: replay the crossing step with short steps
+        const Bracket br = O.br;
+        const double a = O.step.t0, b = O.step.t1;
+        double replay_eq[6];
+        if (!rebase(cur, ct, O.step.y0, a, replay_eq)) return done(ST_REBASE_FAILED);
+        if (!std::isfinite(a) || !std::isfinite(b) || a == b || br.old_side == br.new_side) return done(BRACKET);
+        Rhs Rr = make_rhs(replay_eq, a, br.old_side);
+        if (!envelope_at(Rr.base, a, zero, a)) return done(ENVELOPE);
+        LegIn Lr{a, b, {0, 0, 0, 0, 0, 0}, std::min(dtmax, REFINE_STEP_S), 0.0, &root, false};
+        LegOut Or;
+        leg(Rr, J.C, G, Lr, Or, st, sk, replay_eq);
+        if (Rr.bad) return done(ST_GRAVITY);
+        if (!Or.stopped) {
+            if (Or.status != ST_SUCCESS) return done(Or.status >= ENVELOPE ? Or.status : BRACKET);
+            for (int i = 0; i < 6; ++i) cur[i] = replay_eq[i];
+            ct = a;
+            if (b == tf) {
+                to_original(Or.y_end, tf, cur, ct, eq0, t0, delta);
+                return done(ST_SUCCESS);
+            }
+            double ne[6];
+            if (!rebase(cur, ct, Or.y_end, b, ne)) return done(ST_REBASE_FAILED);
+            for (int i = 0; i < 6; ++i) cur[i] = ne[i];
+            ct = b;
+            root = Root();
+            continue;
+        }
+        const Bracket br2 = Or.br;
+        if (br2.old_side != br.old_side || br2.new_side == br.old_side || !std::isfinite(br2.bound) ||
+            !(br2.bound >= 0.0 && br2.bound <= MAX_SEP_KM))
+            return done(BRACKET);
+        if (!(a <= Or.step.t0 && Or.step.t0 < Or.step.t1 && Or.step.t1 <= b)) return done(NON_PROGRESS);
+        const double a2 = Or.step.t0, b2 = Or.step.t1;
+        if (!rebase(replay_eq, a, Or.step.y0, a2, cur)) return done(ST_REBASE_FAILED);
+        ct = a2;
+        // ---- commit_eclipse_root_transaction
+        const double base_t = ct;
+        double base_eq[6];
+        for (int i = 0; i < 6; ++i) base_eq[i] = cur[i];
+        const int idx_base = sink.idx;
+        double anchor = br2.t_old;
+        int restarts = MAX_PROOF_RESTARTS;
+        double proof_old_t = base_t;
+        bool have_proof = false;
+        LegOut Op;
+        for (;;) {
+            if (anchor == base_t) {
+                proof_old_t = base_t;
+            } else if (int e = G.deepest(anchor, base_t, OLD_SIDE_MARGIN_KM, &proof_old_t)) {
+                return done(e);
+            }
+            sink.idx = idx_base;
+            Rhs Rp = make_rhs(base_eq, base_t, br2.old_side);
+            if (!envelope_at(Rp.base, base_t, zero, base_t)) return done(ENVELOPE);
+            if (proof_old_t == base_t) {
+                have_proof = false;
+                break;
+            }
+            LegIn Lp{base_t, proof_old_t, {0, 0, 0, 0, 0, 0},
+                     std::min(std::min(dtmax, REFINE_STEP_S), std::fabs(proof_old_t - base_t)), 0.0, &root, false};
+            leg(Rp, J.C, G, Lp, Op, st, sk, base_eq);
+            if (Rp.bad) return done(ST_GRAVITY);
+            if (Op.stopped) {
+                const double ft = Op.br.t_old;
+                if (restarts == 0 || !std::isfinite(ft) || !(ft < anchor) || Op.br.old_side != br2.old_side)
+                    return done(BRACKET);
+                --restarts;
+                anchor = ft;
+                continue;
+            }
+            if (Op.status != ST_SUCCESS) return done(Op.status >= ENVELOPE ? Op.status : BRACKET);
+            have_proof = true;
+            break;
+        }
+        double pdelta[6] = {0, 0, 0, 0, 0, 0};
+        const Baseline bb = baseline_new(base_eq);
+        if (have_proof) {
+            for (int i = 0; i < 6; ++i) pdelta[i] = Op.y_end[i];
+            if (!envelope_at(bb, base_t, pdelta, proof_old_t)) return done(ENVELOPE);
+            int ps;
+            double pm;
+            if (int e = geometry_at(G, bb, base_t, pdelta, proof_old_t, &ps, &pm)) return done(e);
+            if (ps != br2.old_side) return done(BRACKET);
+        }
+        double window_limit;
+        if (int e = G.deepest(proof_old_t, b2, MAX_ROOT_UNC_KM, &window_limit)) return done(e);
+        if (window_limit < br2.t_new) return done(NON_PROGRESS);
+        Rhs Rw = make_rhs(base_eq, base_t, br2.old_side);
+        LegIn Lw{proof_old_t, window_limit, {0, 0, 0, 0, 0, 0},
+                 std::min(std::min(dtmax, REFINE_STEP_S), std::fabs(window_limit - proof_old_t)), 0.0, &root, true};
+        for (int i = 0; i < 6; ++i) Lw.y0[i] = pdelta[i];
+        LegOut Ow;
+        leg(Rw, J.C, G, Lw, Ow, st, sk, base_eq);
+        if (Rw.bad) return done(ST_GRAVITY);
+        if (!Ow.stopped) return done(Ow.status >= ENVELOPE ? Ow.status : BRACKET);
+        // validate_eclipse_root_commit (1879-1926)
+        const double ev_t = Ow.step.t1;
+        if (Ow.br.old_side != br2.old_side || Ow.br.new_side != br2.new_side) return done(BRACKET);
+        if (!envelope_at(bb, base_t, Ow.y_end, ev_t)) return done(ENVELOPE);
+        int cs;
+        double cm, unc;
+        if (int e = geometry_at(G, bb, base_t, Ow.y_end, ev_t, &cs, &cm)) return done(e);
+        if (int e = G.replay_unc(proof_old_t, ev_t, &unc)) return done(e);
+        if (cs != Ow.br.new_side || unc > MAX_ROOT_UNC_KM) return done(BRACKET);
+        if (!std::isfinite(ev_t) || ev_t == Ow.step.t0 || (root.have && ev_t <= root.t)) return done(CHATTER);
+        if (++splits > MAX_SPLITS) return done(SPLIT_LIMIT);
+        // rebase_after_eclipse_root (1928-1993)
+        double root_eci[6];
+        eci_of(base_eq, base_t, Ow.y_end, ev_t, root_eci);
+        if (!eci2equinoc(root_eci, cur)) return done(ST_REBASE_FAILED);
+        ct = ev_t;
+        side = Ow.br.new_side;
+        double rb[6];
+        equinoc2eci(cur, 0.0, rb);
+        double terr;
+        if (!outward(dist3(root_eci, rb), &terr)) return done(GEOMETRY);
+        if (terr > MAX_SEP_KM) return done(BRACKET);
+        root.have = true;
+        root.t = ev_t;
+        root.err = terr;
+        if (roots) roots->push_back(ev_t);
+    }
+    return done(SPLIT_LIMIT);
+}
+
+}  // namespace ecl
+
 }  // namespace
 
 // ======================================================================
@@ -2610,6 +3362,95 @@ void orc_propagate_sampled_batch(void* f, const double* ctrl, long n, const doub
         steps[i] = st.steps;
         evals[i] = st.evals;
     }
+}
+
+// Solar radiation pressure switches (ForceConfig force_flags SRP, cr, p_sun).
+void orc_force_set_srp(void* f, int on, double cr, double p_sun) {
+    Force* F = (Force*)f;
+    F->srp = on;
+    F->cr = cr;
+    F->p_sun = p_sun;
+}
+
+// The Sun direction rate bound (rad/day) the eclipse scans use.
+double orc_sun_rate_bound(void* f) {
+    Force* F = (Force*)f;
+    return F->eph[0] ? ecl::table_direction_rate(*F->eph[0]) : ecl::SUN_RATE_ANALYTIC;
+}
+
+// Batch through the binary-eclipse coordinator (rows with SRP in effect:
+// srp on and cr, p_sun, A/m > 0; other rows take propagate_final /
+// propagate_sampled).  eq0 [n][6], epoch_jd[n], tf[n], ballistic [n][2];
+// t_eval[n_t] (may be null with n_t 0) common to every row; delta_out [n][6]
+// the final delta against the initial baseline; smp_out [n][n_t][6] (null
+// when n_t is 0); status[n], steps/evals[n], n_written[n].
+void orc_propagate_srp_batch(void* f, const double* ctrl, long n, const double* eq0, const double* epoch_jd,
+                             const double* tf, const double* ballistic, const double* t_eval, int n_t,
+                             double* delta_out, double* smp_out, int* status, long* steps, long* evals,
+                             int* n_written, int threads) {
+    Force* F = (Force*)f;
+    Ctrl C = ctrl_from(ctrl);
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long i = 0; i < n; ++i) {
+        Job J{F, C, epoch_jd[i], ballistic[2 * i], ballistic[2 * i + 1]};
+        Stats st;
+        double d[6];
+        double* out = smp_out ? smp_out + (size_t)i * n_t * 6 : nullptr;
+        if (out)
+            for (long q = 0; q < (long)n_t * 6; ++q) out[q] = NAN;
+        int nw = 0;
+        int s;
+        if (F->srp && F->cr > 0.0 && F->p_sun > 0.0 && J.am > 0.0) {
+            s = ecl::propagate(J, eq0 + 6 * i, 0.0, tf[i], t_eval, out ? n_t : 0, out, d, st, &nw);
+        } else if (out) {
+            s = propagate_sampled(J, eq0 + 6 * i, 0.0, tf[i], t_eval, n_t, out, st, &nw);
+            for (int q = 0; q < 6; ++q) d[q] = nw > 0 ? out[(size_t)(nw - 1) * 6 + q] : NAN;
+        } else {
+            s = propagate_final(J, eq0 + 6 * i, 0.0, tf[i], d, st);
+        }
+        if (s != ST_SUCCESS)
+            for (int q = 0; q < 6; ++q) d[q] = NAN;
+        for (int q = 0; q < 6; ++q) delta_out[6 * i + q] = d[q];
+        status[i] = s;
+        steps[i] = st.steps;
+        evals[i] = st.evals;
+        if (n_written) n_written[i] = nw;
+    }
+}
+
+// One row through the coordinator, with the committed root instants
+// (roots[max_roots], *n_roots = how many were committed).
+int orc_propagate_srp_roots(void* f, const double* ctrl, const double* eq0, double epoch_jd, double tf, double am,
+                            double cd, double* delta, double* roots, int max_roots, int* n_roots, long* steps_evals) {
+    Force* F = (Force*)f;
+    Job J{F, ctrl_from(ctrl), epoch_jd, am, cd};
+    Stats st;
+    std::vector<double> r;
+    const int s = ecl::propagate(J, eq0, 0.0, tf, nullptr, 0, nullptr, delta, st, nullptr, &r);
+    *n_roots = (int)r.size();
+    for (int i = 0; i < (int)r.size() && i < max_roots; ++i) roots[i] = r[i];
+    steps_evals[0] = st.steps;
+    steps_evals[1] = st.evals;
+    return s;
+}
+
+// The coordinator's bounds (test hooks): decisive margin after a root with
+// the given transport error; replay uncertainty over [t0, t1] and the
+// deepest instant within max_km on the arc of epoch_jd.  Return 0 or an
+// eclipse status word.
+int orc_ecl_decisive_margin(double err, double* out) { return ecl::decisive_margin(err, out); }
+int orc_ecl_replay_unc(void* f, double epoch_jd, double t0, double t1, double* out) {
+    Force* F = (Force*)f;
+    ecl::Geo G{F, epoch_jd, F->earth_radius, F->eph[0] ? ecl::table_direction_rate(*F->eph[0]) : ecl::SUN_RATE_ANALYTIC};
+    return G.replay_unc(t0, t1, out);
+}
+int orc_ecl_deepest(void* f, double epoch_jd, double old_t, double lim, double max_km, double* out) {
+    Force* F = (Force*)f;
+    ecl::Geo G{F, epoch_jd, F->earth_radius, F->eph[0] ? ecl::table_direction_rate(*F->eph[0]) : ecl::SUN_RATE_ANALYTIC};
+    return G.deepest(old_t, lim, max_km, out);
 }
 
 // One fixed-time integration without rectification (for solver tests):
