@@ -27,7 +27,12 @@ STATUS_NAMES = {
     0: "ok", 1: "max_steps_exceeded", 2: "step_underflow", 3: "invalid_input",
     4: "non_finite_state", 5: "max_rejects_exceeded", 6: "gravity_invalidradius",
     7: "rebase_failed", 8: "restart_budget_exhausted", 9: "ground", 10: "watchdog",
+    # the reference's eclipse_error_name (eclipse_coordinator.rs:950-966)
+    11: "eclipse_envelope", 12: "eclipse_chatter", 13: "eclipse_bracket", 14: "eclipse_non_progress",
+    15: "eclipse_geometry", 16: "eclipse_split_limit",
 }
+ST_ECLIPSE_ENVELOPE = 11
+ECLIPSE_STATUSES = frozenset(range(11, 17))
 ST_OK, ST_GROUND, ST_GRAVITY_RADIUS = 0, 9, 6
 
 FORCE_DRAG, FORCE_SRP, FORCE_SUN, FORCE_MOON = 1, 2, 4, 8
@@ -53,6 +58,7 @@ class ForceConfig(C.Structure):
         ("max_kernel_seconds", C.c_double), ("engine", C.c_int32), ("gravity_threads", C.c_int32),
         ("gravity_slots", C.c_int32), ("drag_quadrature", C.c_int32), ("split_degree", C.c_int32),
         ("drag_fp32", C.c_int32), ("surrogate", C.c_int32), ("surrogate_check", C.c_double),
+        ("cr", C.c_double), ("p_sun", C.c_double),
     ]
 
 

@@ -15,8 +15,8 @@ Python binding does not expose): ``propagate_batch_final`` and
 ``propagate_batch_sampled``.
 
 Options this build does not implement raise ``ValueError`` naming the option
-(SRP with binary eclipse; the tsit5/rkv98 tableaus); they are never
-silently replaced.  ``gravity_field`` (extra keyword) takes a normalised
+(the tsit5/rkv98 tableaus, SRP with the dopri5 compatibility stepper or
+rtol/atol control); they are never silently replaced.  ``gravity_field`` (extra keyword) takes a normalised
 ``deg ord C S`` text or a path, which lifts the embedded field's degree-15 cap.
 """
 from __future__ import annotations
@@ -88,9 +88,11 @@ def force_config(gravity_order=5, drag=True, srp=True, sun=True, moon=True, atm_
     if name not in _METHODS:
         raise ValueError(f"unknown integrator method {name!r}; use one of vern7, vern9, dop853, tsit5, rkv98, "
                          "dopri5")
-    if srp:
-        raise ValueError("srp=True needs the binary-eclipse SRP coordinator, which is not built here; "
-                         "pass srp=False")
+    if srp and name == "dopri5":
+        raise ValueError("srp=True runs the binary-eclipse coordinator with vern7, vern9 or dop853 here, not the "
+                         "dopri5 compatibility stepper; pass srp=False or another method")
+    if srp and rtol is not None:
+        raise ValueError("srp=True runs with the absolute tolerance tol here, not rtol/atol")
     cfg = N.default_config()
     cfg.order = int(gravity_order)
     flags = 0
@@ -100,7 +102,10 @@ def force_config(gravity_order=5, drag=True, srp=True, sun=True, moon=True, atm_
         flags |= N.FORCE_SUN
     if moon:
         flags |= N.FORCE_MOON
+    if srp:
+        flags |= N.FORCE_SRP
     cfg.force_flags = flags
+    cfg.cr = float(cr)
     cfg.atm_model = int(atm_model) if drag else 0
     cfg.method = _METHODS[name]
     cfg.am_ratio = float(am_ratio)
@@ -196,6 +201,11 @@ def _equinoctial_of(eci, what):
     return equ[0]
 
 
+def _srp_in_effect(cfg) -> bool:
+    """SRP acts (rhs.rs:31-36): the flag with cr, p_sun and A/m all > 0."""
+    return bool(cfg.force_flags & N.FORCE_SRP) and cfg.cr > 0 and cfg.p_sun > 0 and cfg.am_ratio > 0
+
+
 # ------------------------------------------------------------------ scalar API
 def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
               moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
@@ -241,6 +251,11 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
         terminal = ""
     else:
         terminal = N.STATUS_NAMES.get(status, "incomplete")
+    if _srp_in_effect(cfg) and (status in N.ECLIPSE_STATUSES or status == N.ST_GRAVITY_RADIUS):
+        # an eclipse failure returns no samples (lib.rs:297-303, integrator.rs:2463-2473)
+        n_ok = 0
+        if status == N.ST_GRAVITY_RADIUS:
+            terminal = "eclipse_gravity"
     return {
         "times_s": np.array(grid[:n_ok]),
         "states_eci": states[:n_ok].copy(),
@@ -274,6 +289,9 @@ def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, s
         raise ValueError("physically infeasible arc: trajectory hits the ground")
     if status == N.ST_GRAVITY_RADIUS:
         raise ValueError("physically infeasible arc: radius fell below the Earth's surface")
+    if status == N.ST_ECLIPSE_ENVELOPE:
+        raise ValueError("state outside the SRP eclipse envelope (radius 6000-50000 km, speed <= 20 km/s); "
+                         "pass srp=False")
     if status != N.ST_OK:
         raise RuntimeError(f"propagation failed: {N.STATUS_NAMES.get(status, status)}")
     return out[0].copy()

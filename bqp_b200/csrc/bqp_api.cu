@@ -20,6 +20,7 @@
 
 #include "../../include/bqp_prop.h"
 #include "launch.h"
+#include "eclipse.cuh"
 #include "ephemeris.h"
 #include "space_weather.h"
 #include "surrogate.h"
@@ -513,6 +514,9 @@ struct bqp_ctx {
     jb::DriverTable dtab{};       // the device copy as the kernels see it (n_solar 0: none)
     double* d_eph[2] = {nullptr, nullptr};  // Sun / Moon catalogues (bqp_ctx_set_ephemeris)
     EphemTable eph[2] = {};                 // their device views (n 0: the analytic series)
+    double sun_rate = kSunRateAnalytic;     // bound of the Sun direction's rate, rad/day
+    EclState* d_ecl = nullptr;              // eclipse coordinator state, one per SRP row
+    int64_t ecl_cap = 0;
     bool profile = false;  // kernel timing on (bqp_ctx_profile)
     KernelTimes times{};
     Model* sur = nullptr;          // learned gravity surrogate (bqp_surrogate_*)
@@ -526,8 +530,14 @@ int validate_cfg(const bqp_force_config* c) {
     if (!c) return fail(BQP_E_ARG, "null config");
     if (c->order < 0 || c->order > kMaxOrder)
         return fail(BQP_E_ARG, "order must be in 0..%d, got %d", kMaxOrder, c->order);
-    if (c->force_flags & BQP_FORCE_SRP)
-        return fail(BQP_E_UNSUPPORTED, "solar radiation pressure (binary-eclipse SRP) is not built; pass srp=False");
+    if (c->force_flags & BQP_FORCE_SRP) {
+        if (c->method == BQP_METHOD_DOPRI5_COMPAT)
+            return fail(BQP_E_UNSUPPORTED, "binary-eclipse SRP runs with the dopri5 / dop853 / vern7 / vern9 steppers");
+        if (c->error_control != 0)
+            return fail(BQP_E_UNSUPPORTED, "binary-eclipse SRP runs with absolute error control (error_control 0)");
+    }
+    if (!(std::isfinite(c->cr) && c->cr >= 0.0 && std::isfinite(c->p_sun) && c->p_sun >= 0.0))
+        return fail(BQP_E_ARG, "cr and p_sun must be finite and >= 0");
     if (c->force_flags & ~(BQP_FORCE_DRAG | BQP_FORCE_SUN | BQP_FORCE_MOON | BQP_FORCE_SRP))
         return fail(BQP_E_ARG, "unknown force flags 0x%x", c->force_flags);
     if ((c->force_flags & BQP_FORCE_DRAG) && (c->atm_model < 4 || c->atm_model > 7))
@@ -587,6 +597,10 @@ ForceParams force_params(const bqp_ctx* ctx) {
     fp.ground_check = c.ground_check;
     fp.atm_model = (c.force_flags & BQP_FORCE_DRAG) ? c.atm_model : 4;
     fp.drag_fp32 = c.drag_fp32;
+    fp.srp = (c.force_flags & BQP_FORCE_SRP) ? 1 : 0;
+    fp.cr = c.cr;
+    fp.p_sun = c.p_sun;
+    fp.sun_rate = ctx->sun_rate;
     fp.earth_radius = c.earth_radius;
     fp.omega = c.omega_earth;
     fp.mu_sun = c.mu_sun;
@@ -780,6 +794,20 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.grav = grav_table(ctx);
     if (ctx->cfg.surrogate) {
         if (int rc = surrogate_stage_args(ctx, A.sur)) return rc;
+    }
+    if (A.force.srp) {
+        if (n > ctx->ecl_cap) {
+            if (ctx->d_ecl) {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(ctx->d_ecl);
+                ctx->d_ecl = nullptr;
+                ctx->ecl_cap = 0;
+            }
+            cudaError_t e = cudaMalloc(&ctx->d_ecl, (size_t)n * sizeof(EclState));
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(eclipse coordinator state)");
+            ctx->ecl_cap = n;
+        }
+        A.ecl = ctx->d_ecl;
     }
     if (ctx->cfg.engine == BQP_ENGINE_PIPELINE) {
         const size_t need = pipeline_bytes(n);
@@ -1013,6 +1041,8 @@ void bqp_force_config_default(bqp_force_config* c) {
     c->drag_fp32 = 0;
     c->surrogate = 0;
     c->surrogate_check = 0.0;
+    c->cr = 1.3;                       // Python cr default (lib.rs:241)
+    c->p_sun = kPSun;                  // ForceConfig::default (types.rs:459)
 }
 
 const char* bqp_last_error(void) { return g_err.c_str(); }
@@ -1068,6 +1098,7 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     else cudaDeviceSynchronize();
     if (ctx->d_tab) cudaFree(ctx->d_tab);
     if (ctx->d_queue) cudaFree(ctx->d_queue);
+    if (ctx->d_ecl) cudaFree(ctx->d_ecl);
     if (ctx->d_ws) cudaFree(ctx->d_ws);
     if (ctx->d_pws) cudaFree(ctx->d_pws);
     if (ctx->d_fit) cudaFree(ctx->d_fit);
@@ -1210,6 +1241,7 @@ int bqp_ctx_set_ephemeris(bqp_ctx* ctx, int32_t body, const uint8_t* bytes, int6
     if (ctx->d_eph[body]) cudaFree(ctx->d_eph[body]);
     ctx->d_eph[body] = nullptr;
     ctx->eph[body] = EphemTable{};
+    if (body == BQP_BODY_SUN) ctx->sun_rate = bytes ? ephemeris_direction_rate(e) : kSunRateAnalytic;
     if (!bytes) return 0;
     cudaError_t err = cudaMalloc(&ctx->d_eph[body], e.pos.size() * sizeof(double));
     if (err == cudaSuccess)
@@ -1600,11 +1632,13 @@ int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32
     // this path runs the persistent kernel on the FP64 field; a context set
     // up for a form only the stage-synchronous engine has is refused, not
     // run in plain FP64
-    if (ctx->cfg.split_degree || ctx->cfg.surrogate || ctx->cfg.drag_fp32)
+    if (ctx->cfg.split_degree || ctx->cfg.surrogate || ctx->cfg.drag_fp32 || (ctx->cfg.force_flags & BQP_FORCE_SRP))
         return fail(BQP_E_UNSUPPORTED,
-                    "the no-allocation entry point runs plain FP64 only; this context is configured for %s",
-                    ctx->cfg.surrogate ? "the learned surrogate" : ctx->cfg.split_degree ? "split precision"
-                                                                                     : "the FP32 density");
+                    "the no-allocation entry point runs plain FP64 without SRP only; this context is configured for %s",
+                    ctx->cfg.surrogate ? "the learned surrogate"
+                    : ctx->cfg.split_degree ? "split precision"
+                    : ctx->cfg.drag_fp32 ? "the FP32 density"
+                                         : "binary-eclipse SRP");
     int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
     if (rc) return rc;
     if (n > BQP_NOALLOC_MAX_TRAJ)

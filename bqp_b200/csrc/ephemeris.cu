@@ -6,6 +6,7 @@
 // and every position must be finite.
 #include "ephemeris.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -53,6 +54,29 @@ std::string parse_ephemeris(const uint8_t* b, int64_t len, int body, Ephemeris* 
     e.inv_dt = 1.0 / dt;
     *out = std::move(e);
     return "";
+}
+
+// For p(s) = b + s d on one piece, the unit vector turns at |b x d| / |p(s)|^2
+// per grid step; the largest value is at the point of the piece closest to
+// the origin.
+double ephemeris_direction_rate(const Ephemeris& e) {
+    if (e.n < 2 || !(std::isfinite(e.dt) && e.dt > 0.0)) return 0.0;
+    double sup = 0.0;
+    for (int64_t i = 0; i + 1 < e.n; ++i) {
+        const double* b = &e.pos[3 * i];
+        const double* a = &e.pos[3 * (i + 1)];
+        const double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+        const double c[3] = {b[1] * d[2] - b[2] * d[1], b[2] * d[0] - b[0] * d[2], b[0] * d[1] - b[1] * d[0]};
+        const double cn = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        const double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        const double pr = std::fma(b[0], d[0], std::fma(b[1], d[1], b[2] * d[2]));
+        const double s = d2 > 0.0 ? std::min(std::max(-pr / d2, 0.0), 1.0) : 0.0;
+        const double q[3] = {std::fma(s, d[0], b[0]), std::fma(s, d[1], b[1]), std::fma(s, d[2], b[2])};
+        const double q2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        if (!(std::isfinite(q2) && q2 > 0.0)) return NAN;
+        sup = std::max(sup, cn / (e.dt * q2));
+    }
+    return sup;
 }
 
 }  // namespace bqp

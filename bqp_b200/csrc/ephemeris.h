@@ -22,4 +22,9 @@ struct Ephemeris {
 // Parses a catalogue for body 0 (Sun) or 1 (Moon); "" on success, else the reason.
 std::string parse_ephemeris(const uint8_t* bytes, int64_t len, int body, Ephemeris* out);
 
+// Supremum of the catalogue direction's angular rate over its linear pieces,
+// rad/day (the bound of the eclipse scans, precomputed_ephem.rs:947-1021);
+// NaN when a piece passes through the origin.
+double ephemeris_direction_rate(const Ephemeris& e);
+
 }  // namespace bqp

@@ -25,6 +25,13 @@ enum Status : int32_t {
     kRestartBudget = 8,
     kGround = 9,
     kWatchdog = 10,
+    // binary-eclipse coordinator failures (EclipseError, eclipse.rs)
+    kEclEnvelope = 11,
+    kEclChatter = 12,
+    kEclBracket = 13,
+    kEclNonProgress = 14,
+    kEclGeometry = 15,
+    kEclSplitLimit = 16,
 };
 
 enum Method : int32_t { kDopri5 = 0, kDop853 = 1, kDopri5Compat = 2, kVern7 = 3, kVern9 = 4 };
@@ -37,6 +44,9 @@ struct ForceParams {
     int32_t ground_check;  // terminal ground event (final-state path)
     int32_t atm_model;     // JB2008 profile: 4 exact; 5, 6, 7 the coarse quadrature profiles
     int32_t drag_fp32;     // split precision: the coarse profile's density in FP32
+    int32_t srp;           // solar radiation pressure through the eclipse coordinator
+    double cr, p_sun;      // SRP reflectivity coefficient, pressure at 1 AU (N/m^2)
+    double sun_rate;       // bound of the Sun direction's angular rate, rad/day
     double earth_radius;
     double omega;
     double mu_sun, mu_moon;
@@ -89,7 +99,8 @@ struct Encke {
     double seg_t0;
     double jd0;
     double am, cd;
-    int bad;  // latched invalid-radius gravity error
+    int side;  // SRP eclipse side of the row's leg (1 shadow, 0 lit), -1 without SRP
+    int bad;   // latched invalid-radius gravity error
 
     __device__ __noinline__ void eval(double t, const double* d, double* out) {
         double rs[6];
@@ -137,6 +148,12 @@ struct Encke {
                     acc[2] += k * vr2;
                 }
             }
+        }
+        if (side >= 0) {
+            // after drag, before the third bodies (rhs.rs:4033-4063)
+            if (!have_sun) sun_at(fp->eph_sun, jd, sun);
+            have_sun = true;
+            srp_accel(sp, sun, fp->p_sun, fp->cr, am, side, acc);
         }
         if (fp->sun) {
             if (!have_sun) sun_at(fp->eph_sun, jd, sun);

@@ -48,6 +48,7 @@ struct PropArgs {
     CtrlParams ctrl;
     const jb::JbFit* fit_host;     // host copy of *force.fit (null with it): the stage-synchronous
                                    // drag kernel takes it by value, in kernel parameter space
+    struct EclState* ecl;          // [n] eclipse coordinator state of SRP rows (null without SRP)
 };
 
 struct TrajState;

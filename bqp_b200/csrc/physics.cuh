@@ -448,6 +448,67 @@ BQP_HD void third_body(const double* sat, const double* body, double mu_body, do
     acc[2] += mu_coef * (r2 * inv3 - bn2);
 }
 
+// ------------------------------------------ solar radiation pressure, shadow
+constexpr double kAuKm = 149597870.7;
+constexpr double kPSun = 4.56e-6;  // N/m^2 at 1 AU (types.rs:459)
+
+// Binary shadow cylinder of the Earth along the Sun direction
+// (eclipse.rs:189-262): *shadow 1 behind the Earth inside the cylinder,
+// else 0; *margin the distance to the boundary (the nearer of the axial and
+// radial distances in shadow).  False on invalid geometry.
+BQP_HD bool shadow_cylinder(const double* sat, const double* sun, double earth_radius, int* shadow,
+                            double* margin) {
+    for (int i = 0; i < 3; ++i)
+        if (!isfinite(sat[i]) || !isfinite(sun[i])) return false;
+    if (!(isfinite(earth_radius) && earth_radius > 0.0)) return false;
+    const double sun_sq = sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2];
+    if (!(isfinite(sun_sq) && sun_sq > 0.0)) return false;
+    const double inv = 1.0 / sqrt(sun_sq);
+    const double u0 = sun[0] * inv, u1 = sun[1] * inv, u2 = sun[2] * inv;
+    const double axial = fma(sat[0], u0, fma(sat[1], u1, sat[2] * u2));
+    const double q0 = sat[0] - axial * u0, q1 = sat[1] - axial * u1, q2 = sat[2] - axial * u2;
+    const double rad_sq = fma(q0, q0, fma(q1, q1, q2 * q2));
+    const double r_sq = earth_radius * earth_radius;
+    if (!(isfinite(axial) && isfinite(rad_sq) && isfinite(r_sq))) return false;
+    const double rd = sqrt(rad_sq);
+    const double signed_margin = (rad_sq - r_sq) / (rd + earth_radius);
+    double m;
+    if (axial < 0.0 && rad_sq < r_sq) {
+        *shadow = 1;
+        m = fmin(-axial, -signed_margin);
+    } else {
+        *shadow = 0;
+        const bool a = axial >= 0.0, b = rad_sq >= r_sq;
+        m = a && b ? fmax(axial, signed_margin) : (a ? axial : (b ? signed_margin : 0.0));
+    }
+    if (!(isfinite(m) && m >= 0.0)) return false;
+    *margin = m;
+    return true;
+}
+
+// Cannonball solar radiation pressure (rhs.rs:1269-1310) added into acc
+// (km/s^2): p_sun cr A/m (AU/d)^2 away from the Sun, none in shadow.
+BQP_HD void srp_accel(const double* sat, const double* sun, double p_sun, double cr, double am, int shadow,
+                      double* acc) {
+    if (cr == 0.0 || am == 0.0 || p_sun == 0.0) return;
+    if (!isfinite(sat[0]) || !isfinite(sat[1]) || !isfinite(sat[2])) {
+        acc[0] = acc[1] = acc[2] = NAN;
+        return;
+    }
+    if (shadow) return;
+    const double rx = sun[0] - sat[0], ry = sun[1] - sat[1], rz = sun[2] - sat[2];
+    const double d2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    if (!(isfinite(d2) && d2 > 0.0)) {
+        acc[0] = acc[1] = acc[2] = NAN;
+        return;
+    }
+    const double inv = 1.0 / sqrt(d2);
+    const double a = p_sun * cr * am * ((kAuKm * kAuKm) / d2) * 0.001;
+    acc[0] += -a * rx * inv;
+    acc[1] += -a * ry * inv;
+    acc[2] += -a * rz * inv;
+}
+
 // Battin's f(q) form of the Encke central-body difference (rhs.rs:1071-1104):
 // mu (r_b/|r_b|^3 - r_p/|r_p|^3) = mu/|r_p|^3 (f(q) r_b - dr).
 BQP_HD void battin(const double* rb, const double* dr, double rp2, double rp, double* acc) {

@@ -162,8 +162,9 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
     P.sc[P.cap + slot] = cs;
     double acc[3] = {0.0, 0.0, 0.0};
     double sun[3];
-    const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0);
+    const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0) || s.side >= 0;
     if (need_sun) sun_at(fp.eph_sun, jd, sun);
+    if (s.side >= 0) srp_accel(sp, sun, fp.p_sun, fp.cr, s.am, s.side, acc);  // on the leg's fixed side
     if (fp.sun) third_body(sp, sun, fp.mu_sun, acc);
     if (fp.moon) {
         double moon[3];
@@ -407,7 +408,7 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
             if (T::FSAL) {
                 for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S - 1, i)[slot];
                 dy_next = dyn;
-            } else if (dense && (s.flags & kSegSampled)) {
+            } else if (dense && (s.flags & (kSegSampled | kEcl))) {
                 for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S, i)[slot];
                 dy_next = dyn;
                 ++s.evals;  // counted on accept only, as the reference evaluates it
@@ -483,7 +484,9 @@ template <int M>
 static cudaError_t run(const PropArgs& A, const PipeBufs& P, cudaStream_t user, double max_seconds,
                        int gthreads, int gslots, KernelTimes* times) {
     using T = Tab<M>;
-    const bool dense = A.out_mode != kOutFinalEci && !T::FSAL;
+    // the dense stage: the end-of-step derivative of sampled segments and of
+    // the eclipse coordinator's Hermite scan
+    const bool dense = (A.out_mode != kOutFinalEci || A.force.srp) && !T::FSAL;
     const int stages = T::S + (dense ? 1 : 0);
     const int blocks = (int)((A.n + kBlock - 1) / kBlock);
     constexpr int kLanesHigh = BQP_DRAG_LANES_HIGH, kLanesLow = BQP_DRAG_LANES_LOW;

@@ -77,6 +77,7 @@ __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem,
         R.jd0 = jd0[i];
         R.am = ballistic ? ballistic[2 * i] : am0;
         R.cd = ballistic ? ballistic[2 * i + 1] : cd0;
+        R.side = -1;
         R.bad = 0;
         double d[6], o[6];
         for (int q = 0; q < 6; ++q) d[q] = delta[6 * i + q];
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
     Encke R;
     R.tab = tab;
     R.fp = &A.force;
+    R.side = -1;
     R.bad = 0;
 
     double k[S * 6];
@@ -142,6 +144,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
         R.jd0 = s.jd0;
         R.am = s.am;
         R.cd = s.cd;
+        R.side = s.side;
         R.bad = 0;
         if (s.flags & kHaveK1) {
             for (int i = 0; i < 6; ++i) k[i] = s.k1c[i];
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
             const double* dy_next = nullptr;
             if (T::FSAL) {
                 dy_next = k + (S - 1) * 6;
-            } else if (s.flags & kSegSampled) {
+            } else if (s.flags & (kSegSampled | kEcl)) {
                 R.eval(next_time(s), ynext, dyn);  // the reference's dense k1 (solver.rs:1672-1676)
                 ++s.evals;
                 dy_next = dyn;

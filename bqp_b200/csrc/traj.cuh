@@ -14,6 +14,7 @@
 #pragma once
 #include <cstdint>
 
+#include "eclipse.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -69,13 +70,16 @@ struct Tab<kVern9> {
 
 enum OutMode : int32_t { kOutFinalEci = 0, kOutSampledEci = 1, kOutSampledDelta = 2 };
 enum Phase : int32_t { kNeedTraj = 0, kNeedSegment = 1, kStepping = 2, kDone = 3, kFinished = 4 };
-enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16, kSegSampled = 32 };
+// kEcl: the row runs through the binary-eclipse coordinator (SRP on).
+enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands = 16, kSegSampled = 32, kEcl = 64 };
 
 struct TrajState {
     double tf, ct0, seg_tf, t, h, err_prev, t_comp, hs, hcarry;
     double jd0, am, cd;
+    double lhmax;  // the eclipse leg's maximum step
     double cur[6], equ0[6], y[6], k1c[6];
     int32_t flags, rejects, s_idx, phase, status;
+    int32_t side;  // the eclipse leg's fixed side (1 shadow, 0 lit), -1 without SRP
     int64_t seg_steps, steps, evals, attempts, restarts, max_restarts;
 };
 
@@ -183,6 +187,31 @@ static __device__ __noinline__ void traj_begin(const PropArgs& A, TrajState& s, 
     }
     for (int i = 0; i < 6; ++i) s.cur[i] = s.equ0[i];
     s.ct0 = A.t0;
+    s.side = -1;
+    s.lhmax = 0.0;
+    if (A.force.srp && A.force.cr > 0.0 && A.force.p_sun > 0.0 && s.am > 0.0) {
+        // SRP in effect (rhs.rs:31-36): the eclipse coordinator, whose
+        // samples are always carried to the original baseline
+        EclState& E = A.ecl[traj];
+        E = EclState{};
+        s.flags |= kEcl | kHad;
+        if (s.tf != A.t0) {
+            const Baseline b0 = baseline_new(s.cur);
+            const double zero[6] = {0, 0, 0, 0, 0, 0};
+            if (!ecl_envelope(b0, s.ct0, zero, s.ct0)) {
+                traj_fail(A, s, traj, kEclEnvelope);
+                return;
+            }
+            const EclGeo G{&A.force, s.jd0};
+            int side;
+            double margin;
+            if (int32_t e = ecl_side_at(G, b0, s.ct0, zero, s.ct0, &side, &margin)) {
+                traj_fail(A, s, traj, e);
+                return;
+            }
+            s.side = side;
+        }
+    }
     const double span = fabs(s.tf - A.t0);
     const int64_t mr = (int64_t)ceil(span / (A.ctrl.h_max > 0.0 ? A.ctrl.h_max : 1.0)) + 128;
     s.max_restarts = mr < 100 ? 100 : (mr > 500000 ? 500000 : mr);
@@ -200,7 +229,14 @@ static __device__ __noinline__ void traj_begin(const PropArgs& A, TrajState& s, 
 // Start the next Encke segment, or end the arc.  Leaves kStepping or
 // kFinished.
 template <int M>
+__device__ void ecl_seg_begin(const PropArgs& A, TrajState& s, int64_t traj);
+
+template <int M>
 __device__ __noinline__ void seg_begin(const PropArgs& A, TrajState& s, int64_t traj) {
+    if (s.flags & kEcl) {
+        ecl_seg_begin<M>(A, s, traj);
+        return;
+    }
     for (int guard = 0; guard < 2 && s.phase == kNeedSegment; ++guard) {
         if ((s.flags & kHad) && fabs(s.tf - s.ct0) < 1e-12) {  // integrator.rs:3440-3452
             const double zero[6] = {0, 0, 0, 0, 0, 0};
@@ -254,6 +290,7 @@ __device__ __forceinline__ double next_time(const TrajState& s) {
 }
 
 __device__ __forceinline__ double seg_hmax(const PropArgs& A, const TrajState& s) {
+    if (s.flags & kEcl) return s.lhmax;
     const double hm = fabs(A.ctrl.h_max);
     return (hm > 0.0 && isfinite(hm)) ? hm : fabs(s.seg_tf - s.ct0);
 }
@@ -407,6 +444,34 @@ __device__ __forceinline__ int32_t attempt_decide(const PropArgs& A, TrajState& 
     return kReject;
 }
 
+// Samples inside the accepted step [s.t, tn]: the step's cubic Hermite
+// interpolant (solver.rs:1746-1800), the end state itself at tn.
+static __device__ __noinline__ void emit_samples(const PropArgs& A, TrajState& s, int64_t traj, double tn,
+                                                 const double* ynext, const double* dy_prev, const double* dy_next) {
+    while (s.s_idx < A.n_t) {
+        const double ts = A.t_eval[s.s_idx];
+        if (ts - tn > 0.0) break;
+        double ds[6];
+        if (ts == tn) {
+            for (int i = 0; i < 6; ++i) ds[i] = ynext[i];
+        } else {
+            const double hd = tn - s.t;
+            const double tau = clampd((ts - s.t) / hd, 0.0, 1.0);
+            const double t2 = tau * tau, t3 = t2 * tau;
+            const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
+            const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+            for (int i = 0; i < 6; ++i)
+                ds[i] = h00 * s.y[i] + h10 * hd * dy_prev[i] + h01 * ynext[i] + h11 * hd * dy_next[i];
+        }
+        write_sample(A, s, traj, ds, ts);
+        ++s.s_idx;
+    }
+}
+
+template <int M>
+__device__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+                           const double* dy_prev, const double* dy_next, double en);
+
 // Accepted step: time update, samples, PI controller, ground check and the
 // segment end.  dy_prev = derivative at the step start, dy_next = at its end
 // (FSAL last stage or the dense stage; may be null in final-state mode).
@@ -414,6 +479,10 @@ template <int M>
 __device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
                                             const double* dy_prev, const double* dy_next, double en) {
     using T = Tab<M>;
+    if (M != kDopri5Compat && (s.flags & kEcl)) {
+        ecl_accept<M>(A, s, traj, ynext, dy_prev, dy_next, en);
+        return;
+    }
     const CtrlParams& C = A.ctrl;
     const double order = (double)T::ORDER_ERR + 1.0;
     const double inv_order = 1.0 / order;
@@ -438,26 +507,7 @@ __device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int
         ++s.steps;
     }
     s.rejects = 0;
-    if (sampled_mode(A)) {
-        while (s.s_idx < A.n_t) {
-            const double ts = A.t_eval[s.s_idx];
-            if (ts - tn > 0.0) break;
-            double ds[6];
-            if (ts == tn) {
-                for (int i = 0; i < 6; ++i) ds[i] = ynext[i];
-            } else {
-                const double hd = tn - s.t;
-                const double tau = clampd((ts - s.t) / hd, 0.0, 1.0);
-                const double t2 = tau * tau, t3 = t2 * tau;
-                const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + tau;
-                const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
-                for (int i = 0; i < 6; ++i)
-                    ds[i] = h00 * s.y[i] + h10 * hd * dy_prev[i] + h01 * ynext[i] + h11 * hd * dy_next[i];
-            }
-            write_sample(A, s, traj, ds, ts);
-            ++s.s_idx;
-        }
-    }
+    if (sampled_mode(A)) emit_samples(A, s, traj, tn, ynext, dy_prev, dy_next);
     if (T::FSAL || (s.flags & kSegSampled)) {
         for (int i = 0; i < 6; ++i) s.k1c[i] = dy_next[i];
         s.flags |= kHaveK1;
@@ -517,6 +567,295 @@ __device__ __noinline__ void attempt_accept(const PropArgs& A, TrajState& s, int
             traj_finish_with(A, s, traj, s.y);
         }
     }
+}
+
+// ------------------------------------------------- binary-eclipse coordinator
+// integrate_binary_eclipse_scalar_with_rhs_inner (eclipse_coordinator.rs:
+// 1228-1443), events off, as a per-row state machine over legs.  Every leg
+// integrates the Encke deviation against the row's baseline (cur, ct0) with
+// the eclipse side fixed, absolute max-norm error control, the end-of-step
+// derivative handed forward as the next first stage and a fresh controller
+// (integrate_segment_with_method, integrator.rs:404-556):
+//   main    up to 5400 s; the step-size carry of the previous main leg
+//   refine  the main leg's crossing step replayed with steps <= 10 s
+//   proof   the old side proven up to just before the detected root
+//   window  one short leg past the root; its crossing step commits the root
+// A crossing found in a main / refine / proof step discards that step (its
+// samples are not written); the window's crossing step is kept.
+
+// Equinoctial elements of baseline + delta at t (the coordinator's rebase).
+__device__ __forceinline__ bool ecl_rebase(const double* cur, double ct0, const double* d, double t, double* out) {
+    double b[6], e[6];
+    baseline_state(baseline_new(cur), t - ct0, b);
+    for (int i = 0; i < 6; ++i) e[i] = b[i] + d[i];
+    return eci_to_equinoctial(e, out);
+}
+
+// Open a leg at (t, y0) ending at `end` with maximum step hmax; h0 > 0 is
+// the carried opening step, else span/100 (span/2 up to 60 s).
+__device__ __forceinline__ void ecl_leg_start(TrajState& s, EclState& E, int32_t leg, double t, const double* y0,
+                                              double end, double hmax, double h0) {
+    E.leg = leg;
+    s.t = t;
+    for (int i = 0; i < 6; ++i) s.y[i] = y0[i];
+    s.seg_tf = end;
+    double hm = fabs(hmax);
+    const double hmin = fmin(hm, 1e-12);
+    if (hm < hmin) hm = hmin;
+    s.lhmax = hm;
+    const double span = fabs(end - t);
+    s.h = h0 > 0.0 ? clampd(h0, hmin, hm) : clampd(span <= 60.0 ? span / 2.0 : span / 100.0, hmin, hm);
+    s.err_prev = 0.0;
+    s.t_comp = 0.0;
+    s.flags &= kHad | kEcl;  // fresh controller, no carried first stage
+    s.rejects = 0;
+    s.seg_steps = 0;
+    E.fch = 0.0;
+    s.phase = kStepping;
+}
+
+// Main-loop top: finish at tf or open the next main leg.
+template <int M>
+__device__ void ecl_seg_begin(const PropArgs& A, TrajState& s, int64_t traj) {
+    EclState& E = A.ecl[traj];
+    const double zero[6] = {0, 0, 0, 0, 0, 0};
+    if (s.ct0 == s.tf) {
+        traj_finish_with(A, s, traj, zero);
+        return;
+    }
+    if (++E.iters > kEclMaxIter) {
+        traj_fail(A, s, traj, kEclSplitLimit);
+        return;
+    }
+    const double rem = s.tf - s.ct0;
+    const double end = fabs(rem) > kMaxSegmentS ? s.ct0 + kMaxSegmentS : s.tf;
+    const double dtmax = A.ctrl.h_max;
+    ecl_leg_start(s, E, kLegMain, s.ct0, zero, end, dtmax, dtmax > kEclHcarryMinDtMax ? s.hcarry : 0.0);
+}
+
+// Window leg from the proof point: ends at the deepest instant within the
+// root budget past it (eclipse_coordinator.rs:2224-2290).
+static __device__ __noinline__ void ecl_window_start(const PropArgs& A, TrajState& s, EclState& E, int64_t traj,
+                                              const double* y0) {
+    const EclGeo G{&A.force, s.jd0};
+    double wl;
+    if (int32_t e = G.deepest(E.proof_old_t, E.b2, kEclRootUncKm, &wl)) {
+        traj_fail(A, s, traj, e);
+        return;
+    }
+    if (wl < E.br_tnew) {
+        traj_fail(A, s, traj, kEclNonProgress);
+        return;
+    }
+    const double hm = fmin(fmin(A.ctrl.h_max, kEclRefineStepS), fabs(wl - E.proof_old_t));
+    ecl_leg_start(s, E, kLegWindow, E.proof_old_t, y0, wl, hm, 0.0);
+}
+
+// Old-side proof leg from the transaction base (cur, ct0) to just before
+// the anchor (eclipse_coordinator.rs:1995-2162); none when the base is the
+// crossing itself.
+static __device__ __noinline__ void ecl_proof_start(const PropArgs& A, TrajState& s, EclState& E, int64_t traj) {
+    const EclGeo G{&A.force, s.jd0};
+    const double base_t = s.ct0;
+    const double zero[6] = {0, 0, 0, 0, 0, 0};
+    double pot = base_t;
+    if (E.anchor != base_t) {
+        if (int32_t e = G.deepest(E.anchor, base_t, kEclOldSideMarginKm, &pot)) {
+            traj_fail(A, s, traj, e);
+            return;
+        }
+    }
+    E.proof_old_t = pot;
+    s.s_idx = E.idx_base;  // a restarted proof rewrites its samples
+    if (!ecl_envelope(baseline_new(s.cur), base_t, zero, base_t)) {
+        traj_fail(A, s, traj, kEclEnvelope);
+        return;
+    }
+    if (pot == base_t) {
+        ecl_window_start(A, s, E, traj, zero);
+        return;
+    }
+    const double hm = fmin(fmin(A.ctrl.h_max, kEclRefineStepS), fabs(pot - base_t));
+    ecl_leg_start(s, E, kLegProof, base_t, zero, pot, hm, 0.0);
+}
+
+// A crossing found in the accepted step [s.t, tn] of the current leg.
+static __device__ __noinline__ void ecl_crossing(const PropArgs& A, TrajState& s, EclState& E, int64_t traj,
+                                          const EclBracket& br, double tn, const double* ynext) {
+    const double dtmax = A.ctrl.h_max;
+    const double zero[6] = {0, 0, 0, 0, 0, 0};
+    if (E.leg == kLegMain) {
+        // resolve_eclipse_split (1453-1619): replay the step from its start
+        if (dtmax > kEclHcarryMinDtMax && E.fch > 0.0) s.hcarry = E.fch;
+        const double a = s.t, b = tn;
+        double re[6];
+        if (!ecl_rebase(s.cur, s.ct0, s.y, a, re)) return traj_fail(A, s, traj, kRebaseFailed);
+        if (!isfinite(a) || !isfinite(b) || a == b || br.old_side == br.new_side)
+            return traj_fail(A, s, traj, kEclBracket);
+        for (int i = 0; i < 6; ++i) s.cur[i] = re[i];
+        s.ct0 = a;
+        if (!ecl_envelope(baseline_new(s.cur), a, zero, a)) return traj_fail(A, s, traj, kEclEnvelope);
+        E.a = a;
+        E.b = b;
+        E.br_old = br.old_side;
+        E.br_new = br.new_side;
+        ecl_leg_start(s, E, kLegRefine, a, zero, b, fmin(dtmax, kEclRefineStepS), 0.0);
+        return;
+    }
+    if (E.leg == kLegRefine) {
+        // refine_eclipse_bracket's checks (1621-1738), rebase at the fine
+        // step's start, then the root transaction (2164-2370)
+        if (br.old_side != E.br_old || br.new_side == E.br_old || !isfinite(br.bound) ||
+            !(br.bound >= 0.0 && br.bound <= kEclMaxSepKm))
+            return traj_fail(A, s, traj, kEclBracket);
+        if (!(E.a <= s.t && s.t < tn && tn <= E.b)) return traj_fail(A, s, traj, kEclNonProgress);
+        double re[6];
+        if (!ecl_rebase(s.cur, s.ct0, s.y, s.t, re)) return traj_fail(A, s, traj, kRebaseFailed);
+        for (int i = 0; i < 6; ++i) s.cur[i] = re[i];
+        s.ct0 = s.t;
+        E.b2 = tn;
+        E.br_told = br.t_old;
+        E.br_tnew = br.t_new;
+        E.br_old = br.old_side;
+        E.br_new = br.new_side;
+        E.anchor = br.t_old;
+        E.restarts = kEclProofRestarts;
+        E.idx_base = s.s_idx;
+        ecl_proof_start(A, s, E, traj);
+        return;
+    }
+    if (E.leg == kLegProof) {
+        // the proof leg found the crossing earlier than its anchor: restart
+        // from that better-resolved anchor (2076-2162)
+        const double ft = br.t_old;
+        if (E.restarts == 0 || !isfinite(ft) || !(ft < E.anchor) || br.old_side != E.br_old)
+            return traj_fail(A, s, traj, kEclBracket);
+        --E.restarts;
+        E.anchor = ft;
+        ecl_proof_start(A, s, E, traj);
+        return;
+    }
+    // window: validate_eclipse_root_commit (1879-1926), rebase_after_eclipse_root (1928-1993)
+    const double ev = tn;
+    if (br.old_side != E.br_old || br.new_side != E.br_new) return traj_fail(A, s, traj, kEclBracket);
+    const Baseline bb = baseline_new(s.cur);
+    if (!ecl_envelope(bb, s.ct0, ynext, ev)) return traj_fail(A, s, traj, kEclEnvelope);
+    const EclGeo G{&A.force, s.jd0};
+    int cs;
+    double cm, unc;
+    if (int32_t e = ecl_side_at(G, bb, s.ct0, ynext, ev, &cs, &cm)) return traj_fail(A, s, traj, e);
+    if (int32_t e = G.replay_unc(E.proof_old_t, ev, &unc)) return traj_fail(A, s, traj, e);
+    if (cs != br.new_side || unc > kEclRootUncKm) return traj_fail(A, s, traj, kEclBracket);
+    if (!isfinite(ev) || ev == s.t || (E.have_root && ev <= E.root_t)) return traj_fail(A, s, traj, kEclChatter);
+    if (++E.splits > kEclMaxSplits) return traj_fail(A, s, traj, kEclSplitLimit);
+    double b[6], eci[6], re[6];
+    baseline_state(bb, ev - s.ct0, b);
+    for (int i = 0; i < 6; ++i) eci[i] = b[i] + ynext[i];
+    if (!eci_to_equinoctial(eci, re)) return traj_fail(A, s, traj, kRebaseFailed);
+    for (int i = 0; i < 6; ++i) s.cur[i] = re[i];
+    s.ct0 = ev;
+    s.side = br.new_side;
+    double rb[6], terr;
+    baseline_state(baseline_new(s.cur), 0.0, rb);
+    if (!ecl_outward(dist3(eci, rb), &terr)) return traj_fail(A, s, traj, kEclGeometry);
+    if (terr > kEclMaxSepKm) return traj_fail(A, s, traj, kEclBracket);
+    E.have_root = 1;
+    E.root_t = ev;
+    E.root_err = terr;
+    s.phase = kNeedSegment;
+}
+
+// The current leg reached its end without a crossing.
+static __device__ __noinline__ void ecl_leg_done(const PropArgs& A, TrajState& s, EclState& E, int64_t traj) {
+    if (E.leg == kLegMain || E.leg == kLegRefine) {
+        // complete_non_eclipse_segment (2372-2583)
+        if (E.leg == kLegMain && A.ctrl.h_max > kEclHcarryMinDtMax && E.fch > 0.0) s.hcarry = E.fch;
+        if (s.seg_tf == s.tf) {
+            traj_finish_with(A, s, traj, s.y);
+            return;
+        }
+        double re[6];
+        if (!ecl_rebase(s.cur, s.ct0, s.y, s.seg_tf, re)) return traj_fail(A, s, traj, kRebaseFailed);
+        for (int i = 0; i < 6; ++i) s.cur[i] = re[i];
+        s.ct0 = s.seg_tf;
+        E.have_root = 0;
+        s.phase = kNeedSegment;
+        return;
+    }
+    if (E.leg == kLegProof) {
+        // proven_old_side_delta (2028-2048), then the window leg
+        const Baseline bb = baseline_new(s.cur);
+        if (!ecl_envelope(bb, s.ct0, s.y, s.t)) return traj_fail(A, s, traj, kEclEnvelope);
+        const EclGeo G{&A.force, s.jd0};
+        int ps;
+        double pm;
+        if (int32_t e = ecl_side_at(G, bb, s.ct0, s.y, s.t, &ps, &pm)) return traj_fail(A, s, traj, e);
+        if (ps != E.br_old) return traj_fail(A, s, traj, kEclBracket);
+        double y0[6];
+        for (int i = 0; i < 6; ++i) y0[i] = s.y[i];
+        ecl_window_start(A, s, E, traj, y0);
+        return;
+    }
+    traj_fail(A, s, traj, kEclBracket);  // a window leg without its crossing
+}
+
+// Accepted step of an SRP row: the handler's checks and scan, then samples,
+// the carried first stage, the PI controller and the leg's end.
+template <int M>
+__device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+                                        const double* dy_prev, const double* dy_next, double en) {
+    using T = Tab<M>;
+    const CtrlParams& C = A.ctrl;
+    EclState& E = A.ecl[traj];
+    double tn;
+    if (s.flags & kLands) {
+        tn = s.seg_tf;
+    } else {
+        const double ky = s.hs - s.t_comp;
+        const double nx = s.t + ky;
+        s.t_comp = (nx - s.t) - ky;
+        tn = nx;
+    }
+    if (!isfinite(tn)) return traj_fail(A, s, traj, kNonFinite);
+    ++s.seg_steps;
+    ++s.steps;
+    s.rejects = 0;
+    const EclGeo G{&A.force, s.jd0};
+    bool found = false;
+    EclBracket br;
+    if (int32_t e = ecl_on_step(G, baseline_new(s.cur), s.ct0, s.side, E, s.t, s.y, dy_prev, tn, ynext, dy_next,
+                                &found, &br))
+        return traj_fail(A, s, traj, e);
+    const bool keep = !found || E.leg == kLegWindow;
+    if (keep && sampled_mode(A)) emit_samples(A, s, traj, tn, ynext, dy_prev, dy_next);
+    if (keep && A.force.ground_check) {
+        double bs[6];
+        baseline_state(baseline_new(s.cur), tn - s.ct0, bs);
+        const double alt = geodetic_altitude_km(bs[0] + ynext[0], bs[1] + ynext[1], bs[2] + ynext[2],
+                                                A.force.earth_radius);
+        if (!(alt >= kGroundAltitudeKm)) return traj_fail(A, s, traj, kGround);
+    }
+    if (found) {
+        ecl_crossing(A, s, E, traj, br, tn, ynext);
+        return;
+    }
+    for (int i = 0; i < 6; ++i) s.k1c[i] = dy_next[i];
+    s.flags |= kHaveK1;
+    const double ah = fabs(s.hs);
+    s.t = tn;
+    for (int i = 0; i < 6; ++i) s.y[i] = ynext[i];
+    // pi_controller_accept! (solver.rs:445-503), absolute control
+    const double order = (double)T::ORDER_ERR + 1.0;
+    const double eff = en > 0.0 ? en : C.eps * 0.1;
+    const bool have_prev = (s.flags & kHavePrev) && s.err_prev > 0.0;
+    const double factor = have_prev ? 0.9 * pow(C.eps / eff, 0.7 / order) * pow(s.err_prev / C.eps, 0.4 / order)
+                                    : 0.9 * pow(C.eps / eff, 1.0 / order);
+    const double mgb = fmin(1.0 + 4.0 * (5.0 / order), 5.0);
+    s.h = clampd(ah * clampd(factor, 0.2, (s.flags & kJustRej) ? fmin(mgb, 2.0) : mgb), C.h_min, s.lhmax);
+    E.fch = s.h;
+    s.err_prev = en;
+    s.flags = (s.flags | kHavePrev) & ~kJustRej;
+    if (s.t == s.seg_tf) ecl_leg_done(A, s, E, traj);
 }
 
 }  // namespace bqp

@@ -36,7 +36,7 @@ extern "C" {
 #define BQP_E_ARG (-1)         /* invalid argument */
 #define BQP_E_CUDA (-2)        /* CUDA runtime error or no device */
 #define BQP_E_COEFF (-3)       /* gravity coefficient text rejected */
-#define BQP_E_UNSUPPORTED (-4) /* option outside this build (e.g. SRP) */
+#define BQP_E_UNSUPPORTED (-4) /* option outside this build */
 #define BQP_E_NOMEM (-5)
 
 /* per-trajectory status (IntegrationStatus, odesolve/solver.rs:64-95;
@@ -53,10 +53,17 @@ extern "C" {
 #define BQP_ST_RESTART_BUDGET 8
 #define BQP_ST_GROUND 9
 #define BQP_ST_WATCHDOG 10
+/* binary-eclipse SRP coordinator failures (EclipseError, lightyear_odeint_rs/src/eclipse.rs) */
+#define BQP_ST_ECLIPSE_ENVELOPE 11     /* state outside radius 6000-50000 km, speed <= 20 km/s */
+#define BQP_ST_ECLIPSE_CHATTER 12      /* side changed where a leg held it, or a root out of order */
+#define BQP_ST_ECLIPSE_BRACKET 13      /* a replay or proof leg failed to confirm the crossing */
+#define BQP_ST_ECLIPSE_NON_PROGRESS 14 /* a bracket or window that cannot shrink */
+#define BQP_ST_ECLIPSE_GEOMETRY 15     /* non-finite geometry or a Sun outside the catalogue */
+#define BQP_ST_ECLIPSE_SPLIT_LIMIT 16  /* more than 4096 roots, bisections or iterations */
 
 /* force flags (ForceFlags, lightyear_odeint_rs/src/types.rs:266-286) */
 #define BQP_FORCE_DRAG 1
-#define BQP_FORCE_SRP 2 /* not built: rejected with BQP_E_UNSUPPORTED */
+#define BQP_FORCE_SRP 2 /* solar radiation pressure with binary eclipse (cr, p_sun below) */
 #define BQP_FORCE_SUN 4
 #define BQP_FORCE_MOON 8
 
@@ -106,8 +113,16 @@ typedef struct bqp_force_config {
     double surrogate_check;    /* surrogate only: at each step's first stage the whole exact field
                                   is evaluated too; a row whose surrogate field misses it by more
                                   than this fraction of the whole field's magnitude (central term
-                                  included; e.g. 1e-3) takes the exact field for the whole step.  0: no check (no counterpart in the
-                                  reference) */
+                                  included; e.g. 1e-3) takes the exact field for the whole step.
+                                  0: no check (no counterpart in the reference) */
+    double cr;                 /* SRP reflectivity coefficient (Python cr, default 1.3) */
+    double p_sun;              /* solar radiation pressure at 1 AU, N/m^2 (ForceConfig p_sun 4.56e-6).
+                                  SRP acts on rows with BQP_FORCE_SRP and cr, p_sun, A/m all > 0; such
+                                  rows run the reference's binary-eclipse coordinator
+                                  (eclipse_coordinator.rs, events off): legs that hold the shadow side
+                                  fixed, a crossing scan of every accepted step, a replay of the step
+                                  that crossed and a committed root where the side flips.  Absolute
+                                  error control and the dopri5 / dop853 / vern7 / vern9 steppers only. */
 } bqp_force_config;
 
 /* propagation engines */

@@ -1,0 +1,143 @@
+"""Solar radiation pressure with binary eclipse on the GPU (both engines),
+through the C ABI, against the oracle's restatement of the reference's
+eclipse coordinator (lightyear_odeint_rs/src/eclipse_coordinator.rs,
+events off).
+
+Both sides run the same legs: main legs that hold the shadow side, a replay
+of each step whose Hermite path crosses the shadow cylinder with steps of at
+most 10 s, an old-side proof leg, a window leg that commits the root, and a
+rebase with the side flipped.  Tolerance as for the other adaptive arcs:
+each row within 2 x 10 eps per step of the oracle's final position, and step
+counts within 5 %."""
+import numpy as np
+import pytest
+
+from bqp_b200 import _native as N
+from bqp_b200 import api, workloads
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+EPOCH = workloads.EPOCH_JD
+ENGINES = ["pipeline", "persistent"]
+FLAGS = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON
+
+
+def ctx_srp(text, order, method="dop853", eps=1e-10, engine="pipeline", cr=1.3, am=0.02, srp=True):
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.force_flags = FLAGS | (N.FORCE_SRP if srp else 0)
+    cfg.method = N.METHODS[method]
+    cfg.eps = eps
+    cfg.engine = N.ENGINES[engine]
+    cfg.cr = cr
+    cfg.atm_model = 7
+    cfg.am_ratio = am
+    return N.Context(text, cfg)
+
+
+def oracle_srp(text, order, cr=1.3):
+    F = O.Force(text, order, drag=True, sun=True, moon=True, atm_model=7)
+    F.set_srp(True, cr)
+    return F
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("method", ["dop853", "vern7"])
+def test_srp_final_matches_oracle(engine, method):
+    order, eps, tf, n = 20, 1e-10, 4 * 3600.0, 32
+    text = workloads.synthetic_field(order)
+    states = workloads.leo_states(n, seed=71)
+    bal = workloads.leo_ballistics(n, seed=71)
+    equ, _ = N.eci_to_equinoctial(states)
+    got, st, steps, evals = ctx_srp(text, order, method, eps, engine).propagate_final(states, EPOCH, tf, ballistic=bal)
+    d, _, rst, rsteps, _, _ = O.propagate_srp_batch(oracle_srp(text, order), O.ctrl(method, eps=eps), equ, EPOCH,
+                                                    tf, bal)
+    assert (st == 0).all() and (rst == 0).all(), (st, rst)
+    plain, pst, _, _ = ctx_srp(text, order, method, eps, engine, srp=False).propagate_final(states, EPOCH, tf,
+                                                                                           ballistic=bal)
+    assert (pst == 0).all()
+    moved = 0
+    for i in range(n):
+        ref = O.equinoc2eci(equ[i], tf)[0] + d[i]
+        bound = 2 * max(steps[i], 1) * eps * 10
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= bound, (i, np.linalg.norm(got[i, :3] - ref[:3]))
+        moved += np.linalg.norm(plain[i, :3] - got[i, :3]) > 100 * bound
+    assert moved >= n // 2  # SRP itself is far above the agreement
+    assert np.all(np.abs(steps - rsteps) <= np.maximum(3, 0.05 * rsteps)), (steps, rsteps)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_srp_sampled_matches_oracle(engine):
+    order, eps, tf, n, am = 20, 1e-10, 3 * 3600.0, 16, 0.02
+    text = workloads.synthetic_field(order)
+    states = workloads.leo_states(n, seed=73)
+    equ, _ = N.eci_to_equinoctial(states)
+    grid = np.arange(0.0, tf + 1.0, 300.0)
+    out, st, steps, _ = ctx_srp(text, order, "dop853", eps, engine, am=am).propagate_sampled(
+        states, EPOCH, tf, grid, deltas=True)
+    _, smp, rst, rsteps, _, nw = O.propagate_srp_batch(oracle_srp(text, order), O.ctrl("dop853", eps=eps), equ,
+                                                       EPOCH, tf, (am, 2.2), t_eval=grid)
+    assert (st == 0).all() and (rst == 0).all() and (nw == grid.size).all()
+    for i in range(n):
+        err = np.linalg.norm(out[i, :, :3] - smp[i, :, :3], axis=1)
+        # interior samples are Hermite interpolants of steps that may differ
+        # in the last bits; the final sample is a step end
+        assert err[-1] <= 2 * max(steps[i], 1) * eps * 10, (i, err[-1])
+        assert err.max() <= 1e-6, (i, err.max())
+    assert np.all(np.abs(steps - rsteps) <= np.maximum(3, 0.05 * rsteps))
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_srp_envelope_and_failure_reporting(engine):
+    """A state outside the coordinator's envelope (radius 6000-50000 km) ends
+    with BQP_ST_ECLIPSE_ENVELOPE on both sides; rows with A/m = 0 run
+    without SRP (rhs.rs:31-36)."""
+    order = 8
+    text = workloads.synthetic_field(order)
+    far = api.kep_to_eci(np.array([60000.0, 0.01, 10.0, 0.0, 0.0, 0.0]))
+    leo = workloads.leo_states(2, seed=5)
+    states = np.vstack([far, leo])
+    bal = np.array([[0.02, 2.2], [0.02, 2.2], [0.0, 2.2]])
+    ctx = ctx_srp(text, order, engine=engine)
+    got, st, _, _ = ctx.propagate_final(states, EPOCH, 1800.0, ballistic=bal)
+    equ, _ = N.eci_to_equinoctial(states)
+    d, _, rst, _, _, _ = O.propagate_srp_batch(oracle_srp(text, order), O.ctrl("dop853", eps=1e-10), equ, EPOCH,
+                                               1800.0, bal)
+    assert st[0] == N.ST_ECLIPSE_ENVELOPE and rst[0] == N.ST_ECLIPSE_ENVELOPE
+    assert np.isnan(got[0]).all()
+    assert st[1] == 0 and st[2] == 0 and (rst[1:] == 0).all()
+    plain, _, _, _ = ctx_srp(text, order, engine=engine, srp=False).propagate_final(states[2:], EPOCH, 1800.0,
+                                                                                   ballistic=bal[2:])
+    assert np.abs(plain[0, :3] - got[2, :3]).max() <= 1e-9
+    with pytest.raises(ValueError, match="envelope"):
+        api.propagate_final(far, EPOCH, 600.0, method="dop853")
+    out = api.propagate(far, EPOCH, 600.0, method="dop853")
+    assert not out["completed"] and out["terminal_event"] == "eclipse_envelope" and out["times_s"].size == 0
+
+
+def test_python_defaults_with_srp_match_oracle():
+    """api.propagate with every reference default, SRP included (DIR-R6 at
+    degree 5, JB2008 atm_model 7, Sun/Moon, SRP with cr 1.3, Vern7 at tol
+    1e-8, dt_max 300 s), against the oracle's coordinator on a 300 s grid
+    over three hours."""
+    eci = api.kep_to_eci(np.array([6778.137, 0.001, 51.6, 30.0, 40.0, 50.0]))
+    grid = np.arange(0.0, 3 * 3600.0 + 1.0, 300.0)
+    out = api.propagate(eci, EPOCH, grid[-1], times_s=grid)
+    assert out["completed"] and np.array_equal(out["times_s"], grid), out["terminal_event"]
+    F = O.Force(api._DEFAULT_FIELD.read_text(), 5, drag=True, sun=True, moon=True, atm_model=7)
+    F.set_srp(True, 1.3)
+    equ, rc = O.eci2equinoc(eci)
+    assert rc == 0
+    _, smp, st, steps, _, nw = O.propagate_srp_batch(F, O.ctrl("vern7", eps=1e-8, dt_max=300.0), equ[None], EPOCH,
+                                                     grid[-1], (0.01, 2.2), t_eval=grid)
+    assert st[0] == 0 and nw[0] == grid.size
+    ref = np.array([O.equinoc2eci(equ, t)[0] for t in grid]) + smp[0]
+    err = np.linalg.norm(out["states_eci"][:, :3] - ref[:, :3], axis=1)
+    assert err[-1] <= 2 * 10 * max(out["steps"], steps[0]) * 1e-8, (err[-1], out["steps"])
+    assert err.max() <= 2e-5, err
+    assert abs(out["steps"] - steps[0]) <= max(3, 0.05 * steps[0])
+    plain = api.propagate(eci, EPOCH, grid[-1], times_s=grid, srp=False)
+    assert np.linalg.norm(plain["states_eci"][-1, :3] - out["states_eci"][-1, :3]) > 100 * err[-1]
+    fin = api.propagate_final(eci, EPOCH, grid[-1])
+    assert np.linalg.norm(fin[:3] - out["states_eci"][-1, :3]) <= 2 * 10 * out["steps"] * 1e-8

@@ -32,8 +32,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_config_struct_matches_header_layout():
     # the ctypes mirror must have the C struct's size (4*6 + 8*10 + 8*9 + 8*3 + 4*7,
-    # padded to the 8-byte alignment of its doubles, + 8 for surrogate_check)
-    assert C.sizeof(N.ForceConfig) == 24 + 80 + 72 + 24 + 32 + 8
+    # padded to the 8-byte alignment of its doubles, + 8 for surrogate_check, + 16 for cr and p_sun)
+    assert C.sizeof(N.ForceConfig) == 24 + 80 + 72 + 24 + 32 + 8 + 16
     cfg = N.default_config()
     assert cfg.order == 5 and cfg.eps == 1e-8 and cfg.dt_max == 300.0 and cfg.max_steps == 500000
     assert list(cfg.jb_drivers)[:8] == [150.0] * 8
@@ -91,17 +91,32 @@ def test_python_argument_validation_mirrors_binding():
     with pytest.raises(ValueError, match="not built"):
         api.propagate(eci, 2460310.5, 600.0, srp=False, method="tsit5")
     with pytest.raises(ValueError, match="srp"):
-        api.propagate(eci, 2460310.5, 600.0, method="dop853")
+        api.propagate(eci, 2460310.5, 600.0, method="dopri5")
+    with pytest.raises(ValueError, match="srp"):
+        api.force_config(method="dop853", rtol=1e-9, atol=1e-9)
     with pytest.raises(ValueError, match="atm_model"):
         api.propagate(eci, 2460310.5, 600.0, srp=False, method="dop853", atm_model=2)
 
 
 def test_ctx_config_validation_happens_before_device_use():
+    # SRP's coordinator runs with absolute control and the RK tableaus only
     cfg = N.default_config()
     cfg.force_flags |= N.FORCE_SRP
+    cfg.method = N.METHODS["dopri5"]
     with pytest.raises(N.NativeError) as e:
         N.Context("2 0 -4.8e-4 0", cfg)
     assert e.value.code == N.E_UNSUPPORTED
+    cfg = N.default_config()
+    cfg.force_flags |= N.FORCE_SRP
+    cfg.error_control = 1
+    with pytest.raises(N.NativeError) as e:
+        N.Context("2 0 -4.8e-4 0", cfg)
+    assert e.value.code == N.E_UNSUPPORTED
+    cfg = N.default_config()
+    cfg.cr = -1.0
+    with pytest.raises(N.NativeError) as e:
+        N.Context("2 0 -4.8e-4 0", cfg)
+    assert e.value.code == N.E_ARG
     cfg = N.default_config()
     cfg.order = 129
     with pytest.raises(N.NativeError) as e:
