@@ -34,7 +34,9 @@ by the device per trajectory.
 
 ``--impl reference`` times that CPU implementation alone (rank 0) on the same
 workload and prints its line.  ``--atm-model 7`` measures the reference's
-default (fitted) JB2008 profile instead of the exact model.
+default (fitted) JB2008 profile instead of the exact model; ``--srp`` adds
+solar radiation pressure through the binary-eclipse coordinator (cr 1.3) on
+both arms.
 """
 from __future__ import annotations
 
@@ -98,6 +100,8 @@ def parse(argv=None):
     ap.add_argument("--eps", type=float, default=EPS, help="absolute tolerance, km")
     ap.add_argument("--atm-model", type=int, default=4, choices=[4, 5, 6, 7],
                     help="JB2008 profile (4 exact: the metric's workload; 7 the reference's Python default)")
+    ap.add_argument("--srp", action="store_true",
+                    help="solar radiation pressure with binary eclipse (cr 1.3) on every row, both arms")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the forms block (split precision and other steppers against plain FP64)")
     ap.add_argument("--forms-rows", type=int, default=512, help="rows of the 7-day accuracy runs of the forms")
@@ -172,7 +176,7 @@ def make_workload(n: int, seed: int = 0):
 
 
 def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp32=False, method="dop853",
-                eps=EPS, atm_model=4):
+                eps=EPS, atm_model=4, srp=False):
     from bqp_b200 import _native as N
 
     cfg = N.default_config()
@@ -181,7 +185,8 @@ def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp3
     cfg.engine = N.ENGINES[engine]
     cfg.gravity_threads = gravity_threads
     cfg.order = ORDER
-    cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON
+    cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON | (N.FORCE_SRP if srp else 0)
+    cfg.cr = 1.3
     cfg.atm_model = atm_model
     cfg.method = N.METHODS[method]
     cfg.error_control = 0
@@ -196,15 +201,16 @@ def make_config(engine="pipeline", gravity_threads=256, split_degree=0, drag_fp3
 def bench_config(args) -> dict:
     """The workload's description, the same dict on both arms (the reference
     arm's bounded sample is reported beside it, in its own key)."""
-    return {"workload": f"{args.n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon, "
+    srp = " + SRP with binary eclipse" if args.srp else ""
+    return {"workload": f"{args.n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon{srp}, "
                         f"{args.method.upper()} eps {args.eps:g}, {args.segment:g} s of the arc per step",
             "form": form_name(args), "order": ORDER, "trajectories_per_gpu": args.n, "segment_s": args.segment,
-            "method": args.method, "eps_km": args.eps, "atm_model": args.atm_model,
+            "method": args.method, "eps_km": args.eps, "atm_model": args.atm_model, "srp": bool(args.srp),
             "l2": "256 MiB write between timed steps"}
 
 
 def cpu_reference(sample: int, threads: int, segments: int = 1, method: str = "dop853", eps: float = EPS,
-                  segment_s: float = SEGMENT_S, atm_model: int = 4):
+                  segment_s: float = SEGMENT_S, atm_model: int = 4, srp: bool = False):
     """Time the CPU oracle (restatement of the reference path) on the first
     `sample` trajectories of the workload for `segments` segments, all
     threads.  Only the oracle runs here: the elements come from its own
@@ -216,8 +222,14 @@ def cpu_reference(sample: int, threads: int, segments: int = 1, method: str = "d
     equ = np.array([O.eci2equinoc(s)[0] for s in states])
     F = O.Force(text, ORDER, drag=True, sun=True, moon=True, drivers=DRIVERS, atm_model=atm_model)
     ctl = O.ctrl(method, eps=eps, dt_max=300.0)
+    if srp:
+        F.set_srp(True, 1.3)
     t0 = time.perf_counter()
-    _, st, steps, evals = O.propagate_final_batch(F, ctl, equ, epoch, segment_s * segments, bal, threads=threads)
+    if srp:
+        _, _, st, steps, evals, _ = O.propagate_srp_batch(F, ctl, equ, epoch, segment_s * segments, bal,
+                                                          threads=threads)
+    else:
+        _, st, steps, evals = O.propagate_final_batch(F, ctl, equ, epoch, segment_s * segments, bal, threads=threads)
     dt = time.perf_counter() - t0
     return float(evals.sum()) / dt, dt, int(evals.sum()), int((st == 0).sum())
 
@@ -230,7 +242,7 @@ def run_reference(args):
     evals_s = []
     for i in range(args.warmup + args.steps):
         v, dt, ev, ok = cpu_reference(args.cpu_sample, threads, method=args.method, eps=args.eps,
-                                      segment_s=args.segment, atm_model=args.atm_model)
+                                      segment_s=args.segment, atm_model=args.atm_model, srp=args.srp)
         if i >= args.warmup:
             evals_s.append((v, dt))
     value = statistics.median(v for v, _ in evals_s)
@@ -439,7 +451,7 @@ def run_ours(args):
 
     text, states, bal, epoch = make_workload(args.n, seed=rank)
     cfg = make_config(args.engine, args.gravity_threads, args.split_degree, args.drag_fp32, args.method, args.eps,
-                      args.atm_model)
+                      args.atm_model, args.srp)
     ctx = N.Context(text, cfg)
     seg = args.segment
     stream = torch.cuda.Stream(device=dev)
@@ -576,7 +588,7 @@ def run_ours(args):
         if not args.no_cpu and world >= 1:
             threads = os.cpu_count() or 1
             v, dt, ev, ok = cpu_reference(args.cpu_sample, threads, method=args.method, eps=args.eps,
-                                          segment_s=args.segment, atm_model=args.atm_model)
+                                          segment_s=args.segment, atm_model=args.atm_model, srp=args.srp)
             cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{args.cpu_sample} trajectories x one 5400 s segment ({ev} evals, {dt:.1f} s)"}
         line = {
@@ -605,7 +617,8 @@ def run_ours(args):
             "status_ok_fraction": float((status_last == 0).mean()),
         }
         if not args.no_forms and world == 1 and args.segment == SEGMENT_S and args.method == "dop853" \
-                and args.eps == EPS and not args.split_degree and args.engine == "pipeline" and args.atm_model == 4:
+                and args.eps == EPS and not args.split_degree and args.engine == "pipeline" and args.atm_model == 4 \
+                and not args.srp:
             plain = {"force_evals_per_s": value, "trajectory_days_per_s": line["trajectory_days_per_s"]}
             line["forms"] = run_forms(args, text, states, bal, epoch, dev, plain)
         print(json.dumps(line), flush=True)

@@ -141,3 +141,23 @@ def test_python_defaults_with_srp_match_oracle():
     assert np.linalg.norm(plain["states_eci"][-1, :3] - out["states_eci"][-1, :3]) > 100 * err[-1]
     fin = api.propagate_final(eci, EPOCH, grid[-1])
     assert np.linalg.norm(fin[:3] - out["states_eci"][-1, :3]) <= 2 * 10 * out["steps"] * 1e-8
+
+
+def test_reference_smoke_sequence_with_every_default():
+    """The propagation steps of dust_transfer/tests_smoke.py as written there:
+    every keyword at the reference's default (srp=True, method vern7,
+    atm_model 7) except where the script itself sets one."""
+    epoch = 2460310.5
+    kep = np.array([7178.137, 0.01, 97.4, 125.0, 210.0, 180.0])
+    eci = api.kep_to_eci(kep)
+    assert np.allclose(kep, api.eci_to_kep(eci), rtol=1e-6, atol=1e-6)
+    out = api.propagate(eci, epoch, tof_s=600.0, gravity_order=1, drag=False, srp=False, sun=False, moon=False)
+    assert out["completed"], out
+    assert abs(np.linalg.norm(out["states_eci"][-1][:3]) - np.linalg.norm(eci[:3])) < 200.0
+    full = api.propagate(eci, epoch, tof_s=3600.0, times_s=np.arange(600.0, 3601.0, 600.0))
+    assert full["completed"] and np.isfinite(full["states_eci"]).all(), full["terminal_event"]
+    assert full["states_eci"].shape == (7, 6)
+    fs = api.propagate_final(eci, epoch, tof_s=3600.0)
+    assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3, "final vs sampled disagree"
+    with pytest.raises(ValueError):
+        api.propagate_final(api.kep_to_eci([6600.0, 0.05, 30.0, 0.0, 0.0, 0.0]), epoch, 6000.0, srp=False)
