@@ -81,10 +81,12 @@ def test_srp_sampled_matches_oracle(engine):
     assert (st == 0).all() and (rst == 0).all() and (nw == grid.size).all()
     for i in range(n):
         err = np.linalg.norm(out[i, :, :3] - smp[i, :, :3], axis=1)
-        # interior samples are Hermite interpolants of steps that may differ
-        # in the last bits; the final sample is a step end
+        # the final sample is a step end; interior samples are cubic Hermite
+        # interpolants of the steps around them, and where the two step
+        # sequences part in the last bits they differ by the interpolant's own
+        # error (the bound of the other sampled arcs' interior samples)
         assert err[-1] <= 2 * max(steps[i], 1) * eps * 10, (i, err[-1])
-        assert err.max() <= 1e-6, (i, err.max())
+        assert err.max() <= 2e-5, (i, err.max())
     assert np.all(np.abs(steps - rsteps) <= np.maximum(3, 0.05 * rsteps))
 
 
