@@ -472,10 +472,20 @@ def run_ours(args):
     d_epochs = [torch.full((n,), e, device=dev, dtype=torch.float64) for e in epochs]
     torch.cuda.synchronize()
 
+    with torch.cuda.stream(stream):
+        # per row: the first failing step and its status (later steps of a
+        # failed row see its NaN output as invalid input)
+        first_code = torch.zeros(n, device=dev, dtype=torch.int32)
+        first_step = torch.full((n,), -1, device=dev, dtype=torch.int32)
+
     def step(k, src, dst):
         ctx.propagate_final_device(src.data_ptr(), d_epochs[k].data_ptr(), d_tf.data_ptr(), dst.data_ptr(),
                                    d_status.data_ptr(), d_steps.data_ptr(), d_evals.data_ptr(), n=n,
                                    d_ballistic=d_bal.data_ptr())
+        with torch.cuda.stream(stream):
+            new = (first_code == 0) & (d_status != 0)
+            first_code.copy_(torch.where(new, d_status, first_code))
+            first_step.copy_(torch.where(new, torch.full_like(first_step, k), first_step))
 
     # warm-up (also advances the batch)
     src, dst = d_a, d_b
@@ -616,6 +626,11 @@ def run_ours(args):
             "gpu_launches": launches,
             "status_ok_fraction": float((status_last == 0).mean()),
         }
+        fc, fs = first_code.cpu().numpy(), first_step.cpu().numpy()
+        if (fc != 0).any():
+            bad = np.flatnonzero(fc)
+            line["failures"] = {"first_status_counts": {str(c): int((fc == c).sum()) for c in np.unique(fc[bad])},
+                                "rows": [[int(i), int(fs[i]), int(fc[i])] for i in bad[:16]]}
         if not args.no_forms and world == 1 and args.segment == SEGMENT_S and args.method == "dop853" \
                 and args.eps == EPS and not args.split_degree and args.engine == "pipeline" and args.atm_model == 4 \
                 and not args.srp:
