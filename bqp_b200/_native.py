@@ -83,6 +83,7 @@ SIGNATURES = [
     ("bqp_ctx_info_fit", C.c_int, [_vp, _dp]),
     ("bqp_jb_fit_check", C.c_int, [_dp, _dp]),
     ("bqp_jb_density", C.c_int, [C.c_int32, C.c_int32, C.c_int64, _dp, _dp]),
+    ("bqp_ecl_scan_check", C.c_int, [_vp, C.c_int64, _dp, C.c_int32, _dp]),
     ("bqp_utc_jd", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_ctx_set_jb_drivers", C.c_int, [_vp, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_double,
                                          C.c_double]),
@@ -422,6 +423,14 @@ class Context:
                                                float(t0), _vp(d_tf), _vp(d_ballistic) if d_ballistic else None,
                                                _vp(d_out), _vp(d_status), _vp(d_steps) if d_steps else None,
                                                _vp(d_evals) if d_evals else None))
+
+    def ecl_scan(self, paths, warp=False):
+        """The eclipse crossing scan on Hermite paths [n][16] (see
+        bqp_ecl_scan_check): [n][7] status, found, sides, t_old, t_new, bound."""
+        p = f64(paths).reshape(-1, 16)
+        out = np.empty((p.shape[0], 7))
+        check(lib().bqp_ecl_scan_check(self._h, p.shape[0], dptr(p), int(bool(warp)), dptr(out)))
+        return out
 
     def gravity_device(self, n, d_pos, d_acc, d_status=None):
         check(lib().bqp_gravity_eval_device(self._h, int(n), _vp(d_pos), _vp(d_acc),

@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbqp_b200.so"
-SOURCES = ["propagate.cu", "pipeline.cu", "sigma.cu", "mlp.cu", "surrogate.cu", "space_weather.cu", "ephemeris.cu",
+SOURCES = ["propagate.cu", "pipeline.cu", "eclipse.cu", "sigma.cu", "mlp.cu", "surrogate.cu", "space_weather.cu", "ephemeris.cu",
            "bqp_api.cu"]
 HEADERS = ["kernels.cuh", "gravity.cuh", "gravity_cta.cuh", "jb2008.cuh", "physics.cuh", "launch.h", "rk_tableaus.h",
            "traj.cuh", "eclipse.cuh", "tc_gemm.cuh", "space_weather.h", "ephemeris.h", "surrogate.h"]

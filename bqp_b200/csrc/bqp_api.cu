@@ -1163,6 +1163,24 @@ int bqp_jb_density(int32_t model, int32_t fp32, int64_t n, const double* in, dou
     return 0;
 }
 
+int bqp_ecl_scan_check(bqp_ctx* ctx, int64_t n, const double* paths, int32_t warp, double* out) {
+    if (!ctx || n < 0 || (n > 0 && (!paths || !out))) return fail(BQP_E_ARG, "bad arguments");
+    if (n == 0) return 0;
+    if (int rc = set_device(ctx)) return rc;
+    double *d_in = nullptr, *d_out = nullptr;
+    cudaError_t e = cudaMalloc(&d_in, (size_t)n * 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, (size_t)n * 7 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_in, paths, (size_t)n * 16 * sizeof(double), cudaMemcpyHostToDevice,
+                                              ctx->stream);
+    if (e == cudaSuccess) e = launch_ecl_scan(force_params(ctx), n, d_in, d_out, warp, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, (size_t)n * 7 * sizeof(double), cudaMemcpyDeviceToHost,
+                                              ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "eclipse scan check");
+}
+
 int bqp_ctx_set_jb_drivers(bqp_ctx* ctx, const char* solfsmy, int64_t solfsmy_len, const char* dtcfile,
                            int64_t dtcfile_len, double jd_lo, double jd_hi) {
     if (!ctx) return fail(BQP_E_ARG, "null ctx");

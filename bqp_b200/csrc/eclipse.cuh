@@ -326,45 +326,268 @@ static __device__ __noinline__ int32_t ecl_first_crossing(const EclGeo& G, const
 }
 
 // CoordinatedEventHandler::on_step (eclipse_coordinator.rs:720-934), events
-// off: checks the accepted step [t0, t1] of a leg on side `fixed` (deltas y,
-// derivatives d against baseline `base` from bt0), then scans it.
-static __device__ __noinline__ int32_t ecl_on_step(const EclGeo& G, const Baseline& base, double bt0, int fixed,
-                                            const EclState& E, double t0, const double* y0, const double* d0,
-                                            double t1, const double* y1, const double* d1, bool* found,
-                                            EclBracket* br) {
-    *found = false;
+// off, before its scan: checks the accepted step [t0, t1] of a leg on side
+// `fixed` (deltas y, derivatives d against baseline `base` from bt0), builds
+// the step's Hermite path and the instant the scan starts from.
+static __device__ __noinline__ int32_t ecl_step_pre(const EclGeo& G, const Baseline& base, double bt0, int fixed,
+                                             const EclState& E, double t0, const double* y0, const double* d0,
+                                             double t1, const double* y1, const double* d1, EclPath* H,
+                                             double* from) {
     if (!ecl_envelope(base, bt0, y0, t0) || !ecl_envelope(base, bt0, y1, t1)) return kEclEnvelope;
-    EclPath H;
     double b0[6], b1[6];
     baseline_state(base, t0 - bt0, b0);
     baseline_state(base, t1 - bt0, b1);
     for (int i = 0; i < 3; ++i) {
-        H.p0[i] = b0[i] + y0[i];
-        H.v0[i] = b0[3 + i] + d0[i];
-        H.p1[i] = b1[i] + y1[i];
-        H.v1[i] = b1[3 + i] + d1[i];
+        H->p0[i] = b0[i] + y0[i];
+        H->v0[i] = b0[3 + i] + d0[i];
+        H->p1[i] = b1[i] + y1[i];
+        H->v1[i] = b1[3 + i] + d1[i];
     }
-    H.t0 = t0;
-    H.t1 = t1;
+    H->t0 = t0;
+    H->t1 = t1;
     EclPoint q;
-    if (int32_t e = ecl_point(G, H, t0, &q)) return e;
+    if (int32_t e = ecl_point(G, *H, t0, &q)) return e;
     const bool certified = E.have_root && E.root_t == t0;
     if (q.side != fixed && !certified) return kEclChatter;
-    double from = t0;
+    *from = t0;
     if (certified) {
         // inside the committed root's uncertainty the side is not resolvable:
         // scan from the deepest instant the root bound covers, where it must
         // read the committed side decisively
         double edge, dm;
         if (int32_t e = G.deepest(t0, t1, kEclRootUncKm, &edge)) return e;
-        if (int32_t e = ecl_point(G, H, edge, &q)) return e;
+        if (int32_t e = ecl_point(G, *H, edge, &q)) return e;
         if (int32_t e = ecl_decisive_margin(E.root_err, &dm)) return e;
         if (q.side != fixed || q.margin <= dm) return kEclChatter;
-        from = edge;
+        *from = edge;
     }
-    if (int32_t e = ecl_first_crossing(G, H, from, t1, found, br)) return e;
-    if (*found && br->old_side != fixed) return kEclChatter;
     return kOk;
+}
+
+// ------------------------------------------------ warp-cooperative scan
+// The same depth-first bisection as ecl_first_crossing, with the points and
+// motion bounds it may need evaluated 32 at a time.  Whenever the walk
+// splits the root of its store, the warp fills the store with that node's
+// whole 5-level subtree: the 31 midpoints (one lane each, every lane
+// descending the binary64 midpoint chain the serial walk would form) and the
+// bounds of the 62 sub-intervals (two per lane).  Every lane then walks the
+// subtree with the serial rules on the shared copy, so decisions, split
+// counts, the stack and the errors reported are the serial walk's; only a
+// split at the subtree's bottom level, or a return to a node of an older
+// store, costs another evaluation round.  A few rows near grazing geometry
+// scan thousands of points per step; serially the whole batch waits for
+// them.
+constexpr int kEclGrid = 32;  // grid positions 0..32 of one store; nodes by heap index 1..63
+
+struct EclWarpStore {
+    double t[kEclGrid + 1], p[kEclGrid + 1][3], v[kEclGrid + 1][3], m[kEclGrid + 1];
+    int32_t side[kEclGrid + 1], pst[kEclGrid + 1];  // point status; kEclBadMid: no representable midpoint
+    double bnd[2 * kEclGrid];
+    int32_t bst[2 * kEclGrid];
+    double st_t[kEclScanDepth], st_inh[kEclScanDepth];  // pending right siblings: end time, parent bound
+    int32_t st_h[kEclScanDepth], st_gen[kEclScanDepth];
+};
+constexpr int32_t kEclBadMid = -1;
+
+__device__ __forceinline__ void ecl_store_point(EclWarpStore& W, int pos, const EclPoint& q) {
+    W.t[pos] = q.t;
+    for (int i = 0; i < 3; ++i) {
+        W.p[pos][i] = q.p[i];
+        W.v[pos][i] = q.v[i];
+    }
+    W.m[pos] = q.margin;
+    W.side[pos] = q.side;
+    W.pst[pos] = kOk;
+}
+
+__device__ __forceinline__ EclPoint ecl_load_point(const EclWarpStore& W, int pos) {
+    EclPoint q;
+    q.t = W.t[pos];
+    for (int i = 0; i < 3; ++i) {
+        q.p[i] = W.p[pos][i];
+        q.v[i] = W.v[pos][i];
+    }
+    q.margin = W.m[pos];
+    q.side = W.side[pos];
+    return q;
+}
+
+// Grid positions [a, b] of node h (heap index, level d = floor(log2 h)).
+__device__ __forceinline__ void ecl_node_span(int h, int* a, int* b) {
+    const int d = 31 - __clz(h);
+    const int w = kEclGrid >> d;
+    *a = (h - (1 << d)) * w;
+    *b = *a + w;
+}
+
+// Fill positions 1..31 and the bounds of nodes 2..63 below the store's root
+// (positions 0 and 32 hold its ends).  All lanes.
+static __device__ __noinline__ void ecl_expand(const EclGeo& G, const EclPath& H, EclWarpStore& W, int lane) {
+    if (lane >= 1) {
+        // the midpoint chain from the root down to this lane's position
+        double lo = W.t[0], hi = W.t[kEclGrid];
+        int plo = 0, phi = kEclGrid;
+        for (;;) {
+            const int pm = (plo + phi) >> 1;
+            const double mid = lo + 0.5 * (hi - lo);
+            if (mid == lo || mid == hi || !isfinite(mid)) {
+                W.pst[lane] = kEclBadMid;
+                break;
+            }
+            if (pm == lane) {
+                EclPoint q;
+                const int32_t e = ecl_point(G, H, mid, &q);
+                ecl_store_point(W, lane, q);
+                W.t[lane] = mid;
+                W.pst[lane] = e;
+                break;
+            }
+            if (lane < pm) {
+                hi = mid;
+                phi = pm;
+            } else {
+                lo = mid;
+                plo = pm;
+            }
+        }
+    }
+    __syncwarp();
+    for (int h = 2 + lane; h < 2 * kEclGrid; h += 32) {
+        int a, b;
+        ecl_node_span(h, &a, &b);
+        if (W.pst[a] == kOk && W.pst[b] == kOk) {
+            const EclPoint qa = ecl_load_point(W, a), qb = ecl_load_point(W, b);
+            W.bst[h] = ecl_motion_bound(G, qa, qb, &W.bnd[h]);
+        } else {
+            W.bst[h] = kEclBadMid;  // under a point the walk never passes
+        }
+    }
+    __syncwarp();
+}
+
+// Earliest crossing of the path in [t_a, t_b]: every lane of the warp calls
+// it with the same arguments and returns the same result.
+static __device__ __noinline__ int32_t ecl_first_crossing_warp(const EclGeo& G, const EclPath& H, double t_a, double t_b,
+                                                       EclWarpStore& W, bool* found, EclBracket* br) {
+    const int lane = threadIdx.x & 31;
+    *found = false;
+    if (t_a == t_b) return kEclNonProgress;
+    {
+        EclPoint q;
+        int32_t e = kOk;
+        if (lane == 0) e = ecl_point(G, H, t_a, &q);
+        else if (lane == 1) e = ecl_point(G, H, t_b, &q);
+        if (lane < 2) {
+            ecl_store_point(W, lane == 0 ? 0 : kEclGrid, q);
+            W.pst[lane == 0 ? 0 : kEclGrid] = e;
+        }
+        __syncwarp();
+        if (W.pst[0] != kOk) return W.pst[0];
+        if (W.pst[kEclGrid] != kOk) return W.pst[kEclGrid];
+    }
+    int gen = 0, sp = 0, h = 1;
+    bool expanded = false, inherited = false;
+    double inh = 0.0;
+    int64_t splits_left = kEclMaxSplits;
+    for (;;) {
+        int a, b;
+        ecl_node_span(h, &a, &b);
+        const EclPoint L = ecl_load_point(W, a), R = ecl_load_point(W, b);
+        bool resolved = false;
+        const double sep = dist3(L.p, R.p);
+        if (!isfinite(sep)) return kEclGeometry;
+        if (L.side == R.side && inherited && L.margin + R.margin > inh) {
+            resolved = true;
+        } else {
+            double mb;
+            if (h == 1) {
+                if (int32_t e = ecl_motion_bound(G, L, R, &mb)) return e;
+            } else {
+                if (W.bst[h] != kOk) return W.bst[h];
+                mb = W.bnd[h];
+            }
+            if (!(isfinite(mb) && mb >= sep && mb >= 0.0)) return kEclBracket;
+            if (L.side == R.side && L.margin + R.margin > mb) {
+                resolved = true;
+            } else if (mb <= kEclMaxSepKm && L.side != R.side) {
+                br->t_old = L.t;
+                br->t_new = R.t;
+                br->old_side = L.side;
+                br->new_side = R.side;
+                br->bound = mb;
+                *found = true;
+                return kOk;
+            } else {
+                const double mid = L.t + 0.5 * (R.t - L.t);
+                if (mid == L.t || mid == R.t || !isfinite(mid)) {
+                    if (L.side == R.side && mb <= 1.0e-6) resolved = true;
+                    else return kEclNonProgress;
+                } else {
+                    if (splits_left == 0 || sp == kEclScanDepth) return kEclSplitLimit;
+                    --splits_left;
+                    if (b - a == 1) {
+                        // a bottom-level node: it becomes the root of a new store
+                        __syncwarp();
+                        if (lane == 0) {
+                            ecl_store_point(W, 0, L);
+                            ecl_store_point(W, kEclGrid, R);
+                        }
+                        __syncwarp();
+                        ++gen;
+                        h = 1;
+                        a = 0;
+                        b = kEclGrid;
+                        expanded = false;
+                    }
+                    if (h == 1 && !expanded) {
+                        ecl_expand(G, H, W, lane);
+                        expanded = true;
+                    }
+                    if (lane == 0) {
+                        W.st_t[sp] = R.t;
+                        W.st_inh[sp] = mb;
+                        W.st_h[sp] = 2 * h + 1;
+                        W.st_gen[sp] = gen;
+                    }
+                    __syncwarp();
+                    ++sp;
+                    const int pm = (a + b) >> 1;
+                    if (W.pst[pm] != kOk) return W.pst[pm];
+                    h = 2 * h;
+                    inherited = true;
+                    inh = mb;
+                }
+            }
+        }
+        if (resolved) {
+            if (sp == 0) return kOk;
+            --sp;
+            const int ph = W.st_h[sp], pg = W.st_gen[sp];
+            const double pt = W.st_t[sp], pinh = W.st_inh[sp];
+            if (pg == gen) {
+                h = ph;
+            } else {
+                // a right sibling from an older store: a new store rooted at
+                // it, from this node's right end to the sibling's (its point
+                // evaluated again: the same bits)
+                EclPoint q;
+                const int32_t e = ecl_point(G, H, pt, &q);
+                __syncwarp();
+                if (lane == 0) {
+                    ecl_store_point(W, 0, R);
+                    ecl_store_point(W, kEclGrid, q);
+                    W.pst[kEclGrid] = e;
+                }
+                __syncwarp();
+                if (e != kOk) return e;
+                ++gen;
+                h = 1;
+                expanded = false;
+            }
+            inherited = true;
+            inh = pinh;
+        }
+    }
 }
 
 }  // namespace bqp

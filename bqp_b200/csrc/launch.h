@@ -104,6 +104,8 @@ cudaError_t launch_rhs(const double* gtab, int ncells, int use_smem, const Force
                        const double* delta, const double* ballistic, double am0, double cd0,
                        double* out, cudaStream_t st);
 cudaError_t launch_propagate(const PropArgs& A, int method, int threads, int blocks, cudaStream_t st);
+cudaError_t launch_ecl_scan(const ForceParams& fp, int64_t n, const double* paths, double* out, int warp,
+                            cudaStream_t st);
 cudaError_t launch_jb_lookup(const jb::DriverTable& T, const double* jd, int64_t n, double* out, int32_t* ok,
                              cudaStream_t st);
 cudaError_t launch_body_positions(const EphemTable& E, int body, const double* jd, int64_t n, double* out,

@@ -379,23 +379,30 @@ template <int M>
 __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int cur, int dense,
                                                       int timed_out) {
     using T = Tab<M>;
+    // per warp: the store of the cooperative eclipse scan (SRP rows)
+    __shared__ EclWarpStore ecl_ws[kBlock / 32];
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     const int count = P.count[cur];
+    if (slot - lane >= count) return;  // the whole warp is idle
+    const bool active = slot < count;
     bool keep = false;
     int32_t traj = 0;
-    if (slot < count) {
+    TrajState s;
+    bool scan = false;  // an accepted SRP step waiting for its crossing scan
+    EclScanReq req;
+    double tn = 0.0, en = 0.0, ynext[6], k0[6], dyn[6];
+    if (active) {
         traj = P.idx[cur][slot];
-        TrajState s = P.st[traj];
+        s = P.st[traj];
         const int last = dense ? T::S : T::S - 1;
         if (!(last == 1 && P.skip[slot])) finish_stage(P, last, slot);
         // stage derivatives of this attempt
         const int evaluated = T::S - ((s.flags & kHaveK1) ? 1 : 0);
         s.evals += evaluated;
-        double ynext[6], err[6], err3[6];
+        double err[6], err3[6];
         rk_combine<M>(s, [&](int st, int i) { return K(P, st, i)[slot]; }, ynext, err, err3);
-        double k0[6];
         for (int i = 0; i < 6; ++i) k0[i] = K(P, 0, i)[slot];
-        double en;
         int32_t code = -1;
         const int32_t d = attempt_decide<M>(A, s, k0, ynext, err, err3, &en, &code);
         if (P.bad[slot]) {
@@ -403,7 +410,6 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
         } else if (d == kFail) {
             traj_fail(A, s, traj, code);
         } else if (d == kAccept) {
-            double dyn[6];
             const double* dy_next = nullptr;
             if (T::FSAL) {
                 for (int i = 0; i < 6; ++i) dyn[i] = K(P, T::S - 1, i)[slot];
@@ -413,8 +419,46 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
                 dy_next = dyn;
                 ++s.evals;  // counted on accept only, as the reference evaluates it
             }
-            attempt_accept<M>(A, s, traj, ynext, k0, dy_next, en);
+            if (M != kDopri5Compat && (s.flags & kEcl))
+                scan = ecl_accept_pre<M>(A, s, traj, ynext, k0, dyn, &tn, &req);
+            else
+                attempt_accept<M>(A, s, traj, ynext, k0, dy_next, en);
         }
+    }
+    if (A.force.srp) {
+        // the warp scans each waiting row's step together, one row at a time
+        int32_t scan_err = kOk;
+        bool scan_found = false;
+        EclBracket scan_br{};
+        unsigned want = __ballot_sync(0xffffffffu, scan);
+        while (want) {
+            const int leader = __ffs(want) - 1;
+            want &= want - 1;
+            EclPath H;
+            for (int i = 0; i < 3; ++i) {
+                H.p0[i] = __shfl_sync(0xffffffffu, req.H.p0[i], leader);
+                H.v0[i] = __shfl_sync(0xffffffffu, req.H.v0[i], leader);
+                H.p1[i] = __shfl_sync(0xffffffffu, req.H.p1[i], leader);
+                H.v1[i] = __shfl_sync(0xffffffffu, req.H.v1[i], leader);
+            }
+            H.t0 = __shfl_sync(0xffffffffu, req.H.t0, leader);
+            H.t1 = __shfl_sync(0xffffffffu, req.H.t1, leader);
+            const double from = __shfl_sync(0xffffffffu, req.from, leader);
+            const double t1 = __shfl_sync(0xffffffffu, req.t1, leader);
+            const double jd0 = __shfl_sync(0xffffffffu, s.jd0, leader);
+            const EclGeo G{&A.force, jd0};
+            bool found = false;
+            EclBracket br{};
+            const int32_t e = ecl_first_crossing_warp(G, H, from, t1, ecl_ws[threadIdx.x >> 5], &found, &br);
+            if (lane == leader) {
+                scan_err = e;
+                scan_found = found;
+                scan_br = br;
+            }
+        }
+        if (scan) ecl_accept_post<M>(A, s, traj, tn, ynext, k0, dyn, en, scan_err, scan_found, scan_br);
+    }
+    if (active) {
         if (s.phase == kNeedSegment) seg_begin<M>(A, s, traj);
         if (s.phase == kStepping) {
             const int32_t f = attempt_begin<M>(A, s, timed_out != 0);
@@ -423,8 +467,7 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
         }
         P.st[traj] = s;
     }
-    if (slot - threadIdx.x % 32 < count)  // whole warps take part in the ballot
-        append_active(P.idx[cur ^ 1], &P.count[cur ^ 1], traj, keep);
+    append_active(P.idx[cur ^ 1], &P.count[cur ^ 1], traj, keep);  // whole warps take part in the ballot
 }
 
 // Rows still active when the host gives up (wall-clock watchdog).

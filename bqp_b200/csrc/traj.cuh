@@ -799,14 +799,18 @@ static __device__ __noinline__ void ecl_leg_done(const PropArgs& A, TrajState& s
     traj_fail(A, s, traj, kEclBracket);  // a window leg without its crossing
 }
 
-// Accepted step of an SRP row: the handler's checks and scan, then samples,
-// the carried first stage, the PI controller and the leg's end.
+// The scan an accepted SRP step asks for.
+struct EclScanReq {
+    EclPath H;
+    double from, t1;
+};
+
+// Accepted step of an SRP row, up to its crossing scan: the time update and
+// the handler's checks.  False when the row failed (its status is written).
 template <int M>
-__device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
-                                        const double* dy_prev, const double* dy_next, double en) {
-    using T = Tab<M>;
-    const CtrlParams& C = A.ctrl;
-    EclState& E = A.ecl[traj];
+__device__ __noinline__ bool ecl_accept_pre(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+                                            const double* dy_prev, const double* dy_next, double* tn_out,
+                                            EclScanReq* req) {
     double tn;
     if (s.flags & kLands) {
         tn = s.seg_tf;
@@ -816,16 +820,35 @@ __device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t
         s.t_comp = (nx - s.t) - ky;
         tn = nx;
     }
-    if (!isfinite(tn)) return traj_fail(A, s, traj, kNonFinite);
+    if (!isfinite(tn)) {
+        traj_fail(A, s, traj, kNonFinite);
+        return false;
+    }
     ++s.seg_steps;
     ++s.steps;
     s.rejects = 0;
     const EclGeo G{&A.force, s.jd0};
-    bool found = false;
-    EclBracket br;
-    if (int32_t e = ecl_on_step(G, baseline_new(s.cur), s.ct0, s.side, E, s.t, s.y, dy_prev, tn, ynext, dy_next,
-                                &found, &br))
-        return traj_fail(A, s, traj, e);
+    if (int32_t e = ecl_step_pre(G, baseline_new(s.cur), s.ct0, s.side, A.ecl[traj], s.t, s.y, dy_prev, tn, ynext,
+                                 dy_next, &req->H, &req->from)) {
+        traj_fail(A, s, traj, e);
+        return false;
+    }
+    req->t1 = tn;
+    *tn_out = tn;
+    return true;
+}
+
+// The rest of the accepted step after its scan: samples, the carried first
+// stage, the PI controller, a crossing's leg change or the leg's end.
+template <int M>
+__device__ __noinline__ void ecl_accept_post(const PropArgs& A, TrajState& s, int64_t traj, double tn,
+                                             const double* ynext, const double* dy_prev, const double* dy_next,
+                                             double en, int32_t scan_err, bool found, const EclBracket& br) {
+    using T = Tab<M>;
+    const CtrlParams& C = A.ctrl;
+    EclState& E = A.ecl[traj];
+    if (scan_err) return traj_fail(A, s, traj, scan_err);
+    if (found && br.old_side != s.side) return traj_fail(A, s, traj, kEclChatter);
     const bool keep = !found || E.leg == kLegWindow;
     if (keep && sampled_mode(A)) emit_samples(A, s, traj, tn, ynext, dy_prev, dy_next);
     if (keep && A.force.ground_check) {
@@ -856,6 +879,21 @@ __device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t
     s.err_prev = en;
     s.flags = (s.flags | kHavePrev) & ~kJustRej;
     if (s.t == s.seg_tf) ecl_leg_done(A, s, E, traj);
+}
+
+// Accepted step of an SRP row scanned by its own thread (the persistent
+// engine; the stage-synchronous engine scans warp-cooperatively).
+template <int M>
+__device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+                                        const double* dy_prev, const double* dy_next, double en) {
+    double tn;
+    EclScanReq req;
+    if (!ecl_accept_pre<M>(A, s, traj, ynext, dy_prev, dy_next, &tn, &req)) return;
+    const EclGeo G{&A.force, s.jd0};
+    bool found = false;
+    EclBracket br;
+    const int32_t e = ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br);
+    ecl_accept_post<M>(A, s, traj, tn, ynext, dy_prev, dy_next, en, e, found, br);
 }
 
 }  // namespace bqp

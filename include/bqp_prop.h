@@ -180,6 +180,16 @@ int bqp_ctx_profile_read(const bqp_ctx* ctx, double* ms, int64_t* launches);
  * reference, whose quadrature these fits replace. */
 int bqp_jb_fit_check(const double* drivers, double* worst6);
 
+/* Eclipse crossing scan on given cubic Hermite paths, for tests (no
+ * counterpart in the reference; eclipse.rs:341-491 is the scan itself).
+ * paths [n][16]: p0[3], v0[3], p1[3], v1[3] (km, km/s), t0, t1 (s after the
+ * epoch), the scan start (s) and the epoch (JD UTC); the context's Sun
+ * (catalogue or analytic series) and Earth radius.  warp 0 runs the
+ * per-thread walk of the persistent engine, 1 the warp-cooperative walk of
+ * the stage-synchronous engine.  out [n][7]: status (BQP_ST_OK or an
+ * eclipse code), found, old side, new side, t_old, t_new, motion bound. */
+int bqp_ecl_scan_check(bqp_ctx* ctx, int64_t n, const double* paths, int32_t warp, double* out);
+
 /* JB2008 density on the host, by the same function the force kernels run:
  * in[14 i] = UTC MJD, solar declination (rad), hour angle of the satellite
  * from the Sun (rad), geocentric latitude (rad), altitude (m), F10, F10bar,
