@@ -264,8 +264,12 @@ struct EclBracket {
 // until the geometry motion across a bracket is at most kEclMaxSepKm; an
 // interval whose end margins exceed its motion bound holds no crossing.
 // The recursion runs on an explicit stack of right endpoints.
+// `budget` caps the splits this call may take: a walk that needs more
+// returns kEclDefer with nothing decided, for the warp-cooperative walk to
+// redo from the start (the same result, sooner).
+constexpr int32_t kEclDefer = -2;
 static __device__ __noinline__ int32_t ecl_first_crossing(const EclGeo& G, const EclPath& H, double t_a, double t_b,
-                                                   bool* found, EclBracket* br) {
+                                                   bool* found, EclBracket* br, int64_t budget = kEclMaxSplits) {
     *found = false;
     if (t_a == t_b) return kEclNonProgress;
     double st_t[kEclScanDepth], st_b[kEclScanDepth];
@@ -304,6 +308,7 @@ static __device__ __noinline__ int32_t ecl_first_crossing(const EclGeo& G, const
                     else return kEclNonProgress;
                 } else {
                     if (splits_left == 0 || sp == kEclScanDepth) return kEclSplitLimit;
+                    if (kEclMaxSplits - splits_left >= budget) return kEclDefer;
                     --splits_left;
                     st_t[sp] = R.t;
                     st_b[sp] = mb;

@@ -375,6 +375,10 @@ __global__ void __launch_bounds__(kBlock) pl_drag_coarse(ForceParams fp, PipeBuf
 }
 
 // ------------------------------------------------------------------ control
+// Splits a row's own thread may take on its crossing scan before the warp
+// takes it over.
+constexpr int64_t kEclSoloSplits = 16;
+
 template <int M>
 __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int cur, int dense,
                                                       int timed_out) {
@@ -419,9 +423,18 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
                 dy_next = dyn;
                 ++s.evals;  // counted on accept only, as the reference evaluates it
             }
-            if (M != kDopri5Compat && (s.flags & kEcl))
-                scan = ecl_accept_pre<M>(A, s, traj, ynext, k0, dyn, &tn, &req);
-            else
+            if (M != kDopri5Compat && (s.flags & kEcl)) {
+                // most steps are certified free of crossings after a few
+                // splits; the rest go to the warp
+                if (ecl_accept_pre<M>(A, s, traj, ynext, k0, dyn, &tn, &req)) {
+                    const EclGeo G{&A.force, s.jd0};
+                    bool found = false;
+                    EclBracket br{};
+                    const int32_t e = ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br, kEclSoloSplits);
+                    if (e == kEclDefer) scan = true;
+                    else ecl_accept_post<M>(A, s, traj, tn, ynext, k0, dyn, en, e, found, br);
+                }
+            } else
                 attempt_accept<M>(A, s, traj, ynext, k0, dy_next, en);
         }
     }
