@@ -377,7 +377,10 @@ __global__ void __launch_bounds__(kBlock) pl_drag_coarse(ForceParams fp, PipeBuf
 // ------------------------------------------------------------------ control
 // Splits a row's own thread may take on its crossing scan before the warp
 // takes it over.
-constexpr int64_t kEclSoloSplits = 16;
+#ifndef BQP_ECL_SOLO_SPLITS
+#define BQP_ECL_SOLO_SPLITS 16
+#endif
+constexpr int64_t kEclSoloSplits = BQP_ECL_SOLO_SPLITS;
 
 template <int M>
 __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int cur, int dense,
