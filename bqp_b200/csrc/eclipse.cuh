@@ -389,10 +389,20 @@ struct EclWarpStore {
     int32_t side[kEclGrid + 1], pst[kEclGrid + 1];  // point status; kEclBadMid: no representable midpoint
     double bnd[2 * kEclGrid];
     int32_t bst[2 * kEclGrid];
+    int32_t fl[2 * kEclGrid];  // the walk's tests of each node, evaluated with the bounds (kNode*)
     double st_t[kEclScanDepth], st_inh[kEclScanDepth];  // pending right siblings: end time, parent bound
     int32_t st_h[kEclScanDepth], st_gen[kEclScanDepth];
 };
 constexpr int32_t kEclBadMid = -1;
+// Node tests: end points on one side; chord not finite; certified by the
+// parent's bound (how the walk first tries every node below a split);
+// certified by its own bound; bound below the chord or not finite; a bracket
+// (own bound within the resolution, sides differ); bound within 1 mm (the
+// adjacent-instant rule).
+enum : int32_t {
+    kNodeSame = 1, kNodeSepBad = 2, kNodeCertInh = 4, kNodeCertOwn = 8, kNodeBadBound = 16, kNodeFound = 32,
+    kNodeFine = 64
+};
 
 __device__ __forceinline__ void ecl_store_point(EclWarpStore& W, int pos, const EclPoint& q) {
     W.t[pos] = q.t;
@@ -425,9 +435,11 @@ __device__ __forceinline__ void ecl_node_span(int h, int* a, int* b) {
     *b = *a + w;
 }
 
-// Fill positions 1..31 and the bounds of nodes 2..63 below the store's root
-// (positions 0 and 32 hold its ends).  All lanes.
-static __device__ __noinline__ void ecl_expand(const EclGeo& G, const EclPath& H, EclWarpStore& W, int lane) {
+// Fill positions 1..31, and the bounds and tests of nodes 2..63, below the
+// store's root (positions 0 and 32 hold its ends; root_mb is its bound).
+// All lanes.
+static __device__ __noinline__ void ecl_expand(const EclGeo& G, const EclPath& H, EclWarpStore& W, int lane,
+                                               double root_mb) {
     if (lane >= 1) {
         // the midpoint chain from the root down to this lane's position
         double lo = W.t[0], hi = W.t[kEclGrid];
@@ -468,12 +480,89 @@ static __device__ __noinline__ void ecl_expand(const EclGeo& G, const EclPath& H
         }
     }
     __syncwarp();
+    // the walk's tests of every node, each under its parent's bound
+    for (int h = 2 + lane; h < 2 * kEclGrid; h += 32) {
+        int a, b;
+        ecl_node_span(h, &a, &b);
+        int32_t f = 0;
+        if (W.pst[a] == kOk && W.pst[b] == kOk) {
+            const double sep = dist3(W.p[a], W.p[b]);
+            const double msum = W.m[a] + W.m[b];
+            const double inh = h < 4 ? root_mb : W.bnd[h >> 1];
+            const bool same = W.side[a] == W.side[b];
+            if (same) f |= kNodeSame;
+            if (!isfinite(sep)) f |= kNodeSepBad;
+            if (same && msum > inh) f |= kNodeCertInh;
+            if (W.bst[h] == kOk) {
+                const double mb = W.bnd[h];
+                if (!(isfinite(mb) && mb >= sep && mb >= 0.0)) f |= kNodeBadBound;
+                if (same && msum > mb) f |= kNodeCertOwn;
+                if (mb <= kEclMaxSepKm && !same) f |= kNodeFound;
+                if (mb <= 1.0e-6) f |= kNodeFine;
+            }
+        }
+        W.fl[h] = f;
+    }
+    __syncwarp();
+}
+
+// One node's verdict under the serial rules.
+enum : int32_t { kVerdictResolved = 0, kVerdictFound = 1, kVerdictSplit = 2 };
+struct EclNodeTest {
+    int32_t err, verdict;
+    double mb;
+};
+
+// ... from its end points, the bound computed when needed (a store's root)
+__device__ __forceinline__ EclNodeTest ecl_node_test_points(const EclGeo& G, const EclPoint& L, const EclPoint& R,
+                                                            bool inherited, double inh) {
+    const double sep = dist3(L.p, R.p);
+    if (!isfinite(sep)) return {kEclGeometry, 0, 0.0};
+    const bool same = L.side == R.side;
+    if (same && inherited && L.margin + R.margin > inh) return {kOk, kVerdictResolved, 0.0};
+    double mb;
+    if (int32_t e = ecl_motion_bound(G, L, R, &mb)) return {e, 0, 0.0};
+    if (!(isfinite(mb) && mb >= sep && mb >= 0.0)) return {kEclBracket, 0, 0.0};
+    if (same && L.margin + R.margin > mb) return {kOk, kVerdictResolved, mb};
+    if (mb <= kEclMaxSepKm && !same) return {kOk, kVerdictFound, mb};
+    const double mid = L.t + 0.5 * (R.t - L.t);
+    if (mid == L.t || mid == R.t || !isfinite(mid)) {
+        if (same && mb <= 1.0e-6) return {kOk, kVerdictResolved, mb};
+        return {kEclNonProgress, 0, 0.0};
+    }
+    return {kOk, kVerdictSplit, mb};
+}
+
+// ... from the store's precomputed tests (a node below the root, reached
+// through its parent's split)
+__device__ __forceinline__ EclNodeTest ecl_node_test_store(const EclWarpStore& W, int h, int a, int b) {
+    const int32_t f = W.fl[h];
+    if (f & kNodeSepBad) return {kEclGeometry, 0, 0.0};
+    if (f & kNodeCertInh) return {kOk, kVerdictResolved, 0.0};
+    if (W.bst[h] != kOk) return {W.bst[h], 0, 0.0};
+    const double mb = W.bnd[h];
+    if (f & kNodeBadBound) return {kEclBracket, 0, 0.0};
+    if (f & kNodeCertOwn) return {kOk, kVerdictResolved, mb};
+    if (f & kNodeFound) return {kOk, kVerdictFound, mb};
+    bool no_mid;
+    if (b - a > 1) {
+        no_mid = W.pst[(a + b) >> 1] == kEclBadMid;
+    } else {
+        const double mid = W.t[a] + 0.5 * (W.t[b] - W.t[a]);
+        no_mid = mid == W.t[a] || mid == W.t[b] || !isfinite(mid);
+    }
+    if (no_mid) {
+        if ((f & kNodeSame) && (f & kNodeFine)) return {kOk, kVerdictResolved, mb};
+        return {kEclNonProgress, 0, 0.0};
+    }
+    return {kOk, kVerdictSplit, mb};
 }
 
 // Earliest crossing of the path in [t_a, t_b]: every lane of the warp calls
 // it with the same arguments and returns the same result.
-static __device__ __noinline__ int32_t ecl_first_crossing_warp(const EclGeo& G, const EclPath& H, double t_a, double t_b,
-                                                       EclWarpStore& W, bool* found, EclBracket* br) {
+static __device__ __noinline__ int32_t ecl_first_crossing_warp(const EclGeo& G, const EclPath& H, double t_a,
+                                                               double t_b, EclWarpStore& W, bool* found,
+                                                               EclBracket* br) {
     const int lane = threadIdx.x & 31;
     *found = false;
     if (t_a == t_b) return kEclNonProgress;
@@ -491,107 +580,88 @@ static __device__ __noinline__ int32_t ecl_first_crossing_warp(const EclGeo& G, 
         if (W.pst[kEclGrid] != kOk) return W.pst[kEclGrid];
     }
     int gen = 0, sp = 0, h = 1;
-    bool expanded = false, inherited = false;
+    bool inherited = false;
     double inh = 0.0;
     int64_t splits_left = kEclMaxSplits;
     for (;;) {
         int a, b;
         ecl_node_span(h, &a, &b);
-        const EclPoint L = ecl_load_point(W, a), R = ecl_load_point(W, b);
-        bool resolved = false;
-        const double sep = dist3(L.p, R.p);
-        if (!isfinite(sep)) return kEclGeometry;
-        if (L.side == R.side && inherited && L.margin + R.margin > inh) {
-            resolved = true;
-        } else {
-            double mb;
-            if (h == 1) {
-                if (int32_t e = ecl_motion_bound(G, L, R, &mb)) return e;
-            } else {
-                if (W.bst[h] != kOk) return W.bst[h];
-                mb = W.bnd[h];
-            }
-            if (!(isfinite(mb) && mb >= sep && mb >= 0.0)) return kEclBracket;
-            if (L.side == R.side && L.margin + R.margin > mb) {
-                resolved = true;
-            } else if (mb <= kEclMaxSepKm && L.side != R.side) {
-                br->t_old = L.t;
-                br->t_new = R.t;
-                br->old_side = L.side;
-                br->new_side = R.side;
-                br->bound = mb;
-                *found = true;
-                return kOk;
-            } else {
-                const double mid = L.t + 0.5 * (R.t - L.t);
-                if (mid == L.t || mid == R.t || !isfinite(mid)) {
-                    if (L.side == R.side && mb <= 1.0e-6) resolved = true;
-                    else return kEclNonProgress;
-                } else {
-                    if (splits_left == 0 || sp == kEclScanDepth) return kEclSplitLimit;
-                    --splits_left;
-                    if (b - a == 1) {
-                        // a bottom-level node: it becomes the root of a new store
-                        __syncwarp();
-                        if (lane == 0) {
-                            ecl_store_point(W, 0, L);
-                            ecl_store_point(W, kEclGrid, R);
-                        }
-                        __syncwarp();
-                        ++gen;
-                        h = 1;
-                        a = 0;
-                        b = kEclGrid;
-                        expanded = false;
-                    }
-                    if (h == 1 && !expanded) {
-                        ecl_expand(G, H, W, lane);
-                        expanded = true;
-                    }
+        const EclNodeTest T = h == 1
+                                  ? ecl_node_test_points(G, ecl_load_point(W, a), ecl_load_point(W, b), inherited, inh)
+                                  : ecl_node_test_store(W, h, a, b);
+        if (T.err) return T.err;
+        if (T.verdict == kVerdictFound) {
+            br->t_old = W.t[a];
+            br->t_new = W.t[b];
+            br->old_side = W.side[a];
+            br->new_side = W.side[b];
+            br->bound = T.mb;
+            *found = true;
+            return kOk;
+        }
+        if (T.verdict == kVerdictSplit) {
+            if (splits_left == 0 || sp == kEclScanDepth) return kEclSplitLimit;
+            --splits_left;
+            const double r_t = W.t[b];
+            if (h == 1 || b - a == 1) {
+                if (b - a == 1) {
+                    // a bottom-level node becomes the root of a new store
+                    const EclPoint L = ecl_load_point(W, a), R = ecl_load_point(W, b);
+                    __syncwarp();
                     if (lane == 0) {
-                        W.st_t[sp] = R.t;
-                        W.st_inh[sp] = mb;
-                        W.st_h[sp] = 2 * h + 1;
-                        W.st_gen[sp] = gen;
+                        ecl_store_point(W, 0, L);
+                        ecl_store_point(W, kEclGrid, R);
                     }
                     __syncwarp();
-                    ++sp;
-                    const int pm = (a + b) >> 1;
-                    if (W.pst[pm] != kOk) return W.pst[pm];
-                    h = 2 * h;
-                    inherited = true;
-                    inh = mb;
+                    ++gen;
+                    h = 1;
+                    a = 0;
+                    b = kEclGrid;
                 }
+                ecl_expand(G, H, W, lane, T.mb);
             }
-        }
-        if (resolved) {
-            if (sp == 0) return kOk;
-            --sp;
-            const int ph = W.st_h[sp], pg = W.st_gen[sp];
-            const double pt = W.st_t[sp], pinh = W.st_inh[sp];
-            if (pg == gen) {
-                h = ph;
-            } else {
-                // a right sibling from an older store: a new store rooted at
-                // it, from this node's right end to the sibling's (its point
-                // evaluated again: the same bits)
-                EclPoint q;
-                const int32_t e = ecl_point(G, H, pt, &q);
-                __syncwarp();
-                if (lane == 0) {
-                    ecl_store_point(W, 0, R);
-                    ecl_store_point(W, kEclGrid, q);
-                    W.pst[kEclGrid] = e;
-                }
-                __syncwarp();
-                if (e != kOk) return e;
-                ++gen;
-                h = 1;
-                expanded = false;
+            if (lane == 0) {
+                W.st_t[sp] = r_t;
+                W.st_inh[sp] = T.mb;
+                W.st_h[sp] = 2 * h + 1;
+                W.st_gen[sp] = gen;
             }
+            __syncwarp();
+            ++sp;
+            const int pm = (a + b) >> 1;
+            if (W.pst[pm] != kOk) return W.pst[pm];
+            h = 2 * h;
             inherited = true;
-            inh = pinh;
+            inh = T.mb;
+            continue;
         }
+        // resolved: the next pending right sibling
+        if (sp == 0) return kOk;
+        --sp;
+        const int ph = W.st_h[sp], pg = W.st_gen[sp];
+        const double pt = W.st_t[sp], pinh = W.st_inh[sp];
+        if (pg == gen) {
+            h = ph;
+        } else {
+            // a sibling from an older store: a new store rooted at it, from
+            // this node's right end to the sibling's (evaluated again: the
+            // same bits)
+            const EclPoint R = ecl_load_point(W, b);
+            EclPoint q;
+            const int32_t e = ecl_point(G, H, pt, &q);
+            __syncwarp();
+            if (lane == 0) {
+                ecl_store_point(W, 0, R);
+                ecl_store_point(W, kEclGrid, q);
+                W.pst[kEclGrid] = e;
+            }
+            __syncwarp();
+            if (e != kOk) return e;
+            ++gen;
+            h = 1;
+        }
+        inherited = true;
+        inh = pinh;
     }
 }
 

@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(kBlock) pl_drag_coarse(ForceParams fp, PipeBuf
 // Splits a row's own thread may take on its crossing scan before the warp
 // takes it over.
 #ifndef BQP_ECL_SOLO_SPLITS
-#define BQP_ECL_SOLO_SPLITS 16
+#define BQP_ECL_SOLO_SPLITS 4
 #endif
 constexpr int64_t kEclSoloSplits = BQP_ECL_SOLO_SPLITS;
 
