@@ -469,7 +469,7 @@ static __device__ __noinline__ void emit_samples(const PropArgs& A, TrajState& s
 }
 
 template <int M>
-__device__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
+__device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t traj, const double* ynext,
                            const double* dy_prev, const double* dy_next, double en);
 
 // Accepted step: time update, samples, PI controller, ground check and the
