@@ -157,7 +157,18 @@ __device__ __forceinline__ int32_t ecl_decisive_margin(double err, double* out) 
     return kOk;
 }
 
-// eclipse.rs:124-152 on baseline + delta at solver time t.
+// eclipse.rs:124-152 on a baseline state b plus delta d.
+__device__ __forceinline__ bool ecl_envelope_of(const double* b, const double* d) {
+    const double p0 = b[0] + d[0], p1 = b[1] + d[1], p2 = b[2] + d[2];
+    const double v0 = b[3] + d[3], v1 = b[4] + d[4], v2 = b[5] + d[5];
+    if (!(isfinite(p0) && isfinite(p1) && isfinite(p2) && isfinite(v0) && isfinite(v1) && isfinite(v2)))
+        return false;
+    const double r = sqrt(fma(p0, p0, fma(p1, p1, p2 * p2)));
+    const double s = sqrt(fma(v0, v0, fma(v1, v1, v2 * v2)));
+    return isfinite(r) && isfinite(s) && r >= kEclRadiusMin && r <= kEclRadiusCap && s <= kEclSpeedCap;
+}
+
+// ... on baseline + delta at solver time t.
 __device__ __forceinline__ bool ecl_envelope(const Baseline& base, double bt0, const double* d, double t) {
     double b[6];
     baseline_state(base, t - bt0, b);
@@ -269,14 +280,16 @@ struct EclBracket {
 // redo from the start (the same result, sooner).
 constexpr int32_t kEclDefer = -2;
 static __device__ __noinline__ int32_t ecl_first_crossing(const EclGeo& G, const EclPath& H, double t_a, double t_b,
-                                                   bool* found, EclBracket* br, int64_t budget = kEclMaxSplits) {
+                                                   bool* found, EclBracket* br, int64_t budget = kEclMaxSplits,
+                                                   const EclPoint* start = nullptr) {
     *found = false;
     if (t_a == t_b) return kEclNonProgress;
     double st_t[kEclScanDepth], st_b[kEclScanDepth];
     int sp = 0;
     int64_t splits_left = kEclMaxSplits;
     EclPoint L, R;
-    if (int32_t e = ecl_point(G, H, t_a, &L)) return e;
+    if (start) L = *start;  // the point at t_a, already evaluated
+    else if (int32_t e = ecl_point(G, H, t_a, &L)) return e;
     if (int32_t e = ecl_point(G, H, t_b, &R)) return e;
     bool inherited = false;
     double inh = 0.0;
@@ -337,11 +350,11 @@ static __device__ __noinline__ int32_t ecl_first_crossing(const EclGeo& G, const
 static __device__ __noinline__ int32_t ecl_step_pre(const EclGeo& G, const Baseline& base, double bt0, int fixed,
                                              const EclState& E, double t0, const double* y0, const double* d0,
                                              double t1, const double* y1, const double* d1, EclPath* H,
-                                             double* from) {
-    if (!ecl_envelope(base, bt0, y0, t0) || !ecl_envelope(base, bt0, y1, t1)) return kEclEnvelope;
+                                             double* from, EclPoint* start) {
     double b0[6], b1[6];
     baseline_state(base, t0 - bt0, b0);
     baseline_state(base, t1 - bt0, b1);
+    if (!ecl_envelope_of(b0, y0) || !ecl_envelope_of(b1, y1)) return kEclEnvelope;
     for (int i = 0; i < 3; ++i) {
         H->p0[i] = b0[i] + y0[i];
         H->v0[i] = b0[3 + i] + d0[i];
@@ -366,6 +379,7 @@ static __device__ __noinline__ int32_t ecl_step_pre(const EclGeo& G, const Basel
         if (q.side != fixed || q.margin <= dm) return kEclChatter;
         *from = edge;
     }
+    *start = q;  // the scan's first end point
     return kOk;
 }
 
@@ -562,15 +576,19 @@ __device__ __forceinline__ EclNodeTest ecl_node_test_store(const EclWarpStore& W
 // it with the same arguments and returns the same result.
 static __device__ __noinline__ int32_t ecl_first_crossing_warp(const EclGeo& G, const EclPath& H, double t_a,
                                                                double t_b, EclWarpStore& W, bool* found,
-                                                               EclBracket* br) {
+                                                               EclBracket* br, const EclPoint* start = nullptr) {
     const int lane = threadIdx.x & 31;
     *found = false;
     if (t_a == t_b) return kEclNonProgress;
     {
         EclPoint q;
         int32_t e = kOk;
-        if (lane == 0) e = ecl_point(G, H, t_a, &q);
-        else if (lane == 1) e = ecl_point(G, H, t_b, &q);
+        if (lane == 0) {
+            if (start) q = *start;
+            else e = ecl_point(G, H, t_a, &q);
+        } else if (lane == 1) {
+            e = ecl_point(G, H, t_b, &q);
+        }
         if (lane < 2) {
             ecl_store_point(W, lane == 0 ? 0 : kEclGrid, q);
             W.pst[lane == 0 ? 0 : kEclGrid] = e;

@@ -433,7 +433,8 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
                     const EclGeo G{&A.force, s.jd0};
                     bool found = false;
                     EclBracket br{};
-                    const int32_t e = ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br, kEclSoloSplits);
+                    const int32_t e =
+                        ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br, kEclSoloSplits, &req.start);
                     if (e == kEclDefer) scan = true;
                     else ecl_accept_post<M>(A, s, traj, tn, ynext, k0, dyn, en, e, found, br);
                 }
@@ -462,10 +463,18 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
             const double from = __shfl_sync(0xffffffffu, req.from, leader);
             const double t1 = __shfl_sync(0xffffffffu, req.t1, leader);
             const double jd0 = __shfl_sync(0xffffffffu, s.jd0, leader);
+            EclPoint q;
+            q.t = __shfl_sync(0xffffffffu, req.start.t, leader);
+            for (int i = 0; i < 3; ++i) {
+                q.p[i] = __shfl_sync(0xffffffffu, req.start.p[i], leader);
+                q.v[i] = __shfl_sync(0xffffffffu, req.start.v[i], leader);
+            }
+            q.side = __shfl_sync(0xffffffffu, req.start.side, leader);
+            q.margin = __shfl_sync(0xffffffffu, req.start.margin, leader);
             const EclGeo G{&A.force, jd0};
             bool found = false;
             EclBracket br{};
-            const int32_t e = ecl_first_crossing_warp(G, H, from, t1, ecl_ws[threadIdx.x >> 5], &found, &br);
+            const int32_t e = ecl_first_crossing_warp(G, H, from, t1, ecl_ws[threadIdx.x >> 5], &found, &br, &q);
             if (lane == leader) {
                 scan_err = e;
                 scan_found = found;

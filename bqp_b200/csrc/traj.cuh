@@ -803,6 +803,7 @@ static __device__ __noinline__ void ecl_leg_done(const PropArgs& A, TrajState& s
 struct EclScanReq {
     EclPath H;
     double from, t1;
+    EclPoint start;  // the point at `from`
 };
 
 // Accepted step of an SRP row, up to its crossing scan: the time update and
@@ -829,7 +830,7 @@ __device__ __noinline__ bool ecl_accept_pre(const PropArgs& A, TrajState& s, int
     s.rejects = 0;
     const EclGeo G{&A.force, s.jd0};
     if (int32_t e = ecl_step_pre(G, baseline_new(s.cur), s.ct0, s.side, A.ecl[traj], s.t, s.y, dy_prev, tn, ynext,
-                                 dy_next, &req->H, &req->from)) {
+                                 dy_next, &req->H, &req->from, &req->start)) {
         traj_fail(A, s, traj, e);
         return false;
     }
@@ -892,7 +893,7 @@ __device__ __noinline__ void ecl_accept(const PropArgs& A, TrajState& s, int64_t
     const EclGeo G{&A.force, s.jd0};
     bool found = false;
     EclBracket br;
-    const int32_t e = ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br);
+    const int32_t e = ecl_first_crossing(G, req.H, req.from, req.t1, &found, &br, kEclMaxSplits, &req.start);
     ecl_accept_post<M>(A, s, traj, tn, ynext, dy_prev, dy_next, en, e, found, br);
 }
 
