@@ -298,8 +298,9 @@ int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in,
  * Same arguments, results and per-row status as bqp_propagate_final, always
  * on the persistent kernel (whatever cfg.engine says) with the plain FP64
  * field: a context configured for split precision, the learned surrogate or
- * the FP32 density (forms only the stage-synchronous engine runs) is refused
- * with BQP_E_UNSUPPORTED.  The JB2008 sweep fits it uses are the ones the
+ * the FP32 density (forms only the stage-synchronous engine runs), or for
+ * binary-eclipse SRP (whose per-row coordinator state the fixed array has
+ * no room for), is refused with BQP_E_UNSUPPORTED.  The JB2008 sweep fits it uses are the ones the
  * context built when it was created or last reconfigured (bqp_ctx_set_config,
  * bqp_ctx_set_jb_drivers), so identical calls give identical bits whatever
  * was called in between.  With bqp_ctx_profile on, its kernel time counts

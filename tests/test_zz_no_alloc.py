@@ -90,8 +90,16 @@ def test_noalloc_refuses_forms_it_would_not_run():
     with pytest.raises(N.NativeError) as e:
         ctx.propagate_final_noalloc(s, EPOCH, 600.0)
     assert e.value.code == N.E_UNSUPPORTED and "split precision" in str(e.value)
-    # the same context without the split form runs
+    # SRP's eclipse coordinator keeps per-row state the fixed array has no
+    # room for: refused too
     cfg.split_degree = 0
+    cfg.force_flags |= N.FORCE_SRP
+    ctx.set_config(cfg)
+    with pytest.raises(N.NativeError) as e:
+        ctx.propagate_final_noalloc(s, EPOCH, 600.0)
+    assert e.value.code == N.E_UNSUPPORTED and "SRP" in str(e.value)
+    # the same context in plain FP64 without SRP runs
+    cfg.force_flags &= ~N.FORCE_SRP
     ctx.set_config(cfg)
     out, st, _, _ = ctx.propagate_final_noalloc(s, EPOCH, 600.0)
     assert (st == 0).all() and np.isfinite(out).all()
