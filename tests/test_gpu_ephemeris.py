@@ -141,3 +141,38 @@ def test_python_surface_takes_the_catalogues():
     ref, st2, _, _ = ctx_for(text, 8, cats).propagate_final(states, EPOCH, 3600.0, ballistic=np.array([0.01, 2.2]))
     assert (st == 0).all() and (st2 == 0).all()
     assert np.abs(got[:, :3] - ref[:, :3]).max() < 1e-5
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_srp_with_catalogues_matches_oracle(engine):
+    """Binary-eclipse SRP with the Sun from a catalogue: the shadow geometry,
+    the eclipse scans and their Sun-sweep bound (the catalogue's own rate
+    supremum) on both sides."""
+    order, eps, tf, n = 12, 1e-10, 3 * 3600.0, 16
+    text = workloads.synthetic_field(order)
+    cats = catalogues()
+    ctx = ctx_for(text, order, cats, engine, eps)
+    cfg = N.default_config()
+    cfg.order = order
+    cfg.force_flags = N.FORCE_DRAG | N.FORCE_SUN | N.FORCE_MOON | N.FORCE_SRP
+    cfg.atm_model = 4
+    cfg.method = N.METHODS["dop853"]
+    cfg.eps = eps
+    cfg.engine = N.ENGINES[engine]
+    cfg.cr = 1.3
+    ctx.set_config(cfg)
+    states = workloads.leo_states(n, seed=17)
+    bal = workloads.leo_ballistics(n, seed=17)
+    equ, _ = N.eci_to_equinoctial(states)
+    got, st, steps, _ = ctx.propagate_final(states, EPOCH, tf, ballistic=bal)
+    F = oracle_force(text, order, cats)
+    F.set_srp(True, 1.3)
+    d, _, rst, rsteps, _, _ = O.propagate_srp_batch(F, O.ctrl("dop853", eps=eps), equ, EPOCH, tf, bal)
+    assert (st == 0).all() and (rst == 0).all(), (st, rst)
+    for i in range(n):
+        ref = O.equinoc2eci(equ[i], tf)[0] + d[i]
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+    assert np.all(np.abs(steps - rsteps) <= np.maximum(3, 0.05 * rsteps))
+    # the bound the oracle uses is the catalogue's supremum, near the Sun's
+    # apparent rate and below the analytic series' constant
+    assert 0.0160 < F.sun_rate_bound() < 0.0185
