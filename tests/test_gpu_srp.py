@@ -210,3 +210,25 @@ def test_warp_scan_equals_the_serial_scan():
     # the rest certified free of crossings, bar a few grazing steps that
     # run out of bisections as the reference's scan would
     assert (serial[~found, 0] == 0).mean() > 0.9 and set(np.unique(serial[:, 0])) <= {0.0, 14.0, 16.0}
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_srp_mixed_orbits_match_oracle(engine):
+    """SRP on LEO, MEO, GEO and HEO rows (the uneven workload's orbits, every
+    row with A/m > 0) over one day: long shadows at GEO, perigee passes of
+    HEO rows, both engines against the oracle."""
+    order, eps, tf, n = 20, 1e-10, 86400.0, 24
+    text = workloads.synthetic_field(order)
+    states, _, _ = workloads.mixed_states(n, seed=29)
+    bal = workloads.leo_ballistics(n, seed=29)
+    equ, _ = N.eci_to_equinoctial(states)
+    got, st, steps, _ = ctx_srp(text, order, "dop853", eps, engine).propagate_final(states, EPOCH, tf, ballistic=bal)
+    d, _, rst, rsteps, _, _ = O.propagate_srp_batch(oracle_srp(text, order), O.ctrl("dop853", eps=eps), equ, EPOCH,
+                                                    tf, bal)
+    assert np.array_equal(st, rst), (st, rst)
+    ok = st == 0
+    assert ok.sum() >= n - 2
+    for i in np.flatnonzero(ok):
+        ref = O.equinoc2eci(equ[i], tf)[0] + d[i]
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+    assert np.all(np.abs(steps[ok] - rsteps[ok]) <= np.maximum(5, 0.1 * rsteps[ok]))
