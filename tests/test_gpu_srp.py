@@ -228,7 +228,22 @@ def test_srp_mixed_orbits_match_oracle(engine):
     assert np.array_equal(st, rst), (st, rst)
     ok = st == 0
     assert ok.sum() >= n - 2
+    # over a day of ~30 shadow crossings a LEO row's along-track error grows:
+    # the oracle itself moves by up to ~1e-4 km when its input moves by
+    # 1e-15, so each row is held to the larger of the per-step bound and
+    # twice that spread of the oracle's own result
+    spread = np.zeros(n)
+    for k in (1, 2, 3):
+        pe = equ.copy()
+        pe[:, 0] *= 1.0 + k * 1e-15
+        dk, _, _, _, _, _ = O.propagate_srp_batch(oracle_srp(text, order), O.ctrl("dop853", eps=eps), pe, EPOCH, tf,
+                                                  bal)
+        for i in np.flatnonzero(ok):
+            a = O.equinoc2eci(equ[i], tf)[0] + d[i]
+            b = O.equinoc2eci(pe[i], tf)[0] + dk[i]
+            spread[i] = max(spread[i], np.linalg.norm(a[:3] - b[:3]))
     for i in np.flatnonzero(ok):
         ref = O.equinoc2eci(equ[i], tf)[0] + d[i]
-        assert np.linalg.norm(got[i, :3] - ref[:3]) <= 2 * max(steps[i], 1) * eps * 10, i
+        bound = max(2 * max(steps[i], 1) * eps * 10, 2 * spread[i])
+        assert np.linalg.norm(got[i, :3] - ref[:3]) <= bound, (i, np.linalg.norm(got[i, :3] - ref[:3]), bound)
     assert np.all(np.abs(steps[ok] - rsteps[ok]) <= np.maximum(5, 0.1 * rsteps[ok]))
