@@ -18,9 +18,10 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbqp_b200.so"
 SOURCES = ["propagate.cu", "pipeline.cu", "eclipse.cu", "sigma.cu", "mlp.cu", "surrogate.cu", "space_weather.cu", "ephemeris.cu",
-           "bqp_api.cu"]
+           "bqp_api.cu", "frame_time.cpp"]
 HEADERS = ["kernels.cuh", "gravity.cuh", "gravity_cta.cuh", "jb2008.cuh", "physics.cuh", "launch.h", "rk_tableaus.h",
-           "traj.cuh", "eclipse.cuh", "tc_gemm.cuh", "space_weather.h", "ephemeris.h", "surrogate.h"]
+           "traj.cuh", "eclipse.cuh", "tc_gemm.cuh", "space_weather.h", "ephemeris.h", "surrogate.h",
+           "frame_time.h", "frame_time_host.h", "iau2000a_tables.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -20,6 +20,7 @@
 
 #include "../../include/bqp_prop.h"
 #include "launch.h"
+#include "frame_time_host.h"
 #include "eclipse.cuh"
 #include "ephemeris.h"
 #include "space_weather.h"
@@ -522,6 +523,15 @@ struct bqp_ctx {
     Model* sur = nullptr;          // learned gravity surrogate (bqp_surrogate_*)
     double* d_tab_low = nullptr;   // FP64 table of degrees <= BQP_SURROGATE_DEGREE
     uint32_t low_bytes = 0;
+    // IAU 2006/2000A Earth-fixed frame (bqp_ctx_set_frame): the segment
+    // authority (null: the GMST rotation) and the device copy of the
+    // segments of the latest batch
+    std::unique_ptr<ft::Authority> frame;
+    ft::FrameSeg* d_fseg = nullptr;
+    int64_t* d_fkey = nullptr;
+    int64_t fseg_cap = 0;
+    ft::FrameIntervals* d_fivl = nullptr;
+    ft::FrameTab ftab{};
 };
 
 namespace {
@@ -613,7 +623,101 @@ ForceParams force_params(const bqp_ctx* ctx) {
     // the sweep fits replace the exact model's quadrature only
     fp.fit = (c.drag_quadrature || !fp.drag || fp.atm_model != 4) ? nullptr : ctx->d_fit;
     fp.fit2 = fp.fit ? ctx->d_fit2 : nullptr;
+    fp.frame = ctx->ftab;
     return fp;
+}
+
+// The IAU frame's segments for a batch: every segment holding an instant of
+// a row's [epoch + min(t0, tf), epoch + max(t0, tf)] (one more on each
+// side), built on the host (kept by the authority) and copied to the device
+// sorted by key.  Rows whose instants have no segment fail on the device
+// with the frame-time status.  Host arrays.
+int frame_prepare_host(bqp_ctx* ctx, int64_t n, const double* epoch, const double* lo, const double* hi) {
+    if (!ctx->frame) {
+        ctx->ftab = ft::FrameTab{};
+        return 0;
+    }
+    std::vector<std::pair<int32_t, int64_t>> want;
+    const double pad = ft::kSegWidth;
+    double tmin = INFINITY, tmax = -INFINITY;
+    std::vector<std::pair<double, double>> spans;
+    for (int64_t i = 0; i < n; ++i) {
+        double tai0;
+        if (!ft::tai_seconds_from_utc_jd(epoch[i], &tai0)) continue;
+        const double a = tai0 + std::min(lo[i], hi[i]) - pad, b = tai0 + std::max(lo[i], hi[i]) + pad;
+        if (!(std::isfinite(a) && std::isfinite(b))) continue;
+        spans.push_back({a, b});
+        tmin = std::min(tmin, a);
+        tmax = std::max(tmax, b);
+    }
+    // merge overlapping row spans before listing their segments
+    std::sort(spans.begin(), spans.end());
+    for (size_t i = 0; i < spans.size();) {
+        double a = spans[i].first, b = spans[i].second;
+        size_t j = i + 1;
+        while (j < spans.size() && spans[j].first <= b) b = std::max(b, spans[j++].second);
+        ctx->frame->keys_between(a, b, &want);
+        i = j;
+    }
+    std::vector<int64_t> keys;
+    std::vector<ft::FrameSeg> segs;
+    ctx->frame->ensure(want, &keys, &segs);
+    const int64_t m = (int64_t)keys.size();
+    cudaError_t e = cudaSuccess;
+    if (m > ctx->fseg_cap) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_fseg);
+        cudaFree(ctx->d_fkey);
+        ctx->d_fseg = nullptr;
+        ctx->d_fkey = nullptr;
+        ctx->fseg_cap = 0;
+        const int64_t cap = std::max<int64_t>(m, 64);
+        e = cudaMalloc(&ctx->d_fseg, (size_t)cap * sizeof(ft::FrameSeg));
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_fkey, (size_t)cap * sizeof(int64_t));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(frame segments)");
+        ctx->fseg_cap = cap;
+    }
+    if (!ctx->d_fivl) {
+        e = cudaMalloc(&ctx->d_fivl, sizeof(ft::FrameIntervals));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(frame intervals)");
+    }
+    // synchronous copies: the host vectors go out of scope on return
+    if (m > 0) e = cudaMemcpyAsync(ctx->d_fseg, segs.data(), (size_t)m * sizeof(ft::FrameSeg),
+                                   cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && m > 0)
+        e = cudaMemcpyAsync(ctx->d_fkey, keys.data(), (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->d_fivl, &ctx->frame->intervals(), sizeof(ft::FrameIntervals),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "frame segment upload");
+    ctx->ftab.mode = 1;
+    ctx->ftab.nseg = (int32_t)m;
+    ctx->ftab.seg = ctx->d_fseg;
+    ctx->ftab.key = ctx->d_fkey;
+    ctx->ftab.ivl = ctx->d_fivl;
+    return 0;
+}
+
+// The same for device arrays of epochs and end times (start d_t0 per row,
+// or the common t0 when it is null).
+int frame_prepare_dev(bqp_ctx* ctx, int64_t n, const double* d_epoch, double t0, const double* d_tf,
+                      const double* d_t0 = nullptr) {
+    if (!ctx->frame) {
+        ctx->ftab = ft::FrameTab{};
+        return 0;
+    }
+    std::vector<double> ep((size_t)n), tf((size_t)n), lo((size_t)n, t0);
+    cudaError_t e = cudaSuccess;
+    if (n > 0 && d_t0) e = cudaMemcpyAsync(lo.data(), d_t0, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpyAsync(ep.data(), d_epoch, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpyAsync(tf.data(), d_tf, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "frame span readback");
+    return frame_prepare_host(ctx, n, ep.data(), lo.data(), tf.data());
 }
 
 // Builds (once per driver set) the altitude-dependent sweep fits; they are
@@ -788,6 +892,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
     A.ncells = ctx->ncells;
     A.use_smem = ctx->use_smem;
     if (int rc = ensure_fit2(ctx)) return rc;
+    if (int rc = frame_prepare_dev(ctx, n, epoch, t0, tf)) return rc;
     A.force = force_params(ctx);
     A.fit_host = A.force.fit ? &ctx->h_fit : nullptr;
     A.ctrl = ctrl_params(ctx);
@@ -824,6 +929,7 @@ int launch_prop(bqp_ctx* ctx, int64_t n, const double* in, int32_t input_equ, co
         }
         PipeBufs P{};
         pipeline_carve(P, ctx->d_pws, n);
+        P.iau = A.force.frame.mode == 1 ? 1 : 0;
         cudaError_t e = launch_pipeline(A, P, ctx->cfg.method, ctx->stream, ctx->cfg.max_kernel_seconds,
                                         ctx->cfg.gravity_threads, ctx->cfg.gravity_slots,
                                         ctx->profile ? &ctx->times : nullptr);
@@ -1109,6 +1215,9 @@ int bqp_ctx_destroy(bqp_ctx* ctx) {
     if (ctx->d_sw_dtc) cudaFree(ctx->d_sw_dtc);
     for (double* p : ctx->d_eph)
         if (p) cudaFree(p);
+    if (ctx->d_fseg) cudaFree(ctx->d_fseg);
+    if (ctx->d_fkey) cudaFree(ctx->d_fkey);
+    if (ctx->d_fivl) cudaFree(ctx->d_fivl);
     delete ctx->sur;
     delete ctx;
     return 0;
@@ -1242,6 +1351,34 @@ int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out
     cudaFree(d_out);
     cudaFree(d_ok);
     if (e != cudaSuccess) return cuda_fail(e, "space-weather lookup");
+    return 0;
+}
+
+int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t first_mjd, int32_t n_records) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (mode != BQP_FRAME_GMST && mode != BQP_FRAME_IAU2006)
+        return fail(BQP_E_ARG, "frame mode must be BQP_FRAME_GMST (0) or BQP_FRAME_IAU2006 (1), got %d", mode);
+    if (n_records < 0 || (n_records > 0 && !eop)) return fail(BQP_E_ARG, "bad EOP records");
+    if (mode == BQP_FRAME_GMST) {
+        if (n_records > 0) return fail(BQP_E_ARG, "EOP records are for the IAU frame");
+        ctx->frame.reset();
+        ctx->ftab = ft::FrameTab{};
+        return 0;
+    }
+    if (n_records > 0) {
+        if (first_mjd < ft::kOriginMjd - 3)
+            return fail(BQP_E_ARG, "EOP records start at MJD %d, before the frame's origin MJD %d", first_mjd,
+                        ft::kOriginMjd);
+        for (int64_t i = 0; i < (int64_t)n_records * 5; ++i)
+            if (!std::isfinite(eop[i])) return fail(BQP_E_ARG, "EOP record %lld is not finite", (long long)(i / 5));
+    }
+    ft::Eop e;
+    if (n_records > 0) {
+        e.first_mjd = first_mjd;
+        e.rec.assign(eop, eop + (size_t)n_records * 5);
+    }
+    ctx->frame.reset(new ft::Authority(e));
+    ctx->ftab = ft::FrameTab{};
     return 0;
 }
 
@@ -1401,6 +1538,7 @@ int bqp_rhs_eval_device(bqp_ctx* ctx, int64_t n, const double* equ, const double
         return fail(BQP_E_ARG, "bad buffers");
     int rc = set_device(ctx);
     if (rc) return rc;
+    if ((rc = frame_prepare_dev(ctx, n, epoch_jd, 0.0, t, t))) return rc;
     cudaError_t e = launch_rhs(ctx->d_tab, ctx->ncells, ctx->use_smem, force_params(ctx), n, equ, seg_t0,
                                epoch_jd, t, delta, ballistic, ctx->cfg.am_ratio, ctx->cfg.cd, out, ctx->stream);
     return e == cudaSuccess ? 0 : cuda_fail(e, "k_rhs launch");
@@ -1414,6 +1552,7 @@ int bqp_rhs_eval(bqp_ctx* ctx, int64_t n, const double* equ, const double* seg_t
     if (n == 0) return 0;
     int rc = set_device(ctx);
     if (rc) return rc;
+    if ((rc = frame_prepare_host(ctx, n, epoch_jd, t, t))) return rc;
     const size_t b6 = (size_t)n * 6 * sizeof(double), b1 = (size_t)n * sizeof(double);
     double *de = nullptr, *dt0 = nullptr, *djd = nullptr, *dt = nullptr, *dd = nullptr, *db = nullptr,
            *dout = nullptr;
@@ -1650,13 +1789,16 @@ int bqp_propagate_final_noalloc(bqp_ctx* ctx, int64_t n, const double* in, int32
     // this path runs the persistent kernel on the FP64 field; a context set
     // up for a form only the stage-synchronous engine has is refused, not
     // run in plain FP64
-    if (ctx->cfg.split_degree || ctx->cfg.surrogate || ctx->cfg.drag_fp32 || (ctx->cfg.force_flags & BQP_FORCE_SRP))
+    if (ctx->cfg.split_degree || ctx->cfg.surrogate || ctx->cfg.drag_fp32 || (ctx->cfg.force_flags & BQP_FORCE_SRP) ||
+        ctx->frame)
         return fail(BQP_E_UNSUPPORTED,
-                    "the no-allocation entry point runs plain FP64 without SRP only; this context is configured for %s",
+                    "the no-allocation entry point runs plain FP64 without SRP in the GMST frame only; this context "
+                    "is configured for %s",
                     ctx->cfg.surrogate ? "the learned surrogate"
                     : ctx->cfg.split_degree ? "split precision"
                     : ctx->cfg.drag_fp32 ? "the FP32 density"
-                                         : "binary-eclipse SRP");
+                    : ctx->frame ? "the IAU 2006/2000A frame (segments built per call)"
+                                 : "binary-eclipse SRP");
     int rc = check_prop_args(n, in, epoch_jd, t0, tf, out, status);
     if (rc) return rc;
     if (n > BQP_NOALLOC_MAX_TRAJ)

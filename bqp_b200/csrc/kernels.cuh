@@ -8,6 +8,7 @@
 #include "gravity.cuh"
 #include "jb2008.cuh"
 #include "physics.cuh"
+#include "frame_time.h"
 
 namespace bqp {
 
@@ -32,6 +33,9 @@ enum Status : int32_t {
     kEclNonProgress = 14,
     kEclGeometry = 15,
     kEclSplitLimit = 16,
+    // the Earth-fixed frame has no segment at an evaluation's instant (the
+    // reference's GravityError::InvalidTime from its frame authority)
+    kFrameTime = 17,
 };
 
 enum Method : int32_t { kDopri5 = 0, kDop853 = 1, kDopri5Compat = 2, kVern7 = 3, kVern9 = 4 };
@@ -55,7 +59,18 @@ struct ForceParams {
     EphemTable eph_sun, eph_moon;  // precomputed catalogues (n 0: the analytic series)
     const jb::JbFit* fit;  // device copy of the fixed-node sweep fits, or null
     const jb::JbFit2* fit2;  // altitude-dependent sweep fits (stage-synchronous drag), or null
+    ft::FrameTab frame;      // IAU 2006/2000A segments (frame.mode 1) or the GMST rotation (0)
 };
+
+// The Earth-fixed rotation of an instant under `frame.mode` 1: the segment
+// holding continuous-TAI `tai`; false (a frame-time failure) when the table
+// has none.
+__device__ __forceinline__ bool frame_rot(const ft::FrameTab& F, double tai, ft::FrameRot& R) {
+    const int32_t slot = ft::segment_slot(F, tai);
+    if (slot < 0) return false;
+    ft::rotation_at(F.seg[slot], tai, R);
+    return true;
+}
 
 // Solver controls (IntegratorConfig, solver.rs:35-60 and integrator.rs:404-558).
 struct CtrlParams {
@@ -98,9 +113,10 @@ struct Encke {
     Baseline base;
     double seg_t0;
     double jd0;
+    double tai0;  // continuous TAI seconds of t = 0 (IAU frame)
     double am, cd;
     int side;  // SRP eclipse side of the row's leg (1 shadow, 0 lit), -1 without SRP
-    int bad;   // latched invalid-radius gravity error
+    int bad;   // latched error: 1 invalid-radius gravity, 3 no frame segment
 
     __device__ __noinline__ void eval(double t, const double* d, double* out) {
         double rs[6];
@@ -112,34 +128,69 @@ struct Encke {
         const double r = sqrt(r2);
         double acc[3] = {0.0, 0.0, 0.0};
         const double jd = utc_jd_at(jd0, t);
+        // Earth-fixed position: the GMST z-rotation, or the IAU 2006/2000A
+        // rotation with its angular velocity (rhs.rs:3924-3935)
+        const bool iau = fp->frame.mode == 1;
         double s = 0.0, c = 1.0;
-        if (fp->gravity_on || fp->drag) sincos(gmst_rad(jd), &s, &c);
+        ft::FrameRot F;
         double pi[3];
-        pi[0] = fma(c, sp[0], s * sp[1]);
-        pi[1] = fma(-s, sp[0], c * sp[1]);
-        pi[2] = sp[2];
+        if (iau) {
+            if (fp->gravity_on || fp->drag) {
+                if (!frame_rot(fp->frame, tai0 + t, F)) {
+                    bad = 3;
+                    for (int i = 0; i < 6; ++i) out[i] = NAN;
+                    return;
+                }
+                ft::to_itrs(F.r, sp, pi);
+            }
+        } else {
+            if (fp->gravity_on || fp->drag) sincos(gmst_rad(jd), &s, &c);
+            pi[0] = fma(c, sp[0], s * sp[1]);
+            pi[1] = fma(-s, sp[0], c * sp[1]);
+            pi[2] = sp[2];
+        }
         if (fp->gravity_on) {
             if (!(isfinite(r2) && r2 > 0.0)) bad = 1;
             double ai[3];
             gravity_field(tab, fp->order, pi[0], pi[1], pi[2], ai);
-            acc[0] = fma(c, ai[0], -s * ai[1]);
-            acc[1] = fma(s, ai[0], c * ai[1]);
-            acc[2] = ai[2];
+            if (iau) {
+                ft::to_gcrs(F.r, ai, acc);
+            } else {
+                acc[0] = fma(c, ai[0], -s * ai[1]);
+                acc[1] = fma(s, ai[0], c * ai[1]);
+                acc[2] = ai[2];
+            }
         }
         double sun[3];
         bool have_sun = false;
         if (fp->drag && cd != 0.0 && am != 0.0) {
             sun_at(fp->eph_sun, jd, sun);
             have_sun = true;
-            double rho = density_at(pi, sun, s, c, jd);
+            double si[3];
+            if (iau) {
+                ft::to_itrs(F.r, sun, si);
+            } else {
+                si[0] = fma(c, sun[0], s * sun[1]);
+                si[1] = fma(-s, sun[0], c * sun[1]);
+                si[2] = sun[2];
+            }
+            double rho = density_at(pi, si, jd);
             if (isnan(rho)) {
                 acc[0] = acc[1] = acc[2] = NAN;
             } else if (rho > 0.0) {
                 // co-rotating atmosphere, m/s inside, km/s^2 out (rhs.rs:1119-1163)
-                const double w = fp->omega;
-                const double vr0 = (sp[3] + w * sp[1]) * 1000.0;
-                const double vr1 = (sp[4] - w * sp[0]) * 1000.0;
-                const double vr2 = sp[5] * 1000.0;
+                double vr0, vr1, vr2;
+                if (iau) {
+                    const double* w = F.w;
+                    vr0 = (sp[3] - (w[1] * sp[2] - w[2] * sp[1])) * 1000.0;
+                    vr1 = (sp[4] - (w[2] * sp[0] - w[0] * sp[2])) * 1000.0;
+                    vr2 = (sp[5] - (w[0] * sp[1] - w[1] * sp[0])) * 1000.0;
+                } else {
+                    const double w = fp->omega;
+                    vr0 = (sp[3] + w * sp[1]) * 1000.0;
+                    vr1 = (sp[4] - w * sp[0]) * 1000.0;
+                    vr2 = sp[5] * 1000.0;
+                }
                 const double v2 = fma(vr0, vr0, fma(vr1, vr1, vr2 * vr2));
                 if (v2 != 0.0) {
                     const double k = -0.5 * cd * am * rho * sqrt(v2) * 1e-3;
@@ -175,12 +226,7 @@ struct Encke {
 
     // JB2008 adapter (rhs.rs:3551-3776): Earth-fixed satellite and Sun,
     // geocentric latitude, WGS84 altitude, exospheric ceiling above 2500 km.
-    __device__ __forceinline__ double density_at(const double* pi, const double* sun, double s,
-                                                 double c, double jd) const {
-        double si[3];
-        si[0] = fma(c, sun[0], s * sun[1]);
-        si[1] = fma(-s, sun[0], c * sun[1]);
-        si[2] = sun[2];
+    __device__ __forceinline__ double density_at(const double* pi, const double* si, double jd) const {
         const double sun_r = sqrt(fma(si[0], si[0], fma(si[1], si[1], si[2] * si[2])));
         const double sat_r = sqrt(fma(pi[0], pi[0], fma(pi[1], pi[1], pi[2] * pi[2])));
         if ((sat_r - fp->earth_radius) * 1000.0 > 2500.0e3) return 1.0e-19;

@@ -65,6 +65,8 @@ struct PipeBufs {
     double* k;            // [(S+1)][6][cap] stage derivatives
     double* sp;           // [6][cap] perturbed state of the stage (ECI)
     double* sc;           // [2][cap] sin, cos of the GMST angle
+    double* fr;           // [12][cap] IAU frame: R (row-major) and ITRS angular velocity (GCRS)
+    int32_t iau;          // 1: the Earth-fixed frame is fr (IAU 2006/2000A), 0: sc (GMST)
     double* sun;          // [3][cap] Sun position (ECI), drag only
     double* part;         // [3][cap] third-body + Battin acceleration (ECI)
     double* agrav;        // [3][cap] gravity (Earth-fixed)

@@ -73,11 +73,34 @@ __device__ __forceinline__ void append_active(int32_t* list, int32_t* count, int
 
 // Sum of the stage-`st` force terms into K(st, 3..5).
 __device__ __forceinline__ void finish_stage(const PipeBufs& P, int st, int slot) {
-    const double s = P.sc[slot], c = P.sc[P.cap + slot];
     const double gx = P.agrav[slot], gy = P.agrav[P.cap + slot], gz = P.agrav[2 * P.cap + slot];
+    if (P.iau) {
+        double r[9], g[3];
+        const double gi[3] = {gx, gy, gz};
+        for (int e = 0; e < 9; ++e) r[e] = P.fr[(size_t)e * P.cap + slot];
+        ft::to_gcrs(r, gi, g);
+        for (int i = 0; i < 3; ++i)
+            K(P, st, 3 + i)[slot] = g[i] + P.adrag[(size_t)i * P.cap + slot] + P.part[(size_t)i * P.cap + slot];
+        return;
+    }
+    const double s = P.sc[slot], c = P.sc[P.cap + slot];
     K(P, st, 3)[slot] = fma(c, gx, -s * gy) + P.adrag[slot] + P.part[slot];
     K(P, st, 4)[slot] = fma(s, gx, c * gy) + P.adrag[P.cap + slot] + P.part[P.cap + slot];
     K(P, st, 5)[slot] = gz + P.adrag[2 * P.cap + slot] + P.part[2 * P.cap + slot];
+}
+
+// An ECI vector of slot `slot` in the Earth-fixed frame of its stage.
+__device__ __forceinline__ void slot_to_itrs(const PipeBufs& P, int slot, const double* v, double* o) {
+    if (P.iau) {
+        double r[9];
+        for (int e = 0; e < 9; ++e) r[e] = P.fr[(size_t)e * P.cap + slot];
+        ft::to_itrs(r, v, o);
+    } else {
+        const double s = P.sc[slot], c = P.sc[P.cap + slot];
+        o[0] = fma(c, v[0], s * v[1]);
+        o[1] = fma(-s, v[0], c * v[1]);
+        o[2] = v[2];
+    }
 }
 
 }  // namespace
@@ -156,10 +179,25 @@ __global__ void __launch_bounds__(kBlock) pl_prep(PropArgs A, PipeBufs P, int cu
     for (int i = 0; i < 3; ++i) K(P, st, i)[slot] = yt[3 + i];
     const double jd = utc_jd_at(s.jd0, ts);
     const ForceParams& fp = A.force;
-    double sn = 0.0, cs = 1.0;
-    if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);
-    P.sc[slot] = sn;
-    P.sc[P.cap + slot] = cs;
+    if (P.iau) {
+        // the IAU 2006/2000A rotation of the stage's instant (rhs.rs:3113-3174)
+        ft::FrameRot F;
+        if ((fp.gravity_on || fp.drag) && !frame_rot(fp.frame, s.tai0 + ts, F)) {
+            P.bad[slot] = 3;
+            for (int e = 0; e < 9; ++e) F.r[e] = NAN;
+            F.w[0] = F.w[1] = F.w[2] = NAN;
+        } else if (!(fp.gravity_on || fp.drag)) {
+            for (int e = 0; e < 9; ++e) F.r[e] = (e % 4 == 0) ? 1.0 : 0.0;
+            F.w[0] = F.w[1] = F.w[2] = 0.0;
+        }
+        for (int e = 0; e < 9; ++e) P.fr[(size_t)e * P.cap + slot] = F.r[e];
+        for (int e = 0; e < 3; ++e) P.fr[(size_t)(9 + e) * P.cap + slot] = F.w[e];
+    } else {
+        double sn = 0.0, cs = 1.0;
+        if (fp.gravity_on || fp.drag) sincos(gmst_rad(jd), &sn, &cs);
+        P.sc[slot] = sn;
+        P.sc[P.cap + slot] = cs;
+    }
     double acc[3] = {0.0, 0.0, 0.0};
     double sun[3];
     const bool need_sun = fp.sun || (fp.drag && s.cd != 0.0 && s.am != 0.0) || s.side >= 0;
@@ -218,18 +256,18 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
     auto load = [&](int row, double& x, double& y, double& z) -> bool {
         const int sl = list ? list[row] : row;
         if (P.skip[sl]) return false;
-        const double s = P.sc[sl], c = P.sc[P.cap + sl];
-        const double ex = P.sp[sl], ey = P.sp[P.cap + sl], ez = P.sp[2 * P.cap + sl];
-        const double qx = fma(c, ex, s * ey), qy = fma(-s, ex, c * ey);
-        const double r2 = fma(qx, qx, fma(qy, qy, ez * ez));
+        const double e[3] = {P.sp[sl], P.sp[P.cap + sl], P.sp[2 * P.cap + sl]};
+        double q[3];
+        slot_to_itrs(P, sl, e, q);
+        const double r2 = fma(q[0], q[0], fma(q[1], q[1], q[2] * q[2]));
         if (!(isfinite(r2) && r2 > 0.0)) {
-            P.bad[sl] = 1;
+            if (!P.bad[sl]) P.bad[sl] = 1;
             out[sl] = out[P.cap + sl] = out[2 * P.cap + sl] = NAN;
             return false;
         }
-        x = qx;
-        y = qy;
-        z = ez;
+        x = q[0];
+        y = q[1];
+        z = q[2];
         return true;
     };
     auto store = [&](int row, const double* a, double, double, double) {
@@ -251,11 +289,8 @@ __global__ void __launch_bounds__(256, 1) pl_gravity(GravTable T, int parts_max,
 __global__ void __launch_bounds__(kBlock) pl_earth_fixed(PipeBufs P, int cur) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= P.count[cur]) return;
-    const double s = P.sc[sl], c = P.sc[P.cap + sl];
-    const double ex = P.sp[sl], ey = P.sp[P.cap + sl], ez = P.sp[2 * P.cap + sl];
-    P.ef[3 * (size_t)sl] = fma(c, ex, s * ey);
-    P.ef[3 * (size_t)sl + 1] = fma(-s, ex, c * ey);
-    P.ef[3 * (size_t)sl + 2] = ez;
+    const double e[3] = {P.sp[sl], P.sp[P.cap + sl], P.sp[2 * P.cap + sl]};
+    slot_to_itrs(P, sl, e, P.ef + 3 * (size_t)sl);
 }
 
 // ------------------------------------------------------- surrogate check
@@ -311,10 +346,10 @@ __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs&
     double a[3] = {0.0, 0.0, 0.0};
     if (cd != 0.0 && am != 0.0) {
         // JB2008 adapter (rhs.rs:3551-3776), as Encke::density_at
-        const double s = P.sc[slot], c = P.sc[P.cap + slot];
         const double sun[3] = {P.sun[slot], P.sun[P.cap + slot], P.sun[2 * P.cap + slot]};
-        const double pi[3] = {fma(c, sp[0], s * sp[1]), fma(-s, sp[0], c * sp[1]), sp[2]};
-        const double si[3] = {fma(c, sun[0], s * sun[1]), fma(-s, sun[0], c * sun[1]), sun[2]};
+        double pi[3], si[3];
+        slot_to_itrs(P, slot, sp, pi);
+        slot_to_itrs(P, slot, sun, si);
         const double sun_r = sqrt(fma(si[0], si[0], fma(si[1], si[1], si[2] * si[2])));
         const double sat_r = sqrt(fma(pi[0], pi[0], fma(pi[1], pi[1], pi[2] * pi[2])));
         double rho;
@@ -344,10 +379,20 @@ __device__ __forceinline__ void drag_rows(const ForceParams& fp, const PipeBufs&
         if (isnan(rho)) {
             a[0] = a[1] = a[2] = NAN;
         } else if (rho > 0.0) {
-            const double w = fp.omega;
-            const double vr0 = (sp[3] + w * sp[1]) * 1000.0;
-            const double vr1 = (sp[4] - w * sp[0]) * 1000.0;
-            const double vr2 = sp[5] * 1000.0;
+            double vr0, vr1, vr2;
+            if (P.iau) {
+                // atmosphere co-rotating with the resolved frame (rhs.rs:1134-1139)
+                double w[3];
+                for (int e = 0; e < 3; ++e) w[e] = P.fr[(size_t)(9 + e) * P.cap + slot];
+                vr0 = (sp[3] - (w[1] * sp[2] - w[2] * sp[1])) * 1000.0;
+                vr1 = (sp[4] - (w[2] * sp[0] - w[0] * sp[2])) * 1000.0;
+                vr2 = (sp[5] - (w[0] * sp[1] - w[1] * sp[0])) * 1000.0;
+            } else {
+                const double w = fp.omega;
+                vr0 = (sp[3] + w * sp[1]) * 1000.0;
+                vr1 = (sp[4] - w * sp[0]) * 1000.0;
+                vr2 = sp[5] * 1000.0;
+            }
             const double v2 = fma(vr0, vr0, fma(vr1, vr1, vr2 * vr2));
             if (v2 != 0.0) {
                 const double k = -0.5 * cd * am * rho * sqrt(v2) * 1e-3;
@@ -413,7 +458,7 @@ __global__ void __launch_bounds__(kBlock) pl_control(PropArgs A, PipeBufs P, int
         int32_t code = -1;
         const int32_t d = attempt_decide<M>(A, s, k0, ynext, err, err3, &en, &code);
         if (P.bad[slot]) {
-            traj_fail(A, s, traj, P.bad[slot] == 2 ? kWatchdog : kGravityRadius);
+            traj_fail(A, s, traj, P.bad[slot] == 2 ? kWatchdog : P.bad[slot] == 3 ? kFrameTime : kGravityRadius);
         } else if (d == kFail) {
             traj_fail(A, s, traj, code);
         } else if (d == kAccept) {
@@ -530,6 +575,7 @@ void pipeline_carve(PipeBufs& P, void* base, int64_t cap) {
     P.k = (double*)take((size_t)kStageBufs * 6 * c * 8);
     P.sp = (double*)take(6 * c * 8);
     P.sc = (double*)take(2 * c * 8);
+    P.fr = (double*)take(12 * c * 8);
     P.sun = (double*)take(3 * c * 8);
     P.part = (double*)take(3 * c * 8);
     P.agrav = (double*)take(3 * c * 8);

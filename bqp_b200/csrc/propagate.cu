@@ -75,6 +75,9 @@ __global__ void k_rhs(const double* __restrict__ gtab, int ncells, int use_smem,
         R.base = baseline_new(equ + 6 * i);
         R.seg_t0 = seg_t0[i];
         R.jd0 = jd0[i];
+        R.tai0 = 0.0;
+        if (fp.frame.mode == 1 && !ft::tai_seconds_from_utc_jd(jd0[i], &R.tai0))
+            R.tai0 = NAN;  // no segment: the evaluation returns NaN
         R.am = ballistic ? ballistic[2 * i] : am0;
         R.cd = ballistic ? ballistic[2 * i + 1] : cd0;
         R.side = -1;
@@ -142,6 +145,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
         R.base = baseline_new(s.cur);
         R.seg_t0 = s.ct0;
         R.jd0 = s.jd0;
+        R.tai0 = s.tai0;
         R.am = s.am;
         R.cd = s.cd;
         R.side = s.side;
@@ -171,7 +175,7 @@ __global__ void __launch_bounds__(256, 1) k_propagate(PropArgs A) {
         int32_t code = -1;
         const int32_t d = attempt_decide<M>(A, s, k, ynext, err, err3, &en, &code);
         if (R.bad) {
-            traj_fail(A, s, traj, kGravityRadius);
+            traj_fail(A, s, traj, R.bad == 3 ? kFrameTime : kGravityRadius);
             continue;
         }
         if (d == kFail) {

@@ -76,6 +76,7 @@ enum Flag : int32_t { kHavePrev = 1, kJustRej = 2, kHaveK1 = 4, kHad = 8, kLands
 struct TrajState {
     double tf, ct0, seg_tf, t, h, err_prev, t_comp, hs, hcarry;
     double jd0, am, cd;
+    double tai0;   // continuous TAI seconds of t = 0 (IAU frame), 0 otherwise
     double lhmax;  // the eclipse leg's maximum step
     double cur[6], equ0[6], y[6], k1c[6];
     int32_t flags, rejects, s_idx, phase, status;
@@ -183,6 +184,14 @@ static __device__ __noinline__ void traj_begin(const PropArgs& A, TrajState& s, 
     ok = ok && isfinite(s.tf) && isfinite(s.jd0) && s.tf >= A.t0;
     if (!ok) {
         traj_fail(A, s, traj, kInvalidInput);
+        return;
+    }
+    // the IAU frame's time origin (rhs.rs:2754): a UTC epoch before the
+    // integer-leap era has none, and the first Earth-fixed evaluation fails
+    s.tai0 = 0.0;
+    if (A.force.frame.mode == 1 && (A.force.gravity_on || A.force.drag) &&
+        !ft::tai_seconds_from_utc_jd(s.jd0, &s.tai0)) {
+        traj_fail(A, s, traj, kFrameTime);
         return;
     }
     for (int i = 0; i < 6; ++i) s.cur[i] = s.equ0[i];

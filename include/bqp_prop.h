@@ -60,6 +60,10 @@ extern "C" {
 #define BQP_ST_ECLIPSE_NON_PROGRESS 14 /* a bracket or window that cannot shrink */
 #define BQP_ST_ECLIPSE_GEOMETRY 15     /* non-finite geometry or a Sun outside the catalogue */
 #define BQP_ST_ECLIPSE_SPLIT_LIMIT 16  /* more than 4096 roots, bisections or iterations */
+/* the IAU frame has no segment at an evaluation's instant: a UTC epoch
+ * before 1972 or an instant past the EOP table (GravityError::InvalidTime
+ * from frame_rotation_at_checked, lightyear_odeint_rs/src/rhs.rs:3124-3174) */
+#define BQP_ST_FRAME_TIME 17
 
 /* force flags (ForceFlags, lightyear_odeint_rs/src/types.rs:266-286) */
 #define BQP_FORCE_DRAG 1
@@ -234,6 +238,70 @@ int bqp_ctx_jb_lookup(bqp_ctx* ctx, const double* utc_jd, int64_t n, double* out
 #define BQP_BODY_SUN 0
 #define BQP_BODY_MOON 1
 int bqp_ctx_set_ephemeris(bqp_ctx* ctx, int32_t body, const uint8_t* bytes, int64_t len);
+
+/* ---- IAU 2006/2000A Earth-fixed frame (satpy_core/src/frame_time/) ----
+ * The Earth-fixed frame of gravity and drag.  BQP_FRAME_GMST (the default)
+ * is the z-rotation by GMST of greenwichsrt_impl (satpy_core/src/lib.rs:
+ * 905-936) with the atmosphere turning at cfg.omega_earth.  BQP_FRAME_IAU2006
+ * replaces frame_rotation_at_checked (lightyear_odeint_rs/src/rhs.rs:
+ * 3113-3174) over the reference's frame authority (frame_time/authority.rs):
+ * per stage, R = GCRS->ITRS from 1800 s segments of the CIO-based IAU
+ * 2006/2000A chain, gravity evaluated at R r and rotated back by R^T, the JB2008
+ * inputs from R r and R r_sun, and the atmosphere turning with the frame's
+ * own angular velocity (rhs.rs:1119-1163).  Time is continuous TAI from the
+ * row's UTC epoch (rhs.rs:2754).  eop: n_records x 5 doubles per UTC day
+ * from first_mjd (x_p arcsec, y_p arcsec, UT1-UTC s, dX mas, dY mas: the
+ * layout of the reference's sealed eop_table.bin, which can be passed as
+ * is with first_mjd 41684), interpolated by four-node Lagrange
+ * (authority.rs:925-1022); NULL: zero EOP, over 1973 .. 2049.  Segments are
+ * built on the host for each batch's time span and kept for the next
+ * call.  Not with bqp_propagate_final_noalloc. */
+#define BQP_FRAME_GMST 0
+#define BQP_FRAME_IAU2006 1
+int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t first_mjd, int32_t n_records);
+
+/* The chain's pieces on the host (no GPU), ERFA-restated (frame_time/
+ * iau2006.rs, cio.rs, era.rs): dates are two-part TT Julian days (UT1 for
+ * era).  nut: out[2] = dpsi, deps of IAU 2000A (iau2006 0) or 2006/2000A (1);
+ * pfw06: out[4] = gamb, phib, psib, epsa; xys06a: out[3] = X, Y, s; c2ixys
+ * and pom00: row-major r[9]. */
+void bqp_frame_nut(double d1, double d2, int32_t iau2006, double* out);
+double bqp_frame_obl06(double d1, double d2);
+void bqp_frame_pfw06(double d1, double d2, double* out);
+void bqp_frame_xys06a(double d1, double d2, double* out);
+void bqp_frame_c2ixys(double x, double y, double s, double* r);
+double bqp_frame_sp00(double d1, double d2);
+void bqp_frame_pom00(double xp, double yp, double sp, double* r);
+double bqp_frame_era(double ut1_1, double ut1_2);
+/* UTC calendar instant -> two-part quasi-JD (ERFA dtf2d "UTC", timescale.rs:
+ * 321-380; 23:59:60.x on a leap-second day).  0, or -1 on a bad instant. */
+int bqp_frame_utc_calendar(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, double* out);
+/* Continuous TAI seconds (from 0h TAI of MJD 41684) of UTC Julian days: one
+ * part (utc_jd2 NULL; split as rhs.rs:3090-3093) or two.  Returns 1 and NaN
+ * rows for instants before 1972. (authority.rs:1162-1190) */
+int bqp_frame_tai_seconds(int64_t n, const double* utc_jd, const double* utc_jd2, double* tai_s);
+/* GCRS->ITRS R[9] of the exact chain at a UTC calendar instant plus
+ * `offset` s (frame_time/chain.rs frame_matrix: policy 0 zero EOP, 1 the
+ * records' four-node Lagrange); and R, Rdot, Rddot from its centred
+ * five-point stencil of step h (chain.rs derivatives). */
+int bqp_frame_matrix(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
+                     double offset, const double* eop, int32_t first_mjd, int32_t n_eop, double* r);
+int bqp_frame_derivatives(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
+                          double h, const double* eop, int32_t first_mjd, int32_t n_eop, double* r, double* rdot,
+                          double* rddot);
+/* A standalone segment authority (FrameAuthority, authority.rs:355-650) on
+ * the host: intervals out[98] = n, 48 starts, 48 TAI - UTC, span end;
+ * rotation: R [n][9] and ITRS angular velocity in GCRS [n][3] at TAI
+ * instants (1 and NaN rows outside the span); segments: the keys and
+ * [count][60] segments (M0..M2, K0..K2, theta cubic, centre, TAI - UTC)
+ * holding [lo, hi], or -1 when more than cap. */
+typedef struct bqp_frame_authority bqp_frame_authority;
+bqp_frame_authority* bqp_frame_authority_new(const double* eop, int32_t first_mjd, int32_t n_eop);
+void bqp_frame_authority_free(bqp_frame_authority* h);
+int bqp_frame_authority_intervals(const bqp_frame_authority* h, double* out);
+int bqp_frame_authority_rotation(bqp_frame_authority* h, int64_t n, const double* tai, double* r, double* w);
+int64_t bqp_frame_authority_segments(bqp_frame_authority* h, double lo, double hi, int64_t cap, int64_t* keys,
+                                     double* segs);
 /* Positions (km) of a body at n UTC Julian days as the force kernels take
  * them (catalogue or series), evaluated on the device.  Host buffers. */
 int bqp_ctx_body_positions(bqp_ctx* ctx, int32_t body, const double* utc_jd, int64_t n, double* out);
