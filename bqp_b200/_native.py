@@ -30,10 +30,14 @@ STATUS_NAMES = {
     # the reference's eclipse_error_name (eclipse_coordinator.rs:950-966)
     11: "eclipse_envelope", 12: "eclipse_chatter", 13: "eclipse_bracket", 14: "eclipse_non_progress",
     15: "eclipse_geometry", 16: "eclipse_split_limit",
+    # GravityError::InvalidTime from the IAU frame authority
+    17: "frame_invalid_time",
 }
 ST_ECLIPSE_ENVELOPE = 11
 ECLIPSE_STATUSES = frozenset(range(11, 17))
 ST_OK, ST_GROUND, ST_GRAVITY_RADIUS = 0, 9, 6
+ST_FRAME_TIME = 17
+FRAMES = {"gmst": 0, "iau2006": 1}  # BQP_FRAME_*
 
 FORCE_DRAG, FORCE_SRP, FORCE_SUN, FORCE_MOON = 1, 2, 4, 8
 METHODS = {"dopri5_solver": 0, "dop853": 1, "dopri5": 2, "vern7": 3, "vern9": 4}
@@ -125,6 +129,26 @@ SIGNATURES = [
     ("bqp_equinoctial_to_eci", C.c_int, [C.c_int64, _dp, _dp, _dp]),
     ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),
     ("bqp_eci_to_kep", C.c_int, [C.c_int64, _dp, _dp]),
+    ("bqp_ctx_set_frame", C.c_int, [_vp, C.c_int32, _dp, C.c_int32, C.c_int32]),
+    ("bqp_frame_nut", None, [C.c_double, C.c_double, C.c_int32, _dp]),
+    ("bqp_frame_obl06", C.c_double, [C.c_double, C.c_double]),
+    ("bqp_frame_pfw06", None, [C.c_double, C.c_double, _dp]),
+    ("bqp_frame_xys06a", None, [C.c_double, C.c_double, _dp]),
+    ("bqp_frame_c2ixys", None, [C.c_double, C.c_double, C.c_double, _dp]),
+    ("bqp_frame_sp00", C.c_double, [C.c_double, C.c_double]),
+    ("bqp_frame_pom00", None, [C.c_double, C.c_double, C.c_double, _dp]),
+    ("bqp_frame_era", C.c_double, [C.c_double, C.c_double]),
+    ("bqp_frame_utc_calendar", C.c_int, [C.c_int32] * 5 + [C.c_double, _dp]),
+    ("bqp_frame_tai_seconds", C.c_int, [C.c_int64, _dp, _dp, _dp]),
+    ("bqp_frame_matrix", C.c_int, [C.c_int32] * 5 + [C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
+                                                      C.c_int32, _dp]),
+    ("bqp_frame_derivatives", C.c_int, [C.c_int32] * 5 + [C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
+                                                           C.c_int32, _dp, _dp, _dp]),
+    ("bqp_frame_authority_new", _vp, [_dp, C.c_int32, C.c_int32]),
+    ("bqp_frame_authority_free", None, [_vp]),
+    ("bqp_frame_authority_intervals", C.c_int, [_vp, _dp]),
+    ("bqp_frame_authority_rotation", C.c_int, [_vp, C.c_int64, _dp, _dp, _dp]),
+    ("bqp_frame_authority_segments", C.c_int64, [_vp, C.c_double, C.c_double, C.c_int64, _lp, _dp]),
 ]
 
 
@@ -242,6 +266,22 @@ class Context:
         sol, dtc = _text_bytes(solfsmy), _text_bytes(dtcfile)
         rc = lib().bqp_ctx_set_jb_drivers(self._h, sol, len(sol), dtc, len(dtc), float(span_jd[0]),
                                           float(span_jd[1]))
+        if rc == E_ARG:
+            raise ValueError(last_error())
+        check(rc)
+
+    def set_frame(self, frame: str = "gmst", eop=None, first_mjd: int = 41684):
+        """Earth-fixed frame of gravity and drag: "gmst" (the z-rotation by
+        GMST) or "iau2006" (GCRS->ITRS of the IAU 2006/2000A chain from 1800 s
+        segments).  eop: [n][5] records per UTC day from first_mjd (x_p, y_p
+        arcsec, UT1-UTC s, dX, dY mas; the reference's eop_table.bin as an
+        array), None for zero EOP."""
+        mode = FRAMES[frame]
+        if eop is None:
+            rc = lib().bqp_ctx_set_frame(self._h, mode, None, 0, 0)
+        else:
+            e = f64(eop).reshape(-1, 5)
+            rc = lib().bqp_ctx_set_frame(self._h, mode, dptr(e), int(first_mjd), e.shape[0])
         if rc == E_ARG:
             raise ValueError(last_error())
         check(rc)
@@ -559,3 +599,133 @@ def eci_to_kep(eci):
     out = np.empty_like(e)
     check(lib().bqp_eci_to_kep(e.shape[0], dptr(e), dptr(out)))
     return out
+
+
+# ---------------------------------------------------------- IAU 2006/2000A
+def frame_nut(d1, d2, iau2006=True):
+    o = np.zeros(2)
+    lib().bqp_frame_nut(float(d1), float(d2), int(bool(iau2006)), dptr(o))
+    return o
+
+
+def frame_obl06(d1, d2):
+    return lib().bqp_frame_obl06(float(d1), float(d2))
+
+
+def frame_pfw06(d1, d2):
+    o = np.zeros(4)
+    lib().bqp_frame_pfw06(float(d1), float(d2), dptr(o))
+    return o
+
+
+def frame_xys06a(d1, d2):
+    o = np.zeros(3)
+    lib().bqp_frame_xys06a(float(d1), float(d2), dptr(o))
+    return o
+
+
+def frame_c2ixys(x, y, s):
+    o = np.zeros(9)
+    lib().bqp_frame_c2ixys(float(x), float(y), float(s), dptr(o))
+    return o.reshape(3, 3)
+
+
+def frame_sp00(d1, d2):
+    return lib().bqp_frame_sp00(float(d1), float(d2))
+
+
+def frame_pom00(xp, yp, sp):
+    o = np.zeros(9)
+    lib().bqp_frame_pom00(float(xp), float(yp), float(sp), dptr(o))
+    return o.reshape(3, 3)
+
+
+def frame_era(u1, u2):
+    return lib().bqp_frame_era(float(u1), float(u2))
+
+
+def utc_calendar(y, m, d, hh=0, mm=0, ss=0.0):
+    """Two-part UTC quasi-JD of a calendar instant (ERFA dtf2d "UTC")."""
+    o = np.zeros(2)
+    if lib().bqp_frame_utc_calendar(y, m, d, hh, mm, float(ss), dptr(o)) != 0:
+        raise ValueError("invalid UTC calendar instant")
+    return o[0], o[1]
+
+
+def tai_seconds(utc_jd, utc_jd2=None):
+    """Continuous TAI seconds (from 0h TAI of MJD 41684) of UTC Julian days,
+    one part or two; NaN before 1972."""
+    a = f64(np.atleast_1d(utc_jd))
+    out = np.empty(a.size)
+    b = None if utc_jd2 is None else f64(np.broadcast_to(utc_jd2, a.shape))
+    lib().bqp_frame_tai_seconds(a.size, dptr(a), None if b is None else dptr(b), dptr(out))
+    return out
+
+
+def _eop_args(eop, first_mjd):
+    if eop is None or len(eop) == 0:
+        return None, 0, 0
+    e = f64(eop).reshape(-1, 5)
+    return e, int(first_mjd), e.shape[0]
+
+
+def frame_matrix(epoch, policy=0, offset=0.0, eop=None, first_mjd=0):
+    """R (GCRS->ITRS) of the exact chain at a UTC calendar instant
+    (y, m, d, hh, mm, ss) plus `offset` s; policy 0 zero EOP, 1 the records."""
+    e, f, n = _eop_args(eop, first_mjd)
+    r = np.zeros(9)
+    rc = lib().bqp_frame_matrix(*[int(v) for v in epoch[:5]], float(epoch[5]), int(policy), float(offset),
+                                None if e is None else dptr(e), f, n, dptr(r))
+    if rc != 0:
+        raise ValueError(f"frame chain failed ({rc})")
+    return r.reshape(3, 3)
+
+
+def frame_derivatives(epoch, policy=0, h=0.25, eop=None, first_mjd=0):
+    """R, Rdot, Rddot of the exact chain from its five-point stencil."""
+    e, f, n = _eop_args(eop, first_mjd)
+    r, rd, rdd = np.zeros(9), np.zeros(9), np.zeros(9)
+    rc = lib().bqp_frame_derivatives(*[int(v) for v in epoch[:5]], float(epoch[5]), int(policy), float(h),
+                                     None if e is None else dptr(e), f, n, dptr(r), dptr(rd), dptr(rdd))
+    if rc != 0:
+        raise ValueError(f"frame chain failed ({rc})")
+    return r.reshape(3, 3), rd.reshape(3, 3), rdd.reshape(3, 3)
+
+
+class FrameAuthority:
+    """The 1800 s segment authority on the host (no GPU)."""
+
+    def __init__(self, eop=None, first_mjd=41684):
+        e, f, n = _eop_args(eop, first_mjd)
+        self._keep = e
+        self._h = lib().bqp_frame_authority_new(None if e is None else dptr(e), f, n)
+        if not self._h:
+            raise ValueError("bad EOP records")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().bqp_frame_authority_free(h)
+            self._h = None
+
+    def intervals(self):
+        o = np.zeros(98)
+        check(lib().bqp_frame_authority_intervals(self._h, dptr(o)))
+        n = int(o[0])
+        return {"start": o[1:1 + n].copy(), "delta_at": o[49:49 + n].copy(), "span_end": o[97],
+                "raw": o}
+
+    def rotation(self, tai):
+        t = f64(np.atleast_1d(tai))
+        r = np.empty((t.size, 9))
+        w = np.empty((t.size, 3))
+        lib().bqp_frame_authority_rotation(self._h, t.size, dptr(t), dptr(r), dptr(w))
+        return r.reshape(-1, 3, 3), w
+
+    def segments(self, lo, hi, cap=1 << 16):
+        keys = np.zeros(cap, dtype=np.int64)
+        segs = np.zeros((cap, 60))
+        m = lib().bqp_frame_authority_segments(self._h, float(lo), float(hi), cap, lptr(keys), dptr(segs))
+        if m < 0:
+            raise ValueError("more segments than cap")
+        return keys[:m].copy(), segs[:m].copy()

@@ -1,0 +1,163 @@
+"""The IAU 2006/2000A frame chain and its 1800 s segment authority, on the
+host, against the reference's recorded known answers
+(``tests/golden/frame_time.json``, made by ``make_frame_fixture.py``):
+
+* ERFA's own unit-test values with ERFA's tolerances, as the reference's
+  gates 2-4 hold them (satpy_core/src/frame_time/iau2006.rs, cio.rs, era.rs);
+* the 20 ERFA/SOFA-derived GCRS->ITRS cases (R, Rdot, Rddot) under the
+  reference's acceptance bounds (satpy_core/tests/frame_time_oracle.rs:
+  686-700: 5e-13, 1e-13, 1e-12);
+* the segment authority against the exact chain within the reference's
+  1 mm at 7000 km (authority.rs:1405-1505), and its angular velocity
+  against the fixture's Rdot at 2024-01-01 within 2e-13 rad/s
+  (frame_time_oracle.rs:611-684).
+"""
+import json
+import struct
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bqp_b200 import _native as N
+
+GOLD = json.loads((Path(__file__).parent / "golden" / "frame_time.json").read_text())
+
+
+def hx(h):
+    return struct.unpack(">d", bytes.fromhex(h[2:]))[0]
+
+
+def hxa(seq):
+    return np.array([hx(h) for h in seq])
+
+
+def test_erfa_unit_values():
+    e = GOLD["erfa"]
+    got = N.frame_xys06a(*e["xys06a"]["date"])
+    assert np.all(np.abs(got - hxa(e["xys06a"]["want"])) < e["xys06a"]["tol"])
+    for name, iau2006 in (("nut00a", False), ("nut06a", True)):
+        got = N.frame_nut(*e[name]["date"], iau2006=iau2006)
+        assert np.all(np.abs(got - hxa(e[name]["want"])) < e[name]["tol"]), name
+    assert abs(N.frame_obl06(*e["obl06"]["date"]) - hx(e["obl06"]["want"][0])) < e["obl06"]["tol"][0]
+    got = N.frame_pfw06(*e["pfw06"]["date"])
+    assert np.all(np.abs(got - hxa(e["pfw06"]["want"])) < e["pfw06"]["tol"])
+    c = e["c2ixys"]
+    x, y, s = hxa(c["xys"])
+    r = N.frame_c2ixys(x, y, s).ravel()
+    assert np.all(np.abs(r[c["elements"]] - hxa(c["want"])) < c["tol"])
+    assert abs(r[c["x_element"]] - x) < c["tol"]
+    assert abs(N.frame_sp00(*e["sp00"]["date"]) - hx(e["sp00"]["want"][0])) < e["sp00"]["tol"][0]
+    p = e["pom00"]
+    r = N.frame_pom00(*p["args"]).ravel()
+    assert np.all(np.abs(r[p["elements"]] - hxa(p["want"])) < p["tol"])
+    assert abs(N.frame_era(*e["era00"]["date"]) - hx(e["era00"]["want"][0])) < e["era00"]["tol"][0]
+
+
+@pytest.mark.parametrize("case", GOLD["cases"], ids=[c["id"] for c in GOLD["cases"]])
+def test_chain_matches_erfa_sofa_derived_cases(case):
+    eop = np.array([[hx(v) for v in row] for row in case["eop"]]).reshape(-1, 5)
+    r, rd, rdd = N.frame_derivatives(case["epoch"], case["policy"], GOLD["stencil_h_s"], eop,
+                                     case["eop_first_mjd"])
+    assert np.abs(r.ravel() - hxa(case["R"])).max() <= 5e-13
+    assert np.abs(rd.ravel() - hxa(case["Rdot"])).max() <= 1e-13
+    assert np.abs(rdd.ravel() - hxa(case["Rddot"])).max() <= 1e-12
+    # the rotation is orthonormal to rounding
+    assert np.abs(r @ r.T - np.eye(3)).max() < 1e-15
+
+
+def test_sealed_records_equal_the_finals_rows():
+    for a in GOLD["authority"]:
+        assert np.array_equal(hxa(np.ravel(a["sealed"])), hxa(np.ravel(a["finals"])))
+
+
+@pytest.mark.parametrize("entry", GOLD["authority"], ids=lambda a: "%04d-%02d-%02dT%02d:%02d:%02.0f" % tuple(a["epoch"]))
+def test_segments_track_the_exact_chain(entry):
+    y, m, d, hh, mi, ss = entry["epoch"]
+    sealed = hxa(np.ravel(entry["sealed"])).reshape(-1, 5)
+    auth = N.FrameAuthority(sealed, entry["first_mjd"])
+    u1, u2 = N.utc_calendar(y, m, d, hh, mi, ss)
+    tai = N.tai_seconds(u1, u2)
+    r, w = auth.rotation(tai)
+    exact = N.frame_matrix(entry["epoch"], 1, 0.0, sealed, entry["first_mjd"])
+    worst_m = 0.0
+    for p in ([7000.0, 0, 0], [0, 7000.0, 0], [0, 0, 7000.0], [4041.45, 4041.45, 4041.45]):
+        worst_m = max(worst_m, np.linalg.norm(r[0] @ p - exact @ p) * 1000.0)
+    assert worst_m <= 1.0e-3
+    # the Earth turns at about 7.292e-5 rad/s about the CIP
+    assert abs(np.linalg.norm(w[0]) - 7.2921e-5) < 2e-9
+
+
+def test_angular_velocity_matches_the_fixture_rate():
+    case = next(c for c in GOLD["cases"] if c["id"] == "2024-01-01T00:00:00_real_eop_state_0")
+    r = hxa(case["R"]).reshape(3, 3)
+    rd = hxa(case["Rdot"]).reshape(3, 3)
+    # passive GCRS->ITRS: R^T Rdot = -[w_gcrs x]
+    m = r.T @ rd
+    want = 0.5 * np.array([m[1, 2] - m[2, 1], m[2, 0] - m[0, 2], m[0, 1] - m[1, 0]])
+    entry = next(a for a in GOLD["authority"] if a["epoch"][:3] == [2024, 1, 1])
+    auth = N.FrameAuthority(hxa(np.ravel(entry["sealed"])).reshape(-1, 5), entry["first_mjd"])
+    _, w = auth.rotation(N.tai_seconds(*N.utc_calendar(2024, 1, 1)))
+    assert np.abs(w[0] - want).max() <= 2.0e-13
+
+
+def test_tai_seconds_through_a_leap_second():
+    # 2016-12-31 ends in a leap second: 23:59:60 is one SI second after
+    # 23:59:59 and one before 2017-01-01T00:00:00 (authority.rs:1213-1247)
+    t59 = N.tai_seconds(*N.utc_calendar(2016, 12, 31, 23, 59, 59.0))[0]
+    t60 = N.tai_seconds(*N.utc_calendar(2016, 12, 31, 23, 59, 60.0))[0]
+    t00 = N.tai_seconds(*N.utc_calendar(2017, 1, 1, 0, 0, 0.0))[0]
+    assert t60 - t59 == 1.0 and t00 - t60 == 1.0
+    noon = N.tai_seconds(*N.utc_calendar(2016, 12, 31, 12, 0, 0.0))[0]
+    midnight = N.tai_seconds(*N.utc_calendar(2016, 12, 31, 0, 0, 0.0))[0]
+    assert noon - midnight == 43200.0
+    # the origin: 0h TAI of MJD 41684 is UTC 1973-01-02T00:00:00 less 12 s
+    assert N.tai_seconds(*N.utc_calendar(1973, 1, 2))[0] == 12.0
+    assert np.isnan(N.tai_seconds(2400000.5 + 41000.0))[0]  # 1971: before the integer-leap era
+
+
+def test_segment_index_absorbs_the_interval_remainder():
+    auth = N.FrameAuthority()
+    iv = auth.intervals()
+    # 2017-01-01 starts an interval (TAI - UTC 37 s)
+    j = int(np.searchsorted(iv["start"], N.tai_seconds(*N.utc_calendar(2017, 1, 1)))[0])
+    assert iv["delta_at"][j] == 37.0
+    # the last instant before it belongs to the previous interval's last
+    # whole segment, which therefore runs one second long
+    end = iv["start"][j]
+    keys, segs = auth.segments(end - 10.0, end - 0.5)
+    assert len(keys) == 1
+    width = end - (segs[0, 58] - 900.0)
+    assert width == 1801.0
+    # segments are pure functions of (j, k): the same key twice, same bits
+    k2, s2 = auth.segments(end - 10.0, end - 0.5)
+    assert np.array_equal(keys, k2) and np.array_equal(segs, s2)
+
+
+def test_rotation_is_continuous_across_segment_edges():
+    auth = N.FrameAuthority()
+    t0 = N.tai_seconds(*N.utc_calendar(2024, 3, 1))[0]
+    keys, segs = auth.segments(t0, t0 + 4 * 1800.0)
+    edges = segs[1:, 58] - 900.0
+    eps = 1e-3
+    r_lo, _ = auth.rotation(edges - eps)
+    r_hi, _ = auth.rotation(edges + eps)
+    # 7000 km at the seam: the two interpolants meet within a millimetre
+    jump = np.abs(r_hi - r_lo).max(axis=(1, 2)) * 7000.0 * 1000.0
+    drift = 7.3e-5 * 2 * eps * 7000.0 * 1000.0
+    assert (jump <= drift + 1e-3).all()
+
+
+def test_out_of_span_instants_are_nan():
+    auth = N.FrameAuthority()
+    iv = auth.intervals()
+    r, w = auth.rotation([iv["span_end"] + 10.0, 5.0, np.nan])
+    assert np.isnan(r).all() and np.isnan(w).all()
+    # with a short EOP table the span ends after its last day
+    first = 60300
+    auth2 = N.FrameAuthority(np.zeros((10, 5)), first)
+    end = auth2.intervals()["span_end"]
+    assert end == (first + 10 - 41684) * 86400.0 + 37.0
+    r, _ = auth2.rotation([end - 86400.0 * 5, end - 3600.0])
+    assert np.isfinite(r[0]).all()
+    assert np.isnan(r[1]).all()  # its four-node interpolation runs past the table
