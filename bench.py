@@ -102,6 +102,8 @@ def parse(argv=None):
                     help="JB2008 profile (4 exact: the metric's workload; 7 the reference's Python default)")
     ap.add_argument("--srp", action="store_true",
                     help="solar radiation pressure with binary eclipse (cr 1.3) on every row, both arms")
+    ap.add_argument("--frame", default="gmst", choices=["gmst", "iau2006"],
+                    help="Earth-fixed frame: GMST z-rotation, or the IAU 2006/2000A segments (zero EOP)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the forms block (split precision and other steppers against plain FP64)")
     ap.add_argument("--forms-rows", type=int, default=512, help="rows of the 7-day accuracy runs of the forms")
@@ -202,15 +204,17 @@ def bench_config(args) -> dict:
     """The workload's description, the same dict on both arms (the reference
     arm's bounded sample is reported beside it, in its own key)."""
     srp = " + SRP with binary eclipse" if args.srp else ""
+    srp += ", IAU 2006/2000A Earth-fixed frame" if args.frame == "iau2006" else ""
     return {"workload": f"{args.n} LEO states per GPU, 70x70 Kaula field + JB2008 drag + Sun/Moon{srp}, "
                         f"{args.method.upper()} eps {args.eps:g}, {args.segment:g} s of the arc per step",
             "form": form_name(args), "order": ORDER, "trajectories_per_gpu": args.n, "segment_s": args.segment,
             "method": args.method, "eps_km": args.eps, "atm_model": args.atm_model, "srp": bool(args.srp),
+            "frame": args.frame,
             "l2": "256 MiB write between timed steps"}
 
 
 def cpu_reference(sample: int, threads: int, segments: int = 1, method: str = "dop853", eps: float = EPS,
-                  segment_s: float = SEGMENT_S, atm_model: int = 4, srp: bool = False):
+                  segment_s: float = SEGMENT_S, atm_model: int = 4, srp: bool = False, frame: str = "gmst"):
     """Time the CPU oracle (restatement of the reference path) on the first
     `sample` trajectories of the workload for `segments` segments, all
     threads.  Only the oracle runs here: the elements come from its own
@@ -224,6 +228,15 @@ def cpu_reference(sample: int, threads: int, segments: int = 1, method: str = "d
     ctl = O.ctrl(method, eps=eps, dt_max=300.0)
     if srp:
         F.set_srp(True, 1.3)
+    if frame == "iau2006":
+        # the frame segments are an input of the force model: built by the
+        # library's host authority (zero EOP), outside the timed region
+        from bqp_b200 import _native as N
+
+        auth = N.FrameAuthority()
+        tai0 = N.tai_seconds(epoch)[0]
+        keys, segs = auth.segments(tai0 - 1800.0, tai0 + segment_s * segments + 1800.0)
+        F.set_frame(keys, segs, auth.intervals()["raw"])
     t0 = time.perf_counter()
     if srp:
         _, _, st, steps, evals, _ = O.propagate_srp_batch(F, ctl, equ, epoch, segment_s * segments, bal,
@@ -242,7 +255,8 @@ def run_reference(args):
     evals_s = []
     for i in range(args.warmup + args.steps):
         v, dt, ev, ok = cpu_reference(args.cpu_sample, threads, method=args.method, eps=args.eps,
-                                      segment_s=args.segment, atm_model=args.atm_model, srp=args.srp)
+                                      segment_s=args.segment, atm_model=args.atm_model, srp=args.srp,
+                                      frame=args.frame)
         if i >= args.warmup:
             evals_s.append((v, dt))
     value = statistics.median(v for v, _ in evals_s)
@@ -454,6 +468,11 @@ def run_ours(args):
                       args.atm_model, args.srp)
     ctx = N.Context(text, cfg)
     seg = args.segment
+    if args.frame == "iau2006":
+        # segments for every step's span, built once: the device calls stay
+        # asynchronous (no per-call epoch readback)
+        ctx.set_frame("iau2006")
+        ctx.set_frame_span(epoch - 1.0, epoch + (args.warmup + 2 * args.steps + 2) * seg / 86400.0 + 1.0)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     n = args.n
@@ -598,7 +617,8 @@ def run_ours(args):
         if not args.no_cpu and world >= 1:
             threads = os.cpu_count() or 1
             v, dt, ev, ok = cpu_reference(args.cpu_sample, threads, method=args.method, eps=args.eps,
-                                          segment_s=args.segment, atm_model=args.atm_model, srp=args.srp)
+                                          segment_s=args.segment, atm_model=args.atm_model, srp=args.srp,
+                                          frame=args.frame)
             cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{args.cpu_sample} trajectories x one 5400 s segment ({ev} evals, {dt:.1f} s)"}
         line = {
@@ -633,7 +653,7 @@ def run_ours(args):
                                 "rows": [[int(i), int(fs[i]), int(fc[i])] for i in bad[:16]]}
         if not args.no_forms and world == 1 and args.segment == SEGMENT_S and args.method == "dop853" \
                 and args.eps == EPS and not args.split_degree and args.engine == "pipeline" and args.atm_model == 4 \
-                and not args.srp:
+                and not args.srp and args.frame == "gmst":
             plain = {"force_evals_per_s": value, "trajectory_days_per_s": line["trajectory_days_per_s"]}
             line["forms"] = run_forms(args, text, states, bal, epoch, dev, plain)
         print(json.dumps(line), flush=True)

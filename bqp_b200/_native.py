@@ -130,6 +130,7 @@ SIGNATURES = [
     ("bqp_kep_to_eci", C.c_int, [C.c_int64, _dp, _dp]),
     ("bqp_eci_to_kep", C.c_int, [C.c_int64, _dp, _dp]),
     ("bqp_ctx_set_frame", C.c_int, [_vp, C.c_int32, _dp, C.c_int32, C.c_int32]),
+    ("bqp_ctx_set_frame_span", C.c_int, [_vp, C.c_double, C.c_double]),
     ("bqp_frame_nut", None, [C.c_double, C.c_double, C.c_int32, _dp]),
     ("bqp_frame_obl06", C.c_double, [C.c_double, C.c_double]),
     ("bqp_frame_pfw06", None, [C.c_double, C.c_double, _dp]),
@@ -282,6 +283,14 @@ class Context:
         else:
             e = f64(eop).reshape(-1, 5)
             rc = lib().bqp_ctx_set_frame(self._h, mode, dptr(e), int(first_mjd), e.shape[0])
+        if rc == E_ARG:
+            raise ValueError(last_error())
+        check(rc)
+
+    def set_frame_span(self, jd_lo=0.0, jd_hi=0.0):
+        """Segments of the IAU frame for UTC days [jd_lo, jd_hi], built once;
+        calls then skip the per-call epoch readback.  (0, 0): per call."""
+        rc = lib().bqp_ctx_set_frame_span(self._h, float(jd_lo), float(jd_hi))
         if rc == E_ARG:
             raise ValueError(last_error())
         check(rc)

@@ -166,19 +166,45 @@ def _ephemeris(ephemeris):
     return out
 
 
-def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None) -> N.Context:
+def _frame(frame, eop):
+    """(frame name, EOP records [n][5] or None, first MJD) of frame= / eop=.
+    eop: None (zero EOP), the bytes or path of a sealed EOP table (five
+    little-endian binary64 per UTC day from MJD 41684, the reference's
+    frame_time/eop_table.bin), or (records [n][5], first_mjd)."""
+    if frame not in N.FRAMES:
+        raise ValueError(f"frame must be one of {sorted(N.FRAMES)}, got {frame!r}")
+    if eop is None:
+        return frame, None, 41684
+    if frame != "iau2006":
+        raise ValueError("eop is for frame='iau2006'")
+    if isinstance(eop, tuple) and len(eop) == 2:
+        rec = np.asarray(eop[0], dtype=np.float64).reshape(-1, 5)
+        return frame, rec, int(eop[1])
+    data = N._file_bytes(eop)
+    if len(data) % 40:
+        raise ValueError("a sealed EOP table holds 40-byte records")
+    return frame, np.frombuffer(data, dtype="<f8").reshape(-1, 5).astype(np.float64), 41684
+
+
+def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None, frame="gmst",
+            eop=None) -> N.Context:
     """A cached native context for (field text, configuration, space-weather
     files, ephemeris catalogues).  With space_weather the JB2008 drivers come
     from the SET SOLFSMY / DTCFILE tables at each evaluation's UTC instant (the
     reference's compiled driver catalogue, jb_rs/src/drivers.rs) instead of
     the fixed configured drivers; with ephemeris the Sun and / or Moon come
     from precomputed "DUST" catalogues (the reference's precomputed_ephem.rs)
-    instead of the analytic series."""
+    instead of the analytic series; with frame="iau2006" gravity and drag
+    take the Earth-fixed frame from the IAU 2006/2000A chain (the reference's
+    frame authority, satpy_core/src/frame_time/authority.rs) with the EOP
+    records of eop (zero EOP when None), instead of the GMST rotation."""
     sw = _space_weather(space_weather)
     eph = _ephemeris(ephemeris)
+    fr = _frame(frame, eop)
     sw_key = None if sw is None else (hashlib.sha256(sw[0]).hexdigest(), hashlib.sha256(sw[1]).hexdigest(), sw[2])
     eph_key = tuple(sorted((b, hashlib.sha256(d).hexdigest()) for b, d in eph.items()))
-    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg), sw_key, eph_key)
+    fr_key = (fr[0], None if fr[1] is None else hashlib.sha256(fr[1].tobytes()).hexdigest(), fr[2])
+    key = (hashlib.sha256(text.encode()).hexdigest(), _cfg_key(cfg), sw_key, eph_key, fr_key)
     ctx = _CTX.get(key)
     if ctx is None:
         ctx = N.Context(text, cfg)
@@ -186,6 +212,8 @@ def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None) -
             ctx.set_jb_drivers(sw[0], sw[1], sw[2])
         for body, data in eph.items():
             ctx.set_ephemeris(body, data)
+        if fr[0] != "gmst":
+            ctx.set_frame(fr[0], fr[1], fr[2])
         _CTX[key] = ctx
         while len(_CTX) > _CTX_MAX:
             _CTX.popitem(last=False)[1].close()
@@ -209,12 +237,14 @@ def _srp_in_effect(cfg) -> bool:
 # ------------------------------------------------------------------ scalar API
 def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
               moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-              gravity_field=None, space_weather=None, ephemeris=None):
+              gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None):
     """Propagate one ECI state; sampled, rectified path (lib.rs:237-353).
 
     space_weather = (solfsmy, dtcfile[, (jd_lo, jd_hi)]): JB2008 drivers from
     SET space-weather files; ephemeris = (sun, moon): precomputed catalogues
-    (see ``context``); defaults: the fixed drivers and the analytic series."""
+    (see ``context``); frame="iau2006" with eop: the IAU 2006/2000A
+    Earth-fixed frame; defaults: the fixed drivers, the analytic series and
+    the GMST rotation."""
     init = _six(state_eci, "state_eci")
     if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
         raise ValueError("epoch_jd must be finite and tof_s > 0")
@@ -238,7 +268,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg, space_weather, ephemeris)
+    ctx = context(text, cfg, space_weather, ephemeris, frame, eop)
     t_start = time.perf_counter()
     out, st, steps, evals = ctx.propagate_sampled(init, epoch_jd, tof_s, np.array(grid))
     wall_us = int((time.perf_counter() - t_start) * 1e6)
@@ -270,7 +300,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
 
 def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, srp=True, sun=True, moon=True,
                     atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-                    gravity_field=None, space_weather=None, ephemeris=None):
+                    gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None):
     """Final state with the ground check enforced (lib.rs:361-438).
 
     Raises ValueError for a physically infeasible arc (ground impact, a radius
@@ -282,7 +312,7 @@ def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, s
     cfg = force_config(gravity_order, drag, srp, sun, moon, atm_model, am_ratio, cd, cr, tol, dt_max_s,
                        method, embedded, ground_check=True)
     _equinoctial_of(init, "state_eci")
-    ctx = context(text, cfg, space_weather, ephemeris)
+    ctx = context(text, cfg, space_weather, ephemeris, frame, eop)
     out, st, _, _ = ctx.propagate_final(init, epoch_jd, tof_s)
     status = int(st[0])
     if status == N.ST_GROUND:
@@ -322,22 +352,23 @@ def _batch_cfg(model: dict, embedded: bool):
 
 
 def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctial=False, gravity_field=None,
-                          space_weather=None, ephemeris=None, **model):
+                          space_weather=None, ephemeris=None, frame="gmst", eop=None, **model):
     """Final states of a batch with per-row epoch / duration / ballistics.
 
     The reference's LightyearSession::integrate_variable_final_into
     (session.rs:2325-2430).  Returns (states_eci [n,6], status [n], steps [n],
     rhs_evals [n]); failed rows are NaN."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris)
+    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris, frame, eop)
     return ctx.propagate_final(states, epoch_jd, tof_s, ballistic=ballistic, equinoctial=equinoctial)
 
 
 def propagate_batch_sampled(states, epoch_jd, tof_s, t_eval, *, deltas=False, equinoctial=False,
-                            gravity_field=None, space_weather=None, ephemeris=None, **model):
+                            gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None,
+                            **model):
     """Samples of a batch on one grid; the reference's
     integrate_batch_native_into (batch.rs:247-391) with ``deltas=True``
     (Encke deviations from the initial baseline) or ECI states."""
     text, embedded = _field_text(gravity_field)
-    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris)
+    ctx = context(text, _batch_cfg(model, embedded), space_weather, ephemeris, frame, eop)
     return ctx.propagate_sampled(states, epoch_jd, tof_s, t_eval, deltas=deltas, equinoctial=equinoctial)

@@ -532,6 +532,7 @@ struct bqp_ctx {
     int64_t fseg_cap = 0;
     ft::FrameIntervals* d_fivl = nullptr;
     ft::FrameTab ftab{};
+    bool frame_span = false;  // the table covers a span set once (bqp_ctx_set_frame_span)
 };
 
 namespace {
@@ -637,6 +638,7 @@ int frame_prepare_host(bqp_ctx* ctx, int64_t n, const double* epoch, const doubl
         ctx->ftab = ft::FrameTab{};
         return 0;
     }
+    if (ctx->frame_span) return 0;
     std::vector<std::pair<int32_t, int64_t>> want;
     const double pad = ft::kSegWidth;
     double tmin = INFINITY, tmax = -INFINITY;
@@ -708,6 +710,7 @@ int frame_prepare_dev(bqp_ctx* ctx, int64_t n, const double* d_epoch, double t0,
         ctx->ftab = ft::FrameTab{};
         return 0;
     }
+    if (ctx->frame_span) return 0;  // no readback: the preset span's table stands
     std::vector<double> ep((size_t)n), tf((size_t)n), lo((size_t)n, t0);
     cudaError_t e = cudaSuccess;
     if (n > 0 && d_t0) e = cudaMemcpyAsync(lo.data(), d_t0, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream);
@@ -1363,6 +1366,7 @@ int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t fir
         if (n_records > 0) return fail(BQP_E_ARG, "EOP records are for the IAU frame");
         ctx->frame.reset();
         ctx->ftab = ft::FrameTab{};
+        ctx->frame_span = false;
         return 0;
     }
     if (n_records > 0) {
@@ -1379,6 +1383,22 @@ int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t fir
     }
     ctx->frame.reset(new ft::Authority(e));
     ctx->ftab = ft::FrameTab{};
+    ctx->frame_span = false;
+    return 0;
+}
+
+int bqp_ctx_set_frame_span(bqp_ctx* ctx, double utc_jd_lo, double utc_jd_hi) {
+    if (!ctx) return fail(BQP_E_ARG, "null ctx");
+    if (!ctx->frame) return fail(BQP_E_ARG, "no IAU frame set (bqp_ctx_set_frame)");
+    ctx->frame_span = false;
+    if (utc_jd_lo == 0.0 && utc_jd_hi == 0.0) return 0;
+    if (!(std::isfinite(utc_jd_lo) && std::isfinite(utc_jd_hi) && utc_jd_hi >= utc_jd_lo))
+        return fail(BQP_E_ARG, "bad UTC span");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    const double ep = utc_jd_lo, lo = 0.0, hi = (utc_jd_hi - utc_jd_lo) * 86400.0 + 2.0;
+    if ((rc = frame_prepare_host(ctx, 1, &ep, &lo, &hi))) return rc;
+    ctx->frame_span = true;
     return 0;
 }
 

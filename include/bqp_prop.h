@@ -259,6 +259,12 @@ int bqp_ctx_set_ephemeris(bqp_ctx* ctx, int32_t body, const uint8_t* bytes, int6
 #define BQP_FRAME_GMST 0
 #define BQP_FRAME_IAU2006 1
 int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t first_mjd, int32_t n_records);
+/* Build and upload, once, the IAU frame's segments for the UTC Julian days
+ * [jd_lo, jd_hi]; later calls then launch without reading their epochs back
+ * to the host (the `_device` entry points stay asynchronous), and an
+ * evaluation outside the span fails with BQP_ST_FRAME_TIME.  (0, 0): back to
+ * segments per call. */
+int bqp_ctx_set_frame_span(bqp_ctx* ctx, double utc_jd_lo, double utc_jd_hi);
 
 /* The chain's pieces on the host (no GPU), ERFA-restated (frame_time/
  * iau2006.rs, cio.rs, era.rs): dates are two-part TT Julian days (UT1 for

@@ -106,6 +106,12 @@ def lib():
         L.orc_propagate_srp_batch.restype = None
         L.orc_propagate_srp_batch.argtypes = [C.c_void_p, _dp, C.c_long, _dp, _dp, _dp, _dp, _dp, C.c_int,
                                               _dp, _dp, _ip, _lp, _lp, _ip, C.c_int]
+        L.orc_force_set_frame.restype = None
+        L.orc_force_set_frame.argtypes = [C.c_void_p, C.c_long, C.POINTER(C.c_int64), _dp, _dp]
+        L.orc_frame_rotation.restype = C.c_int
+        L.orc_frame_rotation.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp]
+        L.orc_frame_tai_origin.restype = C.c_double
+        L.orc_frame_tai_origin.argtypes = [C.c_double]
         _lib = L
     return _lib
 
@@ -132,6 +138,26 @@ class Force:
             raise ValueError("oracle: coefficient text rejected")
         if lib().orc_force_set_atm_model(self.h, int(atm_model)) != 0:
             raise ValueError(f"oracle: atm_model {atm_model} is not 4, 5, 6 or 7")
+
+    def set_frame(self, keys=None, segs=None, intervals=None):
+        """The Earth-fixed frame: IAU 2006/2000A segments (keys [n] int64,
+        segs [n][60], intervals [98] as the library exports them), or GMST
+        when keys is None.  The segments are an input: this restates their
+        lookup and evaluation only."""
+        if keys is None:
+            lib().orc_force_set_frame(self.h, -1, None, None, None)
+            return
+        k = np.ascontiguousarray(keys, dtype=np.int64)
+        sg = f64(segs).reshape(-1, 60)
+        iv = f64(intervals).reshape(98)
+        lib().orc_force_set_frame(self.h, k.size, k.ctypes.data_as(C.POINTER(C.c_int64)), _d(sg), _d(iv))
+
+    def frame_rotation(self, tai):
+        t = f64(np.atleast_1d(tai))
+        r = np.zeros((t.size, 9))
+        w = np.zeros((t.size, 3))
+        lib().orc_frame_rotation(self.h, t.size, _d(t), _d(r), _d(w))
+        return r.reshape(-1, 3, 3), w
 
     def set_srp(self, on=True, cr=1.3, p_sun=4.56e-6):
         """Solar radiation pressure with the binary-eclipse coordinator (rows
@@ -431,3 +457,8 @@ def first_crossing_in_step(t_old, t_new, state, bound, max_splits=1_000_000, ear
 
 def no_crossing_certified(m_old, m_new, bound) -> bool:
     return bool(lib().orc_no_crossing_certified(float(m_old), float(m_new), float(bound)))
+
+
+def frame_tai_origin(jd0: float) -> float:
+    """Continuous TAI seconds of t = 0 for a one-part UTC epoch (NaN before 1972)."""
+    return float(lib().orc_frame_tai_origin(float(jd0)))

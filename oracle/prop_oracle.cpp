@@ -53,9 +53,12 @@
 #include <sstream>
 #include <algorithm>
 #include <array>
+#include <map>
+#include <memory>
 #include <cerrno>
 #include <cfloat>
 #include <climits>
+#include <map>
 #include <memory>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1609,6 +1612,89 @@ int first_crossing(double t_old, double t_new, double earth_radius, double max_s
 
 }  // namespace srp
 
+// ------------------------------------------------- IAU 2006/2000A frame
+// The Earth-fixed rotation from the reference's 1800 s frame segments
+// (satpy_core/src/frame_time/authority.rs).  The segments themselves are an
+// input here (their contents are checked against the reference's ERFA-derived
+// fixtures on their own); this restates how a force evaluation finds and
+// evaluates one: the (j, k) index of an instant (authority.rs:416-470), the
+// rotation with its exact derivative and angular velocity (authority.rs:
+// 682-794), and the row's continuous-TAI origin (authority.rs:1162-1190).
+namespace frame {
+struct Seg {
+    double m[3][9], k[3][9], b[4], centre, delta_at;
+};
+struct Table {
+    std::map<int64_t, Seg> segs;  // by (j << 40 | k)
+    int n = 0;
+    double start[48] = {}, delta_at[48] = {};
+    double span_end = 0.0;
+};
+
+bool key_of(const Table& T, double tai, int64_t* key) {
+    if (!std::isfinite(tai) || tai >= T.span_end) return false;
+    int j = -1;
+    for (int q = T.n - 1; q >= 0; --q)
+        if (T.start[q] <= tai) {
+            j = q;
+            break;
+        }
+    if (j < 0) return false;
+    long long k = (long long)std::floor((tai - T.start[j]) / 1800.0);
+    if (k < 0) k = 0;
+    if (j + 1 < T.n) {
+        const long long whole = (long long)std::floor((T.start[j + 1] - T.start[j]) / 1800.0);
+        if (whole > 0 && k >= whole) k = whole - 1;
+    }
+    *key = ((int64_t)j << 40) | (int64_t)k;
+    return true;
+}
+
+// R (row-major GCRS->ITRS) and w (ITRS rate in GCRS) at `tai`.
+bool rotation(const Table& T, double tai, double r[9], double w[3]) {
+    int64_t key;
+    if (!key_of(T, tai, &key)) return false;
+    auto it = T.segs.find(key);
+    if (it == T.segs.end()) return false;
+    const Seg& S = it->second;
+    const double dt = tai - S.centre;
+    const double th = S.b[0] + dt * (S.b[1] + dt * (S.b[2] + dt * S.b[3]));
+    const double sn = std::sin(th), cs = std::cos(th);
+    const double thd = S.b[1] + dt * (2.0 * S.b[2] + dt * 3.0 * S.b[3]);
+    double rd[9];
+    for (int e = 0; e < 9; ++e) {
+        const double a = std::fma(dt, S.k[0][e], S.m[0][e]);
+        const double b = std::fma(dt, S.k[1][e], S.m[1][e]);
+        const double c = std::fma(dt, S.k[2][e], S.m[2][e]);
+        r[e] = std::fma(cs, a, std::fma(sn, b, c));
+        rd[e] = std::fma(thd, std::fma(-sn, a, cs * b), std::fma(cs, S.k[0][e], std::fma(sn, S.k[1][e], S.k[2][e])));
+    }
+    auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    const double wi[3] = {0.5 * (dot(rd + 3, r + 6) - dot(rd + 6, r + 3)), 0.5 * (dot(rd + 6, r) - dot(rd, r + 6)),
+                          0.5 * (dot(rd, r + 3) - dot(rd + 3, r))};
+    for (int i = 0; i < 3; ++i) w[i] = r[i] * wi[0] + r[3 + i] * wi[1] + r[6 + i] * wi[2];
+    return true;
+}
+
+void to_itrs(const double r[9], const double v[3], double o[3]) {
+    for (int i = 0; i < 3; ++i) o[i] = std::fma(r[3 * i], v[0], std::fma(r[3 * i + 1], v[1], r[3 * i + 2] * v[2]));
+}
+void to_gcrs(const double r[9], const double v[3], double o[3]) {
+    for (int i = 0; i < 3; ++i) o[i] = std::fma(r[i], v[0], std::fma(r[3 + i], v[1], r[6 + i] * v[2]));
+}
+
+// Continuous TAI seconds (from 0h TAI of MJD 41684) of t = 0 of a row whose
+// UTC epoch is the one-part Julian day `jd0`; NaN before 1972.  A day that
+// ends in a leap second runs over 86,401 s.
+double tai_origin(double jd0) {
+    const double big = std::floor(jd0 - 0.5) + 0.5;  // the civil day's 0h (rhs.rs:3090-3093)
+    const double day = big - 2400000.5;
+    if (!(day >= tsc::LEAP_MJD[0])) return NAN;
+    const double fd = jd0 - big;
+    return (day - 41684.0) * 86400.0 + tsc::dat(day) + fd * tsc::day_seconds(day);
+}
+}  // namespace frame
+
 struct Force {
     Field field;
     int use_gravity = 1;   // spherical harmonics on (order > 0)
@@ -1625,6 +1711,8 @@ struct Force {
     // srp and cr, p_sun and the row's A/m are all > 0 (rhs.rs:31-36)
     int srp = 0;
     double cr = 0.0, p_sun = 4.56e-6;
+    // Earth-fixed frame: the IAU 2006/2000A segments when set, else GMST
+    std::shared_ptr<frame::Table> frame;
 };
 
 // Sun (body 0) or Moon (1) at a UTC Julian day: the catalogue when set
@@ -1662,9 +1750,12 @@ double density_at(const Force& F, const double pos_itrs[3], const double sun_itr
     return rho;
 }
 
-void drag_acc(const Force& F, const double st[6], double rho, double am, double cd, double acc[3]) {
+void drag_acc(const Force& F, const double st[6], double rho, double am, double cd, double acc[3],
+              const double* w_frame = nullptr) {
     if (cd == 0.0 || am == 0.0 || rho <= 0.0) return;
     double w[3] = {0.0, 0.0, F.omega};
+    if (w_frame)
+        for (int i = 0; i < 3; ++i) w[i] = w_frame[i];
     double vr[3] = {st[3] - (w[1] * st[2] - w[2] * st[1]), st[4] - (w[2] * st[0] - w[0] * st[2]),
                     st[5] - (w[0] * st[1] - w[1] * st[0])};
     double vm[3] = {vr[0] * KM_TO_M, vr[1] * KM_TO_M, vr[2] * KM_TO_M};
@@ -1683,6 +1774,7 @@ struct Rhs {
     double am, cd;
     int side = -1;     // SRP eclipse side of the leg: 1 shadow, 0 lit (-1: SRP off)
     bool bad = false;  // latched invalid-radius gravity error
+    bool frame_bad = false;  // latched: no frame segment at an evaluation's instant
     long evals = 0;
 
     // rhs.rs:3885-4118 -> [dv; a]
@@ -1697,18 +1789,38 @@ struct Rhs {
         double r = std::sqrt(r2);
         double acc[3] = {0, 0, 0};
         double jd = tsc::utc_jd_at(jd0, t);
-        double th = gmst_rad(jd);
-        double s = std::sin(th), c = std::cos(th);
+        // Earth-fixed frame: the IAU segments' rotation, or GMST
+        double fr[9], fw[3];
+        const bool iau = (bool)F->frame;
+        double s = 0.0, c = 1.0;
+        if (iau) {
+            if ((F->use_gravity && F->field.order > 0) || F->drag) {
+                if (!frame::rotation(*F->frame, frame::tai_origin(jd0) + t, fr, fw)) {
+                    frame_bad = true;
+                    for (int i = 0; i < 6; ++i) out[i] = NAN;
+                    return;
+                }
+            }
+        } else {
+            double th = gmst_rad(jd);
+            s = std::sin(th);
+            c = std::cos(th);
+        }
+        auto into = [&](const double* v, double* o) {
+            if (iau) frame::to_itrs(fr, v, o);
+            else eci_to_itrs(s, c, v, o);
+        };
         if (F->use_gravity && F->field.order > 0) {
             double pi[3];
-            eci_to_itrs(s, c, sp, pi);
+            into(sp, pi);
             double ai[3];
             if (!gravity_itrs(F->field, pi, ai)) {
                 bad = true;
                 ai[0] = ai[1] = ai[2] = NAN;
             }
             double ae[3];
-            itrs_to_eci(s, c, ai, ae);
+            if (iau) frame::to_gcrs(fr, ai, ae);
+            else itrs_to_eci(s, c, ai, ae);
             for (int i = 0; i < 3; ++i) acc[i] += ae[i];
             double k = MU / (r2 * r);
             for (int i = 0; i < 3; ++i) acc[i] = std::fma(sp[i], k, acc[i]);
@@ -1719,14 +1831,14 @@ struct Rhs {
             body_position(*F, 0, jd, sun);
             have_sun = true;
             double pi[3], si[3];
-            eci_to_itrs(s, c, sp, pi);
-            eci_to_itrs(s, c, sun, si);
+            into(sp, pi);
+            into(sun, si);
             double rho = density_at(*F, pi, si, jd);
             if (std::isnan(rho) || rho > 0.0) {
                 if (std::isnan(rho)) {
                     for (int i = 0; i < 3; ++i) acc[i] = NAN;
                 } else {
-                    drag_acc(*F, sp, rho, am, cd, acc);
+                    drag_acc(*F, sp, rho, am, cd, acc, iau ? fw : nullptr);
                 }
             }
         }
@@ -1759,7 +1871,7 @@ enum Method { METHOD_DOPRI5 = 0, METHOD_DOP853 = 1, METHOD_DOPRI5_COMPAT = 2, ME
 enum Status {
     ST_SUCCESS = 0, ST_MAX_STEPS = 1, ST_STEP_UNDERFLOW = 2, ST_INVALID_INPUT = 3,
     ST_NON_FINITE = 4, ST_MAX_REJECTS = 5, ST_GRAVITY = 6, ST_REBASE_FAILED = 7,
-    ST_RESTARTS = 8
+    ST_RESTARTS = 8, ST_FRAME_TIME = 17
 };
 
 struct Tab {
@@ -2235,6 +2347,7 @@ int propagate_final(const Job& J, const double eq0[6], double t0, double tf, dou
         st.steps += seg.steps;
         st.evals += seg.evals;
         st.rejects += seg.rejects;
+        if (R.frame_bad) return ST_FRAME_TIME;
         if (R.bad) return ST_GRAVITY;
         if (s != ST_SUCCESS) return s;
         if (!finite6(d)) return ST_NON_FINITE;
@@ -2309,6 +2422,7 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
             st.steps += seg.steps;
             st.evals += seg.evals;
             st.rejects += seg.rejects;
+            if (R.frame_bad) return ST_FRAME_TIME;
             if (R.bad) return ST_GRAVITY;
             int off = hs ? 1 : 0;
             for (int i = 0; i < cnt; ++i) {
@@ -2331,6 +2445,7 @@ int propagate_sampled(const Job& J, const double eq0[6], double t0, double tf,
             st.steps += seg.steps;
             st.evals += seg.evals;
             st.rejects += seg.rejects;
+            if (R.frame_bad) return ST_FRAME_TIME;
             if (R.bad) return ST_GRAVITY;
             if (s != ST_SUCCESS) {
                 *n_written = consumed;
@@ -2949,6 +3064,7 @@ int propagate(const Job& J, const double eq0[6], double t0, double tf, const dou
         LegIn L{ct, seg_tf, {0, 0, 0, 0, 0, 0}, dtmax, dtmax > HCARRY_MIN_DTMAX ? hcarry : 0.0, &root, false};
         LegOut O;
         leg(R, J.C, G, L, O, st, sk, cur);
+        if (R.frame_bad) return done(ST_FRAME_TIME);
         if (R.bad) return done(ST_GRAVITY);
         if (dtmax > HCARRY_MIN_DTMAX && std::isfinite(O.fch) && O.fch > 0.0) hcarry = O.fch;
         // a handler error, or complete_non_eclipse_segment's failed solver status
@@ -2976,6 +3092,7 @@ int propagate(const Job& J, const double eq0[6], double t0, double tf, const dou
         LegIn Lr{a, b, {0, 0, 0, 0, 0, 0}, std::min(dtmax, REFINE_STEP_S), 0.0, &root, false};
         LegOut Or;
         leg(Rr, J.C, G, Lr, Or, st, sk, replay_eq);
+        if (Rr.frame_bad) return done(ST_FRAME_TIME);
         if (Rr.bad) return done(ST_GRAVITY);
         if (!Or.stopped) {
             if (Or.status != ST_SUCCESS) return done(Or.status >= ENVELOPE ? Or.status : BRACKET);
@@ -3026,6 +3143,7 @@ int propagate(const Job& J, const double eq0[6], double t0, double tf, const dou
             LegIn Lp{base_t, proof_old_t, {0, 0, 0, 0, 0, 0},
                      std::min(std::min(dtmax, REFINE_STEP_S), std::fabs(proof_old_t - base_t)), 0.0, &root, false};
             leg(Rp, J.C, G, Lp, Op, st, sk, base_eq);
+            if (Rp.frame_bad) return done(ST_FRAME_TIME);
             if (Rp.bad) return done(ST_GRAVITY);
             if (Op.stopped) {
                 const double ft = Op.br.t_old;
@@ -3058,6 +3176,7 @@ int propagate(const Job& J, const double eq0[6], double t0, double tf, const dou
         for (int i = 0; i < 6; ++i) Lw.y0[i] = pdelta[i];
         LegOut Ow;
         leg(Rw, J.C, G, Lw, Ow, st, sk, base_eq);
+        if (Rw.frame_bad) return done(ST_FRAME_TIME);
         if (Rw.bad) return done(ST_GRAVITY);
         if (!Ow.stopped) return done(Ow.status >= ENVELOPE ? Ow.status : BRACKET);
         // validate_eclipse_root_commit (1879-1926)
@@ -3365,6 +3484,44 @@ void orc_propagate_sampled_batch(void* f, const double* ctrl, long n, const doub
 }
 
 // Solar radiation pressure switches (ForceConfig force_flags SRP, cr, p_sun).
+// Earth-fixed frame of the force model: n IAU segments (keys [n], segs
+// [n][60] as M0..M2, K0..K2, theta cubic, centre, TAI - UTC) over the leap
+// intervals ivl[98] (count, 48 starts, 48 TAI - UTC, span end); n < 0: GMST.
+void orc_force_set_frame(void* f, long n, const int64_t* keys, const double* segs, const double* ivl) {
+    Force* F = (Force*)f;
+    if (n < 0) {
+        F->frame.reset();
+        return;
+    }
+    auto T = std::make_shared<frame::Table>();
+    T->n = (int)ivl[0];
+    for (int i = 0; i < 48; ++i) {
+        T->start[i] = ivl[1 + i];
+        T->delta_at[i] = ivl[49 + i];
+    }
+    T->span_end = ivl[97];
+    for (long i = 0; i < n; ++i) {
+        frame::Seg S;
+        std::memcpy(&S, segs + 60 * i, sizeof(S));
+        T->segs[keys[i]] = S;
+    }
+    F->frame = T;
+}
+
+int orc_frame_rotation(void* f, long n, const double* tai, double* r, double* w) {
+    Force* F = (Force*)f;
+    int bad = 0;
+    for (long i = 0; i < n; ++i)
+        if (!F->frame || !frame::rotation(*F->frame, tai[i], r + 9 * i, w + 3 * i)) {
+            for (int e = 0; e < 9; ++e) r[9 * i + e] = NAN;
+            for (int e = 0; e < 3; ++e) w[3 * i + e] = NAN;
+            bad = 1;
+        }
+    return bad;
+}
+
+double orc_frame_tai_origin(double jd0) { return frame::tai_origin(jd0); }
+
 void orc_force_set_srp(void* f, int on, double cr, double p_sun) {
     Force* F = (Force*)f;
     F->srp = on;
