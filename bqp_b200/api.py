@@ -186,7 +186,7 @@ def _frame(frame, eop):
     return frame, np.frombuffer(data, dtype="<f8").reshape(-1, 5).astype(np.float64), 41684
 
 
-def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None, frame="gmst",
+def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None, frame="iau2006",
             eop=None) -> N.Context:
     """A cached native context for (field text, configuration, space-weather
     files, ephemeris catalogues).  With space_weather the JB2008 drivers come
@@ -194,10 +194,11 @@ def context(text: str, cfg: N.ForceConfig, space_weather=None, ephemeris=None, f
     reference's compiled driver catalogue, jb_rs/src/drivers.rs) instead of
     the fixed configured drivers; with ephemeris the Sun and / or Moon come
     from precomputed "DUST" catalogues (the reference's precomputed_ephem.rs)
-    instead of the analytic series; with frame="iau2006" gravity and drag
-    take the Earth-fixed frame from the IAU 2006/2000A chain (the reference's
+    instead of the analytic series.  Gravity and drag take the Earth-fixed
+    frame from the IAU 2006/2000A chain (frame="iau2006", the reference's
     frame authority, satpy_core/src/frame_time/authority.rs) with the EOP
-    records of eop (zero EOP when None), instead of the GMST rotation."""
+    records of eop (zero EOP when None), or from the GMST rotation
+    (frame="gmst")."""
     sw = _space_weather(space_weather)
     eph = _ephemeris(ephemeris)
     fr = _frame(frame, eop)
@@ -237,14 +238,15 @@ def _srp_in_effect(cfg) -> bool:
 # ------------------------------------------------------------------ scalar API
 def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag=True, srp=True, sun=True,
               moon=True, atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-              gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None):
+              gravity_field=None, space_weather=None, ephemeris=None, frame="iau2006", eop=None):
     """Propagate one ECI state; sampled, rectified path (lib.rs:237-353).
 
     space_weather = (solfsmy, dtcfile[, (jd_lo, jd_hi)]): JB2008 drivers from
     SET space-weather files; ephemeris = (sun, moon): precomputed catalogues
-    (see ``context``); frame="iau2006" with eop: the IAU 2006/2000A
-    Earth-fixed frame; defaults: the fixed drivers, the analytic series and
-    the GMST rotation."""
+    (see ``context``); defaults: the fixed drivers, the analytic series and,
+    as in the reference (rhs.rs:3113-3174), the IAU 2006/2000A Earth-fixed
+    frame -- with zero EOP unless eop passes the reference's sealed table or
+    records (frame="gmst": the GMST z-rotation instead)."""
     init = _six(state_eci, "state_eci")
     if not (np.isfinite(epoch_jd) and np.isfinite(tof_s) and tof_s > 0):
         raise ValueError("epoch_jd must be finite and tof_s > 0")
@@ -300,7 +302,7 @@ def propagate(state_eci, epoch_jd, tof_s, times_s=None, *, gravity_order=5, drag
 
 def propagate_final(state_eci, epoch_jd, tof_s, *, gravity_order=5, drag=True, srp=True, sun=True, moon=True,
                     atm_model=7, am_ratio=0.01, cd=2.2, cr=1.3, tol=1e-8, dt_max_s=300.0, method="vern7",
-                    gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None):
+                    gravity_field=None, space_weather=None, ephemeris=None, frame="iau2006", eop=None):
     """Final state with the ground check enforced (lib.rs:361-438).
 
     Raises ValueError for a physically infeasible arc (ground impact, a radius
@@ -352,7 +354,7 @@ def _batch_cfg(model: dict, embedded: bool):
 
 
 def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctial=False, gravity_field=None,
-                          space_weather=None, ephemeris=None, frame="gmst", eop=None, **model):
+                          space_weather=None, ephemeris=None, frame="iau2006", eop=None, **model):
     """Final states of a batch with per-row epoch / duration / ballistics.
 
     The reference's LightyearSession::integrate_variable_final_into
@@ -364,7 +366,7 @@ def propagate_batch_final(states, epoch_jd, tof_s, *, ballistic=None, equinoctia
 
 
 def propagate_batch_sampled(states, epoch_jd, tof_s, t_eval, *, deltas=False, equinoctial=False,
-                            gravity_field=None, space_weather=None, ephemeris=None, frame="gmst", eop=None,
+                            gravity_field=None, space_weather=None, ephemeris=None, frame="iau2006", eop=None,
                             **model):
     """Samples of a batch on one grid; the reference's
     integrate_batch_native_into (batch.rs:247-391) with ``deltas=True``

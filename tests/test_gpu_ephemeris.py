@@ -137,7 +137,7 @@ def test_python_surface_takes_the_catalogues():
     states = workloads.leo_states(4, seed=12)
     text = workloads.synthetic_field(8)
     got, st, _, _ = api.propagate_batch_final(states, EPOCH, 3600.0, gravity_order=8, gravity_field=text,
-                                              tol=1e-10, ephemeris=cats)
+                                              tol=1e-10, ephemeris=cats, frame="gmst")
     ref, st2, _, _ = ctx_for(text, 8, cats).propagate_final(states, EPOCH, 3600.0, ballistic=np.array([0.01, 2.2]))
     assert (st == 0).all() and (st2 == 0).all()
     assert np.abs(got[:, :3] - ref[:, :3]).max() < 1e-5

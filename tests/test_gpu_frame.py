@@ -172,10 +172,16 @@ def test_python_surface_takes_the_frame():
     eop = eop_records(first, 30)
     r_iau = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False,
                                 frame="iau2006", eop=(eop, first))
-    r_gm = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False)
+    r_gm = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False,
+                               frame="gmst")
     assert np.linalg.norm(r_iau[:3] - r_gm[:3]) > 1e-4
+    # the default frame is the IAU one (zero EOP), as in the reference
+    r_def = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False)
+    r_zero = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False,
+                                 frame="iau2006")
+    assert np.array_equal(r_def, r_zero) and np.linalg.norm(r_def[:3] - r_iau[:3]) > 0.0
     # a sealed-format byte table from MJD 41684 is accepted as is
-    sealed = np.zeros((60320 - 41684, 5))
+    sealed = np.zeros((first + 40 - 41684, 5))
     sealed[first - 41684:first - 41684 + 30] = eop
     r_sealed = api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False,
                                    frame="iau2006", eop=sealed.astype("<f8").tobytes())

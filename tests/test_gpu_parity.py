@@ -568,11 +568,21 @@ def test_reference_smoke_sequence():
     assert np.linalg.norm(fs[:3] - full["states_eci"][-1][:3]) < 1e-3
 
 
+def oracle_iau_frame(F, epoch, span_s):
+    """Give the oracle the zero-EOP IAU segments of [epoch, epoch + span_s]
+    (the Python surface's default frame)."""
+    auth = N.FrameAuthority()
+    tai0 = N.tai_seconds(epoch)[0]
+    keys, segs = auth.segments(tai0 - 1800.0, tai0 + span_s + 1800.0)
+    F.set_frame(keys, segs, auth.intervals()["raw"])
+
+
 def test_python_defaults_match_oracle():
     """api.propagate with every reference default but srp (DIR-R6 at degree
     5, JB2008 atm_model 7 with the default drivers, Sun/Moon, Vern7 at tol
-    1e-8, dt_max 300 s) against the oracle's sampled path with the same
-    settings, on a 300 s grid over one hour."""
+    1e-8, dt_max 300 s, the IAU 2006/2000A frame with zero EOP) against the
+    oracle's sampled path with the same settings, on a 300 s grid over one
+    hour."""
     from bqp_b200 import api as A
 
     eci = A.kep_to_eci(np.array([6778.137, 0.001, 51.6, 30.0, 40.0, 50.0]))
@@ -581,6 +591,7 @@ def test_python_defaults_match_oracle():
     assert out["completed"] and np.array_equal(out["times_s"], grid)
     text = A._DEFAULT_FIELD.read_text()
     F = O.Force(text, 5, drag=True, sun=True, moon=True, atm_model=7)
+    oracle_iau_frame(F, EPOCH, 3600.0)
     equ, rc = O.eci2equinoc(eci)
     assert rc == 0
     d, st, steps, evals, nw = O.propagate_sampled(F, O.ctrl("vern7", eps=1e-8, dt_max=300.0), equ, EPOCH, 3600.0,

@@ -170,7 +170,8 @@ def test_python_surface_takes_the_tables():
     sol, dtc = tables(2460300, 24, seed=8)
     states = workloads.leo_states(4, seed=11)
     got, st, _, _ = api.propagate_batch_final(states, EPOCH, 3600.0, gravity_order=8, gravity_field=
-                                              workloads.synthetic_field(8), tol=1e-10, space_weather=(sol, dtc))
+                                              workloads.synthetic_field(8), tol=1e-10, space_weather=(sol, dtc),
+                                              frame="gmst")
     cfg_ctx = ctx_for(workloads.synthetic_field(8), 8, sol, dtc)
     assert (st == 0).all()
     ref, st2, _, _ = cfg_ctx.propagate_final(states, EPOCH, 3600.0, ballistic=np.array([0.01, 2.2]))

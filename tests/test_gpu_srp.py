@@ -121,14 +121,18 @@ def test_srp_envelope_and_failure_reporting(engine):
 def test_python_defaults_with_srp_match_oracle():
     """api.propagate with every reference default, SRP included (DIR-R6 at
     degree 5, JB2008 atm_model 7, Sun/Moon, SRP with cr 1.3, Vern7 at tol
-    1e-8, dt_max 300 s), against the oracle's coordinator on a 300 s grid
-    over three hours."""
+    1e-8, dt_max 300 s, the IAU 2006/2000A frame with zero EOP), against the
+    oracle's coordinator on a 300 s grid over three hours."""
     eci = api.kep_to_eci(np.array([6778.137, 0.001, 51.6, 30.0, 40.0, 50.0]))
     grid = np.arange(0.0, 3 * 3600.0 + 1.0, 300.0)
     out = api.propagate(eci, EPOCH, grid[-1], times_s=grid)
     assert out["completed"] and np.array_equal(out["times_s"], grid), out["terminal_event"]
     F = O.Force(api._DEFAULT_FIELD.read_text(), 5, drag=True, sun=True, moon=True, atm_model=7)
     F.set_srp(True, 1.3)
+    auth = N.FrameAuthority()
+    tai0 = N.tai_seconds(EPOCH)[0]
+    keys, segs = auth.segments(tai0 - 1800.0, tai0 + grid[-1] + 1800.0)
+    F.set_frame(keys, segs, auth.intervals()["raw"])
     equ, rc = O.eci2equinoc(eci)
     assert rc == 0
     _, smp, st, steps, _, nw = O.propagate_srp_batch(F, O.ctrl("vern7", eps=1e-8, dt_max=300.0), equ[None], EPOCH,
