@@ -98,9 +98,15 @@ def test_noalloc_refuses_forms_it_would_not_run():
     with pytest.raises(N.NativeError) as e:
         ctx.propagate_final_noalloc(s, EPOCH, 600.0)
     assert e.value.code == N.E_UNSUPPORTED and "SRP" in str(e.value)
-    # the same context in plain FP64 without SRP runs
+    # the IAU frame builds its segment table per call: refused as well
     cfg.force_flags &= ~N.FORCE_SRP
     ctx.set_config(cfg)
+    ctx.set_frame("iau2006")
+    with pytest.raises(N.NativeError) as e:
+        ctx.propagate_final_noalloc(s, EPOCH, 600.0)
+    assert e.value.code == N.E_UNSUPPORTED and "IAU" in str(e.value)
+    # the same context in plain FP64 without SRP, in the GMST frame, runs
+    ctx.set_frame("gmst")
     out, st, _, _ = ctx.propagate_final_noalloc(s, EPOCH, 600.0)
     assert (st == 0).all() and np.isfinite(out).all()
 
