@@ -161,3 +161,34 @@ def test_out_of_span_instants_are_nan():
     r, _ = auth2.rotation([end - 86400.0 * 5, end - 3600.0])
     assert np.isfinite(r[0]).all()
     assert np.isnan(r[1]).all()  # its four-node interpolation runs past the table
+
+
+def test_oracle_restatement_of_the_lookup_matches_the_library():
+    """The oracle's own segment lookup, rotation and TAI origin (its frame
+    namespace) against the library's host authority on the same segments."""
+    from oracle import oracle as O
+    from bqp_b200 import workloads
+
+    auth = N.FrameAuthority()
+    rng = np.random.default_rng(11)
+    # UTC epochs over 1973-2049 and the half day either side of three leap seconds
+    jd = np.concatenate([rng.uniform(2441684.5, 2469807.0, 400),
+                         2457754.5 + rng.uniform(-0.5, 0.5, 50),
+                         2450630.5 + rng.uniform(-0.5, 0.5, 50),
+                         2441499.5 + rng.uniform(-0.5, 0.5, 50)])
+    lib_tai = N.tai_seconds(jd)
+    orc_tai = np.array([O.frame_tai_origin(j) for j in jd])
+    assert np.all(np.abs(lib_tai - orc_tai) <= 2e-6)
+    assert np.isnan(O.frame_tai_origin(2441000.5))  # 1971
+    # rotations at instants inside one table of segments
+    t0 = N.tai_seconds(2460310.5)[0]
+    keys, segs = auth.segments(t0, t0 + 3 * 86400.0)
+    F = O.Force(workloads.synthetic_field(2), 2)
+    F.set_frame(keys, segs, auth.intervals()["raw"])
+    tai = t0 + rng.uniform(0.0, 3 * 86400.0, 500)
+    r_lib, w_lib = auth.rotation(tai)
+    r_orc, w_orc = F.frame_rotation(tai)
+    assert np.array_equal(r_lib, r_orc) and np.array_equal(w_lib, w_orc)
+    # outside the segments it was given the oracle has none
+    r_out, _ = F.frame_rotation([t0 - 7200.0, t0 + 4 * 86400.0])
+    assert np.isnan(r_out).all()
