@@ -26,10 +26,16 @@ def fixed_step_ctx(text, order, flags):
     return N.Context(text, cfg)
 
 
-def oracle_sigma_propagate(text, order, flags, mean, cov, tf, bal, sigma_set, alpha, beta, kappa):
+def oracle_sigma_propagate(text, order, flags, mean, cov, tf, bal, sigma_set, alpha, beta, kappa, iau=False):
     # the atmosphere of N.default_config(), the reference's default (model 7)
     F = O.Force(text, order, drag=bool(flags & 1), sun=bool(flags & 4), moon=bool(flags & 8),
                 atm_model=N.default_config().atm_model)
+    if iau:
+        # the zero-EOP IAU 2006/2000A segments of the arc, as the context builds them
+        auth = N.FrameAuthority()
+        tai0 = N.tai_seconds(EPOCH)[0]
+        keys, segs = auth.segments(tai0 - 1800.0, tai0 + float(np.max(tf)) + 1800.0)
+        F.set_frame(keys, segs, auth.intervals()["raw"])
     ctl = O.ctrl("dop853", eps=1e3, dt_max=60.0)
     wm, wc, _ = U.weights(sigma_set, alpha, beta, kappa)
     means, covs = [], []
@@ -70,6 +76,32 @@ def test_sigma_propagate_matches_oracle(sigma_set, alpha, mean_tol, cov_tol):
     rel = np.linalg.norm(c - oc, axis=(1, 2)) / np.linalg.norm(oc, axis=(1, 2))
     assert rel.max() <= cov_tol, rel.max()
     assert np.allclose(c, np.transpose(c, (0, 2, 1)), rtol=0, atol=0)  # symmetrised
+
+
+def test_sigma_propagate_in_the_iau_frame_matches_oracle():
+    """The sigma rows generated on the device carry their object's epoch into
+    the IAU frame's per-call segment table (the epochs are read back from the
+    device)."""
+    order, flags = 20, 1 | 4 | 8
+    text = workloads.synthetic_field(order)
+    n = 4
+    mean, cov = workloads.ukf_objects(n, seed=6)
+    bal = workloads.leo_ballistics(n, seed=6)
+    tf = 0.5 * workloads.orbit_period_s(mean)
+    ctx = fixed_step_ctx(text, order, flags)
+    ctx.set_frame("iau2006")
+    m, c, st, _ = ctx.sigma_propagate(mean, cov, EPOCH, tf, sigma_set="julier7", alpha=1e-3, beta=2.0,
+                                      kappa=0.0, ballistic=bal)
+    assert (st == 0).all()
+    om, oc = oracle_sigma_propagate(text, order, flags, mean, cov, tf, bal, "julier7", 1e-3, 2.0, 0.0, iau=True)
+    assert np.abs(m - om).max() <= 1e-8, np.abs(m - om).max()
+    rel = np.linalg.norm(c - oc, axis=(1, 2)) / np.linalg.norm(oc, axis=(1, 2))
+    assert rel.max() <= 1e-7, rel.max()
+    # and it is not the GMST answer
+    g = fixed_step_ctx(text, order, flags)
+    gm, _, _, _ = g.sigma_propagate(mean, cov, EPOCH, tf, sigma_set="julier7", alpha=1e-3, beta=2.0, kappa=0.0,
+                                    ballistic=bal)
+    assert np.abs(gm - m).max() > 1e-6
 
 
 def test_sigma_propagate_repair_and_failure():
