@@ -36,7 +36,9 @@ by the device per trajectory.
 workload and prints its line.  ``--atm-model 7`` measures the reference's
 default (fitted) JB2008 profile instead of the exact model; ``--srp`` adds
 solar radiation pressure through the binary-eclipse coordinator (cr 1.3) on
-both arms.
+both arms; ``--frame iau2006`` takes the Earth-fixed frame from the IAU
+2006/2000A segments (zero EOP; the reference's production frame) instead of
+the GMST rotation, on both arms (the oracle evaluates the same segments).
 """
 from __future__ import annotations
 
