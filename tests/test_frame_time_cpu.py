@@ -192,3 +192,22 @@ def test_oracle_restatement_of_the_lookup_matches_the_library():
     # outside the segments it was given the oracle has none
     r_out, _ = F.frame_rotation([t0 - 7200.0, t0 + 4 * 86400.0])
     assert np.isnan(r_out).all()
+
+
+def test_python_frame_arguments():
+    """frame= / eop= of the Python calls, parsed without a GPU."""
+    from bqp_b200 import api
+
+    assert api._frame("iau2006", None)[0] == "iau2006" and api._frame("gmst", None)[1] is None
+    rec = np.arange(20.0).reshape(4, 5)
+    name, got, first = api._frame("iau2006", (rec, 60300))
+    assert np.array_equal(got, rec) and first == 60300
+    # the sealed layout: 40-byte records from MJD 41684, passed as bytes
+    name, got, first = api._frame("iau2006", rec.astype("<f8").tobytes())
+    assert np.array_equal(got, rec) and first == 41684
+    with pytest.raises(ValueError):
+        api._frame("iau2006", b"\0" * 41)  # not whole records
+    with pytest.raises(ValueError):
+        api._frame("gmst", (rec, 60300))  # EOP belong to the IAU frame
+    with pytest.raises(ValueError):
+        api._frame("itrf93", None)
