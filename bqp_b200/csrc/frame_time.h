@@ -105,6 +105,11 @@ BQP_HD int32_t segment_slot(const FrameTab& T, double tai) {
     int64_t k;
     if (!T.ivl || !segment_index(*T.ivl, tai, &j, &k)) return -1;
     const int64_t key = seg_key(j, k);
+    if (T.nseg <= 0) return -1;
+    // a table built for one span holds consecutive keys: the key's offset
+    // from the first one is its slot (one load); otherwise binary search
+    const int64_t g = key - T.key[0];
+    if (g >= 0 && g < T.nseg && T.key[g] == key) return (int32_t)g;
     int32_t lo = 0, hi = T.nseg - 1;
     while (lo <= hi) {
         const int32_t mid = (lo + hi) >> 1;

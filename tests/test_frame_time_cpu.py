@@ -211,3 +211,68 @@ def test_python_frame_arguments():
         api._frame("gmst", (rec, 60300))  # EOP belong to the IAU frame
     with pytest.raises(ValueError):
         api._frame("itrf93", None)
+
+
+def test_device_segment_lookup_on_the_host(tmp_path):
+    """The kernels' segment lookup (segment_index + segment_slot of
+    frame_time.h, host-compiled here) on key tables with one span (the
+    offset fast path), with gaps and across a leap interval (the binary
+    search), against the library authority's own (j, k) keys."""
+    import subprocess
+
+    csrc = Path(__file__).resolve().parents[1] / "bqp_b200" / "csrc"
+    src = tmp_path / "lookup.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <vector>
+#include "frame_time.h"
+using namespace bqp::ft;
+int main() {
+    // three intervals 1000 s, 5000 s and 1e9 s long from t = 12
+    FrameIntervals I{};
+    I.n = 3;
+    I.start[0] = 12.0; I.start[1] = 1012.0; I.start[2] = 6013.0;
+    I.span_end = 1e9;
+    // keys: interval 0 (k 0), interval 1 (k 0, 1), interval 2 (k 0..3, 7, 8)
+    std::vector<long long> k = {seg_key(0, 0), seg_key(1, 0), seg_key(1, 1), seg_key(2, 0), seg_key(2, 1),
+                                seg_key(2, 2), seg_key(2, 3), seg_key(2, 7), seg_key(2, 8)};
+    std::vector<int64_t> keys(k.begin(), k.end());
+    FrameTab T{1, (int32_t)keys.size(), nullptr, keys.data(), &I};
+    const double t[] = {5.0, 12.0, 500.0, 1011.9, 1012.0, 2811.9, 2812.0, 6012.9, 6013.0, 6013.0 + 3 * 1800 + 5,
+                        6013.0 + 5 * 1800, 6013.0 + 7 * 1800 + 1, 6013.0 + 8 * 1800 + 1799, 6013.0 + 9 * 1800, 2e9};
+    for (double x : t) {
+        int32_t j = -1;
+        int64_t kk = -1;
+        const bool ok = segment_index(I, x, &j, &kk);
+        std::printf("%d %d %lld %d\n", ok ? 1 : 0, j, (long long)kk, segment_slot(T, x));
+    }
+    // one span only: every slot by the offset path
+    std::vector<int64_t> one;
+    for (int q = 0; q < 40; ++q) one.push_back(seg_key(2, 100 + q));
+    FrameTab T1{1, 40, nullptr, one.data(), &I};
+    int bad = 0;
+    for (int q = 0; q < 40; ++q) bad += segment_slot(T1, 6013.0 + (100 + q) * 1800.0 + 900.0) != q;
+    std::printf("%d\n", bad);
+    return 0;
+}
+''')
+    exe = tmp_path / "lookup"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", str(csrc), str(src), "-o", str(exe)], check=True)
+    lines = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = [tuple(int(v) for v in ln.split()) for ln in lines[:15]]
+    assert got == [
+        (0, -1, -1, -1),          # before the first interval
+        (1, 0, 0, 0), (1, 0, 0, 0), (1, 0, 0, 0),  # interval 0: 1000 s, one (short) segment
+        (1, 1, 0, 1),             # interval 1 starts
+        (1, 1, 0, 1),             # 1799.9 s in: still k 0
+        (1, 1, 1, 2),             # k 1, the last: it absorbs the remainder (5000 s = 2 x 1800 + 1400)
+        (1, 1, 1, 2),
+        (1, 2, 0, 3),             # interval 2
+        (1, 2, 3, 6),
+        (1, 2, 5, -1),            # a gap in the table: no segment
+        (1, 2, 7, 7),
+        (1, 2, 8, 8),
+        (1, 2, 9, -1),            # past the table's last key
+        (0, -1, -1, -1),          # past the span
+    ], got
+    assert lines[15].strip() == "0"
