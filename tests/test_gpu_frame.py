@@ -192,3 +192,35 @@ def test_python_surface_takes_the_frame():
     with pytest.raises(ValueError):
         api.propagate_final(state, EPOCH, 3600.0, gravity_order=8, gravity_field=text, srp=False,
                             frame="itrf")
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_preset_span_gives_the_same_bits(engine):
+    """Segments built once for a span (bqp_ctx_set_frame_span) and per call
+    are the same segments: the same rows give the same bits, and a second
+    run of the same batch repeats them."""
+    order, eps, n = 12, 1e-10, 64
+    text = workloads.synthetic_field(order)
+    states = workloads.leo_states(n, seed=31)
+    bal = workloads.leo_ballistics(n, seed=31)
+    epochs = EPOCH + np.linspace(0.0, 1.0, n)
+    tf = 3 * 3600.0
+    per_call = make_ctx(text, order, engine, eps)
+    per_call.set_frame("iau2006")
+    a = per_call.propagate_final(states, epochs, tf, ballistic=bal)
+    b = per_call.propagate_final(states, epochs, tf, ballistic=bal)
+    span = make_ctx(text, order, engine, eps)
+    span.set_frame("iau2006")
+    span.set_frame_span(EPOCH - 0.5, EPOCH + 2.0)
+    c = span.propagate_final(states, epochs, tf, ballistic=bal)
+    assert (a[1] == 0).all()
+    for other in (b, c):
+        assert np.array_equal(a[0], other[0]) and np.array_equal(a[1], other[1])
+        assert np.array_equal(a[2], other[2]) and np.array_equal(a[3], other[3])
+    # a row outside the preset span fails with the frame-time status
+    late = span.propagate_final(states[:2], EPOCH + 3.0, tf, ballistic=bal[:2])
+    assert (late[1] == N.ST_FRAME_TIME).all()
+    # back to per-call segments
+    span.set_frame_span(0.0, 0.0)
+    late = span.propagate_final(states[:2], EPOCH + 3.0, tf, ballistic=bal[:2])
+    assert (late[1] == 0).all()
