@@ -276,3 +276,60 @@ int main() {
         (0, -1, -1, -1),          # past the span
     ], got
     assert lines[15].strip() == "0"
+
+
+def test_gmst_time_staircase_against_continuous_tai():
+    """Why the IAU frame takes fewer steps at eps 1e-12 than the GMST frame:
+    the GMST angle is read from a one-part UTC Julian day (~2.46e6), whose
+    resolution is 2^-31 d = 40 us, so the Earth-fixed frame moves in steps
+    of ~2.9e-9 rad; the IAU rotation reads continuous TAI seconds (2.4e-7 s
+    resolution at 1.6e9 s) and moves smoothly."""
+    import ctypes as C
+
+    from oracle import oracle as O
+
+    L = O.lib()
+    L.orc_gmst.restype = C.c_double
+    L.orc_gmst.argtypes = [C.c_double]
+    jd0 = 2460310.5
+    t = np.arange(0.0, 400e-6, 1e-6)  # 400 us in 1 us steps
+    g = np.array([L.orc_gmst(jd0 + x / 86400.0) for x in t])
+    jumps = np.flatnonzero(np.diff(g) != 0.0)
+    assert 5 <= jumps.size <= 15  # one jump per 40 us
+    step = np.max(np.abs(np.diff(g)))
+    assert 2e-9 < step < 4e-9
+    auth = N.FrameAuthority()
+    tai0 = N.tai_seconds(jd0)[0]
+    r, _ = auth.rotation(tai0 + t)
+    d = np.abs(np.diff(r[:, 0, 0]))
+    assert np.count_nonzero(d) > 300  # a new value almost every microsecond
+    assert d.max() < 1e-9
+
+
+def test_staircase_costs_steps_at_the_tightest_tolerance():
+    """The same arcs (8 of the bench's LEO rows, 70x70 + JB2008 + Sun/Moon,
+    one 5400 s segment, DOP853 eps 1e-12) in the oracle: the GMST frame's
+    staircase makes the step controller take many more evaluations than the
+    IAU frame's smooth rotation; at eps 1e-10 the two cost the same."""
+    from bqp_b200 import workloads
+    from oracle import oracle as O
+
+    text = workloads.synthetic_field(70)
+    states = workloads.leo_states(65536, seed=0)[::8192]
+    bal = workloads.leo_ballistics(65536, seed=0)[::8192]
+    equ = np.array([O.eci2equinoc(s)[0] for s in states])
+    epoch = workloads.EPOCH_JD
+    F = O.Force(text, 70, drag=True, sun=True, moon=True)
+    auth = N.FrameAuthority()
+    tai0 = N.tai_seconds(epoch)[0]
+    keys, segs = auth.segments(tai0 - 1800.0, tai0 + 5400.0 + 1800.0)
+    ev = {}
+    for eps in (1e-12, 1e-10):
+        F.set_frame()
+        _, s1, _, e1 = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, epoch, 5400.0, bal)
+        F.set_frame(keys, segs, auth.intervals()["raw"])
+        _, s2, _, e2 = O.propagate_final_batch(F, O.ctrl("dop853", eps=eps), equ, epoch, 5400.0, bal)
+        assert (s1 == 0).all() and (s2 == 0).all()
+        ev[eps] = (e1.sum(), e2.sum())
+    assert ev[1e-12][1] < 0.8 * ev[1e-12][0], ev
+    assert abs(ev[1e-10][1] - ev[1e-10][0]) < 0.05 * ev[1e-10][0], ev
