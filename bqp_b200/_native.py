@@ -145,6 +145,7 @@ SIGNATURES = [
                                                       C.c_int32, _dp]),
     ("bqp_frame_derivatives", C.c_int, [C.c_int32] * 5 + [C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
                                                            C.c_int32, _dp, _dp, _dp]),
+    ("bqp_frame_eop_from_finals", C.c_int64, [C.c_char_p, C.c_int64, C.c_int64, _ip, _dp]),
     ("bqp_frame_authority_new", _vp, [_dp, C.c_int32, C.c_int32]),
     ("bqp_frame_authority_free", None, [_vp]),
     ("bqp_frame_authority_intervals", C.c_int, [_vp, _dp]),
@@ -699,6 +700,21 @@ def frame_derivatives(epoch, policy=0, h=0.25, eop=None, first_mjd=0):
     if rc != 0:
         raise ValueError(f"frame chain failed ({rc})")
     return r.reshape(3, 3), rd.reshape(3, 3), rdd.reshape(3, 3)
+
+
+def eop_from_finals(finals):
+    """(records [n][5], first_mjd) from IERS finals2000A text (str, bytes or
+    a path): the contiguous run of complete days, in the units of the sealed
+    table (x_p, y_p arcsec, UT1-UTC s, dX, dY mas).  Pass it as eop=."""
+    data = _text_bytes(finals)
+    first = C.c_int32(0)
+    n = lib().bqp_frame_eop_from_finals(data, len(data), 0, C.byref(first), None)
+    if n < 0:
+        raise ValueError("finals text rejected (a day given twice)")
+    rec = np.zeros((max(n, 0), 5))
+    if n > 0:
+        lib().bqp_frame_eop_from_finals(data, len(data), n, C.byref(first), dptr(rec))
+    return rec, int(first.value)
 
 
 class FrameAuthority:

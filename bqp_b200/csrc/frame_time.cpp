@@ -11,6 +11,8 @@
 #include "frame_time_host.h"
 
 #include <algorithm>
+#include <array>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -920,3 +922,63 @@ int64_t bqp_frame_authority_segments(bqp_frame_authority* h, double lo, double h
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ IERS finals text
+// Earth-orientation records from IERS finals2000A text, by the reference's
+// column rules (frame_time/eop.rs load_eop): lines of at least 125
+// characters, MJD in columns 7..15, the three I/P flags at 16, 57 and 95,
+// x_p 18..27 and y_p 37..46 (arcsec), UT1-UTC 58..68 (s), dX 97..106 and
+// dY 116..125 (mas).  Rows whose flags or fields fail are skipped; the
+// table is the contiguous run of days from the first complete one.
+namespace {
+bool fixed_field(const char* line, int start, int width, double* out) {
+    char buf[32];
+    int a = start, b = start + width;
+    while (a < b && line[a] == ' ') ++a;
+    while (b > a && line[b - 1] == ' ') --b;
+    if (b <= a || b - a >= (int)sizeof(buf)) return false;
+    std::memcpy(buf, line + a, (size_t)(b - a));
+    buf[b - a] = '\0';
+    char* end = nullptr;
+    const double v = std::strtod(buf, &end);
+    if (end != buf + (b - a) || !std::isfinite(v)) return false;
+    *out = v;
+    return true;
+}
+}  // namespace
+
+extern "C" int64_t bqp_frame_eop_from_finals(const char* text, int64_t len, int64_t cap, int32_t* first_mjd,
+                                             double* records) {
+    if (!text || len < 0 || !first_mjd) return -1;
+    std::map<int32_t, std::array<double, 5>> rows;
+    int64_t pos = 0;
+    while (pos < len) {
+        int64_t end = pos;
+        while (end < len && text[end] != '\n') ++end;
+        const int64_t n = end - pos - ((end > pos && text[end - 1] == '\r') ? 1 : 0);
+        if (n >= 125) {
+            const char* ln = text + pos;
+            double mjd, v[5];
+            const bool flags = (ln[16] == 'I' || ln[16] == 'P') && (ln[57] == 'I' || ln[57] == 'P') &&
+                               (ln[95] == 'I' || ln[95] == 'P');
+            if (flags && fixed_field(ln, 7, 8, &mjd) && mjd == std::floor(mjd) && fixed_field(ln, 18, 9, &v[0]) &&
+                fixed_field(ln, 37, 9, &v[1]) && fixed_field(ln, 58, 10, &v[2]) && fixed_field(ln, 97, 9, &v[3]) &&
+                fixed_field(ln, 116, 9, &v[4])) {
+                const int32_t m = (int32_t)mjd;
+                if (rows.count(m)) return -3;  // a day given twice
+                rows[m] = {v[0], v[1], v[2], v[3], v[4]};
+            }
+        }
+        pos = end + 1;
+    }
+    if (rows.empty()) return 0;
+    const int32_t first = rows.begin()->first;
+    int64_t count = 0;
+    for (auto it = rows.begin(); it != rows.end() && it->first == first + count; ++it) ++count;
+    *first_mjd = first;
+    if (!records || cap < count) return count;
+    int64_t i = 0;
+    for (auto it = rows.begin(); i < count; ++it, ++i)
+        for (int q = 0; q < 5; ++q) records[i * 5 + q] = it->second[q];
+    return count;
+}

@@ -8,7 +8,7 @@
 // attempt:
 //
 //   pl_prep<M>(s)   finish stage s-1, form y_s = y + h sum a_sj k_j, the Encke
-//                   baseline (Kepler solve), GMST rotation, Sun/Moon third body
+//                   baseline (Kepler solve), Earth rotation, Sun/Moon third body
 //                   and Battin's term                       (latency / SFU bound)
 //   pl_gravity      normalised column recursion, table in shared memory,
 //                   one trajectory per thread               (FP64-FMA bound)

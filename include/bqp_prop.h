@@ -301,6 +301,14 @@ int bqp_frame_derivatives(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t m
  * instants (1 and NaN rows outside the span); segments: the keys and
  * [count][60] segments (M0..M2, K0..K2, theta cubic, centre, TAI - UTC)
  * holding [lo, hi], or -1 when more than cap. */
+/* EOP records from IERS finals2000A text, by the reference's column rules
+ * (frame_time/eop.rs load_eop): rows of >= 125 characters with I/P flags at
+ * 16, 57, 95; x_p, y_p, UT1-UTC, dX, dY read from their fixed columns;
+ * incomplete rows skipped.  Returns the length of the contiguous run of days
+ * from the first complete one (*first_mjd its MJD), writing records [count][5]
+ * when cap >= count (records NULL: size query); -3 for a day given twice. */
+int64_t bqp_frame_eop_from_finals(const char* text, int64_t len, int64_t cap, int32_t* first_mjd,
+                                  double* records);
 typedef struct bqp_frame_authority bqp_frame_authority;
 bqp_frame_authority* bqp_frame_authority_new(const double* eop, int32_t first_mjd, int32_t n_eop);
 void bqp_frame_authority_free(bqp_frame_authority* h);

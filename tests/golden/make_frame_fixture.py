@@ -22,7 +22,8 @@ frame chain -- nothing is recomputed here:
   (``authority.rs`` segment_cache_matches_the_exact_chain_within_the_
   declared_bound) ten consecutive records of the sealed ``eop_table.bin``
   (five little-endian binary64 per UTC day from MJD 41684) around each, and
-  the same days from ``finals2000A.all``.
+  the same days from ``finals2000A.all``, as numbers and as the raw text
+  lines (the input of the library's finals reader).
 
 Bounds stay in the tests that read the file; binary64 values are stored as
 hex strings.
@@ -67,6 +68,15 @@ def bits_in(src, fn_name):
     return ["0x" + h.replace("_", "") for h in re.findall(r"from_bits\(0x([0-9a-f_]+)\)", body)]
 
 
+def finals_lines(text):
+    """Raw text line of each MJD that has one of 125 characters or more."""
+    lines = {}
+    for line in text.splitlines():
+        if len(line) >= 125:
+            lines[int(float(line[7:15]))] = line
+    return lines
+
+
 def finals_rows(text):
     rows = {}
     for line in text.splitlines():
@@ -103,6 +113,7 @@ def main(ref_root=None):
 
     fixture = json.loads((root / FIXTURE).read_text())
     finals = finals_rows((root / FINALS).read_text())
+    raw = finals_lines((root / FINALS).read_text())
     cases = []
     for c in fixture["cases"]:
         y, m, d, hh, mi, ss = EPOCHS[c["epoch_utc"]]
@@ -125,7 +136,8 @@ def main(ref_root=None):
             off = (k - SEALED_FIRST_MJD) * 40
             rec.append([h64(v) for v in struct.unpack("<5d", sealed[off:off + 40])])
         auth.append({"epoch": [y, m, d, hh, mi, ss], "first_mjd": first, "sealed": rec,
-                     "finals": [[h64(v) for v in finals[k]] for k in range(first, first + 10)]})
+                     "finals": [[h64(v) for v in finals[k]] for k in range(first, first + 10)],
+                     "finals_lines": [raw[k] for k in range(first, first + 10)]})
 
     out = {
         "source": "tdude78/bqp dust_transfer satpy_core frame_time (ERFA 2.0.1 / SOFA 20231011-derived)",

@@ -333,3 +333,29 @@ def test_staircase_costs_steps_at_the_tightest_tolerance():
         ev[eps] = (e1.sum(), e2.sum())
     assert ev[1e-12][1] < 0.8 * ev[1e-12][0], ev
     assert abs(ev[1e-10][1] - ev[1e-10][0]) < 0.05 * ev[1e-10][0], ev
+
+
+def test_finals_text_reader():
+    """IERS finals2000A lines -> the sealed table's records (the reference's
+    own lines and values), contiguity, skipped incomplete rows, duplicates."""
+    for entry in GOLD["authority"]:
+        text = "\n".join(entry["finals_lines"]) + "\n"
+        rec, first = N.eop_from_finals(text)
+        assert first == entry["first_mjd"] and rec.shape == (10, 5)
+        assert np.array_equal(rec, hxa(np.ravel(entry["sealed"])).reshape(-1, 5))
+        # CRLF line ends, and a header line, read the same
+        rec2, _ = N.eop_from_finals("header\r\n" + text.replace("\n", "\r\n"))
+        assert np.array_equal(rec, rec2)
+    lines = GOLD["authority"][0]["finals_lines"]
+    # a day whose dY field is blank ends the contiguous run
+    broken = list(lines)
+    broken[6] = broken[6][:116] + " " * 9 + broken[6][125:]
+    rec, first = N.eop_from_finals("\n".join(broken))
+    assert rec.shape == (6, 5) and first == GOLD["authority"][0]["first_mjd"]
+    # a bad flag is skipped the same way; a day given twice is refused
+    bad = list(lines)
+    bad[3] = bad[3][:16] + "X" + bad[3][17:]
+    assert N.eop_from_finals("\n".join(bad))[0].shape == (3, 5)
+    with pytest.raises(ValueError):
+        N.eop_from_finals("\n".join(lines + lines[:1]))
+    assert N.eop_from_finals("")[0].shape == (0, 5)
