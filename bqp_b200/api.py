@@ -18,6 +18,13 @@ Options this build does not implement raise ``ValueError`` naming the option
 (the tsit5/rkv98 tableaus, SRP with the dopri5 compatibility stepper or
 rtol/atol control); they are never silently replaced.  ``gravity_field`` (extra keyword) takes a normalised
 ``deg ord C S`` text or a path, which lifts the embedded field's degree-15 cap.
+
+Extra keywords for the inputs the reference reads from its own tree:
+``space_weather`` (SET SOLFSMY / DTCFILE), ``ephemeris`` (Sun / Moon "DUST"
+catalogues) and ``eop`` (the sealed EOP table or IERS finals2000A text) for
+the Earth-fixed frame, which is the reference's IAU 2006/2000A chain
+(``frame="iau2006"``, the default; zero EOP without ``eop``) or the GMST
+z-rotation (``frame="gmst"``).
 """
 from __future__ import annotations
 
@@ -170,7 +177,8 @@ def _frame(frame, eop):
     """(frame name, EOP records [n][5] or None, first MJD) of frame= / eop=.
     eop: None (zero EOP), the bytes or path of a sealed EOP table (five
     little-endian binary64 per UTC day from MJD 41684, the reference's
-    frame_time/eop_table.bin), or (records [n][5], first_mjd)."""
+    frame_time/eop_table.bin) or of IERS finals2000A text (told apart by
+    being ASCII lines), or (records [n][5], first_mjd)."""
     if frame not in N.FRAMES:
         raise ValueError(f"frame must be one of {sorted(N.FRAMES)}, got {frame!r}")
     if eop is None:
@@ -181,6 +189,12 @@ def _frame(frame, eop):
         rec = np.asarray(eop[0], dtype=np.float64).reshape(-1, 5)
         return frame, rec, int(eop[1])
     data = N._file_bytes(eop)
+    head = data[:4096]
+    if b"\n" in head and head.isascii():
+        rec, first = N.eop_from_finals(data)
+        if rec.shape[0] == 0:
+            raise ValueError("no complete finals2000A row in the EOP text")
+        return frame, rec, first
     if len(data) % 40:
         raise ValueError("a sealed EOP table holds 40-byte records")
     return frame, np.frombuffer(data, dtype="<f8").reshape(-1, 5).astype(np.float64), 41684

@@ -207,6 +207,12 @@ def test_python_frame_arguments():
     assert np.array_equal(got, rec) and first == 41684
     with pytest.raises(ValueError):
         api._frame("iau2006", b"\0" * 41)  # not whole records
+    # IERS finals2000A text (the reference's own lines) is read as such
+    entry = GOLD["authority"][0]
+    name, got, first = api._frame("iau2006", ("\n".join(entry["finals_lines"]) + "\n").encode())
+    assert first == entry["first_mjd"] and np.array_equal(got, hxa(np.ravel(entry["sealed"])).reshape(-1, 5))
+    with pytest.raises(ValueError):
+        api._frame("iau2006", b"no finals rows here\n")
     with pytest.raises(ValueError):
         api._frame("gmst", (rec, 60300))  # EOP belong to the IAU frame
     with pytest.raises(ValueError):
