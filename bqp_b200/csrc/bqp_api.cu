@@ -633,7 +633,7 @@ ForceParams force_params(const bqp_ctx* ctx) {
 // side), built on the host (kept by the authority) and copied to the device
 // sorted by key.  Rows whose instants have no segment fail on the device
 // with the frame-time status.  Host arrays.
-int frame_prepare_host(bqp_ctx* ctx, int64_t n, const double* epoch, const double* lo, const double* hi) {
+int frame_prepare_host_impl(bqp_ctx* ctx, int64_t n, const double* epoch, const double* lo, const double* hi) {
     if (!ctx->frame) {
         ctx->ftab = ft::FrameTab{};
         return 0;
@@ -702,6 +702,16 @@ int frame_prepare_host(bqp_ctx* ctx, int64_t n, const double* epoch, const doubl
     return 0;
 }
 
+// The host side builds with standard containers and threads: a failure to
+// allocate comes back as a status, not as an exception through the C ABI.
+int frame_prepare_host(bqp_ctx* ctx, int64_t n, const double* epoch, const double* lo, const double* hi) {
+    try {
+        return frame_prepare_host_impl(ctx, n, epoch, lo, hi);
+    } catch (const std::exception& e) {
+        return fail(BQP_E_NOMEM, "frame segments: %s", e.what());
+    }
+}
+
 // The same for device arrays of epochs and end times (start d_t0 per row,
 // or the common t0 when it is null).
 int frame_prepare_dev(bqp_ctx* ctx, int64_t n, const double* d_epoch, double t0, const double* d_tf,
@@ -711,7 +721,14 @@ int frame_prepare_dev(bqp_ctx* ctx, int64_t n, const double* d_epoch, double t0,
         return 0;
     }
     if (ctx->frame_span) return 0;  // no readback: the preset span's table stands
-    std::vector<double> ep((size_t)n), tf((size_t)n), lo((size_t)n, t0);
+    std::vector<double> ep, tf, lo;
+    try {
+        ep.resize((size_t)n);
+        tf.resize((size_t)n);
+        lo.assign((size_t)n, t0);
+    } catch (const std::exception& ex) {
+        return fail(BQP_E_NOMEM, "frame span readback: %s", ex.what());
+    }
     cudaError_t e = cudaSuccess;
     if (n > 0 && d_t0) e = cudaMemcpyAsync(lo.data(), d_t0, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && n > 0)
@@ -1376,12 +1393,16 @@ int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t fir
         for (int64_t i = 0; i < (int64_t)n_records * 5; ++i)
             if (!std::isfinite(eop[i])) return fail(BQP_E_ARG, "EOP record %lld is not finite", (long long)(i / 5));
     }
-    ft::Eop e;
-    if (n_records > 0) {
-        e.first_mjd = first_mjd;
-        e.rec.assign(eop, eop + (size_t)n_records * 5);
+    try {
+        ft::Eop e;
+        if (n_records > 0) {
+            e.first_mjd = first_mjd;
+            e.rec.assign(eop, eop + (size_t)n_records * 5);
+        }
+        ctx->frame.reset(new ft::Authority(e));
+    } catch (const std::exception& ex) {
+        return fail(BQP_E_NOMEM, "frame authority: %s", ex.what());
     }
-    ctx->frame.reset(new ft::Authority(e));
     ctx->ftab = ft::FrameTab{};
     ctx->frame_span = false;
     return 0;

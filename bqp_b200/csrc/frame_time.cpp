@@ -11,6 +11,7 @@
 #include "frame_time_host.h"
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cstdlib>
 #include <cmath>
@@ -751,16 +752,23 @@ void Authority::ensure(const std::vector<std::pair<int32_t, int64_t>>& want, std
         std::vector<char> ok(todo.size(), 0);
         const size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
                                            std::max<size_t>(1, todo.size() / 8));
-        auto work = [&](size_t w) {
-            for (size_t i = w; i < todo.size(); i += nt) ok[i] = build(todo[i].first, todo[i].second, &segs[i]);
+        // workers take segments from a shared counter; the calling thread
+        // works too, so a thread that cannot be started costs only speed
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            for (size_t i; (i = next.fetch_add(1)) < todo.size();)
+                ok[i] = build(todo[i].first, todo[i].second, &segs[i]);
         };
-        if (nt <= 1) {
-            work(0);
-        } else {
-            std::vector<std::thread> th;
-            for (size_t w = 0; w < nt; ++w) th.emplace_back(work, w);
-            for (auto& t : th) t.join();
+        std::vector<std::thread> th;
+        for (size_t w = 1; w < nt; ++w) {
+            try {
+                th.emplace_back(work);
+            } catch (...) {
+                break;
+            }
         }
+        work();
+        for (auto& t : th) t.join();
         std::lock_guard<std::mutex> g(mu_);
         for (size_t i = 0; i < todo.size(); ++i) {
             const int64_t key = seg_key(todo[i].first, todo[i].second);
@@ -833,14 +841,22 @@ static Eop make_eop(const double* eop, int32_t first_mjd, int32_t n) {
 int bqp_frame_matrix(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
                      double offset, const double* eop, int32_t first_mjd, int32_t n_eop, double* r) {
     if (!r || (policy != 0 && policy != 1)) return -1;
-    return frame_matrix(y, m, d, hh, mm, ss, policy, offset, make_eop(eop, first_mjd, n_eop), r, nullptr);
+    try {
+        return frame_matrix(y, m, d, hh, mm, ss, policy, offset, make_eop(eop, first_mjd, n_eop), r, nullptr);
+    } catch (...) {
+        return -5;
+    }
 }
 
 int bqp_frame_derivatives(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
                           double h, const double* eop, int32_t first_mjd, int32_t n_eop, double* r, double* rdot,
                           double* rddot) {
     if (!r || !rdot || !rddot || (policy != 0 && policy != 1) || !(h > 0.0)) return -1;
-    return frame_derivatives(y, m, d, hh, mm, ss, policy, h, make_eop(eop, first_mjd, n_eop), r, rdot, rddot);
+    try {
+        return frame_derivatives(y, m, d, hh, mm, ss, policy, h, make_eop(eop, first_mjd, n_eop), r, rdot, rddot);
+    } catch (...) {
+        return -5;
+    }
 }
 
 }  // extern "C"
@@ -883,22 +899,26 @@ int bqp_frame_authority_intervals(const bqp_frame_authority* h, double* out) {
 // (or whose segment does not build) get NaN and make the return 1.
 int bqp_frame_authority_rotation(bqp_frame_authority* h, int64_t n, const double* tai, double* r, double* w) {
     if (!h || n < 0 || (n > 0 && (!tai || !r || !w))) return -1;
-    int bad = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        FrameSeg s;
-        int64_t key;
-        if (!h->a.segment(tai[i], &key, &s)) {
-            for (int e = 0; e < 9; ++e) r[i * 9 + e] = NAN;
-            for (int e = 0; e < 3; ++e) w[i * 3 + e] = NAN;
-            bad = 1;
-            continue;
+    try {
+        int bad = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            FrameSeg s;
+            int64_t key;
+            if (!h->a.segment(tai[i], &key, &s)) {
+                for (int e = 0; e < 9; ++e) r[i * 9 + e] = NAN;
+                for (int e = 0; e < 3; ++e) w[i * 3 + e] = NAN;
+                bad = 1;
+                continue;
+            }
+            FrameRot fr;
+            rotation_at(s, tai[i], fr);
+            for (int e = 0; e < 9; ++e) r[i * 9 + e] = fr.r[e];
+            for (int e = 0; e < 3; ++e) w[i * 3 + e] = fr.w[e];
         }
-        FrameRot fr;
-        rotation_at(s, tai[i], fr);
-        for (int e = 0; e < 9; ++e) r[i * 9 + e] = fr.r[e];
-        for (int e = 0; e < 3; ++e) w[i * 3 + e] = fr.w[e];
+        return bad;
+    } catch (...) {
+        return -5;
     }
-    return bad;
 }
 
 // The segments holding [lo, hi]: keys [cap] and segments [cap][60] (M0..M2,
@@ -907,18 +927,22 @@ int bqp_frame_authority_rotation(bqp_frame_authority* h, int64_t n, const double
 int64_t bqp_frame_authority_segments(bqp_frame_authority* h, double lo, double hi, int64_t cap, int64_t* keys,
                                      double* segs) {
     if (!h || cap < 0) return -1;
-    std::vector<std::pair<int32_t, int64_t>> want;
-    h->a.keys_between(lo, hi, &want);
-    std::vector<int64_t> k;
-    std::vector<FrameSeg> s;
-    h->a.ensure(want, &k, &s);
-    if ((int64_t)k.size() > cap || (!k.empty() && (!keys || !segs))) return -1;
-    static_assert(sizeof(FrameSeg) == 60 * sizeof(double), "segment layout");
-    for (size_t i = 0; i < k.size(); ++i) {
-        keys[i] = k[i];
-        std::memcpy(segs + i * 60, &s[i], sizeof(FrameSeg));
+    try {
+        std::vector<std::pair<int32_t, int64_t>> want;
+        h->a.keys_between(lo, hi, &want);
+        std::vector<int64_t> k;
+        std::vector<FrameSeg> s;
+        h->a.ensure(want, &k, &s);
+        if ((int64_t)k.size() > cap || (!k.empty() && (!keys || !segs))) return -1;
+        static_assert(sizeof(FrameSeg) == 60 * sizeof(double), "segment layout");
+        for (size_t i = 0; i < k.size(); ++i) {
+            keys[i] = k[i];
+            std::memcpy(segs + i * 60, &s[i], sizeof(FrameSeg));
+        }
+        return (int64_t)k.size();
+    } catch (...) {
+        return -5;
     }
-    return (int64_t)k.size();
 }
 
 }  // extern "C"
@@ -950,35 +974,39 @@ bool fixed_field(const char* line, int start, int width, double* out) {
 extern "C" int64_t bqp_frame_eop_from_finals(const char* text, int64_t len, int64_t cap, int32_t* first_mjd,
                                              double* records) {
     if (!text || len < 0 || !first_mjd) return -1;
-    std::map<int32_t, std::array<double, 5>> rows;
-    int64_t pos = 0;
-    while (pos < len) {
-        int64_t end = pos;
-        while (end < len && text[end] != '\n') ++end;
-        const int64_t n = end - pos - ((end > pos && text[end - 1] == '\r') ? 1 : 0);
-        if (n >= 125) {
-            const char* ln = text + pos;
-            double mjd, v[5];
-            const bool flags = (ln[16] == 'I' || ln[16] == 'P') && (ln[57] == 'I' || ln[57] == 'P') &&
-                               (ln[95] == 'I' || ln[95] == 'P');
-            if (flags && fixed_field(ln, 7, 8, &mjd) && mjd == std::floor(mjd) && fixed_field(ln, 18, 9, &v[0]) &&
-                fixed_field(ln, 37, 9, &v[1]) && fixed_field(ln, 58, 10, &v[2]) && fixed_field(ln, 97, 9, &v[3]) &&
-                fixed_field(ln, 116, 9, &v[4])) {
-                const int32_t m = (int32_t)mjd;
-                if (rows.count(m)) return -3;  // a day given twice
-                rows[m] = {v[0], v[1], v[2], v[3], v[4]};
+    try {
+        std::map<int32_t, std::array<double, 5>> rows;
+        int64_t pos = 0;
+        while (pos < len) {
+            int64_t end = pos;
+            while (end < len && text[end] != '\n') ++end;
+            const int64_t n = end - pos - ((end > pos && text[end - 1] == '\r') ? 1 : 0);
+            if (n >= 125) {
+                const char* ln = text + pos;
+                double mjd, v[5];
+                const bool flags = (ln[16] == 'I' || ln[16] == 'P') && (ln[57] == 'I' || ln[57] == 'P') &&
+                                   (ln[95] == 'I' || ln[95] == 'P');
+                if (flags && fixed_field(ln, 7, 8, &mjd) && mjd == std::floor(mjd) && fixed_field(ln, 18, 9, &v[0]) &&
+                    fixed_field(ln, 37, 9, &v[1]) && fixed_field(ln, 58, 10, &v[2]) && fixed_field(ln, 97, 9, &v[3]) &&
+                    fixed_field(ln, 116, 9, &v[4])) {
+                    const int32_t m = (int32_t)mjd;
+                    if (rows.count(m)) return -3;  // a day given twice
+                    rows[m] = {v[0], v[1], v[2], v[3], v[4]};
+                }
             }
+            pos = end + 1;
         }
-        pos = end + 1;
+        if (rows.empty()) return 0;
+        const int32_t first = rows.begin()->first;
+        int64_t count = 0;
+        for (auto it = rows.begin(); it != rows.end() && it->first == first + count; ++it) ++count;
+        *first_mjd = first;
+        if (!records || cap < count) return count;
+        int64_t i = 0;
+        for (auto it = rows.begin(); i < count; ++it, ++i)
+            for (int q = 0; q < 5; ++q) records[i * 5 + q] = it->second[q];
+        return count;
+    } catch (...) {
+        return -5;
     }
-    if (rows.empty()) return 0;
-    const int32_t first = rows.begin()->first;
-    int64_t count = 0;
-    for (auto it = rows.begin(); it != rows.end() && it->first == first + count; ++it) ++count;
-    *first_mjd = first;
-    if (!records || cap < count) return count;
-    int64_t i = 0;
-    for (auto it = rows.begin(); i < count; ++it, ++i)
-        for (int q = 0; q < 5; ++q) records[i * 5 + q] = it->second[q];
-    return count;
 }

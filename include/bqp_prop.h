@@ -266,7 +266,9 @@ int bqp_ctx_set_frame(bqp_ctx* ctx, int32_t mode, const double* eop, int32_t fir
  * segments per call. */
 int bqp_ctx_set_frame_span(bqp_ctx* ctx, double utc_jd_lo, double utc_jd_hi);
 
-/* The chain's pieces on the host (no GPU), ERFA-restated (frame_time/
+/* The host functions below return -5 (NULL for _new) when host memory
+ * cannot be had.
+ * The chain's pieces on the host (no GPU), ERFA-restated (frame_time/
  * iau2006.rs, cio.rs, era.rs): dates are two-part TT Julian days (UT1 for
  * era).  nut: out[2] = dpsi, deps of IAU 2000A (iau2006 0) or 2006/2000A (1);
  * pfw06: out[4] = gamb, phib, psib, epsa; xys06a: out[3] = X, Y, s; c2ixys
