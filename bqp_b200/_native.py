@@ -146,6 +146,8 @@ SIGNATURES = [
     ("bqp_frame_derivatives", C.c_int, [C.c_int32] * 5 + [C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
                                                            C.c_int32, _dp, _dp, _dp]),
     ("bqp_frame_eop_from_finals", C.c_int64, [C.c_char_p, C.c_int64, C.c_int64, _ip, _dp]),
+    ("bqp_frame_transform_state", C.c_int, [C.c_int32] * 5 + [C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
+                                                               C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp]),
     ("bqp_frame_authority_new", _vp, [_dp, C.c_int32, C.c_int32]),
     ("bqp_frame_authority_free", None, [_vp]),
     ("bqp_frame_authority_intervals", C.c_int, [_vp, _dp]),
@@ -700,6 +702,20 @@ def frame_derivatives(epoch, policy=0, h=0.25, eop=None, first_mjd=0):
     if rc != 0:
         raise ValueError(f"frame chain failed ({rc})")
     return r.reshape(3, 3), rd.reshape(3, 3), rdd.reshape(3, 3)
+
+
+def frame_transform_state(epoch, r, v, a, policy=0, h=0.25, eop=None, first_mjd=0):
+    """A GCRS position, velocity and acceleration in ITRS at a UTC calendar
+    instant (y, m, d, hh, mm, ss), through the exact chain's stencil."""
+    e, f, n = _eop_args(eop, first_mjd)
+    rv, vv, av = f64(r).reshape(3), f64(v).reshape(3), f64(a).reshape(3)
+    ro, vo, ao = np.zeros(3), np.zeros(3), np.zeros(3)
+    rc = lib().bqp_frame_transform_state(*[int(x) for x in epoch[:5]], float(epoch[5]), int(policy), float(h),
+                                         None if e is None else dptr(e), f, n, dptr(rv), dptr(vv), dptr(av),
+                                         dptr(ro), dptr(vo), dptr(ao))
+    if rc != 0:
+        raise ValueError(f"frame chain failed ({rc})")
+    return ro, vo, ao
 
 
 def eop_from_finals(finals):

@@ -527,8 +527,12 @@ int frame_matrix(int iy, int im, int id, int ihr, int imn, double sec, int polic
     return 0;
 }
 
-int frame_derivatives(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h,
-                      const Eop& eop, Mat3 r, Mat3 rdot, Mat3 rddot) {
+namespace {
+
+// R, Rdot, Rddot in pairs from the centred five-point stencil of step h
+// (chain.rs:299-360).
+int derivatives_dd(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h, const Eop& eop,
+                   DdMat r, DdMat rdot, DdMat rddot) {
     DdMat smp[5];
     for (int q = 0; q < 5; ++q) {
         const int rc = frame_matrix_dd(iy, im, id, ihr, imn, sec, policy, (double)(q - 2) * h, eop, smp[q]);
@@ -539,9 +543,48 @@ int frame_derivatives(int iy, int im, int id, int ihr, int imn, double sec, int 
         const Dd near = dd_sub(p1, m1), far = dd_sub(p2, m2);
         const Dd near2 = dd_add(dd_sub(p1, v), dd_sub(m1, v));
         const Dd far2 = dd_add(dd_sub(p2, v), dd_sub(m2, v));
-        r[e] = dd_f64(v);
-        rdot[e] = dd_f64(dd_div(dd_sub(dd_scale(near, 8.0), far), dd_from(12.0 * h)));
-        rddot[e] = dd_f64(dd_div(dd_sub(dd_scale(near2, 16.0), far2), dd_from(12.0 * h * h)));
+        r[e] = v;
+        rdot[e] = dd_div(dd_sub(dd_scale(near, 8.0), far), dd_from(12.0 * h));
+        rddot[e] = dd_div(dd_sub(dd_scale(near2, 16.0), far2), dd_from(12.0 * h * h));
+    }
+    return 0;
+}
+
+}  // namespace
+
+int frame_derivatives(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h,
+                      const Eop& eop, Mat3 r, Mat3 rdot, Mat3 rddot) {
+    DdMat a, b, c;
+    const int rc = derivatives_dd(iy, im, id, ihr, imn, sec, policy, h, eop, a, b, c);
+    if (rc < 0) return rc;
+    for (int e = 0; e < 9; ++e) {
+        r[e] = dd_f64(a[e]);
+        rdot[e] = dd_f64(b[e]);
+        rddot[e] = dd_f64(c[e]);
+    }
+    return 0;
+}
+
+// A GCRS state (position, velocity, acceleration) in ITRS through R, Rdot
+// and Rddot, summed in pairs (chain.rs transform_state):
+//   r' = R r,  v' = R v + Rdot r,  a' = R a + 2 Rdot v + Rddot r.
+int frame_transform_state(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h,
+                          const Eop& eop, const double* r, const double* v, const double* a, double* ro,
+                          double* vo, double* ao) {
+    DdMat R, Rd, Rdd;
+    const int rc = derivatives_dd(iy, im, id, ihr, imn, sec, policy, h, eop, R, Rd, Rdd);
+    if (rc < 0) return rc;
+    for (int i = 0; i < 3; ++i) {
+        Dd p = dd_from(0.0), q = dd_from(0.0), w = dd_from(0.0);
+        for (int j = 0; j < 3; ++j) {
+            const int e = 3 * i + j;
+            p = dd_add(p, dd_scale(R[e], r[j]));
+            q = dd_add(q, dd_add(dd_scale(R[e], v[j]), dd_scale(Rd[e], r[j])));
+            w = dd_add(w, dd_add(dd_add(dd_scale(R[e], a[j]), dd_scale(Rd[e], 2.0 * v[j])), dd_scale(Rdd[e], r[j])));
+        }
+        ro[i] = dd_f64(p);
+        vo[i] = dd_f64(q);
+        ao[i] = dd_f64(w);
     }
     return 0;
 }
@@ -843,6 +886,18 @@ int bqp_frame_matrix(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, do
     if (!r || (policy != 0 && policy != 1)) return -1;
     try {
         return frame_matrix(y, m, d, hh, mm, ss, policy, offset, make_eop(eop, first_mjd, n_eop), r, nullptr);
+    } catch (...) {
+        return -5;
+    }
+}
+
+int bqp_frame_transform_state(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
+                              double h, const double* eop, int32_t first_mjd, int32_t n_eop, const double* r,
+                              const double* v, const double* a, double* r_out, double* v_out, double* a_out) {
+    if (!r || !v || !a || !r_out || !v_out || !a_out || (policy != 0 && policy != 1) || !(h > 0.0)) return -1;
+    try {
+        return frame_transform_state(y, m, d, hh, mm, ss, policy, h, make_eop(eop, first_mjd, n_eop), r, v, a,
+                                     r_out, v_out, a_out);
     } catch (...) {
         return -5;
     }

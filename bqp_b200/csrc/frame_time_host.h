@@ -50,6 +50,12 @@ int frame_matrix(int iy, int im, int id, int ihr, int imn, double sec, int polic
 int frame_derivatives(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h,
                       const Eop& eop, Mat3 r, Mat3 rdot, Mat3 rddot);
 
+// A GCRS position, velocity and acceleration in ITRS through that stencil's
+// R, Rdot, Rddot, summed in pairs (chain.rs transform_state).
+int frame_transform_state(int iy, int im, int id, int ihr, int imn, double sec, int policy, double h,
+                          const Eop& eop, const double* r, const double* v, const double* a, double* ro,
+                          double* vo, double* ao);
+
 // The segment authority over one EOP table (authority.rs:355-650).
 class Authority {
 public:

@@ -303,6 +303,12 @@ int bqp_frame_derivatives(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t m
  * instants (1 and NaN rows outside the span); segments: the keys and
  * [count][60] segments (M0..M2, K0..K2, theta cubic, centre, TAI - UTC)
  * holding [lo, hi], or -1 when more than cap. */
+/* A GCRS position (km), velocity and acceleration in ITRS through the
+ * stencil's R, Rdot, Rddot, summed in double-double (chain.rs
+ * transform_state): r' = R r, v' = R v + Rdot r, a' = R a + 2 Rdot v + Rddot r. */
+int bqp_frame_transform_state(int32_t y, int32_t m, int32_t d, int32_t hh, int32_t mm, double ss, int32_t policy,
+                              double h, const double* eop, int32_t first_mjd, int32_t n_eop, const double* r,
+                              const double* v, const double* a, double* r_out, double* v_out, double* a_out);
 /* EOP records from IERS finals2000A text, by the reference's column rules
  * (frame_time/eop.rs load_eop): rows of >= 125 characters with I/P flags at
  * 16, 57, 95; x_p, y_p, UT1-UTC, dX, dY read from their fixed columns;

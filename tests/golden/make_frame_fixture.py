@@ -13,7 +13,8 @@ frame chain -- nothing is recomputed here:
   gate 4 (c2ixys, sp00, pom00) and ``era.rs`` gate 2 (era00).
 * ``cases``: the 20 cases of ``satpy_core/tests/data/erfa_sofa_derived_
   frame_time_v1.json`` (five UTC epochs, zero and real EOP): R, Rdot and
-  Rddot of GCRS->ITRS from the five-point stencil with h = 0.25 s, and for
+  Rddot of GCRS->ITRS from the five-point stencil with h = 0.25 s, a GCRS
+  position / velocity / acceleration and its ITRS image, and for
   the real-EOP cases the four ``finals2000A.all`` records (MJD centre-1 ..
   centre+2) the chain interpolates, read with the reference's column rules
   (``frame_time/eop.rs`` load_eop: MJD 7..15, x_p 18..27, y_p 37..46,
@@ -124,6 +125,8 @@ def main(ref_root=None):
             "eop_first_mjd": centre - 1 if real else 0,
             "eop": [[h64(v) for v in finals[k]] for k in range(centre - 1, centre + 3)] if real else [],
             "R": c["R_gcrs_to_itrs"], "Rdot": c["Rdot_s1"], "Rddot": c["Rddot_s2"],
+            "r_gcrs": c["r_gcrs_km"], "v_gcrs": c["v_gcrs_km_s"], "a_gcrs": c["a_gcrs_km_s2"],
+            "r_itrs": c["r_itrs_km"], "v_itrs": c["v_itrs_km_s"], "a_itrs": c["a_itrs_km_s2"],
         })
     assert len(cases) == 20
 

@@ -365,3 +365,17 @@ def test_finals_text_reader():
     with pytest.raises(ValueError):
         N.eop_from_finals("\n".join(lines + lines[:1]))
     assert N.eop_from_finals("")[0].shape == (0, 5)
+
+
+@pytest.mark.parametrize("case", GOLD["cases"], ids=[c["id"] for c in GOLD["cases"]])
+def test_state_transform_matches_the_fixture(case):
+    """GCRS position / velocity / acceleration -> ITRS through R, Rdot, Rddot
+    (chain.rs transform_state) against the fixture's, under the reference's
+    state bounds (frame_time_oracle.rs:686-760: 1e-8 km, 2e-11 km/s,
+    3e-10 km/s^2)."""
+    eop = np.array([[hx(v) for v in row] for row in case["eop"]]).reshape(-1, 5)
+    r, v, a = N.frame_transform_state(case["epoch"], hxa(case["r_gcrs"]), hxa(case["v_gcrs"]), hxa(case["a_gcrs"]),
+                                      case["policy"], GOLD["stencil_h_s"], eop, case["eop_first_mjd"])
+    assert np.abs(r - hxa(case["r_itrs"])).max() <= 1e-8
+    assert np.abs(v - hxa(case["v_itrs"])).max() <= 2e-11
+    assert np.abs(a - hxa(case["a_itrs"])).max() <= 3e-10
