@@ -13,6 +13,7 @@ host, against the reference's recorded known answers
   (frame_time_oracle.rs:611-684).
 """
 import json
+import os
 import struct
 from pathlib import Path
 
@@ -379,3 +380,18 @@ def test_state_transform_matches_the_fixture(case):
     assert np.abs(r - hxa(case["r_itrs"])).max() <= 1e-8
     assert np.abs(v - hxa(case["v_itrs"])).max() <= 2e-11
     assert np.abs(a - hxa(case["a_itrs"])).max() <= 3e-10
+
+
+_REF = os.environ.get("BQP_REFERENCE_ROOT", "/nonexistent")
+_FINALS = Path(_REF) / "dust_transfer/assets/reference/frame_time/finals2000A.all"
+_SEALED = Path(_REF) / "dust_transfer/crates/satpy_core/src/frame_time/eop_table.bin"
+
+
+@pytest.mark.skipif(not (_FINALS.exists() and _SEALED.exists()), reason="reference tree not present")
+def test_finals_reader_rebuilds_the_sealed_table():
+    """The reference's whole finals2000A.all, read by the library, is its
+    sealed eop_table.bin bit for bit (19,645 days from MJD 41684)."""
+    rec, first = N.eop_from_finals(_FINALS)
+    sealed = np.frombuffer(_SEALED.read_bytes(), dtype="<f8").reshape(-1, 5)
+    assert first == 41684 and rec.shape == sealed.shape == (19645, 5)
+    assert np.array_equal(rec, sealed)
