@@ -188,7 +188,7 @@ def _frame(frame, eop):
     if isinstance(eop, tuple) and len(eop) == 2:
         rec = np.asarray(eop[0], dtype=np.float64).reshape(-1, 5)
         return frame, rec, int(eop[1])
-    data = N._file_bytes(eop)
+    data = eop.encode() if isinstance(eop, str) and "\n" in eop else N._file_bytes(eop)
     head = data[:4096]
     if b"\n" in head and head.isascii():
         rec, first = N.eop_from_finals(data)

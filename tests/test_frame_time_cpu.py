@@ -212,6 +212,8 @@ def test_python_frame_arguments():
     entry = GOLD["authority"][0]
     name, got, first = api._frame("iau2006", ("\n".join(entry["finals_lines"]) + "\n").encode())
     assert first == entry["first_mjd"] and np.array_equal(got, hxa(np.ravel(entry["sealed"])).reshape(-1, 5))
+    name, got2, _ = api._frame("iau2006", "\n".join(entry["finals_lines"]) + "\n")  # as str
+    assert np.array_equal(got2, got)
     with pytest.raises(ValueError):
         api._frame("iau2006", b"no finals rows here\n")
     with pytest.raises(ValueError):
