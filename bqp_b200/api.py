@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import hashlib
 import time
+import warnings
 from collections import OrderedDict
 from pathlib import Path
 
@@ -173,15 +174,24 @@ def _ephemeris(ephemeris):
     return out
 
 
+_ZERO_EOP_WARNED = False  # the zero-EOP notice is given once per process
+
+
 def _frame(frame, eop):
     """(frame name, EOP records [n][5] or None, first MJD) of frame= / eop=.
     eop: None (zero EOP), the bytes or path of a sealed EOP table (five
     little-endian binary64 per UTC day from MJD 41684, the reference's
     frame_time/eop_table.bin) or of IERS finals2000A text (told apart by
     being ASCII lines), or (records [n][5], first_mjd)."""
+    global _ZERO_EOP_WARNED
     if frame not in N.FRAMES:
         raise ValueError(f"frame must be one of {sorted(N.FRAMES)}, got {frame!r}")
     if eop is None:
+        if frame == "iau2006" and not _ZERO_EOP_WARNED:
+            _ZERO_EOP_WARNED = True
+            warnings.warn("the IAU 2006/2000A frame runs with zero EOP (UT1-UTC = polar motion = 0): pass "
+                          "eop= the reference's eop_table.bin or IERS finals2000A text for its Earth orientation",
+                          UserWarning, stacklevel=4)
         return frame, None, 41684
     if frame != "iau2006":
         raise ValueError("eop is for frame='iau2006'")

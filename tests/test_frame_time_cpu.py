@@ -199,7 +199,15 @@ def test_python_frame_arguments():
     """frame= / eop= of the Python calls, parsed without a GPU."""
     from bqp_b200 import api
 
-    assert api._frame("iau2006", None)[0] == "iau2006" and api._frame("gmst", None)[1] is None
+    api._ZERO_EOP_WARNED = False
+    with pytest.warns(UserWarning, match="zero EOP"):
+        assert api._frame("iau2006", None)[0] == "iau2006"
+    import warnings
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")  # once per process
+        assert api._frame("iau2006", None)[1] is None
+    assert api._frame("gmst", None)[1] is None
     rec = np.arange(20.0).reshape(4, 5)
     name, got, first = api._frame("iau2006", (rec, 60300))
     assert np.array_equal(got, rec) and first == 60300
