@@ -390,7 +390,8 @@ int bqp_propagate_final_device(bqp_ctx* ctx, int64_t n, const double* in,
  * field: a context configured for split precision, the learned surrogate or
  * the FP32 density (forms only the stage-synchronous engine runs), or for
  * binary-eclipse SRP (whose per-row coordinator state the fixed array has
- * no room for), is refused with BQP_E_UNSUPPORTED.  The JB2008 sweep fits it uses are the ones the
+ * no room for), or for the IAU frame (whose segment table is built per call),
+ * is refused with BQP_E_UNSUPPORTED.  The JB2008 sweep fits it uses are the ones the
  * context built when it was created or last reconfigured (bqp_ctx_set_config,
  * bqp_ctx_set_jb_drivers), so identical calls give identical bits whatever
  * was called in between.  With bqp_ctx_profile on, its kernel time counts
